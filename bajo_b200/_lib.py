@@ -1,0 +1,124 @@
+"""Loader for the C-ABI CUDA library ``libbajo_b200.so`` (ctypes).
+
+This is the only native code the package uses.  There is no CPU fallback:
+if the shared object is missing, or a GPU entry point is called without a
+CUDA device, the call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbajo_b200.so")
+
+# status codes (include/bajo_b200.h)
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_WORKSPACE_TOO_SMALL = 2
+ERR_TOO_LARGE = 3
+ERR_CUDA = 4
+ERR_DEVICE = 5
+STATUS_LOOKBACK_TIMEOUT = 0x1
+STATUS_STACK_OVERFLOW = 0x2
+STATUS_BAD_TOPOLOGY = 0x4
+TRI_MT = 0
+TRI_WATERTIGHT = 1
+SORT_MAX_KEYS = (1 << 30) - 1
+
+_ERRORS = {
+    ERR_INVALID_ARGUMENT: "invalid argument",
+    ERR_WORKSPACE_TOO_SMALL: "workspace too small",
+    ERR_TOO_LARGE: "size exceeds the supported maximum",
+    ERR_CUDA: "CUDA error",
+    ERR_DEVICE: "device status error",
+}
+
+
+class BajoError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        super().__init__(f"{what}: {_ERRORS.get(code, 'error')} (code {code})")
+        self.code = code
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_I32 = ctypes.c_int32
+_SZ = ctypes.c_size_t
+_F = ctypes.c_float
+
+
+class BajoLbvhC(ctypes.Structure):
+    """Mirror of ``struct BajoLbvh`` (include/bajo_b200.h)."""
+    _fields_ = [
+        ("n_leaves", _U32), ("n_segments", _U32), ("seg_offsets", _P), ("internal_offsets", _P),
+        ("leaf_bounds", _P), ("seg_bounds", _P), ("sort_keys", _P), ("leaf_ids", _P), ("morton_codes", _P),
+        ("node_meta", _P), ("node_bounds", _P), ("node_leaf_counts", _P), ("node_flags", _P),
+        ("leaf_parent", _P), ("roots", _P), ("leaf_tris", _P),
+    ]
+
+
+LBVH_ARRAYS = ("internal_offsets", "leaf_bounds", "seg_bounds", "sort_keys", "leaf_ids", "morton_codes",
+               "node_meta", "node_bounds", "node_leaf_counts", "node_flags", "leaf_parent", "roots", "leaf_tris")
+
+
+class BajoLbvhSizesC(ctypes.Structure):
+    _fields_ = [(name, _SZ) for name in LBVH_ARRAYS] + [("workspace", _SZ)]
+
+
+# every symbol the header declares, with its ctypes signature
+SIGNATURES = {
+    "bajo_workspace_status": (_I32, [_P, _P, ctypes.POINTER(_U32)]),
+    "bajo_workspace_status_clear": (_I32, [_P, _P]),
+    "bajo_sort_workspace_size": (_I32, [_U32, _U32, _I32, _I32, _I32, ctypes.POINTER(_SZ)]),
+    "bajo_sort_keys_u32": (_I32, [_P, _U32, _I32, _I32, _P, _SZ, _P]),
+    "bajo_sort_pairs_u32": (_I32, [_P, _P, _U32, _I32, _I32, _P, _SZ, _P]),
+    "bajo_sort_keys_u64": (_I32, [_P, _U32, _I32, _I32, _P, _SZ, _P]),
+    "bajo_sort_pairs_u64": (_I32, [_P, _P, _U32, _I32, _I32, _P, _SZ, _P]),
+    "bajo_lbvh_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoLbvhSizesC)]),
+    "bajo_lbvh_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
+    "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
+    "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
+    "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
+    "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
+    "bajo_trace_camera_stats": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P]),
+    "bajo_camera_make": (_I32, [_P, _P, _P, _F, _P]),
+    "bajo_camera_from_vfov": (_I32, [_P, _P, _P, _F, _P]),
+    "bajo_version": (ctypes.c_char_p, []),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load ``libbajo_b200.so``; raise if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python -m bajo_b200.build` "
+                              "(there is no CPU fallback)")
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def check(code: int, what: str) -> None:
+    if code != OK:
+        raise BajoError(code, what)
+
+
+def require_cuda(t) -> None:
+    """Raise unless `t` is a CUDA tensor (the library has no host path)."""
+    import torch
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise TypeError("bajo_b200 kernels take CUDA tensors; there is no CPU fallback")
+
+
+def stream_handle(stream=None) -> int:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

@@ -1,0 +1,71 @@
+"""Builds ``bajo_b200/libbajo_b200.so`` (the C-ABI CUDA library) for sm_100a.
+
+The library is compiled in-tree with nvcc directly, so the shared object
+travels with the source tree and is the only native code the package loads.
+
+``-fmad=false``: no implicit multiply-add contraction.  The reference's float
+formulas are restated with their own rounding (explicit fmaf() only where the
+reference spells fma()), which is what makes results bit-identical to the CPU
+oracle built with ``-ffp-contract=off``.
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB = os.path.join(HERE, "libbajo_b200.so")
+SOURCES = ["sort.cu", "lbvh.cu", "trace.cu", "camera.cu"]
+HEADERS = ["bajo_common.cuh", "onesweep.cuh"]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-O3,-ffp-contract=off",
+         "-I", os.path.join(ROOT, "include")]
+
+
+def _sources():
+    return [os.path.join(CSRC, s) for s in SOURCES]
+
+
+def _inputs():
+    return _sources() + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(ROOT, "include", "bajo_b200.h"),
+                                                                  __file__]
+
+
+def up_to_date() -> bool:
+    if not os.path.exists(LIB):
+        return False
+    t = os.path.getmtime(LIB)
+    return all(os.path.getmtime(p) <= t for p in _inputs())
+
+
+def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False) -> str:
+    if not force and up_to_date():
+        return LIB
+    build_dir = os.path.join(HERE, "_build")
+    os.makedirs(build_dir, exist_ok=True)
+    objs = []
+    for src in _sources():
+        obj = os.path.join(build_dir, os.path.basename(src) + ".o")
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
+        if ptxas_verbose:
+            cmd += ["-Xptxas", "-v"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    tmp = LIB + ".tmp"
+    cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    subprocess.run(cmd, check=True)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_verbose="-v" in sys.argv, force=True)

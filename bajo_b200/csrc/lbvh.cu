@@ -1,0 +1,502 @@
+// lbvh.cu -- sm_100a LBVH build: triangle bounds, per-segment bounds, Morton
+// keys, onesweep sort, Karras topology, atomic-flag refit.  Restates
+// bajo/bvh/gpu/builder/lbvh.mojo (GPU driver) and binary_layout.mojo with the
+// reference's buffer layouts; see include/bajo_b200.h for the boundary.
+#include "onesweep.cuh"
+
+namespace bajo {
+
+int sm_count();
+
+namespace {
+
+constexpr int kBlock = 256;
+
+// Per segment, 12 ordered words: [min bounds xyz, max bounds xyz,
+// min centroid xyz, max centroid xyz].  Minima are stored complemented so
+// that every slot is an atomicMax that starts from 0.
+__device__ __forceinline__ uint32_t enc_min(float f) { return ~float_to_ordered(f); }
+__device__ __forceinline__ uint32_t enc_max(float f) { return float_to_ordered(f); }
+__device__ __forceinline__ float dec_min(uint32_t u) { return u == 0 ? FLT_MAX : ordered_to_float(~u); }
+__device__ __forceinline__ float dec_max(uint32_t u) { return u == 0 ? -FLT_MAX : ordered_to_float(u); }
+
+// ---------------------------------------------------------------------------
+// 1. triangle bounds + per-segment root / centroid bounds
+//    (compute_triangle_bounds_kernel, triangle_bvh.mojo:680;
+//     compute/reduce_segment_bounds_partials, binary_layout.mojo:128-205)
+//    One pass: coalesced vertex loads staged in shared memory, warp max
+//    reductions on order-preserving integer images, one set of atomics per
+//    block.  Block 0 also writes the internal-node offsets
+//    (_internal_segment_offsets, binary_layout.mojo:219).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) bounds_kernel(const float* __restrict__ verts, uint32_t n,
+                                                        const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
+                                                        uint32_t* __restrict__ internal_offsets,
+                                                        float* __restrict__ leaf_bounds,
+                                                        uint32_t* __restrict__ seg_ord) {
+  __shared__ float s_v[kBlock * 9];
+  __shared__ uint32_t s_red[kBlock / 32][12];
+  __shared__ uint32_t s_scan[8];
+  const uint32_t tid = threadIdx.x;
+
+  if (blockIdx.x == 0) {
+    // internal offsets: exclusive scan of max(count - 1, 0)
+    uint32_t carry = 0;
+    for (uint32_t base = 0; base < n_seg; base += kBlock) {
+      uint32_t s = base + tid, c = 0;
+      if (s < n_seg) {
+        uint32_t cnt = seg_offsets[s + 1] - seg_offsets[s];
+        c = cnt > 0 ? cnt - 1 : 0;
+      }
+      uint32_t ex = onesweep::scan256_exclusive<kBlock>(c, s_scan);
+      if (s < n_seg) internal_offsets[s] = carry + ex;
+      if (tid == kBlock - 1) s_scan[0] = ex + c;  // chunk total
+      __syncthreads();
+      carry += s_scan[0];
+      __syncthreads();
+    }
+    if (tid == 0) internal_offsets[n_seg] = carry;
+  }
+
+  const uint32_t base = blockIdx.x * kBlock;
+  if (base >= n) return;
+  const uint32_t cnt = min((uint32_t)kBlock, n - base);
+  const float* src = verts + (size_t)base * 9;
+  for (uint32_t k = tid; k < cnt * 9; k += kBlock) s_v[k] = src[k];
+  __syncthreads();
+
+  const bool live = tid < cnt;
+  f3 mn = mk(FLT_MAX, FLT_MAX, FLT_MAX), mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+  if (live) {
+    const float* v = s_v + tid * 9;
+    f3 a = mk(v[0], v[1], v[2]), b = mk(v[3], v[4], v[5]), c = mk(v[6], v[7], v[8]);
+    mn = vmin(vmin(a, b), c);
+    mx = vmax(vmax(a, b), c);
+  }
+  __syncthreads();
+  // stage the 6-float bounds and write them coalesced
+  if (live) {
+    float* o = s_v + tid * 6;
+    o[0] = mn.x; o[1] = mn.y; o[2] = mn.z; o[3] = mx.x; o[4] = mx.y; o[5] = mx.z;
+  }
+  __syncthreads();
+  float* dst = leaf_bounds + (size_t)base * 6;
+  for (uint32_t k = tid; k < cnt * 6; k += kBlock) dst[k] = s_v[k];
+
+  // centroid = (min + max) * 0.5   (core/aabb.mojo:53)
+  f3 c = (mn + mx) * 0.5f;
+  uint32_t w[12] = {0};
+  if (live) {
+    w[0] = enc_min(mn.x); w[1] = enc_min(mn.y); w[2] = enc_min(mn.z);
+    w[3] = enc_max(mx.x); w[4] = enc_max(mx.y); w[5] = enc_max(mx.z);
+    w[6] = enc_min(c.x); w[7] = enc_min(c.y); w[8] = enc_min(c.z);
+    w[9] = enc_max(c.x); w[10] = enc_max(c.y); w[11] = enc_max(c.z);
+  }
+  uint32_t seg_first = 0, seg_last = 0, seg = 0;
+  if (n_seg > 1) {
+    seg_first = segment_for_item(seg_offsets, n_seg + 1, base);
+    seg_last = segment_for_item(seg_offsets, n_seg + 1, base + cnt - 1);
+    seg = live ? segment_for_item(seg_offsets, n_seg + 1, base + tid) : seg_last;
+  }
+  if (seg_first == seg_last) {
+    const uint32_t warp = tid >> 5, lane = tid & 31;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) {
+      uint32_t r = __reduce_max_sync(0xFFFFFFFFu, w[k]);
+      if (lane == 0) s_red[warp][k] = r;
+    }
+    __syncthreads();
+    if (tid < 12) {
+      uint32_t r = 0;
+#pragma unroll
+      for (int q = 0; q < kBlock / 32; ++q) r = max(r, s_red[q][tid]);
+      if (r) atomicMax(&seg_ord[(size_t)seg_first * 12 + tid], r);
+    }
+  } else if (live) {
+#pragma unroll
+    for (int k = 0; k < 12; ++k) atomicMax(&seg_ord[(size_t)seg * 12 + k], w[k]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 2. Morton keys + every live digit histogram of the sort
+//    (compute_bounds_morton_codes_kernel, lbvh.mojo:30-62, fused with
+//     global_histogram, onesweep.mojo:31).  Grid-strided so that each block
+//    flushes its shared histograms once.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict__ leaf_bounds, uint32_t n,
+                                                        const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
+                                                        const uint32_t* __restrict__ seg_ord,
+                                                        float* __restrict__ seg_bounds_out,
+                                                        uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                                                        uint32_t passes, uint32_t end_bit,
+                                                        uint32_t* __restrict__ ghist) {
+  extern __shared__ uint32_t s_hist[];  // passes * copies * 256
+  const uint32_t copies = passes <= 4 ? 8 : 4;
+  const uint32_t words = passes * copies * 256;
+  for (uint32_t i = threadIdx.x; i < words; i += kBlock) s_hist[i] = 0;
+  if (blockIdx.x == 0) {
+    for (uint32_t k = threadIdx.x; k < n_seg * 12; k += kBlock) {
+      uint32_t u = seg_ord[k];
+      uint32_t f = k % 12;
+      bool is_min = (f < 3) || (f >= 6 && f < 9);
+      seg_bounds_out[k] = is_min ? dec_min(u) : dec_max(u);
+    }
+  }
+  __syncthreads();
+  const uint32_t copy = (threadIdx.x >> 5) % copies;
+  // single-segment fast path keeps the centroid frame in registers
+  uint32_t cur_seg = 0xFFFFFFFFu;
+  f3 cmin = mk(0, 0, 0), inv = mk(0, 0, 0);
+  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+    uint32_t seg = n_seg > 1 ? segment_for_item(seg_offsets, n_seg + 1, i) : 0;
+    if (seg != cur_seg) {
+      const uint32_t* o = seg_ord + (size_t)seg * 12;
+      cmin = mk(dec_min(__ldg(o + 6)), dec_min(__ldg(o + 7)), dec_min(__ldg(o + 8)));
+      f3 cmax = mk(dec_max(__ldg(o + 9)), dec_max(__ldg(o + 10)), dec_max(__ldg(o + 11)));
+      f3 ext = cmax - cmin;
+      inv = mk(safe_inv1(ext.x), safe_inv1(ext.y), safe_inv1(ext.z));
+      cur_seg = seg;
+    }
+    const float2* b = reinterpret_cast<const float2*>(leaf_bounds + (size_t)i * 6);
+    float2 b0 = b[0], b1 = b[1], b2 = b[2];
+    f3 mn = mk(b0.x, b0.y, b1.x), mx = mk(b1.y, b2.x, b2.y);
+    f3 c = (mn + mx) * 0.5f;
+    f3 d = c - cmin;
+    uint32_t code = morton3(d.x * inv.x, d.y * inv.y, d.z * inv.z);
+    uint64_t key = ((uint64_t)seg << 32) | code;
+    keys[i] = key;
+    vals[i] = i;
+    for (uint32_t p = 0; p < passes; ++p) {
+      uint32_t sh = 8 * p;
+      uint32_t bits = min(8u, end_bit - sh);
+      uint32_t dg = (uint32_t)(key >> sh) & ((1u << bits) - 1u);
+      atomicAdd(&s_hist[(p * copies + copy) * 256 + dg], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < passes * 256; i += kBlock) {
+    uint32_t p = i >> 8, dg = i & 255, s = 0;
+    for (uint32_t c = 0; c < copies; ++c) s += s_hist[(p * copies + c) * 256 + dg];
+    if (s) atomicAdd(&ghist[i], s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 3. Karras topology (init_segmented_lbvh_roots_kernel, lbvh.mojo:235;
+//    build_lbvh_topology_kernel, lbvh.mojo:257-329).
+// ---------------------------------------------------------------------------
+// lbvh.mojo:221-232 + core/morton.mojo:22: clz64 of the (code, local index)
+// keys, -1 outside the segment.
+__device__ __forceinline__ int delta(const uint32_t* __restrict__ codes, int64_t len, int64_t i, int64_t j) {
+  if (j < 0 || j >= len) return -1;
+  uint64_t a = ((uint64_t)__ldg(codes + i) << 32) | (uint32_t)i;
+  uint64_t b = ((uint64_t)__ldg(codes + j) << 32) | (uint32_t)j;
+  uint64_t x = a ^ b;
+  return x ? __clzll((long long)x) : 64;
+}
+
+__global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __restrict__ codes_all,
+                                                          const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
+                                                          const uint32_t* __restrict__ internal_offsets,
+                                                          uint32_t n, uint32_t* __restrict__ node_meta,
+                                                          uint32_t* __restrict__ leaf_parent,
+                                                          uint32_t* __restrict__ node_leaf_counts,
+                                                          uint32_t* __restrict__ node_flags,
+                                                          uint32_t* __restrict__ roots) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i < n_seg) {
+    uint32_t lb = seg_offsets[i], le = seg_offsets[i + 1];
+    if (le == lb) roots[i] = kSentinel;
+    else if (le - lb == 1) {
+      roots[i] = kLeafFlag | lb;
+      leaf_parent[lb] = kSentinel;
+    } else roots[i] = internal_offsets[i];
+  }
+  const uint32_t total = internal_offsets[n_seg];
+  if (i >= total) return;
+  const uint32_t seg = n_seg > 1 ? segment_for_item(internal_offsets, n_seg + 1, i) : 0;
+  const uint32_t ib = internal_offsets[seg], lb = seg_offsets[seg];
+  const int64_t len = (int64_t)seg_offsets[seg + 1] - lb;
+  const uint32_t* codes = codes_all + lb;
+  const int64_t li = (int64_t)i - ib;
+
+  // _lbvh_find_range, lbvh.mojo:164-191
+  int d_next = delta(codes, len, li, li + 1);
+  int d_prev = delta(codes, len, li, li - 1);
+  int64_t d = (d_next < d_prev) ? -1 : 1;
+  int delta_min = delta(codes, len, li, li - d);
+  int64_t lmax = 2;
+  while (delta(codes, len, li, li + lmax * d) > delta_min) {
+    lmax <<= 1;
+    if (lmax > len * 2) break;
+  }
+  int64_t l = 0;
+  for (int64_t t = lmax >> 1; t > 0; t >>= 1)
+    if (delta(codes, len, li, li + (l + t) * d) > delta_min) l += t;
+  int64_t j = li + l * d;
+  int64_t first = li < j ? li : j, last = li < j ? j : li;
+
+  // _lbvh_find_split, lbvh.mojo:194-218
+  int node_prefix = delta(codes, len, first, last);
+  int64_t split = first, step = last - first;
+  while (step > 1) {
+    step = (step + 1) >> 1;
+    int64_t ns = split + step;
+    if (ns < last && delta(codes, len, first, ns) > node_prefix) split = ns;
+  }
+
+  node_leaf_counts[i] = (uint32_t)(last - first + 1);
+  node_flags[i] = 0;
+  if (first == 0 && last == len - 1) node_meta[(size_t)i * 4 + 0] = kSentinel;
+  uint32_t left = ib + (uint32_t)split, right = ib + (uint32_t)split + 1;
+  if (split == first) {
+    left = kLeafFlag | (lb + (uint32_t)split);
+    leaf_parent[lb + split] = i;
+  } else {
+    node_meta[(size_t)(ib + split) * 4 + 0] = i;
+  }
+  if (split + 1 == last) {
+    right = kLeafFlag | (lb + (uint32_t)split + 1);
+    leaf_parent[lb + split + 1] = i;
+  } else {
+    node_meta[(size_t)(ib + split + 1) * 4 + 0] = i;
+  }
+  node_meta[(size_t)i * 4 + 1] = left;
+  node_meta[(size_t)i * 4 + 2] = right;
+  node_meta[(size_t)i * 4 + 3] = lb + (uint32_t)last;
+}
+
+// ---------------------------------------------------------------------------
+// 4. refit + sorted triangle records
+//    (refit_lbvh_bounds_from_leaves_kernel, lbvh.mojo:116-161;
+//     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
+//    One thread per sorted leaf climbs towards the root; the first arrival at
+//    a node stops, the second merges both child boxes and continues.  Release
+//    / acquire fences around the arrival counter make the sibling's box
+//    visible (the reference uses relaxed atomics with no fence).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__ verts,
+                                                       const uint32_t* __restrict__ leaf_ids, uint32_t n,
+                                                       const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
+                                                       const uint32_t* __restrict__ node_meta,
+                                                       const uint32_t* __restrict__ leaf_parent,
+                                                       float* __restrict__ node_bounds,
+                                                       uint32_t* __restrict__ node_flags,
+                                                       float* __restrict__ leaf_tris, uint32_t* __restrict__ status) {
+  const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
+  if (s >= n) return;
+  const uint32_t item = leaf_ids[s];
+  if (item >= n) {  // only after a failed sort
+    raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+    return;
+  }
+  const float* v = verts + (size_t)item * 9;
+  f3 a = mk(__ldg(v + 0), __ldg(v + 1), __ldg(v + 2));
+  f3 b = mk(__ldg(v + 3), __ldg(v + 4), __ldg(v + 5));
+  f3 c = mk(__ldg(v + 6), __ldg(v + 7), __ldg(v + 8));
+  uint32_t prim = item;
+  if (n_seg > 1) prim = item - seg_offsets[segment_for_item(seg_offsets, n_seg + 1, s)];
+  float4* rec = reinterpret_cast<float4*>(leaf_tris + (size_t)s * 12);
+  rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(prim));
+  rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
+  rec[2] = make_float4(c.x, c.y, c.z, 0.0f);
+
+  f3 mn = vmin(vmin(a, b), c), mx = vmax(vmax(a, b), c);
+  uint32_t cur = kLeafFlag | s;
+  uint32_t parent = leaf_parent[s];
+  // A Karras tree over 64-bit keys is at most 64 levels deep; a longer climb
+  // or an out-of-range parent means the topology is corrupt.
+  for (int depth = 0; parent != kSentinel; ++depth) {
+    if (depth > 128 || parent >= n) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      break;
+    }
+    const uint4 m = *reinterpret_cast<const uint4*>(node_meta + (size_t)parent * 4);
+    const bool is_left = m.y == cur;
+    if (!is_left && m.z != cur) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      break;
+    }
+    float* slot = node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6);
+    slot[0] = mn.x; slot[1] = mn.y; slot[2] = mn.z; slot[3] = mx.x; slot[4] = mx.y; slot[5] = mx.z;
+    __threadfence();
+    if (atomicAdd(&node_flags[parent], 1u) == 0) break;
+    __threadfence();
+    const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
+    mn = vmin(mn, mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2)));
+    mx = vmax(mx, mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5)));
+    cur = parent;
+    parent = m.x;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host plan
+// ---------------------------------------------------------------------------
+struct BuildPlan {
+  onesweep::Plan sort;
+  int end_bit;
+  size_t off_seg_ord, off_keys_alt, off_vals_alt, zero_bytes, total;
+};
+
+BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
+  BuildPlan b{};
+  int seg_bits = 0;
+  while (seg_bits < 32 && ((n_seg - 1) >> seg_bits)) ++seg_bits;
+  b.end_bit = 32 + seg_bits;
+  const uint32_t passes = onesweep::num_passes(0, b.end_bit);
+  const uint32_t tile = onesweep::tile_keys<uint64_t, true>();
+  onesweep::Plan& p = b.sort;
+  p.n = n;
+  p.passes = passes;
+  p.tiles = (n + tile - 1) / tile;
+  size_t o = 256;
+  p.off_ghist = o;
+  o += (size_t)passes * 256 * 4;
+  p.off_counters = o;
+  o += (size_t)passes * 4;
+  o = (o + 15) & ~(size_t)15;
+  p.off_lookback = o;
+  o += (size_t)passes * p.tiles * 256 * 4;
+  b.off_seg_ord = o;
+  o += (size_t)n_seg * 12 * 4;
+  b.zero_bytes = o - p.off_ghist;
+  p.zero_bytes = b.zero_bytes;
+  o = onesweep::align256(o);
+  b.off_keys_alt = o;
+  o = onesweep::align256(o + (size_t)n * 8);
+  b.off_vals_alt = o;
+  o = onesweep::align256(o + (size_t)n * 4);
+  b.total = o;
+  p.off_keys_alt = b.off_keys_alt;
+  p.off_vals_alt = b.off_vals_alt;
+  p.total = b.total;
+  return b;
+}
+
+}  // namespace
+}  // namespace bajo
+
+extern "C" {
+
+int32_t bajo_lbvh_sizes(uint32_t n, uint32_t n_seg, BajoLbvhSizes* s) {
+  if (!s || n_seg == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  if (n > BAJO_SORT_MAX_KEYS) return BAJO_ERR_TOO_LARGE;
+  const size_t N = n ? n : 1, M = N;
+  s->internal_offsets = (size_t)(n_seg + 1) * 4;
+  s->leaf_bounds = N * 24;
+  s->seg_bounds = (size_t)n_seg * 48;
+  s->sort_keys = N * 8;
+  s->leaf_ids = N * 4;
+  s->morton_codes = N * 4;
+  s->node_meta = M * 16;
+  s->node_bounds = M * 48;
+  s->node_leaf_counts = M * 4;
+  s->node_flags = M * 4;
+  s->leaf_parent = N * 4;
+  s->roots = (size_t)n_seg * 4;
+  s->leaf_tris = N * 48;
+  s->workspace = bajo::make_build_plan(n, n_seg).total;
+  return BAJO_OK;
+}
+
+static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, size_t ws_bytes, void* stream_,
+                               cudaEvent_t* ev, int32_t n_ev) {
+  using namespace bajo;
+  if (!bvh || !ws_ || bvh->n_segments == 0 || !bvh->seg_offsets) return BAJO_ERR_INVALID_ARGUMENT;
+  const uint32_t n = bvh->n_leaves, S = bvh->n_segments;
+  if (n > BAJO_SORT_MAX_KEYS) return BAJO_ERR_TOO_LARGE;
+  if (n > 0 && (!d_verts || !bvh->internal_offsets || !bvh->leaf_bounds || !bvh->seg_bounds || !bvh->sort_keys ||
+                !bvh->leaf_ids || !bvh->morton_codes || !bvh->node_meta || !bvh->node_bounds ||
+                !bvh->node_leaf_counts || !bvh->node_flags || !bvh->leaf_parent || !bvh->roots || !bvh->leaf_tris))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  BuildPlan plan = make_build_plan(n, S);
+  if (ws_bytes < plan.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
+  if (ev && n_ev < (int32_t)(5 + plan.sort.passes)) return BAJO_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream_;
+  // stage events: [start, bounds, morton, pass 0..P-1, topology, refit]
+  auto mark = [&](int i) { return !ev || cudaEventRecord(ev[i], st) == cudaSuccess; };
+  if (!mark(0)) return BAJO_ERR_CUDA;
+  unsigned char* ws = (unsigned char*)ws_;
+  uint32_t* status = (uint32_t*)ws;
+  if (cudaMemsetAsync(ws + plan.sort.off_ghist, 0, plan.zero_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
+  uint32_t* seg_ord = (uint32_t*)(ws + plan.off_seg_ord);
+  const uint32_t blocks = (n + kBlock - 1) / kBlock;
+
+  bounds_kernel<<<blocks ? blocks : 1, kBlock, 0, st>>>(d_verts, n, bvh->seg_offsets, S, bvh->internal_offsets,
+                                                        bvh->leaf_bounds, seg_ord);
+  if (cudaGetLastError() != cudaSuccess || !mark(1)) return BAJO_ERR_CUDA;
+
+  // sort buffers: the Morton kernel writes where an even/odd pass count lands
+  // the result in bvh->sort_keys / bvh->leaf_ids
+  const uint32_t passes = plan.sort.passes;
+  uint64_t* kalt = (uint64_t*)(ws + plan.off_keys_alt);
+  uint32_t* valt = (uint32_t*)(ws + plan.off_vals_alt);
+  // (with n <= 1 nothing is sorted and the keys stay where they are written)
+  const bool even = (passes % 2) == 0 || n <= 1;
+  uint64_t* k0 = even ? bvh->sort_keys : kalt;
+  uint32_t* v0 = even ? bvh->leaf_ids : valt;
+  uint64_t* k1 = even ? kalt : bvh->sort_keys;
+  uint32_t* v1 = even ? valt : bvh->leaf_ids;
+  uint32_t* ghist = (uint32_t*)(ws + plan.sort.off_ghist);
+  {
+    const uint32_t copies = passes <= 4 ? 8 : 4;
+    const size_t smem = (size_t)passes * copies * 256 * 4;
+    uint32_t grid = blocks;
+    const uint32_t cap = (uint32_t)sm_count() * 8;
+    if (grid > cap) grid = cap;
+    if (grid == 0) grid = 1;
+    if (smem > 48 * 1024) {
+      if (cudaFuncSetAttribute(morton_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+          cudaSuccess)
+        return BAJO_ERR_CUDA;
+    }
+    morton_kernel<<<grid, kBlock, smem, st>>>(bvh->leaf_bounds, n, bvh->seg_offsets, S, seg_ord, bvh->seg_bounds, k0,
+                                              v0, passes, (uint32_t)plan.end_bit, ghist);
+    if (cudaGetLastError() != cudaSuccess || !mark(2)) return BAJO_ERR_CUDA;
+  }
+  if (n > 1) {
+    bool in_first = true;
+    if (onesweep::run_passes<uint64_t, true>(k0, v0, k1, v1, bvh->morton_codes, plan.sort, ws, 0, plan.end_bit, st,
+                                             &in_first, ev ? ev + 3 : nullptr) != cudaSuccess)
+      return BAJO_ERR_CUDA;
+  } else {
+    // nothing to sort; keep the low word in step with the key
+    if (n == 1 &&
+        cudaMemcpyAsync(bvh->morton_codes, bvh->sort_keys, 4, cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+      return BAJO_ERR_CUDA;
+    for (uint32_t p = 0; p < passes; ++p)
+      if (!mark(3 + p)) return BAJO_ERR_CUDA;
+  }
+  topology_kernel<<<(max(n, S) + kBlock - 1) / kBlock, kBlock, 0, st>>>(
+      bvh->morton_codes, bvh->seg_offsets, S, bvh->internal_offsets, n, bvh->node_meta, bvh->leaf_parent,
+      bvh->node_leaf_counts, bvh->node_flags, bvh->roots);
+  if (cudaGetLastError() != cudaSuccess || !mark(3 + passes)) return BAJO_ERR_CUDA;
+  if (n > 0) {
+    refit_kernel<<<blocks, kBlock, 0, st>>>(d_verts, bvh->leaf_ids, n, bvh->seg_offsets, S, bvh->node_meta,
+                                            bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris,
+                                            status);
+    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
+  }
+  if (!mark(4 + passes)) return BAJO_ERR_CUDA;
+  return BAJO_OK;
+}
+
+int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* ws, size_t ws_bytes, void* stream) {
+  return lbvh_build_impl(d_verts, bvh, ws, ws_bytes, stream, nullptr, 0);
+}
+
+int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* ws, size_t ws_bytes, void* stream,
+                              void* const* events, int32_t n_events) {
+  if (!events) return BAJO_ERR_INVALID_ARGUMENT;
+  return lbvh_build_impl(d_verts, bvh, ws, ws_bytes, stream, (cudaEvent_t*)events, n_events);
+}
+
+int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {
+  if (!n_events || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  *n_events = (int32_t)(5 + bajo::make_build_plan(n_tris, n_segments).sort.passes);
+  return BAJO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,420 @@
+// onesweep.cuh -- stable LSD radix sort, one scatter kernel per 8-bit digit
+// with decoupled look-back (Merrill & Garland / Adinets & Merrill "Onesweep").
+//
+// Restates the reference's onesweep (bajo/sort/gpu/onesweep.mojo:31-328) for
+// sm_100a, with these changes:
+//  - keys are staged in shared memory with their own type, so 64-bit keys are
+//    sorted correctly (the reference stages them through UInt32 shared memory,
+//    onesweep.mojo:244,311,321, which truncates 64-bit keys);
+//  - digit ranking uses __match_any_sync on the digit (one instruction)
+//    instead of 8 ballots per key (bajo/sort/gpu/utils.mojo:46-103);
+//  - the look-back spin is bounded by elapsed time and reports
+//    BAJO_STATUS_LOOKBACK_TIMEOUT instead of spinning forever
+//    (onesweep.mojo:246-270);
+//  - the per-pass global digit offsets are scanned inside each scatter CTA
+//    (one fewer launch than scan_global, onesweep.mojo:102);
+//  - any digit range [begin_bit, end_bit) can be sorted, so constant key bits
+//    cost no pass.
+#pragma once
+
+#include "bajo_common.cuh"
+
+namespace bajo {
+namespace onesweep {
+
+constexpr uint32_t kRadix = 256;
+constexpr uint32_t kFlagAgg = 1u << 30;   // tile aggregate published
+constexpr uint32_t kFlagInc = 2u << 30;   // inclusive prefix published
+constexpr uint32_t kFlagMask = 3u << 30;
+constexpr uint32_t kValueMask = (1u << 30) - 1u;
+constexpr uint64_t kLookbackTimeoutNs = 200ull * 1000ull * 1000ull;  // 200 ms
+
+template <typename K>
+struct KeyTraits;
+template <>
+struct KeyTraits<uint32_t> {
+  static constexpr uint32_t kMax = 0xFFFFFFFFu;
+};
+template <>
+struct KeyTraits<uint64_t> {
+  static constexpr uint64_t kMax = 0xFFFFFFFFFFFFFFFFull;
+};
+
+// Tile shapes (threads x keys per thread), chosen per key type.
+template <typename K, bool HAS_V>
+struct TileConfig;
+template <bool HAS_V>
+struct TileConfig<uint32_t, HAS_V> {
+  static constexpr int kBlock = 512;
+  static constexpr int kKpt = 15;
+};
+template <bool HAS_V>
+struct TileConfig<uint64_t, HAS_V> {
+  static constexpr int kBlock = 512;
+  static constexpr int kKpt = 11;
+};
+
+__device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
+  const uint32_t lane = lane_id();
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t u = __shfl_up_sync(0xFFFFFFFFu, v, o);
+    if (lane >= (uint32_t)o) v += u;
+  }
+  return v;
+}
+
+// Exclusive scan of one value per thread over threads [0, 256) of the block.
+// Every thread of the block must call it (threads >= 256 pass anything).
+template <int BLOCK>
+__device__ __forceinline__ uint32_t scan256_exclusive(uint32_t v, uint32_t* tmp8) {
+  static_assert(BLOCK >= 256, "needs 256 threads");
+  const uint32_t tid = threadIdx.x;
+  uint32_t inc = 0;
+  if (tid < 256) {
+    inc = warp_inclusive_scan(v);
+    if ((tid & 31) == 31) tmp8[tid >> 5] = inc;
+  }
+  __syncthreads();
+  uint32_t excl = 0;
+  if (tid < 256) {
+    uint32_t w = tid >> 5, add = 0;
+#pragma unroll
+    for (uint32_t k = 0; k < 8; ++k) add += (k < w) ? tmp8[k] : 0u;
+    excl = add + inc - v;
+  }
+  __syncthreads();
+  return excl;
+}
+
+// ---------------------------------------------------------------------------
+// Global digit histogram of every pass in one read of the keys
+// (global_histogram, onesweep.mojo:31-99).  Grid-strided over the keys;
+// each warp pair owns a private shared histogram copy to limit contention.
+// ---------------------------------------------------------------------------
+constexpr int kHistBlock = 256;
+constexpr int kHistCopies = 4;  // copies per pass inside a CTA
+
+template <typename K>
+__global__ void __launch_bounds__(kHistBlock) global_histogram_kernel(const K* __restrict__ keys, uint32_t n,
+                                                                      uint32_t begin_bit, uint32_t n_passes,
+                                                                      uint32_t end_bit,
+                                                                      uint32_t* __restrict__ ghist) {
+  extern __shared__ uint32_t s_hist[];  // n_passes * kHistCopies * 256
+  const uint32_t words = n_passes * kHistCopies * kRadix;
+  for (uint32_t i = threadIdx.x; i < words; i += kHistBlock) s_hist[i] = 0;
+  __syncthreads();
+  const uint32_t copy = (threadIdx.x >> 5) % kHistCopies;
+  const uint32_t stride = gridDim.x * kHistBlock;
+  for (uint32_t i = blockIdx.x * kHistBlock + threadIdx.x; i < n; i += stride) {
+    K k = keys[i];
+    for (uint32_t p = 0; p < n_passes; ++p) {
+      uint32_t sh = begin_bit + 8 * p;
+      uint32_t bits = min(8u, end_bit - sh);
+      uint32_t d = (uint32_t)(k >> sh) & ((1u << bits) - 1u);
+      atomicAdd(&s_hist[(p * kHistCopies + copy) * kRadix + d], 1u);
+    }
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < n_passes * kRadix; i += kHistBlock) {
+    uint32_t p = i / kRadix, d = i % kRadix, s = 0;
+#pragma unroll
+    for (int c = 0; c < kHistCopies; ++c) s += s_hist[(p * kHistCopies + c) * kRadix + d];
+    if (s) atomicAdd(&ghist[p * kRadix + d], s);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One digit pass (digit_binning, onesweep.mojo:121-328).
+// ---------------------------------------------------------------------------
+template <typename K, int BLOCK, int KPT>
+struct BinSmem {
+  static constexpr int kWarps = BLOCK / 32;
+  static constexpr int kTile = BLOCK * KPT;
+  union {
+    K keys[kTile];
+    uint32_t vals[kTile];
+    uint32_t warp_hist[kWarps * kRadix];
+  } u;
+  uint32_t digit_offset[kRadix];
+  uint32_t tile_start[kRadix];
+  uint32_t scan_tmp[8];
+  uint32_t tile;
+  uint32_t abort;  // a look-back wait timed out: publish, skip the scatter
+};
+
+template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT>
+__global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
+    const K* __restrict__ keys_in, K* __restrict__ keys_out, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
+    uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
+    uint32_t n, uint32_t shift, uint32_t digit_mask) {
+  using S = BinSmem<K, BLOCK, KPT>;
+  constexpr int kWarps = S::kWarps;
+  constexpr uint32_t kTile = S::kTile;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+
+  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = tid & 31, warp = tid >> 5;
+
+  for (uint32_t i = tid; i < kWarps * kRadix; i += BLOCK) s.u.warp_hist[i] = 0;
+  if (tid == 0) {
+    s.tile = atomicAdd(tile_counter, 1u);  // tiles in launch order
+    s.abort = 0;
+  }
+  __syncthreads();
+  const uint32_t tile = s.tile;
+  const uint32_t tile_base = tile * kTile;
+  const uint32_t valid = min(kTile, n - tile_base);
+
+  // warp-striped load: key i of this thread sits at tile position
+  // warp*32*KPT + 32*i + lane, so (warp, i, lane) order is position order.
+  K key[KPT];
+  uint32_t val[HAS_V ? KPT : 1];
+  const uint32_t pos0 = tile_base + warp * 32 * KPT + lane;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t p = pos0 + 32 * i;
+    key[i] = (p < n) ? keys_in[p] : KeyTraits<K>::kMax;
+  }
+  if constexpr (HAS_V) {
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      uint32_t p = pos0 + 32 * i;
+      val[i] = (p < n) ? vals_in[p] : 0u;
+    }
+  }
+
+  // rank every key among equal digits of its warp, in position order
+  uint32_t* wh = s.u.warp_hist + warp * kRadix;
+  const uint32_t lt = lanemask_lt();
+  uint32_t rank[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    uint32_t leader = __ffs(peers) - 1;
+    uint32_t before = 0;
+    if (lane == leader) {
+      before = wh[d];
+      wh[d] = before + __popc(peers);
+    }
+    before = __shfl_sync(0xFFFFFFFFu, before, leader);
+    rank[i] = before + __popc(peers & lt);
+    __syncwarp();
+  }
+  __syncthreads();
+
+  // per digit: warp prefixes, tile total, publish the tile aggregate
+  uint32_t total = 0, agg = 0, gcount = 0;
+  if (tid < kRadix) {
+    uint32_t run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      uint32_t c = s.u.warp_hist[w * kRadix + tid];
+      s.u.warp_hist[w * kRadix + tid] = run;
+      run += c;
+    }
+    total = run;
+    agg = total - ((tid == digit_mask) ? (kTile - valid) : 0u);  // padding keys carry the top digit
+    uint32_t word = agg | (tile == 0 ? kFlagInc : kFlagAgg);
+    st_relaxed_gpu(&lookback[tile * kRadix + tid], word);
+    gcount = ghist[tid];
+  }
+  const uint32_t tstart = scan256_exclusive<BLOCK>(total, s.scan_tmp);
+  const uint32_t gstart = scan256_exclusive<BLOCK>(gcount, s.scan_tmp);
+
+  // decoupled look-back over the preceding tiles, one thread per digit
+  if (tid < kRadix) {
+    uint32_t excl = 0;
+    if (tile > 0) {
+      int32_t k = (int32_t)tile - 1;
+      uint32_t spins = 0;
+      uint64_t t0 = 0;
+      while (k >= 0) {
+        uint32_t f = ld_relaxed_gpu(&lookback[(uint32_t)k * kRadix + tid]);
+        uint32_t flag = f & kFlagMask;
+        if (flag == kFlagInc) {
+          excl += f & kValueMask;
+          break;
+        }
+        if (flag == kFlagAgg) {
+          excl += f & kValueMask;
+          --k;
+          continue;
+        }
+        // not ready: back off, give up after kLookbackTimeoutNs
+        if (spins == 0) t0 = global_timer_ns();
+        ++spins;
+        if ((spins & 63u) == 0 && global_timer_ns() - t0 > kLookbackTimeoutNs) {
+          raise_status(status, BAJO_STATUS_LOOKBACK_TIMEOUT);
+          s.abort = 1;
+          break;
+        }
+        __nanosleep(spins < 64 ? 32 : 256);
+      }
+      st_relaxed_gpu(&lookback[tile * kRadix + tid], ((excl + agg) & kValueMask) | kFlagInc);
+    }
+    s.digit_offset[tid] = gstart + excl - tstart;
+    s.tile_start[tid] = tstart;
+  }
+  __syncthreads();
+  // The successors are released (inclusive prefixes published); without a
+  // complete prefix the scatter addresses are unknown, so write nothing.
+  if (s.abort) return;
+
+  // tile-local sorted position of every key
+  uint32_t lidx[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    lidx[i] = s.tile_start[d] + s.u.warp_hist[warp * kRadix + d] + rank[i];
+  }
+  __syncthreads();  // warp_hist is overwritten by the key staging below
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) s.u.keys[lidx[i]] = key[i];
+  __syncthreads();
+
+  // scatter: consecutive tile slots of one digit go to consecutive addresses
+  uint8_t dig[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t j = tid + i * BLOCK;
+    if (j < valid) {
+      K k = s.u.keys[j];
+      uint32_t d = (uint32_t)(k >> shift) & digit_mask;
+      dig[i] = (uint8_t)d;
+      uint32_t dst = s.digit_offset[d] + j;
+      if (dst < n) {  // holds whenever the digit counts are consistent
+        keys_out[dst] = k;
+        if constexpr (EMIT_LOW32) low32_out[dst] = (uint32_t)k;
+      }
+    }
+  }
+  if constexpr (HAS_V) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) s.u.vals[lidx[i]] = val[i];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      uint32_t j = tid + i * BLOCK;
+      if (j < valid) {
+        uint32_t dst = s.digit_offset[dig[i]] + j;
+        if (dst < n) vals_out[dst] = s.u.vals[j];
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host-side plan
+// ---------------------------------------------------------------------------
+inline uint32_t num_passes(int begin_bit, int end_bit) { return (uint32_t)((end_bit - begin_bit + 7) / 8); }
+
+template <typename K, bool HAS_V>
+inline uint32_t tile_keys() {
+  return (uint32_t)(TileConfig<K, HAS_V>::kBlock * TileConfig<K, HAS_V>::kKpt);
+}
+
+inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Workspace of one sort: [status | ghist (P*256) | tile counters (P) |
+// lookback (P*tiles*256) | keys_alt | vals_alt].  The part from ghist to the
+// end of lookback must start zeroed every call; it is contiguous so that one
+// memset clears it.
+struct Plan {
+  uint32_t n, passes, tiles;
+  size_t off_ghist, off_counters, off_lookback, zero_bytes, off_keys_alt, off_vals_alt, total;
+};
+
+inline Plan make_plan(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t passes, uint32_t tile) {
+  Plan p{};
+  p.n = n;
+  p.passes = passes;
+  p.tiles = (n + tile - 1) / tile;
+  size_t o = 256;  // status word
+  p.off_ghist = o;
+  o += (size_t)passes * kRadix * 4;
+  p.off_counters = o;
+  o += (size_t)passes * 4;
+  o = (o + 15) & ~(size_t)15;
+  p.off_lookback = o;
+  o += (size_t)passes * p.tiles * kRadix * 4;
+  p.zero_bytes = o - p.off_ghist;
+  o = align256(o);
+  p.off_keys_alt = o;
+  o = align256(o + (size_t)n * key_bytes);
+  p.off_vals_alt = o;
+  if (has_values) o = align256(o + (size_t)n * 4);
+  p.total = o;
+  return p;
+}
+
+template <typename K, bool HAS_V, bool EMIT_LOW32>
+inline cudaError_t launch_pass(const K* kin, K* kout, const uint32_t* vin, uint32_t* vout, uint32_t* low32,
+                               const uint32_t* ghist, uint32_t* lookback, uint32_t* counter, uint32_t* status,
+                               uint32_t n, uint32_t tiles, uint32_t shift, uint32_t digit_mask,
+                               cudaStream_t stream) {
+  constexpr int B = TileConfig<K, HAS_V>::kBlock;
+  constexpr int KPT = TileConfig<K, HAS_V>::kKpt;
+  auto kern = onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
+  const size_t smem = sizeof(BinSmem<K, B, KPT>);
+  static bool configured[64] = {};  // per template instance and device
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (dev < 0 || dev >= 64 || !configured[dev]) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) configured[dev] = true;
+  }
+  kern<<<tiles, B, smem, stream>>>(kin, kout, vin, vout, low32, ghist, lookback, counter, status, n, shift,
+                                   digit_mask);
+  return cudaGetLastError();
+}
+
+// Runs every digit pass of [begin_bit, end_bit) over keys that start in
+// (k0, v0); the workspace gives the other buffer (k1, v1).  The histograms in
+// `ghist` must already hold the counts of every pass.  Returns through
+// *result_in_first whether the sorted keys ended in (k0, v0).
+template <typename K, bool HAS_V>
+inline cudaError_t run_passes(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t* low32_last, const Plan& p,
+                              unsigned char* ws, int begin_bit, int end_bit, cudaStream_t stream,
+                              bool* result_in_first, cudaEvent_t* pass_events = nullptr) {
+  uint32_t* status = reinterpret_cast<uint32_t*>(ws);
+  uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + p.off_ghist);
+  uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
+  uint32_t* lookback = reinterpret_cast<uint32_t*>(ws + p.off_lookback);
+  K* src = k0;
+  K* dst = k1;
+  uint32_t* vs = v0;
+  uint32_t* vd = v1;
+  for (uint32_t pass = 0; pass < p.passes; ++pass) {
+    uint32_t sh = (uint32_t)begin_bit + 8 * pass;
+    uint32_t bits = min(8u, (uint32_t)end_bit - sh);
+    uint32_t mask = (1u << bits) - 1u;
+    uint32_t* lb = lookback + (size_t)pass * p.tiles * kRadix;
+    cudaError_t e;
+    bool last = pass + 1 == p.passes;
+    if (last && low32_last)
+      e = launch_pass<K, HAS_V, true>(src, dst, vs, vd, low32_last, ghist + pass * kRadix, lb, counters + pass,
+                                      status, p.n, p.tiles, sh, mask, stream);
+    else
+      e = launch_pass<K, HAS_V, false>(src, dst, vs, vd, nullptr, ghist + pass * kRadix, lb, counters + pass,
+                                       status, p.n, p.tiles, sh, mask, stream);
+    if (e != cudaSuccess) return e;
+    if (pass_events && (e = cudaEventRecord(pass_events[pass], stream)) != cudaSuccess) return e;
+    K* t = src;
+    src = dst;
+    dst = t;
+    uint32_t* tv = vs;
+    vs = vd;
+    vd = tv;
+  }
+  *result_in_first = (src == k0);
+  return cudaSuccess;
+}
+
+}  // namespace onesweep
+}  // namespace bajo

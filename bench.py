@@ -1,0 +1,500 @@
+#!/usr/bin/env python
+"""Benchmark of the LBVH build + closest-hit path on B200.
+
+Workload (plain LBVH): 65,536 triangles, each a centroid uniform in [0,1]^3
+plus three vertex offsets uniform in +-0.01 per axis (seed 0, FP32); 30-bit
+Morton codes; one LBVH build per step.  The closest-hit figure traces
+1024x1024 pinhole rays from (0.5, 0.5, -1.5) looking +z with a 60 degree
+vertical field of view against the built tree.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl bajo|reference]
+
+One JSON line on rank 0.  `value` is the device-timed LBVH build throughput
+(Mtri/s, inputs resident in HBM, L2 flushed before every timed step); `e2e`
+is the same metric through the public API with the vertex upload from pinned
+host memory and the read-back of the root bounds + status inside the timed
+region; `closest_hit` reports MRays/s of the traversal.  With --impl
+reference the restated reference CPU builder runs on the host cores.
+Multi-GPU runs are replicas: every rank builds its own copy of the scene.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+N_TRIS = 65536
+WIDTH = HEIGHT = 1024
+METRIC = "LBVH build Mtri/s"
+UNIT = "Mtri/s"
+WORKLOAD = "plain LBVH build of 65,536 random triangles (seed 0) + 1024x1024 closest-hit camera rays"
+# Algorithmic bytes of one onesweep digit pass over the LBVH sort: read and
+# write one u64 key and one u32 payload per triangle.
+PASS_BYTES_PER_KEY = 24
+HIT_BYTES = 32      # 8-word hit written per ray
+NODE_BYTES = 64     # 48 B child boxes + 16 B child refs per visited node
+TRI_BYTES = 48      # packed triangle record per triangle test
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="bajo", choices=["bajo", "reference"])
+    p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-sweep", action="store_true")
+    return p.parse_args()
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """DRAM bytes per launch of the onesweep pass from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    REASONS = ["clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+               "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, index=0):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        q = "clocks.sm,clocks.max.sm,power.draw," + ",".join(self.REASONS)
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        reasons = []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for k, name in enumerate(names):
+            if any(s[3 + k].lower().startswith("active") for s in self.samples):
+                reasons.append(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------- distributed
+def dist_setup(args):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(world, x: float) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------- CPU baseline
+def cpu_baseline(verts, seconds):
+    """The restated reference CPU LBVH builder (bajo/bvh/cpu/builder/lbvh.mojo)
+    on every host thread: a bounded sample of repeated 65,536-tri builds."""
+    from oracle import oracle as O
+    O.build()
+    cb = O.CpuLbvh(verts)
+    cb.build()
+    t0 = time.perf_counter()
+    builds = 0
+    while time.perf_counter() - t0 < seconds:
+        cb.build()
+        builds += 1
+    dt = time.perf_counter() - t0
+    return {"value": round(N_TRIS * builds / dt / 1e6, 3), "unit": UNIT, "cores": cb.threads, "kind": "port",
+            "sample": f"{builds} builds of the 65,536-triangle scene in {dt:.1f} s (C restatement of the "
+                      "reference CPU LBVH builder, all host threads)"}
+
+
+def cpu_trace_sample(verts, stride=16):
+    from oracle import oracle as O
+    from bajo_b200 import camera
+    cb = O.CpuLbvh(verts)
+    cb.build()
+    rays = O.camera_rays(camera.plain_lbvh_camera(), WIDTH * HEIGHT, WIDTH, HEIGHT).reshape(8, -1)
+    sub = rays[:, ::stride].copy().reshape(-1)
+    n = sub.size // 8
+    cb.trace(sub)
+    t0 = time.perf_counter()
+    reps = 0
+    while True:
+        cb.trace(sub)
+        reps += 1
+        if time.perf_counter() - t0 > 2.0:
+            break
+    dt = (time.perf_counter() - t0) / reps
+    return n / dt / 1e6, cb.threads, n
+
+
+# ----------------------------------------------------------------- reference arm
+def run_reference(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from bajo_b200 import scenes
+    from oracle import oracle as O
+    O.build()
+    verts = scenes.random_triangles(N_TRIS, seed=0)
+    cb = O.CpuLbvh(verts)
+    for _ in range(max(args.warmup, 1)):
+        cb.build()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        cb.build()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = N_TRIS * args.steps / total / 1e6
+    mrays, cores, nsample = cpu_trace_sample(verts)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays": WIDTH * HEIGHT, "seed": 0,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cb.threads, "kind": "port",
+                         "sample": f"{args.steps} full builds of the 65,536-triangle scene (C restatement of the "
+                                   "reference CPU LBVH builder; Mojo is unavailable here)"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "closest_hit": {"value": round(mrays, 3), "unit": "MRays/s",
+                        "sample": f"{nsample} of the 1024x1024 camera rays (every 16th), {cores} threads"},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ----------------------------------------------------------------- GPU arm
+def run_bajo(args):
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args)
+    from bajo_b200 import build as B
+    if rank == 0 or world == 1:
+        B.build()
+    barrier(world)
+    from bajo_b200 import _lib, bvh, camera, scenes
+
+    L = _lib.load()
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream()
+    sh = stream.cuda_stream
+
+    verts_h = scenes.random_triangles(N_TRIS, seed=0)
+    verts = torch.from_numpy(verts_h).to(dev)
+    ws = bvh.GpuBvhBuildWorkspace(N_TRIS, 1, device=dev)
+    tree = bvh.build_triangle_bvh(verts, workspace=ws)
+    c = tree.c_struct()
+    cam = torch.from_numpy(camera.plain_lbvh_camera()).to(dev)
+    n_rays = WIDTH * HEIGHT
+    hits = torch.empty(8 * n_rays, dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
+
+    n_ev = ctypes.c_int32(0)
+    L.bajo_lbvh_stage_count(N_TRIS, 1, ctypes.byref(n_ev))
+    n_ev = n_ev.value
+    passes = n_ev - 5
+    kernels_per_build = 4 + passes  # bounds, morton, passes, topology, refit
+
+    def build_timed(events):
+        arr = (ctypes.c_void_p * n_ev)(*[e.cuda_event for e in events])
+        _lib.check(L.bajo_lbvh_build_timed(verts.data_ptr(), ctypes.byref(c), ws.buffer.data_ptr(),
+                                           ws.buffer.numel(), sh, arr, n_ev), "bajo_lbvh_build_timed")
+
+    def new_events(k):
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(k)]
+        for e in evs:
+            e.record(stream)  # materialise the handles
+        return evs
+
+    def trace(h=None):
+        _lib.check(L.bajo_trace_camera(ctypes.byref(c), cam.data_ptr(), n_rays, WIDTH, HEIGHT, _lib.TRI_WATERTIGHT,
+                                       h.data_ptr(), None, None, None, sh), "bajo_trace_camera")
+
+    # ---- warm-up
+    evs = new_events(n_ev)
+    for _ in range(args.warmup):
+        build_timed(evs)
+        trace(hits)
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: K builds (+ K traces timed separately)
+    step_events = [new_events(n_ev) for _ in range(args.steps)]
+    trace_events = [new_events(2) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            flush.zero_()
+            build_timed(step_events[k])
+            flush.zero_()
+            trace_events[k][0].record(stream)
+            trace(hits)
+            trace_events[k][1].record(stream)
+        torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    build_ms = [e[0].elapsed_time(e[-1]) for e in step_events]
+    pass_ms = [e[2 + p].elapsed_time(e[3 + p]) for e in step_events for p in range(passes)]
+    stage = {
+        "bounds": statistics.mean(e[0].elapsed_time(e[1]) for e in step_events),
+        "morton": statistics.mean(e[1].elapsed_time(e[2]) for e in step_events),
+        "sort": statistics.mean(e[2].elapsed_time(e[2 + passes]) for e in step_events),
+        "topology": statistics.mean(e[2 + passes].elapsed_time(e[3 + passes]) for e in step_events),
+        "refit": statistics.mean(e[3 + passes].elapsed_time(e[4 + passes]) for e in step_events),
+    }
+    trace_ms = [e[0].elapsed_time(e[1]) for e in trace_events]
+    build_total = max_over_ranks(world, sum(build_ms) / 1e3)
+    trace_total = max_over_ranks(world, sum(trace_ms) / 1e3)
+    value = world * N_TRIS * args.steps / build_total / 1e6
+    mrays = world * n_rays * args.steps / trace_total / 1e6
+
+    # ---- roofline: onesweep digit pass, the build's dominant kernel
+    peak, peak_kind = measured_peaks()
+    pass_avg_s = statistics.mean(pass_ms) / 1e3
+    pass_bytes = PASS_BYTES_PER_KEY * N_TRIS
+    achieved = pass_bytes / pass_avg_s / 1e9
+    traffic = committed_traffic().get("onesweep_pass_65536")
+
+    # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
+    stats = torch.empty(2 * n_rays, dtype=torch.int32, device=dev)
+    _lib.check(L.bajo_trace_camera_stats(ctypes.byref(c), cam.data_ptr(), n_rays, WIDTH, HEIGHT,
+                                         _lib.TRI_WATERTIGHT, None, stats.data_ptr(), sh), "bajo_trace_camera_stats")
+    torch.cuda.synchronize()
+    st = stats.view(-1, 2).double()
+    nodes_per_ray, tris_per_ray = float(st[:, 0].mean()), float(st[:, 1].mean())
+    trace_bytes = n_rays * (nodes_per_ray * NODE_BYTES + tris_per_ray * TRI_BYTES + HIT_BYTES)
+    trace_achieved = trace_bytes / (statistics.mean(trace_ms) / 1e3) / 1e9
+
+    # ---- e2e through the public API: upload, build, read back root bounds + status
+    pinned_v = torch.from_numpy(verts_h).pin_memory()
+    out_h = torch.empty(12, dtype=torch.float32).pin_memory()
+    st_h = torch.empty(1, dtype=torch.int32).pin_memory()
+    e2e_v = torch.empty_like(verts)
+    for _ in range(2):
+        e2e_v.copy_(pinned_v, non_blocking=True)
+        t2 = bvh.build_triangle_bvh(e2e_v, workspace=ws, out=tree)
+        out_h.copy_(t2.node_bounds[:12], non_blocking=True)
+        st_h.copy_(ws.buffer[:4].view(torch.int32), non_blocking=True)
+    torch.cuda.synchronize()
+    barrier(world)
+    e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2e_ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e_start.record(stream)
+        e2e_v.copy_(pinned_v, non_blocking=True)
+        t2 = bvh.build_triangle_bvh(e2e_v, workspace=ws, out=tree)
+        out_h.copy_(t2.node_bounds[:12], non_blocking=True)
+        st_h.copy_(ws.buffer[:4].view(torch.int32), non_blocking=True)
+        e_end.record(stream)
+        e_end.synchronize()
+        e2e_ms.append(e_start.elapsed_time(e_end))
+        if int(st_h.item()) != 0:
+            raise RuntimeError(f"device status {int(st_h.item())}")
+    e2e_total = max_over_ranks(world, sum(e2e_ms) / 1e3)
+    e2e_value = world * N_TRIS * args.steps / e2e_total / 1e6
+
+    # ---- sweep (sort and build at larger sizes), rank 0 only
+    sweep = None
+    if rank == 0 and not args.no_sweep:
+        sweep = run_sweep(torch, bvh, _lib, L, dev, stream, peak)
+
+    if rank != 0:
+        barrier(world)
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(verts_h, args.cpu_seconds)
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(build_total / args.steps * 1e3, 5), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays": n_rays, "seed": 0,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "flushed (256 MiB write) before every timed build and trace", "sort_passes": passes},
+        "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
+                "d2h_bytes_per_step": 12 * 4 + 4,
+                "what": "pinned H2D of the vertices + build + D2H of the root child boxes and device status"},
+        "roofline": {"kernel": "onesweep digit pass (u64 key + u32 id)", "bound": "hbm",
+                     "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": traffic,
+                     "algorithmic_bytes_per_launch": pass_bytes, "avg_launch_us": round(pass_avg_s * 1e6, 3),
+                     "peak_kind": peak_kind},
+        "stages_ms": {k: round(v, 5) for k, v in stage.items()},
+        "closest_hit": {"value": round(mrays, 3), "unit": "MRays/s", "ms": round(statistics.mean(trace_ms), 4),
+                        "nodes_per_ray": round(nodes_per_ray, 3), "tris_per_ray": round(tris_per_ray, 3),
+                        "roofline": {"bound": "hbm (instrumented bytes: node + triangle loads, mostly L2)",
+                                     "achieved": round(trace_achieved, 2), "peak": peak, "unit": "GB/s",
+                                     "frac": round(trace_achieved / peak, 4)}},
+        "gpu_launches": args.steps * (kernels_per_build + 1),
+        "clocks": clocks.summary(),
+    }
+    if cpu:
+        line["cpu_baseline"] = cpu
+        try:
+            mr, cores, ns = cpu_trace_sample(verts_h)
+            line["closest_hit"]["cpu_baseline"] = {"value": round(mr, 3), "unit": "MRays/s", "cores": cores,
+                                                   "kind": "port", "sample": f"{ns} rays (every 16th)"}
+        except Exception as e:  # pragma: no cover
+            line["closest_hit"]["cpu_baseline"] = {"error": str(e)}
+    if sweep:
+        line["sweep"] = sweep
+    print(json.dumps(line), flush=True)
+    barrier(world)
+
+
+def run_sweep(torch, bvh, _lib, L, dev, stream, peak):
+    """Throughput at larger sizes: sort (u32 pairs, u64/u32 pairs) and build."""
+    from bajo_b200 import sort
+    out = {"sort_u32_pairs": {}, "sort_u64_pairs": {}, "build": {}}
+    g = torch.Generator(device=dev).manual_seed(0)
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+
+    def timeit(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(reps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    for lg in (20, 22, 24, 26):
+        n = 1 << lg
+        k32 = torch.randint(-2**31, 2**31, (n,), dtype=torch.int32, device=dev, generator=g)
+        v32 = torch.arange(n, dtype=torch.int32, device=dev)
+        src_k, src_v = k32.clone(), v32.clone()
+        ws = sort.RadixSortWorkspace(n, 4, True, device=dev)
+
+        def f32():
+            k32.copy_(src_k)
+            v32.copy_(src_v)
+            sort.onesweep_radix_sort_pairs(k32, v32, workspace=ws)
+        copy_ms = timeit(lambda: (k32.copy_(src_k), v32.copy_(src_v)))
+        ms = timeit(f32) - copy_ms
+        out["sort_u32_pairs"][f"2^{lg}"] = {"gkeys_s": round(n / ms / 1e6, 2),
+                                           "hbm_frac": round(68 * n / (ms / 1e3) / 1e9 / peak, 3)}
+        del k32, v32, src_k, src_v, ws
+        k64 = torch.randint(0, 2**62, (n,), dtype=torch.int64, device=dev, generator=g) & 0x00000FFF3FFFFFFF
+        v32 = torch.arange(n, dtype=torch.int32, device=dev)
+        src_k, src_v = k64.clone(), v32.clone()
+        ws = sort.RadixSortWorkspace(n, 8, True, 0, 44, device=dev)
+
+        def f64():
+            k64.copy_(src_k)
+            v32.copy_(src_v)
+            sort.onesweep_radix_sort_pairs(k64, v32, workspace=ws, begin_bit=0, end_bit=44)
+        copy_ms = timeit(lambda: (k64.copy_(src_k), v32.copy_(src_v)))
+        ms = timeit(f64) - copy_ms
+        out["sort_u64_pairs"][f"2^{lg}"] = {"bits": 44, "gkeys_s": round(n / ms / 1e6, 2),
+                                           "hbm_frac": round((6 * 24 + 8) * n / (ms / 1e3) / 1e9 / peak, 3)}
+        del k64, v32, src_k, src_v, ws
+    for lg in (20, 22, 24):
+        n = 1 << lg
+        c = torch.rand((n, 1, 3), generator=g, device=dev)
+        off = (torch.rand((n, 3, 3), generator=g, device=dev) * 2 - 1) * 0.004
+        v = (c + off).reshape(-1).contiguous()
+        ws = bvh.GpuBvhBuildWorkspace(n, 1, device=dev)
+        tree = bvh.build_triangle_bvh(v, workspace=ws)
+        ms = timeit(lambda: bvh.build_triangle_bvh(v, workspace=ws, out=tree))
+        # bytes per triangle: bounds 36+24, Morton 24+12, 4 passes x 24, topology ~24, refit 36+48+48
+        out["build"][f"2^{lg}"] = {"mtri_s": round(n / ms / 1e3, 1), "ms": round(ms, 4),
+                                   "hbm_frac": round(348 * n / (ms / 1e3) / 1e9 / peak, 3)}
+        del c, off, v, ws, tree
+    return out
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    run_bajo(args)
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

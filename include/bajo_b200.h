@@ -1,0 +1,184 @@
+/*
+ * bajo_b200.h -- C ABI of the sm_100a LBVH build + closest-hit library.
+ *
+ * Drop-in boundary for the GPU path of jgsimard/bajo (Mojo).  The reference
+ * exposes this path as Mojo generics over a DeviceContext; a Mojo host binds
+ * these symbols with `external_call` / `DLHandle` instead.
+ *
+ * Conventions
+ *  - Every pointer named d_* is DEVICE memory allocated by the caller.  The
+ *    library never allocates: size queries (bajo_*_size) tell the caller how
+ *    much workspace to provide.
+ *  - `stream` is a cudaStream_t passed as void* (0 = legacy default stream).
+ *    Calls only enqueue work; nothing synchronises unless the name says so.
+ *  - Every function returns an int32 status (BAJO_OK = 0).  Errors found on
+ *    the device (look-back timeout, traversal stack overflow) are OR-ed into a
+ *    status word at the start of the workspace; read it with
+ *    bajo_workspace_status after the stream has run.
+ *  - Buffer layouts are the reference's (cited per field).
+ */
+#ifndef BAJO_B200_H
+#define BAJO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (mirrors the reference's raise sites and device status
+ *      words: bajo/rt/wavefront_contract.mojo:25-29,
+ *      bajo/bvh/gpu/builder/wide_collapse.mojo:34-38) ----------------------- */
+#define BAJO_OK 0
+#define BAJO_ERR_INVALID_ARGUMENT 1
+#define BAJO_ERR_WORKSPACE_TOO_SMALL 2
+#define BAJO_ERR_TOO_LARGE 3
+#define BAJO_ERR_CUDA 4
+#define BAJO_ERR_DEVICE 5 /* a device status bit is set */
+
+/* device status word bits */
+#define BAJO_STATUS_LOOKBACK_TIMEOUT 0x1u /* sort look-back gave up waiting    */
+#define BAJO_STATUS_STACK_OVERFLOW 0x2u   /* traversal stack would overflow    */
+#define BAJO_STATUS_BAD_TOPOLOGY 0x4u     /* refit met an inconsistent parent  */
+
+/* triangle tests */
+#define BAJO_TRI_MT 0         /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
+#define BAJO_TRI_WATERTIGHT 1 /* Woop/Benthin/Wald 2013 watertight test        */
+
+/* Largest key count one sort call accepts (30-bit look-back counters). */
+#define BAJO_SORT_MAX_KEYS ((1u << 30) - 1u)
+
+/* ======================================================================== */
+/* Workspace status                                                          */
+/* ======================================================================== */
+/* Synchronises `stream`, then copies the device status word that starts every
+ * workspace into *status (0 = no device error). */
+int32_t bajo_workspace_status(const void* d_workspace, void* stream, uint32_t* status);
+/* Enqueues a reset of the status word to 0. */
+int32_t bajo_workspace_status_clear(void* d_workspace, void* stream);
+
+/* ======================================================================== */
+/* Onesweep radix sort (stable, LSD, 8-bit digits, decoupled look-back)       */
+/* ======================================================================== */
+/* Replaces bajo/sort/gpu/onesweep.mojo:362 onesweep_radix_sort_keys,
+ * :454 onesweep_radix_sort_pairs and bajo/sort/gpu/radix_sort.mojo:510
+ * device_radix_sort_pairs (the sort the LBVH calls, lbvh.mojo:101).
+ * Sorts bits [begin_bit, end_bit) in place: the result lands in d_keys /
+ * d_vals, as the reference's DoubleBuffer does after an even pass count
+ * (bajo/sort/gpu/utils.mojo:8-37).  Workspace holds the alternate buffers,
+ * the digit histograms and the look-back flags.  n <= BAJO_SORT_MAX_KEYS. */
+int32_t bajo_sort_workspace_size(uint32_t n, uint32_t key_bytes, int32_t has_values, int32_t begin_bit,
+                                 int32_t end_bit, size_t* bytes);
+int32_t bajo_sort_keys_u32(uint32_t* d_keys, uint32_t n, int32_t begin_bit, int32_t end_bit, void* d_workspace,
+                           size_t workspace_bytes, void* stream);
+int32_t bajo_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit, int32_t end_bit,
+                            void* d_workspace, size_t workspace_bytes, void* stream);
+int32_t bajo_sort_keys_u64(uint64_t* d_keys, uint32_t n, int32_t begin_bit, int32_t end_bit, void* d_workspace,
+                           size_t workspace_bytes, void* stream);
+int32_t bajo_sort_pairs_u64(uint64_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit, int32_t end_bit,
+                            void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* ======================================================================== */
+/* LBVH build                                                                */
+/* ======================================================================== */
+/* Device buffers of one (optionally segmented) binary LBVH.  Field layouts
+ * follow GpuBinaryBoundsBvh (bajo/bvh/gpu/builder/binary_layout.mojo:303-329)
+ * and GpuBinaryTopologyWorkspace (:226-249).  N = n_leaves (triangles),
+ * S = n_segments, M = max(N, 1) (upper bound on internal nodes). */
+typedef struct BajoLbvh {
+  uint32_t n_leaves;           /* N                                                      */
+  uint32_t n_segments;         /* S >= 1                                                 */
+  const uint32_t* seg_offsets; /* S+1 item offsets, [0] = 0, [S] = N (input)             */
+  uint32_t* internal_offsets;  /* S+1 internal-node offsets, max(count-1,0) per segment  */
+  float* leaf_bounds;          /* 6*N   per-item AABB [min xyz, max xyz]  (item order)    */
+  float* seg_bounds;           /* 12*S  root AABB then centroid AABB per segment          */
+  uint64_t* sort_keys;         /* N     sorted (segment << 32) | morton                   */
+  uint32_t* leaf_ids;          /* N     sorted item ids (sort payload)                    */
+  uint32_t* morton_codes;      /* N     low 32 bits of sort_keys                          */
+  uint32_t* node_meta;         /* 4*M   [parent, left, right, fence], tagged child refs   */
+  float* node_bounds;          /* 12*M  left-child AABB then right-child AABB             */
+  uint32_t* node_leaf_counts;  /* M     leaves under each internal node                   */
+  uint32_t* node_flags;        /* M     refit arrival counters (2 after a build)          */
+  uint32_t* leaf_parent;       /* N     parent internal node of each sorted leaf          */
+  uint32_t* roots;             /* S     tagged root ref per segment (SENTINEL if empty)   */
+  float* leaf_tris;            /* 12*N  sorted triangle records [v0,prim | v1,0 | v2,0]   */
+} BajoLbvh;
+
+/* Byte size of every BajoLbvh array for N triangles in S segments (in field
+ * order: internal_offsets, leaf_bounds, seg_bounds, sort_keys, leaf_ids,
+ * morton_codes, node_meta, node_bounds, node_leaf_counts, node_flags,
+ * leaf_parent, roots, leaf_tris) and of the build workspace. */
+typedef struct BajoLbvhSizes {
+  size_t internal_offsets, leaf_bounds, seg_bounds, sort_keys, leaf_ids, morton_codes, node_meta, node_bounds,
+      node_leaf_counts, node_flags, leaf_parent, roots, leaf_tris;
+  size_t workspace;
+} BajoLbvhSizes;
+int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* sizes);
+
+/* Replaces build_triangle_bvh (bajo/bvh/gpu/triangle_bvh.mojo:617) and the
+ * segmented driver enqueue_segmented_wide_build
+ * (bajo/bvh/gpu/builder/segmented_build.mojo:89) up to the binary LBVH
+ * (build_binary_bvh_with_lbvh, bajo/bvh/gpu/builder/lbvh.mojo:332):
+ * triangle bounds, per-segment bounds, Morton keys, onesweep sort of the live
+ * key bits, Karras topology, atomic-flag refit, sorted triangle packing.
+ * d_verts: 9 floats per triangle [v0 xyz, v1 xyz, v2 xyz].  bvh->seg_offsets
+ * and every output array must be set by the caller. */
+int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Stage-timed build, the sync-free counterpart of the reference's
+ * measure_stages / GpuBuildTimings (bajo/bvh/gpu/builder/lbvh.mojo:347-422):
+ * `events` holds n_events cudaEvent_t handles created by the caller; the
+ * build records them on `stream` at [start, bounds, morton, sort pass 0..P-1,
+ * topology, refit].  bajo_lbvh_stage_count gives n_events = P + 5. */
+int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
+                              void* stream, void* const* events, int32_t n_events);
+int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);
+
+/* ======================================================================== */
+/* Closest-hit traversal                                                     */
+/* ======================================================================== */
+/* Replaces GpuTriangleBvh.launch_rays[CLOSEST_HIT]
+ * (bajo/bvh/gpu/triangle_bvh.mojo:587).  d_rays: SoA, 8 planes of n floats
+ * [ox, oy, oz, tmin, dx, dy, dz, tmax] (bajo/bvh/gpu/ray_launch.mojo:95).
+ * Outputs (either may be NULL): d_hits8, 8 words per ray
+ * [u, v, prim, inst, nx, ny, nz, t] (bajo/bvh/types.mojo:16-27); d_t / d_prim,
+ * compact SoA closest distance and primitive id.  Misses report t = tmax and
+ * prim = 0xFFFFFFFF.  Ties in t go to the lowest primitive id.  Segment 0's
+ * root is traced.  d_status (may be NULL) receives BAJO_STATUS_* bits. */
+int32_t bajo_trace_rays(const BajoLbvh* bvh, const float* d_rays, uint32_t n_rays, int32_t tri_mode,
+                        float* d_hits8, float* d_t, uint32_t* d_prim, uint32_t* d_status, void* stream);
+
+/* Replaces GpuTriangleBvh.launch_camera (bajo/bvh/gpu/triangle_bvh.mojo:520):
+ * primary rays generated in-kernel from 20-float camera records
+ * (bajo/bvh/camera.mojo:19-37, make_ray_raster :137), one camera per
+ * width*height rays (camera_launch.mojo:34). */
+int32_t bajo_trace_camera(const BajoLbvh* bvh, const float* d_cameras, uint32_t n_rays, uint32_t width,
+                          uint32_t height, int32_t tri_mode, float* d_hits8, float* d_t, uint32_t* d_prim,
+                          uint32_t* d_status, void* stream);
+
+/* Instrumented camera trace (trace_triangle_bvh_camera_instrumented_kernel,
+ * bajo/bvh/gpu/triangle_bvh.mojo:813; GpuTraversalStats,
+ * bajo/bvh/gpu/trace.mojo:62): same hits as bajo_trace_camera plus, per ray,
+ * d_stats[2i] = internal nodes visited, d_stats[2i+1] = triangles tested. */
+int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cameras, uint32_t n_rays, uint32_t width,
+                                uint32_t height, int32_t tri_mode, float* d_hits8, uint32_t* d_stats,
+                                void* stream);
+
+/* Host-side camera records (no device work).  Camera.__init__ and
+ * Camera.from_vfov (bajo/bvh/camera.mojo:77-116): out20 receives
+ * [origin, forward, right, up, fov_scale, focus_dist, disk_u, disk_v]
+ * with a zero defocus angle. */
+int32_t bajo_camera_make(const float* origin, const float* target, const float* world_up, float fov_scale,
+                         float* out20);
+int32_t bajo_camera_from_vfov(const float* origin, const float* target, const float* world_up, float vfov_deg,
+                              float* out20);
+
+/* Library version string. */
+const char* bajo_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BAJO_B200_H */

@@ -1,0 +1,1062 @@
+/*
+ * bajo_oracle.c -- CPU oracle for the LBVH build + closest-hit path.
+ *
+ * TEST INFRASTRUCTURE ONLY (see bajo_oracle.h).  Plain C11 + pthreads,
+ * compiled with -O2 -ffp-contract=off so that float arithmetic is rounded
+ * exactly as written.  Reference citations are paths inside jgsimard/bajo.
+ */
+#define _GNU_SOURCE
+#include "bajo_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define BO_FLT_MAX FLT_MAX
+/* Slack on the far slab distance: a box is entered when
+ * t_near <= t_far * (1 + 2^-20).  Keeps the closest hit independent of the
+ * traversal order (the reference compares t_near <= t_far exactly,
+ * bajo/core/intersect.mojo:213); the CUDA traversal uses the same constant. */
+#define BO_SLACK 1.00000095367431640625f
+
+/* ------------------------------------------------------------------------- */
+/* tiny thread pool                                                           */
+/* ------------------------------------------------------------------------- */
+typedef void (*bo_range_fn)(void* ctx, uint32_t begin, uint32_t end);
+
+typedef struct {
+  bo_range_fn fn;
+  void* ctx;
+  uint32_t n, chunk;
+  uint32_t next;
+  pthread_mutex_t mu;
+} bo_job;
+
+typedef struct {
+  bo_job* job;
+} bo_worker_arg;
+
+static void* bo_worker(void* p) {
+  bo_job* job = ((bo_worker_arg*)p)->job;
+  for (;;) {
+    uint32_t b;
+    pthread_mutex_lock(&job->mu);
+    b = job->next;
+    if (b < job->n) job->next = (job->n - b > job->chunk) ? b + job->chunk : job->n;
+    pthread_mutex_unlock(&job->mu);
+    if (b >= job->n) break;
+    uint32_t e = (job->n - b > job->chunk) ? b + job->chunk : job->n;
+    job->fn(job->ctx, b, e);
+  }
+  return NULL;
+}
+
+/* Runs fn over [0, n) in chunks on n_threads threads (the caller included). */
+static void bo_parallel_for(uint32_t n, uint32_t n_threads, uint32_t chunk,
+                            bo_range_fn fn, void* ctx) {
+  if (n == 0) return;
+  if (chunk == 0) chunk = 1;
+  if (n_threads <= 1 || n <= chunk) {
+    fn(ctx, 0, n);
+    return;
+  }
+  if (n_threads > 256) n_threads = 256;
+  bo_job job;
+  job.fn = fn;
+  job.ctx = ctx;
+  job.n = n;
+  job.chunk = chunk;
+  job.next = 0;
+  pthread_mutex_init(&job.mu, NULL);
+  pthread_t th[256];
+  bo_worker_arg arg = {&job};
+  for (uint32_t i = 1; i < n_threads; ++i) pthread_create(&th[i], NULL, bo_worker, &arg);
+  bo_worker(&arg);
+  for (uint32_t i = 1; i < n_threads; ++i) pthread_join(th[i], NULL);
+  pthread_mutex_destroy(&job.mu);
+}
+
+/* ------------------------------------------------------------------------- */
+/* vector helpers (bajo/core/vec.mojo)                                         */
+/* ------------------------------------------------------------------------- */
+typedef struct { float x, y, z; } v3;
+
+static inline v3 v3make(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline v3 v3sub(v3 a, v3 b) { return v3make(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 v3add(v3 a, v3 b) { return v3make(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 v3muls(v3 a, float s) { return v3make(a.x * s, a.y * s, a.z * s); }
+static inline v3 v3min(v3 a, v3 b) { return v3make(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
+static inline v3 v3max(v3 a, v3 b) { return v3make(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+/* dot = fma(a.x, b.x, fma(a.y, b.y, a.z * b.z))  -- vec.mojo:440 */
+static inline float v3dot(v3 a, v3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
+/* cross -- vec.mojo:522-526 */
+static inline v3 v3cross(v3 a, v3 b) {
+  return v3make(fmaf(a.y, b.z, -(a.z * b.y)), fmaf(a.z, b.x, -(a.x * b.z)),
+                fmaf(a.x, b.y, -(a.y * b.x)));
+}
+/* normalize -- vec.mojo:529-539 */
+static inline v3 v3normalize(v3 v) {
+  float l = sqrtf(v3dot(v, v));
+  float inv_l = (l > 1.0e-20f) ? 1.0f / l : 0.0f;
+  return v3muls(v, inv_l);
+}
+/* safe_inv -- vec.mojo:373-394 */
+static inline float safe_inv1(float e) { return (fabsf(e) > 1.0e-20f) ? 1.0f / e : 0.0f; }
+
+static inline v3 load3(const float* p) { return v3make(p[0], p[1], p[2]); }
+
+/* ------------------------------------------------------------------------- */
+/* a1: triangle bounds                                                        */
+/* ------------------------------------------------------------------------- */
+/* bajo/bvh/gpu/triangle_bvh.mojo:680-727: bmin = vmin(vmin(v0,v1),v2). */
+void bo_triangle_bounds(const float* verts, uint32_t n, float* b6) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* v = verts + (size_t)9 * i;
+    v3 a = load3(v), b = load3(v + 3), c = load3(v + 6);
+    v3 mn = v3min(v3min(a, b), c), mx = v3max(v3max(a, b), c);
+    float* o = b6 + (size_t)6 * i;
+    o[0] = mn.x; o[1] = mn.y; o[2] = mn.z;
+    o[3] = mx.x; o[4] = mx.y; o[5] = mx.z;
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* a2: segment bounds                                                         */
+/* ------------------------------------------------------------------------- */
+/* binary_layout.mojo:128-205 -- root AABB and centroid AABB per segment.
+ * AABB.invalid() is (+FLT_MAX, -FLT_MAX) (core/aabb.mojo:28); the centroid is
+ * (min + max) * 0.5 (core/aabb.mojo:53).  min/max are exact, so the reduction
+ * order of the reference's multi-level tree does not change the result. */
+void bo_segment_bounds(const float* b6, const uint32_t* so, uint32_t ns, float* out12) {
+  for (uint32_t s = 0; s < ns; ++s) {
+    v3 bmn = v3make(BO_FLT_MAX, BO_FLT_MAX, BO_FLT_MAX), bmx = v3make(-BO_FLT_MAX, -BO_FLT_MAX, -BO_FLT_MAX);
+    v3 cmn = bmn, cmx = bmx;
+    for (uint32_t i = so[s]; i < so[s + 1]; ++i) {
+      v3 mn = load3(b6 + (size_t)6 * i), mx = load3(b6 + (size_t)6 * i + 3);
+      bmn = v3min(bmn, mn);
+      bmx = v3max(bmx, mx);
+      v3 c = v3muls(v3add(mn, mx), 0.5f);
+      cmn = v3min(cmn, c);
+      cmx = v3max(cmx, c);
+    }
+    float* o = out12 + (size_t)12 * s;
+    o[0] = bmn.x; o[1] = bmn.y; o[2] = bmn.z; o[3] = bmx.x; o[4] = bmx.y; o[5] = bmx.z;
+    o[6] = cmn.x; o[7] = cmn.y; o[8] = cmn.z; o[9] = cmx.x; o[10] = cmx.y; o[11] = cmx.z;
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* a3: Morton                                                                 */
+/* ------------------------------------------------------------------------- */
+/* core/morton.mojo:48-58 */
+uint32_t bo_expand_bits_3d(uint32_t n) {
+  n = (n ^ (n << 16)) & 0xFF0000FFu;
+  n = (n ^ (n << 8)) & 0x0300F00Fu;
+  n = (n ^ (n << 4)) & 0x030C30C3u;
+  n = (n ^ (n << 2)) & 0x09249249u;
+  return n;
+}
+
+/* float -> u32 with truncation, clamped to [0, 1023]  (core/morton.mojo:78) */
+static inline uint32_t quantize1024(float c) {
+  float s = c * 1024.0f;
+  uint32_t u;
+  if (!(s > 0.0f)) u = 0;                 /* negatives and NaN -> 0 */
+  else if (s >= 4294967296.0f) u = 1023;  /* out of u32 range -> saturate */
+  else u = (uint32_t)s;
+  return u > 1023u ? 1023u : u;
+}
+
+/* core/morton.mojo:61-89: code = e(z)<<2 | e(y)<<1 | e(x). */
+uint32_t bo_morton3(float x, float y, float z) {
+  return (bo_expand_bits_3d(quantize1024(z)) << 2) | (bo_expand_bits_3d(quantize1024(y)) << 1) |
+         bo_expand_bits_3d(quantize1024(x));
+}
+
+/* core/morton.mojo:22-31: clz64((ca<<32|ia) ^ (cb<<32|ib)), 64 when equal. */
+int bo_morton_common_prefix(uint32_t ca, uint32_t ia, uint32_t cb, uint32_t ib) {
+  uint64_t x = (((uint64_t)ca << 32) | ia) ^ (((uint64_t)cb << 32) | ib);
+  return x ? __builtin_clzll(x) : 64;
+}
+
+/* binary_layout.mojo:116-125 */
+static uint32_t segment_for_item(const uint32_t* off, uint32_t n_off, uint32_t item) {
+  uint32_t lo = 0, hi = n_off - 1;
+  while (lo + 1 < hi) {
+    uint32_t mid = (lo + hi) / 2;
+    if (item < off[mid]) hi = mid; else lo = mid;
+  }
+  return lo;
+}
+
+/* bajo/bvh/gpu/builder/lbvh.mojo:30-62: normalise the leaf centroid over the
+ * segment's CENTROID bounds with safe_inv, key = (segment << 32) | morton,
+ * value = global item index. */
+void bo_morton_keys(const float* b6, const uint32_t* so, uint32_t ns, const float* sb12,
+                    uint32_t n, uint64_t* keys, uint32_t* values) {
+  for (uint32_t i = 0; i < n; ++i) {
+    uint32_t s = segment_for_item(so, ns + 1, i);
+    const float* cb = sb12 + (size_t)12 * s + 6;
+    v3 cmin = load3(cb), cmax = load3(cb + 3);
+    v3 ext = v3sub(cmax, cmin);
+    v3 inv = v3make(safe_inv1(ext.x), safe_inv1(ext.y), safe_inv1(ext.z));
+    v3 mn = load3(b6 + (size_t)6 * i), mx = load3(b6 + (size_t)6 * i + 3);
+    v3 c = v3muls(v3add(mn, mx), 0.5f);
+    v3 d = v3sub(c, cmin);
+    v3 u = v3make(d.x * inv.x, d.y * inv.y, d.z * inv.z);
+    keys[i] = ((uint64_t)s << 32) | bo_morton3(u.x, u.y, u.z);
+    values[i] = i;
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* a4/a5: stable LSD radix sort, 8-bit digits                                 */
+/* ------------------------------------------------------------------------- */
+/* bajo/bvh/cpu/builder/lbvh.mojo:36-62 (one counting pass per byte).  Any
+ * stable sort yields the same permutation; the digit range [begin_bit,
+ * end_bit) mirrors the library's API. */
+#define BO_SORT_IMPL(NAME, KT, HASV)                                              \
+  void NAME(KT* keys, uint32_t* vals, uint32_t n, int begin_bit, int end_bit) {   \
+    if (n == 0) return;                                                           \
+    KT* kt = (KT*)malloc(sizeof(KT) * n);                                         \
+    uint32_t* vt = HASV ? (uint32_t*)malloc(sizeof(uint32_t) * n) : NULL;         \
+    KT* ks = keys; KT* kd = kt;                                                   \
+    uint32_t* vs = vals; uint32_t* vd = vt;                                       \
+    for (int sh = begin_bit; sh < end_bit; sh += 8) {                             \
+      int bits = end_bit - sh < 8 ? end_bit - sh : 8;                             \
+      KT mask = (KT)((1u << bits) - 1u);                                          \
+      uint32_t cnt[256];                                                          \
+      memset(cnt, 0, sizeof cnt);                                                 \
+      for (uint32_t i = 0; i < n; ++i) cnt[(ks[i] >> sh) & mask]++;               \
+      uint32_t off[256], acc = 0;                                                 \
+      for (int b = 0; b < 256; ++b) { off[b] = acc; acc += cnt[b]; }              \
+      for (uint32_t i = 0; i < n; ++i) {                                          \
+        uint32_t d = (uint32_t)((ks[i] >> sh) & mask);                            \
+        uint32_t o = off[d]++;                                                    \
+        kd[o] = ks[i];                                                            \
+        if (HASV) vd[o] = vs[i];                                                  \
+      }                                                                           \
+      KT* tk = ks; ks = kd; kd = tk;                                              \
+      uint32_t* tv = vs; vs = vd; vd = tv;                                        \
+    }                                                                             \
+    if (ks != keys) {                                                             \
+      memcpy(keys, ks, sizeof(KT) * n);                                           \
+      if (HASV) memcpy(vals, vs, sizeof(uint32_t) * n);                           \
+    }                                                                             \
+    free(kt);                                                                     \
+    free(vt);                                                                     \
+  }
+
+BO_SORT_IMPL(bo_sort_pairs_u64, uint64_t, 1)
+BO_SORT_IMPL(bo_sort_pairs_u32, uint32_t, 1)
+static BO_SORT_IMPL(bo_sort_keys_u32_impl, uint32_t, 0)
+static BO_SORT_IMPL(bo_sort_keys_u64_impl, uint64_t, 0)
+void bo_sort_keys_u32(uint32_t* k, uint32_t n, int b, int e) { bo_sort_keys_u32_impl(k, NULL, n, b, e); }
+void bo_sort_keys_u64(uint64_t* k, uint32_t n, int b, int e) { bo_sort_keys_u64_impl(k, NULL, n, b, e); }
+
+/* ------------------------------------------------------------------------- */
+/* a7/a8: Karras topology                                                     */
+/* ------------------------------------------------------------------------- */
+/* binary_layout.mojo:219-223: internal count per segment = max(count-1, 0). */
+void bo_internal_offsets(const uint32_t* so, uint32_t ns, uint32_t* io) {
+  io[0] = 0;
+  for (uint32_t s = 0; s < ns; ++s) {
+    uint32_t c = so[s + 1] - so[s];
+    io[s + 1] = io[s] + (c > 0 ? c - 1 : 0);
+  }
+}
+
+/* lbvh.mojo:221-232 -- delta over segment-local sorted positions, -1 outside */
+static inline int cp_(const uint32_t* codes, int64_t len, int64_t i, int64_t j) {
+  if (j < 0 || j >= len) return -1;
+  return bo_morton_common_prefix(codes[i], (uint32_t)i, codes[j], (uint32_t)j);
+}
+
+/* lbvh.mojo:164-191 */
+static void find_range(const uint32_t* codes, int64_t len, int64_t i, int64_t* first, int64_t* last) {
+  int d_next = cp_(codes, len, i, i + 1);
+  int d_prev = cp_(codes, len, i, i - 1);
+  int64_t d = (d_next < d_prev) ? -1 : 1;
+  int delta_min = cp_(codes, len, i, i - d);
+  int64_t lmax = 2;
+  while (cp_(codes, len, i, i + lmax * d) > delta_min) {
+    lmax <<= 1;
+    if (lmax > len * 2) break;
+  }
+  int64_t l = 0;
+  for (int64_t t = lmax >> 1; t > 0; t >>= 1)
+    if (cp_(codes, len, i, i + (l + t) * d) > delta_min) l += t;
+  int64_t j = i + l * d;
+  *first = i < j ? i : j;
+  *last = i < j ? j : i;
+}
+
+/* lbvh.mojo:194-218 (identical to bajo/bvh/cpu/builder/lbvh.mojo:144-163) */
+static int64_t find_split(const uint32_t* codes, int64_t len, int64_t first, int64_t last) {
+  int node_prefix = cp_(codes, len, first, last);
+  int64_t split = first, step = last - first;
+  while (step > 1) {
+    step = (step + 1) >> 1;
+    int64_t ns = split + step;
+    if (ns < last && cp_(codes, len, first, ns) > node_prefix) split = ns;
+  }
+  return split;
+}
+
+static void set_invalid12(float* b) {
+  for (int k = 0; k < 2; ++k) {
+    b[6 * k + 0] = b[6 * k + 1] = b[6 * k + 2] = BO_FLT_MAX;
+    b[6 * k + 3] = b[6 * k + 4] = b[6 * k + 5] = -BO_FLT_MAX;
+  }
+}
+
+/* lbvh.mojo:235-255 (roots) + 257-329 (one internal node per step) */
+void bo_lbvh_topology(const uint32_t* codes_all, const uint32_t* so, const uint32_t* io, uint32_t ns,
+                      uint32_t* meta, uint32_t* leaf_parent, uint32_t* leaf_counts, uint32_t* roots,
+                      float* node_bounds) {
+  for (uint32_t s = 0; s < ns; ++s) {
+    uint32_t lb = so[s], le = so[s + 1];
+    if (le == lb) roots[s] = BO_SENTINEL;
+    else if (le - lb == 1) { roots[s] = BO_LEAF_FLAG | lb; leaf_parent[lb] = BO_SENTINEL; }
+    else roots[s] = io[s];
+  }
+  for (uint32_t s = 0; s < ns; ++s) {
+    uint32_t ib = io[s], lb = so[s];
+    int64_t len = (int64_t)so[s + 1] - lb;
+    const uint32_t* codes = codes_all + lb;
+    for (uint32_t i = ib; i < io[s + 1]; ++i) {
+      int64_t li = i - ib, first, last;
+      if (node_bounds) set_invalid12(node_bounds + (size_t)12 * i);
+      find_range(codes, len, li, &first, &last);
+      leaf_counts[i] = (uint32_t)(last - first + 1);
+      if (first == 0 && last == len - 1) meta[4 * (size_t)i + 0] = BO_SENTINEL;
+      int64_t split = find_split(codes, len, first, last);
+      uint32_t left = ib + (uint32_t)split, right = ib + (uint32_t)split + 1;
+      if (split == first) { left = BO_LEAF_FLAG | (lb + (uint32_t)split); leaf_parent[lb + split] = i; }
+      else meta[4 * (size_t)(ib + split) + 0] = i;
+      if (split + 1 == last) { right = BO_LEAF_FLAG | (lb + (uint32_t)split + 1); leaf_parent[lb + split + 1] = i; }
+      else meta[4 * (size_t)(ib + split + 1) + 0] = i;
+      meta[4 * (size_t)i + 1] = left;
+      meta[4 * (size_t)i + 2] = right;
+      meta[4 * (size_t)i + 3] = lb + (uint32_t)last;
+    }
+  }
+}
+
+/* Top-down restatement following bajo/bvh/cpu/builder/lbvh.mojo:270-315 but
+ * numbering nodes with the Karras rule, so it must reproduce
+ * bo_lbvh_topology exactly. */
+static void topdown_rec(const uint32_t* codes, int64_t len, uint32_t lb, uint32_t ib, uint32_t node,
+                        uint32_t parent, int64_t first, int64_t last, uint32_t* meta, uint32_t* lp,
+                        uint32_t* lc) {
+  for (;;) {
+    meta[4 * (size_t)node + 0] = parent;
+    lc[node] = (uint32_t)(last - first + 1);
+    meta[4 * (size_t)node + 3] = lb + (uint32_t)last;
+    int64_t split = find_split(codes, len, first, last);
+    uint32_t l, r;
+    if (split == first) { l = BO_LEAF_FLAG | (lb + (uint32_t)split); lp[lb + split] = node; }
+    else l = ib + (uint32_t)split;
+    if (split + 1 == last) { r = BO_LEAF_FLAG | (lb + (uint32_t)split + 1); lp[lb + split + 1] = node; }
+    else r = ib + (uint32_t)split + 1;
+    meta[4 * (size_t)node + 1] = l;
+    meta[4 * (size_t)node + 2] = r;
+    if (!(l & BO_LEAF_FLAG)) topdown_rec(codes, len, lb, ib, l, node, first, split, meta, lp, lc);
+    if (r & BO_LEAF_FLAG) return;
+    parent = node;
+    node = r;
+    first = split + 1;
+  }
+}
+
+void bo_lbvh_topology_topdown(const uint32_t* codes_all, const uint32_t* so, const uint32_t* io,
+                              uint32_t ns, uint32_t* meta, uint32_t* lp, uint32_t* lc, uint32_t* roots) {
+  for (uint32_t s = 0; s < ns; ++s) {
+    uint32_t lb = so[s], le = so[s + 1];
+    int64_t len = (int64_t)le - lb;
+    if (len == 0) { roots[s] = BO_SENTINEL; continue; }
+    if (len == 1) { roots[s] = BO_LEAF_FLAG | lb; lp[lb] = BO_SENTINEL; continue; }
+    roots[s] = io[s];
+    topdown_rec(codes_all + lb, len, lb, io[s], io[s], BO_SENTINEL, 0, len - 1, meta, lp, lc);
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* a9: refit                                                                  */
+/* ------------------------------------------------------------------------- */
+static void child_box(uint32_t ref, const float* lb6, const uint32_t* ids, const float* nb, float out[6]) {
+  if (ref & BO_LEAF_FLAG) {
+    memcpy(out, lb6 + (size_t)6 * ids[ref & 0x7FFFFFFFu], 6 * sizeof(float));
+  } else {
+    const float* b = nb + (size_t)12 * ref;
+    for (int k = 0; k < 3; ++k) {
+      out[k] = fminf(b[k], b[6 + k]);
+      out[3 + k] = fmaxf(b[3 + k], b[9 + k]);
+    }
+  }
+}
+
+/* lbvh.mojo:116-161 -- bottom-up climb with an arrival counter.  Processing
+ * nodes children-first gives the same values (min/max are exact) and the
+ * same final counters (2 per internal node). */
+void bo_lbvh_refit(const float* lb6, const uint32_t* ids, const uint32_t* meta, const uint32_t* lp,
+                   uint32_t n_leaves, uint32_t n_internal, float* nb, uint32_t* flags) {
+  (void)lp;
+  (void)n_leaves;
+  /* post-order over every tree: iterative, visiting children before parents */
+  uint8_t* done = (uint8_t*)calloc(n_internal ? n_internal : 1, 1);
+  uint32_t* stack = (uint32_t*)malloc(sizeof(uint32_t) * (n_internal ? n_internal : 1) * 2 + 16);
+  for (uint32_t root = 0; root < n_internal; ++root) {
+    if (meta[4 * (size_t)root] != BO_SENTINEL || done[root]) continue;
+    uint32_t sp = 0;
+    stack[sp++] = root;
+    while (sp) {
+      uint32_t node = stack[sp - 1];
+      uint32_t l = meta[4 * (size_t)node + 1], r = meta[4 * (size_t)node + 2];
+      int pushed = 0;
+      if (!(l & BO_LEAF_FLAG) && !done[l]) { stack[sp++] = l; pushed = 1; }
+      if (!(r & BO_LEAF_FLAG) && !done[r]) { stack[sp++] = r; pushed = 1; }
+      if (pushed) continue;
+      --sp;
+      child_box(l, lb6, ids, nb, nb + (size_t)12 * node);
+      child_box(r, lb6, ids, nb, nb + (size_t)12 * node + 6);
+      flags[node] = 2;
+      done[node] = 1;
+    }
+  }
+  free(stack);
+  free(done);
+}
+
+/* ------------------------------------------------------------------------- */
+/* full build                                                                 */
+/* ------------------------------------------------------------------------- */
+/* bajo/bvh/gpu/builder/lbvh.mojo:332-424 in order: bounds, Morton, sort of the
+ * live digits (bits 0..29 and the segment bits), gather low words, roots,
+ * topology, refit.  The caller allocates every array in BoLbvh. */
+void bo_lbvh_build(const float* verts, const uint32_t* so, uint32_t ns, BoLbvh* o) {
+  uint32_t n = so[ns];
+  o->n_leaves = n;
+  o->n_segments = ns;
+  o->seg_offsets = so;
+  bo_internal_offsets(so, ns, o->internal_offsets);
+  o->n_internal = o->internal_offsets[ns];
+  bo_triangle_bounds(verts, n, o->leaf_bounds);
+  bo_segment_bounds(o->leaf_bounds, so, ns, o->seg_bounds);
+  bo_morton_keys(o->leaf_bounds, so, ns, o->seg_bounds, n, o->sort_keys, o->leaf_ids);
+  int seg_bits = 0;
+  while (seg_bits < 32 && (ns - 1) >> seg_bits) ++seg_bits;
+  bo_sort_pairs_u64(o->sort_keys, o->leaf_ids, n, 0, 32 + seg_bits);
+  for (uint32_t i = 0; i < n; ++i) o->morton_codes[i] = (uint32_t)(o->sort_keys[i] & 0xFFFFFFFFu);
+  if (o->n_internal == 0) {
+    o->node_meta[0] = o->node_meta[1] = o->node_meta[2] = o->node_meta[3] = 0;
+    set_invalid12(o->node_bounds);
+    o->node_leaf_counts[0] = 0;
+    o->node_flags[0] = 0;
+  }
+  bo_lbvh_topology(o->morton_codes, so, o->internal_offsets, ns, o->node_meta, o->leaf_parent,
+                   o->node_leaf_counts, o->roots, o->n_internal ? o->node_bounds : NULL);
+  for (uint32_t i = 0; i < o->n_internal; ++i) o->node_flags[i] = 0;
+  bo_lbvh_refit(o->leaf_bounds, o->leaf_ids, o->node_meta, o->leaf_parent, n, o->n_internal,
+                o->node_bounds, o->node_flags);
+}
+
+/* ------------------------------------------------------------------------- */
+/* a12: camera                                                                */
+/* ------------------------------------------------------------------------- */
+/* camera.mojo:77-97 (defocus angle 0 -> zero disk vectors) */
+void bo_camera_make(const float o[3], const float t[3], const float up[3], float fov_scale, float out[20]) {
+  v3 org = load3(o), tgt = load3(t), wup = load3(up);
+  v3 fwd = v3normalize(v3sub(tgt, org));
+  v3 right = v3normalize(v3cross(fwd, wup));
+  v3 u = v3normalize(v3cross(right, fwd));
+  memset(out, 0, 20 * sizeof(float));
+  out[0] = org.x; out[1] = org.y; out[2] = org.z;
+  out[3] = fwd.x; out[4] = fwd.y; out[5] = fwd.z;
+  out[6] = right.x; out[7] = right.y; out[8] = right.z;
+  out[9] = u.x; out[10] = u.y; out[11] = u.z;
+  out[12] = fov_scale;
+  out[13] = 1.0f; /* focus distance */
+}
+
+/* camera.mojo:100-116: fov_scale = tan(radians(vfov) / 2) */
+void bo_camera_from_vfov(const float o[3], const float t[3], const float up[3], float vfov, float out[20]) {
+  float theta = vfov * (float)(3.14159265358979323846 / 180.0);
+  bo_camera_make(o, t, up, tanf(theta / 2.0f), out);
+}
+
+/* camera.mojo:137-154 make_ray_raster; camera_launch.mojo:34-55 view select */
+static void camera_ray(const float* cams, uint32_t idx, uint32_t w, uint32_t h, float inv_h, v3* o, v3* d) {
+  uint32_t ppv = w * h;
+  uint32_t view = idx / ppv, local = idx - view * ppv;
+  const float* c = cams + (size_t)20 * view;
+  uint32_t px = local % w, py = local / w;
+  float sx = (2.0f * ((float)px + 0.5f) - (float)w) * inv_h;
+  float sy = 1.0f - 2.0f * ((float)py + 0.5f) * inv_h;
+  float fs = c[12];
+  v3 fwd = load3(c + 3), right = load3(c + 6), up = load3(c + 9);
+  v3 dir = v3add(v3add(fwd, v3muls(right, sx * fs)), v3muls(up, sy * fs));
+  *o = load3(c);
+  *d = v3normalize(dir);
+}
+
+void bo_camera_rays(const float* cams, uint32_t n, uint32_t w, uint32_t h, float* rays) {
+  float inv_h = 1.0f / (float)h;
+  for (uint32_t i = 0; i < n; ++i) {
+    v3 o, d;
+    camera_ray(cams, i, w, h, inv_h, &o, &d);
+    rays[0 * (size_t)n + i] = o.x; rays[1 * (size_t)n + i] = o.y; rays[2 * (size_t)n + i] = o.z;
+    rays[3 * (size_t)n + i] = 0.0f;
+    rays[4 * (size_t)n + i] = d.x; rays[5 * (size_t)n + i] = d.y; rays[6 * (size_t)n + i] = d.z;
+    rays[7 * (size_t)n + i] = BO_FLT_MAX;
+  }
+}
+
+/* ------------------------------------------------------------------------- */
+/* a11: ray / box and ray / triangle                                          */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+  v3 o, d, rcp;
+  float tmin, tmax;
+  int kx, ky, kz;
+  float sx, sy, sz;
+  int par[3]; /* |d| <= 1e-9 on this axis */
+} bo_ray;
+
+static inline float idx3(v3 v, int k) { return k == 0 ? v.x : (k == 1 ? v.y : v.z); }
+
+/* ray.mojo:86-111 rcp_direction: |d| > 1e-9 ? 1/d : +-1e9 */
+static inline float rcp1(float d) {
+  const float eps = 1.0e-9f;
+  const float large = 1.0f / eps;
+  return fabsf(d) > eps ? 1.0f / d : (d < 0.0f ? -large : large);
+}
+
+static bo_ray make_ray(const float* rays, uint32_t n, uint32_t i) {
+  bo_ray r;
+  r.o = v3make(rays[i], rays[(size_t)n + i], rays[2 * (size_t)n + i]);
+  r.tmin = rays[3 * (size_t)n + i];
+  r.d = v3make(rays[4 * (size_t)n + i], rays[5 * (size_t)n + i], rays[6 * (size_t)n + i]);
+  r.tmax = rays[7 * (size_t)n + i];
+  r.rcp = v3make(rcp1(r.d.x), rcp1(r.d.y), rcp1(r.d.z));
+  r.par[0] = !(fabsf(r.d.x) > 1.0e-9f);
+  r.par[1] = !(fabsf(r.d.y) > 1.0e-9f);
+  r.par[2] = !(fabsf(r.d.z) > 1.0e-9f);
+  /* watertight set-up (Woop, Benthin, Wald, JCGT 2(1) 2013, section 3) */
+  float ax = fabsf(r.d.x), ay = fabsf(r.d.y), az = fabsf(r.d.z);
+  r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  r.kx = r.kz == 2 ? 0 : r.kz + 1;
+  r.ky = r.kx == 2 ? 0 : r.kx + 1;
+  float dz = idx3(r.d, r.kz);
+  if (dz < 0.0f) { int t = r.kx; r.kx = r.ky; r.ky = t; }
+  r.sx = idx3(r.d, r.kx) / dz;
+  r.sy = idx3(r.d, r.ky) / dz;
+  r.sz = 1.0f / dz;
+  return r;
+}
+
+/* one slab: (b - o) * rcp, except on axes the ray is parallel to
+ * (|d| <= 1e-9), which are tested by containment: [-inf, inf] when the origin
+ * lies inside [bmin, bmax], empty otherwise.  The reference's +-1e9 reciprocal
+ * (ray.mojo:86-111) gives a ray that runs exactly along a box face an empty
+ * slab; containment keeps such rays inside the (closed) box. */
+static inline void slab(float bmin, float bmax, float o, float rcp, int par, float* t0, float* t1) {
+  if (par) {
+    *t0 = bmin <= o ? -INFINITY : INFINITY;
+    *t1 = bmax >= o ? INFINITY : -INFINITY;
+  } else {
+    *t0 = (bmin - o) * rcp;
+    *t1 = (bmax - o) * rcp;
+  }
+}
+
+/* intersect.mojo:193-215 with the far bound scaled by BO_SLACK */
+static inline int box_hit(const bo_ray* r, const float* b, float tlimit, float* tnear) {
+  float t0x, t1x, t0y, t1y, t0z, t1z;
+  slab(b[0], b[3], r->o.x, r->rcp.x, r->par[0], &t0x, &t1x);
+  slab(b[1], b[4], r->o.y, r->rcp.y, r->par[1], &t0y, &t1y);
+  slab(b[2], b[5], r->o.z, r->rcp.z, r->par[2], &t0z, &t1z);
+  float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+  float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlimit));
+  *tnear = tn;
+  return tn <= tf * BO_SLACK;
+}
+
+typedef struct { float t, u, v; uint32_t prim; v3 n; } bo_hit;
+
+/* closest-hit order: smaller t wins, equal t goes to the lower prim id.  The
+ * reference keeps the first-visited candidate on ties (strict t < t_max,
+ * intersect.mojo:451). */
+static inline int better(float t, uint32_t prim, const bo_hit* h) {
+  return t < h->t || (t == h->t && prim < h->prim);
+}
+
+/* intersect.mojo:415-459 Moller-Trumbore with precomputed edges */
+static inline int tri_mt(const bo_ray* r, v3 v0, v3 e1, v3 e2, float* t, float* u, float* v) {
+  v3 p = v3cross(r->d, e2);
+  float det = v3dot(e1, p);
+  int det_ok = det > 1e-8f || det < -1e-8f;
+  float inv_det = 1.0f / det;
+  v3 tv = v3sub(r->o, v0);
+  float uu = v3dot(tv, p) * inv_det;
+  v3 q = v3cross(tv, e1);
+  float vv = v3dot(r->d, q) * inv_det;
+  float tt = v3dot(e2, q) * inv_det;
+  *t = tt; *u = uu; *v = vv;
+  return det_ok && uu >= 0.0f && uu <= 1.0f && vv >= 0.0f && (uu + vv) <= 1.0f && tt > r->tmin;
+}
+
+/* Woop/Benthin/Wald 2013, algorithm of section 3 (no backface culling):
+ * shear to ray space, 2D edge functions without contraction (so a shared edge
+ * evaluates to exactly opposite values on both triangles), double-precision
+ * re-evaluation when an edge function is exactly zero. */
+static inline int tri_wt(const bo_ray* r, v3 v0, v3 v1, v3 v2, float* t, float* u, float* v) {
+  v3 A = v3sub(v0, r->o), B = v3sub(v1, r->o), C = v3sub(v2, r->o);
+  float Akz = idx3(A, r->kz), Bkz = idx3(B, r->kz), Ckz = idx3(C, r->kz);
+  float Ax = idx3(A, r->kx) - r->sx * Akz, Ay = idx3(A, r->ky) - r->sy * Akz;
+  float Bx = idx3(B, r->kx) - r->sx * Bkz, By = idx3(B, r->ky) - r->sy * Bkz;
+  float Cx = idx3(C, r->kx) - r->sx * Ckz, Cy = idx3(C, r->ky) - r->sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return 0;
+  float det = U + V + W;
+  if (det == 0.0f) return 0;
+  float Az = r->sz * Akz, Bz = r->sz * Bkz, Cz = r->sz * Ckz;
+  float T = U * Az + V * Bz + W * Cz;
+  float tt = T / det;
+  *t = tt;
+  *u = V / det;
+  *v = W / det;
+  return tt > r->tmin;
+}
+
+/* one triangle, item id `item`, reported as `prim` */
+static inline void test_tri(const bo_ray* r, const float* verts, uint32_t item, uint32_t prim, int mode,
+                            bo_hit* h) {
+  const float* p = verts + (size_t)9 * item;
+  v3 v0 = load3(p), v1 = load3(p + 3), v2 = load3(p + 6);
+  v3 e1 = v3sub(v1, v0), e2 = v3sub(v2, v0);
+  float t, u, v;
+  int ok = mode == BO_TRI_MT ? tri_mt(r, v0, e1, e2, &t, &u, &v) : tri_wt(r, v0, v1, v2, &t, &u, &v);
+  if (ok && t < r->tmax && better(t, prim, h)) {
+    h->t = t; h->u = u; h->v = v; h->prim = prim;
+    h->n = v3normalize(v3cross(e1, e2));
+  }
+}
+
+static void store_hit(float* hits8, uint32_t i, const bo_hit* h) {
+  float* o = hits8 + (size_t)8 * i;
+  o[0] = h->u; o[1] = h->v;
+  memcpy(&o[2], &h->prim, 4);
+  uint32_t inst = BO_EMPTY;
+  memcpy(&o[3], &inst, 4);
+  o[4] = h->n.x; o[5] = h->n.y; o[6] = h->n.z;
+  o[7] = h->t;
+}
+
+static bo_hit miss_hit(float tmax) {
+  bo_hit h;
+  h.t = tmax; h.u = h.v = 0.0f; h.prim = BO_EMPTY; h.n = v3make(0, 0, 0);
+  return h;
+}
+
+/* Near-first BVH2 closest hit following the two-child loop of
+ * bajo/bvh/gpu/trace.mojo:340-428: test both child boxes against the current
+ * hit distance, intersect leaf children immediately, continue with the nearer
+ * internal child and push the other one if it is still within reach. */
+static bo_hit trace_one(const BoLbvh* bvh, const float* verts, const bo_ray* r, uint32_t seg, int mode,
+                        uint32_t* nodes_visited, uint32_t* tris_tested) {
+  bo_hit h = miss_hit(r->tmax);
+  uint32_t root = bvh->roots[seg];
+  /* prim ids are reported relative to the segment's first item
+   * (pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:117-120) */
+  uint32_t first_item = bvh->seg_offsets ? bvh->seg_offsets[seg] : 0;
+  uint32_t nv = 0, nt = 0;
+  if (root == BO_SENTINEL) goto done;
+  if (root & BO_LEAF_FLAG) {
+    uint32_t item = bvh->leaf_ids[root & 0x7FFFFFFFu];
+    test_tri(r, verts, item, item - first_item, mode, &h);
+    nt++;
+    goto done;
+  }
+  uint32_t stack[128];
+  uint32_t sp = 0, cur = root;
+  for (;;) {
+    nv++;
+    const float* b = bvh->node_bounds + (size_t)12 * cur;
+    uint32_t c[2] = {bvh->node_meta[4 * (size_t)cur + 1], bvh->node_meta[4 * (size_t)cur + 2]};
+    float ct[2];
+    int valid[2] = {0, 0};
+    /* both child boxes are tested against the same hit distance before any
+     * leaf is intersected (_intersect_trace_node_precomputed, trace.mojo:361) */
+    int bh[2];
+    float tn2[2];
+    for (int k = 0; k < 2; ++k) bh[k] = box_hit(r, b + 6 * k, h.t, &tn2[k]);
+    for (int k = 0; k < 2; ++k) {
+      float tn = tn2[k];
+      if (!bh[k]) continue;
+      if (c[k] & BO_LEAF_FLAG) {
+        uint32_t item = bvh->leaf_ids[c[k] & 0x7FFFFFFFu];
+        test_tri(r, verts, item, item - first_item, mode, &h);
+        nt++;
+      } else {
+        valid[k] = 1;
+        ct[k] = tn;
+      }
+    }
+    int near = -1;
+    if (valid[0]) near = 0;
+    if (valid[1] && (near == -1 || ct[1] < ct[0])) near = 1;
+    if (near >= 0) {
+      int far = 1 - near;
+      if (valid[far] && ct[far] <= h.t * BO_SLACK) stack[sp++] = c[far];
+      if (ct[near] <= h.t * BO_SLACK) { cur = c[near]; continue; }
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+done:
+  if (nodes_visited) *nodes_visited = nv;
+  if (tris_tested) *tris_tested = nt;
+  return h;
+}
+
+typedef struct {
+  const BoLbvh* bvh;
+  const float* verts;
+  const float* rays;
+  uint32_t n;
+  int mode;
+  float* hits;
+  uint32_t n_tris;
+} trace_ctx;
+
+static void trace_range(void* p, uint32_t b, uint32_t e) {
+  trace_ctx* c = (trace_ctx*)p;
+  for (uint32_t i = b; i < e; ++i) {
+    bo_ray r = make_ray(c->rays, c->n, i);
+    bo_hit h = trace_one(c->bvh, c->verts, &r, 0, c->mode, NULL, NULL);
+    store_hit(c->hits, i, &h);
+  }
+}
+
+void bo_trace_bvh2(const BoLbvh* bvh, const float* verts, const float* rays, uint32_t n, int mode,
+                   float* hits8, uint32_t n_threads) {
+  trace_ctx c = {bvh, verts, rays, n, mode, hits8, 0};
+  bo_parallel_for(n, n_threads, 1024, trace_range, &c);
+}
+
+void bo_trace_bvh2_stats(const BoLbvh* bvh, const float* verts, const float* rays, uint32_t n, int mode,
+                         uint32_t* stats) {
+  for (uint32_t i = 0; i < n; ++i) {
+    bo_ray r = make_ray(rays, n, i);
+    trace_one(bvh, verts, &r, 0, mode, &stats[2 * (size_t)i], &stats[2 * (size_t)i + 1]);
+  }
+}
+
+static void brute_range(void* p, uint32_t b, uint32_t e) {
+  trace_ctx* c = (trace_ctx*)p;
+  for (uint32_t i = b; i < e; ++i) {
+    bo_ray r = make_ray(c->rays, c->n, i);
+    bo_hit h = miss_hit(r.tmax);
+    for (uint32_t t = 0; t < c->n_tris; ++t) test_tri(&r, c->verts, t, t, c->mode, &h);
+    store_hit(c->hits, i, &h);
+  }
+}
+
+void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays, uint32_t n, int mode,
+                    float* hits8, uint32_t n_threads) {
+  trace_ctx c = {NULL, verts, rays, n, mode, hits8, n_tris};
+  bo_parallel_for(n, n_threads, 64, brute_range, &c);
+}
+
+/* ------------------------------------------------------------------------- */
+/* reference CPU builder (timed CPU baseline)                                 */
+/* ------------------------------------------------------------------------- */
+typedef struct { uint32_t code, item; } bo_mitem;
+
+typedef struct {
+  const float* verts;
+  uint32_t n;
+  float* bounds6;
+  float cmin[3], inv[3];
+  bo_mitem* pairs;
+  /* radix */
+  bo_mitem* src;
+  bo_mitem* dst;
+  int shift;
+  uint32_t workers;
+  uint32_t* counts;  /* workers x 256 */
+  uint32_t* offsets; /* workers x 256 */
+} cpu_build_ctx;
+
+static void cb_bounds(void* p, uint32_t b, uint32_t e) {
+  cpu_build_ctx* c = (cpu_build_ctx*)p;
+  bo_triangle_bounds(c->verts + (size_t)9 * b, e - b, c->bounds6 + (size_t)6 * b);
+}
+
+/* bajo/bvh/cpu/builder/lbvh.mojo:190-199 morton_worker */
+static void cb_morton(void* p, uint32_t b, uint32_t e) {
+  cpu_build_ctx* c = (cpu_build_ctx*)p;
+  for (uint32_t i = b; i < e; ++i) {
+    const float* bb = c->bounds6 + (size_t)6 * i;
+    float cx = (bb[0] + bb[3]) * 0.5f, cy = (bb[1] + bb[4]) * 0.5f, cz = (bb[2] + bb[5]) * 0.5f;
+    c->pairs[i].code = bo_morton3((cx - c->cmin[0]) * c->inv[0], (cy - c->cmin[1]) * c->inv[1],
+                                  (cz - c->cmin[2]) * c->inv[2]);
+    c->pairs[i].item = i;
+  }
+}
+
+/* bajo/bvh/cpu/builder/lbvh.mojo:65-112: per-worker histograms over
+ * contiguous chunks, offsets assigned bucket-major then worker-major (stable). */
+static void cb_hist(void* p, uint32_t b, uint32_t e) {
+  cpu_build_ctx* c = (cpu_build_ctx*)p;
+  for (uint32_t w = b; w < e; ++w) {
+    uint32_t* cnt = c->counts + 256 * (size_t)w;
+    memset(cnt, 0, 256 * sizeof(uint32_t));
+    uint32_t first = (uint32_t)((uint64_t)c->n * w / c->workers), end = (uint32_t)((uint64_t)c->n * (w + 1) / c->workers);
+    for (uint32_t i = first; i < end; ++i) cnt[(c->src[i].code >> c->shift) & 0xFF]++;
+  }
+}
+static void cb_scatter(void* p, uint32_t b, uint32_t e) {
+  cpu_build_ctx* c = (cpu_build_ctx*)p;
+  for (uint32_t w = b; w < e; ++w) {
+    uint32_t off[256];
+    memcpy(off, c->offsets + 256 * (size_t)w, sizeof off);
+    uint32_t first = (uint32_t)((uint64_t)c->n * w / c->workers), end = (uint32_t)((uint64_t)c->n * (w + 1) / c->workers);
+    for (uint32_t i = first; i < end; ++i) c->dst[off[(c->src[i].code >> c->shift) & 0xFF]++] = c->src[i];
+  }
+}
+
+typedef struct {
+  const bo_mitem* pairs;
+  int64_t len;
+  BoCpuNode* nodes;
+  uint32_t* item_indices;
+  const float* bounds6;
+  uint32_t next; /* atomic node allocator */
+} cpu_tree_ctx;
+
+static int cp_pairs(const bo_mitem* p, int64_t len, int64_t i, int64_t j) {
+  if (j < 0 || j >= len) return -1;
+  return bo_morton_common_prefix(p[i].code, (uint32_t)i, p[j].code, (uint32_t)j);
+}
+/* bajo/bvh/cpu/builder/lbvh.mojo:144-163 */
+static int64_t split_pairs(const bo_mitem* p, int64_t len, int64_t first, int64_t last) {
+  int np = cp_pairs(p, len, first, last);
+  int64_t split = first, step = last - first;
+  while (step > 1) {
+    step = (step + 1) >> 1;
+    int64_t ns = split + step;
+    if (ns < last && cp_pairs(p, len, first, ns) > np) split = ns;
+  }
+  return split;
+}
+
+static void node_set_box(BoCpuNode* nd, const float* mn, const float* mx) {
+  for (int k = 0; k < 3; ++k) { nd->bmin[k] = mn[k]; nd->bmax[k] = mx[k]; }
+}
+
+/* bajo/bvh/cpu/builder/lbvh.mojo:252-267 (leaf, leaf_size 1) and 401-437 */
+static void cpu_build_rec(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t count) {
+  BoCpuNode* nd = &c->nodes[node];
+  if (count <= 1) {
+    const float* b = c->bounds6 + (size_t)6 * c->item_indices[first];
+    node_set_box(nd, b, b + 3);
+    nd->left_or_first = (uint32_t)first;
+    nd->count = (uint32_t)count;
+    return;
+  }
+  int64_t last = first + count - 1;
+  int64_t split = split_pairs(c->pairs, c->len, first, last);
+  int64_t lc = split - first + 1;
+  uint32_t left = __atomic_fetch_add(&c->next, 2u, __ATOMIC_RELAXED);
+  cpu_build_rec(c, left, first, lc);
+  cpu_build_rec(c, left + 1, split + 1, count - lc);
+  BoCpuNode* L = &c->nodes[left];
+  BoCpuNode* R = &c->nodes[left + 1];
+  float mn[3], mx[3];
+  for (int k = 0; k < 3; ++k) { mn[k] = fminf(L->bmin[k], R->bmin[k]); mx[k] = fmaxf(L->bmax[k], R->bmax[k]); }
+  node_set_box(nd, mn, mx);
+  nd->left_or_first = left;
+  nd->count = 0;
+}
+
+typedef struct { uint32_t node; int64_t first, count; } frontier_task;
+typedef struct { cpu_tree_ctx* t; frontier_task* tasks; } frontier_ctx;
+
+static void cpu_collect(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t count, int depth,
+                        frontier_task* out, uint32_t* n_out) {
+  if (count <= 1 || depth == 0) {
+    out[(*n_out)++] = (frontier_task){node, first, count};
+    return;
+  }
+  int64_t last = first + count - 1;
+  int64_t split = split_pairs(c->pairs, c->len, first, last);
+  int64_t lc = split - first + 1;
+  uint32_t left = c->next;
+  c->next += 2;
+  c->nodes[node].left_or_first = left;
+  c->nodes[node].count = 0;
+  cpu_collect(c, left, first, lc, depth - 1, out, n_out);
+  cpu_collect(c, left + 1, split + 1, count - lc, depth - 1, out, n_out);
+}
+
+static void frontier_worker(void* p, uint32_t b, uint32_t e) {
+  frontier_ctx* f = (frontier_ctx*)p;
+  for (uint32_t k = b; k < e; ++k) {
+    frontier_task t = f->tasks[k];
+    for (int64_t i = t.first; i < t.first + t.count; ++i) f->t->item_indices[i] = f->t->pairs[i].item;
+    cpu_build_rec(f->t, t.node, t.first, t.count);
+  }
+}
+
+static void refit_frontier(BoCpuNode* nodes, uint32_t node, int depth) {
+  BoCpuNode* nd = &nodes[node];
+  if (depth == 0 || nd->count != 0) return;
+  uint32_t l = nd->left_or_first;
+  refit_frontier(nodes, l, depth - 1);
+  refit_frontier(nodes, l + 1, depth - 1);
+  for (int k = 0; k < 3; ++k) {
+    nd->bmin[k] = fminf(nodes[l].bmin[k], nodes[l + 1].bmin[k]);
+    nd->bmax[k] = fmaxf(nodes[l].bmax[k], nodes[l + 1].bmax[k]);
+  }
+}
+
+typedef struct { const float* b6; uint32_t n; float* part; } cbounds_ctx;
+
+/* bajo/bvh/cpu/builder/lbvh.mojo:166-216 + 318-359 */
+uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads, BoCpuNode* nodes,
+                           uint32_t* item_indices) {
+  if (n == 0) return 0;
+  if (n_threads == 0) n_threads = 1;
+  cpu_build_ctx c;
+  memset(&c, 0, sizeof c);
+  c.verts = verts;
+  c.n = n;
+  c.bounds6 = (float*)malloc(sizeof(float) * 6 * (size_t)n);
+  bo_parallel_for(n, n_threads, 8192, cb_bounds, &c);
+  /* centroid bounds (grown serially, as _sorted_morton_pairs does) */
+  float cmn[3] = {BO_FLT_MAX, BO_FLT_MAX, BO_FLT_MAX}, cmx[3] = {-BO_FLT_MAX, -BO_FLT_MAX, -BO_FLT_MAX};
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* b = c.bounds6 + (size_t)6 * i;
+    for (int k = 0; k < 3; ++k) {
+      float cc = (b[k] + b[3 + k]) * 0.5f;
+      cmn[k] = fminf(cmn[k], cc);
+      cmx[k] = fmaxf(cmx[k], cc);
+    }
+  }
+  for (int k = 0; k < 3; ++k) { c.cmin[k] = cmn[k]; c.inv[k] = safe_inv1(cmx[k] - cmn[k]); }
+  bo_mitem* pairs = (bo_mitem*)malloc(sizeof(bo_mitem) * n);
+  bo_mitem* scratch = (bo_mitem*)malloc(sizeof(bo_mitem) * n);
+  c.pairs = pairs;
+  bo_parallel_for(n, n_threads, 8192, cb_morton, &c);
+  /* stable LSD radix over the 32-bit code, workers over contiguous chunks */
+  uint32_t workers = n_threads < n ? n_threads : n;
+  c.workers = workers;
+  c.counts = (uint32_t*)malloc(sizeof(uint32_t) * 256 * workers);
+  c.offsets = (uint32_t*)malloc(sizeof(uint32_t) * 256 * workers);
+  bo_mitem* src = pairs;
+  bo_mitem* dst = scratch;
+  for (int sh = 0; sh < 32; sh += 8) {
+    c.src = src;
+    c.dst = dst;
+    c.shift = sh;
+    bo_parallel_for(workers, workers, 1, cb_hist, &c);
+    uint32_t acc = 0;
+    for (int b = 0; b < 256; ++b)
+      for (uint32_t w = 0; w < workers; ++w) { c.offsets[256 * w + b] = acc; acc += c.counts[256 * w + b]; }
+    bo_parallel_for(workers, workers, 1, cb_scatter, &c);
+    bo_mitem* t = src; src = dst; dst = t;
+  }
+  /* four passes: the sorted pairs are back in `pairs` */
+  cpu_tree_ctx t;
+  t.pairs = pairs;
+  t.len = n;
+  t.nodes = nodes;
+  t.item_indices = item_indices;
+  t.bounds6 = c.bounds6;
+  t.next = 1;
+  frontier_task tasks[16];
+  uint32_t nt = 0;
+  cpu_collect(&t, 0, 0, n, 3, tasks, &nt);
+  frontier_ctx f = {&t, tasks};
+  bo_parallel_for(nt, n_threads, 1, frontier_worker, &f);
+  refit_frontier(nodes, 0, 3);
+  uint32_t used = t.next;
+  free(c.counts);
+  free(c.offsets);
+  free(pairs);
+  free(scratch);
+  free(c.bounds6);
+  return used;
+}
+
+typedef struct {
+  const BoCpuNode* nodes;
+  const uint32_t* items;
+  const float* verts;
+  const float* rays;
+  uint32_t n;
+  int mode;
+  float* hits;
+} cpu_trace_ctx;
+
+static void cpu_trace_range(void* p, uint32_t b, uint32_t e) {
+  cpu_trace_ctx* c = (cpu_trace_ctx*)p;
+  for (uint32_t i = b; i < e; ++i) {
+    bo_ray r = make_ray(c->rays, c->n, i);
+    bo_hit h = miss_hit(r.tmax);
+    uint32_t stack[128], sp = 0;
+    uint32_t cur = 0;
+    float tn0;
+    float rb[6];
+    const BoCpuNode* root = &c->nodes[0];
+    for (int k = 0; k < 3; ++k) { rb[k] = root->bmin[k]; rb[3 + k] = root->bmax[k]; }
+    if (box_hit(&r, rb, h.t, &tn0)) {
+      for (;;) {
+        const BoCpuNode* nd = &c->nodes[cur];
+        if (nd->count) {
+          for (uint32_t k = 0; k < nd->count; ++k) {
+            uint32_t item = c->items[nd->left_or_first + k];
+            test_tri(&r, c->verts, item, item, c->mode, &h);
+          }
+        } else {
+          uint32_t l = nd->left_or_first;
+          float tl, tr;
+          float bl[6], br[6];
+          for (int k = 0; k < 3; ++k) {
+            bl[k] = c->nodes[l].bmin[k]; bl[3 + k] = c->nodes[l].bmax[k];
+            br[k] = c->nodes[l + 1].bmin[k]; br[3 + k] = c->nodes[l + 1].bmax[k];
+          }
+          int hl = box_hit(&r, bl, h.t, &tl), hr = box_hit(&r, br, h.t, &tr);
+          if (hl && hr) {
+            uint32_t nearc = tl <= tr ? l : l + 1, farc = tl <= tr ? l + 1 : l;
+            stack[sp++] = farc;
+            cur = nearc;
+            continue;
+          }
+          if (hl) { cur = l; continue; }
+          if (hr) { cur = l + 1; continue; }
+        }
+        if (!sp) break;
+        cur = stack[--sp];
+      }
+    }
+    store_hit(c->hits, i, &h);
+  }
+}
+
+void bo_cpu_trace(const BoCpuNode* nodes, const uint32_t* items, const float* verts, const float* rays,
+                  uint32_t n, int mode, float* hits8, uint32_t n_threads) {
+  cpu_trace_ctx c = {nodes, items, verts, rays, n, mode, hits8};
+  bo_parallel_for(n, n_threads, 1024, cpu_trace_range, &c);
+}

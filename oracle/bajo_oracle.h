@@ -1,0 +1,159 @@
+/*
+ * bajo_oracle.h -- CPU oracle for the LBVH build + closest-hit path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * (jgsimard/bajo, pure Mojo) algorithms on the GPU LBVH / traversal path.  It
+ * exists to check the CUDA library bit-for-bit and to provide the timed CPU
+ * baseline.  Nothing in the product library links, loads or calls it; only the
+ * tests, the smoke check and the benchmark's CPU-baseline leg do.
+ *
+ * Every function cites the reference file:line it follows.  Where this oracle
+ * deliberately differs from the reference it says so (tie rule, conservative
+ * box test, watertight triangle test).
+ *
+ * Floating point: compiled with -ffp-contract=off so that every product and
+ * sum is rounded exactly as written; fused multiply-adds appear only where the
+ * reference spells fma() itself (bajo/core/vec.mojo:440, :523-525).
+ */
+#ifndef BAJO_ORACLE_H
+#define BAJO_ORACLE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BO_SENTINEL 0xFFFFFFFFu   /* LBVH_SENTINEL, bajo/bvh/constants.mojo:6 */
+#define BO_LEAF_FLAG 0x80000000u  /* _BVH_LEAF_FLAG, bajo/bvh/tagged_ref.mojo:3 */
+#define BO_EMPTY 0xFFFFFFFFu      /* EMPTY_LANE / MISS_PRIM, constants.mojo:19-20 */
+
+/* triangle test selector */
+#define BO_TRI_MT 0          /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
+#define BO_TRI_WATERTIGHT 1  /* Woop/Benthin/Wald 2013 watertight test */
+
+/* ---- a1: per-triangle AABB (bajo/bvh/gpu/triangle_bvh.mojo:680) ---------- */
+void bo_triangle_bounds(const float* verts, uint32_t n, float* bounds6);
+
+/* ---- a2: per-segment root + centroid bounds, 12 floats per segment
+ *      (bajo/bvh/gpu/builder/binary_layout.mojo:128-205) -------------------- */
+void bo_segment_bounds(const float* bounds6, const uint32_t* seg_offsets,
+                       uint32_t n_segments, float* seg_bounds12);
+
+/* ---- a3: Morton composite keys (bajo/bvh/gpu/builder/lbvh.mojo:30) -------- */
+uint32_t bo_expand_bits_3d(uint32_t v);                  /* core/morton.mojo:48 */
+uint32_t bo_morton3(float x, float y, float z);          /* core/morton.mojo:61 */
+int bo_morton_common_prefix(uint32_t ca, uint32_t ia,
+                            uint32_t cb, uint32_t ib);   /* core/morton.mojo:22 */
+void bo_morton_keys(const float* bounds6, const uint32_t* seg_offsets,
+                    uint32_t n_segments, const float* seg_bounds12,
+                    uint32_t n, uint64_t* keys, uint32_t* values);
+
+/* ---- a4/a5: stable LSD radix sort, 8-bit digits --------------------------- */
+void bo_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint32_t n,
+                       int begin_bit, int end_bit);
+void bo_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t n,
+                       int begin_bit, int end_bit);
+void bo_sort_keys_u32(uint32_t* keys, uint32_t n, int begin_bit, int end_bit);
+void bo_sort_keys_u64(uint64_t* keys, uint32_t n, int begin_bit, int end_bit);
+
+/* ---- a8: internal segment offsets (binary_layout.mojo:219) --------------- */
+void bo_internal_offsets(const uint32_t* seg_offsets, uint32_t n_segments,
+                         uint32_t* internal_offsets);
+
+/* ---- a7/a8: Karras topology, bottom-up per node, GPU node numbering
+ *      (lbvh.mojo:164-330).  node_meta is 4 u32 per internal node
+ *      [parent, left, right, fence]; node_bounds (12 f32) initialised invalid.
+ * ------------------------------------------------------------------------- */
+void bo_lbvh_topology(const uint32_t* sorted_codes, const uint32_t* seg_offsets,
+                      const uint32_t* internal_offsets, uint32_t n_segments,
+                      uint32_t* node_meta, uint32_t* leaf_parent,
+                      uint32_t* node_leaf_counts, uint32_t* roots,
+                      float* node_bounds);
+/* Top-down cross-check (bajo/bvh/cpu/builder/lbvh.mojo:144,270): same tree,
+ * numbered with the Karras rule (root 0, children `split` / `split+1`). */
+void bo_lbvh_topology_topdown(const uint32_t* sorted_codes,
+                              const uint32_t* seg_offsets,
+                              const uint32_t* internal_offsets,
+                              uint32_t n_segments, uint32_t* node_meta,
+                              uint32_t* leaf_parent, uint32_t* node_leaf_counts,
+                              uint32_t* roots);
+
+/* ---- a9: refit (lbvh.mojo:116) -> node_bounds, node_flags (==2) ----------- */
+void bo_lbvh_refit(const float* leaf_bounds6, const uint32_t* leaf_ids,
+                   const uint32_t* node_meta, const uint32_t* leaf_parent,
+                   uint32_t n_leaves, uint32_t n_internal, float* node_bounds,
+                   uint32_t* node_flags);
+
+/* ---- full single-call build (Morton -> sort -> topology -> refit) --------- */
+typedef struct BoLbvh {
+  uint32_t n_leaves, n_internal, n_segments;
+  float* leaf_bounds;        /* 6 * n_leaves                */
+  float* seg_bounds;         /* 12 * n_segments             */
+  uint64_t* sort_keys;       /* n_leaves, sorted            */
+  uint32_t* leaf_ids;        /* n_leaves, sorted item ids   */
+  uint32_t* morton_codes;    /* n_leaves, sorted low words  */
+  uint32_t* node_meta;       /* 4 * max(n_internal,1)       */
+  float* node_bounds;        /* 12 * max(n_internal,1)      */
+  uint32_t* node_leaf_counts;/* max(n_internal,1)           */
+  uint32_t* node_flags;      /* max(n_internal,1)           */
+  uint32_t* leaf_parent;     /* n_leaves                    */
+  uint32_t* roots;           /* n_segments                  */
+  uint32_t* internal_offsets;/* n_segments + 1              */
+  const uint32_t* seg_offsets; /* n_segments + 1, set by bo_lbvh_build */
+} BoLbvh;
+void bo_lbvh_build(const float* verts, const uint32_t* seg_offsets,
+                   uint32_t n_segments, BoLbvh* out);
+
+/* ---- a12: camera (bajo/bvh/camera.mojo:19-154) ----------------------------- */
+/* 20-float camera record from origin/target/world_up and a vertical FOV in
+ * degrees (Camera.from_vfov, camera.mojo:100). */
+void bo_camera_from_vfov(const float origin[3], const float target[3],
+                         const float world_up[3], float vfov_deg,
+                         float out20[20]);
+/* Camera.__init__ with an explicit fov_scale (camera.mojo:77). */
+void bo_camera_make(const float origin[3], const float target[3],
+                    const float world_up[3], float fov_scale, float out20[20]);
+/* make_ray_raster (camera.mojo:137) via _camera_ray (camera_launch.mojo:34):
+ * writes rays SoA, 8 planes x n ([ox,oy,oz,tmin,dx,dy,dz,tmax]). */
+void bo_camera_rays(const float* cameras20, uint32_t n_rays, uint32_t width,
+                    uint32_t height, float* rays_soa);
+
+/* ---- a11: closest hit ------------------------------------------------------ */
+/* Hit AoS, 8 words per ray: [u, v, prim, inst, nx, ny, nz, t]
+ * (bajo/bvh/types.mojo:16-27).  Triangle records are read straight from the
+ * 9-float vertex buffer through leaf_ids. */
+void bo_trace_bvh2(const BoLbvh* bvh, const float* verts, const float* rays_soa,
+                   uint32_t n_rays, int tri_mode, float* hits8,
+                   uint32_t n_threads);
+/* All triangles, no BVH: the order-free reference answer. */
+void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays_soa,
+                    uint32_t n_rays, int tri_mode, float* hits8,
+                    uint32_t n_threads);
+/* per-ray node visits / triangle tests on the BVH2 (GpuTraversalStats,
+ * bajo/bvh/gpu/trace.mojo:62) -> stats[2*i] = nodes, stats[2*i+1] = tris */
+void bo_trace_bvh2_stats(const BoLbvh* bvh, const float* verts,
+                         const float* rays_soa, uint32_t n_rays, int tri_mode,
+                         uint32_t* stats);
+
+/* ---- reference CPU builder, timed CPU baseline ---------------------------- */
+/* bajo/bvh/cpu/builder/lbvh.mojo:166-359 restated with pthreads: parallel
+ * Morton, parallel stable LSD radix sort, top-down parallel frontier build
+ * (depth 3) with recursive AABB merge.  Returns the node count. */
+typedef struct BoCpuNode {
+  float bmin[3], bmax[3];
+  uint32_t left_or_first; /* internal: left child index; leaf: first item */
+  uint32_t count;         /* 0 = internal, else leaf item count          */
+} BoCpuNode;
+uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads,
+                           BoCpuNode* nodes /* 2n-1 */,
+                           uint32_t* item_indices /* n */);
+void bo_cpu_trace(const BoCpuNode* nodes, const uint32_t* item_indices,
+                  const float* verts, const float* rays_soa, uint32_t n_rays,
+                  int tri_mode, float* hits8, uint32_t n_threads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

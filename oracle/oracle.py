@@ -1,0 +1,335 @@
+"""ctypes wrapper around the C oracle (``oracle/libbajo_oracle.so``).
+
+TEST INFRASTRUCTURE ONLY.  The oracle is a CPU restatement of the reference's
+LBVH build and closest-hit path (jgsimard/bajo, Mojo); see ``bajo_oracle.h``
+for the per-function reference citations.  Only ``tests/``, the smoke check in
+``__graft_entry__.py`` and the CPU-baseline leg of ``bench.py`` may import this
+module.  The product library never loads it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "libbajo_oracle.so")
+
+TRI_MT = 0
+TRI_WATERTIGHT = 1
+SENTINEL = 0xFFFFFFFF
+LEAF_FLAG = 0x80000000
+EMPTY = 0xFFFFFFFF
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (idempotent)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        _lib = ctypes.CDLL(_LIB_PATH)
+        _declare(_lib)
+    return _lib
+
+
+_P = ctypes.c_void_p
+_U32 = ctypes.c_uint32
+_I = ctypes.c_int
+_F = ctypes.c_float
+
+
+class _BoLbvh(ctypes.Structure):
+    _fields_ = [
+        ("n_leaves", _U32), ("n_internal", _U32), ("n_segments", _U32),
+        ("leaf_bounds", _P), ("seg_bounds", _P), ("sort_keys", _P), ("leaf_ids", _P),
+        ("morton_codes", _P), ("node_meta", _P), ("node_bounds", _P),
+        ("node_leaf_counts", _P), ("node_flags", _P), ("leaf_parent", _P), ("roots", _P),
+        ("internal_offsets", _P), ("seg_offsets", _P),
+    ]
+
+
+def _declare(L: ctypes.CDLL) -> None:
+    sig = {
+        "bo_triangle_bounds": (None, [_P, _U32, _P]),
+        "bo_segment_bounds": (None, [_P, _P, _U32, _P]),
+        "bo_expand_bits_3d": (_U32, [_U32]),
+        "bo_morton3": (_U32, [_F, _F, _F]),
+        "bo_morton_common_prefix": (_I, [_U32, _U32, _U32, _U32]),
+        "bo_morton_keys": (None, [_P, _P, _U32, _P, _U32, _P, _P]),
+        "bo_sort_pairs_u64": (None, [_P, _P, _U32, _I, _I]),
+        "bo_sort_pairs_u32": (None, [_P, _P, _U32, _I, _I]),
+        "bo_sort_keys_u32": (None, [_P, _U32, _I, _I]),
+        "bo_sort_keys_u64": (None, [_P, _U32, _I, _I]),
+        "bo_internal_offsets": (None, [_P, _U32, _P]),
+        "bo_lbvh_topology": (None, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
+        "bo_lbvh_topology_topdown": (None, [_P, _P, _P, _U32, _P, _P, _P, _P]),
+        "bo_lbvh_refit": (None, [_P, _P, _P, _P, _U32, _U32, _P, _P]),
+        "bo_lbvh_build": (None, [_P, _P, _U32, ctypes.POINTER(_BoLbvh)]),
+        "bo_camera_from_vfov": (None, [_P, _P, _P, _F, _P]),
+        "bo_camera_make": (None, [_P, _P, _P, _F, _P]),
+        "bo_camera_rays": (None, [_P, _U32, _U32, _U32, _P]),
+        "bo_trace_bvh2": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _I, _P, _U32]),
+        "bo_trace_brute": (None, [_P, _U32, _P, _U32, _I, _P, _U32]),
+        "bo_trace_bvh2_stats": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _I, _P]),
+        "bo_cpu_build_lbvh": (_U32, [_P, _U32, _U32, _P, _P]),
+        "bo_cpu_trace": (None, [_P, _P, _P, _P, _U32, _I, _P, _U32]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+
+
+def _ptr(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+def n_threads() -> int:
+    return max(1, len(os.sched_getaffinity(0)))
+
+
+# ---------------------------------------------------------------- primitives
+def expand_bits_3d(v: int) -> int:
+    return lib().bo_expand_bits_3d(v)
+
+
+def morton3(x: float, y: float, z: float) -> int:
+    return lib().bo_morton3(x, y, z)
+
+
+def morton_common_prefix(ca: int, ia: int, cb: int, ib: int) -> int:
+    return lib().bo_morton_common_prefix(ca, ia, cb, ib)
+
+
+def triangle_bounds(verts: np.ndarray) -> np.ndarray:
+    v = np.ascontiguousarray(verts, dtype=np.float32).reshape(-1)
+    n = v.size // 9
+    out = np.empty(n * 6, np.float32)
+    lib().bo_triangle_bounds(_ptr(v), n, _ptr(out))
+    return out
+
+
+def segment_bounds(bounds6: np.ndarray, seg_offsets: np.ndarray) -> np.ndarray:
+    so = np.ascontiguousarray(seg_offsets, np.uint32)
+    ns = so.size - 1
+    out = np.empty(ns * 12, np.float32)
+    lib().bo_segment_bounds(_ptr(bounds6), _ptr(so), ns, _ptr(out))
+    return out
+
+
+def morton_keys(bounds6, seg_offsets, seg_bounds12):
+    so = np.ascontiguousarray(seg_offsets, np.uint32)
+    n = bounds6.size // 6
+    keys = np.empty(n, np.uint64)
+    vals = np.empty(n, np.uint32)
+    lib().bo_morton_keys(_ptr(bounds6), _ptr(so), so.size - 1, _ptr(seg_bounds12), n, _ptr(keys), _ptr(vals))
+    return keys, vals
+
+
+def sort_pairs(keys: np.ndarray, vals: np.ndarray, begin_bit=0, end_bit=None):
+    k = np.array(keys, copy=True)
+    v = np.array(vals, dtype=np.uint32, copy=True)
+    if end_bit is None:
+        end_bit = k.dtype.itemsize * 8
+    if k.dtype == np.uint64:
+        lib().bo_sort_pairs_u64(_ptr(k), _ptr(v), k.size, begin_bit, end_bit)
+    elif k.dtype == np.uint32:
+        lib().bo_sort_pairs_u32(_ptr(k), _ptr(v), k.size, begin_bit, end_bit)
+    else:
+        raise TypeError(k.dtype)
+    return k, v
+
+
+def sort_keys(keys: np.ndarray, begin_bit=0, end_bit=None):
+    k = np.array(keys, copy=True)
+    if end_bit is None:
+        end_bit = k.dtype.itemsize * 8
+    if k.dtype == np.uint64:
+        lib().bo_sort_keys_u64(_ptr(k), k.size, begin_bit, end_bit)
+    elif k.dtype == np.uint32:
+        lib().bo_sort_keys_u32(_ptr(k), k.size, begin_bit, end_bit)
+    else:
+        raise TypeError(k.dtype)
+    return k
+
+
+def internal_offsets(seg_offsets) -> np.ndarray:
+    so = np.ascontiguousarray(seg_offsets, np.uint32)
+    io = np.empty(so.size, np.uint32)
+    lib().bo_internal_offsets(_ptr(so), so.size - 1, _ptr(io))
+    return io
+
+
+def topology(codes, seg_offsets, topdown=False):
+    so = np.ascontiguousarray(seg_offsets, np.uint32)
+    ns = so.size - 1
+    io = internal_offsets(so)
+    ni = int(io[-1])
+    n = codes.size
+    meta = np.zeros(max(ni, 1) * 4, np.uint32)
+    lp = np.zeros(max(n, 1), np.uint32)
+    lc = np.zeros(max(ni, 1), np.uint32)
+    roots = np.zeros(max(ns, 1), np.uint32)
+    codes = np.ascontiguousarray(codes, np.uint32)
+    if topdown:
+        lib().bo_lbvh_topology_topdown(_ptr(codes), _ptr(so), _ptr(io), ns, _ptr(meta), _ptr(lp), _ptr(lc), _ptr(roots))
+    else:
+        lib().bo_lbvh_topology(_ptr(codes), _ptr(so), _ptr(io), ns, _ptr(meta), _ptr(lp), _ptr(lc), _ptr(roots), None)
+    return meta, lp, lc, roots
+
+
+# ---------------------------------------------------------------- full build
+@dataclass
+class OracleLbvh:
+    verts: np.ndarray
+    seg_offsets: np.ndarray
+    n_leaves: int
+    n_internal: int
+    leaf_bounds: np.ndarray
+    seg_bounds: np.ndarray
+    sort_keys: np.ndarray
+    leaf_ids: np.ndarray
+    morton_codes: np.ndarray
+    node_meta: np.ndarray
+    node_bounds: np.ndarray
+    node_leaf_counts: np.ndarray
+    node_flags: np.ndarray
+    leaf_parent: np.ndarray
+    roots: np.ndarray
+    internal_offsets: np.ndarray
+    _struct: _BoLbvh = None
+
+    def struct(self) -> _BoLbvh:
+        s = _BoLbvh()
+        s.n_leaves, s.n_internal, s.n_segments = self.n_leaves, self.n_internal, self.seg_offsets.size - 1
+        for name in ("leaf_bounds", "seg_bounds", "sort_keys", "leaf_ids", "morton_codes", "node_meta",
+                     "node_bounds", "node_leaf_counts", "node_flags", "leaf_parent", "roots",
+                     "internal_offsets", "seg_offsets"):
+            setattr(s, name, _ptr(getattr(self, name)))
+        return s
+
+
+def lbvh_build(verts: np.ndarray, seg_offsets=None) -> OracleLbvh:
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1)
+    n = v.size // 9
+    so = np.array([0, n] if seg_offsets is None else seg_offsets, np.uint32)
+    ns = so.size - 1
+    io = np.zeros(ns + 1, np.uint32)
+    lib().bo_internal_offsets(_ptr(so), ns, _ptr(io))
+    ni = int(io[-1])
+    m = max(ni, 1)
+    o = OracleLbvh(
+        verts=v, seg_offsets=so, n_leaves=n, n_internal=ni,
+        leaf_bounds=np.zeros(max(n, 1) * 6, np.float32), seg_bounds=np.zeros(ns * 12, np.float32),
+        sort_keys=np.zeros(max(n, 1), np.uint64), leaf_ids=np.zeros(max(n, 1), np.uint32),
+        morton_codes=np.zeros(max(n, 1), np.uint32), node_meta=np.zeros(m * 4, np.uint32),
+        node_bounds=np.zeros(m * 12, np.float32), node_leaf_counts=np.zeros(m, np.uint32),
+        node_flags=np.zeros(m, np.uint32), leaf_parent=np.zeros(max(n, 1), np.uint32),
+        roots=np.zeros(ns, np.uint32), internal_offsets=io,
+    )
+    s = o.struct()
+    lib().bo_lbvh_build(_ptr(v), _ptr(so), ns, ctypes.byref(s))
+    o._struct = s
+    return o
+
+
+# ---------------------------------------------------------------- camera/trace
+def camera_from_vfov(origin, target, world_up, vfov_deg) -> np.ndarray:
+    out = np.zeros(20, np.float32)
+    a = [np.ascontiguousarray(x, np.float32) for x in (origin, target, world_up)]
+    lib().bo_camera_from_vfov(_ptr(a[0]), _ptr(a[1]), _ptr(a[2]), float(vfov_deg), _ptr(out))
+    return out
+
+
+def camera_make(origin, target, world_up, fov_scale) -> np.ndarray:
+    out = np.zeros(20, np.float32)
+    a = [np.ascontiguousarray(x, np.float32) for x in (origin, target, world_up)]
+    lib().bo_camera_make(_ptr(a[0]), _ptr(a[1]), _ptr(a[2]), float(fov_scale), _ptr(out))
+    return out
+
+
+def camera_rays(cameras20: np.ndarray, n_rays: int, width: int, height: int) -> np.ndarray:
+    cams = np.ascontiguousarray(cameras20, np.float32)
+    out = np.empty(8 * n_rays, np.float32)
+    lib().bo_camera_rays(_ptr(cams), n_rays, width, height, _ptr(out))
+    return out
+
+
+def trace_bvh2(bvh: OracleLbvh, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT, threads=None) -> np.ndarray:
+    rays = np.ascontiguousarray(rays_soa, np.float32)
+    n = rays.size // 8
+    hits = np.empty(8 * n, np.float32)
+    s = bvh.struct()
+    lib().bo_trace_bvh2(ctypes.byref(s), _ptr(bvh.verts), _ptr(rays), n, tri_mode, _ptr(hits),
+                        threads or n_threads())
+    return hits
+
+
+def trace_bvh2_stats(bvh: OracleLbvh, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT) -> np.ndarray:
+    rays = np.ascontiguousarray(rays_soa, np.float32)
+    n = rays.size // 8
+    stats = np.empty(2 * n, np.uint32)
+    s = bvh.struct()
+    lib().bo_trace_bvh2_stats(ctypes.byref(s), _ptr(bvh.verts), _ptr(rays), n, tri_mode, _ptr(stats))
+    return stats
+
+
+def trace_brute(verts: np.ndarray, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT, threads=None) -> np.ndarray:
+    v = np.ascontiguousarray(verts, np.float32).reshape(-1)
+    rays = np.ascontiguousarray(rays_soa, np.float32)
+    n = rays.size // 8
+    hits = np.empty(8 * n, np.float32)
+    lib().bo_trace_brute(_ptr(v), v.size // 9, _ptr(rays), n, tri_mode, _ptr(hits), threads or n_threads())
+    return hits
+
+
+# ---------------------------------------------------------------- CPU baseline
+class CpuLbvh:
+    """The reference's CPU LBVH (BVH2, leaf size 1) restated in C; the timed
+    CPU baseline.  ``build`` returns the node count."""
+
+    NODE_DTYPE = np.dtype([("bmin", np.float32, 3), ("bmax", np.float32, 3), ("left_or_first", np.uint32),
+                           ("count", np.uint32)])
+
+    def __init__(self, verts: np.ndarray, threads=None):
+        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.n = self.verts.size // 9
+        self.threads = threads or n_threads()
+        self.nodes = np.zeros(max(2 * self.n - 1, 1), self.NODE_DTYPE)
+        self.items = np.zeros(max(self.n, 1), np.uint32)
+        self.node_count = 0
+
+    def build(self) -> int:
+        self.node_count = lib().bo_cpu_build_lbvh(_ptr(self.verts), self.n, self.threads, _ptr(self.nodes),
+                                                  _ptr(self.items))
+        return self.node_count
+
+    def trace(self, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT, hits=None) -> np.ndarray:
+        rays = np.ascontiguousarray(rays_soa, np.float32)
+        n = rays.size // 8
+        if hits is None:
+            hits = np.empty(8 * n, np.float32)
+        lib().bo_cpu_trace(_ptr(self.nodes), _ptr(self.items), _ptr(self.verts), _ptr(rays), n, tri_mode,
+                           _ptr(hits), self.threads)
+        return hits
+
+
+def hits_prim(hits8: np.ndarray) -> np.ndarray:
+    return hits8.reshape(-1, 8)[:, 2].view(np.uint32)
+
+
+def hits_t(hits8: np.ndarray) -> np.ndarray:
+    return hits8.reshape(-1, 8)[:, 7]

@@ -1,0 +1,127 @@
+"""GPU parity of closest-hit traversal against the oracle: bit-identical 8-word
+hits (prim ids, t, barycentrics, normals) for both triangle tests."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+from bajo_b200 import scenes  # noqa: E402
+
+
+def dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a)).cuda()
+
+
+def build(verts):
+    from bajo_b200 import bvh
+    b = bvh.build_triangle_bvh(dev(verts.astype(np.float32)))
+    return b
+
+
+def trace_rays(b, rays, mode):
+    n = rays.size // 8
+    hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+    t = torch.empty(n, dtype=torch.float32, device="cuda")
+    p = torch.empty(n, dtype=torch.int32, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    b.launch_rays(dev(rays), hits, n, tri_mode=mode, d_t=t, d_prim=p, d_status=st)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    hh = hits.cpu().numpy()
+    assert np.array_equal(hh.reshape(-1, 8)[:, 7].view(np.uint32), t.cpu().numpy().view(np.uint32))
+    assert np.array_equal(hh.reshape(-1, 8)[:, 2].view(np.uint32), p.cpu().numpy().view(np.uint32))
+    return hh
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_plain_lbvh_camera_matches_oracle(oracle, mode):
+    """65,536 triangles, 1024x1024 pinhole rays from (0.5, 0.5, -1.5), +z, 60 deg."""
+    from bajo_b200 import camera
+    v = scenes.random_triangles(65536, seed=0)
+    b = build(v)
+    cam = camera.plain_lbvh_camera()
+    n = 1024 * 1024
+    hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+    b.launch_camera(dev(cam), hits, n, 1024, 1024, tri_mode=mode)
+    torch.cuda.synchronize()
+    o = oracle.lbvh_build(v)
+    rays = oracle.camera_rays(cam, n, 1024, 1024)
+    ref = oracle.trace_bvh2(o, rays, mode)
+    got = hits.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert (oracle.hits_prim(got) != oracle.EMPTY).mean() > 0.1
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_random_rays_match_oracle(oracle, mode):
+    v = scenes.random_triangles(30000, seed=2, spread=0.03)
+    b = build(v)
+    rng = np.random.default_rng(5)
+    n = 200_000
+    o = rng.uniform(-0.5, 1.5, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    d[:100, 0] = 0.0  # axis-parallel components
+    d[100:200, 1:] = 0.0
+    rays = np.zeros((8, n), np.float32)
+    rays[0:3] = o.T
+    rays[3] = rng.uniform(0.0, 0.1, n)
+    rays[4:7] = d.T
+    rays[7] = rng.uniform(0.5, 5.0, n)
+    rays = rays.reshape(-1)
+    got = trace_rays(b, rays, mode)
+    ref = oracle.trace_bvh2(oracle.lbvh_build(v), rays, mode)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+FIXTURES = ["small", "single", "duplicate_centroid", "strip16", "two_depth", "degenerate_axis", "grid8",
+            "random1000"]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+@pytest.mark.parametrize("mode", [0, 1])
+def test_fixture_scenes(oracle, golden_dir, name, mode):
+    g = np.load(os.path.join(golden_dir, "lbvh_fixtures.npz"))
+    tg = np.load(os.path.join(golden_dir, "trace_fixtures.npz"))
+    verts = g[name + "__verts"]
+    rays = tg[name + "__rays"]
+    got = trace_rays(build(verts), rays, mode)
+    ref = oracle.trace_bvh2(oracle.lbvh_build(verts), rays, mode)
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    brute = oracle.trace_brute(verts, rays, mode)
+    assert np.array_equal(got.view(np.uint32), brute.view(np.uint32))
+    robust = tg[name + "__robust"]
+    assert np.array_equal(oracle.hits_prim(got)[robust], tg[name + "__prim"][robust])
+
+
+def test_shared_edges_lowest_prim(oracle):
+    v = scenes.grid_mesh(16, 16, z=0.5)
+    xs = np.linspace(0.0, 1.0, 17, dtype=np.float32)
+    pts = [(x, y) for x in xs[1:-1] for y in xs[1:-1]] + [(x + 1 / 32, y) for x in xs[:-1] for y in xs[1:-1]]
+    n = len(pts)
+    rays = np.zeros((8, n), np.float32)
+    for i, (x, y) in enumerate(pts):
+        rays[:, i] = [x, y, -1.0, 0.0, 0.0, 0.0, 1.0, np.finfo(np.float32).max]
+    rays = rays.reshape(-1)
+    got = trace_rays(build(v), rays, oracle.TRI_WATERTIGHT)
+    assert np.all(oracle.hits_prim(got) != oracle.EMPTY)
+    brute = oracle.trace_brute(v, rays, oracle.TRI_WATERTIGHT)
+    assert np.array_equal(got.view(np.uint32), brute.view(np.uint32))
+
+
+def test_large_scene_camera_property(oracle):
+    """2^20 triangles: GPU hits equal the oracle on a 256x256 camera."""
+    from bajo_b200 import camera
+    v = scenes.random_triangles(1 << 20, seed=1, spread=0.004)
+    b = build(v)
+    cam = camera.plain_lbvh_camera()
+    n = 256 * 256
+    hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+    b.launch_camera(dev(cam), hits, n, 256, 256)
+    torch.cuda.synchronize()
+    ref = oracle.trace_bvh2(oracle.lbvh_build(v), oracle.camera_rays(cam, n, 256, 256), oracle.TRI_WATERTIGHT)
+    assert np.array_equal(hits.cpu().numpy().view(np.uint32), ref.view(np.uint32))
