@@ -24,7 +24,6 @@ import ctypes
 import json
 import os
 import statistics
-import subprocess
 import sys
 import threading
 import time
@@ -80,53 +79,79 @@ def committed_traffic():
 
 # ----------------------------------------------------------------- clocks
 class ClockSampler:
-    REASONS = ["clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
-               "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+    """Samples SM clock and clock-event reasons through NVML every 5 ms while
+    the timed region runs (nvidia-smi's 200 ms loop is longer than the
+    region itself)."""
+    BITS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+            "hw_thermal_slowdown": 0x40, "hw_power_brake_slowdown": 0x80}
 
-    def __init__(self, index=0):
-        self.index = index
+    def __init__(self, device_index=0, period=0.005):
+        self.device_index = device_index
+        self.period = period
         self.samples = []
-        self.proc = None
-        self.thread = None
+        self.max_mhz = None
+        self._stop = threading.Event()
+        self._thread = None
+        self._h = None
+        self._nvml = None
+
+    def _handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        self._nvml = pynvml
+        try:
+            props = torch.cuda.get_device_properties(self.device_index)
+            bus = f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml.nvmlDeviceGetHandleByIndex(self.device_index)
+
+    def _sample(self):
+        n = self._nvml
+        sm = n.nvmlDeviceGetClockInfo(self._h, n.NVML_CLOCK_SM)
+        try:
+            reasons = n.nvmlDeviceGetCurrentClocksEventReasons(self._h)
+        except Exception:
+            reasons = n.nvmlDeviceGetCurrentClocksThrottleReasons(self._h)
+        self.samples.append((sm, reasons))
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                self._sample()
+            except Exception:
+                return
+            time.sleep(self.period)
 
     def __enter__(self):
-        q = "clocks.sm,clocks.max.sm,power.draw," + ",".join(self.REASONS)
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
-            self.thread.start()
+            self._h = self._handle()
+            self.max_mhz = self._nvml.nvmlDeviceGetMaxClockInfo(self._h, self._nvml.NVML_CLOCK_SM)
+            self._sample()
+            self._thread = threading.Thread(target=self._run, daemon=True)
+            self._thread.start()
         except Exception:
-            self.proc = None
+            self._h = None
         return self
 
-    def _read(self):
-        for line in self.proc.stdout:
-            parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 7:
-                self.samples.append(parts)
-
     def __exit__(self, *a):
-        if self.proc:
-            self.proc.terminate()
+        self._stop.set()
+        if self._thread:
+            self._thread.join(timeout=1)
+        if self._h is not None:
             try:
-                self.proc.wait(timeout=5)
+                self._sample()
             except Exception:
-                self.proc.kill()
+                pass
 
     def summary(self):
         if not self.samples:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        reasons = []
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for k, name in enumerate(names):
-            if any(s[3 + k].lower().startswith("active") for s in self.samples):
-                reasons.append(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": ["unsampled"]}
+        sm = [s[0] for s in self.samples]
+        reasons = sorted(name for name, bit in self.BITS.items() if any(r & bit for _, r in self.samples))
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(self.samples), "source": "nvml"}
 
 
 # ----------------------------------------------------------------- distributed
