@@ -25,6 +25,7 @@ STATUS_BAD_TOPOLOGY = 0x4
 TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
+SORT_NOALLOC_MAX_KEYS = 1 << 20
 
 _ERRORS = {
     ERR_INVALID_ARGUMENT: "invalid argument",
@@ -75,6 +76,7 @@ SIGNATURES = {
     "bajo_sort_pairs_u32": (_I32, [_P, _P, _U32, _I32, _I32, _P, _SZ, _P]),
     "bajo_sort_keys_u64": (_I32, [_P, _U32, _I32, _I32, _P, _SZ, _P]),
     "bajo_sort_pairs_u64": (_I32, [_P, _P, _U32, _I32, _I32, _P, _SZ, _P]),
+    "bajo_sort_pairs_u32_noalloc": (_I32, [_P, _P, _U32, _I32, _I32, _P, _P]),
     "bajo_lbvh_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoLbvhSizesC)]),
     "bajo_lbvh_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),

@@ -18,7 +18,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbajo_b200.so")
-SOURCES = ["sort.cu", "lbvh.cu", "trace.cu", "camera.cu"]
+SOURCES = ["sort.cu", "sort_static.cu", "lbvh.cu", "trace.cu", "camera.cu"]
 HEADERS = ["bajo_common.cuh", "onesweep.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

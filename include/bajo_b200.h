@@ -79,6 +79,22 @@ int32_t bajo_sort_keys_u64(uint64_t* d_keys, uint32_t n, int32_t begin_bit, int3
 int32_t bajo_sort_pairs_u64(uint64_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit, int32_t end_bit,
                             void* d_workspace, size_t workspace_bytes, void* stream);
 
+/* Sort without any allocation by the library or the caller, for callers that
+ * cannot call cudaMalloc or provide a workspace: hosts that own all device
+ * memory and pass only the buffers they compute on, or frame loops where an
+ * allocation would stall the device.  No counterpart in the reference.  Same
+ * result as bajo_sort_pairs_u32 (stable, in place).  Its scratch is one fixed
+ * device array inside the library (about 8.6 MB, held on every GPU that loads
+ * the library until exit), so n <= BAJO_SORT_NOALLOC_MAX_KEYS; larger n
+ * returns BAJO_ERR_TOO_LARGE.  All calls on a device share that array: calls
+ * whose device work overlaps race and must be serialised by the caller.  The
+ * first call on a device looks up the array's address; make it before any
+ * stream capture.  d_status (may be NULL) receives the BAJO_STATUS_* bits of
+ * this call. */
+#define BAJO_SORT_NOALLOC_MAX_KEYS (1u << 20)
+int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit,
+                                    int32_t end_bit, uint32_t* d_status, void* stream);
+
 /* ======================================================================== */
 /* LBVH build                                                                */
 /* ======================================================================== */
