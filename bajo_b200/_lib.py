@@ -26,6 +26,7 @@ TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
 SORT_NOALLOC_MAX_KEYS = 1 << 20
+SORT_VARIANTS = 4
 
 _ERRORS = {
     ERR_INVALID_ARGUMENT: "invalid argument",
@@ -77,6 +78,8 @@ SIGNATURES = {
     "bajo_sort_keys_u64": (_I32, [_P, _U32, _I32, _I32, _P, _SZ, _P]),
     "bajo_sort_pairs_u64": (_I32, [_P, _P, _U32, _I32, _I32, _P, _SZ, _P]),
     "bajo_sort_pairs_u32_noalloc": (_I32, [_P, _P, _U32, _I32, _I32, _P, _P]),
+    "bajo_sort_tuning_set": (_I32, [_U32, _I32, _U32, _I32]),
+    "bajo_sort_tuning_get": (_I32, [_U32, _I32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoLbvhSizesC)]),
     "bajo_lbvh_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
@@ -105,7 +108,20 @@ def load() -> ctypes.CDLL:
             fn.restype = res
             fn.argtypes = args
         _lib = lib
+        _install_tuning()
     return _lib
+
+
+def _install_tuning() -> None:
+    """Load the autotuner's cached tile choices for this GPU, if any."""
+    try:
+        import torch
+        if not torch.cuda.is_available():
+            return
+        from . import autotune
+        autotune.load()
+    except Exception:  # a missing or stale cache only means built-in choices
+        pass
 
 
 def check(code: int, what: str) -> None:

@@ -114,7 +114,16 @@ __device__ __forceinline__ void st_relaxed_gpu(uint32_t* p, uint32_t v) {
   asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Device status word bits (read back by bajo_status_read).
+// Fetch-add with acquire-release semantics at GPU scope: the writes before it
+// are visible to whoever reads its result, and the writes released by an
+// earlier atomic whose value it reads are visible after it.
+__device__ __forceinline__ uint32_t atomic_add_acq_rel_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.acq_rel.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+
+// Device status word bits (read back by bajo_workspace_status).
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bit) {
   if (status) atomicOr(status, bit);
 }

@@ -272,9 +272,9 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 //    (refit_lbvh_bounds_from_leaves_kernel, lbvh.mojo:116-161;
 //     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
 //    One thread per sorted leaf climbs towards the root; the first arrival at
-//    a node stops, the second merges both child boxes and continues.  Release
-//    / acquire fences around the arrival counter make the sibling's box
-//    visible (the reference uses relaxed atomics with no fence).
+//    a node stops, the second merges both child boxes and continues.  The
+//    arrival counter is an acquire-release atomic, which makes the sibling's
+//    box visible (the reference uses relaxed atomics with no fence).
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__ verts,
                                                        const uint32_t* __restrict__ leaf_ids, uint32_t n,
@@ -320,9 +320,9 @@ __global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__
     }
     float* slot = node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6);
     slot[0] = mn.x; slot[1] = mn.y; slot[2] = mn.z; slot[3] = mx.x; slot[4] = mx.y; slot[5] = mx.z;
-    __threadfence();
-    if (atomicAdd(&node_flags[parent], 1u) == 0) break;
-    __threadfence();
+    // release our slot, acquire the sibling's (the second arrival reads the
+    // first arrival's release)
+    if (atomic_add_acq_rel_gpu(&node_flags[parent], 1u) == 0) break;
     const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
     mn = vmin(mn, mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2)));
     mx = vmax(mx, mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5)));
@@ -334,10 +334,12 @@ __global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__
 // ---------------------------------------------------------------------------
 // host plan
 // ---------------------------------------------------------------------------
+// Build workspace: the sort plan of the u64 keys, with the per-segment
+// ordered bounds as the extra zeroed region.
 struct BuildPlan {
   onesweep::Plan sort;
   int end_bit;
-  size_t off_seg_ord, off_keys_alt, off_vals_alt, zero_bytes, total;
+  size_t off_seg_ord, off_keys_alt, off_vals_alt, total;
 };
 
 BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
@@ -346,32 +348,11 @@ BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
   while (seg_bits < 32 && ((n_seg - 1) >> seg_bits)) ++seg_bits;
   b.end_bit = 32 + seg_bits;
   const uint32_t passes = onesweep::num_passes(0, b.end_bit);
-  const uint32_t tile = onesweep::tile_keys<uint64_t, true>();
-  onesweep::Plan& p = b.sort;
-  p.n = n;
-  p.passes = passes;
-  p.tiles = (n + tile - 1) / tile;
-  size_t o = 256;
-  p.off_ghist = o;
-  o += (size_t)passes * 256 * 4;
-  p.off_counters = o;
-  o += (size_t)passes * 4;
-  o = (o + 15) & ~(size_t)15;
-  p.off_lookback = o;
-  o += (size_t)passes * p.tiles * 256 * 4;
-  b.off_seg_ord = o;
-  o += (size_t)n_seg * 12 * 4;
-  b.zero_bytes = o - p.off_ghist;
-  p.zero_bytes = b.zero_bytes;
-  o = onesweep::align256(o);
-  b.off_keys_alt = o;
-  o = onesweep::align256(o + (size_t)n * 8);
-  b.off_vals_alt = o;
-  o = onesweep::align256(o + (size_t)n * 4);
-  b.total = o;
-  p.off_keys_alt = b.off_keys_alt;
-  p.off_vals_alt = b.off_vals_alt;
-  p.total = b.total;
+  b.sort = onesweep::make_plan<uint64_t>(n, true, passes, (size_t)n_seg * 12 * 4);
+  b.off_seg_ord = b.sort.off_extra;
+  b.off_keys_alt = b.sort.off_keys_alt;
+  b.off_vals_alt = b.sort.off_vals_alt;
+  b.total = b.sort.total;
   return b;
 }
 
@@ -420,7 +401,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   if (!mark(0)) return BAJO_ERR_CUDA;
   unsigned char* ws = (unsigned char*)ws_;
   uint32_t* status = (uint32_t*)ws;
-  if (cudaMemsetAsync(ws + plan.sort.off_ghist, 0, plan.zero_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
+  if (cudaMemsetAsync(ws + plan.sort.off_zero, 0, plan.sort.zero_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
   uint32_t* seg_ord = (uint32_t*)(ws + plan.off_seg_ord);
   const uint32_t blocks = (n + kBlock - 1) / kBlock;
 
@@ -458,8 +439,9 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   }
   if (n > 1) {
     bool in_first = true;
+    const int variant = onesweep::choose_variant<uint64_t, true>(n, sm_count());
     if (onesweep::run_passes<uint64_t, true>(k0, v0, k1, v1, bvh->morton_codes, plan.sort, ws, 0, plan.end_bit, st,
-                                             &in_first, ev ? ev + 3 : nullptr) != cudaSuccess)
+                                             &in_first, variant, ev ? ev + 3 : nullptr) != cudaSuccess)
       return BAJO_ERR_CUDA;
   } else {
     // nothing to sort; keep the low word in step with the key

@@ -8,11 +8,14 @@
 //    onesweep.mojo:244,311,321, which truncates 64-bit keys);
 //  - digit ranking uses __match_any_sync on the digit (one instruction)
 //    instead of 8 ballots per key (bajo/sort/gpu/utils.mojo:46-103);
-//  - the look-back spin is bounded by elapsed time and reports
-//    BAJO_STATUS_LOOKBACK_TIMEOUT instead of spinning forever
-//    (onesweep.mojo:246-270);
+//  - the look-back loads a batch of predecessor flags at once and is bounded
+//    by elapsed time (BAJO_STATUS_LOOKBACK_TIMEOUT) instead of spinning
+//    forever one flag at a time (onesweep.mojo:246-270);
 //  - the per-pass global digit offsets are scanned inside each scatter CTA
 //    (one fewer launch than scan_global, onesweep.mojo:102);
+//  - two look-back regions alternate between passes and every pass clears the
+//    other region's slots, so only the first region needs a memset;
+//  - several tile shapes are compiled and chosen at run time (tuning table);
 //  - any digit range [begin_bit, end_bit) can be sorted, so constant key bits
 //    cost no pass.
 #pragma once
@@ -28,6 +31,7 @@ constexpr uint32_t kFlagInc = 2u << 30;   // inclusive prefix published
 constexpr uint32_t kFlagMask = 3u << 30;
 constexpr uint32_t kValueMask = (1u << 30) - 1u;
 constexpr uint64_t kLookbackTimeoutNs = 200ull * 1000ull * 1000ull;  // 200 ms
+constexpr int kLookbackBatch = 8;
 
 template <typename K>
 struct KeyTraits;
@@ -40,19 +44,65 @@ struct KeyTraits<uint64_t> {
   static constexpr uint64_t kMax = 0xFFFFFFFFFFFFFFFFull;
 };
 
-// Tile shapes (threads x keys per thread), chosen per key type.
+// ---------------------------------------------------------------------------
+// Tile shapes.  Variant 0 is the large default; smaller tiles give small
+// sorts more CTAs.  max_log2n: the largest sort (log2 of n) a variant may
+// serve, which bounds the look-back memory a workspace must hold.
+// ---------------------------------------------------------------------------
+constexpr int kNumVariants = 4;
+struct Shape {
+  int block, kpt, max_log2n;
+};
+template <typename K>
+struct Shapes;
+template <>
+struct Shapes<uint32_t> {
+  static constexpr Shape v[kNumVariants] = {{512, 15, 30}, {256, 15, 30}, {256, 8, 24}, {256, 4, 20}};
+};
+template <>
+struct Shapes<uint64_t> {
+  static constexpr Shape v[kNumVariants] = {{512, 11, 30}, {256, 11, 30}, {256, 6, 24}, {256, 3, 20}};
+};
+
+constexpr uint32_t ceil_log2(uint32_t n) {
+  uint32_t l = 0;
+  while (l < 32 && (1ull << l) < n) ++l;
+  return l;
+}
+template <typename K>
+constexpr bool variant_allowed(int v, uint32_t n) {
+  return v >= 0 && v < kNumVariants && ceil_log2(n) <= (uint32_t)Shapes<K>::v[v].max_log2n;
+}
+template <typename K>
+constexpr uint32_t variant_tile(int v) {
+  return (uint32_t)(Shapes<K>::v[v].block * Shapes<K>::v[v].kpt);
+}
+// smallest tile any allowed variant uses for n keys (sizes the look-back)
+template <typename K>
+constexpr uint32_t min_tile(uint32_t n) {
+  uint32_t t = variant_tile<K>(0);
+  for (int v = 1; v < kNumVariants; ++v)
+    if (variant_allowed<K>(v, n) && variant_tile<K>(v) < t) t = variant_tile<K>(v);
+  return t;
+}
+
+// Process-wide tuning table: variant per (key bytes, values, log2 n).  A
+// negative entry means "use the built-in choice".
+int tuned_variant(int key_bytes, bool has_values, uint32_t n);
+
 template <typename K, bool HAS_V>
-struct TileConfig;
-template <bool HAS_V>
-struct TileConfig<uint32_t, HAS_V> {
-  static constexpr int kBlock = 512;
-  static constexpr int kKpt = 15;
-};
-template <bool HAS_V>
-struct TileConfig<uint64_t, HAS_V> {
-  static constexpr int kBlock = 512;
-  static constexpr int kKpt = 11;
-};
+inline int choose_variant(uint32_t n, int sm_count) {
+  int v = tuned_variant((int)sizeof(K), HAS_V, n);
+  if (variant_allowed<K>(v, n)) return v;
+  // built-in: the largest tile that still gives every SM two tiles
+  for (int c = 0; c < kNumVariants; ++c) {
+    if (!variant_allowed<K>(c, n)) continue;
+    if ((n + variant_tile<K>(c) - 1) / variant_tile<K>(c) >= (uint32_t)(2 * sm_count)) return c;
+  }
+  for (int c = kNumVariants - 1; c >= 0; --c)
+    if (variant_allowed<K>(c, n)) return c;
+  return 0;
+}
 
 __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
   const uint32_t lane = lane_id();
@@ -90,7 +140,7 @@ __device__ __forceinline__ uint32_t scan256_exclusive(uint32_t v, uint32_t* tmp8
 // ---------------------------------------------------------------------------
 // Global digit histogram of every pass in one read of the keys
 // (global_histogram, onesweep.mojo:31-99).  Grid-strided over the keys;
-// each warp pair owns a private shared histogram copy to limit contention.
+// warps own private shared histogram copies to limit contention.
 // ---------------------------------------------------------------------------
 constexpr int kHistBlock = 256;
 constexpr int kHistCopies = 4;  // copies per pass inside a CTA
@@ -131,9 +181,10 @@ template <typename K, int BLOCK, int KPT>
 struct BinSmem {
   static constexpr int kWarps = BLOCK / 32;
   static constexpr int kTile = BLOCK * KPT;
+  static constexpr int kStage = kTile > kWarps * (int)kRadix ? kTile : kWarps * (int)kRadix;
   union {
-    K keys[kTile];
-    uint32_t vals[kTile];
+    K keys[kStage];
+    uint32_t vals[kStage];
     uint32_t warp_hist[kWarps * kRadix];
   } u;
   uint32_t digit_offset[kRadix];
@@ -143,12 +194,14 @@ struct BinSmem {
   uint32_t abort;  // a look-back wait timed out: publish, skip the scatter
 };
 
+// lookback: this pass's flags; lookback_next: the other region, whose slot of
+// this tile is cleared for the next pass.
 template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT>
-__global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
+__global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
     const K* __restrict__ keys_in, K* __restrict__ keys_out, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
-    uint32_t* __restrict__ lookback, uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ status,
-    uint32_t n, uint32_t shift, uint32_t digit_mask) {
+    uint32_t* __restrict__ lookback, uint32_t* __restrict__ lookback_next, uint32_t* __restrict__ tile_counter,
+    uint32_t* __restrict__ status, uint32_t n, uint32_t shift, uint32_t digit_mask) {
   using S = BinSmem<K, BLOCK, KPT>;
   constexpr int kWarps = S::kWarps;
   constexpr uint32_t kTile = S::kTile;
@@ -167,6 +220,7 @@ __global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
   const uint32_t tile = s.tile;
   const uint32_t tile_base = tile * kTile;
   const uint32_t valid = min(kTile, n - tile_base);
+  if (lookback_next && tid < kRadix) lookback_next[tile * kRadix + tid] = 0;
 
   // warp-striped load: key i of this thread sits at tile position
   // warp*32*KPT + 32*i + lane, so (warp, i, lane) order is position order.
@@ -225,7 +279,9 @@ __global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
   const uint32_t tstart = scan256_exclusive<BLOCK>(total, s.scan_tmp);
   const uint32_t gstart = scan256_exclusive<BLOCK>(gcount, s.scan_tmp);
 
-  // decoupled look-back over the preceding tiles, one thread per digit
+  // Decoupled look-back, one thread per digit.  The flags of up to
+  // kLookbackBatch predecessors are loaded at once (independent loads), so a
+  // chain of ready aggregates costs one L2 round trip per batch.
   if (tid < kRadix) {
     uint32_t excl = 0;
     if (tile > 0) {
@@ -233,15 +289,28 @@ __global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
       uint32_t spins = 0;
       uint64_t t0 = 0;
       while (k >= 0) {
-        uint32_t f = ld_relaxed_gpu(&lookback[(uint32_t)k * kRadix + tid]);
-        uint32_t flag = f & kFlagMask;
-        if (flag == kFlagInc) {
-          excl += f & kValueMask;
-          break;
+        uint32_t f[kLookbackBatch];
+#pragma unroll
+        for (int q = 0; q < kLookbackBatch; ++q)
+          f[q] = (k - q >= 0) ? ld_relaxed_gpu(&lookback[(uint32_t)(k - q) * kRadix + tid]) : kFlagInc;
+        int consumed = 0;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < kLookbackBatch; ++q) {
+          if (done || consumed != q) continue;  // stop at the first flag not ready
+          const uint32_t flag = f[q] & kFlagMask;
+          if (flag == kFlagInc) {
+            excl += f[q] & kValueMask;
+            done = true;
+          } else if (flag == kFlagAgg) {
+            excl += f[q] & kValueMask;
+            ++consumed;
+          }
         }
-        if (flag == kFlagAgg) {
-          excl += f & kValueMask;
-          --k;
+        if (done) break;
+        k -= consumed;
+        if (consumed > 0) {
+          spins = 0;
           continue;
         }
         // not ready: back off, give up after kLookbackTimeoutNs
@@ -313,36 +382,37 @@ __global__ void __launch_bounds__(BLOCK) onesweep_pass_kernel(
 // ---------------------------------------------------------------------------
 inline uint32_t num_passes(int begin_bit, int end_bit) { return (uint32_t)((end_bit - begin_bit + 7) / 8); }
 
-template <typename K, bool HAS_V>
-inline uint32_t tile_keys() {
-  return (uint32_t)(TileConfig<K, HAS_V>::kBlock * TileConfig<K, HAS_V>::kKpt);
-}
-
-inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 // Workspace of one sort: [status | ghist (P*256) | tile counters (P) |
-// lookback (P*tiles*256) | keys_alt | vals_alt].  The part from ghist to the
-// end of lookback must start zeroed every call; it is contiguous so that one
-// memset clears it.
+// look-back region 0 | look-back region 1 | keys_alt | vals_alt].  ghist,
+// the counters and region 0 must start zeroed (one memset of zero_bytes from
+// off_ghist); region 1 is cleared by the first pass.
+// An optional `extra` region (caller data that must also start zeroed) sits
+// between the status word and ghist, inside the zeroed range.
 struct Plan {
-  uint32_t n, passes, tiles;
-  size_t off_ghist, off_counters, off_lookback, zero_bytes, off_keys_alt, off_vals_alt, total;
+  uint32_t n, passes, tiles_cap;
+  size_t off_extra, off_zero, off_ghist, off_counters, off_lookback, zero_bytes, off_keys_alt, off_vals_alt, total;
 };
 
-inline Plan make_plan(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t passes, uint32_t tile) {
+constexpr Plan make_plan_tiles(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t passes,
+                               uint32_t tiles_cap, size_t extra_zero_bytes = 0) {
   Plan p{};
   p.n = n;
   p.passes = passes;
-  p.tiles = (n + tile - 1) / tile;
+  p.tiles_cap = tiles_cap;
   size_t o = 256;  // status word
+  p.off_extra = o;
+  p.off_zero = o;
+  o += (extra_zero_bytes + 15) & ~(size_t)15;
   p.off_ghist = o;
   o += (size_t)passes * kRadix * 4;
   p.off_counters = o;
   o += (size_t)passes * 4;
   o = (o + 15) & ~(size_t)15;
   p.off_lookback = o;
-  o += (size_t)passes * p.tiles * kRadix * 4;
-  p.zero_bytes = o - p.off_ghist;
+  p.zero_bytes = o + (size_t)tiles_cap * kRadix * 4 - p.off_zero;
+  o += 2 * (size_t)tiles_cap * kRadix * 4;
   o = align256(o);
   p.off_keys_alt = o;
   o = align256(o + (size_t)n * key_bytes);
@@ -352,13 +422,19 @@ inline Plan make_plan(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t 
   return p;
 }
 
-template <typename K, bool HAS_V, bool EMIT_LOW32>
-inline cudaError_t launch_pass(const K* kin, K* kout, const uint32_t* vin, uint32_t* vout, uint32_t* low32,
-                               const uint32_t* ghist, uint32_t* lookback, uint32_t* counter, uint32_t* status,
-                               uint32_t n, uint32_t tiles, uint32_t shift, uint32_t digit_mask,
-                               cudaStream_t stream) {
-  constexpr int B = TileConfig<K, HAS_V>::kBlock;
-  constexpr int KPT = TileConfig<K, HAS_V>::kKpt;
+template <typename K>
+constexpr Plan make_plan(uint32_t n, bool has_values, uint32_t passes, size_t extra_zero_bytes = 0) {
+  const uint32_t t = min_tile<K>(n);
+  return make_plan_tiles(n, (uint32_t)sizeof(K), has_values, passes, (n + t - 1) / t, extra_zero_bytes);
+}
+
+template <typename K, bool HAS_V, bool EMIT_LOW32, int V>
+inline cudaError_t launch_variant(const K* kin, K* kout, const uint32_t* vin, uint32_t* vout, uint32_t* low32,
+                                  const uint32_t* ghist, uint32_t* lb, uint32_t* lb_next, uint32_t* counter,
+                                  uint32_t* status, uint32_t n, uint32_t shift, uint32_t digit_mask,
+                                  cudaStream_t stream) {
+  constexpr int B = Shapes<K>::v[V].block;
+  constexpr int KPT = Shapes<K>::v[V].kpt;
   auto kern = onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
   const size_t smem = sizeof(BinSmem<K, B, KPT>);
   static bool configured[64] = {};  // per template instance and device
@@ -369,23 +445,52 @@ inline cudaError_t launch_pass(const K* kin, K* kout, const uint32_t* vin, uint3
     if (e != cudaSuccess) return e;
     if (dev >= 0 && dev < 64) configured[dev] = true;
   }
-  kern<<<tiles, B, smem, stream>>>(kin, kout, vin, vout, low32, ghist, lookback, counter, status, n, shift,
+  const uint32_t tiles = (n + B * KPT - 1) / (B * KPT);
+  kern<<<tiles, B, smem, stream>>>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter, status, n, shift,
                                    digit_mask);
   return cudaGetLastError();
 }
 
+template <typename K, bool HAS_V, bool EMIT_LOW32>
+inline cudaError_t launch_pass(int variant, const K* kin, K* kout, const uint32_t* vin, uint32_t* vout,
+                               uint32_t* low32, const uint32_t* ghist, uint32_t* lb, uint32_t* lb_next,
+                               uint32_t* counter, uint32_t* status, uint32_t n, uint32_t shift, uint32_t digit_mask,
+                               cudaStream_t stream) {
+  switch (variant) {
+    case 1:
+      return launch_variant<K, HAS_V, EMIT_LOW32, 1>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                     status, n, shift, digit_mask, stream);
+    case 2:
+      return launch_variant<K, HAS_V, EMIT_LOW32, 2>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                     status, n, shift, digit_mask, stream);
+    case 3:
+      return launch_variant<K, HAS_V, EMIT_LOW32, 3>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                     status, n, shift, digit_mask, stream);
+    default:
+      return launch_variant<K, HAS_V, EMIT_LOW32, 0>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                     status, n, shift, digit_mask, stream);
+  }
+}
+
 // Runs every digit pass of [begin_bit, end_bit) over keys that start in
 // (k0, v0); the workspace gives the other buffer (k1, v1).  The histograms in
-// `ghist` must already hold the counts of every pass.  Returns through
-// *result_in_first whether the sorted keys ended in (k0, v0).
+// the workspace must already hold the counts of every pass, and ghist, the
+// counters and look-back region 0 must be zero.  Returns through
+// *result_in_first whether the sorted keys ended in (k0, v0).  `variant`
+// selects the tile shape (it must be allowed for p.n); pass_events, when
+// given, receive one record after each pass.
 template <typename K, bool HAS_V>
 inline cudaError_t run_passes(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t* low32_last, const Plan& p,
                               unsigned char* ws, int begin_bit, int end_bit, cudaStream_t stream,
-                              bool* result_in_first, cudaEvent_t* pass_events = nullptr) {
+                              bool* result_in_first, int variant, cudaEvent_t* pass_events = nullptr) {
   uint32_t* status = reinterpret_cast<uint32_t*>(ws);
   uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + p.off_ghist);
   uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
-  uint32_t* lookback = reinterpret_cast<uint32_t*>(ws + p.off_lookback);
+  uint32_t* region[2] = {reinterpret_cast<uint32_t*>(ws + p.off_lookback),
+                         reinterpret_cast<uint32_t*>(ws + p.off_lookback) + (size_t)p.tiles_cap * kRadix};
+  if (!variant_allowed<K>(variant, p.n) ||
+      (p.n + variant_tile<K>(variant) - 1) / variant_tile<K>(variant) > p.tiles_cap)
+    return cudaErrorInvalidValue;
   K* src = k0;
   K* dst = k1;
   uint32_t* vs = v0;
@@ -394,15 +499,16 @@ inline cudaError_t run_passes(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t
     uint32_t sh = (uint32_t)begin_bit + 8 * pass;
     uint32_t bits = min(8u, (uint32_t)end_bit - sh);
     uint32_t mask = (1u << bits) - 1u;
-    uint32_t* lb = lookback + (size_t)pass * p.tiles * kRadix;
+    uint32_t* lb = region[pass & 1];
+    uint32_t* lb_next = (pass + 1 < p.passes) ? region[(pass + 1) & 1] : nullptr;
     cudaError_t e;
     bool last = pass + 1 == p.passes;
     if (last && low32_last)
-      e = launch_pass<K, HAS_V, true>(src, dst, vs, vd, low32_last, ghist + pass * kRadix, lb, counters + pass,
-                                      status, p.n, p.tiles, sh, mask, stream);
+      e = launch_pass<K, HAS_V, true>(variant, src, dst, vs, vd, low32_last, ghist + pass * kRadix, lb, lb_next,
+                                      counters + pass, status, p.n, sh, mask, stream);
     else
-      e = launch_pass<K, HAS_V, false>(src, dst, vs, vd, nullptr, ghist + pass * kRadix, lb, counters + pass,
-                                       status, p.n, p.tiles, sh, mask, stream);
+      e = launch_pass<K, HAS_V, false>(variant, src, dst, vs, vd, nullptr, ghist + pass * kRadix, lb, lb_next,
+                                       counters + pass, status, p.n, sh, mask, stream);
     if (e != cudaSuccess) return e;
     if (pass_events && (e = cudaEventRecord(pass_events[pass], stream)) != cudaSuccess) return e;
     K* t = src;

@@ -36,15 +36,9 @@ constexpr uint32_t kNoAllocPasses = 4;  // 32-bit keys, 8-bit digits
 // Scratch layout of a 32-bit key / 32-bit value sort of kNoAllocMaxKeys keys
 // (onesweep::make_plan): status word, histograms, tile counters, look-back
 // flags, alternate keys, alternate values.  Computed at compile time so the
-// array has a fixed size.
-constexpr size_t align256c(size_t x) { return (x + 255) & ~(size_t)255; }
-constexpr size_t kTileKeys = (size_t)onesweep::TileConfig<uint32_t, true>::kBlock *
-                             (size_t)onesweep::TileConfig<uint32_t, true>::kKpt;
-constexpr size_t kMaxTiles = (kNoAllocMaxKeys + kTileKeys - 1) / kTileKeys;
-constexpr size_t kLookbackEnd =
-    ((256 + kNoAllocPasses * 256 * 4 + kNoAllocPasses * 4 + 15) & ~(size_t)15) + kNoAllocPasses * kMaxTiles * 256 * 4;
+// array has a fixed size; smaller sorts use a prefix-compatible, smaller plan.
 constexpr size_t kNoAllocScratchBytes =
-    align256c(align256c(align256c(kLookbackEnd) + (size_t)kNoAllocMaxKeys * 4) + (size_t)kNoAllocMaxKeys * 4);
+    onesweep::make_plan<uint32_t>(kNoAllocMaxKeys, true, kNoAllocPasses).total;
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -80,7 +74,7 @@ extern "C" int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_val
   if (n > kNoAllocMaxKeys) return BAJO_ERR_TOO_LARGE;
   if (n > 0 && (!d_keys || !d_vals)) return BAJO_ERR_INVALID_ARGUMENT;
   const uint32_t passes = onesweep::num_passes(begin_bit, end_bit);
-  const onesweep::Plan p = onesweep::make_plan(n, 4, true, passes, onesweep::tile_keys<uint32_t, true>());
+  const onesweep::Plan p = onesweep::make_plan<uint32_t>(n, true, passes);
   if (p.total > kNoAllocScratchBytes) return BAJO_ERR_TOO_LARGE;
   cudaStream_t stream = (cudaStream_t)stream_;
   void* base = nullptr;
@@ -90,7 +84,7 @@ extern "C" int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_val
   // every counter / flag that must start at zero
   if (cudaMemsetAsync(w, 0, 4, stream) != cudaSuccess) return BAJO_ERR_CUDA;
   if (n > 1 && passes > 0) {
-    if (cudaMemsetAsync(w + p.off_ghist, 0, p.zero_bytes, stream) != cudaSuccess) return BAJO_ERR_CUDA;
+    if (cudaMemsetAsync(w + p.off_zero, 0, p.zero_bytes, stream) != cudaSuccess) return BAJO_ERR_CUDA;
     uint32_t* ghist = (uint32_t*)(w + p.off_ghist);
     const size_t hsmem = (size_t)passes * onesweep::kHistCopies * onesweep::kRadix * 4;
     uint32_t grid = (n + onesweep::kHistBlock * 16 - 1) / (onesweep::kHistBlock * 16);
@@ -103,8 +97,9 @@ extern "C" int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_val
     uint32_t* kalt = (uint32_t*)(w + p.off_keys_alt);
     uint32_t* valt = (uint32_t*)(w + p.off_vals_alt);
     bool in_first = true;
+    const int variant = onesweep::choose_variant<uint32_t, true>(n, sm_count());
     if (onesweep::run_passes<uint32_t, true>(d_keys, d_vals, kalt, valt, nullptr, p, w, begin_bit, end_bit, stream,
-                                             &in_first) != cudaSuccess)
+                                             &in_first, variant) != cudaSuccess)
       return BAJO_ERR_CUDA;
     if (!in_first) {
       if (cudaMemcpyAsync(d_keys, kalt, (size_t)n * 4, cudaMemcpyDeviceToDevice, stream) != cudaSuccess ||

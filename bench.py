@@ -54,6 +54,12 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune"],
+                   help="time one piece alone (profiling runs) instead of the benchmark line")
+    p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
+    p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
+    p.add_argument("--end-bit", type=int, default=None, help="--case sort: sort bits [0, end-bit)")
+    p.add_argument("--keys-only", action="store_true", help="--case sort without payload")
     return p.parse_args()
 
 
@@ -510,8 +516,73 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak):
     return out
 
 
+def run_case(args):
+    """One piece of the path alone, for ncu captures and tuning runs."""
+    import torch
+    from bajo_b200 import build as B
+    B.build()
+    from bajo_b200 import autotune, bvh, camera, sort
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream()
+    n = args.n
+    out = {"case": args.case, "n": n}
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    if args.case == "tune":
+        out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
+        out["device"] = autotune.device_key()
+    elif args.case == "sort":
+        kb = args.bits // 8
+        g = torch.Generator(device="cuda").manual_seed(0)
+        dt = torch.int32 if kb == 4 else torch.int64
+        keys = torch.randint(-2**31, 2**31, (n,), dtype=dt, device="cuda", generator=g)
+        vals = None if args.keys_only else torch.arange(n, dtype=torch.int32, device="cuda")
+        end_bit = args.end_bit or args.bits
+        ws = sort.RadixSortWorkspace(n, kb, vals is not None, 0, end_bit)
+        if vals is None:
+            ms = timed(lambda: sort.onesweep_radix_sort_keys(keys, workspace=ws, end_bit=end_bit))
+        else:
+            ms = timed(lambda: sort.onesweep_radix_sort_pairs(keys, vals, workspace=ws, end_bit=end_bit))
+        v = ctypes.c_int32(0)
+        from bajo_b200 import _lib
+        _lib.load().bajo_sort_tuning_get(kb, int(vals is not None), n, ctypes.byref(v))
+        out.update({"bits": args.bits, "end_bit": end_bit, "pairs": vals is not None, "ms": round(ms, 5),
+                    "gkeys_s": round(n / ms / 1e6, 3), "variant": v.value, "status": ws.status()})
+    elif args.case in ("build", "trace"):
+        from bajo_b200 import scenes
+        verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
+        ws = bvh.GpuBvhBuildWorkspace(n, 1)
+        tree = bvh.build_triangle_bvh(verts, workspace=ws)
+        if args.case == "build":
+            ms = timed(lambda: bvh.build_triangle_bvh(verts, workspace=ws, out=tree))
+            out.update({"ms": round(ms, 5), "mtri_s": round(n / ms / 1e3, 2)})
+        else:
+            cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+            hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
+            ms = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
+            out.update({"ms": round(ms, 5), "mrays_s": round(WIDTH * HEIGHT / ms / 1e3, 2)})
+        out["status"] = ws.status()
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.case:
+        run_case(args)
+        return
     if args.impl == "reference":
         run_reference(args)
         return

@@ -142,3 +142,50 @@ def test_full_size_properties(n, kind):
     # stability: equal keys keep increasing payloads
     eq = sk[1:] == sk[:-1]
     assert bool((vals[1:][eq] > vals[:-1][eq]).all())
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("kind", ["u32", "u64"])
+def test_every_tile_variant_matches_oracle(oracle, variant, kind):
+    """Each compiled tile shape the autotuner may pick sorts exactly."""
+    from bajo_b200 import _lib
+    L = _lib.load()
+    kb = 4 if kind == "u32" else 8
+    rng = np.random.default_rng(variant)
+    try:
+        for n in (1000, 70_001, 300_000):
+            lg = int(np.ceil(np.log2(n)))
+            assert L.bajo_sort_tuning_set(kb, 1, lg, variant) == _lib.OK
+            assert L.bajo_sort_tuning_set(kb, 0, lg, variant) == _lib.OK
+            if kb == 4:
+                keys = rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+            else:
+                keys = rng.integers(0, 2**62, size=n, dtype=np.uint64)
+            keys[: n // 4] = keys[0]  # long runs of equal keys
+            vals = np.arange(n, dtype=np.uint32)
+            k, v = gpu_sort(keys, vals)
+            ok, ov = oracle.sort_pairs(keys, vals)
+            assert np.array_equal(k, ok) and np.array_equal(v, ov)
+            k2, _ = gpu_sort(keys, None)
+            assert np.array_equal(k2, ok)
+    finally:
+        for lg in range(33):
+            L.bajo_sort_tuning_set(kb, 1, lg, -1)
+            L.bajo_sort_tuning_set(kb, 0, lg, -1)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_lbvh_build_with_every_variant(oracle, variant):
+    from bajo_b200 import _lib, bvh, scenes
+    L = _lib.load()
+    v = scenes.random_triangles(50_000, seed=variant)
+    lg = int(np.ceil(np.log2(50_000)))
+    try:
+        assert L.bajo_sort_tuning_set(8, 1, lg, variant) == _lib.OK
+        b = bvh.build_triangle_bvh(torch.from_numpy(v).cuda())
+        torch.cuda.synchronize()
+        o = oracle.lbvh_build(v)
+        assert np.array_equal(b.leaf_ids.cpu().numpy().view(np.uint32), o.leaf_ids)
+        assert np.array_equal(b.node_meta.cpu().numpy().view(np.uint32)[: 4 * 49_999], o.node_meta[: 4 * 49_999])
+    finally:
+        L.bajo_sort_tuning_set(8, 1, lg, -1)
