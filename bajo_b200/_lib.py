@@ -87,6 +87,11 @@ SIGNATURES = {
     "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera_stats": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P]),
+    "bajo_rt_build_lights": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(_U32),
+                                    ctypes.POINTER(_F)]),
+    "bajo_render_workspace_size": (_I32, [_P, ctypes.POINTER(_SZ)]),
+    "bajo_render": (_I32, [_P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "bajo_render_stats": (_I32, [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
     "bajo_camera_make": (_I32, [_P, _P, _P, _F, _P]),
     "bajo_camera_from_vfov": (_I32, [_P, _P, _P, _F, _P]),
     "bajo_version": (ctypes.c_char_p, []),

@@ -118,8 +118,8 @@ def load(path: str = CACHE) -> int:
 def tune_all(reps: int = 5, save_cache: bool = True) -> dict:
     """The shapes the LBVH build and the sort sweep use."""
     res = {
-        _kernel_key(8, True): tune_sort(8, True, range(10, 27, 2), end_bit=44, reps=reps),
-        _kernel_key(4, True): tune_sort(4, True, range(10, 27, 2), reps=reps),
+        _kernel_key(8, True): tune_sort(8, True, range(10, 27), end_bit=44, reps=reps),
+        _kernel_key(4, True): tune_sort(4, True, range(10, 27), reps=reps),
     }
     if save_cache:
         save(res)

@@ -57,11 +57,11 @@ template <typename K>
 struct Shapes;
 template <>
 struct Shapes<uint32_t> {
-  static constexpr Shape v[kNumVariants] = {{512, 15, 30}, {256, 15, 30}, {256, 8, 24}, {256, 4, 20}};
+  static constexpr Shape v[kNumVariants] = {{512, 12, 30}, {256, 12, 30}, {256, 8, 24}, {256, 4, 20}};
 };
 template <>
 struct Shapes<uint64_t> {
-  static constexpr Shape v[kNumVariants] = {{512, 11, 30}, {256, 11, 30}, {256, 6, 24}, {256, 3, 20}};
+  static constexpr Shape v[kNumVariants] = {{512, 8, 30}, {256, 8, 30}, {256, 5, 24}, {256, 3, 20}};
 };
 
 constexpr uint32_t ceil_log2(uint32_t n) {
@@ -176,23 +176,64 @@ __global__ void __launch_bounds__(kHistBlock) global_histogram_kernel(const K* _
 
 // ---------------------------------------------------------------------------
 // One digit pass (digit_binning, onesweep.mojo:121-328).
+//
+// The pass is bound by shared-memory instruction issue, so every per-key
+// shared access is counted: ranking costs one match, one shuffle and one
+// shared atomic by the run leader; the per-(warp, digit) start is a single
+// lookup; key and value are staged together (one 8- or 16-byte store and
+// load); the scatter looks up one destination base per key.
 // ---------------------------------------------------------------------------
-template <typename K, int BLOCK, int KPT>
+template <typename K, bool HAS_V>
+struct Staged;
+template <>
+struct Staged<uint32_t, false> {
+  using T = uint32_t;
+  __device__ static T pack(uint32_t k, uint32_t) { return k; }
+  __device__ static uint32_t key(T t) { return t; }
+  __device__ static uint32_t val(T) { return 0; }
+};
+template <>
+struct Staged<uint32_t, true> {
+  using T = uint2;
+  __device__ static T pack(uint32_t k, uint32_t v) { return make_uint2(k, v); }
+  __device__ static uint32_t key(T t) { return t.x; }
+  __device__ static uint32_t val(T t) { return t.y; }
+};
+template <>
+struct Staged<uint64_t, false> {
+  using T = uint64_t;
+  __device__ static T pack(uint64_t k, uint32_t) { return k; }
+  __device__ static uint64_t key(T t) { return t; }
+  __device__ static uint32_t val(T) { return 0; }
+};
+template <>
+struct Staged<uint64_t, true> {
+  using T = uint4;
+  __device__ static T pack(uint64_t k, uint32_t v) {
+    return make_uint4((uint32_t)k, (uint32_t)(k >> 32), v, 0u);
+  }
+  __device__ static uint64_t key(T t) { return ((uint64_t)t.y << 32) | t.x; }
+  __device__ static uint32_t val(T t) { return t.z; }
+};
+
+template <typename K, bool HAS_V, int BLOCK, int KPT>
 struct BinSmem {
+  using T = typename Staged<K, HAS_V>::T;
   static constexpr int kWarps = BLOCK / 32;
   static constexpr int kTile = BLOCK * KPT;
-  static constexpr int kStage = kTile > kWarps * (int)kRadix ? kTile : kWarps * (int)kRadix;
   union {
-    K keys[kStage];
-    uint32_t vals[kStage];
-    uint32_t warp_hist[kWarps * kRadix];
+    T staged[kTile];
+    uint32_t warp_hist[kWarps * kRadix];  // per (warp, digit): count, then start
   } u;
   uint32_t digit_offset[kRadix];
-  uint32_t tile_start[kRadix];
   uint32_t scan_tmp[8];
   uint32_t tile;
   uint32_t abort;  // a look-back wait timed out: publish, skip the scatter
 };
+
+__device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
 // lookback: this pass's flags; lookback_next: the other region, whose slot of
 // this tile is cleared for the next pass.
@@ -202,7 +243,8 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
     uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
     uint32_t* __restrict__ lookback, uint32_t* __restrict__ lookback_next, uint32_t* __restrict__ tile_counter,
     uint32_t* __restrict__ status, uint32_t n, uint32_t shift, uint32_t digit_mask) {
-  using S = BinSmem<K, BLOCK, KPT>;
+  using S = BinSmem<K, HAS_V, BLOCK, KPT>;
+  using ST = Staged<K, HAS_V>;
   constexpr int kWarps = S::kWarps;
   constexpr uint32_t kTile = S::kTile;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -220,24 +262,18 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
   const uint32_t tile = s.tile;
   const uint32_t tile_base = tile * kTile;
   const uint32_t valid = min(kTile, n - tile_base);
+  if (HAS_V && tid == 0 && (((uintptr_t)(vals_in + tile_base)) & 15) == 0)
+    prefetch_l2_bulk(vals_in + tile_base, (valid * 4u) & ~15u);  // values are read after the look-back
   if (lookback_next && tid < kRadix) lookback_next[tile * kRadix + tid] = 0;
 
   // warp-striped load: key i of this thread sits at tile position
   // warp*32*KPT + 32*i + lane, so (warp, i, lane) order is position order.
   K key[KPT];
-  uint32_t val[HAS_V ? KPT : 1];
   const uint32_t pos0 = tile_base + warp * 32 * KPT + lane;
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
     uint32_t p = pos0 + 32 * i;
     key[i] = (p < n) ? keys_in[p] : KeyTraits<K>::kMax;
-  }
-  if constexpr (HAS_V) {
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      uint32_t p = pos0 + 32 * i;
-      val[i] = (p < n) ? vals_in[p] : 0u;
-    }
   }
 
   // rank every key among equal digits of its warp, in position order
@@ -246,31 +282,21 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
   uint32_t rank[KPT];
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
-    uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
-    uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
-    uint32_t leader = __ffs(peers) - 1;
+    const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t leader = __ffs(peers) - 1;
     uint32_t before = 0;
-    if (lane == leader) {
-      before = wh[d];
-      wh[d] = before + __popc(peers);
-    }
+    if (lane == leader) before = atomicAdd(&wh[d], (uint32_t)__popc(peers));
     before = __shfl_sync(0xFFFFFFFFu, before, leader);
     rank[i] = before + __popc(peers & lt);
-    __syncwarp();
   }
   __syncthreads();
 
-  // per digit: warp prefixes, tile total, publish the tile aggregate
+  // per digit: tile total, publish the tile aggregate
   uint32_t total = 0, agg = 0, gcount = 0;
   if (tid < kRadix) {
-    uint32_t run = 0;
 #pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-      uint32_t c = s.u.warp_hist[w * kRadix + tid];
-      s.u.warp_hist[w * kRadix + tid] = run;
-      run += c;
-    }
-    total = run;
+    for (int w = 0; w < kWarps; ++w) total += s.u.warp_hist[w * kRadix + tid];
     agg = total - ((tid == digit_mask) ? (kTile - valid) : 0u);  // padding keys carry the top digit
     uint32_t word = agg | (tile == 0 ? kFlagInc : kFlagAgg);
     st_relaxed_gpu(&lookback[tile * kRadix + tid], word);
@@ -278,6 +304,24 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
   }
   const uint32_t tstart = scan256_exclusive<BLOCK>(total, s.scan_tmp);
   const uint32_t gstart = scan256_exclusive<BLOCK>(gcount, s.scan_tmp);
+  if (tid < kRadix) {
+    // per (warp, digit) start inside the tile: tile start of the digit plus
+    // the counts of the earlier warps
+    uint32_t run = tstart;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      uint32_t c = s.u.warp_hist[w * kRadix + tid];
+      s.u.warp_hist[w * kRadix + tid] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+  // tile-local sorted position of every key (rank becomes the position)
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    rank[i] += s.u.warp_hist[warp * kRadix + d];
+  }
 
   // Decoupled look-back, one thread per digit.  The flags of up to
   // kLookbackBatch predecessors are loaded at once (independent loads), so a
@@ -326,52 +370,38 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
       st_relaxed_gpu(&lookback[tile * kRadix + tid], ((excl + agg) & kValueMask) | kFlagInc);
     }
     s.digit_offset[tid] = gstart + excl - tstart;
-    s.tile_start[tid] = tstart;
   }
   __syncthreads();
   // The successors are released (inclusive prefixes published); without a
   // complete prefix the scatter addresses are unknown, so write nothing.
   if (s.abort) return;
 
-  // tile-local sorted position of every key
-  uint32_t lidx[KPT];
+  // stage key (+ value) at its tile-local position (the barrier above also
+  // ends every read of warp_hist, which the staging overwrites)
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
-    uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
-    lidx[i] = s.tile_start[d] + s.u.warp_hist[warp * kRadix + d] + rank[i];
+    uint32_t v = 0;
+    if constexpr (HAS_V) {
+      const uint32_t p = pos0 + 32 * i;
+      v = (p < n) ? vals_in[p] : 0u;
+    }
+    s.u.staged[rank[i]] = ST::pack(key[i], v);
   }
-  __syncthreads();  // warp_hist is overwritten by the key staging below
-#pragma unroll
-  for (int i = 0; i < KPT; ++i) s.u.keys[lidx[i]] = key[i];
   __syncthreads();
 
   // scatter: consecutive tile slots of one digit go to consecutive addresses
-  uint8_t dig[KPT];
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
-    uint32_t j = tid + i * BLOCK;
+    const uint32_t j = tid + i * BLOCK;
     if (j < valid) {
-      K k = s.u.keys[j];
-      uint32_t d = (uint32_t)(k >> shift) & digit_mask;
-      dig[i] = (uint8_t)d;
-      uint32_t dst = s.digit_offset[d] + j;
+      const auto e = s.u.staged[j];
+      const K k = ST::key(e);
+      const uint32_t d = (uint32_t)(k >> shift) & digit_mask;
+      const uint32_t dst = s.digit_offset[d] + j;
       if (dst < n) {  // holds whenever the digit counts are consistent
         keys_out[dst] = k;
+        if constexpr (HAS_V) vals_out[dst] = ST::val(e);
         if constexpr (EMIT_LOW32) low32_out[dst] = (uint32_t)k;
-      }
-    }
-  }
-  if constexpr (HAS_V) {
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) s.u.vals[lidx[i]] = val[i];
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < KPT; ++i) {
-      uint32_t j = tid + i * BLOCK;
-      if (j < valid) {
-        uint32_t dst = s.digit_offset[dig[i]] + j;
-        if (dst < n) vals_out[dst] = s.u.vals[j];
       }
     }
   }
@@ -436,7 +466,7 @@ inline cudaError_t launch_variant(const K* kin, K* kout, const uint32_t* vin, ui
   constexpr int B = Shapes<K>::v[V].block;
   constexpr int KPT = Shapes<K>::v[V].kpt;
   auto kern = onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
-  const size_t smem = sizeof(BinSmem<K, B, KPT>);
+  const size_t smem = sizeof(BinSmem<K, HAS_V, B, KPT>);
   static bool configured[64] = {};  // per template instance and device
   int dev = 0;
   cudaGetDevice(&dev);

@@ -1,0 +1,690 @@
+// rt.cu -- wavefront path tracing (PATH / NEE / MIS) of Lambertian + emissive
+// triangle scenes over the binary LBVH, on sm_100a.
+//
+// Restates the reference's GPU wavefront renderer for triangle scenes:
+//  - primary rays: gpu_rt_primary_kernel (bajo/rt/gpu/common_kernels.mojo:22),
+//    Camera.make_ray_sampled (bajo/bvh/camera.mojo:156-209);
+//  - closest hit + fused shading: gpu_rt_scene_trace_kernel
+//    (bajo/rt/gpu/scene_trace.mojo:41-369): sky on miss (bajo/rt/common.mojo:24),
+//    oriented normal (bajo/rt/geometry.mojo:20), next-event estimation with
+//    the alias-table light sample (bajo/rt/gpu/path_shading.mojo:261-413),
+//    MIS-weighted emission (:543-573), inline Lambertian sampling
+//    (bajo/rt/shading.mojo:92-118) and Russian roulette (bajo/rt/common.mojo:43);
+//  - any-hit shadow rays (scene_trace.mojo:586);
+//  - per-pixel resolve (common_kernels.mojo:97).
+// Queues keep the reference's field-major ABI (bajo/rt/wavefront_contract.mojo:
+// 41-96): path id (delta flag in bit 31) + 12 f32 planes, shadow id + 11
+// planes, 3 planes of per-sample radiance.  Appends are warp-aggregated (one
+// atomic per warp instead of one per thread, wavefront_contract.mojo:460).
+//
+// Random numbers: every (path, stage) pair owns a Philox-4x32-10 stream
+// (Salmon et al., SC'11) keyed by the seed with counter
+// (0, 0, stage, path_id) -- the reference's (path_id << 32) | stage
+// subsequence (wavefront_contract.mojo:107-133); each stage uses at most the
+// four floats of its first block.  Angles use sincos_turns (below), a
+// polynomial shared with the oracle, so results are bit-identical to it.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "traverse.cuh"
+
+namespace bajo {
+int sm_count();
+
+namespace rt {
+
+using trav::Ray;
+using trav::Hit;
+
+constexpr uint32_t kDeltaBit = 0x80000000u;    // WAVE_PATH_DELTA_BIT, wavefront_contract.mojo:60
+constexpr uint32_t kIdMask = 0x7FFFFFFFu;
+constexpr int kPathPlanes = 12;                 // WavePathFloatAbi.PLANES
+constexpr int kShadowPlanes = 11;               // WaveShadowFloatAbi.PLANES
+constexpr uint32_t kIndexMask28 = 0x0FFFFFFFu;  // SURFACE_INDEX_MASK
+constexpr float kInvPi = 0.3183098861837907f;   // BSDF_INV_PI, bajo/rt/shading.mojo:9
+constexpr int kBlock = 128;
+
+// stage domains (wavefront_contract.mojo:32-133)
+__device__ __forceinline__ uint32_t stage_bsdf(uint32_t b) { return (0u << 30) | (b + 1); }
+__device__ __forceinline__ uint32_t stage_roulette(uint32_t b) { return (1u << 30) | (b + 1); }
+__device__ __forceinline__ uint32_t stage_light(uint32_t b) { return (2u << 30) | (b + 1); }
+
+// Philox-4x32-10: 10 rounds of the multiply-xor bijection with Weyl key bumps.
+__device__ __forceinline__ float4 uniform4(uint64_t seed, uint32_t path_id, uint32_t stage) {
+  uint32_t c0 = 0, c1 = 0, c2 = stage, c3 = path_id;
+  uint32_t k0 = (uint32_t)seed, k1 = (uint32_t)(seed >> 32);
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    const uint32_t hi0 = __umulhi(0xD2511F53u, c0), lo0 = 0xD2511F53u * c0;
+    const uint32_t hi1 = __umulhi(0xCD9E8D57u, c2), lo1 = 0xCD9E8D57u * c2;
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  const float s = 1.0f / 16777216.0f;  // 24-bit uniforms in [0, 1)
+  return make_float4((float)(c0 >> 8) * s, (float)(c1 >> 8) * s, (float)(c2 >> 8) * s, (float)(c3 >> 8) * s);
+}
+
+// sin and cos of 2*pi*u for u in [0, 1): reduce to the nearest quarter turn,
+// evaluate the Taylor series of sin and cos on |a| <= pi/4 (terms to a^9 and
+// a^10, truncation below 2e-9), rotate by the quadrant.
+__device__ __forceinline__ void sincos_turns(float u, float& s_out, float& c_out) {
+  const float qf = floorf(u * 4.0f + 0.5f);
+  const int q = (int)qf & 3;
+  const float r = u - qf * 0.25f;
+  const float a = r * 6.28318530717958647692f;
+  const float a2 = a * a;
+  float s = fmaf(a2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  s = fmaf(a2, s, 1.0f / 120.0f);
+  s = fmaf(a2, s, -1.0f / 6.0f);
+  s = fmaf(a2, s, 1.0f);
+  s = a * s;
+  float c = fmaf(a2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+  c = fmaf(a2, c, -1.0f / 720.0f);
+  c = fmaf(a2, c, 1.0f / 24.0f);
+  c = fmaf(a2, c, -0.5f);
+  c = fmaf(a2, c, 1.0f);
+  if (q == 0) { s_out = s; c_out = c; }
+  else if (q == 1) { s_out = c; c_out = -s; }
+  else if (q == 2) { s_out = -s; c_out = -c; }
+  else { s_out = -c; c_out = s; }
+}
+
+__device__ __forceinline__ float length2(f3 v) { return dot(v, v); }
+__device__ __forceinline__ f3 neg(f3 v) { return mk(-v.x, -v.y, -v.z); }
+__device__ __forceinline__ f3 mul(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ f3 divs(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+
+// power_heuristic, bajo/rt/lighting.mojo:7-19
+__device__ __forceinline__ float power_heuristic(float a, float b) {
+  const float a2 = a * a, b2 = b * b, den = a2 + b2;
+  return den > 0.0f ? a2 / den : 0.0f;
+}
+
+// sky_color, bajo/rt/common.mojo:24-33
+__device__ __forceinline__ f3 sky(f3 d) {
+  const f3 u = normalize(d);
+  const float a = 0.5f * (u.y + 1.0f);
+  return mk((1.0f - a) * 1.0f + a * 0.5f, (1.0f - a) * 1.0f + a * 0.7f, (1.0f - a) * 1.0f + a * 1.0f);
+}
+
+struct Queues {
+  uint32_t* ids[2];
+  float* fields[2];
+  uint32_t* shadow_ids;
+  float* shadow_fields;
+  float* radiance;
+  uint32_t* counters;  // [2b] = paths active at bounce b, [2b+1] = shadow rays of bounce b
+  uint32_t* status;
+  uint32_t capacity;
+};
+
+struct SceneView {
+  const uint32_t* roots;
+  const float4* nb;
+  const uint4* meta;
+  const float4* tris;
+  uint32_t n_nodes;
+  const uint32_t* surfaces;
+  const float* lambertians;
+  const float* emissives;
+  const float* lights;
+  uint32_t n_lights;
+  float total_light_weight;
+};
+
+// warp-aggregated queue append: one atomic per warp; every lane of the warp
+// must call it (want = false for lanes with nothing to append)
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+  const uint32_t mask = __ballot_sync(0xFFFFFFFFu, want);
+  if (!mask) return 0;
+  const uint32_t lane = lane_id();
+  const uint32_t leader = __ffs(mask) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  return base + __popc(mask & lanemask_lt());
+}
+
+// ---------------------------------------------------------------------------
+// primary rays (gpu_rt_primary_kernel, common_kernels.mojo:22-93;
+// Camera.make_ray_sampled, camera.mojo:156-209; random_in_unit_disk,
+// bajo/core/random.mojo:56)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) primary_kernel(const float* __restrict__ cam, Queues q, uint32_t count,
+                                                         uint32_t sample_base, uint32_t width, uint32_t height,
+                                                         uint32_t spp, uint64_t seed) {
+  const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
+  if (idx == 0) q.counters[0] = count;
+  if (idx >= count) return;
+  const uint32_t cap = q.capacity;
+  const uint32_t path_id = sample_base + idx;
+  const uint32_t pixel = path_id / spp;
+  const uint32_t px = pixel % width, py = pixel / width;
+  const float4 r = uniform4(seed, path_id, 0);
+  float st, ct;
+  sincos_turns(r.x, st, ct);
+  const float lr = sqrtf(r.y);
+  const float lens_u = lr * ct, lens_v = lr * st;
+  const float w = (float)width, h = (float)height;
+  const float aspect = w / h;
+  const float sx = (((float)px + r.z) / w) * 2.0f - 1.0f;
+  const float sy = 1.0f - (((float)py + r.w) / h) * 2.0f;
+  const f3 origin = mk(cam[0], cam[1], cam[2]);
+  const f3 fwd = mk(cam[3], cam[4], cam[5]), right = mk(cam[6], cam[7], cam[8]), up = mk(cam[9], cam[10], cam[11]);
+  const float fs = cam[12], focus = cam[13];
+  const f3 du = mk(cam[14], cam[15], cam[16]), dv = mk(cam[17], cam[18], cam[19]);
+  const f3 inner = (fwd + right * ((sx * aspect) * fs)) + up * (sy * fs);
+  const f3 focal = origin + mk(focus * inner.x, focus * inner.y, focus * inner.z);
+  const f3 ro = (origin + mk(lens_u * du.x, lens_u * du.y, lens_u * du.z)) + mk(lens_v * dv.x, lens_v * dv.y, lens_v * dv.z);
+  const f3 d = normalize(focal - ro);
+  q.ids[0][idx] = path_id | kDeltaBit;
+  float* f = q.fields[0];
+  f[0 * cap + idx] = ro.x; f[1 * cap + idx] = ro.y; f[2 * cap + idx] = ro.z; f[3 * cap + idx] = 0.001f;
+  f[4 * cap + idx] = d.x; f[5 * cap + idx] = d.y; f[6 * cap + idx] = d.z; f[7 * cap + idx] = FLT_MAX;
+  f[8 * cap + idx] = 1.0f; f[9 * cap + idx] = 1.0f; f[10 * cap + idx] = 1.0f; f[11 * cap + idx] = 0.0f;
+  q.radiance[0 * cap + idx] = 0.0f;
+  q.radiance[1 * cap + idx] = 0.0f;
+  q.radiance[2 * cap + idx] = 0.0f;
+}
+
+__device__ __forceinline__ void accumulate(const Queues& q, uint32_t sidx, f3 v) {
+  q.radiance[0 * q.capacity + sidx] += v.x;
+  q.radiance[1 * q.capacity + sidx] += v.y;
+  q.radiance[2 * q.capacity + sidx] += v.z;
+}
+
+// ---------------------------------------------------------------------------
+// closest hit + shading of bounce `bounce` (gpu_rt_scene_trace_kernel and
+// _route_surface_hit / _shade_lambertian_inline, path_shading.mojo:460-590)
+// ---------------------------------------------------------------------------
+template <int ALGO>
+__global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queues q, uint32_t bounce,
+                                                             uint32_t max_depth, uint32_t sample_base,
+                                                             uint64_t seed) {
+  const uint32_t count = q.counters[2 * bounce];
+  const uint32_t cap = q.capacity;
+  const uint32_t* src_ids = q.ids[bounce & 1];
+  const float* src = q.fields[bounce & 1];
+  uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
+  float* dst = q.fields[(bounce + 1) & 1];
+  const uint32_t stride = gridDim.x * kBlock;
+  for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
+    const uint32_t idx = base + threadIdx.x;
+    const bool live = idx < count;
+    bool want_shadow = false, want_next = false;
+    f3 sh_o, sh_d, sh_c, nx_o, nx_d, nx_t;
+    float sh_tmax = 0.0f, nx_pdf = 0.0f;
+    uint32_t path_id = 0;
+    if (live) {
+      const uint32_t idw = src_ids[idx];
+      path_id = idw & kIdMask;
+      const bool delta = (idw & kDeltaBit) != 0;
+      const f3 o = mk(src[0 * cap + idx], src[1 * cap + idx], src[2 * cap + idx]);
+      const float tmin = src[3 * cap + idx];
+      const f3 d = mk(src[4 * cap + idx], src[5 * cap + idx], src[6 * cap + idx]);
+      const float tmax = src[7 * cap + idx];
+      const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
+      const float prev_pdf = src[11 * cap + idx];
+      const uint32_t sidx = path_id - sample_base;
+      const Ray r = trav::make_ray(o, d, tmin, tmax);
+      const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
+                                                          q.status);
+      if (h.leaf == kEmpty) {
+        accumulate(q, sidx, mul(T, sky(d)));
+      } else {
+        const float t = h.t;
+        const float4 a = __ldg(sc.tris + (size_t)h.leaf * 3 + 0);
+        const float4 b = __ldg(sc.tris + (size_t)h.leaf * 3 + 1);
+        const float4 c = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
+        const f3 v0 = mk(a.x, a.y, a.z);
+        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(c.x, c.y, c.z) - v0));
+        const bool front = dot(d, outward) < 0.0f;
+        const f3 normal = front ? outward : neg(outward);
+        const uint32_t surface = __ldg(sc.surfaces + h.prim);
+        const uint32_t kind = surface >> 28, midx = surface & kIndexMask28;
+        const f3 p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+        if (kind == BAJO_MAT_EMISSIVE) {
+          if (front) {
+            const f3 L = mk(sc.emissives[3 * midx], sc.emissives[3 * midx + 1], sc.emissives[3 * midx + 2]);
+            float wgt = 1.0f;
+            if (ALGO == BAJO_RENDER_NEE && bounce > 0 && !delta) wgt = 0.0f;
+            if (ALGO == BAJO_RENDER_MIS && bounce > 0 && !delta) {
+              const float lc = fmaxf(dot(normal, neg(normalize(d))), 0.0f);
+              float lpdf = 0.0f;
+              if (lc > 0.0f && sc.total_light_weight > 0.0f) {
+                const float d2 = (t * t) * length2(d);
+                lpdf = (d2 * ((L.x + L.y) + L.z)) / ((3.0f * lc) * sc.total_light_weight);
+              }
+              wgt = power_heuristic(prev_pdf, lpdf);
+            }
+            const f3 TL = mul(T, L);
+            accumulate(q, sidx, mk(TL.x * wgt, TL.y * wgt, TL.z * wgt));
+          }
+        } else if (kind == BAJO_MAT_LAMBERTIAN) {
+          const f3 albedo = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
+          if ((ALGO == BAJO_RENDER_NEE || ALGO == BAJO_RENDER_MIS) && sc.n_lights > 0 &&
+              sc.total_light_weight > 0.0f) {
+            // _sample_direct_light_candidate, path_shading.mojo:261-413
+            const float4 u = uniform4(seed, path_id, stage_light(bounce));
+            const float as = u.x * (float)sc.n_lights;
+            uint32_t li = (uint32_t)as;
+            const float frac = as - (float)li;
+            const float* lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+            if (frac > lrec[12]) li = __float_as_uint(lrec[13]);
+            lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+            const f3 p0 = mk(lrec[0], lrec[1], lrec[2]), p1 = mk(lrec[3], lrec[4], lrec[5]),
+                     p2 = mk(lrec[6], lrec[7], lrec[8]);
+            const f3 e1 = p1 - p0, e2 = p2 - p0;
+            const f3 av = cross(e1, e2);
+            const float tas = length2(av);
+            if (tas > 0.0f) {
+              const f3 ln = divs(av, sqrtf(tas));
+              const float ru = sqrtf(u.y);
+              const float b1 = ru * (1.0f - u.z);
+              const float b2 = ru - b1;
+              const f3 lp = (p0 + e1 * b1) + e2 * b2;
+              const f3 tl = lp - p;
+              const float d2 = length2(tl);
+              if (d2 > 1.0e-8f) {
+                const float dist = sqrtf(d2);
+                const f3 dir = divs(tl, dist);
+                const float scos = fmaxf(dot(normal, dir), 0.0f);
+                const float lcos = fmaxf(dot(ln, neg(dir)), 0.0f);
+                const float smax = dist - 0.002f;
+                if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
+                  const f3 E = mk(lrec[9], lrec[10], lrec[11]);
+                  const float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * sc.total_light_weight);
+                  const float bpdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
+                  if (lpdf > 0.0f && bpdf > 0.0f) {
+                    const float wgt = ALGO == BAJO_RENDER_MIS ? power_heuristic(lpdf, bpdf) : 1.0f;
+                    const float scale = (scos * wgt) / lpdf;
+                    if (scale > 0.0f) {
+                      const f3 value = albedo * kInvPi;
+                      const f3 tv = mul(mul(T, value), E);
+                      want_shadow = true;
+                      sh_o = p;
+                      sh_d = dir;
+                      sh_tmax = smax;
+                      sh_c = tv * scale;
+                    }
+                  }
+                }
+              }
+            }
+          }
+          if (bounce + 1 < max_depth) {
+            // _sample_lambertian, bajo/rt/shading.mojo:92-118
+            const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
+            float st, ct;
+            sincos_turns(u.x, st, ct);
+            const float z = 1.0f - 2.0f * u.y;
+            const float rad = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+            f3 sd = normal + mk(rad * ct, rad * st, z);
+            if (fabsf(sd.x) < 1.0e-8f && fabsf(sd.y) < 1.0e-8f && fabsf(sd.z) < 1.0e-8f) sd = normal;
+            const f3 dir = normalize(sd);
+            const float pdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
+            f3 Tn = mul(T, albedo);
+            // russian_roulette, bajo/rt/common.mojo:43-67 (depth = bounce + 1)
+            bool alive = true;
+            if (bounce + 1 >= 5u) {
+              const float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+              if (m <= 0.0f) alive = false;
+              else {
+                const float survival = fminf(fmaxf(m, 0.05f), 0.95f);
+                const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
+                if (rr.x >= survival) alive = false;
+                else Tn = divs(Tn, survival);
+              }
+            }
+            if (alive) {
+              want_next = true;
+              nx_o = p;
+              nx_d = dir;
+              nx_t = Tn;
+              nx_pdf = pdf;
+            }
+          }
+        }
+      }
+    }
+    if (ALGO == BAJO_RENDER_NEE || ALGO == BAJO_RENDER_MIS) {
+      const uint32_t slot = warp_append(&q.counters[2 * bounce + 1], want_shadow);
+      if (want_shadow) {
+        if (slot < cap) {
+          q.shadow_ids[slot] = path_id;
+          float* f = q.shadow_fields;
+          f[0 * cap + slot] = sh_o.x; f[1 * cap + slot] = sh_o.y; f[2 * cap + slot] = sh_o.z;
+          f[3 * cap + slot] = 0.001f;
+          f[4 * cap + slot] = sh_d.x; f[5 * cap + slot] = sh_d.y; f[6 * cap + slot] = sh_d.z;
+          f[7 * cap + slot] = sh_tmax;
+          f[8 * cap + slot] = sh_c.x; f[9 * cap + slot] = sh_c.y; f[10 * cap + slot] = sh_c.z;
+        } else {
+          raise_status(q.status, BAJO_WAVE_SHADOW_OVERFLOW);
+        }
+      }
+    }
+    const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], want_next);
+    if (want_next) {
+      if (slot < cap) {
+        dst_ids[slot] = path_id;  // delta = false after a Lambertian bounce
+        dst[0 * cap + slot] = nx_o.x; dst[1 * cap + slot] = nx_o.y; dst[2 * cap + slot] = nx_o.z;
+        dst[3 * cap + slot] = 0.001f;
+        dst[4 * cap + slot] = nx_d.x; dst[5 * cap + slot] = nx_d.y; dst[6 * cap + slot] = nx_d.z;
+        dst[7 * cap + slot] = FLT_MAX;
+        dst[8 * cap + slot] = nx_t.x; dst[9 * cap + slot] = nx_t.y; dst[10 * cap + slot] = nx_t.z;
+        dst[11 * cap + slot] = nx_pdf;
+      } else {
+        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// any-hit shadow rays (gpu_rt_shadow_kernel, scene_trace.mojo:586)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(kBlock) shadow_kernel(SceneView sc, Queues q, uint32_t bounce,
+                                                        uint32_t sample_base) {
+  const uint32_t count = q.counters[2 * bounce + 1];
+  const uint32_t cap = q.capacity;
+  const float* f = q.shadow_fields;
+  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < count; i += gridDim.x * kBlock) {
+    const f3 o = mk(f[0 * cap + i], f[1 * cap + i], f[2 * cap + i]);
+    const f3 d = mk(f[4 * cap + i], f[5 * cap + i], f[6 * cap + i]);
+    const Ray r = trav::make_ray(o, d, f[3 * cap + i], f[7 * cap + i]);
+    const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT, false, true>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris,
+                                                                     sc.n_nodes, q.status);
+    if (h.leaf == kEmpty) {
+      const uint32_t sidx = q.shadow_ids[i] - sample_base;
+      accumulate(q, sidx, mk(f[8 * cap + i], f[9 * cap + i], f[10 * cap + i]));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// per-pixel resolve (gpu_rt_resolve_kernel, common_kernels.mojo:97-136)
+// ---------------------------------------------------------------------------
+// Thread 0 also adds this chunk's traced rays (closest-hit and shadow, one
+// per queue entry of every bounce) to the 64-bit totals.
+__global__ void __launch_bounds__(kBlock) resolve_kernel(const float* __restrict__ radiance, uint32_t cap,
+                                                         uint32_t pixel_base, uint32_t pixel_count, uint32_t spp,
+                                                         float* __restrict__ pixels, double* __restrict__ pixels64,
+                                                         const uint32_t* __restrict__ counters, uint32_t max_depth,
+                                                         unsigned long long* __restrict__ totals) {
+  const uint32_t p = blockIdx.x * kBlock + threadIdx.x;
+  if (p == 0) {
+    unsigned long long rays = 0, shadows = 0;
+    for (uint32_t b = 0; b < max_depth; ++b) {
+      rays += counters[2 * b];
+      shadows += counters[2 * b + 1];
+    }
+    totals[0] += rays;
+    totals[1] += shadows;
+  }
+  if (p >= pixel_count) return;
+  float r = 0.0f, g = 0.0f, b = 0.0f;
+  double r64 = 0.0, g64 = 0.0, b64 = 0.0;
+  const uint32_t s0 = p * spp;
+  for (uint32_t s = s0; s < s0 + spp; ++s) {
+    const float x = radiance[s], y = radiance[cap + s], z = radiance[2 * cap + s];
+    r += x;
+    g += y;
+    b += z;
+    if (pixels64) {
+      r64 += (double)x;
+      g64 += (double)y;
+      b64 += (double)z;
+    }
+  }
+  const float scale = 1.0f / (float)spp;
+  const size_t o = 3 * (size_t)(pixel_base + p);
+  pixels[o + 0] = r * scale;
+  pixels[o + 1] = g * scale;
+  pixels[o + 2] = b * scale;
+  if (pixels64) {
+    pixels64[o + 0] += r64;
+    pixels64[o + 1] += g64;
+    pixels64[o + 2] += b64;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// host
+// ---------------------------------------------------------------------------
+constexpr uint32_t kDefaultChunk = 1u << 22;
+
+struct Layout {
+  uint32_t cap, pixels_per_chunk;
+  size_t off_counters, off_ids[2], off_fields[2], off_shadow_ids, off_shadow_fields, off_radiance, total;
+};
+
+inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+bool make_layout(const BajoRenderSettings* s, Layout* L) {
+  if (!s || s->width == 0 || s->height == 0 || s->spp == 0 || s->max_depth == 0 || s->max_depth > 1024) return false;
+  uint32_t want = s->chunk_paths ? s->chunk_paths : kDefaultChunk;
+  const uint64_t total_paths = (uint64_t)s->width * s->height * s->spp;
+  if (total_paths > 0x7FFFFFFFull) return false;  // path ids carry the delta flag in bit 31
+  if (want < s->spp) want = s->spp;
+  uint32_t ppc = want / s->spp;
+  const uint64_t npix = (uint64_t)s->width * s->height;
+  if (ppc > npix) ppc = (uint32_t)npix;
+  L->pixels_per_chunk = ppc;
+  L->cap = ppc * s->spp;
+  const size_t cap = L->cap;
+  size_t o = 256;  // status word, then two 64-bit ray totals at offset 8
+  L->off_counters = o;
+  o = a256(o + (2 * (size_t)s->max_depth + 2) * 4);
+  for (int k = 0; k < 2; ++k) {
+    L->off_ids[k] = o;
+    o = a256(o + cap * 4);
+    L->off_fields[k] = o;
+    o = a256(o + cap * 4 * kPathPlanes);
+  }
+  L->off_shadow_ids = o;
+  o = a256(o + cap * 4);
+  L->off_shadow_fields = o;
+  o = a256(o + cap * 4 * kShadowPlanes);
+  L->off_radiance = o;
+  o = a256(o + cap * 4 * 3);
+  L->total = o;
+  return true;
+}
+
+template <int ALGO>
+cudaError_t launch_bounce(const SceneView& sc, const Queues& q, uint32_t grid, uint32_t b, uint32_t max_depth,
+                          uint32_t sample_base, uint64_t seed, cudaStream_t st) {
+  trace_shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, b, max_depth, sample_base, seed);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  if (ALGO != BAJO_RENDER_PATH) {
+    shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
+    e = cudaGetLastError();
+  }
+  return e;
+}
+
+}  // namespace rt
+}  // namespace bajo
+
+extern "C" {
+
+int32_t bajo_render_workspace_size(const BajoRenderSettings* settings, size_t* bytes) {
+  bajo::rt::Layout L;
+  if (!bytes || !bajo::rt::make_layout(settings, &L)) return BAJO_ERR_INVALID_ARGUMENT;
+  *bytes = L.total;
+  return BAJO_OK;
+}
+
+int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoRenderSettings* s, float* d_pixels,
+                    double* d_pixels64, void* d_ws, size_t ws_bytes, void* stream) {
+  using namespace bajo;
+  using namespace bajo::rt;
+  Layout L;
+  if (!scene || !scene->bvh || !d_camera || !d_pixels || !d_ws || !make_layout(s, &L)) return BAJO_ERR_INVALID_ARGUMENT;
+  if (s->algorithm != BAJO_RENDER_PATH && s->algorithm != BAJO_RENDER_NEE && s->algorithm != BAJO_RENDER_MIS)
+    return BAJO_ERR_INVALID_ARGUMENT;
+  if (ws_bytes < L.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
+  const BajoLbvh* b = scene->bvh;
+  if (!b->roots || !b->node_bounds || !b->node_meta || !b->leaf_tris || !scene->surfaces || !scene->lambertians ||
+      !scene->emissives || (scene->n_lights && !scene->lights))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  unsigned char* w = (unsigned char*)d_ws;
+  SceneView sc;
+  sc.roots = b->roots;
+  sc.nb = reinterpret_cast<const float4*>(b->node_bounds);
+  sc.meta = reinterpret_cast<const uint4*>(b->node_meta);
+  sc.tris = reinterpret_cast<const float4*>(b->leaf_tris);
+  sc.n_nodes = b->n_leaves;
+  sc.surfaces = scene->surfaces;
+  sc.lambertians = scene->lambertians;
+  sc.emissives = scene->emissives;
+  sc.lights = scene->lights;
+  sc.n_lights = scene->n_lights;
+  sc.total_light_weight = scene->total_light_weight;
+  Queues q;
+  for (int k = 0; k < 2; ++k) {
+    q.ids[k] = (uint32_t*)(w + L.off_ids[k]);
+    q.fields[k] = (float*)(w + L.off_fields[k]);
+  }
+  q.shadow_ids = (uint32_t*)(w + L.off_shadow_ids);
+  q.shadow_fields = (float*)(w + L.off_shadow_fields);
+  q.radiance = (float*)(w + L.off_radiance);
+  q.counters = (uint32_t*)(w + L.off_counters);
+  q.status = (uint32_t*)w;
+  q.capacity = L.cap;
+  const uint32_t n_pixels = s->width * s->height;
+  uint32_t grid = (L.cap + kBlock - 1) / kBlock;
+  const uint32_t max_grid = (uint32_t)sm_count() * 16;
+  if (grid > max_grid) grid = max_grid;
+  const size_t counter_bytes = (2 * (size_t)s->max_depth + 2) * 4;
+  unsigned long long* totals = (unsigned long long*)(w + 8);
+  if (cudaMemsetAsync(totals, 0, 16, st) != cudaSuccess) return BAJO_ERR_CUDA;
+  for (uint32_t pb = 0; pb < n_pixels; pb += L.pixels_per_chunk) {
+    const uint32_t pc = std::min(L.pixels_per_chunk, n_pixels - pb);
+    const uint32_t count = pc * s->spp;
+    const uint32_t sample_base = pb * s->spp;
+    if (cudaMemsetAsync(q.counters, 0, counter_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
+    primary_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, st>>>(d_camera, q, count, sample_base, s->width,
+                                                                    s->height, s->spp, s->seed);
+    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
+    for (uint32_t bnc = 0; bnc < s->max_depth; ++bnc) {
+      cudaError_t e;
+      if (s->algorithm == BAJO_RENDER_PATH)
+        e = launch_bounce<BAJO_RENDER_PATH>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
+      else if (s->algorithm == BAJO_RENDER_NEE)
+        e = launch_bounce<BAJO_RENDER_NEE>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
+      else
+        e = launch_bounce<BAJO_RENDER_MIS>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
+      if (e != cudaSuccess) return BAJO_ERR_CUDA;
+    }
+    resolve_kernel<<<(pc + kBlock - 1) / kBlock, kBlock, 0, st>>>(q.radiance, L.cap, pb, pc, s->spp, d_pixels,
+                                                                  d_pixels64, q.counters, s->max_depth, totals);
+    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
+  }
+  return BAJO_OK;
+}
+
+int32_t bajo_render_stats(const void* d_ws, void* stream, uint64_t* rays, uint64_t* shadow_rays) {
+  if (!d_ws || !rays || !shadow_rays) return BAJO_ERR_INVALID_ARGUMENT;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return BAJO_ERR_CUDA;
+  unsigned long long t[2];
+  if (cudaMemcpy(t, (const unsigned char*)d_ws + 8, 16, cudaMemcpyDeviceToHost) != cudaSuccess) return BAJO_ERR_CUDA;
+  *rays = t[0];
+  *shadow_rays = t[1];
+  return BAJO_OK;
+}
+
+// LightStore._build_light_store + build_alias_table (bajo/rt/types.mojo:
+// 190-247, 490-525): one record per emissive triangle with positive power
+// area * mean(radiance); Walker-Vose alias table with the reference's
+// small / large stacks.
+int32_t bajo_rt_build_lights(const float* v, const uint32_t* surf, uint32_t n, const float* em, uint32_t n_em,
+                             float* out, uint32_t max_lights, uint32_t* n_lights, float* total_weight) {
+  if (!v || !surf || !n_lights || !total_weight || (max_lights && !out)) return BAJO_ERR_INVALID_ARGUMENT;
+  struct Rec {
+    uint32_t tri;
+    float w;
+  };
+  std::vector<Rec> recs;
+  float total = 0.0f;
+  for (uint32_t i = 0; i < n; ++i) {
+    const uint32_t s = surf[i];
+    if ((s >> 28) != BAJO_MAT_EMISSIVE) continue;
+    const uint32_t m = s & 0x0FFFFFFFu;
+    if (m >= n_em || !em) return BAJO_ERR_INVALID_ARGUMENT;
+    const float* p = v + (size_t)9 * i;
+    const float e1x = p[3] - p[0], e1y = p[4] - p[1], e1z = p[5] - p[2];
+    const float e2x = p[6] - p[0], e2y = p[7] - p[1], e2z = p[8] - p[2];
+    const float cx = std::fmaf(e1y, e2z, -(e1z * e2y));
+    const float cy = std::fmaf(e1z, e2x, -(e1x * e2z));
+    const float cz = std::fmaf(e1x, e2y, -(e1y * e2x));
+    const float len2 = std::fmaf(cx, cx, std::fmaf(cy, cy, cz * cz));
+    const float area = 0.5f * std::sqrt(len2);
+    const float* L = em + 3 * (size_t)m;
+    const float imp = std::max(((L[0] + L[1]) + L[2]) / 3.0f, 0.0f);
+    const float w = area * imp;
+    if (w > 0.0f) {
+      total += w;
+      recs.push_back({i, w});
+    }
+  }
+  const uint32_t count = (uint32_t)recs.size();
+  if (count > max_lights) return BAJO_ERR_TOO_LARGE;
+  std::vector<float> prob(count, 1.0f), scaled(count, 0.0f);
+  std::vector<uint32_t> alias(count, 0);
+  if (count > 0 && total > 0.0f) {
+    std::vector<uint32_t> small, large;
+    for (uint32_t i = 0; i < count; ++i) {
+      alias[i] = i;
+      scaled[i] = recs[i].w * (float)count / total;
+      if (scaled[i] < 1.0f) small.push_back(i);
+      else large.push_back(i);
+    }
+    while (!small.empty() && !large.empty()) {
+      const uint32_t si = small.back();
+      small.pop_back();
+      const uint32_t li = large.back();
+      large.pop_back();
+      prob[si] = scaled[si];
+      alias[si] = li;
+      scaled[li] = scaled[li] + scaled[si] - 1.0f;
+      if (scaled[li] < 1.0f) small.push_back(li);
+      else large.push_back(li);
+    }
+    for (uint32_t i : small) {
+      prob[i] = 1.0f;
+      alias[i] = i;
+    }
+    for (uint32_t i : large) {
+      prob[i] = 1.0f;
+      alias[i] = i;
+    }
+  }
+  for (uint32_t k = 0; k < count; ++k) {
+    float* r = out + (size_t)k * BAJO_LIGHT_STRIDE;
+    const float* p = v + (size_t)9 * recs[k].tri;
+    for (int j = 0; j < 9; ++j) r[j] = p[j];
+    const float* L = em + 3 * (size_t)(surf[recs[k].tri] & 0x0FFFFFFFu);
+    r[9] = L[0];
+    r[10] = L[1];
+    r[11] = L[2];
+    r[12] = prob[k];
+    std::memcpy(&r[13], &alias[k], 4);
+    r[14] = 0.0f;
+    r[15] = 0.0f;
+  }
+  *n_lights = count;
+  *total_weight = total;
+  return BAJO_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,246 @@
+// traverse.cuh -- closest-hit / any-hit traversal of the binary LBVH.
+//
+// Restates the reference's two-child near-first loop
+// (bajo/bvh/gpu/trace.mojo:340-428) over the binary node layout the build
+// emits: node_bounds holds both child boxes of a node (48 B) and node_meta its
+// tagged child refs (16 B), so one node costs four 16-byte loads; leaves are
+// the sorted 48-byte triangle records.  Leaf children are intersected at once,
+// the nearer internal child is taken, the other is pushed while it is still
+// within reach.
+//
+// Differences from the reference, shared with the oracle:
+//  - ties in t go to the lowest primitive id (the reference keeps the first
+//    candidate visited);
+//  - child boxes are entered while t_near <= t_far * (1 + 2^-20), which makes
+//    the result independent of the visiting order;
+//  - ray axes with |d| <= 1e-9 are tested by containment;
+//  - BAJO_TRI_WATERTIGHT selects the watertight test of Woop, Benthin and
+//    Wald (JCGT 2013); BAJO_TRI_MT is the reference's Moller-Trumbore
+//    (bajo/core/intersect.mojo:415-459).
+#pragma once
+
+#include "bajo_common.cuh"
+
+namespace bajo {
+namespace trav {
+
+constexpr int kTraceBlock = 128;
+constexpr int kStack = 64;  // Karras trees over 64-bit keys are at most 64 levels deep
+
+struct Ray {
+  f3 o, d, rcp;
+  float tmin, tmax;
+  int kx, ky, kz;
+  float sx, sy, sz;
+  bool px, py, pz;  // |d| <= 1e-9 on this axis
+};
+
+// ray.mojo:86-111 rcp_direction (|d| > 1e-9 ? 1/d : +-1e9)
+__device__ __forceinline__ float rcp1(float d) {
+  const float eps = 1.0e-9f;
+  const float large = 1.0f / eps;
+  return fabsf(d) > eps ? 1.0f / d : (d < 0.0f ? -large : large);
+}
+
+__device__ __forceinline__ Ray make_ray(f3 o, f3 d, float tmin, float tmax) {
+  Ray r;
+  r.o = o;
+  r.d = d;
+  r.tmin = tmin;
+  r.tmax = tmax;
+  r.rcp = mk(rcp1(d.x), rcp1(d.y), rcp1(d.z));
+  r.px = !(fabsf(d.x) > 1.0e-9f);
+  r.py = !(fabsf(d.y) > 1.0e-9f);
+  r.pz = !(fabsf(d.z) > 1.0e-9f);
+  float ax = fabsf(d.x), ay = fabsf(d.y), az = fabsf(d.z);
+  r.kz = (ax > ay) ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+  r.kx = r.kz == 2 ? 0 : r.kz + 1;
+  r.ky = r.kx == 2 ? 0 : r.kx + 1;
+  float dz = comp(d, r.kz);
+  if (dz < 0.0f) {
+    int t = r.kx;
+    r.kx = r.ky;
+    r.ky = t;
+  }
+  r.sx = comp(d, r.kx) / dz;
+  r.sy = comp(d, r.ky) / dz;
+  r.sz = 1.0f / dz;
+  return r;
+}
+
+struct Hit {
+  float t, u, v;
+  uint32_t prim, leaf;
+};
+
+__device__ __forceinline__ bool better(float t, uint32_t prim, const Hit& h) {
+  return t < h.t || (t == h.t && prim < h.prim);
+}
+
+// One slab: (b - o) * rcp, except on axes the ray is parallel to
+// (|d| <= 1e-9), which are tested by containment ([-inf, inf] when the origin
+// lies in [bmin, bmax], empty otherwise).  With the reference's +-1e9
+// reciprocal (ray.mojo:86-111) a ray running exactly along a box face gets an
+// empty slab; containment keeps such rays inside the closed box.
+__device__ __forceinline__ void slab(float bmin, float bmax, float o, float rcp, bool par, float& t0, float& t1) {
+  const float a = (bmin - o) * rcp, b = (bmax - o) * rcp;
+  t0 = par ? (bmin <= o ? -INFINITY : INFINITY) : a;
+  t1 = par ? (bmax >= o ? INFINITY : -INFINITY) : b;
+}
+
+// intersect.mojo:193-215, far bound scaled by kSlack
+__device__ __forceinline__ bool box_hit(const Ray& r, float4 a, float2 b, float tlimit, float& tnear) {
+  // a = (min x, min y, min z, max x), b = (max y, max z)
+  float t0x, t1x, t0y, t1y, t0z, t1z;
+  slab(a.x, a.w, r.o.x, r.rcp.x, r.px, t0x, t1x);
+  slab(a.y, b.x, r.o.y, r.rcp.y, r.py, t0y, t1y);
+  slab(a.z, b.y, r.o.z, r.rcp.z, r.pz, t0z, t1z);
+  float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
+  float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlimit));
+  tnear = tn;
+  return tn <= tf * kSlack;
+}
+
+// intersect.mojo:415-459
+__device__ __forceinline__ bool tri_mt(const Ray& r, f3 v0, f3 e1, f3 e2, float& t, float& u, float& v) {
+  f3 p = cross(r.d, e2);
+  float det = dot(e1, p);
+  bool det_ok = det > 1e-8f || det < -1e-8f;
+  float inv_det = 1.0f / det;
+  f3 tv = r.o - v0;
+  float uu = dot(tv, p) * inv_det;
+  f3 q = cross(tv, e1);
+  float vv = dot(r.d, q) * inv_det;
+  float tt = dot(e2, q) * inv_det;
+  t = tt;
+  u = uu;
+  v = vv;
+  return det_ok && uu >= 0.0f && uu <= 1.0f && vv >= 0.0f && (uu + vv) <= 1.0f && tt > r.tmin;
+}
+
+// Woop, Benthin, Wald, "Watertight Ray/Triangle Intersection", JCGT 2(1)
+// 2013: shear into ray space, edge functions without contraction (built with
+// -fmad=false), double-precision re-evaluation of exactly-zero edges.
+__device__ __forceinline__ bool tri_wt(const Ray& r, f3 v0, f3 v1, f3 v2, float& t, float& u, float& v) {
+  f3 A = v0 - r.o, B = v1 - r.o, C = v2 - r.o;
+  float Akz = comp(A, r.kz), Bkz = comp(B, r.kz), Ckz = comp(C, r.kz);
+  float Ax = comp(A, r.kx) - r.sx * Akz, Ay = comp(A, r.ky) - r.sy * Akz;
+  float Bx = comp(B, r.kx) - r.sx * Bkz, By = comp(B, r.ky) - r.sy * Bkz;
+  float Cx = comp(C, r.kx) - r.sx * Ckz, Cy = comp(C, r.ky) - r.sy * Ckz;
+  float U = Cx * By - Cy * Bx;
+  float V = Ax * Cy - Ay * Cx;
+  float W = Bx * Ay - By * Ax;
+  if (U == 0.0f || V == 0.0f || W == 0.0f) {
+    U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+    V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+    W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+  }
+  if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+  float det = U + V + W;
+  if (det == 0.0f) return false;
+  float Az = r.sz * Akz, Bz = r.sz * Bkz, Cz = r.sz * Ckz;
+  float T = U * Az + V * Bz + W * Cz;
+  float tt = T / det;
+  t = tt;
+  u = V / det;
+  v = W / det;
+  return tt > r.tmin;
+}
+
+template <int MODE>
+__device__ __forceinline__ void test_tri(const Ray& r, const float4* __restrict__ tris, uint32_t leaf, Hit& h) {
+  const float4 a = __ldg(tris + (size_t)leaf * 3 + 0);
+  const float4 b = __ldg(tris + (size_t)leaf * 3 + 1);
+  const float4 c = __ldg(tris + (size_t)leaf * 3 + 2);
+  const uint32_t prim = __float_as_uint(a.w);
+  f3 v0 = mk(a.x, a.y, a.z), v1 = mk(b.x, b.y, b.z), v2 = mk(c.x, c.y, c.z);
+  float t, u, v;
+  bool ok;
+  if constexpr (MODE == BAJO_TRI_MT) ok = tri_mt(r, v0, v1 - v0, v2 - v0, t, u, v);
+  else ok = tri_wt(r, v0, v1, v2, t, u, v);
+  if (ok && t < r.tmax && better(t, prim, h)) {
+    h.t = t;
+    h.u = u;
+    h.v = v;
+    h.prim = prim;
+    h.leaf = leaf;
+  }
+}
+
+// max_nodes: node visits allowed (the node count): a tree is never visited
+// twice per node, so more visits means a corrupt tree.
+template <int MODE, bool STATS = false, bool ANY = false>
+__device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const float4* __restrict__ nb,
+                                          const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                                          uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes = nullptr,
+                                          uint32_t* n_tris = nullptr) {
+  Hit h;
+  h.t = r.tmax;
+  h.u = h.v = 0.0f;
+  h.prim = kEmpty;
+  h.leaf = kEmpty;
+  if (root == kSentinel) return h;
+  if (root & kLeafFlag) {
+    test_tri<MODE>(r, tris, root & kIndexMask, h);
+    if constexpr (STATS) ++*n_tris;
+    return h;
+  }
+  // any-hit queries stop at the first accepted triangle; boxes are culled
+  // against the ray's own t_max (bajo/bvh/gpu/trace.mojo:458-499)
+  uint32_t stack[kStack];
+  int sp = 0;
+  uint32_t cur = root;
+  for (uint32_t visits = 0;; ++visits) {
+    if (visits >= max_nodes || cur >= max_nodes) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      break;
+    }
+    if constexpr (STATS) ++*n_nodes;
+    const float4 b0 = __ldg(nb + (size_t)cur * 3 + 0);  // L: min xyz, max x
+    const float4 b1 = __ldg(nb + (size_t)cur * 3 + 1);  // L: max yz | R: min xy
+    const float4 b2 = __ldg(nb + (size_t)cur * 3 + 2);  // R: min z, max xyz
+    const uint4 m = __ldg(meta + cur);
+    float tl, tr;
+    const float limit0 = ANY ? r.tmax : h.t;
+    const bool hl = box_hit(r, b0, make_float2(b1.x, b1.y), limit0, tl);
+    const bool hr = box_hit(r, make_float4(b1.z, b1.w, b2.x, b2.y), make_float2(b2.z, b2.w), limit0, tr);
+    bool vl = false, vr = false;
+    if (hl) {
+      if (m.y & kLeafFlag) {
+        test_tri<MODE>(r, tris, m.y & kIndexMask, h);
+        if constexpr (STATS) ++*n_tris;
+        if (ANY && h.leaf != kEmpty) return h;
+      } else vl = true;
+    }
+    if (hr) {
+      if (m.z & kLeafFlag) {
+        test_tri<MODE>(r, tris, m.z & kIndexMask, h);
+        if constexpr (STATS) ++*n_tris;
+        if (ANY && h.leaf != kEmpty) return h;
+      } else vr = true;
+    }
+    int near = -1;
+    if (vl) near = 0;
+    if (vr && (near == -1 || tr < tl)) near = 1;
+    if (near >= 0) {
+      const float limit = (ANY ? r.tmax : h.t) * kSlack;
+      const bool far_valid = near == 0 ? vr : vl;
+      const float far_t = near == 0 ? tr : tl;
+      const float near_t = near == 0 ? tl : tr;
+      if (far_valid && far_t <= limit) {
+        if (sp < kStack) stack[sp++] = near == 0 ? m.z : m.y;
+        else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+      }
+      if (near_t <= limit) {
+        cur = near == 0 ? m.y : m.z;
+        continue;
+      }
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+  return h;
+}
+
+}  // namespace trav
+}  // namespace bajo

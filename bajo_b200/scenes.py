@@ -101,3 +101,111 @@ def grid_mesh(nx: int, ny: int, z: float = 0.5) -> np.ndarray:
 def bounds_of(verts: np.ndarray):
     v = verts.reshape(-1, 3)
     return v.min(axis=0), v.max(axis=0)
+
+
+# --- path-tracing scenes ------------------------------------------------------
+MAT_LAMBERTIAN = 0
+MAT_EMISSIVE = 3
+
+
+def surface_id(kind: int, index: int) -> int:
+    """SurfaceId: kind in the top 4 bits (bajo/rt/types.mojo:24-34)."""
+    return (kind << 28) | (index & 0x0FFFFFFF)
+
+
+def icosphere(subdivisions: int) -> np.ndarray:
+    """Unit icosphere as (n_tris, 3, 3) float64, outward winding:
+    20 * 4^subdivisions triangles."""
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+         (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+         (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    verts = np.array(v, np.float64)
+    verts /= np.linalg.norm(verts, axis=1, keepdims=True)
+    tris = verts[np.array(f)]
+    for _ in range(subdivisions):
+        a, b, c = tris[:, 0], tris[:, 1], tris[:, 2]
+        ab, bc, ca = a + b, b + c, c + a
+        ab /= np.linalg.norm(ab, axis=1, keepdims=True)
+        bc /= np.linalg.norm(bc, axis=1, keepdims=True)
+        ca /= np.linalg.norm(ca, axis=1, keepdims=True)
+        tris = np.stack([np.stack([a, ab, ca], 1), np.stack([ab, b, bc], 1), np.stack([ca, bc, c], 1),
+                         np.stack([ab, bc, ca], 1)], 1).reshape(-1, 3, 3)
+    return tris
+
+
+def _quad(p0, p1, p2, p3):
+    return [[p0, p1, p2], [p0, p2, p3]]
+
+
+def unit_box_inward():
+    """The 12 triangles of [0,1]^3 with normals pointing into the box."""
+    q = []
+    q += _quad((0, 0, 0), (0, 0, 1), (1, 0, 1), (1, 0, 0))  # floor, normal +y
+    q += _quad((0, 1, 0), (1, 1, 0), (1, 1, 1), (0, 1, 1))  # ceiling, normal -y
+    q += _quad((0, 0, 1), (0, 1, 1), (1, 1, 1), (1, 0, 1))  # back wall z=1, normal -z
+    q += _quad((0, 0, 0), (1, 0, 0), (1, 1, 0), (0, 1, 0))  # front wall z=0, normal +z
+    q += _quad((0, 0, 0), (0, 1, 0), (0, 1, 1), (0, 0, 1))  # left x=0, normal +x
+    q += _quad((1, 0, 0), (1, 0, 1), (1, 1, 1), (1, 1, 0))  # right x=1, normal -x
+    return np.array(q, np.float64)
+
+
+def ceiling_light(size: float = 0.25, y: float = 0.999):
+    """A size x size quad centred under the ceiling, facing down (-y)."""
+    h = size / 2
+    return np.array(_quad((0.5 - h, y, 0.5 - h), (0.5 + h, y, 0.5 - h), (0.5 + h, y, 0.5 + h),
+                          (0.5 - h, y, 0.5 + h)), np.float64)
+
+
+class RtScene:
+    """Triangle scene for the path tracer: vertices (9 f32 per triangle),
+    per-triangle surface ids and material tables (SceneData,
+    bajo/rt/types.mojo:382)."""
+
+    def __init__(self, vertices, surfaces, lambertians, emissives, camera=None, description=""):
+        self.vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1)
+        self.surfaces = np.ascontiguousarray(surfaces, np.uint32)
+        self.lambertians = np.ascontiguousarray(lambertians, np.float32).reshape(-1)
+        self.emissives = np.ascontiguousarray(emissives, np.float32).reshape(-1)
+        self.camera = camera
+        self.description = description
+
+    @property
+    def n_tris(self):
+        return self.vertices.size // 9
+
+
+def spheres_in_box(n_spheres: int = 64, subdivisions: int = 5, seed: int = 0, emission: float = 15.0,
+                   rmin: float = 0.03, rmax: float = 0.1) -> RtScene:
+    """The procedural path-tracing workload: a 12-triangle unit box (albedo
+    0.75) with a 0.25 x 0.25 emissive quad (emission 15) just below the
+    ceiling, and n_spheres icospheres (radius uniform in [rmin, rmax], centres
+    uniform inside the box and clear of the walls and of the camera) with
+    Lambertian albedo uniform in [0.2, 0.8] per channel.  The camera sits just
+    inside the front wall looking at the back wall, 60 degree vertical FOV."""
+    rng = np.random.default_rng(seed)
+    unit = icosphere(subdivisions)
+    parts, surf = [unit_box_inward(), ceiling_light()], [[surface_id(MAT_LAMBERTIAN, 0)] * 12,
+                                                        [surface_id(MAT_EMISSIVE, 0)] * 2]
+    albedo = [[0.75, 0.75, 0.75]]
+    for s in range(n_spheres):
+        r = rng.uniform(rmin, rmax)
+        lo = np.array([r + 0.01, r + 0.01, r + 0.2])
+        hi = np.array([1 - r - 0.01, 1 - r - 0.06, 1 - r - 0.01])
+        c = lo + rng.random(3) * (hi - lo)
+        parts.append(unit * r + c)
+        albedo.append(list(rng.uniform(0.2, 0.8, 3)))
+        surf.append([surface_id(MAT_LAMBERTIAN, s + 1)] * unit.shape[0])
+    from .camera import camera_from_vfov
+    cam = camera_from_vfov([0.5, 0.5, 0.02], [0.5, 0.5, 1.0], [0.0, 1.0, 0.0], 60.0)
+    return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
+                   np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
+                   f"unit box + {n_spheres} icospheres (subdivision {subdivisions}) + ceiling light")
+
+
+def small_rt_scene(seed: int = 1) -> RtScene:
+    """A small scene for parity tests: the box, the light and 4 icospheres of
+    subdivision 2 (1,294 triangles)."""
+    return spheres_in_box(n_spheres=4, subdivisions=2, seed=seed, rmin=0.1, rmax=0.2)

@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
-    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune"],
+    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune", "render"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -541,7 +541,19 @@ def run_case(args):
             ms.append(a.elapsed_time(b))
         return statistics.median(ms)
 
-    if args.case == "tune":
+    if args.case == "render":
+        from bajo_b200 import rt, scenes
+        sc = scenes.spheres_in_box()
+        gsc = rt.GpuRtTriangleScene(sc)
+        settings = rt.RenderSettings(1280, 720, 64, rng_seed=2026, max_depth=8)
+        ws = rt.RenderWorkspace(settings, rt.MIS)
+        ms = timed(lambda: rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws))
+        rays, shadows = ws.ray_counts()
+        paths = 1280 * 720 * 64
+        out.update({"ms": round(ms, 3), "samples_s": round(paths / ms * 1e3, 1),
+                    "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
+                    "triangles": sc.n_tris, "status": ws.status()})
+    elif args.case == "tune":
         out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
         out["device"] = autotune.device_key()
     elif args.case == "sort":

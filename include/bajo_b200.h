@@ -192,6 +192,75 @@ int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cameras, uin
                                 uint32_t height, int32_t tri_mode, float* d_hits8, uint32_t* d_stats,
                                 void* stream);
 
+/* ======================================================================== */
+/* Wavefront path tracing over one triangle LBVH                             */
+/* ======================================================================== */
+/* Render algorithms (RENDER, bajo/rt/types.mojo:53-59). */
+#define BAJO_RENDER_PATH 0
+#define BAJO_RENDER_NEE 3
+#define BAJO_RENDER_MIS 4
+
+/* Surface ids: kind in the top 4 bits, table index below
+ * (SurfaceId, bajo/rt/types.mojo:24-34). */
+#define BAJO_MAT_LAMBERTIAN 0u
+#define BAJO_MAT_EMISSIVE 3u
+#define BAJO_SURFACE(kind, index) (((uint32_t)(kind) << 28) | ((uint32_t)(index) & 0x0FFFFFFFu))
+
+/* Light records, 16 floats: [p0 xyz, p1 xyz, p2 xyz, emission rgb,
+ * alias probability, alias index (u32 bits), pad, pad]
+ * (GpuRtLights, bajo/rt/gpu/path_shading.mojo:60-74,146). */
+#define BAJO_LIGHT_STRIDE 16
+
+/* Queue status words (WAVE_STATUS, bajo/rt/wavefront_contract.mojo:25-29). */
+#define BAJO_WAVE_PATH_OVERFLOW 0x10u
+#define BAJO_WAVE_SHADOW_OVERFLOW 0x20u
+
+typedef struct BajoRtScene {
+  const BajoLbvh* bvh;       /* single-segment tree over the scene triangles       */
+  const uint32_t* surfaces;  /* per triangle, item order: BAJO_SURFACE(kind, idx)  */
+  const float* lambertians;  /* 3 f32 albedo per Lambertian material               */
+  const float* emissives;    /* 3 f32 radiance per emissive material               */
+  const float* lights;       /* BAJO_LIGHT_STRIDE f32 per emissive triangle        */
+  uint32_t n_lights;
+  float total_light_weight;  /* sum of area * mean(radiance) over the lights        */
+} BajoRtScene;
+
+typedef struct BajoRenderSettings {
+  uint32_t width, height, spp, max_depth;
+  uint64_t seed;
+  int32_t algorithm;     /* BAJO_RENDER_*                                         */
+  uint32_t chunk_paths;  /* queue capacity in paths (0 = default); whole pixels   */
+} BajoRenderSettings;
+
+/* Host: emissive-triangle light records with a Walker-Vose alias table over
+ * their power (LightStore, bajo/rt/types.mojo:190-247,490-525).  h_* are HOST
+ * arrays; out_lights holds max_lights * BAJO_LIGHT_STRIDE floats. */
+int32_t bajo_rt_build_lights(const float* h_verts, const uint32_t* h_surfaces, uint32_t n_tris,
+                             const float* h_emissives, uint32_t n_emissives, float* out_lights, uint32_t max_lights,
+                             uint32_t* n_lights, float* total_weight);
+
+/* Workspace: two path queues (id + 12 f32 planes), a shadow queue (id + 11
+ * planes), per-sample radiance (3 planes), per-bounce counters
+ * (GpuRtRenderTarget, bajo/rt/gpu/resources.mojo:38). */
+int32_t bajo_render_workspace_size(const BajoRenderSettings* settings, size_t* bytes);
+
+/* Replaces render_gpu_triangles / enqueue_render_gpu_triangles
+ * (bajo/rt/gpu/triangle_path.mojo:143,172) for Lambertian + emissive
+ * triangle scenes: per chunk of whole pixels, primary rays
+ * (gpu_rt_primary_kernel, bajo/rt/gpu/common_kernels.mojo:22), then per
+ * bounce one closest-hit + shading kernel (gpu_rt_scene_trace_kernel,
+ * bajo/rt/gpu/scene_trace.mojo:369) and one any-hit shadow kernel
+ * (:586), then the per-pixel resolve (common_kernels.mojo:97).
+ * d_pixels: 3 f32 per pixel (mean radiance).  d_pixels64 (may be NULL): 3 f64
+ * per pixel to which the SUM of every sample is added (long reference
+ * renders accumulate across calls). */
+int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoRenderSettings* settings,
+                    float* d_pixels, double* d_pixels64, void* d_workspace, size_t workspace_bytes, void* stream);
+
+/* Synchronises `stream` and reads the closest-hit and shadow rays traced by
+ * the last bajo_render call on this workspace. */
+int32_t bajo_render_stats(const void* d_workspace, void* stream, uint64_t* rays, uint64_t* shadow_rays);
+
 /* Host-side camera records (no device work).  Camera.__init__ and
  * Camera.from_vfov (bajo/bvh/camera.mojo:77-116): out20 receives
  * [origin, forward, right, up, fov_scale, focus_dist, disk_u, disk_v]

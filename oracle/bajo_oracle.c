@@ -534,12 +534,12 @@ static inline float rcp1(float d) {
   return fabsf(d) > eps ? 1.0f / d : (d < 0.0f ? -large : large);
 }
 
-static bo_ray make_ray(const float* rays, uint32_t n, uint32_t i) {
+static bo_ray make_ray_od(v3 o, v3 d, float tmin, float tmax) {
   bo_ray r;
-  r.o = v3make(rays[i], rays[(size_t)n + i], rays[2 * (size_t)n + i]);
-  r.tmin = rays[3 * (size_t)n + i];
-  r.d = v3make(rays[4 * (size_t)n + i], rays[5 * (size_t)n + i], rays[6 * (size_t)n + i]);
-  r.tmax = rays[7 * (size_t)n + i];
+  r.o = o;
+  r.tmin = tmin;
+  r.d = d;
+  r.tmax = tmax;
   r.rcp = v3make(rcp1(r.d.x), rcp1(r.d.y), rcp1(r.d.z));
   r.par[0] = !(fabsf(r.d.x) > 1.0e-9f);
   r.par[1] = !(fabsf(r.d.y) > 1.0e-9f);
@@ -555,6 +555,11 @@ static bo_ray make_ray(const float* rays, uint32_t n, uint32_t i) {
   r.sy = idx3(r.d, r.ky) / dz;
   r.sz = 1.0f / dz;
   return r;
+}
+
+static bo_ray make_ray(const float* rays, uint32_t n, uint32_t i) {
+  return make_ray_od(v3make(rays[i], rays[(size_t)n + i], rays[2 * (size_t)n + i]), v3make(rays[4 * (size_t)n + i], rays[5 * (size_t)n + i], rays[6 * (size_t)n + i]),
+                     rays[3 * (size_t)n + i], rays[7 * (size_t)n + i]);
 }
 
 /* one slab: (b - o) * rcp, except on axes the ray is parallel to
@@ -1059,4 +1064,377 @@ void bo_cpu_trace(const BoCpuNode* nodes, const uint32_t* items, const float* ve
                   uint32_t n, int mode, float* hits8, uint32_t n_threads) {
   cpu_trace_ctx c = {nodes, items, verts, rays, n, mode, hits8};
   bo_parallel_for(n, n_threads, 1024, cpu_trace_range, &c);
+}
+
+/* ========================================================================= */
+/* Wavefront path tracer (PATH / NEE / MIS), restated per path               */
+/* ========================================================================= */
+/* The GPU renderer runs one kernel per bounce over queues; every path is
+ * independent and owns its random streams, so a per-path loop that adds the
+ * same contributions in the same order (bounce b: the hit's emission or sky,
+ * then the shadow ray's light) produces the same per-sample radiance.
+ * References: bajo/rt/gpu/common_kernels.mojo:22-136 (primary, resolve),
+ * bajo/rt/gpu/scene_trace.mojo:41-369,586 (trace, shadow),
+ * bajo/rt/gpu/path_shading.mojo:261-590 (NEE, MIS emission, Lambertian),
+ * bajo/rt/shading.mojo:92-118, bajo/rt/common.mojo:12-67,
+ * bajo/rt/lighting.mojo:7-39, bajo/rt/wavefront_contract.mojo:107-133. */
+
+/* Philox-4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11); counter
+ * (0, 0, stage, path_id), key = seed: the first block of the stream owned by
+ * the (path, stage) pair.  24-bit uniforms in [0, 1). */
+void bo_rt_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+  uint32_t k0 = key[0], k1 = key[1];
+  for (int r = 0; r < 10; ++r) {
+    uint64_t p0 = (uint64_t)0xD2511F53u * c0, p1 = (uint64_t)0xCD9E8D57u * c2;
+    uint32_t hi0 = (uint32_t)(p0 >> 32), lo0 = (uint32_t)p0, hi1 = (uint32_t)(p1 >> 32), lo1 = (uint32_t)p1;
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+void bo_rt_uniform4(uint64_t seed, uint32_t path_id, uint32_t stage, float out[4]) {
+  const uint32_t ctr[4] = {0u, 0u, stage, path_id};
+  const uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+  uint32_t x[4];
+  bo_rt_philox4x32_10(ctr, key, x);
+  uint32_t c0 = x[0], c1 = x[1], c2 = x[2], c3 = x[3];
+  const float s = 1.0f / 16777216.0f;
+  out[0] = (float)(c0 >> 8) * s; out[1] = (float)(c1 >> 8) * s;
+  out[2] = (float)(c2 >> 8) * s; out[3] = (float)(c3 >> 8) * s;
+}
+
+/* sin / cos of 2*pi*u: nearest quarter turn, Taylor series on |a| <= pi/4. */
+void bo_rt_sincos_turns(float u, float* s_out, float* c_out) {
+  const float qf = floorf(u * 4.0f + 0.5f);
+  const int q = (int)qf & 3;
+  const float r = u - qf * 0.25f;
+  const float a = r * 6.28318530717958647692f;
+  const float a2 = a * a;
+  float s = fmaf(a2, 1.0f / 362880.0f, -1.0f / 5040.0f);
+  s = fmaf(a2, s, 1.0f / 120.0f);
+  s = fmaf(a2, s, -1.0f / 6.0f);
+  s = fmaf(a2, s, 1.0f);
+  s = a * s;
+  float c = fmaf(a2, -1.0f / 3628800.0f, 1.0f / 40320.0f);
+  c = fmaf(a2, c, -1.0f / 720.0f);
+  c = fmaf(a2, c, 1.0f / 24.0f);
+  c = fmaf(a2, c, -0.5f);
+  c = fmaf(a2, c, 1.0f);
+  if (q == 0) { *s_out = s; *c_out = c; }
+  else if (q == 1) { *s_out = c; *c_out = -s; }
+  else if (q == 2) { *s_out = -s; *c_out = -c; }
+  else { *s_out = -c; *c_out = s; }
+}
+
+#define BO_MAT_LAMBERTIAN 0u
+#define BO_MAT_EMISSIVE 3u
+#define BO_LIGHT_STRIDE 16
+static const float BO_INV_PI = 0.3183098861837907f;
+
+static inline v3 vmul(v3 a, v3 b) { return v3make(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline v3 vneg(v3 a) { return v3make(-a.x, -a.y, -a.z); }
+static inline v3 vdivs(v3 a, float s) { return v3make(a.x / s, a.y / s, a.z / s); }
+static inline float power_heuristic(float a, float b) {
+  float a2 = a * a, b2 = b * b, den = a2 + b2;
+  return den > 0.0f ? a2 / den : 0.0f;
+}
+
+/* LightStore (bajo/rt/types.mojo:190-247, 490-525) */
+int bo_rt_build_lights(const float* v, const uint32_t* surf, uint32_t n, const float* em, float* out,
+                       uint32_t max_lights, uint32_t* n_lights, float* total_weight) {
+  uint32_t* tri = (uint32_t*)malloc(sizeof(uint32_t) * (n ? n : 1));
+  float* w = (float*)malloc(sizeof(float) * (n ? n : 1));
+  uint32_t count = 0;
+  float total = 0.0f;
+  for (uint32_t i = 0; i < n; ++i) {
+    if ((surf[i] >> 28) != BO_MAT_EMISSIVE) continue;
+    const float* p = v + (size_t)9 * i;
+    v3 v0 = load3(p), e1 = v3sub(load3(p + 3), v0), e2 = v3sub(load3(p + 6), v0);
+    v3 c = v3cross(e1, e2);
+    float area = 0.5f * sqrtf(v3dot(c, c));
+    const float* L = em + 3 * (size_t)(surf[i] & 0x0FFFFFFFu);
+    float imp = fmaxf(((L[0] + L[1]) + L[2]) / 3.0f, 0.0f);
+    float wt = area * imp;
+    if (wt > 0.0f) {
+      total += wt;
+      tri[count] = i;
+      w[count] = wt;
+      ++count;
+    }
+  }
+  if (count > max_lights) { free(tri); free(w); return 1; }
+  float* prob = (float*)malloc(sizeof(float) * (count ? count : 1));
+  float* scaled = (float*)malloc(sizeof(float) * (count ? count : 1));
+  uint32_t* alias = (uint32_t*)malloc(sizeof(uint32_t) * (count ? count : 1));
+  uint32_t* small = (uint32_t*)malloc(sizeof(uint32_t) * (count ? count : 1));
+  uint32_t* large = (uint32_t*)malloc(sizeof(uint32_t) * (count ? count : 1));
+  uint32_t ns = 0, nl = 0;
+  for (uint32_t i = 0; i < count; ++i) { prob[i] = 1.0f; alias[i] = 0; }
+  if (count > 0 && total > 0.0f) {
+    for (uint32_t i = 0; i < count; ++i) {
+      alias[i] = i;
+      scaled[i] = w[i] * (float)count / total;
+      if (scaled[i] < 1.0f) small[ns++] = i; else large[nl++] = i;
+    }
+    while (ns > 0 && nl > 0) {
+      uint32_t si = small[--ns], li = large[--nl];
+      prob[si] = scaled[si];
+      alias[si] = li;
+      scaled[li] = scaled[li] + scaled[si] - 1.0f;
+      if (scaled[li] < 1.0f) small[ns++] = li; else large[nl++] = li;
+    }
+    while (ns > 0) { uint32_t i = small[--ns]; prob[i] = 1.0f; alias[i] = i; }
+    while (nl > 0) { uint32_t i = large[--nl]; prob[i] = 1.0f; alias[i] = i; }
+  }
+  for (uint32_t k = 0; k < count; ++k) {
+    float* r = out + (size_t)k * BO_LIGHT_STRIDE;
+    memcpy(r, v + (size_t)9 * tri[k], 9 * sizeof(float));
+    const float* L = em + 3 * (size_t)(surf[tri[k]] & 0x0FFFFFFFu);
+    r[9] = L[0]; r[10] = L[1]; r[11] = L[2];
+    r[12] = prob[k];
+    memcpy(&r[13], &alias[k], 4);
+    r[14] = 0.0f; r[15] = 0.0f;
+  }
+  *n_lights = count;
+  *total_weight = total;
+  free(tri); free(w); free(prob); free(scaled); free(alias); free(small); free(large);
+  return 0;
+}
+
+/* any hit on (tmin, tmax): boxes culled against the ray's t_max */
+static int any_hit(const BoLbvh* bvh, const float* verts, const bo_ray* r) {
+  bo_hit h = miss_hit(r->tmax);
+  uint32_t root = bvh->roots[0];
+  if (root == BO_SENTINEL) return 0;
+  if (root & BO_LEAF_FLAG) {
+    uint32_t item = bvh->leaf_ids[root & 0x7FFFFFFFu];
+    test_tri(r, verts, item, item, BO_TRI_WATERTIGHT, &h);
+    return h.prim != BO_EMPTY;
+  }
+  uint32_t stack[128], sp = 0, cur = root;
+  for (;;) {
+    const float* b = bvh->node_bounds + (size_t)12 * cur;
+    uint32_t c[2] = {bvh->node_meta[4 * (size_t)cur + 1], bvh->node_meta[4 * (size_t)cur + 2]};
+    for (int k = 0; k < 2; ++k) {
+      float tn;
+      if (!box_hit(r, b + 6 * k, r->tmax, &tn)) continue;
+      if (c[k] & BO_LEAF_FLAG) {
+        uint32_t item = bvh->leaf_ids[c[k] & 0x7FFFFFFFu];
+        test_tri(r, verts, item, item, BO_TRI_WATERTIGHT, &h);
+        if (h.prim != BO_EMPTY) return 1;
+      } else {
+        stack[sp++] = c[k];
+      }
+    }
+    if (sp == 0) return 0;
+    cur = stack[--sp];
+  }
+}
+
+typedef struct {
+  const BoLbvh* bvh;
+  const float* verts;
+  const uint32_t* surfaces;
+  const float* lambertians;
+  const float* emissives;
+  const float* lights;
+  uint32_t n_lights;
+  float total_weight;
+  const float* cam;
+  uint32_t width, height, spp, max_depth;
+  uint64_t seed;
+  int algorithm;
+  float* sample_radiance; /* 3 per path, path_id order */
+} rt_ctx;
+
+static inline uint32_t st_bsdf(uint32_t b) { return (0u << 30) | (b + 1); }
+static inline uint32_t st_roulette(uint32_t b) { return (1u << 30) | (b + 1); }
+static inline uint32_t st_light(uint32_t b) { return (2u << 30) | (b + 1); }
+
+static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
+  const float* cam = c->cam;
+  float r[4];
+  bo_rt_uniform4(c->seed, path_id, 0, r);
+  uint32_t pixel = path_id / c->spp;
+  uint32_t px = pixel % c->width, py = pixel / c->width;
+  float st, ct;
+  bo_rt_sincos_turns(r[0], &st, &ct);
+  float lr = sqrtf(r[1]);
+  float lens_u = lr * ct, lens_v = lr * st;
+  float w = (float)c->width, h = (float)c->height;
+  float aspect = w / h;
+  float sx = (((float)px + r[2]) / w) * 2.0f - 1.0f;
+  float sy = 1.0f - (((float)py + r[3]) / h) * 2.0f;
+  v3 origin = load3(cam), fwd = load3(cam + 3), right = load3(cam + 6), up = load3(cam + 9);
+  float fs = cam[12], focus = cam[13];
+  v3 du = load3(cam + 14), dv = load3(cam + 17);
+  v3 inner = v3add(v3add(fwd, v3muls(right, (sx * aspect) * fs)), v3muls(up, sy * fs));
+  v3 focal = v3add(origin, v3make(focus * inner.x, focus * inner.y, focus * inner.z));
+  v3 ro = v3add(v3add(origin, v3make(lens_u * du.x, lens_u * du.y, lens_u * du.z)),
+                v3make(lens_v * dv.x, lens_v * dv.y, lens_v * dv.z));
+  v3 o = ro, d = v3normalize(v3sub(focal, ro));
+  float tmin = 0.001f, tmax = BO_FLT_MAX;
+  v3 T = v3make(1.0f, 1.0f, 1.0f);
+  float prev_pdf = 0.0f;
+  int delta = 1;
+  float rad[3] = {0.0f, 0.0f, 0.0f};
+  for (uint32_t b = 0; b < c->max_depth; ++b) {
+    bo_ray ray = make_ray_od(o, d, tmin, tmax);
+    bo_hit hit = trace_one(c->bvh, c->verts, &ray, 0, BO_TRI_WATERTIGHT, NULL, NULL);
+    if (hit.prim == BO_EMPTY) {
+      v3 un = v3normalize(d);
+      float a = 0.5f * (un.y + 1.0f);
+      v3 sk = v3make((1.0f - a) * 1.0f + a * 0.5f, (1.0f - a) * 1.0f + a * 0.7f, (1.0f - a) * 1.0f + a * 1.0f);
+      v3 add = vmul(T, sk);
+      rad[0] += add.x; rad[1] += add.y; rad[2] += add.z;
+      break;
+    }
+    float t = hit.t;
+    v3 outward = hit.n;
+    int front = v3dot(d, outward) < 0.0f;
+    v3 normal = front ? outward : vneg(outward);
+    uint32_t surface = c->surfaces[hit.prim];
+    uint32_t kind = surface >> 28, midx = surface & 0x0FFFFFFFu;
+    v3 p = v3make(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+    if (kind == BO_MAT_EMISSIVE) {
+      if (front) {
+        v3 L = load3(c->emissives + 3 * (size_t)midx);
+        float wgt = 1.0f;
+        if (c->algorithm == 3 && b > 0 && !delta) wgt = 0.0f;
+        if (c->algorithm == 4 && b > 0 && !delta) {
+          float lc = fmaxf(v3dot(normal, vneg(v3normalize(d))), 0.0f);
+          float lpdf = 0.0f;
+          if (lc > 0.0f && c->total_weight > 0.0f) {
+            float d2 = (t * t) * v3dot(d, d);
+            lpdf = (d2 * ((L.x + L.y) + L.z)) / ((3.0f * lc) * c->total_weight);
+          }
+          wgt = power_heuristic(prev_pdf, lpdf);
+        }
+        v3 TL = vmul(T, L);
+        rad[0] += TL.x * wgt; rad[1] += TL.y * wgt; rad[2] += TL.z * wgt;
+      }
+      break;
+    }
+    if (kind != BO_MAT_LAMBERTIAN) break;
+    v3 albedo = load3(c->lambertians + 3 * (size_t)midx);
+    int want_shadow = 0;
+    v3 sh_c = v3make(0, 0, 0);
+    bo_ray shadow;
+    if ((c->algorithm == 3 || c->algorithm == 4) && c->n_lights > 0 && c->total_weight > 0.0f) {
+      float u[4];
+      bo_rt_uniform4(c->seed, path_id, st_light(b), u);
+      float as = u[0] * (float)c->n_lights;
+      uint32_t li = (uint32_t)as;
+      float frac = as - (float)li;
+      const float* lrec = c->lights + (size_t)li * BO_LIGHT_STRIDE;
+      if (frac > lrec[12]) memcpy(&li, &lrec[13], 4);
+      lrec = c->lights + (size_t)li * BO_LIGHT_STRIDE;
+      v3 p0 = load3(lrec), e1 = v3sub(load3(lrec + 3), p0), e2 = v3sub(load3(lrec + 6), p0);
+      v3 av = v3cross(e1, e2);
+      float tas = v3dot(av, av);
+      if (tas > 0.0f) {
+        v3 ln = vdivs(av, sqrtf(tas));
+        float ru = sqrtf(u[1]);
+        float b1 = ru * (1.0f - u[2]);
+        float b2 = ru - b1;
+        v3 lp = v3add(v3add(p0, v3muls(e1, b1)), v3muls(e2, b2));
+        v3 tl = v3sub(lp, p);
+        float d2 = v3dot(tl, tl);
+        if (d2 > 1.0e-8f) {
+          float dist = sqrtf(d2);
+          v3 dir = vdivs(tl, dist);
+          float scos = fmaxf(v3dot(normal, dir), 0.0f);
+          float lcos = fmaxf(v3dot(ln, vneg(dir)), 0.0f);
+          float smax = dist - 0.002f;
+          if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
+            v3 E = load3(lrec + 9);
+            float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * c->total_weight);
+            float bpdf = fmaxf(v3dot(normal, v3normalize(dir)), 0.0f) * BO_INV_PI;
+            if (lpdf > 0.0f && bpdf > 0.0f) {
+              float wgt = c->algorithm == 4 ? power_heuristic(lpdf, bpdf) : 1.0f;
+              float scale = (scos * wgt) / lpdf;
+              if (scale > 0.0f) {
+                v3 value = v3muls(albedo, BO_INV_PI);
+                v3 tv = vmul(vmul(T, value), E);
+                want_shadow = 1;
+                sh_c = v3muls(tv, scale);
+                shadow = make_ray_od(p, dir, 0.001f, smax);
+              }
+            }
+          }
+        }
+      }
+    }
+    int alive = 0;
+    v3 nd = v3make(0, 0, 0), Tn = T;
+    float pdf = 0.0f;
+    if (b + 1 < c->max_depth) {
+      float u[4];
+      bo_rt_uniform4(c->seed, path_id, st_bsdf(b), u);
+      float s2, c2;
+      bo_rt_sincos_turns(u[0], &s2, &c2);
+      float z = 1.0f - 2.0f * u[1];
+      float radius = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+      v3 sd = v3add(normal, v3make(radius * c2, radius * s2, z));
+      if (fabsf(sd.x) < 1.0e-8f && fabsf(sd.y) < 1.0e-8f && fabsf(sd.z) < 1.0e-8f) sd = normal;
+      nd = v3normalize(sd);
+      pdf = fmaxf(v3dot(normal, v3normalize(nd)), 0.0f) * BO_INV_PI;
+      Tn = vmul(T, albedo);
+      alive = 1;
+      if (b + 1 >= 5u) {
+        float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+        if (m <= 0.0f) alive = 0;
+        else {
+          float survival = fminf(fmaxf(m, 0.05f), 0.95f);
+          float rr[4];
+          bo_rt_uniform4(c->seed, path_id, st_roulette(b), rr);
+          if (rr[0] >= survival) alive = 0;
+          else Tn = vdivs(Tn, survival);
+        }
+      }
+    }
+    if (want_shadow && !any_hit(c->bvh, c->verts, &shadow)) {
+      rad[0] += sh_c.x; rad[1] += sh_c.y; rad[2] += sh_c.z;
+    }
+    if (!alive) break;
+    o = p; d = nd; tmin = 0.001f; tmax = BO_FLT_MAX; T = Tn; prev_pdf = pdf; delta = 0;
+  }
+  out[0] = rad[0]; out[1] = rad[1]; out[2] = rad[2];
+}
+
+typedef struct { const rt_ctx* c; } rt_job;
+
+static void rt_range(void* p, uint32_t b, uint32_t e) {
+  const rt_ctx* c = ((rt_job*)p)->c;
+  for (uint32_t i = b; i < e; ++i) rt_path(c, i, c->sample_radiance + 3 * (size_t)i);
+}
+
+/* bo_render: pixels (3 f32, mean over samples in sample order) and optional
+ * per-sample radiance.  Scene arrays as in BajoRtScene. */
+void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, const float* lambertians,
+               const float* emissives, const float* lights, uint32_t n_lights, float total_weight,
+               const float* cam, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth, uint64_t seed,
+               int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads) {
+  uint64_t n_paths = (uint64_t)width * height * spp;
+  float* rad = sample_radiance ? sample_radiance : (float*)malloc(sizeof(float) * 3 * n_paths);
+  rt_ctx c = {bvh, verts, surfaces, lambertians, emissives, lights, n_lights, total_weight, cam,
+              width, height, spp, max_depth, seed, algorithm, rad};
+  rt_job job = {&c};
+  bo_parallel_for((uint32_t)n_paths, n_threads, 256, rt_range, &job);
+  float scale = 1.0f / (float)spp;
+  for (uint64_t px = 0; px < (uint64_t)width * height; ++px) {
+    float r = 0.0f, g = 0.0f, b = 0.0f;
+    for (uint32_t s = 0; s < spp; ++s) {
+      const float* v = rad + 3 * (px * spp + s);
+      r += v[0]; g += v[1]; b += v[2];
+    }
+    pixels[3 * px + 0] = r * scale;
+    pixels[3 * px + 1] = g * scale;
+    pixels[3 * px + 2] = b * scale;
+  }
+  if (!sample_radiance) free(rad);
 }

@@ -153,6 +153,18 @@ void bo_cpu_trace(const BoCpuNode* nodes, const uint32_t* item_indices,
                   const float* verts, const float* rays_soa, uint32_t n_rays,
                   int tri_mode, float* hits8, uint32_t n_threads);
 
+/* ---- wavefront path tracer (PATH=0 / NEE=3 / MIS=4) ---------------------- */
+/* Philox-4x32-10 block (Salmon et al., SC'11) */
+void bo_rt_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void bo_rt_uniform4(uint64_t seed, uint32_t path_id, uint32_t stage, float out[4]);
+void bo_rt_sincos_turns(float u, float* s, float* c);
+int bo_rt_build_lights(const float* verts, const uint32_t* surfaces, uint32_t n_tris, const float* emissives,
+                       float* out_lights, uint32_t max_lights, uint32_t* n_lights, float* total_weight);
+void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, const float* lambertians,
+               const float* emissives, const float* lights, uint32_t n_lights, float total_weight,
+               const float* camera20, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth,
+               uint64_t seed, int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads);
+
 #ifdef __cplusplus
 }
 #endif

@@ -85,6 +85,12 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_trace_bvh2_stats": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _I, _P]),
         "bo_cpu_build_lbvh": (_U32, [_P, _U32, _U32, _P, _P]),
         "bo_cpu_trace": (None, [_P, _P, _P, _P, _U32, _I, _P, _U32]),
+        "bo_rt_philox4x32_10": (None, [_P, _P, _P]),
+        "bo_rt_uniform4": (None, [ctypes.c_uint64, _U32, _U32, _P]),
+        "bo_rt_sincos_turns": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
+        "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
+        "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
+                             ctypes.c_uint64, _I, _P, _P, _U32]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -333,3 +339,55 @@ def hits_prim(hits8: np.ndarray) -> np.ndarray:
 
 def hits_t(hits8: np.ndarray) -> np.ndarray:
     return hits8.reshape(-1, 8)[:, 7]
+
+
+# ---------------------------------------------------------------- path tracer
+def philox4x32_10(ctr, key) -> list:
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().bo_rt_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
+    return [int(x) for x in out]
+
+
+def rt_uniform4(seed: int, path_id: int, stage: int) -> np.ndarray:
+    out = np.zeros(4, np.float32)
+    lib().bo_rt_uniform4(seed, path_id, stage, _ptr(out))
+    return out
+
+
+def rt_sincos_turns(u: float):
+    s, c = ctypes.c_float(), ctypes.c_float()
+    lib().bo_rt_sincos_turns(u, ctypes.byref(s), ctypes.byref(c))
+    return s.value, c.value
+
+
+def rt_build_lights(scene):
+    n_em = int(np.count_nonzero((scene.surfaces >> 28) == 3))
+    out = np.zeros(max(n_em, 1) * 16, np.float32)
+    n = ctypes.c_uint32(0)
+    w = ctypes.c_float(0.0)
+    rc = lib().bo_rt_build_lights(_ptr(scene.vertices), _ptr(scene.surfaces), scene.n_tris, _ptr(scene.emissives),
+                                  _ptr(out), max(n_em, 1), ctypes.byref(n), ctypes.byref(w))
+    assert rc == 0
+    return out, n.value, w.value
+
+
+def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=4, lights=None, bvh=None,
+           threads=None, return_samples=False):
+    """CPU restatement of the wavefront tracer: (height, width, 3) pixels."""
+    if bvh is None:
+        bvh = lbvh_build(scene.vertices)
+    if lights is None:
+        lights, n_lights, total = rt_build_lights(scene)
+    else:
+        lights, n_lights, total = lights
+    cam = np.ascontiguousarray(camera, np.float32)
+    pixels = np.zeros(3 * width * height, np.float32)
+    samples = np.zeros(3 * width * height * spp, np.float32) if return_samples else None
+    s = bvh.struct()
+    lib().bo_render(ctypes.byref(s), _ptr(bvh.verts), _ptr(scene.surfaces), _ptr(scene.lambertians),
+                    _ptr(scene.emissives), _ptr(lights), n_lights, total, _ptr(cam), width, height, spp, max_depth,
+                    seed, algorithm, _ptr(pixels), None if samples is None else _ptr(samples), threads or n_threads())
+    img = pixels.reshape(height, width, 3)
+    return (img, samples.reshape(height, width, spp, 3)) if return_samples else img
