@@ -86,6 +86,8 @@ SIGNATURES = {
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
     "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
+    "bajo_trace_batch": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, ctypes.c_uint64, _I32, _P, _P,
+                                _P, _P, _P, _P]),
     "bajo_trace_camera_stats": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P]),
     "bajo_rt_build_lights": (_I32, [_P, _P, _U32, _P, _U32, _P, _U32, ctypes.POINTER(_U32),
                                     ctypes.POINTER(_F)]),

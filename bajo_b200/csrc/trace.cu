@@ -1,9 +1,11 @@
 // trace.cu -- closest-hit traversal entry points (GpuTriangleBvh.launch_rays /
 // launch_camera, bajo/bvh/gpu/triangle_bvh.mojo:520-614).  The traversal
 // itself is in traverse.cuh.
+#include "sampling.cuh"
 #include "traverse.cuh"
 
 namespace bajo {
+int sm_count();
 namespace {
 
 using namespace trav;
@@ -86,6 +88,56 @@ __global__ void __launch_bounds__(kTraceBlock) trace_camera_kernel(const float* 
   if constexpr (STATS) reinterpret_cast<uint2*>(stats)[i] = make_uint2(nn, nt);
 }
 
+// Batched closest hits over a segmented LBVH: ray i belongs to scene
+// i / (width * height), starts at that scene's camera (cam_stride floats
+// apart; 0 = one shared camera) and is traced against that scene's root.  A
+// primary hit spawns one cosine-weighted bounce ray about the geometric normal
+// oriented against the ray (the Lambertian sample of bajo/rt/shading.mojo:92,
+// Philox stream (ray, stage 1)).  Misses report t = FLT_MAX / prim = EMPTY.
+template <int MODE>
+__global__ void __launch_bounds__(kTraceBlock) batch_trace_kernel(
+    const float* __restrict__ cams, uint32_t cam_stride, uint32_t n, uint32_t n_nodes, uint32_t width,
+    uint32_t height, float inv_h, const uint32_t* __restrict__ roots, const float4* __restrict__ nb,
+    const uint4* __restrict__ meta, const float4* __restrict__ tris, uint64_t seed, float* __restrict__ t0,
+    uint32_t* __restrict__ p0, float* __restrict__ t1, uint32_t* __restrict__ p1, uint32_t* __restrict__ status) {
+  const uint32_t ppv = width * height;
+  for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+    const uint32_t view = i / ppv, local = i - view * ppv;
+    const float* c = cams + (size_t)view * cam_stride;
+    const uint32_t px = local % width, py = local / width;
+    const float sx = (2.0f * ((float)px + 0.5f) - (float)width) * inv_h;
+    const float sy = 1.0f - 2.0f * ((float)py + 0.5f) * inv_h;
+    const float fs = __ldg(c + 12);
+    const f3 fwd = mk(__ldg(c + 3), __ldg(c + 4), __ldg(c + 5));
+    const f3 right = mk(__ldg(c + 6), __ldg(c + 7), __ldg(c + 8));
+    const f3 up = mk(__ldg(c + 9), __ldg(c + 10), __ldg(c + 11));
+    const f3 d = normalize((fwd + right * (sx * fs)) + up * (sy * fs));
+    const f3 o = mk(__ldg(c + 0), __ldg(c + 1), __ldg(c + 2));
+    const uint32_t root = __ldg(roots + view);
+    const Hit h = trace_bvh2<MODE>(make_ray(o, d, 0.0f, FLT_MAX), root, nb, meta, tris, n_nodes, status);
+    t0[i] = h.t;
+    p0[i] = h.prim;
+    float bt = FLT_MAX;
+    uint32_t bp = kEmpty;
+    if (h.leaf != kEmpty) {
+      const float4 a = __ldg(tris + (size_t)h.leaf * 3 + 0);
+      const float4 b = __ldg(tris + (size_t)h.leaf * 3 + 1);
+      const float4 e = __ldg(tris + (size_t)h.leaf * 3 + 2);
+      const f3 v0 = mk(a.x, a.y, a.z);
+      const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(e.x, e.y, e.z) - v0));
+      const f3 normal = dot(d, outward) < 0.0f ? outward : mk(-outward.x, -outward.y, -outward.z);
+      const float4 u = smp::uniform4(seed, i, smp::stage_bsdf(0));
+      const f3 dir = smp::lambertian_dir(normal, u.x, u.y);
+      const f3 p = mk(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+      const Hit h2 = trace_bvh2<MODE>(make_ray(p, dir, 0.001f, FLT_MAX), root, nb, meta, tris, n_nodes, status);
+      bt = h2.t;
+      bp = h2.prim;
+    }
+    t1[i] = bt;
+    p1[i] = bp;
+  }
+}
+
 bool bvh_ok(const BajoLbvh* b) {
   return b && b->roots && b->node_bounds && b->node_meta && b->leaf_tris && b->n_segments >= 1;
 }
@@ -136,6 +188,36 @@ int32_t bajo_trace_camera(const BajoLbvh* bvh, const float* d_cams, uint32_t n, 
   else
     trace_camera_kernel<BAJO_TRI_WATERTIGHT><<<grid, kTraceBlock, 0, st>>>(
         d_cams, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb, meta, tris, d_hits8, d_t, d_prim, d_status);
+  return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_trace_batch(const BajoLbvh* bvh, const float* d_cams, uint32_t cam_stride, uint32_t width,
+                         uint32_t height, uint64_t seed, int32_t mode, float* d_t0, uint32_t* d_prim0, float* d_t1,
+                         uint32_t* d_prim1, uint32_t* d_status, void* stream) {
+  using namespace bajo;
+  if (!bvh_ok(bvh) || !d_cams || !d_t0 || !d_prim0 || !d_t1 || !d_prim1 || width == 0 || height == 0 ||
+      (cam_stride != 0 && cam_stride < 20) || (mode != BAJO_TRI_MT && mode != BAJO_TRI_WATERTIGHT))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  const uint64_t n64 = (uint64_t)bvh->n_segments * width * height;
+  if (n64 > 0xFFFFFFFFull) return BAJO_ERR_TOO_LARGE;
+  const uint32_t n = (uint32_t)n64;
+  if (n == 0) return BAJO_OK;
+  uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
+  const uint32_t cap = (uint32_t)sm_count() * 32;
+  if (grid > cap) grid = cap;
+  const float inv_h = 1.0f / (float)height;
+  const float4* nb = reinterpret_cast<const float4*>(bvh->node_bounds);
+  const uint4* meta = reinterpret_cast<const uint4*>(bvh->node_meta);
+  const float4* tris = reinterpret_cast<const float4*>(bvh->leaf_tris);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (mode == BAJO_TRI_MT)
+    batch_trace_kernel<BAJO_TRI_MT><<<grid, kTraceBlock, 0, st>>>(d_cams, cam_stride, n, bvh->n_leaves, width, height,
+                                                                  inv_h, bvh->roots, nb, meta, tris, seed, d_t0,
+                                                                  d_prim0, d_t1, d_prim1, d_status);
+  else
+    batch_trace_kernel<BAJO_TRI_WATERTIGHT><<<grid, kTraceBlock, 0, st>>>(
+        d_cams, cam_stride, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb, meta, tris, seed, d_t0, d_prim0,
+        d_t1, d_prim1, d_status);
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 

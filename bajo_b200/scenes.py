@@ -209,3 +209,17 @@ def small_rt_scene(seed: int = 1) -> RtScene:
     """A small scene for parity tests: the box, the light and 4 icospheres of
     subdivision 2 (1,294 triangles)."""
     return spheres_in_box(n_spheres=4, subdivisions=2, seed=seed, rmin=0.1, rmax=0.2)
+
+
+def batched_scenes(n_scenes: int = 4096, lo: int = 256, hi: int = 65536, seed: int = 0):
+    """The batched workload: n_scenes independent scenes whose triangle counts
+    are log-uniform in [lo, hi], each generated like the plain LBVH workload
+    with its own seed.  Returns (vertices, segment offsets)."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), size=n_scenes)).astype(np.int64)
+    counts = np.clip(counts, lo, hi)
+    offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    verts = np.empty(int(offsets[-1]) * 9, np.float32)
+    for s, c in enumerate(counts):
+        verts[offsets[s] * 9: offsets[s + 1] * 9] = random_triangles(int(c), seed=seed * 100003 + s + 1)
+    return verts, offsets.astype(np.uint32)

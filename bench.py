@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
-    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune", "render"],
+    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune", "render", "batched"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -516,6 +516,36 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak):
     return out
 
 
+def run_batched(steps, warmup, n_scenes=4096):
+    """Batched workload: 4,096 scenes (log-uniform 256..65,536 triangles),
+    256x256 primary + one cosine bounce per pixel, build + trace replayed as
+    one CUDA graph."""
+    import torch
+    from bajo_b200 import batch, camera, scenes
+    verts, so = scenes.batched_scenes(n_scenes=n_scenes)
+    v = torch.from_numpy(verts).cuda()
+    g = batch.BatchedGraph(v, so, camera.plain_lbvh_camera(), 256, 256, seed=7)
+    stream = torch.cuda.current_stream()
+    for _ in range(warmup):
+        g.replay()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        g.replay()
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    t = statistics.median(ms)
+    p0 = g.result.p0
+    bounce = int((p0 != -1).sum().item())
+    rays = n_scenes * 256 * 256 + bounce
+    return {"scenes": n_scenes, "triangles": int(so[-1]), "ms": round(t, 3),
+            "build_trace_mtri_s": round(int(so[-1]) / t / 1e3, 1), "mrays_s": round(rays / t / 1e3, 1),
+            "rays": rays, "status": g.status()}
+
+
 def run_case(args):
     """One piece of the path alone, for ncu captures and tuning runs."""
     import torch
@@ -553,6 +583,8 @@ def run_case(args):
         out.update({"ms": round(ms, 3), "samples_s": round(paths / ms * 1e3, 1),
                     "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
                     "triangles": sc.n_tris, "status": ws.status()})
+    elif args.case == "batched":
+        out.update(run_batched(args.steps, args.warmup))
     elif args.case == "tune":
         out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
         out["device"] = autotune.device_key()

@@ -184,6 +184,19 @@ int32_t bajo_trace_camera(const BajoLbvh* bvh, const float* d_cameras, uint32_t 
                           uint32_t height, int32_t tri_mode, float* d_hits8, float* d_t, uint32_t* d_prim,
                           uint32_t* d_status, void* stream);
 
+/* Batched build + trace workload over a segmented LBVH (one scene per
+ * segment; enqueue_segmented_wide_build + the BLAS-set trace,
+ * bajo/bvh/gpu/builder/segmented_build.mojo:89, bajo/bvh/gpu/triangle_bvh.mojo:
+ * 469): ray i belongs to scene i / (width*height), starts at that scene's
+ * camera (cam_stride floats apart, 0 = one shared camera) and is traced
+ * against that scene's root; a primary hit spawns one cosine-weighted bounce
+ * ray about the oriented geometric normal (Philox stream (ray, stage 1)).
+ * Outputs, n_segments*width*height each: primary t / prim, bounce t / prim
+ * (segment-local prim ids; misses: t = FLT_MAX, prim = 0xFFFFFFFF). */
+int32_t bajo_trace_batch(const BajoLbvh* bvh, const float* d_cameras, uint32_t cam_stride, uint32_t width,
+                         uint32_t height, uint64_t seed, int32_t tri_mode, float* d_t0, uint32_t* d_prim0,
+                         float* d_t1, uint32_t* d_prim1, uint32_t* d_status, void* stream);
+
 /* Instrumented camera trace (trace_triangle_bvh_camera_instrumented_kernel,
  * bajo/bvh/gpu/triangle_bvh.mojo:813; GpuTraversalStats,
  * bajo/bvh/gpu/trace.mojo:62): same hits as bajo_trace_camera plus, per ray,

@@ -1438,3 +1438,74 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
   }
   if (!sample_radiance) free(rad);
 }
+
+/* ========================================================================= */
+/* Batched primary + bounce trace over a segmented LBVH                      */
+/* ========================================================================= */
+static inline uint32_t st_bsdf0(void) { return (0u << 30) | 1u; }
+
+/* _sample_lambertian (bajo/rt/shading.mojo:92-118), same operations as the
+ * CUDA lambertian_dir */
+static v3 lambertian_dir(v3 normal, float u, float v) {
+  float st, ct;
+  bo_rt_sincos_turns(u, &st, &ct);
+  float z = 1.0f - 2.0f * v;
+  float rad = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+  v3 sd = v3add(normal, v3make(rad * ct, rad * st, z));
+  if (fabsf(sd.x) < 1.0e-8f && fabsf(sd.y) < 1.0e-8f && fabsf(sd.z) < 1.0e-8f) sd = normal;
+  return v3normalize(sd);
+}
+
+typedef struct {
+  const BoLbvh* bvh;
+  const float* verts;
+  const float* cams;
+  uint32_t cam_stride, width, height;
+  uint64_t seed;
+  int mode;
+  float *t0, *t1;
+  uint32_t *p0, *p1;
+} batch_ctx;
+
+static void batch_range(void* p, uint32_t b, uint32_t e) {
+  const batch_ctx* c = (const batch_ctx*)p;
+  const uint32_t ppv = c->width * c->height;
+  const float inv_h = 1.0f / (float)c->height;
+  for (uint32_t i = b; i < e; ++i) {
+    uint32_t view = i / ppv, local = i - view * ppv;
+    const float* cam = c->cams + (size_t)view * c->cam_stride;
+    uint32_t px = local % c->width, py = local / c->width;
+    float sx = (2.0f * ((float)px + 0.5f) - (float)c->width) * inv_h;
+    float sy = 1.0f - 2.0f * ((float)py + 0.5f) * inv_h;
+    float fs = cam[12];
+    v3 d = v3normalize(v3add(v3add(load3(cam + 3), v3muls(load3(cam + 6), sx * fs)), v3muls(load3(cam + 9), sy * fs)));
+    v3 o = load3(cam);
+    bo_ray r = make_ray_od(o, d, 0.0f, BO_FLT_MAX);
+    bo_hit h = trace_one(c->bvh, c->verts, &r, view, c->mode, NULL, NULL);
+    c->t0[i] = h.t;
+    c->p0[i] = h.prim;
+    float bt = BO_FLT_MAX;
+    uint32_t bp = BO_EMPTY;
+    if (h.prim != BO_EMPTY) {
+      v3 normal = v3dot(d, h.n) < 0.0f ? h.n : vneg(h.n);
+      float u[4];
+      bo_rt_uniform4(c->seed, i, st_bsdf0(), u);
+      v3 dir = lambertian_dir(normal, u[0], u[1]);
+      v3 p = v3make(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
+      bo_ray r2 = make_ray_od(p, dir, 0.001f, BO_FLT_MAX);
+      bo_hit h2 = trace_one(c->bvh, c->verts, &r2, view, c->mode, NULL, NULL);
+      bt = h2.t;
+      bp = h2.prim;
+    }
+    c->t1[i] = bt;
+    c->p1[i] = bp;
+  }
+}
+
+void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride, uint32_t width,
+                    uint32_t height, uint64_t seed, int mode, float* t0, uint32_t* p0, float* t1, uint32_t* p1,
+                    uint32_t n_threads) {
+  batch_ctx c = {bvh, verts, cams, cam_stride, width, height, seed, mode, t0, t1, p0, p1};
+  uint32_t n = bvh->n_segments * width * height;
+  bo_parallel_for(n, n_threads, 512, batch_range, &c);
+}

@@ -165,6 +165,11 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
                const float* camera20, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth,
                uint64_t seed, int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads);
 
+/* batched primary + one cosine bounce per pixel, segmented LBVH */
+void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride, uint32_t width,
+                    uint32_t height, uint64_t seed, int mode, float* t0, uint32_t* p0, float* t1, uint32_t* p1,
+                    uint32_t n_threads);
+
 #ifdef __cplusplus
 }
 #endif

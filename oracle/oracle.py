@@ -86,6 +86,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_cpu_build_lbvh": (_U32, [_P, _U32, _U32, _P, _P]),
         "bo_cpu_trace": (None, [_P, _P, _P, _P, _U32, _I, _P, _U32]),
         "bo_rt_philox4x32_10": (None, [_P, _P, _P]),
+        "bo_trace_batch": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _U32, _U32, ctypes.c_uint64, _I, _P, _P, _P,
+                                  _P, _U32]),
         "bo_rt_uniform4": (None, [ctypes.c_uint64, _U32, _U32, _P]),
         "bo_rt_sincos_turns": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
@@ -391,3 +393,14 @@ def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=
                     seed, algorithm, _ptr(pixels), None if samples is None else _ptr(samples), threads or n_threads())
     img = pixels.reshape(height, width, 3)
     return (img, samples.reshape(height, width, spp, 3)) if return_samples else img
+
+
+def trace_batch(bvh: OracleLbvh, cams, cam_stride, width, height, seed=7, tri_mode=TRI_WATERTIGHT, threads=None):
+    n = (bvh.seg_offsets.size - 1) * width * height
+    t0, t1 = np.zeros(n, np.float32), np.zeros(n, np.float32)
+    p0, p1 = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
+    c = np.ascontiguousarray(cams, np.float32)
+    s = bvh.struct()
+    lib().bo_trace_batch(ctypes.byref(s), _ptr(bvh.verts), _ptr(c), cam_stride, width, height, seed, tri_mode,
+                         _ptr(t0), _ptr(p0), _ptr(t1), _ptr(p1), threads or n_threads())
+    return t0, p0, t1, p1
