@@ -94,6 +94,13 @@ SIGNATURES = {
     "bajo_render_workspace_size": (_I32, [_P, ctypes.POINTER(_SZ)]),
     "bajo_render": (_I32, [_P, _P, _P, _P, _P, _P, _SZ, _P]),
     "bajo_render_stats": (_I32, [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "bajo_mlp_param_count": (_I32, [ctypes.POINTER(_U32)]),
+    "bajo_mlp_forward": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
+    "bajo_mlp_grad": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
+    "bajo_mlp_adam": (_I32, [_P, _P, _P, _P, _P, _U32, _F, _F, _F, _F, _F, _P]),
+    "bajo_guide_records_size": (_I32, [_U32, ctypes.POINTER(_SZ)]),
+    "bajo_render_guided": (_I32, [_P, _P, _P, _P, _P, _P, _P, _SZ, _P]),
+    "bajo_guide_train": (_I32, [_P, _P, _U32, _P, _U32, _U32, _F, _P]),
     "bajo_camera_make": (_I32, [_P, _P, _P, _F, _P]),
     "bajo_camera_from_vfov": (_I32, [_P, _P, _P, _F, _P]),
     "bajo_version": (ctypes.c_char_p, []),

@@ -1,0 +1,399 @@
+// mlp.cu -- kernels of the path-guiding network: batched forward, the
+// vMF-mixture negative-log-likelihood gradient (forward recompute +
+// backpropagation, weight gradients on the tensor cores), Adam, and the
+// training loop over the records the guided tracer writes.  The network, its
+// encoding and the mixture math live in mlp.cuh.  New on this path (the
+// reference has no guiding); the CPU FP64 oracle checks outputs and
+// gradients.
+#include <cmath>
+
+#include "mlp.cuh"
+
+namespace bajo {
+int sm_count();
+
+namespace mlp {
+
+constexpr int kWarps = 8, kThreads = 256, kRows = 16 * kWarps;  // 128 rows per CTA tile
+
+// feature rows of a tile: 5 encoding groups per row spread over the block;
+// rows past the end are zero.  Row j reads sample (offset + j) % count when
+// `wrap`, else sample j.
+__device__ void encode_tile(__half* x, const float* __restrict__ pos, const float* __restrict__ nrm,
+                            const float* box, uint64_t row_base, uint32_t rows, uint32_t offset, uint32_t count,
+                            bool wrap) {
+  for (int w = threadIdx.x; w < kRows * 5; w += kThreads) {
+    const int r = w / 5, grp = w % 5;
+    const uint64_t j = row_base + r;
+    __half* row = x + r * 64;
+    if (j < rows) {
+      const uint64_t i = wrap ? ((uint64_t)offset + j) % count : j;
+      const float p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+      const float q[3] = {nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]};
+      encode_group(grp, p, q, box, row);
+    } else {
+      const int col = grp < 3 ? grp * kPosBins : 3 * kPosBins + (grp - 3) * kDirBins;
+      const int bins = grp < 3 ? kPosBins : kDirBins;
+      for (int k = 0; k < bins; k += 2) st32(row + col + k, 0u);
+    }
+  }
+}
+
+struct FwdSmem {
+  Net net;
+  __half x[kRows * 64];
+  float out[kRows * kOutPad];
+};
+
+__global__ void __launch_bounds__(kThreads) forward_kernel(const __half* __restrict__ p16,
+                                                           const float* __restrict__ pos,
+                                                           const float* __restrict__ nrm, const float* box,
+                                                           uint32_t n, float* __restrict__ out20) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  FwdSmem& s = *reinterpret_cast<FwdSmem*>(raw);
+  load_net<kThreads>(s.net, p16);
+  const int warp = threadIdx.x >> 5;
+  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < n; base += (uint64_t)gridDim.x * kRows) {
+    __syncthreads();
+    encode_tile(s.x, pos, nrm, box, base, n, 0, n, false);
+    __syncthreads();
+    forward_rows(s.net, s.x, warp * 16, nullptr, s.out);
+    __syncthreads();
+    for (int k = threadIdx.x; k < kRows * kOut; k += kThreads) {
+      const int r = k / kOut, c = k % kOut;
+      if (base + r < n) out20[(base + r) * kOut + c] = s.out[r * kOutPad + c];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// gradient of sum_j -w_j log pdf_j(dir_j) over a batch of rows.
+// Persistent CTAs; each warp owns fixed 16x8 tiles of every weight gradient
+// and accumulates them in registers over all of the CTA's row tiles; bias
+// gradients in shared memory; one atomicAdd per element at the end.
+// Rows j < min(n_rows, count) read sample (offset + j) % count when a device
+// count is given (the training records; count = min(*d_count, count_cap)),
+// else sample j.
+// ---------------------------------------------------------------------------
+constexpr float kGradScale = 256.0f;  // keeps FP16 dL/dz away from underflow
+
+// dW[out][in] tile (16 out x 8 in) += dZ^T x A over the tile's 128 rows:
+// A operand (m = out, k = row) = dz[row][out]; B operand (k = row, n = in) =
+// act[row][in].
+__device__ __forceinline__ uint32_t pk2(__half lo, __half hi) {
+  __half2 h;
+  h.x = lo;
+  h.y = hi;
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ void dw_tile(const __half* dz, int dz_ld, int out0, const __half* act, int in0,
+                                        float c[4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll 2
+  for (int kt = 0; kt < kRows / 16; ++kt) {
+    const int r = 16 * kt + 2 * tq;
+    uint32_t a[4], b[2];
+    a[0] = pk2(dz[r * dz_ld + out0 + g], dz[(r + 1) * dz_ld + out0 + g]);
+    a[1] = pk2(dz[r * dz_ld + out0 + g + 8], dz[(r + 1) * dz_ld + out0 + g + 8]);
+    a[2] = pk2(dz[(r + 8) * dz_ld + out0 + g], dz[(r + 9) * dz_ld + out0 + g]);
+    a[3] = pk2(dz[(r + 8) * dz_ld + out0 + g + 8], dz[(r + 9) * dz_ld + out0 + g + 8]);
+    b[0] = pk2(act[r * 64 + in0 + g], act[(r + 1) * 64 + in0 + g]);
+    b[1] = pk2(act[(r + 8) * 64 + in0 + g], act[(r + 9) * 64 + in0 + g]);
+    mma16816(c, a, b);
+  }
+}
+
+struct TrainSmem {
+  Net net;
+  __half WT[3][kIn * kHid];    // transposes [in][out]
+  __half W4T[kHid * kOutPad];  // [in][out]
+  __half act[4][kRows * 64];   // X, A1, A2, A3 of the tile, row-major
+  __half dz[kRows * 64];       // dZ of the layer being reduced
+  __half g[kRows * kOutPad];   // scaled dL/dout
+  float out[kRows * kOutPad];  // outputs of the tile
+  float db[4][kHid];
+  float loss;
+};
+
+__global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restrict__ p16,
+                                                         const float* __restrict__ pos,
+                                                         const float* __restrict__ nrm,
+                                                         const float* __restrict__ dir,
+                                                         const float* __restrict__ weight, const float* box,
+                                                         uint32_t n_rows, uint32_t offset,
+                                                         const uint32_t* __restrict__ d_count, uint32_t count_cap,
+                                                         float* __restrict__ grad32, float* __restrict__ loss_out) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  TrainSmem& s = *reinterpret_cast<TrainSmem*>(raw);
+  load_net<kThreads>(s.net, p16);
+  for (int i = threadIdx.x; i < kHid * kIn; i += kThreads)
+    for (int l = 0; l < 3; ++l) s.WT[l][(i % kIn) * kHid + i / kIn] = p16[kOffW(l) + i];
+  for (int i = threadIdx.x; i < kOutPad * kHid; i += kThreads)
+    s.W4T[(i % kHid) * kOutPad + i / kHid] = p16[kOffW(3) + i];
+  for (int i = threadIdx.x; i < 4 * kHid; i += kThreads) (&s.db[0][0])[i] = 0.0f;
+  if (threadIdx.x == 0) s.loss = 0.0f;
+  const bool wrap = d_count != nullptr;
+  const uint32_t count = wrap ? min(*d_count, count_cap) : n_rows;
+  const uint32_t rows = wrap ? min(n_rows, count) : n_rows;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+  const int row0 = warp * 16;
+  __half* const keep[3] = {s.act[1], s.act[2], s.act[3]};
+  // weight-gradient tiles of this warp: hidden layers 64x64 = 4 x 8 tiles of
+  // 16x8 (out tile warp / 2, in tiles 4 * (warp % 2) + q); output layer
+  // 32x64 = 2 x 8 tiles (tile 2 * warp + t: out tile / 8, in tile % 8)
+  float dw[3][4][4] = {};
+  float dw4[2][4] = {};
+  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < rows; base += (uint64_t)gridDim.x * kRows) {
+    __syncthreads();
+    encode_tile(s.act[0], pos, nrm, box, base, rows, offset, count, wrap);
+    __syncthreads();
+    forward_rows(s.net, s.act[0], row0, keep, s.out);
+    __syncwarp();
+    // dL/dout of the warp's rows, lanes 0..15 one row each
+    if (lane < 16) {
+      const int r = row0 + lane;
+      const uint64_t j = base + r;
+      float gr[kOut];
+      float l = 0.0f;
+      if (j < rows) {
+        const uint64_t i = wrap ? ((uint64_t)offset + j) % count : j;
+        const float d[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+        l = mixture_nll_grad(&s.out[r * kOutPad], d, weight[i], gr);
+      } else {
+        for (int k = 0; k < kOut; ++k) gr[k] = 0.0f;
+      }
+      for (int k = 0; k < kOutPad; k += 2)
+        st32(&s.g[r * kOutPad + k], pack_h2_sat(k < kOut ? gr[k] * kGradScale : 0.0f,
+                                                 k + 1 < kOut ? gr[k + 1] * kGradScale : 0.0f));
+      if (l != 0.0f) atomicAdd(&s.loss, l);
+    }
+    __syncwarp();
+    uint32_t ga[2][4];  // G as A fragments (k = 32 outputs = 2 k-tiles)
+#pragma unroll
+    for (int kt = 0; kt < 2; ++kt) {
+      const int c = 16 * kt + 2 * tq;
+      ga[kt][0] = ld32(&s.g[(row0 + g) * kOutPad + c]);
+      ga[kt][1] = ld32(&s.g[(row0 + g + 8) * kOutPad + c]);
+      ga[kt][2] = ld32(&s.g[(row0 + g) * kOutPad + c + 8]);
+      ga[kt][3] = ld32(&s.g[(row0 + g + 8) * kOutPad + c + 8]);
+    }
+    __syncthreads();  // every warp's G and activations are in shared memory
+    for (int t2 = 0; t2 < 2; ++t2) {
+      const int tile = warp * 2 + t2;
+      dw_tile(s.g, kOutPad, 16 * (tile / 8), s.act[3], 8 * (tile % 8), dw4[t2]);
+    }
+    if (threadIdx.x < kOutPad) {
+      float acc = 0.0f;
+      for (int r = 0; r < kRows; ++r) acc += __half2float(s.g[r * kOutPad + threadIdx.x]);
+      s.db[3][threadIdx.x] += acc;
+    }
+    // dA3 = G x W4: B operand (k = out, n = in) = W4T[in][out]
+    float acc[8][4];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll
+      for (int kt = 0; kt < 2; ++kt) {
+        uint32_t b[2];
+        const __half* w = s.W4T + (8 * j + g) * kOutPad + 16 * kt + 2 * tq;
+        b[0] = ld32(w);
+        b[1] = ld32(w + 8);
+        mma16816(acc[j], ga[kt], b);
+      }
+    }
+    for (int l = 2; l >= 0; --l) {
+      __syncthreads();  // the previous layer's readers of s.dz are done
+      // dZ_l = dA_{l+1} * (A_{l+1} > 0), row-major for the weight gradient
+      const __half* A = s.act[l + 1];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int c = 8 * j + 2 * tq;
+        const __half2 lo = *reinterpret_cast<const __half2*>(&A[(row0 + g) * 64 + c]);
+        const __half2 hi = *reinterpret_cast<const __half2*>(&A[(row0 + g + 8) * 64 + c]);
+        if (!(__low2float(lo) > 0.0f)) acc[j][0] = 0.0f;
+        if (!(__high2float(lo) > 0.0f)) acc[j][1] = 0.0f;
+        if (!(__low2float(hi) > 0.0f)) acc[j][2] = 0.0f;
+        if (!(__high2float(hi) > 0.0f)) acc[j][3] = 0.0f;
+        st32(&s.dz[(row0 + g) * 64 + c], pack_h2_sat(acc[j][0], acc[j][1]));
+        st32(&s.dz[(row0 + g + 8) * 64 + c], pack_h2_sat(acc[j][2], acc[j][3]));
+      }
+      __syncthreads();
+      for (int qd = 0; qd < 4; ++qd)
+        dw_tile(s.dz, 64, 16 * (warp / 2), s.act[l], 8 * (4 * (warp % 2) + qd), dw[l][qd]);
+      if (threadIdx.x < kHid) {
+        float sacc = 0.0f;
+        for (int r = 0; r < kRows; ++r) sacc += __half2float(s.dz[r * 64 + threadIdx.x]);
+        s.db[l][threadIdx.x] += sacc;
+      }
+      if (l == 0) break;
+      // dA_l = dZ_l x W_l: A = the warp's dZ_l rows, B (k = out, n = in) = WT[in][out]
+      uint32_t a[4][4];
+      load_afrag64(s.dz, row0, a);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.0f;
+#pragma unroll
+        for (int kt = 0; kt < 4; ++kt) {
+          uint32_t b[2];
+          const __half* w = s.WT[l] + (8 * j + g) * kHid + 16 * kt + 2 * tq;
+          b[0] = ld32(w);
+          b[1] = ld32(w + 8);
+          mma16816(acc[j], a[kt], b);
+        }
+      }
+    }
+  }
+  __syncthreads();
+  // flush the weight-gradient tiles (C fragments) and biases, unscaled
+  const float inv = 1.0f / kGradScale;
+  for (int l = 0; l < 3; ++l)
+    for (int qd = 0; qd < 4; ++qd) {
+      const int out0 = 16 * (warp / 2), in0 = 8 * (4 * (warp % 2) + qd);
+      float* G = grad32 + kOffW(l);
+      atomicAdd(&G[(out0 + g) * kIn + in0 + 2 * tq], dw[l][qd][0] * inv);
+      atomicAdd(&G[(out0 + g) * kIn + in0 + 2 * tq + 1], dw[l][qd][1] * inv);
+      atomicAdd(&G[(out0 + g + 8) * kIn + in0 + 2 * tq], dw[l][qd][2] * inv);
+      atomicAdd(&G[(out0 + g + 8) * kIn + in0 + 2 * tq + 1], dw[l][qd][3] * inv);
+    }
+  for (int t2 = 0; t2 < 2; ++t2) {
+    const int tile = warp * 2 + t2, out0 = 16 * (tile / 8), in0 = 8 * (tile % 8);
+    float* G = grad32 + kOffW(3);
+    atomicAdd(&G[(out0 + g) * kHid + in0 + 2 * tq], dw4[t2][0] * inv);
+    atomicAdd(&G[(out0 + g) * kHid + in0 + 2 * tq + 1], dw4[t2][1] * inv);
+    atomicAdd(&G[(out0 + g + 8) * kHid + in0 + 2 * tq], dw4[t2][2] * inv);
+    atomicAdd(&G[(out0 + g + 8) * kHid + in0 + 2 * tq + 1], dw4[t2][3] * inv);
+  }
+  for (int i = threadIdx.x; i < kHid; i += kThreads)
+    for (int l = 0; l < 3; ++l) atomicAdd(&grad32[kOffB(l) + i], s.db[l][i] * inv);
+  for (int i = threadIdx.x; i < kOutPad; i += kThreads) atomicAdd(&grad32[kOffB(3) + i], s.db[3][i] * inv);
+  if (threadIdx.x == 0 && loss_out) atomicAdd(loss_out, s.loss);
+}
+
+// Adam (Kingma & Ba 2015) on the FP32 master weights; FP16 copies refreshed.
+// grad_scale multiplies the raw gradient; the padded rows of the output layer
+// stay zero.
+__global__ void adam_kernel(float* __restrict__ p32, __half* __restrict__ p16, const float* __restrict__ grad,
+                            float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
+                            float bc1, float bc2, float grad_scale) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= kParams) return;
+  const bool pad_w = i >= kOffW(3) && i < kOffB(3) && (i - kOffW(3)) / kHid >= kOut;
+  const bool pad_b = i >= kOffB(3) && i - kOffB(3) >= kOut;
+  if (pad_w || pad_b) {
+    p32[i] = 0.0f;
+    p16[i] = __float2half(0.0f);
+    return;
+  }
+  const float gr = grad[i] * grad_scale;
+  const float mi = b1 * m[i] + (1.0f - b1) * gr;
+  const float vi = b2 * v[i] + (1.0f - b2) * gr * gr;
+  m[i] = mi;
+  v[i] = vi;
+  const float w = p32[i] - lr * (mi / bc1) / (sqrtf(vi / bc2) + eps);
+  p32[i] = w;
+  p16[i] = __float2half(w);
+}
+
+uint32_t grid_for(uint64_t rows) {
+  uint64_t grid = (rows + kRows - 1) / kRows;
+  const uint64_t cap = (uint64_t)sm_count();
+  if (grid > cap) grid = cap;
+  return grid ? (uint32_t)grid : 1u;
+}
+
+cudaError_t launch_grad(const __half* p16, const float* pos, const float* nrm, const float* dir, const float* w,
+                        const float* box, uint32_t n, uint32_t offset, const uint32_t* d_count, uint32_t count_cap,
+                        float* grad, float* loss, cudaStream_t st) {
+  static_assert(sizeof(TrainSmem) <= 227 * 1024, "training tile exceeds shared memory");
+  const size_t smem = sizeof(TrainSmem);
+  cudaError_t e = cudaFuncSetAttribute(train_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st)) != cudaSuccess) return e;
+  if (loss && (e = cudaMemsetAsync(loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+  if (n == 0) return cudaSuccess;
+  train_kernel<<<grid_for(n), kThreads, smem, st>>>(p16, pos, nrm, dir, w, box, n, offset, d_count, count_cap, grad,
+                                                    loss);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adam(float* p32, __half* p16, const float* grad, float* m, float* v, uint32_t step, float lr,
+                        float b1, float b2, float eps, float grad_scale, cudaStream_t st) {
+  const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(p32, p16, grad, m, v, lr, b1, b2, eps, bc1, bc2, grad_scale);
+  return cudaGetLastError();
+}
+
+}  // namespace mlp
+}  // namespace bajo
+
+extern "C" {
+
+int32_t bajo_mlp_param_count(uint32_t* count) {
+  if (!count) return BAJO_ERR_INVALID_ARGUMENT;
+  *count = bajo::mlp::kParams;
+  return BAJO_OK;
+}
+
+int32_t bajo_mlp_forward(const void* d_params16, const float* d_pos, const float* d_nrm, uint32_t n,
+                         const float* d_box6, float* d_out20, void* stream) {
+  using namespace bajo::mlp;
+  if (!d_params16 || !d_box6 || (n && (!d_pos || !d_nrm || !d_out20))) return BAJO_ERR_INVALID_ARGUMENT;
+  if (n == 0) return BAJO_OK;
+  const size_t smem = sizeof(FwdSmem);
+  if (cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    return BAJO_ERR_CUDA;
+  forward_kernel<<<grid_for(n), kThreads, smem, (cudaStream_t)stream>>>((const __half*)d_params16, d_pos, d_nrm,
+                                                                         d_box6, n, d_out20);
+  return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_mlp_grad(const void* d_params16, const float* d_pos, const float* d_nrm, const float* d_dir,
+                      const float* d_weight, uint32_t n, const float* d_box6, float* d_grad32, float* d_loss,
+                      void* stream) {
+  using namespace bajo::mlp;
+  if (!d_params16 || !d_box6 || !d_grad32 || (n && (!d_pos || !d_nrm || !d_dir || !d_weight)))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  const cudaError_t e = launch_grad((const __half*)d_params16, d_pos, d_nrm, d_dir, d_weight, d_box6, n, 0, nullptr,
+                                    0, d_grad32, d_loss, (cudaStream_t)stream);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_mlp_adam(float* d_params32, void* d_params16, const float* d_grad32, float* d_m, float* d_v,
+                      uint32_t step, float lr, float beta1, float beta2, float eps, float grad_scale, void* stream) {
+  if (!d_params32 || !d_params16 || !d_grad32 || !d_m || !d_v || step == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  const cudaError_t e = bajo::mlp::launch_adam(d_params32, (__half*)d_params16, d_grad32, d_m, d_v, step, lr, beta1,
+                                               beta2, eps, grad_scale, (cudaStream_t)stream);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_guide_records_size(uint32_t capacity, size_t* bytes) {
+  if (!bytes) return BAJO_ERR_INVALID_ARGUMENT;
+  *bytes = bajo::mlp::record_layout(capacity).total;
+  return BAJO_OK;
+}
+
+int32_t bajo_guide_train(BajoGuideNet* net, const void* d_records, uint32_t record_capacity, const float* d_box6,
+                         uint32_t batch, uint32_t steps, float lr, void* stream) {
+  using namespace bajo::mlp;
+  if (!net || !net->params32 || !net->params16 || !net->adam_m || !net->adam_v || !net->grad || !d_records ||
+      !d_box6 || record_capacity == 0 || batch == 0)
+    return BAJO_ERR_INVALID_ARGUMENT;
+  const RecordLayout L = record_layout(record_capacity);
+  const unsigned char* r = (const unsigned char*)d_records;
+  cudaStream_t st = (cudaStream_t)stream;
+  for (uint32_t s = 0; s < steps; ++s) {
+    const uint32_t offset = (uint32_t)((uint64_t)net->step * batch % 0xFFFFFFFFull);
+    cudaError_t e = launch_grad((const __half*)net->params16, (const float*)(r + L.pos), (const float*)(r + L.nrm),
+                                (const float*)(r + L.dir), (const float*)(r + L.weight), d_box6, batch, offset,
+                                (const uint32_t*)r, record_capacity, net->grad, net->loss, st);
+    if (e != cudaSuccess) return BAJO_ERR_CUDA;
+    net->step += 1;
+    e = launch_adam(net->params32, (__half*)net->params16, net->grad, net->adam_m, net->adam_v, net->step, lr, 0.9f,
+                    0.999f, 1e-8f, 1.0f / (float)batch, st);
+    if (e != cudaSuccess) return BAJO_ERR_CUDA;
+  }
+  return BAJO_OK;
+}
+
+}  // extern "C"

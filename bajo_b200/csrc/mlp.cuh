@@ -1,0 +1,328 @@
+// mlp.cuh -- device pieces of the path-guiding network shared by the MLP
+// kernels (mlp.cu) and the guided wavefront shading kernel (rt.cu).
+//
+// Network: features (64) = one-blob(position, 3 x 16 bins) ++ one-blob(normal,
+// octahedral coordinates, 2 x 8 bins); three hidden layers of 64 with ReLU;
+// output 20 = 4 lobes x (mean xyz, log kappa, weight logit).
+// Parameter layout (floats / halves): W1[64x64] b1[64] W2 b2 W3 b3 W4[32x64]
+// b4[32] (rows 20..31 of W4 and b4 are zero), weights row-major [out][in].
+//
+// Dense layers run on the tensor cores with mma.sync m16n8k16 (f16 inputs,
+// f32 accumulation).  Fragment layouts (PTX ISA), g = lane / 4, t = lane % 4:
+//   A (16x16): a0a1 = (g, 2t..2t+1), a2a3 = (g+8, 2t..), a4a5 = (g, 2t+8..),
+//              a6a7 = (g+8, 2t+8..)
+//   B (16x8):  b0b1 = (k 2t..2t+1, n g), b2b3 = (k 2t+8.., n g)
+//   C (16x8):  c0c1 = (g, 2t..2t+1), c2c3 = (g+8, 2t..2t+1)
+// The C fragments of n-tiles 2j and 2j+1 are exactly the A fragment of k-tile
+// j, so a layer's output feeds the next layer without leaving registers.
+#pragma once
+
+#include <cuda_fp16.h>
+
+#include "bajo_common.cuh"
+
+namespace bajo {
+namespace mlp {
+
+constexpr int kIn = 64, kHid = 64, kOut = 20, kOutPad = 32, kLobes = 4;
+constexpr int kLayerSize = kHid * kIn + kHid;  // 4160
+__host__ __device__ constexpr int kOffW(int l) { return l * kLayerSize; }
+__host__ __device__ constexpr int kOffB(int l) {
+  return l < 3 ? l * kLayerSize + kHid * kIn : 3 * kLayerSize + kOutPad * kHid;
+}
+constexpr int kParams = 3 * kLayerSize + kOutPad * kHid + kOutPad;  // 14560
+constexpr int kPosBins = 16, kDirBins = 8;
+constexpr float kPi = 3.14159265358979323846f;
+constexpr float kLogKappaMin = -2.0f, kLogKappaMax = 8.0f;
+
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const uint32_t b[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+__device__ __forceinline__ uint32_t pack_h2(float lo, float hi) {
+  __half2 h = __floats2half2_rn(lo, hi);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+// saturating pack for gradients: FP16 overflows at 65504
+__device__ __forceinline__ uint32_t pack_h2_sat(float lo, float hi) {
+  const float m = 65000.0f;
+  return pack_h2(fminf(fmaxf(lo, -m), m), fminf(fmaxf(hi, -m), m));
+}
+__device__ __forceinline__ uint32_t ld32(const __half* p) { return *reinterpret_cast<const uint32_t*>(p); }
+__device__ __forceinline__ void st32(__half* p, uint32_t v) { *reinterpret_cast<uint32_t*>(p) = v; }
+
+// ---------------------------------------------------------------------------
+// encoding
+// ---------------------------------------------------------------------------
+// One-blob encoding (Mueller et al., "Neural Importance Sampling", 2019) with a
+// hat kernel one bin wide: v in [0, 1] lands on the two nearest bin centres
+// with linear weights; bin value k of the blob.
+__device__ __forceinline__ void blob_bins(float v, int bins, int& i0, int& i1, float& f) {
+  v = fminf(fmaxf(v, 0.0f), 1.0f);
+  const float s = v * (float)bins - 0.5f;
+  const float fl = floorf(s);
+  f = s - fl;
+  i0 = max((int)fl, 0);
+  i1 = min((int)fl + 1, bins - 1);
+}
+__device__ __forceinline__ float blob_value(int k, int i0, int i1, float f) {
+  return (k == i0 ? 1.0f - f : 0.0f) + (k == i1 ? f : 0.0f);
+}
+
+// octahedral coordinates of a unit normal in [0, 1]^2 (no transcendentals)
+__device__ __forceinline__ void octahedral(float nx, float ny, float nz, float& u, float& v) {
+  const float l1 = fabsf(nx) + fabsf(ny) + fabsf(nz);
+  float x = l1 > 0.0f ? nx / l1 : 0.0f, y = l1 > 0.0f ? ny / l1 : 0.0f;
+  if (nz < 0.0f) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    x = (1.0f - ay) * (x >= 0.0f ? 1.0f : -1.0f);
+    y = (1.0f - ax) * (y >= 0.0f ? 1.0f : -1.0f);
+  }
+  u = x * 0.5f + 0.5f;
+  v = y * 0.5f + 0.5f;
+}
+
+// Encoding group `grp` (0..2 position axes, 3..4 normal coordinates) of one
+// sample, written as half pairs into its 64-feature row.
+__device__ __forceinline__ void encode_group(int grp, const float* p, const float* n, const float* box,
+                                             __half* row) {
+  float v;
+  int bins, col;
+  if (grp < 3) {
+    const float ext = box[3 + grp] - box[grp];
+    v = ext > 0.0f ? (p[grp] - box[grp]) / ext : 0.5f;
+    bins = kPosBins;
+    col = grp * kPosBins;
+  } else {
+    float u, w;
+    octahedral(n[0], n[1], n[2], u, w);
+    v = grp == 3 ? u : w;
+    bins = kDirBins;
+    col = 3 * kPosBins + (grp - 3) * kDirBins;
+  }
+  int i0, i1;
+  float f;
+  blob_bins(v, bins, i0, i1, f);
+  for (int k = 0; k < bins; k += 2) st32(row + col + k, pack_h2(blob_value(k, i0, i1, f), blob_value(k + 1, i0, i1, f)));
+}
+
+// ---------------------------------------------------------------------------
+// network in shared memory and the per-warp forward pass
+// ---------------------------------------------------------------------------
+struct Net {
+  __half W[3][kHid * kIn];    // hidden layers, [out][in]
+  __half W4[kOutPad * kHid];  // output layer, [out][in]
+  float B[3][kHid];
+  float B4[kOutPad];
+};
+
+template <int THREADS>
+__device__ void load_net(Net& s, const __half* __restrict__ p16) {
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(p16);
+  for (int i = threadIdx.x; i < kHid * kIn / 2; i += THREADS)
+    for (int l = 0; l < 3; ++l) reinterpret_cast<uint32_t*>(s.W[l])[i] = src[kOffW(l) / 2 + i];
+  for (int i = threadIdx.x; i < kOutPad * kHid / 2; i += THREADS)
+    reinterpret_cast<uint32_t*>(s.W4)[i] = src[kOffW(3) / 2 + i];
+  for (int i = threadIdx.x; i < kHid; i += THREADS)
+    for (int l = 0; l < 3; ++l) s.B[l][i] = __half2float(p16[kOffB(l) + i]);
+  for (int i = threadIdx.x; i < kOutPad; i += THREADS) s.B4[i] = __half2float(p16[kOffB(3) + i]);
+}
+
+// A fragments (4 k-tiles of 16) of 16 rows starting at row0 of a row-major
+// [rows x 64] half tile
+__device__ __forceinline__ void load_afrag64(const __half* t, int row0, uint32_t a[4][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    const int c = 16 * kt + 2 * tq;
+    a[kt][0] = ld32(t + (row0 + g) * 64 + c);
+    a[kt][1] = ld32(t + (row0 + g + 8) * 64 + c);
+    a[kt][2] = ld32(t + (row0 + g) * 64 + c + 8);
+    a[kt][3] = ld32(t + (row0 + g + 8) * 64 + c + 8);
+  }
+}
+
+__device__ __forceinline__ void store_afrag64(__half* t, int row0, const uint32_t a[4][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    const int c = 16 * kt + 2 * tq;
+    st32(t + (row0 + g) * 64 + c, a[kt][0]);
+    st32(t + (row0 + g + 8) * 64 + c, a[kt][1]);
+    st32(t + (row0 + g) * 64 + c + 8, a[kt][2]);
+    st32(t + (row0 + g + 8) * 64 + c + 8, a[kt][3]);
+  }
+}
+
+// one dense layer on 16 rows: acc[n-tile] = A x W^T + b, W [out][in]
+template <int NT, int KT>
+__device__ __forceinline__ void dense(const uint32_t a[][4], const __half* W, int in_dim, const float* bias,
+                                      float acc[][4]) {
+  const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int j = 0; j < NT; ++j) {
+    const float b0 = bias[8 * j + 2 * tq], b1 = bias[8 * j + 2 * tq + 1];
+    acc[j][0] = b0;
+    acc[j][1] = b1;
+    acc[j][2] = b0;
+    acc[j][3] = b1;
+#pragma unroll
+    for (int kt = 0; kt < KT; ++kt) {
+      uint32_t b[2];
+      const __half* w = W + (8 * j + g) * in_dim + 16 * kt + 2 * tq;
+      b[0] = ld32(w);
+      b[1] = ld32(w + 8);
+      mma16816(acc[j], a[kt], b);
+    }
+  }
+}
+
+// ReLU on the C fragments of 8 n-tiles, repacked as the 4 A k-tiles
+__device__ __forceinline__ void relu_to_afrag(const float acc[8][4], uint32_t a[4][4]) {
+#pragma unroll
+  for (int kt = 0; kt < 4; ++kt) {
+    const float* lo = acc[2 * kt];
+    const float* hi = acc[2 * kt + 1];
+    a[kt][0] = pack_h2(fmaxf(lo[0], 0.0f), fmaxf(lo[1], 0.0f));
+    a[kt][1] = pack_h2(fmaxf(lo[2], 0.0f), fmaxf(lo[3], 0.0f));
+    a[kt][2] = pack_h2(fmaxf(hi[0], 0.0f), fmaxf(hi[1], 0.0f));
+    a[kt][3] = pack_h2(fmaxf(hi[2], 0.0f), fmaxf(hi[3], 0.0f));
+  }
+}
+
+// Forward of the warp's 16 rows (row0..row0+15) of the feature tile `x`;
+// hidden activations go to keep[0..2] when keep is non-null; the 32 padded
+// outputs to out[row * 32 + c].
+__device__ __forceinline__ void forward_rows(const Net& s, const __half* x, int row0, __half* const* keep,
+                                             float* out) {
+  uint32_t a[4][4];
+  float acc[8][4];
+  load_afrag64(x, row0, a);
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    dense<8, 4>(a, s.W[l], kIn, s.B[l], acc);
+    relu_to_afrag(acc, a);
+    if (keep) store_afrag64(keep[l], row0, a);
+  }
+  float o[4][4];
+  dense<4, 4>(a, s.W4, kHid, s.B4, o);
+  const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    const int c = 8 * j + 2 * tq;
+    *reinterpret_cast<float2*>(&out[(row0 + g) * kOutPad + c]) = make_float2(o[j][0], o[j][1]);
+    *reinterpret_cast<float2*>(&out[(row0 + g + 8) * kOutPad + c]) = make_float2(o[j][2], o[j][3]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// vMF mixture: mean = m / len, len = sqrt(|m|^2 + 1e-12) (so d mean / dm =
+// (I - mean mean^T) / len exactly), kappa = exp(clamp(s, -2, 8)),
+// weights = softmax(logits);
+// pdf(w) = sum_k pi_k kappa_k / (2 pi (1 - e^-2kappa)) exp(kappa (mu.w - 1)).
+// ---------------------------------------------------------------------------
+struct Mixture {
+  float pi[kLobes], mu[kLobes][3], kap[kLobes], norm[kLobes], len[kLobes];
+};
+
+__device__ __forceinline__ void mixture_from_outputs(const float* o, Mixture& m) {
+  float mx = -FLT_MAX;
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) mx = fmaxf(mx, o[5 * k + 4]);
+  float z = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    m.pi[k] = expf(o[5 * k + 4] - mx);
+    z += m.pi[k];
+  }
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    m.pi[k] /= z;
+    const float x = o[5 * k], y = o[5 * k + 1], w = o[5 * k + 2];
+    m.len[k] = sqrtf(x * x + y * y + w * w + 1e-12f);
+    m.mu[k][0] = x / m.len[k];
+    m.mu[k][1] = y / m.len[k];
+    m.mu[k][2] = w / m.len[k];
+    m.kap[k] = expf(fminf(fmaxf(o[5 * k + 3], kLogKappaMin), kLogKappaMax));
+    m.norm[k] = m.kap[k] / (2.0f * kPi * (-expm1f(-2.0f * m.kap[k])));
+  }
+}
+
+__device__ __forceinline__ float mixture_pdf(const Mixture& m, const float* d) {
+  float q = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    const float c = m.mu[k][0] * d[0] + m.mu[k][1] * d[1] + m.mu[k][2] * d[2];
+    q += m.pi[k] * m.norm[k] * expf(m.kap[k] * (c - 1.0f));
+  }
+  return q;
+}
+
+// Loss -weight * log pdf(dir) of one sample and its gradient w.r.t. the 20
+// raw outputs.
+__device__ __forceinline__ float mixture_nll_grad(const float* o, const float* dir, float weight, float* grad) {
+  Mixture m;
+  mixture_from_outputs(o, m);
+  float v[kLobes], c[kLobes];
+  float q = 0.0f;
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    c[k] = m.mu[k][0] * dir[0] + m.mu[k][1] * dir[1] + m.mu[k][2] * dir[2];
+    v[k] = m.norm[k] * expf(m.kap[k] * (c[k] - 1.0f));
+    q += m.pi[k] * v[k];
+  }
+  q = fmaxf(q, 1e-30f);
+#pragma unroll
+  for (int k = 0; k < kLobes; ++k) {
+    const float r = m.pi[k] * v[k] / q;
+    grad[5 * k + 4] = weight * (m.pi[k] - r);
+    const float kap = m.kap[k];
+    const float dlogv_ds = 1.0f - 2.0f * kap * expf(-2.0f * kap) / (-expm1f(-2.0f * kap)) + kap * (c[k] - 1.0f);
+    const bool clamped = o[5 * k + 3] < kLogKappaMin || o[5 * k + 3] > kLogKappaMax;
+    grad[5 * k + 3] = clamped ? 0.0f : -weight * r * dlogv_ds;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) grad[5 * k + a] = -weight * r * kap * (dir[a] - m.mu[k][a] * c[k]) / m.len[k];
+  }
+  return -weight * logf(q);
+}
+
+// ---------------------------------------------------------------------------
+// training-record buffer written by the guided tracer: 256-byte header (u32
+// count, u32 first record of the current chunk), then arrays on 256-byte
+// boundaries
+// ---------------------------------------------------------------------------
+struct RecordLayout {
+  size_t pos, nrm, dir, weight, sidx, tn, snap, wpre, total;
+};
+
+inline RecordLayout record_layout(uint32_t cap) {
+  auto a256 = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  RecordLayout L;
+  size_t o = 256;
+  const size_t c = cap;
+  L.pos = o;
+  o = a256(o + 12 * c);
+  L.nrm = o;
+  o = a256(o + 12 * c);
+  L.dir = o;
+  o = a256(o + 12 * c);
+  L.weight = o;
+  o = a256(o + 4 * c);
+  L.sidx = o;
+  o = a256(o + 4 * c);
+  L.tn = o;
+  o = a256(o + 12 * c);
+  L.snap = o;
+  o = a256(o + 12 * c);
+  L.wpre = o;
+  o = a256(o + 4 * c);
+  L.total = o;
+  return L;
+}
+
+}  // namespace mlp
+}  // namespace bajo

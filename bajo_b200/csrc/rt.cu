@@ -23,6 +23,7 @@
 #include <cstring>
 #include <vector>
 
+#include "mlp.cuh"
 #include "sampling.cuh"
 #include "traverse.cuh"
 
@@ -46,6 +47,7 @@ constexpr int kShadowPlanes = 11;               // WaveShadowFloatAbi.PLANES
 constexpr uint32_t kIndexMask28 = 0x0FFFFFFFu;  // SURFACE_INDEX_MASK
 constexpr float kInvPi = 0.3183098861837907f;   // BSDF_INV_PI, bajo/rt/shading.mojo:9
 constexpr int kBlock = 128;
+constexpr uint32_t kNoRecord = 0xFFFFFFFFu;
 
 __device__ __forceinline__ float length2(f3 v) { return dot(v, v); }
 __device__ __forceinline__ f3 neg(f3 v) { return mk(-v.x, -v.y, -v.z); }
@@ -74,6 +76,7 @@ struct Queues {
   uint32_t* counters;  // [2b] = paths active at bounce b, [2b+1] = shadow rays of bounce b
   uint32_t* status;
   uint32_t capacity;
+  uint32_t* rec[2];    // guided only: training-record index per path-queue slot (else null)
 };
 
 struct SceneView {
@@ -143,6 +146,7 @@ __global__ void __launch_bounds__(kBlock) primary_kernel(const float* __restrict
   q.radiance[0 * cap + idx] = 0.0f;
   q.radiance[1 * cap + idx] = 0.0f;
   q.radiance[2 * cap + idx] = 0.0f;
+  if (q.rec[0]) q.rec[0][idx] = kNoRecord;
 }
 
 __device__ __forceinline__ void accumulate(const Queues& q, uint32_t sidx, f3 v) {
@@ -401,13 +405,382 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const float* __restrict
 }
 
 // ---------------------------------------------------------------------------
+// guided tracing (BAJO_RENDER_GUIDED): MIS tracing whose continuation comes
+// from one-sample MIS between the cosine BSDF and the network's vMF mixture.
+// Per bounce: guided_trace_kernel (closest hit, sky, MIS-weighted emission,
+// Lambertian vertices -> vertex queue), guided_shade_kernel (network on the
+// tensor cores over 128-vertex tiles, then NEE + continuation per vertex),
+// shadow_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kVtxPlanes = 12;  // p xyz, oriented normal xyz, albedo rgb, throughput rgb
+constexpr int kShadeThreads = 256, kShadeRows = 128;
+
+struct GuideCtx {
+  const __half* params16;
+  const float* box;
+  float frac;           // probability of sampling the mixture
+  float rec_frac;       // probability a continued vertex becomes a training record
+  uint32_t rec_cap;
+  uint32_t* rec_hdr;    // [0] = records appended, [1] = first record of the chunk
+  float* rec_pos;
+  float* rec_nrm;
+  float* rec_dir;
+  float* rec_weight;
+  uint32_t* rec_sidx;
+  float* rec_tn;
+  float* rec_snap;
+  float* rec_wpre;
+  uint32_t* vtx_ids;
+  float* vtx;
+  uint32_t* vcount;     // [b] = Lambertian vertices of bounce b
+};
+
+// integer hash "lowbias32" (C. Wellons, hash-prospector): record selection
+__device__ __forceinline__ uint32_t lowbias32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// vMF direction around unit mean mu (Jakob, "Numerically stable sampling of
+// the von Mises-Fisher distribution on S^2", 2012): cos theta = 1 +
+// log(u + (1 - u) e^-2kappa) / kappa, azimuth 2 pi v, in the orthonormal
+// basis of Duff et al. (JCGT 2017).
+__device__ __forceinline__ f3 vmf_sample(const float* mu, float kappa, float u, float v) {
+  float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * kappa)) / kappa;
+  w = fminf(fmaxf(w, -1.0f), 1.0f);
+  const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  float sp, cp;
+  sincos_turns(v, sp, cp);
+  const float x = mu[0], y = mu[1], z = mu[2];
+  const float sgn = z >= 0.0f ? 1.0f : -1.0f;
+  const float a = -1.0f / (sgn + z);
+  const float b = x * y * a;
+  const f3 t1 = mk(1.0f + sgn * x * x * a, sgn * b, -sgn * x);
+  const f3 t2 = mk(b, sgn + y * y * a, -y);
+  const f3 d = (t1 * (st * cp) + t2 * (st * sp)) + mk(x, y, z) * w;
+  return normalize(d);
+}
+
+__global__ void __launch_bounds__(kBlock) guided_trace_kernel(SceneView sc, Queues q, GuideCtx gc, uint32_t bounce,
+                                                              uint32_t sample_base) {
+  const uint32_t count = q.counters[2 * bounce];
+  const uint32_t cap = q.capacity;
+  const uint32_t* src_ids = q.ids[bounce & 1];
+  const float* src = q.fields[bounce & 1];
+  const uint32_t* src_rec = q.rec[bounce & 1];
+  const uint32_t stride = gridDim.x * kBlock;
+  for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
+    const uint32_t idx = base + threadIdx.x;
+    bool want_vtx = false;
+    uint32_t path_id = 0;
+    f3 vp, vn, va, vt;
+    if (idx < count) {
+      const uint32_t idw = src_ids[idx];
+      path_id = idw & kIdMask;
+      const bool delta = (idw & kDeltaBit) != 0;
+      const f3 o = mk(src[0 * cap + idx], src[1 * cap + idx], src[2 * cap + idx]);
+      const float tmin = src[3 * cap + idx];
+      const f3 d = mk(src[4 * cap + idx], src[5 * cap + idx], src[6 * cap + idx]);
+      const float tmax = src[7 * cap + idx];
+      const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
+      const float prev_pdf = src[11 * cap + idx];
+      const uint32_t sidx = path_id - sample_base;
+      const uint32_t rec = src_rec[idx];
+      if (rec != kNoRecord) {  // radiance gathered before this ray: the record's baseline
+        gc.rec_snap[3 * (size_t)rec + 0] = q.radiance[0 * cap + sidx];
+        gc.rec_snap[3 * (size_t)rec + 1] = q.radiance[1 * cap + sidx];
+        gc.rec_snap[3 * (size_t)rec + 2] = q.radiance[2 * cap + sidx];
+      }
+      const Ray r = trav::make_ray(o, d, tmin, tmax);
+      const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
+                                                          q.status);
+      if (h.leaf == kEmpty) {
+        accumulate(q, sidx, mul(T, sky(d)));
+      } else {
+        const float t = h.t;
+        const float4 a = __ldg(sc.tris + (size_t)h.leaf * 3 + 0);
+        const float4 b = __ldg(sc.tris + (size_t)h.leaf * 3 + 1);
+        const float4 c = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
+        const f3 v0 = mk(a.x, a.y, a.z);
+        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(c.x, c.y, c.z) - v0));
+        const bool front = dot(d, outward) < 0.0f;
+        const f3 normal = front ? outward : neg(outward);
+        const uint32_t surface = __ldg(sc.surfaces + h.prim);
+        const uint32_t kind = surface >> 28, midx = surface & kIndexMask28;
+        const f3 p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+        if (kind == BAJO_MAT_EMISSIVE) {
+          if (front) {
+            const f3 L = mk(sc.emissives[3 * midx], sc.emissives[3 * midx + 1], sc.emissives[3 * midx + 2]);
+            float wgt = 1.0f;
+            if (bounce > 0 && !delta) {
+              const float lc = fmaxf(dot(normal, neg(normalize(d))), 0.0f);
+              float lpdf = 0.0f;
+              if (lc > 0.0f && sc.total_light_weight > 0.0f) {
+                const float d2 = (t * t) * length2(d);
+                lpdf = (d2 * ((L.x + L.y) + L.z)) / ((3.0f * lc) * sc.total_light_weight);
+              }
+              wgt = power_heuristic(prev_pdf, lpdf);
+            }
+            const f3 TL = mul(T, L);
+            accumulate(q, sidx, mk(TL.x * wgt, TL.y * wgt, TL.z * wgt));
+          }
+        } else if (kind == BAJO_MAT_LAMBERTIAN) {
+          want_vtx = true;
+          vp = p;
+          vn = normal;
+          va = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
+          vt = T;
+        }
+      }
+    }
+    const uint32_t slot = warp_append(&gc.vcount[bounce], want_vtx);
+    if (want_vtx) {
+      if (slot < cap) {
+        gc.vtx_ids[slot] = path_id;
+        float* f = gc.vtx;
+        f[0 * cap + slot] = vp.x; f[1 * cap + slot] = vp.y; f[2 * cap + slot] = vp.z;
+        f[3 * cap + slot] = vn.x; f[4 * cap + slot] = vn.y; f[5 * cap + slot] = vn.z;
+        f[6 * cap + slot] = va.x; f[7 * cap + slot] = va.y; f[8 * cap + slot] = va.z;
+        f[9 * cap + slot] = vt.x; f[10 * cap + slot] = vt.y; f[11 * cap + slot] = vt.z;
+      } else {
+        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
+      }
+    }
+  }
+}
+
+struct ShadeSmem {
+  mlp::Net net;
+  __half x[kShadeRows * 64];
+  float out[kShadeRows * mlp::kOutPad];
+};
+
+__global__ void __launch_bounds__(kShadeThreads) guided_shade_kernel(SceneView sc, Queues q, GuideCtx gc,
+                                                                     uint32_t bounce, uint32_t max_depth,
+                                                                     uint32_t sample_base, uint64_t seed) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  ShadeSmem& s = *reinterpret_cast<ShadeSmem*>(raw);
+  mlp::load_net<kShadeThreads>(s.net, gc.params16);
+  const uint32_t count = min(gc.vcount[bounce], q.capacity);
+  const uint32_t cap = q.capacity;
+  uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
+  float* dst = q.fields[(bounce + 1) & 1];
+  uint32_t* dst_rec = q.rec[(bounce + 1) & 1];
+  const float g = gc.frac;
+  const int warp = threadIdx.x >> 5;
+  for (uint32_t base = blockIdx.x * kShadeRows; base < count; base += gridDim.x * kShadeRows) {
+    __syncthreads();
+    for (int w = threadIdx.x; w < kShadeRows * 5; w += kShadeThreads) {
+      const int r = w / 5, grp = w % 5;
+      const uint32_t i = base + r;
+      __half* row = s.x + r * 64;
+      if (i < count) {
+        const float p[3] = {gc.vtx[0 * cap + i], gc.vtx[1 * cap + i], gc.vtx[2 * cap + i]};
+        const float n[3] = {gc.vtx[3 * cap + i], gc.vtx[4 * cap + i], gc.vtx[5 * cap + i]};
+        mlp::encode_group(grp, p, n, gc.box, row);
+      } else {
+        const int col = grp < 3 ? grp * mlp::kPosBins : 3 * mlp::kPosBins + (grp - 3) * mlp::kDirBins;
+        const int bins = grp < 3 ? mlp::kPosBins : mlp::kDirBins;
+        for (int k = 0; k < bins; k += 2) mlp::st32(row + col + k, 0u);
+      }
+    }
+    __syncthreads();
+    mlp::forward_rows(s.net, s.x, warp * 16, nullptr, s.out);
+    __syncthreads();
+    if (threadIdx.x >= kShadeRows) continue;  // warps 0..3 shade one vertex per thread
+    const uint32_t i = base + threadIdx.x;
+    bool want_shadow = false, want_next = false, want_rec = false;
+    f3 sh_o, sh_d, sh_c, nx_o, nx_d, nx_t;
+    float sh_tmax = 0.0f, nx_pdf = 0.0f, wpre = 0.0f;
+    uint32_t path_id = 0;
+    f3 normal;
+    if (i < count) {
+      path_id = gc.vtx_ids[i];
+      const f3 p = mk(gc.vtx[0 * cap + i], gc.vtx[1 * cap + i], gc.vtx[2 * cap + i]);
+      normal = mk(gc.vtx[3 * cap + i], gc.vtx[4 * cap + i], gc.vtx[5 * cap + i]);
+      const f3 albedo = mk(gc.vtx[6 * cap + i], gc.vtx[7 * cap + i], gc.vtx[8 * cap + i]);
+      const f3 T = mk(gc.vtx[9 * cap + i], gc.vtx[10 * cap + i], gc.vtx[11 * cap + i]);
+      mlp::Mixture mix;
+      mlp::mixture_from_outputs(&s.out[threadIdx.x * mlp::kOutPad], mix);
+      if (sc.n_lights > 0 && sc.total_light_weight > 0.0f) {
+        // light sample as in MIS tracing; its MIS weight is against the
+        // combined continuation pdf
+        const float4 u = uniform4(seed, path_id, stage_light(bounce));
+        const float as = u.x * (float)sc.n_lights;
+        uint32_t li = (uint32_t)as;
+        const float frac = as - (float)li;
+        const float* lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+        if (frac > lrec[12]) li = __float_as_uint(lrec[13]);
+        lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+        const f3 p0 = mk(lrec[0], lrec[1], lrec[2]), p1 = mk(lrec[3], lrec[4], lrec[5]),
+                 p2 = mk(lrec[6], lrec[7], lrec[8]);
+        const f3 e1 = p1 - p0, e2 = p2 - p0;
+        const f3 av = cross(e1, e2);
+        const float tas = length2(av);
+        if (tas > 0.0f) {
+          const f3 ln = divs(av, sqrtf(tas));
+          const float ru = sqrtf(u.y);
+          const float b1 = ru * (1.0f - u.z);
+          const float b2 = ru - b1;
+          const f3 lp = (p0 + e1 * b1) + e2 * b2;
+          const f3 tl = lp - p;
+          const float d2 = length2(tl);
+          if (d2 > 1.0e-8f) {
+            const float dist = sqrtf(d2);
+            const f3 dir = divs(tl, dist);
+            const float scos = fmaxf(dot(normal, dir), 0.0f);
+            const float lcos = fmaxf(dot(ln, neg(dir)), 0.0f);
+            const float smax = dist - 0.002f;
+            if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
+              const f3 E = mk(lrec[9], lrec[10], lrec[11]);
+              const float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * sc.total_light_weight);
+              const float bpdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
+              const float dd[3] = {dir.x, dir.y, dir.z};
+              const float qpdf = (1.0f - g) * bpdf + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
+              if (lpdf > 0.0f && bpdf > 0.0f) {
+                const float scale = (scos * power_heuristic(lpdf, qpdf)) / lpdf;
+                if (scale > 0.0f) {
+                  want_shadow = true;
+                  sh_o = p;
+                  sh_d = dir;
+                  sh_tmax = smax;
+                  sh_c = mul(mul(T, albedo * kInvPi), E) * scale;
+                }
+              }
+            }
+          }
+        }
+      }
+      if (bounce + 1 < max_depth) {
+        const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
+        f3 dir;
+        if (u.w < g) {
+          int k = 0;
+          float acc = mix.pi[0];
+          while (k < mlp::kLobes - 1 && u.z >= acc) acc += mix.pi[++k];
+          dir = vmf_sample(mix.mu[k], mix.kap[k], u.x, u.y);
+        } else {
+          dir = smp::lambertian_dir(normal, u.x, u.y);
+        }
+        // cosine and BSDF pdf as the MIS tracer forms them, so that f = 0
+        // reproduces it exactly (factor 1, same stored pdf)
+        const float cosv = fmaxf(dot(normal, normalize(dir)), 0.0f);
+        const float bp = cosv * kInvPi;
+        if (bp > 0.0f) {
+          const float dd[3] = {dir.x, dir.y, dir.z};
+          const float qpdf = (1.0f - g) * bp + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
+          const float factor = bp / qpdf;
+          f3 Tn = mul(T, albedo);
+          if (factor != 1.0f) Tn = Tn * factor;
+          bool alive = qpdf > 0.0f;
+          if (alive && bounce + 1 >= 5u) {
+            const float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+            if (m <= 0.0f) alive = false;
+            else {
+              const float survival = fminf(fmaxf(m, 0.05f), 0.95f);
+              const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
+              if (rr.x >= survival) alive = false;
+              else Tn = divs(Tn, survival);
+            }
+          }
+          if (alive) {
+            want_next = true;
+            nx_o = p;
+            nx_d = dir;
+            nx_t = Tn;
+            nx_pdf = qpdf;
+            wpre = cosv / qpdf;
+            const uint32_t h = lowbias32(path_id ^ lowbias32(bounce * 0x9E3779B9u + (uint32_t)seed));
+            want_rec = gc.rec_cap > 0 && (float)(h >> 8) * (1.0f / 16777216.0f) < gc.rec_frac;
+          }
+        }
+      }
+    }
+    const uint32_t sslot = warp_append(&q.counters[2 * bounce + 1], want_shadow);
+    if (want_shadow) {
+      if (sslot < cap) {
+        q.shadow_ids[sslot] = path_id;
+        float* f = q.shadow_fields;
+        f[0 * cap + sslot] = sh_o.x; f[1 * cap + sslot] = sh_o.y; f[2 * cap + sslot] = sh_o.z;
+        f[3 * cap + sslot] = 0.001f;
+        f[4 * cap + sslot] = sh_d.x; f[5 * cap + sslot] = sh_d.y; f[6 * cap + sslot] = sh_d.z;
+        f[7 * cap + sslot] = sh_tmax;
+        f[8 * cap + sslot] = sh_c.x; f[9 * cap + sslot] = sh_c.y; f[10 * cap + sslot] = sh_c.z;
+      } else {
+        raise_status(q.status, BAJO_WAVE_SHADOW_OVERFLOW);
+      }
+    }
+    const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], want_next);
+    const uint32_t rslot = warp_append(&gc.rec_hdr[0], want_rec);
+    if (want_next) {
+      if (slot < cap) {
+        const uint32_t sidx = path_id - sample_base;
+        uint32_t rec = kNoRecord;
+        if (want_rec && rslot < gc.rec_cap) {
+          rec = rslot;
+          const size_t r3 = 3 * (size_t)rslot;
+          gc.rec_pos[r3] = nx_o.x; gc.rec_pos[r3 + 1] = nx_o.y; gc.rec_pos[r3 + 2] = nx_o.z;
+          gc.rec_nrm[r3] = normal.x; gc.rec_nrm[r3 + 1] = normal.y; gc.rec_nrm[r3 + 2] = normal.z;
+          gc.rec_dir[r3] = nx_d.x; gc.rec_dir[r3 + 1] = nx_d.y; gc.rec_dir[r3 + 2] = nx_d.z;
+          gc.rec_tn[r3] = nx_t.x; gc.rec_tn[r3 + 1] = nx_t.y; gc.rec_tn[r3 + 2] = nx_t.z;
+          gc.rec_snap[r3] = q.radiance[0 * cap + sidx];
+          gc.rec_snap[r3 + 1] = q.radiance[1 * cap + sidx];
+          gc.rec_snap[r3 + 2] = q.radiance[2 * cap + sidx];
+          gc.rec_sidx[rslot] = sidx;
+          gc.rec_wpre[rslot] = wpre;
+          gc.rec_weight[rslot] = 0.0f;
+        }
+        dst_rec[slot] = rec;
+        dst_ids[slot] = path_id;
+        dst[0 * cap + slot] = nx_o.x; dst[1 * cap + slot] = nx_o.y; dst[2 * cap + slot] = nx_o.z;
+        dst[3 * cap + slot] = 0.001f;
+        dst[4 * cap + slot] = nx_d.x; dst[5 * cap + slot] = nx_d.y; dst[6 * cap + slot] = nx_d.z;
+        dst[7 * cap + slot] = FLT_MAX;
+        dst[8 * cap + slot] = nx_t.x; dst[9 * cap + slot] = nx_t.y; dst[10 * cap + slot] = nx_t.z;
+        dst[11 * cap + slot] = nx_pdf;
+      } else {
+        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
+      }
+    }
+  }
+}
+
+// first record of the chunk = records appended so far (capped)
+__global__ void records_begin_chunk_kernel(uint32_t* hdr, uint32_t cap) { hdr[1] = min(hdr[0], cap); }
+
+// Records of the chunk: weight = mean_rgb((R_end - R_before) / T_after) *
+// cos / pdf, the radiance gathered after the vertex per unit throughput.
+__global__ void __launch_bounds__(kBlock) records_finish_chunk_kernel(GuideCtx gc, const float* __restrict__ radiance,
+                                                                      uint32_t cap) {
+  const uint32_t start = gc.rec_hdr[1], end = min(gc.rec_hdr[0], gc.rec_cap);
+  for (uint32_t i = start + blockIdx.x * kBlock + threadIdx.x; i < end; i += gridDim.x * kBlock) {
+    const uint32_t sidx = gc.rec_sidx[i];
+    float L = 0.0f;
+    for (int c = 0; c < 3; ++c) {
+      const float tn = gc.rec_tn[3 * (size_t)i + c];
+      const float gathered = radiance[c * (size_t)cap + sidx] - gc.rec_snap[3 * (size_t)i + c];
+      if (tn > 0.0f) L += gathered / tn;
+    }
+    float w = (L * (1.0f / 3.0f)) * gc.rec_wpre[i];
+    if (!(w > 0.0f) || !isfinite(w)) w = 0.0f;
+    gc.rec_weight[i] = w;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host
 // ---------------------------------------------------------------------------
 constexpr uint32_t kDefaultChunk = 1u << 22;
 
 struct Layout {
-  uint32_t cap, pixels_per_chunk;
-  size_t off_counters, off_ids[2], off_fields[2], off_shadow_ids, off_shadow_fields, off_radiance, total;
+  uint32_t cap, pixels_per_chunk, n_counters;
+  size_t off_counters, off_ids[2], off_fields[2], off_shadow_ids, off_shadow_fields, off_radiance;
+  size_t off_rec[2], off_vtx_ids, off_vtx;  // guided tracing only
+  size_t total;
 };
 
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
@@ -421,12 +794,16 @@ bool make_layout(const BajoRenderSettings* s, Layout* L) {
   uint32_t ppc = want / s->spp;
   const uint64_t npix = (uint64_t)s->width * s->height;
   if (ppc > npix) ppc = (uint32_t)npix;
+  const bool guided = s->algorithm == BAJO_RENDER_GUIDED;
   L->pixels_per_chunk = ppc;
   L->cap = ppc * s->spp;
+  // [2b] paths of bounce b, [2b+1] its shadow rays; guided: then the
+  // Lambertian vertices of every bounce
+  L->n_counters = 2 * s->max_depth + 2 + (guided ? s->max_depth : 0);
   const size_t cap = L->cap;
   size_t o = 256;  // status word, then two 64-bit ray totals at offset 8
   L->off_counters = o;
-  o = a256(o + (2 * (size_t)s->max_depth + 2) * 4);
+  o = a256(o + (size_t)L->n_counters * 4);
   for (int k = 0; k < 2; ++k) {
     L->off_ids[k] = o;
     o = a256(o + cap * 4);
@@ -439,7 +816,49 @@ bool make_layout(const BajoRenderSettings* s, Layout* L) {
   o = a256(o + cap * 4 * kShadowPlanes);
   L->off_radiance = o;
   o = a256(o + cap * 4 * 3);
+  L->off_rec[0] = L->off_rec[1] = L->off_vtx_ids = L->off_vtx = 0;
+  if (guided) {
+    for (int k = 0; k < 2; ++k) {
+      L->off_rec[k] = o;
+      o = a256(o + cap * 4);
+    }
+    L->off_vtx_ids = o;
+    o = a256(o + cap * 4);
+    L->off_vtx = o;
+    o = a256(o + cap * 4 * kVtxPlanes);
+  }
   L->total = o;
+  return true;
+}
+
+// scene and queue views over the caller's buffers; false on a missing array
+bool make_views(const BajoRtScene* scene, unsigned char* w, const Layout& L, SceneView& sc, Queues& q) {
+  const BajoLbvh* b = scene->bvh;
+  if (!b->roots || !b->node_bounds || !b->node_meta || !b->leaf_tris || !scene->surfaces || !scene->lambertians ||
+      !scene->emissives || (scene->n_lights && !scene->lights))
+    return false;
+  sc.roots = b->roots;
+  sc.nb = reinterpret_cast<const float4*>(b->node_bounds);
+  sc.meta = reinterpret_cast<const uint4*>(b->node_meta);
+  sc.tris = reinterpret_cast<const float4*>(b->leaf_tris);
+  sc.n_nodes = b->n_leaves;
+  sc.surfaces = scene->surfaces;
+  sc.lambertians = scene->lambertians;
+  sc.emissives = scene->emissives;
+  sc.lights = scene->lights;
+  sc.n_lights = scene->n_lights;
+  sc.total_light_weight = scene->total_light_weight;
+  for (int k = 0; k < 2; ++k) {
+    q.ids[k] = (uint32_t*)(w + L.off_ids[k]);
+    q.fields[k] = (float*)(w + L.off_fields[k]);
+    q.rec[k] = L.off_rec[k] ? (uint32_t*)(w + L.off_rec[k]) : nullptr;
+  }
+  q.shadow_ids = (uint32_t*)(w + L.off_shadow_ids);
+  q.shadow_fields = (float*)(w + L.off_shadow_fields);
+  q.radiance = (float*)(w + L.off_radiance);
+  q.counters = (uint32_t*)(w + L.off_counters);
+  q.status = (uint32_t*)w;
+  q.capacity = L.cap;
   return true;
 }
 
@@ -454,6 +873,40 @@ cudaError_t launch_bounce(const SceneView& sc, const Queues& q, uint32_t grid, u
     e = cudaGetLastError();
   }
   return e;
+}
+
+// Chunks of whole pixels: primary rays, `bounce(chunk, b)` per bounce, an
+// optional per-chunk hook, the per-pixel resolve.
+template <class Bounce, class Before, class After>
+cudaError_t render_chunks(const BajoRenderSettings* s, const Layout& L, const Queues& q, const float* d_camera,
+                          float* d_pixels, double* d_pixels64, unsigned long long* totals, cudaStream_t st,
+                          Bounce bounce, Before before, After after) {
+  const uint32_t n_pixels = s->width * s->height;
+  cudaError_t e = cudaMemsetAsync(totals, 0, 16, st);
+  if (e != cudaSuccess) return e;
+  for (uint32_t pb = 0; pb < n_pixels; pb += L.pixels_per_chunk) {
+    const uint32_t pc = std::min(L.pixels_per_chunk, n_pixels - pb);
+    const uint32_t count = pc * s->spp;
+    const uint32_t sample_base = pb * s->spp;
+    if ((e = cudaMemsetAsync(q.counters, 0, (size_t)L.n_counters * 4, st)) != cudaSuccess) return e;
+    if ((e = before()) != cudaSuccess) return e;
+    primary_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, st>>>(d_camera, q, count, sample_base, s->width,
+                                                                    s->height, s->spp, s->seed);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    for (uint32_t bnc = 0; bnc < s->max_depth; ++bnc)
+      if ((e = bounce(bnc, sample_base)) != cudaSuccess) return e;
+    if ((e = after()) != cudaSuccess) return e;
+    resolve_kernel<<<(pc + kBlock - 1) / kBlock, kBlock, 0, st>>>(q.radiance, L.cap, pb, pc, s->spp, d_pixels,
+                                                                  d_pixels64, q.counters, s->max_depth, totals);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
+  return cudaSuccess;
+}
+
+uint32_t bounce_grid(uint32_t cap) {
+  uint32_t grid = (cap + kBlock - 1) / kBlock;
+  const uint32_t max_grid = (uint32_t)sm_count() * 16;
+  return grid > max_grid ? max_grid : grid;
 }
 
 }  // namespace rt
@@ -477,65 +930,102 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
   if (s->algorithm != BAJO_RENDER_PATH && s->algorithm != BAJO_RENDER_NEE && s->algorithm != BAJO_RENDER_MIS)
     return BAJO_ERR_INVALID_ARGUMENT;
   if (ws_bytes < L.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
-  const BajoLbvh* b = scene->bvh;
-  if (!b->roots || !b->node_bounds || !b->node_meta || !b->leaf_tris || !scene->surfaces || !scene->lambertians ||
-      !scene->emissives || (scene->n_lights && !scene->lights))
-    return BAJO_ERR_INVALID_ARGUMENT;
-  cudaStream_t st = (cudaStream_t)stream;
-  unsigned char* w = (unsigned char*)d_ws;
   SceneView sc;
-  sc.roots = b->roots;
-  sc.nb = reinterpret_cast<const float4*>(b->node_bounds);
-  sc.meta = reinterpret_cast<const uint4*>(b->node_meta);
-  sc.tris = reinterpret_cast<const float4*>(b->leaf_tris);
-  sc.n_nodes = b->n_leaves;
-  sc.surfaces = scene->surfaces;
-  sc.lambertians = scene->lambertians;
-  sc.emissives = scene->emissives;
-  sc.lights = scene->lights;
-  sc.n_lights = scene->n_lights;
-  sc.total_light_weight = scene->total_light_weight;
   Queues q;
-  for (int k = 0; k < 2; ++k) {
-    q.ids[k] = (uint32_t*)(w + L.off_ids[k]);
-    q.fields[k] = (float*)(w + L.off_fields[k]);
-  }
-  q.shadow_ids = (uint32_t*)(w + L.off_shadow_ids);
-  q.shadow_fields = (float*)(w + L.off_shadow_fields);
-  q.radiance = (float*)(w + L.off_radiance);
-  q.counters = (uint32_t*)(w + L.off_counters);
-  q.status = (uint32_t*)w;
-  q.capacity = L.cap;
-  const uint32_t n_pixels = s->width * s->height;
-  uint32_t grid = (L.cap + kBlock - 1) / kBlock;
-  const uint32_t max_grid = (uint32_t)sm_count() * 16;
-  if (grid > max_grid) grid = max_grid;
-  const size_t counter_bytes = (2 * (size_t)s->max_depth + 2) * 4;
-  unsigned long long* totals = (unsigned long long*)(w + 8);
-  if (cudaMemsetAsync(totals, 0, 16, st) != cudaSuccess) return BAJO_ERR_CUDA;
-  for (uint32_t pb = 0; pb < n_pixels; pb += L.pixels_per_chunk) {
-    const uint32_t pc = std::min(L.pixels_per_chunk, n_pixels - pb);
-    const uint32_t count = pc * s->spp;
-    const uint32_t sample_base = pb * s->spp;
-    if (cudaMemsetAsync(q.counters, 0, counter_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
-    primary_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, st>>>(d_camera, q, count, sample_base, s->width,
-                                                                    s->height, s->spp, s->seed);
-    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
-    for (uint32_t bnc = 0; bnc < s->max_depth; ++bnc) {
-      cudaError_t e;
-      if (s->algorithm == BAJO_RENDER_PATH)
-        e = launch_bounce<BAJO_RENDER_PATH>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
-      else if (s->algorithm == BAJO_RENDER_NEE)
-        e = launch_bounce<BAJO_RENDER_NEE>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
-      else
-        e = launch_bounce<BAJO_RENDER_MIS>(sc, q, grid, bnc, s->max_depth, sample_base, s->seed, st);
-      if (e != cudaSuccess) return BAJO_ERR_CUDA;
-    }
-    resolve_kernel<<<(pc + kBlock - 1) / kBlock, kBlock, 0, st>>>(q.radiance, L.cap, pb, pc, s->spp, d_pixels,
-                                                                  d_pixels64, q.counters, s->max_depth, totals);
-    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
-  }
-  return BAJO_OK;
+  unsigned char* w = (unsigned char*)d_ws;
+  if (!make_views(scene, w, L, sc, q)) return BAJO_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  const uint32_t grid = bounce_grid(L.cap);
+  const int algo = s->algorithm;
+  auto bounce = [&](uint32_t b, uint32_t sample_base) {
+    if (algo == BAJO_RENDER_PATH)
+      return launch_bounce<BAJO_RENDER_PATH>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
+    if (algo == BAJO_RENDER_NEE)
+      return launch_bounce<BAJO_RENDER_NEE>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
+    return launch_bounce<BAJO_RENDER_MIS>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
+  };
+  auto none = []() { return cudaSuccess; };
+  const cudaError_t e = render_chunks(s, L, q, d_camera, d_pixels, d_pixels64, (unsigned long long*)(w + 8), st,
+                                      bounce, none, none);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, const BajoRenderSettings* s,
+                           const BajoGuide* guide, float* d_pixels, double* d_pixels64, void* d_ws, size_t ws_bytes,
+                           void* stream) {
+  using namespace bajo;
+  using namespace bajo::rt;
+  Layout L;
+  if (!scene || !scene->bvh || !d_camera || !d_pixels || !d_ws || !guide || !make_layout(s, &L))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  if (s->algorithm != BAJO_RENDER_GUIDED || !guide->params16 || !guide->box6 || !(guide->guide_fraction >= 0.0f) ||
+      !(guide->guide_fraction <= 1.0f) || (guide->record_capacity && !guide->records))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  if (ws_bytes < L.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
+  SceneView sc;
+  Queues q;
+  unsigned char* w = (unsigned char*)d_ws;
+  if (!make_views(scene, w, L, sc, q)) return BAJO_ERR_INVALID_ARGUMENT;
+  cudaStream_t st = (cudaStream_t)stream;
+  GuideCtx gc;
+  gc.params16 = (const __half*)guide->params16;
+  gc.box = guide->box6;
+  gc.frac = guide->guide_fraction;
+  gc.rec_frac = guide->record_fraction;
+  gc.rec_cap = guide->record_capacity;
+  // without a record buffer the record counter lives in the workspace header
+  // (bytes 24..31, after the status word and the two ray totals)
+  unsigned char* rb = (unsigned char*)guide->records;
+  const mlp::RecordLayout RL = mlp::record_layout(guide->record_capacity);
+  gc.rec_hdr = rb ? (uint32_t*)rb : (uint32_t*)(w + 24);
+  gc.rec_pos = rb ? (float*)(rb + RL.pos) : nullptr;
+  gc.rec_nrm = rb ? (float*)(rb + RL.nrm) : nullptr;
+  gc.rec_dir = rb ? (float*)(rb + RL.dir) : nullptr;
+  gc.rec_weight = rb ? (float*)(rb + RL.weight) : nullptr;
+  gc.rec_sidx = rb ? (uint32_t*)(rb + RL.sidx) : nullptr;
+  gc.rec_tn = rb ? (float*)(rb + RL.tn) : nullptr;
+  gc.rec_snap = rb ? (float*)(rb + RL.snap) : nullptr;
+  gc.rec_wpre = rb ? (float*)(rb + RL.wpre) : nullptr;
+  if (!rb) gc.rec_cap = 0;
+  gc.vtx_ids = (uint32_t*)(w + L.off_vtx_ids);
+  gc.vtx = (float*)(w + L.off_vtx);
+  gc.vcount = q.counters + 2 * s->max_depth + 2;
+  const size_t smem = sizeof(ShadeSmem);
+  if (cudaFuncSetAttribute(guided_shade_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return BAJO_ERR_CUDA;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, guided_shade_kernel, kShadeThreads, smem) !=
+          cudaSuccess ||
+      per_sm < 1)
+    return BAJO_ERR_CUDA;
+  uint32_t shade_grid = (L.cap + kShadeRows - 1) / kShadeRows;
+  const uint32_t shade_max = (uint32_t)(sm_count() * per_sm);
+  if (shade_grid > shade_max) shade_grid = shade_max;
+  const uint32_t grid = bounce_grid(L.cap);
+  if (!rb && cudaMemsetAsync(gc.rec_hdr, 0, 8, st) != cudaSuccess) return BAJO_ERR_CUDA;
+  auto bounce = [&](uint32_t b, uint32_t sample_base) {
+    guided_trace_kernel<<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    guided_shade_kernel<<<shade_grid, kShadeThreads, smem, st>>>(sc, q, gc, b, s->max_depth, sample_base, s->seed);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
+    return cudaGetLastError();
+  };
+  auto before = [&]() {
+    if (gc.rec_cap == 0) return cudaSuccess;
+    records_begin_chunk_kernel<<<1, 1, 0, st>>>(gc.rec_hdr, gc.rec_cap);
+    return cudaGetLastError();
+  };
+  auto after = [&]() {
+    if (gc.rec_cap == 0) return cudaSuccess;
+    records_finish_chunk_kernel<<<grid, kBlock, 0, st>>>(gc, q.radiance, L.cap);
+    return cudaGetLastError();
+  };
+  const cudaError_t e = render_chunks(s, L, q, d_camera, d_pixels, d_pixels64, (unsigned long long*)(w + 8), st,
+                                      bounce, before, after);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
 int32_t bajo_render_stats(const void* d_ws, void* stream, uint64_t* rays, uint64_t* shadow_rays) {

@@ -205,6 +205,33 @@ def spheres_in_box(n_spheres: int = 64, subdivisions: int = 5, seed: int = 0, em
                    f"unit box + {n_spheres} icospheres (subdivision {subdivisions}) + ceiling light")
 
 
+def indirect_box_scene(emission: float = 40.0, size: float = 0.2, y: float = 0.85, n_spheres: int = 3,
+                       seed: int = 5) -> RtScene:
+    """The unit box lit only indirectly: its light is a size x size panel at
+    height y facing the ceiling (the emissive side is its top), so apart from
+    the ceiling patch above it every surface receives light that bounced off
+    that patch -- light that next-event estimation cannot reach and cosine
+    sampling finds rarely, the case path guiding exists for.  A few
+    subdivision-2 icospheres sit on the floor half."""
+    rng = np.random.default_rng(seed)
+    panel = ceiling_light(size, y)[:, ::-1]  # reversed winding: normal +y
+    parts = [unit_box_inward(), panel]
+    surf = [[surface_id(MAT_LAMBERTIAN, 0)] * 12, [surface_id(MAT_EMISSIVE, 0)] * 2]
+    albedo = [[0.75, 0.75, 0.75]]
+    unit = icosphere(2)
+    for s in range(n_spheres):
+        r = rng.uniform(0.08, 0.15)
+        c = np.array([rng.uniform(r + 0.05, 1 - r - 0.05), r, rng.uniform(0.4, 0.9)])
+        parts.append(unit * r + c)
+        albedo.append(list(rng.uniform(0.3, 0.8, 3)))
+        surf.append([surface_id(MAT_LAMBERTIAN, s + 1)] * unit.shape[0])
+    from .camera import camera_from_vfov
+    cam = camera_from_vfov([0.5, 0.5, 0.02], [0.5, 0.4, 1.0], [0.0, 1.0, 0.0], 70.0)
+    return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
+                   np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
+                   f"unit box lit by an upward-facing {size} x {size} panel + {n_spheres} icospheres")
+
+
 def small_rt_scene(seed: int = 1) -> RtScene:
     """A small scene for parity tests: the box, the light and 4 icospheres of
     subdivision 2 (1,294 triangles)."""

@@ -274,6 +274,88 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
  * the last bajo_render call on this workspace. */
 int32_t bajo_render_stats(const void* d_workspace, void* stream, uint64_t* rays, uint64_t* shadow_rays);
 
+/* ======================================================================== */
+/* Path guiding: a small MLP proposal trained online (new on this path; the  */
+/* reference has no guiding)                                                 */
+/* ======================================================================== */
+/* Network: one-blob(position in box6, 3 x 16 bins) ++ one-blob(octahedral
+ * normal, 2 x 8 bins) = 64 features -> 3 x (64, ReLU) -> 20 outputs =
+ * 4 vMF lobes x (mean xyz, log kappa, weight logit).  FP16 weights and
+ * activations, FP32 accumulation on the tensor cores.  Parameter layout
+ * (bajo_mlp_param_count elements): W1[64x64] b1[64] W2 b2 W3 b3 W4[32x64]
+ * b4[32], weights row-major [out][in]; rows 20..31 of W4/b4 are kept zero.
+ * Mixture: mean = m / sqrt(|m|^2 + 1e-12), kappa = exp(clamp(s, -2, 8)), weights =
+ * softmax(logits), lobe pdf kappa / (2 pi (1 - e^-2kappa)) e^(kappa (mu.w-1)). */
+#define BAJO_MLP_OUTPUTS 20
+int32_t bajo_mlp_param_count(uint32_t* count);
+
+/* d_out20[20 i + c] = raw outputs for sample i (positions and normals are
+ * 3 f32 each, box6 = [min xyz, max xyz]). */
+int32_t bajo_mlp_forward(const void* d_params16, const float* d_pos, const float* d_nrm, uint32_t n,
+                         const float* d_box6, float* d_out20, void* stream);
+
+/* d_grad32 = gradient of sum_i -w_i log pdf_i(dir_i) w.r.t. the parameters
+ * (overwritten); *d_loss (may be NULL) = that sum. */
+int32_t bajo_mlp_grad(const void* d_params16, const float* d_pos, const float* d_nrm, const float* d_dir,
+                      const float* d_weight, uint32_t n, const float* d_box6, float* d_grad32, float* d_loss,
+                      void* stream);
+
+/* One Adam step (Kingma & Ba) on FP32 master weights with gradient
+ * grad_scale * d_grad32; refreshes the FP16 copy.  step counts from 1. */
+int32_t bajo_mlp_adam(float* d_params32, void* d_params16, const float* d_grad32, float* d_m, float* d_v,
+                      uint32_t step, float lr, float beta1, float beta2, float eps, float grad_scale, void* stream);
+
+/* Guided wavefront rendering: BAJO_RENDER_MIS with the continuation drawn by
+ * one-sample MIS from (1 - f) * cosine BSDF + f * network mixture and every
+ * MIS weight (emission hits, light samples) taken against that combined
+ * pdf, so the estimator stays unbiased for any network.  Per bounce: closest
+ * hit + emission, then one fused kernel that runs the network over the
+ * bounce's Lambertian vertices on the tensor cores and does next-event
+ * estimation and the continuation sample, then the shadow rays.
+ * Training records: a fraction of the continued vertices (chosen by a hash
+ * of path and bounce) is kept, up to record_capacity per call; at the end of
+ * each chunk a record holds position, normal, sampled direction and weight
+ * mean_rgb(L_i(dir)) * cos / pdf, L_i being the radiance the path gathered
+ * after the vertex divided by its throughput.
+ * Record buffer (bajo_guide_records_size bytes): u32 count at byte 0 (zero
+ * it to start collecting), then, each array starting on a 256-byte boundary
+ * after a 256-byte header: pos f32[3 cap], nrm f32[3 cap], dir f32[3 cap],
+ * weight f32[cap], then internal scratch. */
+#define BAJO_RENDER_GUIDED 5
+typedef struct BajoGuide {
+  const void* params16;     /* network parameters (FP16)                         */
+  const float* box6;        /* device: scene box for the position encoding       */
+  float guide_fraction;     /* probability of sampling the network (0.5)         */
+  float record_fraction;    /* probability a continued vertex becomes a record   */
+  uint32_t record_capacity; /* records kept per call (0 = none)                  */
+  void* records;            /* device buffer, bajo_guide_records_size bytes      */
+} BajoGuide;
+
+int32_t bajo_guide_records_size(uint32_t capacity, size_t* bytes);
+
+/* settings->algorithm must be BAJO_RENDER_GUIDED; workspace from
+ * bajo_render_workspace_size with the same settings. */
+int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, const BajoRenderSettings* settings,
+                           const BajoGuide* guide, float* d_pixels, double* d_pixels64, void* d_workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* Online training state (device arrays of bajo_mlp_param_count elements). */
+typedef struct BajoGuideNet {
+  float* params32;
+  void* params16;
+  float* adam_m;
+  float* adam_v;
+  float* grad;
+  float* loss;   /* 1 f32: summed loss of the last step */
+  uint32_t step; /* Adam steps taken so far (advanced by bajo_guide_train) */
+} BajoGuideNet;
+
+/* `steps` Adam steps (beta 0.9 / 0.999, eps 1e-8, learning rate lr), each
+ * on `batch` records taken cyclically from the buffer (count read on the
+ * device, so no host synchronisation). */
+int32_t bajo_guide_train(BajoGuideNet* net, const void* d_records, uint32_t record_capacity, const float* d_box6,
+                         uint32_t batch, uint32_t steps, float lr, void* stream);
+
 /* Host-side camera records (no device work).  Camera.__init__ and
  * Camera.from_vfov (bajo/bvh/camera.mojo:77-116): out20 receives
  * [origin, forward, right, up, fov_scale, focus_dist, disk_u, disk_v]

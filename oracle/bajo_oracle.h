@@ -170,6 +170,19 @@ void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, ui
                     uint32_t height, uint64_t seed, int mode, float* t0, uint32_t* p0, float* t1, uint32_t* p1,
                     uint32_t n_threads);
 
+/* ---- path-guiding network (bajo_oracle_mlp.c), FP64 ---------------------- */
+/* Parameters as doubles in the library's layout: W1[64x64] b1[64] W2 b2 W3 b3
+ * W4[32x64] b4[32] (rows 20..31 of the output layer unused). */
+uint32_t bo_mlp_param_count(void);
+void bo_mlp_encode(const float* p, const float* n, const float* box6, float* feat64);
+void bo_mlp_forward_f64(const double* params, const float* pos, const float* nrm, const float* box6, uint32_t n,
+                        double* out20);
+double bo_vmf_mixture_pdf(const double* out20, const float* dir);
+double bo_mlp_loss_f64(const double* params, const float* pos, const float* nrm, const float* dir, const float* w,
+                       uint32_t n, const float* box6);
+double bo_mlp_grad_f64(const double* params, const float* pos, const float* nrm, const float* dir, const float* w,
+                       uint32_t n, const float* box6, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

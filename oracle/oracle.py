@@ -93,6 +93,12 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
         "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
+        "bo_mlp_param_count": (_U32, []),
+        "bo_mlp_encode": (None, [_P, _P, _P, _P]),
+        "bo_mlp_forward_f64": (None, [_P, _P, _P, _P, _U32, _P]),
+        "bo_vmf_mixture_pdf": (ctypes.c_double, [_P, _P]),
+        "bo_mlp_loss_f64": (ctypes.c_double, [_P, _P, _P, _P, _P, _U32, _P]),
+        "bo_mlp_grad_f64": (ctypes.c_double, [_P, _P, _P, _P, _P, _U32, _P, _P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -404,3 +410,50 @@ def trace_batch(bvh: OracleLbvh, cams, cam_stride, width, height, seed=7, tri_mo
     lib().bo_trace_batch(ctypes.byref(s), _ptr(bvh.verts), _ptr(c), cam_stride, width, height, seed, tri_mode,
                          _ptr(t0), _ptr(p0), _ptr(t1), _ptr(p1), threads or n_threads())
     return t0, p0, t1, p1
+
+
+# ---- path-guiding network (FP64) -------------------------------------------
+def _f32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def mlp_param_count() -> int:
+    return int(lib().bo_mlp_param_count())
+
+
+def mlp_encode(p, n, box) -> np.ndarray:
+    out = np.zeros(64, np.float32)
+    p, n, box = _f32(p), _f32(n), _f32(box)
+    lib().bo_mlp_encode(_ptr(p), _ptr(n), _ptr(box), _ptr(out))
+    return out
+
+
+def mlp_forward(params, pos, nrm, box) -> np.ndarray:
+    params = np.ascontiguousarray(params, np.float64)
+    pos, nrm, box = _f32(pos), _f32(nrm), _f32(box)
+    n = pos.size // 3
+    out = np.zeros((n, 20), np.float64)
+    lib().bo_mlp_forward_f64(_ptr(params), _ptr(pos), _ptr(nrm), _ptr(box), n, _ptr(out))
+    return out
+
+
+def vmf_mixture_pdf(out20, d) -> float:
+    o = np.ascontiguousarray(out20, np.float64)
+    d = _f32(d)
+    return float(lib().bo_vmf_mixture_pdf(_ptr(o), _ptr(d)))
+
+
+def mlp_loss(params, pos, nrm, dirs, w, box) -> float:
+    params = np.ascontiguousarray(params, np.float64)
+    pos, nrm, dirs, w, box = _f32(pos), _f32(nrm), _f32(dirs), _f32(w), _f32(box)
+    return float(lib().bo_mlp_loss_f64(_ptr(params), _ptr(pos), _ptr(nrm), _ptr(dirs), _ptr(w), w.size, _ptr(box)))
+
+
+def mlp_grad(params, pos, nrm, dirs, w, box):
+    """(gradient [n_params] f64, loss) of sum -w log pdf(dir)."""
+    params = np.ascontiguousarray(params, np.float64)
+    pos, nrm, dirs, w, box = _f32(pos), _f32(nrm), _f32(dirs), _f32(w), _f32(box)
+    g = np.zeros(params.size, np.float64)
+    loss = lib().bo_mlp_grad_f64(_ptr(params), _ptr(pos), _ptr(nrm), _ptr(dirs), _ptr(w), w.size, _ptr(box),
+                                 _ptr(g))
+    return g, float(loss)
