@@ -25,7 +25,7 @@ __device__ void encode_tile(__half* x, const float* __restrict__ pos, const floa
   for (int w = threadIdx.x; w < kRows * 5; w += kThreads) {
     const int r = w / 5, grp = w % 5;
     const uint64_t j = row_base + r;
-    __half* row = x + r * 64;
+    __half* row = x + r * kLd;
     if (j < rows) {
       const uint64_t i = wrap ? ((uint64_t)offset + j) % count : j;
       const float p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
@@ -41,28 +41,40 @@ __device__ void encode_tile(__half* x, const float* __restrict__ pos, const floa
 
 struct FwdSmem {
   Net net;
-  __half x[kRows * 64];
-  float out[kRows * kOutPad];
+  WarpTile tile[kWarps];
 };
 
-__global__ void __launch_bounds__(kThreads) forward_kernel(const __half* __restrict__ p16,
-                                                           const float* __restrict__ pos,
-                                                           const float* __restrict__ nrm, const float* box,
-                                                           uint32_t n, float* __restrict__ out20) {
+// warp-autonomous: every warp encodes 32 samples (one per lane), runs them
+// through the network and writes their outputs
+__global__ void __launch_bounds__(kThreads, 2) forward_kernel(const __half* __restrict__ p16,
+                                                              const float* __restrict__ pos,
+                                                              const float* __restrict__ nrm, const float* box,
+                                                              uint32_t n, float* __restrict__ out20) {
   extern __shared__ __align__(16) unsigned char raw[];
   FwdSmem& s = *reinterpret_cast<FwdSmem*>(raw);
   load_net<kThreads>(s.net, p16);
-  const int warp = threadIdx.x >> 5;
-  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < n; base += (uint64_t)gridDim.x * kRows) {
-    __syncthreads();
-    encode_tile(s.x, pos, nrm, box, base, n, 0, n, false);
-    __syncthreads();
-    forward_rows(s.net, s.x, warp * 16, nullptr, s.out);
-    __syncthreads();
-    for (int k = threadIdx.x; k < kRows * kOut; k += kThreads) {
-      const int r = k / kOut, c = k % kOut;
-      if (base + r < n) out20[(base + r) * kOut + c] = s.out[r * kOutPad + c];
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  WarpTile& t = s.tile[warp];
+  const uint64_t warps = (uint64_t)gridDim.x * kWarps;
+  for (uint64_t base = ((uint64_t)blockIdx.x * kWarps + warp) * 32; base < n; base += warps * 32) {
+    const uint64_t i = base + lane;
+    __half* row = t.x + lane * kLd;
+    if (i < n) {
+      const float p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+      const float q[3] = {nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]};
+      encode_row(p, q, box, row);
+    } else {
+      for (int k = 0; k < kIn; k += 2) st32(row + k, 0u);
     }
+    __syncwarp();
+    forward_tile<2>(s.net, t.x, 0, nullptr, t.out);
+    __syncwarp();
+    for (int k = lane; k < 32 * kOut; k += 32) {
+      const int r = k / kOut, c = k % kOut;
+      if (base + r < n) out20[(base + r) * kOut + c] = t.out[r * kOutLd + c];
+    }
+    __syncwarp();
   }
 }
 
@@ -98,20 +110,20 @@ __device__ __forceinline__ void dw_tile(const __half* dz, int dz_ld, int out0, c
     a[1] = pk2(dz[r * dz_ld + out0 + g + 8], dz[(r + 1) * dz_ld + out0 + g + 8]);
     a[2] = pk2(dz[(r + 8) * dz_ld + out0 + g], dz[(r + 9) * dz_ld + out0 + g]);
     a[3] = pk2(dz[(r + 8) * dz_ld + out0 + g + 8], dz[(r + 9) * dz_ld + out0 + g + 8]);
-    b[0] = pk2(act[r * 64 + in0 + g], act[(r + 1) * 64 + in0 + g]);
-    b[1] = pk2(act[(r + 8) * 64 + in0 + g], act[(r + 9) * 64 + in0 + g]);
+    b[0] = pk2(act[r * kLd + in0 + g], act[(r + 1) * kLd + in0 + g]);
+    b[1] = pk2(act[(r + 8) * kLd + in0 + g], act[(r + 9) * kLd + in0 + g]);
     mma16816(c, a, b);
   }
 }
 
 struct TrainSmem {
   Net net;
-  __half WT[3][kIn * kHid];    // transposes [in][out]
-  __half W4T[kHid * kOutPad];  // [in][out]
-  __half act[4][kRows * 64];   // X, A1, A2, A3 of the tile, row-major
-  __half dz[kRows * 64];       // dZ of the layer being reduced
-  __half g[kRows * kOutPad];   // scaled dL/dout
-  float out[kRows * kOutPad];  // outputs of the tile
+  __half WT[3][kIn * kLd];     // transposes [in][out]
+  __half W4T[kHid * kLd32];    // [in][out]
+  __half act[4][kRows * kLd];  // X, A1, A2, A3 of the tile, row-major
+  __half dz[kRows * kLd];      // dZ of the layer being reduced
+  __half g[kRows * kLd32];     // scaled dL/dout
+  float out[kRows * kOutLd];   // outputs of the tile
   float db[4][kHid];
   float loss;
 };
@@ -128,9 +140,9 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
   TrainSmem& s = *reinterpret_cast<TrainSmem*>(raw);
   load_net<kThreads>(s.net, p16);
   for (int i = threadIdx.x; i < kHid * kIn; i += kThreads)
-    for (int l = 0; l < 3; ++l) s.WT[l][(i % kIn) * kHid + i / kIn] = p16[kOffW(l) + i];
+    for (int l = 0; l < 3; ++l) s.WT[l][(i % kIn) * kLd + i / kIn] = p16[kOffW(l) + i];
   for (int i = threadIdx.x; i < kOutPad * kHid; i += kThreads)
-    s.W4T[(i % kHid) * kOutPad + i / kHid] = p16[kOffW(3) + i];
+    s.W4T[(i % kHid) * kLd32 + i / kHid] = p16[kOffW(3) + i];
   for (int i = threadIdx.x; i < 4 * kHid; i += kThreads) (&s.db[0][0])[i] = 0.0f;
   if (threadIdx.x == 0) s.loss = 0.0f;
   const bool wrap = d_count != nullptr;
@@ -148,7 +160,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
     __syncthreads();
     encode_tile(s.act[0], pos, nrm, box, base, rows, offset, count, wrap);
     __syncthreads();
-    forward_rows(s.net, s.act[0], row0, keep, s.out);
+    forward_tile<1>(s.net, s.act[0], row0, keep, s.out);
     __syncwarp();
     // dL/dout of the warp's rows, lanes 0..15 one row each
     if (lane < 16) {
@@ -159,12 +171,12 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
       if (j < rows) {
         const uint64_t i = wrap ? ((uint64_t)offset + j) % count : j;
         const float d[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
-        l = mixture_nll_grad(&s.out[r * kOutPad], d, weight[i], gr);
+        l = mixture_nll_grad(&s.out[r * kOutLd], d, weight[i], gr);
       } else {
         for (int k = 0; k < kOut; ++k) gr[k] = 0.0f;
       }
       for (int k = 0; k < kOutPad; k += 2)
-        st32(&s.g[r * kOutPad + k], pack_h2_sat(k < kOut ? gr[k] * kGradScale : 0.0f,
+        st32(&s.g[r * kLd32 + k], pack_h2_sat(k < kOut ? gr[k] * kGradScale : 0.0f,
                                                  k + 1 < kOut ? gr[k + 1] * kGradScale : 0.0f));
       if (l != 0.0f) atomicAdd(&s.loss, l);
     }
@@ -173,19 +185,19 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
 #pragma unroll
     for (int kt = 0; kt < 2; ++kt) {
       const int c = 16 * kt + 2 * tq;
-      ga[kt][0] = ld32(&s.g[(row0 + g) * kOutPad + c]);
-      ga[kt][1] = ld32(&s.g[(row0 + g + 8) * kOutPad + c]);
-      ga[kt][2] = ld32(&s.g[(row0 + g) * kOutPad + c + 8]);
-      ga[kt][3] = ld32(&s.g[(row0 + g + 8) * kOutPad + c + 8]);
+      ga[kt][0] = ld32(&s.g[(row0 + g) * kLd32 + c]);
+      ga[kt][1] = ld32(&s.g[(row0 + g + 8) * kLd32 + c]);
+      ga[kt][2] = ld32(&s.g[(row0 + g) * kLd32 + c + 8]);
+      ga[kt][3] = ld32(&s.g[(row0 + g + 8) * kLd32 + c + 8]);
     }
     __syncthreads();  // every warp's G and activations are in shared memory
     for (int t2 = 0; t2 < 2; ++t2) {
       const int tile = warp * 2 + t2;
-      dw_tile(s.g, kOutPad, 16 * (tile / 8), s.act[3], 8 * (tile % 8), dw4[t2]);
+      dw_tile(s.g, kLd32, 16 * (tile / 8), s.act[3], 8 * (tile % 8), dw4[t2]);
     }
     if (threadIdx.x < kOutPad) {
       float acc = 0.0f;
-      for (int r = 0; r < kRows; ++r) acc += __half2float(s.g[r * kOutPad + threadIdx.x]);
+      for (int r = 0; r < kRows; ++r) acc += __half2float(s.g[r * kLd32 + threadIdx.x]);
       s.db[3][threadIdx.x] += acc;
     }
     // dA3 = G x W4: B operand (k = out, n = in) = W4T[in][out]
@@ -196,7 +208,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
 #pragma unroll
       for (int kt = 0; kt < 2; ++kt) {
         uint32_t b[2];
-        const __half* w = s.W4T + (8 * j + g) * kOutPad + 16 * kt + 2 * tq;
+        const __half* w = s.W4T + (8 * j + g) * kLd32 + 16 * kt + 2 * tq;
         b[0] = ld32(w);
         b[1] = ld32(w + 8);
         mma16816(acc[j], ga[kt], b);
@@ -209,21 +221,21 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
         const int c = 8 * j + 2 * tq;
-        const __half2 lo = *reinterpret_cast<const __half2*>(&A[(row0 + g) * 64 + c]);
-        const __half2 hi = *reinterpret_cast<const __half2*>(&A[(row0 + g + 8) * 64 + c]);
+        const __half2 lo = *reinterpret_cast<const __half2*>(&A[(row0 + g) * kLd + c]);
+        const __half2 hi = *reinterpret_cast<const __half2*>(&A[(row0 + g + 8) * kLd + c]);
         if (!(__low2float(lo) > 0.0f)) acc[j][0] = 0.0f;
         if (!(__high2float(lo) > 0.0f)) acc[j][1] = 0.0f;
         if (!(__low2float(hi) > 0.0f)) acc[j][2] = 0.0f;
         if (!(__high2float(hi) > 0.0f)) acc[j][3] = 0.0f;
-        st32(&s.dz[(row0 + g) * 64 + c], pack_h2_sat(acc[j][0], acc[j][1]));
-        st32(&s.dz[(row0 + g + 8) * 64 + c], pack_h2_sat(acc[j][2], acc[j][3]));
+        st32(&s.dz[(row0 + g) * kLd + c], pack_h2_sat(acc[j][0], acc[j][1]));
+        st32(&s.dz[(row0 + g + 8) * kLd + c], pack_h2_sat(acc[j][2], acc[j][3]));
       }
       __syncthreads();
       for (int qd = 0; qd < 4; ++qd)
-        dw_tile(s.dz, 64, 16 * (warp / 2), s.act[l], 8 * (4 * (warp % 2) + qd), dw[l][qd]);
+        dw_tile(s.dz, kLd, 16 * (warp / 2), s.act[l], 8 * (4 * (warp % 2) + qd), dw[l][qd]);
       if (threadIdx.x < kHid) {
         float sacc = 0.0f;
-        for (int r = 0; r < kRows; ++r) sacc += __half2float(s.dz[r * 64 + threadIdx.x]);
+        for (int r = 0; r < kRows; ++r) sacc += __half2float(s.dz[r * kLd + threadIdx.x]);
         s.db[l][threadIdx.x] += sacc;
       }
       if (l == 0) break;
@@ -236,7 +248,7 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
 #pragma unroll
         for (int kt = 0; kt < 4; ++kt) {
           uint32_t b[2];
-          const __half* w = s.WT[l] + (8 * j + g) * kHid + 16 * kt + 2 * tq;
+          const __half* w = s.WT[l] + (8 * j + g) * kLd + 16 * kt + 2 * tq;
           b[0] = ld32(w);
           b[1] = ld32(w + 8);
           mma16816(acc[j], a[kt], b);
@@ -343,7 +355,9 @@ int32_t bajo_mlp_forward(const void* d_params16, const float* d_pos, const float
   const size_t smem = sizeof(FwdSmem);
   if (cudaFuncSetAttribute(forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
     return BAJO_ERR_CUDA;
-  forward_kernel<<<grid_for(n), kThreads, smem, (cudaStream_t)stream>>>((const __half*)d_params16, d_pos, d_nrm,
+  uint64_t grid = ((uint64_t)n + 32 * kWarps - 1) / (32 * kWarps);
+  if (grid > 2 * (uint64_t)bajo::sm_count()) grid = 2 * (uint64_t)bajo::sm_count();
+  forward_kernel<<<(uint32_t)grid, kThreads, smem, (cudaStream_t)stream>>>((const __half*)d_params16, d_pos, d_nrm,
                                                                          d_box6, n, d_out20);
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }

@@ -110,12 +110,24 @@ __device__ __forceinline__ void encode_group(int grp, const float* p, const floa
   for (int k = 0; k < bins; k += 2) st32(row + col + k, pack_h2(blob_value(k, i0, i1, f), blob_value(k + 1, i0, i1, f)));
 }
 
+// every group of one sample's row
+__device__ __forceinline__ void encode_row(const float* p, const float* n, const float* box, __half* row) {
+#pragma unroll 1
+  for (int grp = 0; grp < 5; ++grp) encode_group(grp, p, n, box, row);
+}
+
 // ---------------------------------------------------------------------------
 // network in shared memory and the per-warp forward pass
 // ---------------------------------------------------------------------------
+// Shared-memory row strides: 64-wide FP16 tiles use 72 halves (144 B), so the
+// 8 rows a fragment load touches fall in distinct banks (a 128-byte stride
+// would put all 8 in one bank); 32-wide FP16 tiles use 40 halves; FP32
+// output tiles 36 floats.
+constexpr int kLd = 72, kLd32 = 40, kOutLd = 36;
+
 struct Net {
-  __half W[3][kHid * kIn];    // hidden layers, [out][in]
-  __half W4[kOutPad * kHid];  // output layer, [out][in]
+  __half W[3][kHid * kLd];    // hidden layers, [out][in]
+  __half W4[kOutPad * kLd];   // output layer, [out][in]
   float B[3][kHid];
   float B4[kOutPad];
 };
@@ -123,26 +135,27 @@ struct Net {
 template <int THREADS>
 __device__ void load_net(Net& s, const __half* __restrict__ p16) {
   const uint32_t* src = reinterpret_cast<const uint32_t*>(p16);
-  for (int i = threadIdx.x; i < kHid * kIn / 2; i += THREADS)
-    for (int l = 0; l < 3; ++l) reinterpret_cast<uint32_t*>(s.W[l])[i] = src[kOffW(l) / 2 + i];
+  for (int i = threadIdx.x; i < kHid * kIn / 2; i += THREADS) {
+    const int dst = (i >> 5) * (kLd / 2) + (i & 31);  // 32 words per source row
+    for (int l = 0; l < 3; ++l) reinterpret_cast<uint32_t*>(s.W[l])[dst] = src[kOffW(l) / 2 + i];
+  }
   for (int i = threadIdx.x; i < kOutPad * kHid / 2; i += THREADS)
-    reinterpret_cast<uint32_t*>(s.W4)[i] = src[kOffW(3) / 2 + i];
+    reinterpret_cast<uint32_t*>(s.W4)[(i >> 5) * (kLd / 2) + (i & 31)] = src[kOffW(3) / 2 + i];
   for (int i = threadIdx.x; i < kHid; i += THREADS)
     for (int l = 0; l < 3; ++l) s.B[l][i] = __half2float(p16[kOffB(l) + i]);
   for (int i = threadIdx.x; i < kOutPad; i += THREADS) s.B4[i] = __half2float(p16[kOffB(3) + i]);
 }
 
-// A fragments (4 k-tiles of 16) of 16 rows starting at row0 of a row-major
-// [rows x 64] half tile
+// A fragments (4 k-tiles of 16) of the 16 rows from row0 of a [rows x kLd] tile
 __device__ __forceinline__ void load_afrag64(const __half* t, int row0, uint32_t a[4][4]) {
   const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
 #pragma unroll
   for (int kt = 0; kt < 4; ++kt) {
     const int c = 16 * kt + 2 * tq;
-    a[kt][0] = ld32(t + (row0 + g) * 64 + c);
-    a[kt][1] = ld32(t + (row0 + g + 8) * 64 + c);
-    a[kt][2] = ld32(t + (row0 + g) * 64 + c + 8);
-    a[kt][3] = ld32(t + (row0 + g + 8) * 64 + c + 8);
+    a[kt][0] = ld32(t + (row0 + g) * kLd + c);
+    a[kt][1] = ld32(t + (row0 + g + 8) * kLd + c);
+    a[kt][2] = ld32(t + (row0 + g) * kLd + c + 8);
+    a[kt][3] = ld32(t + (row0 + g + 8) * kLd + c + 8);
   }
 }
 
@@ -151,32 +164,38 @@ __device__ __forceinline__ void store_afrag64(__half* t, int row0, const uint32_
 #pragma unroll
   for (int kt = 0; kt < 4; ++kt) {
     const int c = 16 * kt + 2 * tq;
-    st32(t + (row0 + g) * 64 + c, a[kt][0]);
-    st32(t + (row0 + g + 8) * 64 + c, a[kt][1]);
-    st32(t + (row0 + g) * 64 + c + 8, a[kt][2]);
-    st32(t + (row0 + g + 8) * 64 + c + 8, a[kt][3]);
+    st32(t + (row0 + g) * kLd + c, a[kt][0]);
+    st32(t + (row0 + g + 8) * kLd + c, a[kt][1]);
+    st32(t + (row0 + g) * kLd + c + 8, a[kt][2]);
+    st32(t + (row0 + g + 8) * kLd + c + 8, a[kt][3]);
   }
 }
 
-// one dense layer on 16 rows: acc[n-tile] = A x W^T + b, W [out][in]
-template <int NT, int KT>
-__device__ __forceinline__ void dense(const uint32_t a[][4], const __half* W, int in_dim, const float* bias,
-                                      float acc[][4]) {
+// one dense layer on MT m-tiles of 16 rows: acc[m][n-tile] = A x W^T + b,
+// W [out][in] with row stride kLd; each B fragment is loaded once for all
+// m-tiles
+template <int MT, int NT>
+__device__ __forceinline__ void dense(const uint32_t a[MT][4][4], const __half* W, const float* bias,
+                                      float acc[MT][NT][4]) {
   const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
 #pragma unroll
   for (int j = 0; j < NT; ++j) {
     const float b0 = bias[8 * j + 2 * tq], b1 = bias[8 * j + 2 * tq + 1];
-    acc[j][0] = b0;
-    acc[j][1] = b1;
-    acc[j][2] = b0;
-    acc[j][3] = b1;
 #pragma unroll
-    for (int kt = 0; kt < KT; ++kt) {
+    for (int m = 0; m < MT; ++m) {
+      acc[m][j][0] = b0;
+      acc[m][j][1] = b1;
+      acc[m][j][2] = b0;
+      acc[m][j][3] = b1;
+    }
+#pragma unroll
+    for (int kt = 0; kt < 4; ++kt) {
       uint32_t b[2];
-      const __half* w = W + (8 * j + g) * in_dim + 16 * kt + 2 * tq;
+      const __half* w = W + (8 * j + g) * kLd + 16 * kt + 2 * tq;
       b[0] = ld32(w);
       b[1] = ld32(w + 8);
-      mma16816(acc[j], a[kt], b);
+#pragma unroll
+      for (int m = 0; m < MT; ++m) mma16816(acc[m][j], a[m][kt], b);
     }
   }
 }
@@ -194,30 +213,45 @@ __device__ __forceinline__ void relu_to_afrag(const float acc[8][4], uint32_t a[
   }
 }
 
-// Forward of the warp's 16 rows (row0..row0+15) of the feature tile `x`;
-// hidden activations go to keep[0..2] when keep is non-null; the 32 padded
-// outputs to out[row * 32 + c].
-__device__ __forceinline__ void forward_rows(const Net& s, const __half* x, int row0, __half* const* keep,
+// Forward of MT m-tiles (rows row0 .. row0 + 16 MT - 1) of the feature tile
+// `x` ([rows x kLd]); hidden activations go to keep[0..2] (same layout) when
+// keep is non-null; the 32 padded outputs to out[row * kOutLd + c].
+template <int MT>
+__device__ __forceinline__ void forward_tile(const Net& s, const __half* x, int row0, __half* const* keep,
                                              float* out) {
-  uint32_t a[4][4];
-  float acc[8][4];
-  load_afrag64(x, row0, a);
+  uint32_t a[MT][4][4];
+  float acc[MT][8][4];
+#pragma unroll
+  for (int m = 0; m < MT; ++m) load_afrag64(x, row0 + 16 * m, a[m]);
 #pragma unroll
   for (int l = 0; l < 3; ++l) {
-    dense<8, 4>(a, s.W[l], kIn, s.B[l], acc);
-    relu_to_afrag(acc, a);
-    if (keep) store_afrag64(keep[l], row0, a);
+    dense<MT, 8>(a, s.W[l], s.B[l], acc);
+#pragma unroll
+    for (int m = 0; m < MT; ++m) {
+      relu_to_afrag(acc[m], a[m]);
+      if (keep) store_afrag64(keep[l], row0 + 16 * m, a[m]);
+    }
   }
-  float o[4][4];
-  dense<4, 4>(a, s.W4, kHid, s.B4, o);
+  float o[MT][4][4];
+  dense<MT, 4>(a, s.W4, s.B4, o);
   const int lane = threadIdx.x & 31, g = lane >> 2, tq = lane & 3;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    const int c = 8 * j + 2 * tq;
-    *reinterpret_cast<float2*>(&out[(row0 + g) * kOutPad + c]) = make_float2(o[j][0], o[j][1]);
-    *reinterpret_cast<float2*>(&out[(row0 + g + 8) * kOutPad + c]) = make_float2(o[j][2], o[j][3]);
-  }
+  for (int m = 0; m < MT; ++m)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = 8 * j + 2 * tq, r = row0 + 16 * m + g;
+      *reinterpret_cast<float2*>(&out[r * kOutLd + c]) = make_float2(o[m][j][0], o[m][j][1]);
+      *reinterpret_cast<float2*>(&out[(r + 8) * kOutLd + c]) = make_float2(o[m][j][2], o[m][j][3]);
+    }
 }
+
+// Per-warp working set of the warp-autonomous forward: 32 feature rows and
+// their 32 outputs.  A warp encodes, evaluates and consumes its own rows, so
+// no block-wide barrier is needed after the weights are loaded.
+struct WarpTile {
+  __half x[32 * kLd];
+  float out[32 * kOutLd];
+};
 
 // ---------------------------------------------------------------------------
 // vMF mixture: mean = m / len, len = sqrt(|m|^2 + 1e-12) (so d mean / dm =

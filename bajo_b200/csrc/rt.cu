@@ -1,15 +1,18 @@
-// rt.cu -- wavefront path tracing (PATH / NEE / MIS) of Lambertian + emissive
-// triangle scenes over the binary LBVH, on sm_100a.
+// rt.cu -- wavefront path tracing (PATH / NEE / MIS, and GUIDED with the
+// learned proposal of mlp.cuh) of Lambertian + emissive triangle scenes over
+// the binary LBVH, on sm_100a.
 //
 // Restates the reference's GPU wavefront renderer for triangle scenes:
 //  - primary rays: gpu_rt_primary_kernel (bajo/rt/gpu/common_kernels.mojo:22),
 //    Camera.make_ray_sampled (bajo/bvh/camera.mojo:156-209);
-//  - closest hit + fused shading: gpu_rt_scene_trace_kernel
+//  - closest hit + shading: gpu_rt_scene_trace_kernel
 //    (bajo/rt/gpu/scene_trace.mojo:41-369): sky on miss (bajo/rt/common.mojo:24),
 //    oriented normal (bajo/rt/geometry.mojo:20), next-event estimation with
 //    the alias-table light sample (bajo/rt/gpu/path_shading.mojo:261-413),
 //    MIS-weighted emission (:543-573), inline Lambertian sampling
-//    (bajo/rt/shading.mojo:92-118) and Russian roulette (bajo/rt/common.mojo:43);
+//    (bajo/rt/shading.mojo:92-118) and Russian roulette (bajo/rt/common.mojo:43),
+//    here split into a traversal kernel and a shading kernel joined by a
+//    vertex queue;
 //  - any-hit shadow rays (scene_trace.mojo:586);
 //  - per-pixel resolve (common_kernels.mojo:97).
 // Queues keep the reference's field-major ABI (bajo/rt/wavefront_contract.mojo:
@@ -156,28 +159,95 @@ __device__ __forceinline__ void accumulate(const Queues& q, uint32_t sidx, f3 v)
 }
 
 // ---------------------------------------------------------------------------
-// closest hit + shading of bounce `bounce` (gpu_rt_scene_trace_kernel and
-// _route_surface_hit / _shade_lambertian_inline, path_shading.mojo:460-590)
+// Bounce kernels.  Every bounce runs three launches over the queues:
+//  - trace_kernel<ALGO>: closest hit of every active path; sky on a miss,
+//    (MIS-weighted) emission on an emitter (_route_surface_hit,
+//    path_shading.mojo:543-573), Lambertian hits appended to a vertex queue;
+//  - shade_kernel<ALGO> (guided_shade_kernel for BAJO_RENDER_GUIDED): per
+//    vertex, next-event estimation (_sample_direct_light_candidate,
+//    path_shading.mojo:261-413) and the continuation (_sample_lambertian,
+//    bajo/rt/shading.mojo:92-118; russian_roulette, bajo/rt/common.mojo:43-67),
+//    appending shadow rays and next-bounce paths;
+//  - shadow_kernel: any-hit visibility of the light samples.
+// The reference fuses the first two in gpu_rt_scene_trace_kernel
+// (scene_trace.mojo:41-369).  Split, the traversal kernel keeps a smaller
+// register footprint and no shading divergence, and the guided tracer runs
+// its network between the two.  The arithmetic is the fused kernel's, so
+// images are unchanged bit for bit.
+// Guided tracing (BAJO_RENDER_GUIDED) draws the continuation by one-sample
+// MIS between the cosine BSDF and the network's vMF mixture and weighs every
+// MIS decision against that combined pdf.
 // ---------------------------------------------------------------------------
+constexpr int kVtxPlanes = 12;  // p xyz, oriented normal xyz, albedo rgb, throughput rgb
+constexpr int kShadeThreads = 256;
+
+struct ShadeCtx {
+  uint32_t* vtx_ids;
+  float* vtx;
+  uint32_t* vcount;     // [b] = Lambertian vertices of bounce b
+  // guided tracing only
+  const __half* params16;
+  const float* box;
+  float frac;           // probability of sampling the mixture
+  float rec_frac;       // probability a continued vertex becomes a training record
+  uint32_t rec_cap;
+  uint32_t* rec_hdr;    // [0] = records appended, [1] = first record of the chunk
+  float* rec_pos;
+  float* rec_nrm;
+  float* rec_dir;
+  float* rec_weight;
+  uint32_t* rec_sidx;
+  float* rec_tn;
+  float* rec_snap;
+  float* rec_wpre;
+};
+
+// integer hash "lowbias32" (C. Wellons, hash-prospector): record selection
+__device__ __forceinline__ uint32_t lowbias32(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// vMF direction around unit mean mu (Jakob, "Numerically stable sampling of
+// the von Mises-Fisher distribution on S^2", 2012): cos theta = 1 +
+// log(u + (1 - u) e^-2kappa) / kappa, azimuth 2 pi v, in the orthonormal
+// basis of Duff et al. (JCGT 2017).
+__device__ __forceinline__ f3 vmf_sample(const float* mu, float kappa, float u, float v) {
+  float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * kappa)) / kappa;
+  w = fminf(fmaxf(w, -1.0f), 1.0f);
+  const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
+  float sp, cp;
+  sincos_turns(v, sp, cp);
+  const float x = mu[0], y = mu[1], z = mu[2];
+  const float sgn = z >= 0.0f ? 1.0f : -1.0f;
+  const float a = -1.0f / (sgn + z);
+  const float b = x * y * a;
+  const f3 t1 = mk(1.0f + sgn * x * x * a, sgn * b, -sgn * x);
+  const f3 t2 = mk(b, sgn + y * y * a, -y);
+  const f3 d = (t1 * (st * cp) + t2 * (st * sp)) + mk(x, y, z) * w;
+  return normalize(d);
+}
+
 template <int ALGO>
-__global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queues q, uint32_t bounce,
-                                                             uint32_t max_depth, uint32_t sample_base,
-                                                             uint64_t seed) {
+__global__ void __launch_bounds__(kBlock) trace_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
+                                                       uint32_t sample_base) {
+  constexpr bool kMisWeights = ALGO == BAJO_RENDER_MIS || ALGO == BAJO_RENDER_GUIDED;
   const uint32_t count = q.counters[2 * bounce];
   const uint32_t cap = q.capacity;
   const uint32_t* src_ids = q.ids[bounce & 1];
   const float* src = q.fields[bounce & 1];
-  uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
-  float* dst = q.fields[(bounce + 1) & 1];
+  const uint32_t* src_rec = q.rec[bounce & 1];
   const uint32_t stride = gridDim.x * kBlock;
   for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
     const uint32_t idx = base + threadIdx.x;
-    const bool live = idx < count;
-    bool want_shadow = false, want_next = false;
-    f3 sh_o, sh_d, sh_c, nx_o, nx_d, nx_t;
-    float sh_tmax = 0.0f, nx_pdf = 0.0f;
+    bool want_vtx = false;
     uint32_t path_id = 0;
-    if (live) {
+    f3 vp, vn, va, vt;
+    if (idx < count) {
       const uint32_t idw = src_ids[idx];
       path_id = idw & kIdMask;
       const bool delta = (idw & kDeltaBit) != 0;
@@ -188,6 +258,14 @@ __global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queue
       const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
       const float prev_pdf = src[11 * cap + idx];
       const uint32_t sidx = path_id - sample_base;
+      if (ALGO == BAJO_RENDER_GUIDED) {
+        const uint32_t rec = src_rec[idx];
+        if (rec != kNoRecord) {  // radiance gathered before this ray: the record's baseline
+          c.rec_snap[3 * (size_t)rec + 0] = q.radiance[0 * cap + sidx];
+          c.rec_snap[3 * (size_t)rec + 1] = q.radiance[1 * cap + sidx];
+          c.rec_snap[3 * (size_t)rec + 2] = q.radiance[2 * cap + sidx];
+        }
+      }
       const Ray r = trav::make_ray(o, d, tmin, tmax);
       const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
                                                           q.status);
@@ -197,9 +275,9 @@ __global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queue
         const float t = h.t;
         const float4 a = __ldg(sc.tris + (size_t)h.leaf * 3 + 0);
         const float4 b = __ldg(sc.tris + (size_t)h.leaf * 3 + 1);
-        const float4 c = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
+        const float4 cc = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
         const f3 v0 = mk(a.x, a.y, a.z);
-        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(c.x, c.y, c.z) - v0));
+        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(cc.x, cc.y, cc.z) - v0));
         const bool front = dot(d, outward) < 0.0f;
         const f3 normal = front ? outward : neg(outward);
         const uint32_t surface = __ldg(sc.surfaces + h.prim);
@@ -210,7 +288,7 @@ __global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queue
             const f3 L = mk(sc.emissives[3 * midx], sc.emissives[3 * midx + 1], sc.emissives[3 * midx + 2]);
             float wgt = 1.0f;
             if (ALGO == BAJO_RENDER_NEE && bounce > 0 && !delta) wgt = 0.0f;
-            if (ALGO == BAJO_RENDER_MIS && bounce > 0 && !delta) {
+            if (kMisWeights && bounce > 0 && !delta) {
               const float lc = fmaxf(dot(normal, neg(normalize(d))), 0.0f);
               float lpdf = 0.0f;
               if (lc > 0.0f && sc.total_light_weight > 0.0f) {
@@ -223,116 +301,276 @@ __global__ void __launch_bounds__(kBlock) trace_shade_kernel(SceneView sc, Queue
             accumulate(q, sidx, mk(TL.x * wgt, TL.y * wgt, TL.z * wgt));
           }
         } else if (kind == BAJO_MAT_LAMBERTIAN) {
-          const f3 albedo = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
-          if ((ALGO == BAJO_RENDER_NEE || ALGO == BAJO_RENDER_MIS) && sc.n_lights > 0 &&
-              sc.total_light_weight > 0.0f) {
-            // _sample_direct_light_candidate, path_shading.mojo:261-413
-            const float4 u = uniform4(seed, path_id, stage_light(bounce));
-            const float as = u.x * (float)sc.n_lights;
-            uint32_t li = (uint32_t)as;
-            const float frac = as - (float)li;
-            const float* lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
-            if (frac > lrec[12]) li = __float_as_uint(lrec[13]);
-            lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
-            const f3 p0 = mk(lrec[0], lrec[1], lrec[2]), p1 = mk(lrec[3], lrec[4], lrec[5]),
-                     p2 = mk(lrec[6], lrec[7], lrec[8]);
-            const f3 e1 = p1 - p0, e2 = p2 - p0;
-            const f3 av = cross(e1, e2);
-            const float tas = length2(av);
-            if (tas > 0.0f) {
-              const f3 ln = divs(av, sqrtf(tas));
-              const float ru = sqrtf(u.y);
-              const float b1 = ru * (1.0f - u.z);
-              const float b2 = ru - b1;
-              const f3 lp = (p0 + e1 * b1) + e2 * b2;
-              const f3 tl = lp - p;
-              const float d2 = length2(tl);
-              if (d2 > 1.0e-8f) {
-                const float dist = sqrtf(d2);
-                const f3 dir = divs(tl, dist);
-                const float scos = fmaxf(dot(normal, dir), 0.0f);
-                const float lcos = fmaxf(dot(ln, neg(dir)), 0.0f);
-                const float smax = dist - 0.002f;
-                if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
-                  const f3 E = mk(lrec[9], lrec[10], lrec[11]);
-                  const float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * sc.total_light_weight);
-                  const float bpdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
-                  if (lpdf > 0.0f && bpdf > 0.0f) {
-                    const float wgt = ALGO == BAJO_RENDER_MIS ? power_heuristic(lpdf, bpdf) : 1.0f;
-                    const float scale = (scos * wgt) / lpdf;
-                    if (scale > 0.0f) {
-                      const f3 value = albedo * kInvPi;
-                      const f3 tv = mul(mul(T, value), E);
-                      want_shadow = true;
-                      sh_o = p;
-                      sh_d = dir;
-                      sh_tmax = smax;
-                      sh_c = tv * scale;
-                    }
-                  }
-                }
-              }
-            }
-          }
-          if (bounce + 1 < max_depth) {
-            // _sample_lambertian, bajo/rt/shading.mojo:92-118
-            const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
-            const f3 dir = smp::lambertian_dir(normal, u.x, u.y);
-            const float pdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
-            f3 Tn = mul(T, albedo);
-            // russian_roulette, bajo/rt/common.mojo:43-67 (depth = bounce + 1)
-            bool alive = true;
-            if (bounce + 1 >= 5u) {
-              const float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
-              if (m <= 0.0f) alive = false;
-              else {
-                const float survival = fminf(fmaxf(m, 0.05f), 0.95f);
-                const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
-                if (rr.x >= survival) alive = false;
-                else Tn = divs(Tn, survival);
-              }
-            }
-            if (alive) {
-              want_next = true;
-              nx_o = p;
-              nx_d = dir;
-              nx_t = Tn;
-              nx_pdf = pdf;
-            }
-          }
+          want_vtx = true;
+          vp = p;
+          vn = normal;
+          va = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
+          vt = T;
         }
       }
     }
-    if (ALGO == BAJO_RENDER_NEE || ALGO == BAJO_RENDER_MIS) {
-      const uint32_t slot = warp_append(&q.counters[2 * bounce + 1], want_shadow);
-      if (want_shadow) {
-        if (slot < cap) {
-          q.shadow_ids[slot] = path_id;
-          float* f = q.shadow_fields;
-          f[0 * cap + slot] = sh_o.x; f[1 * cap + slot] = sh_o.y; f[2 * cap + slot] = sh_o.z;
-          f[3 * cap + slot] = 0.001f;
-          f[4 * cap + slot] = sh_d.x; f[5 * cap + slot] = sh_d.y; f[6 * cap + slot] = sh_d.z;
-          f[7 * cap + slot] = sh_tmax;
-          f[8 * cap + slot] = sh_c.x; f[9 * cap + slot] = sh_c.y; f[10 * cap + slot] = sh_c.z;
-        } else {
-          raise_status(q.status, BAJO_WAVE_SHADOW_OVERFLOW);
-        }
-      }
-    }
-    const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], want_next);
-    if (want_next) {
+    const uint32_t slot = warp_append(&c.vcount[bounce], want_vtx);
+    if (want_vtx) {
       if (slot < cap) {
-        dst_ids[slot] = path_id;  // delta = false after a Lambertian bounce
-        dst[0 * cap + slot] = nx_o.x; dst[1 * cap + slot] = nx_o.y; dst[2 * cap + slot] = nx_o.z;
-        dst[3 * cap + slot] = 0.001f;
-        dst[4 * cap + slot] = nx_d.x; dst[5 * cap + slot] = nx_d.y; dst[6 * cap + slot] = nx_d.z;
-        dst[7 * cap + slot] = FLT_MAX;
-        dst[8 * cap + slot] = nx_t.x; dst[9 * cap + slot] = nx_t.y; dst[10 * cap + slot] = nx_t.z;
-        dst[11 * cap + slot] = nx_pdf;
+        c.vtx_ids[slot] = path_id;
+        float* f = c.vtx;
+        f[0 * cap + slot] = vp.x; f[1 * cap + slot] = vp.y; f[2 * cap + slot] = vp.z;
+        f[3 * cap + slot] = vn.x; f[4 * cap + slot] = vn.y; f[5 * cap + slot] = vn.z;
+        f[6 * cap + slot] = va.x; f[7 * cap + slot] = va.y; f[8 * cap + slot] = va.z;
+        f[9 * cap + slot] = vt.x; f[10 * cap + slot] = vt.y; f[11 * cap + slot] = vt.z;
       } else {
         raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
       }
     }
+  }
+}
+
+struct ShadeOut {
+  bool want_shadow = false, want_next = false, want_rec = false;
+  f3 sh_o, sh_d, sh_c, nx_o, nx_d, nx_t, normal;
+  float sh_tmax = 0.0f, nx_pdf = 0.0f, wpre = 0.0f;
+  uint32_t path_id = 0;
+};
+
+// Next-event estimation and continuation of vertex i of bounce `bounce`.
+template <int ALGO>
+__device__ __forceinline__ void shade_vertex(const SceneView& sc, const ShadeCtx& c, uint32_t cap, uint32_t i,
+                                             uint32_t bounce, uint32_t max_depth, uint64_t seed,
+                                             const mlp::Mixture& mix, ShadeOut& o) {
+  constexpr bool kGuided = ALGO == BAJO_RENDER_GUIDED;
+  const float g = kGuided ? c.frac : 0.0f;
+  const uint32_t path_id = c.vtx_ids[i];
+  o.path_id = path_id;
+  const f3 p = mk(c.vtx[0 * cap + i], c.vtx[1 * cap + i], c.vtx[2 * cap + i]);
+  const f3 normal = mk(c.vtx[3 * cap + i], c.vtx[4 * cap + i], c.vtx[5 * cap + i]);
+  o.normal = normal;
+  const f3 albedo = mk(c.vtx[6 * cap + i], c.vtx[7 * cap + i], c.vtx[8 * cap + i]);
+  const f3 T = mk(c.vtx[9 * cap + i], c.vtx[10 * cap + i], c.vtx[11 * cap + i]);
+  if ((ALGO == BAJO_RENDER_NEE || ALGO == BAJO_RENDER_MIS || kGuided) && sc.n_lights > 0 &&
+      sc.total_light_weight > 0.0f) {
+    // _sample_direct_light_candidate, path_shading.mojo:261-413
+    const float4 u = uniform4(seed, path_id, stage_light(bounce));
+    const float as = u.x * (float)sc.n_lights;
+    uint32_t li = (uint32_t)as;
+    const float frac = as - (float)li;
+    const float* lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+    if (frac > lrec[12]) li = __float_as_uint(lrec[13]);
+    lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
+    const f3 p0 = mk(lrec[0], lrec[1], lrec[2]), p1 = mk(lrec[3], lrec[4], lrec[5]),
+             p2 = mk(lrec[6], lrec[7], lrec[8]);
+    const f3 e1 = p1 - p0, e2 = p2 - p0;
+    const f3 av = cross(e1, e2);
+    const float tas = length2(av);
+    if (tas > 0.0f) {
+      const f3 ln = divs(av, sqrtf(tas));
+      const float ru = sqrtf(u.y);
+      const float b1 = ru * (1.0f - u.z);
+      const float b2 = ru - b1;
+      const f3 lp = (p0 + e1 * b1) + e2 * b2;
+      const f3 tl = lp - p;
+      const float d2 = length2(tl);
+      if (d2 > 1.0e-8f) {
+        const float dist = sqrtf(d2);
+        const f3 dir = divs(tl, dist);
+        const float scos = fmaxf(dot(normal, dir), 0.0f);
+        const float lcos = fmaxf(dot(ln, neg(dir)), 0.0f);
+        const float smax = dist - 0.002f;
+        if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
+          const f3 E = mk(lrec[9], lrec[10], lrec[11]);
+          const float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * sc.total_light_weight);
+          const float bpdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
+          if (lpdf > 0.0f && bpdf > 0.0f) {
+            float wgt = 1.0f;
+            if (ALGO == BAJO_RENDER_MIS) wgt = power_heuristic(lpdf, bpdf);
+            if (kGuided) {
+              const float dd[3] = {dir.x, dir.y, dir.z};
+              const float qpdf = (1.0f - g) * bpdf + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
+              wgt = power_heuristic(lpdf, qpdf);
+            }
+            const float scale = (scos * wgt) / lpdf;
+            if (scale > 0.0f) {
+              const f3 value = albedo * kInvPi;
+              const f3 tv = mul(mul(T, value), E);
+              o.want_shadow = true;
+              o.sh_o = p;
+              o.sh_d = dir;
+              o.sh_tmax = smax;
+              o.sh_c = tv * scale;
+            }
+          }
+        }
+      }
+    }
+  }
+  if (bounce + 1 < max_depth) {
+    const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
+    f3 dir;
+    if (kGuided && u.w < g) {
+      int k = 0;
+      float acc = mix.pi[0];
+      while (k < mlp::kLobes - 1 && u.z >= acc) acc += mix.pi[++k];
+      dir = vmf_sample(mix.mu[k], mix.kap[k], u.x, u.y);
+    } else {
+      dir = smp::lambertian_dir(normal, u.x, u.y);
+    }
+    const float cosv = fmaxf(dot(normal, normalize(dir)), 0.0f);
+    const float bp = cosv * kInvPi;
+    if (!kGuided || bp > 0.0f) {
+      float qpdf = bp;
+      f3 Tn = mul(T, albedo);
+      if (kGuided) {
+        const float dd[3] = {dir.x, dir.y, dir.z};
+        qpdf = (1.0f - g) * bp + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
+        const float factor = bp / qpdf;
+        if (factor != 1.0f) Tn = Tn * factor;
+      }
+      bool alive = !kGuided || qpdf > 0.0f;
+      if (alive && bounce + 1 >= 5u) {
+        const float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+        if (m <= 0.0f) alive = false;
+        else {
+          const float survival = fminf(fmaxf(m, 0.05f), 0.95f);
+          const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
+          if (rr.x >= survival) alive = false;
+          else Tn = divs(Tn, survival);
+        }
+      }
+      if (alive) {
+        o.want_next = true;
+        o.nx_o = p;
+        o.nx_d = dir;
+        o.nx_t = Tn;
+        o.nx_pdf = qpdf;
+        if (kGuided) {
+          o.wpre = cosv / qpdf;
+          const uint32_t h = lowbias32(path_id ^ lowbias32(bounce * 0x9E3779B9u + (uint32_t)seed));
+          o.want_rec = c.rec_cap > 0 && (float)(h >> 8) * (1.0f / 16777216.0f) < c.rec_frac;
+        }
+      }
+    }
+  }
+}
+
+// Queue appends of one shaded vertex; every lane of the warp calls this.
+template <int ALGO>
+__device__ __forceinline__ void emit(const Queues& q, const ShadeCtx& c, uint32_t bounce, uint32_t sample_base,
+                                     const ShadeOut& o) {
+  const uint32_t cap = q.capacity;
+  if (ALGO != BAJO_RENDER_PATH) {
+    const uint32_t sslot = warp_append(&q.counters[2 * bounce + 1], o.want_shadow);
+    if (o.want_shadow) {
+      if (sslot < cap) {
+        q.shadow_ids[sslot] = o.path_id;
+        float* f = q.shadow_fields;
+        f[0 * cap + sslot] = o.sh_o.x; f[1 * cap + sslot] = o.sh_o.y; f[2 * cap + sslot] = o.sh_o.z;
+        f[3 * cap + sslot] = 0.001f;
+        f[4 * cap + sslot] = o.sh_d.x; f[5 * cap + sslot] = o.sh_d.y; f[6 * cap + sslot] = o.sh_d.z;
+        f[7 * cap + sslot] = o.sh_tmax;
+        f[8 * cap + sslot] = o.sh_c.x; f[9 * cap + sslot] = o.sh_c.y; f[10 * cap + sslot] = o.sh_c.z;
+      } else {
+        raise_status(q.status, BAJO_WAVE_SHADOW_OVERFLOW);
+      }
+    }
+  }
+  const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], o.want_next);
+  uint32_t rslot = kNoRecord;
+  if (ALGO == BAJO_RENDER_GUIDED) rslot = warp_append(&c.rec_hdr[0], o.want_rec);
+  if (o.want_next) {
+    if (slot < cap) {
+      uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
+      float* dst = q.fields[(bounce + 1) & 1];
+      if (ALGO == BAJO_RENDER_GUIDED) {
+        const uint32_t sidx = o.path_id - sample_base;
+        uint32_t rec = kNoRecord;
+        if (o.want_rec && rslot < c.rec_cap) {
+          rec = rslot;
+          const size_t r3 = 3 * (size_t)rslot;
+          c.rec_pos[r3] = o.nx_o.x; c.rec_pos[r3 + 1] = o.nx_o.y; c.rec_pos[r3 + 2] = o.nx_o.z;
+          c.rec_nrm[r3] = o.normal.x; c.rec_nrm[r3 + 1] = o.normal.y; c.rec_nrm[r3 + 2] = o.normal.z;
+          c.rec_dir[r3] = o.nx_d.x; c.rec_dir[r3 + 1] = o.nx_d.y; c.rec_dir[r3 + 2] = o.nx_d.z;
+          c.rec_tn[r3] = o.nx_t.x; c.rec_tn[r3 + 1] = o.nx_t.y; c.rec_tn[r3 + 2] = o.nx_t.z;
+          c.rec_snap[r3] = q.radiance[0 * cap + sidx];
+          c.rec_snap[r3 + 1] = q.radiance[1 * cap + sidx];
+          c.rec_snap[r3 + 2] = q.radiance[2 * cap + sidx];
+          c.rec_sidx[rslot] = sidx;
+          c.rec_wpre[rslot] = o.wpre;
+          c.rec_weight[rslot] = 0.0f;
+        }
+        q.rec[(bounce + 1) & 1][slot] = rec;
+      }
+      dst_ids[slot] = o.path_id;  // delta = false after a Lambertian bounce
+      dst[0 * cap + slot] = o.nx_o.x; dst[1 * cap + slot] = o.nx_o.y; dst[2 * cap + slot] = o.nx_o.z;
+      dst[3 * cap + slot] = 0.001f;
+      dst[4 * cap + slot] = o.nx_d.x; dst[5 * cap + slot] = o.nx_d.y; dst[6 * cap + slot] = o.nx_d.z;
+      dst[7 * cap + slot] = FLT_MAX;
+      dst[8 * cap + slot] = o.nx_t.x; dst[9 * cap + slot] = o.nx_t.y; dst[10 * cap + slot] = o.nx_t.z;
+      dst[11 * cap + slot] = o.nx_pdf;
+    } else {
+      raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
+    }
+  }
+}
+
+template <int ALGO>
+__global__ void __launch_bounds__(kBlock) shade_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
+                                                       uint32_t max_depth, uint32_t sample_base, uint64_t seed) {
+  const uint32_t cap = q.capacity;
+  const uint32_t count = min(c.vcount[bounce], cap);
+  const mlp::Mixture none{};
+  for (uint32_t base = blockIdx.x * kBlock; base < count; base += gridDim.x * kBlock) {
+    const uint32_t i = base + threadIdx.x;
+    ShadeOut o;
+    if (i < count) shade_vertex<ALGO>(sc, c, cap, i, bounce, max_depth, seed, none, o);
+    emit<ALGO>(q, c, bounce, sample_base, o);
+  }
+}
+
+struct ShadeSmem {
+  mlp::Net net;
+  mlp::WarpTile tile[kShadeThreads / 32];
+};
+
+// Guided shading.  Warp-autonomous: each warp takes 32 vertices, encodes one
+// per lane, runs the network on its 32 rows (two m16 tiles on the tensor
+// cores), then every lane shades its own vertex; only the weight load is
+// block-wide.
+__global__ void __launch_bounds__(kShadeThreads, 2) guided_shade_kernel(SceneView sc, Queues q, ShadeCtx c,
+                                                                        uint32_t bounce, uint32_t max_depth,
+                                                                        uint32_t sample_base, uint64_t seed) {
+  extern __shared__ __align__(16) unsigned char raw[];
+  ShadeSmem& s = *reinterpret_cast<ShadeSmem*>(raw);
+  mlp::load_net<kShadeThreads>(s.net, c.params16);
+  __syncthreads();
+  const uint32_t cap = q.capacity;
+  const uint32_t count = min(c.vcount[bounce], cap);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  mlp::WarpTile& tile = s.tile[warp];
+  const uint32_t warps = gridDim.x * (kShadeThreads / 32);
+  for (uint32_t base = (blockIdx.x * (kShadeThreads / 32) + warp) * 32; base < count; base += warps * 32) {
+    const uint32_t i = base + lane;
+    {
+      __half* row = tile.x + lane * mlp::kLd;
+      if (i < count) {
+        const float p[3] = {c.vtx[0 * cap + i], c.vtx[1 * cap + i], c.vtx[2 * cap + i]};
+        const float n[3] = {c.vtx[3 * cap + i], c.vtx[4 * cap + i], c.vtx[5 * cap + i]};
+        mlp::encode_row(p, n, c.box, row);
+      } else {
+        for (int k = 0; k < mlp::kIn; k += 2) mlp::st32(row + k, 0u);
+      }
+    }
+    __syncwarp();
+    // one m16 tile at a time: two at once spill under the 128-register cap
+    mlp::forward_tile<1>(s.net, tile.x, 0, nullptr, tile.out);
+    mlp::forward_tile<1>(s.net, tile.x, 16, nullptr, tile.out);
+    __syncwarp();
+    ShadeOut o;
+    if (i < count) {
+      mlp::Mixture mix;
+      mlp::mixture_from_outputs(&tile.out[lane * mlp::kOutLd], mix);
+      shade_vertex<BAJO_RENDER_GUIDED>(sc, c, cap, i, bounce, max_depth, seed, mix, o);
+    }
+    emit<BAJO_RENDER_GUIDED>(q, c, bounce, sample_base, o);
+    __syncwarp();
   }
 }
 
@@ -404,357 +642,12 @@ __global__ void __launch_bounds__(kBlock) resolve_kernel(const float* __restrict
   }
 }
 
-// ---------------------------------------------------------------------------
-// guided tracing (BAJO_RENDER_GUIDED): MIS tracing whose continuation comes
-// from one-sample MIS between the cosine BSDF and the network's vMF mixture.
-// Per bounce: guided_trace_kernel (closest hit, sky, MIS-weighted emission,
-// Lambertian vertices -> vertex queue), guided_shade_kernel (network on the
-// tensor cores over 128-vertex tiles, then NEE + continuation per vertex),
-// shadow_kernel.
-// ---------------------------------------------------------------------------
-constexpr int kVtxPlanes = 12;  // p xyz, oriented normal xyz, albedo rgb, throughput rgb
-constexpr int kShadeThreads = 256, kShadeRows = 128;
-
-struct GuideCtx {
-  const __half* params16;
-  const float* box;
-  float frac;           // probability of sampling the mixture
-  float rec_frac;       // probability a continued vertex becomes a training record
-  uint32_t rec_cap;
-  uint32_t* rec_hdr;    // [0] = records appended, [1] = first record of the chunk
-  float* rec_pos;
-  float* rec_nrm;
-  float* rec_dir;
-  float* rec_weight;
-  uint32_t* rec_sidx;
-  float* rec_tn;
-  float* rec_snap;
-  float* rec_wpre;
-  uint32_t* vtx_ids;
-  float* vtx;
-  uint32_t* vcount;     // [b] = Lambertian vertices of bounce b
-};
-
-// integer hash "lowbias32" (C. Wellons, hash-prospector): record selection
-__device__ __forceinline__ uint32_t lowbias32(uint32_t x) {
-  x ^= x >> 16;
-  x *= 0x7feb352du;
-  x ^= x >> 15;
-  x *= 0x846ca68bu;
-  x ^= x >> 16;
-  return x;
-}
-
-// vMF direction around unit mean mu (Jakob, "Numerically stable sampling of
-// the von Mises-Fisher distribution on S^2", 2012): cos theta = 1 +
-// log(u + (1 - u) e^-2kappa) / kappa, azimuth 2 pi v, in the orthonormal
-// basis of Duff et al. (JCGT 2017).
-__device__ __forceinline__ f3 vmf_sample(const float* mu, float kappa, float u, float v) {
-  float w = 1.0f + logf(u + (1.0f - u) * expf(-2.0f * kappa)) / kappa;
-  w = fminf(fmaxf(w, -1.0f), 1.0f);
-  const float st = sqrtf(fmaxf(0.0f, 1.0f - w * w));
-  float sp, cp;
-  sincos_turns(v, sp, cp);
-  const float x = mu[0], y = mu[1], z = mu[2];
-  const float sgn = z >= 0.0f ? 1.0f : -1.0f;
-  const float a = -1.0f / (sgn + z);
-  const float b = x * y * a;
-  const f3 t1 = mk(1.0f + sgn * x * x * a, sgn * b, -sgn * x);
-  const f3 t2 = mk(b, sgn + y * y * a, -y);
-  const f3 d = (t1 * (st * cp) + t2 * (st * sp)) + mk(x, y, z) * w;
-  return normalize(d);
-}
-
-__global__ void __launch_bounds__(kBlock) guided_trace_kernel(SceneView sc, Queues q, GuideCtx gc, uint32_t bounce,
-                                                              uint32_t sample_base) {
-  const uint32_t count = q.counters[2 * bounce];
-  const uint32_t cap = q.capacity;
-  const uint32_t* src_ids = q.ids[bounce & 1];
-  const float* src = q.fields[bounce & 1];
-  const uint32_t* src_rec = q.rec[bounce & 1];
-  const uint32_t stride = gridDim.x * kBlock;
-  for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
-    const uint32_t idx = base + threadIdx.x;
-    bool want_vtx = false;
-    uint32_t path_id = 0;
-    f3 vp, vn, va, vt;
-    if (idx < count) {
-      const uint32_t idw = src_ids[idx];
-      path_id = idw & kIdMask;
-      const bool delta = (idw & kDeltaBit) != 0;
-      const f3 o = mk(src[0 * cap + idx], src[1 * cap + idx], src[2 * cap + idx]);
-      const float tmin = src[3 * cap + idx];
-      const f3 d = mk(src[4 * cap + idx], src[5 * cap + idx], src[6 * cap + idx]);
-      const float tmax = src[7 * cap + idx];
-      const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
-      const float prev_pdf = src[11 * cap + idx];
-      const uint32_t sidx = path_id - sample_base;
-      const uint32_t rec = src_rec[idx];
-      if (rec != kNoRecord) {  // radiance gathered before this ray: the record's baseline
-        gc.rec_snap[3 * (size_t)rec + 0] = q.radiance[0 * cap + sidx];
-        gc.rec_snap[3 * (size_t)rec + 1] = q.radiance[1 * cap + sidx];
-        gc.rec_snap[3 * (size_t)rec + 2] = q.radiance[2 * cap + sidx];
-      }
-      const Ray r = trav::make_ray(o, d, tmin, tmax);
-      const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
-                                                          q.status);
-      if (h.leaf == kEmpty) {
-        accumulate(q, sidx, mul(T, sky(d)));
-      } else {
-        const float t = h.t;
-        const float4 a = __ldg(sc.tris + (size_t)h.leaf * 3 + 0);
-        const float4 b = __ldg(sc.tris + (size_t)h.leaf * 3 + 1);
-        const float4 c = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
-        const f3 v0 = mk(a.x, a.y, a.z);
-        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(c.x, c.y, c.z) - v0));
-        const bool front = dot(d, outward) < 0.0f;
-        const f3 normal = front ? outward : neg(outward);
-        const uint32_t surface = __ldg(sc.surfaces + h.prim);
-        const uint32_t kind = surface >> 28, midx = surface & kIndexMask28;
-        const f3 p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
-        if (kind == BAJO_MAT_EMISSIVE) {
-          if (front) {
-            const f3 L = mk(sc.emissives[3 * midx], sc.emissives[3 * midx + 1], sc.emissives[3 * midx + 2]);
-            float wgt = 1.0f;
-            if (bounce > 0 && !delta) {
-              const float lc = fmaxf(dot(normal, neg(normalize(d))), 0.0f);
-              float lpdf = 0.0f;
-              if (lc > 0.0f && sc.total_light_weight > 0.0f) {
-                const float d2 = (t * t) * length2(d);
-                lpdf = (d2 * ((L.x + L.y) + L.z)) / ((3.0f * lc) * sc.total_light_weight);
-              }
-              wgt = power_heuristic(prev_pdf, lpdf);
-            }
-            const f3 TL = mul(T, L);
-            accumulate(q, sidx, mk(TL.x * wgt, TL.y * wgt, TL.z * wgt));
-          }
-        } else if (kind == BAJO_MAT_LAMBERTIAN) {
-          want_vtx = true;
-          vp = p;
-          vn = normal;
-          va = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
-          vt = T;
-        }
-      }
-    }
-    const uint32_t slot = warp_append(&gc.vcount[bounce], want_vtx);
-    if (want_vtx) {
-      if (slot < cap) {
-        gc.vtx_ids[slot] = path_id;
-        float* f = gc.vtx;
-        f[0 * cap + slot] = vp.x; f[1 * cap + slot] = vp.y; f[2 * cap + slot] = vp.z;
-        f[3 * cap + slot] = vn.x; f[4 * cap + slot] = vn.y; f[5 * cap + slot] = vn.z;
-        f[6 * cap + slot] = va.x; f[7 * cap + slot] = va.y; f[8 * cap + slot] = va.z;
-        f[9 * cap + slot] = vt.x; f[10 * cap + slot] = vt.y; f[11 * cap + slot] = vt.z;
-      } else {
-        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
-      }
-    }
-  }
-}
-
-struct ShadeSmem {
-  mlp::Net net;
-  __half x[kShadeRows * 64];
-  float out[kShadeRows * mlp::kOutPad];
-};
-
-__global__ void __launch_bounds__(kShadeThreads) guided_shade_kernel(SceneView sc, Queues q, GuideCtx gc,
-                                                                     uint32_t bounce, uint32_t max_depth,
-                                                                     uint32_t sample_base, uint64_t seed) {
-  extern __shared__ __align__(16) unsigned char raw[];
-  ShadeSmem& s = *reinterpret_cast<ShadeSmem*>(raw);
-  mlp::load_net<kShadeThreads>(s.net, gc.params16);
-  const uint32_t count = min(gc.vcount[bounce], q.capacity);
-  const uint32_t cap = q.capacity;
-  uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
-  float* dst = q.fields[(bounce + 1) & 1];
-  uint32_t* dst_rec = q.rec[(bounce + 1) & 1];
-  const float g = gc.frac;
-  const int warp = threadIdx.x >> 5;
-  for (uint32_t base = blockIdx.x * kShadeRows; base < count; base += gridDim.x * kShadeRows) {
-    __syncthreads();
-    for (int w = threadIdx.x; w < kShadeRows * 5; w += kShadeThreads) {
-      const int r = w / 5, grp = w % 5;
-      const uint32_t i = base + r;
-      __half* row = s.x + r * 64;
-      if (i < count) {
-        const float p[3] = {gc.vtx[0 * cap + i], gc.vtx[1 * cap + i], gc.vtx[2 * cap + i]};
-        const float n[3] = {gc.vtx[3 * cap + i], gc.vtx[4 * cap + i], gc.vtx[5 * cap + i]};
-        mlp::encode_group(grp, p, n, gc.box, row);
-      } else {
-        const int col = grp < 3 ? grp * mlp::kPosBins : 3 * mlp::kPosBins + (grp - 3) * mlp::kDirBins;
-        const int bins = grp < 3 ? mlp::kPosBins : mlp::kDirBins;
-        for (int k = 0; k < bins; k += 2) mlp::st32(row + col + k, 0u);
-      }
-    }
-    __syncthreads();
-    mlp::forward_rows(s.net, s.x, warp * 16, nullptr, s.out);
-    __syncthreads();
-    if (threadIdx.x >= kShadeRows) continue;  // warps 0..3 shade one vertex per thread
-    const uint32_t i = base + threadIdx.x;
-    bool want_shadow = false, want_next = false, want_rec = false;
-    f3 sh_o, sh_d, sh_c, nx_o, nx_d, nx_t;
-    float sh_tmax = 0.0f, nx_pdf = 0.0f, wpre = 0.0f;
-    uint32_t path_id = 0;
-    f3 normal;
-    if (i < count) {
-      path_id = gc.vtx_ids[i];
-      const f3 p = mk(gc.vtx[0 * cap + i], gc.vtx[1 * cap + i], gc.vtx[2 * cap + i]);
-      normal = mk(gc.vtx[3 * cap + i], gc.vtx[4 * cap + i], gc.vtx[5 * cap + i]);
-      const f3 albedo = mk(gc.vtx[6 * cap + i], gc.vtx[7 * cap + i], gc.vtx[8 * cap + i]);
-      const f3 T = mk(gc.vtx[9 * cap + i], gc.vtx[10 * cap + i], gc.vtx[11 * cap + i]);
-      mlp::Mixture mix;
-      mlp::mixture_from_outputs(&s.out[threadIdx.x * mlp::kOutPad], mix);
-      if (sc.n_lights > 0 && sc.total_light_weight > 0.0f) {
-        // light sample as in MIS tracing; its MIS weight is against the
-        // combined continuation pdf
-        const float4 u = uniform4(seed, path_id, stage_light(bounce));
-        const float as = u.x * (float)sc.n_lights;
-        uint32_t li = (uint32_t)as;
-        const float frac = as - (float)li;
-        const float* lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
-        if (frac > lrec[12]) li = __float_as_uint(lrec[13]);
-        lrec = sc.lights + (size_t)li * BAJO_LIGHT_STRIDE;
-        const f3 p0 = mk(lrec[0], lrec[1], lrec[2]), p1 = mk(lrec[3], lrec[4], lrec[5]),
-                 p2 = mk(lrec[6], lrec[7], lrec[8]);
-        const f3 e1 = p1 - p0, e2 = p2 - p0;
-        const f3 av = cross(e1, e2);
-        const float tas = length2(av);
-        if (tas > 0.0f) {
-          const f3 ln = divs(av, sqrtf(tas));
-          const float ru = sqrtf(u.y);
-          const float b1 = ru * (1.0f - u.z);
-          const float b2 = ru - b1;
-          const f3 lp = (p0 + e1 * b1) + e2 * b2;
-          const f3 tl = lp - p;
-          const float d2 = length2(tl);
-          if (d2 > 1.0e-8f) {
-            const float dist = sqrtf(d2);
-            const f3 dir = divs(tl, dist);
-            const float scos = fmaxf(dot(normal, dir), 0.0f);
-            const float lcos = fmaxf(dot(ln, neg(dir)), 0.0f);
-            const float smax = dist - 0.002f;
-            if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
-              const f3 E = mk(lrec[9], lrec[10], lrec[11]);
-              const float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * sc.total_light_weight);
-              const float bpdf = fmaxf(dot(normal, normalize(dir)), 0.0f) * kInvPi;
-              const float dd[3] = {dir.x, dir.y, dir.z};
-              const float qpdf = (1.0f - g) * bpdf + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
-              if (lpdf > 0.0f && bpdf > 0.0f) {
-                const float scale = (scos * power_heuristic(lpdf, qpdf)) / lpdf;
-                if (scale > 0.0f) {
-                  want_shadow = true;
-                  sh_o = p;
-                  sh_d = dir;
-                  sh_tmax = smax;
-                  sh_c = mul(mul(T, albedo * kInvPi), E) * scale;
-                }
-              }
-            }
-          }
-        }
-      }
-      if (bounce + 1 < max_depth) {
-        const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
-        f3 dir;
-        if (u.w < g) {
-          int k = 0;
-          float acc = mix.pi[0];
-          while (k < mlp::kLobes - 1 && u.z >= acc) acc += mix.pi[++k];
-          dir = vmf_sample(mix.mu[k], mix.kap[k], u.x, u.y);
-        } else {
-          dir = smp::lambertian_dir(normal, u.x, u.y);
-        }
-        // cosine and BSDF pdf as the MIS tracer forms them, so that f = 0
-        // reproduces it exactly (factor 1, same stored pdf)
-        const float cosv = fmaxf(dot(normal, normalize(dir)), 0.0f);
-        const float bp = cosv * kInvPi;
-        if (bp > 0.0f) {
-          const float dd[3] = {dir.x, dir.y, dir.z};
-          const float qpdf = (1.0f - g) * bp + (g > 0.0f ? g * mlp::mixture_pdf(mix, dd) : 0.0f);
-          const float factor = bp / qpdf;
-          f3 Tn = mul(T, albedo);
-          if (factor != 1.0f) Tn = Tn * factor;
-          bool alive = qpdf > 0.0f;
-          if (alive && bounce + 1 >= 5u) {
-            const float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
-            if (m <= 0.0f) alive = false;
-            else {
-              const float survival = fminf(fmaxf(m, 0.05f), 0.95f);
-              const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
-              if (rr.x >= survival) alive = false;
-              else Tn = divs(Tn, survival);
-            }
-          }
-          if (alive) {
-            want_next = true;
-            nx_o = p;
-            nx_d = dir;
-            nx_t = Tn;
-            nx_pdf = qpdf;
-            wpre = cosv / qpdf;
-            const uint32_t h = lowbias32(path_id ^ lowbias32(bounce * 0x9E3779B9u + (uint32_t)seed));
-            want_rec = gc.rec_cap > 0 && (float)(h >> 8) * (1.0f / 16777216.0f) < gc.rec_frac;
-          }
-        }
-      }
-    }
-    const uint32_t sslot = warp_append(&q.counters[2 * bounce + 1], want_shadow);
-    if (want_shadow) {
-      if (sslot < cap) {
-        q.shadow_ids[sslot] = path_id;
-        float* f = q.shadow_fields;
-        f[0 * cap + sslot] = sh_o.x; f[1 * cap + sslot] = sh_o.y; f[2 * cap + sslot] = sh_o.z;
-        f[3 * cap + sslot] = 0.001f;
-        f[4 * cap + sslot] = sh_d.x; f[5 * cap + sslot] = sh_d.y; f[6 * cap + sslot] = sh_d.z;
-        f[7 * cap + sslot] = sh_tmax;
-        f[8 * cap + sslot] = sh_c.x; f[9 * cap + sslot] = sh_c.y; f[10 * cap + sslot] = sh_c.z;
-      } else {
-        raise_status(q.status, BAJO_WAVE_SHADOW_OVERFLOW);
-      }
-    }
-    const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], want_next);
-    const uint32_t rslot = warp_append(&gc.rec_hdr[0], want_rec);
-    if (want_next) {
-      if (slot < cap) {
-        const uint32_t sidx = path_id - sample_base;
-        uint32_t rec = kNoRecord;
-        if (want_rec && rslot < gc.rec_cap) {
-          rec = rslot;
-          const size_t r3 = 3 * (size_t)rslot;
-          gc.rec_pos[r3] = nx_o.x; gc.rec_pos[r3 + 1] = nx_o.y; gc.rec_pos[r3 + 2] = nx_o.z;
-          gc.rec_nrm[r3] = normal.x; gc.rec_nrm[r3 + 1] = normal.y; gc.rec_nrm[r3 + 2] = normal.z;
-          gc.rec_dir[r3] = nx_d.x; gc.rec_dir[r3 + 1] = nx_d.y; gc.rec_dir[r3 + 2] = nx_d.z;
-          gc.rec_tn[r3] = nx_t.x; gc.rec_tn[r3 + 1] = nx_t.y; gc.rec_tn[r3 + 2] = nx_t.z;
-          gc.rec_snap[r3] = q.radiance[0 * cap + sidx];
-          gc.rec_snap[r3 + 1] = q.radiance[1 * cap + sidx];
-          gc.rec_snap[r3 + 2] = q.radiance[2 * cap + sidx];
-          gc.rec_sidx[rslot] = sidx;
-          gc.rec_wpre[rslot] = wpre;
-          gc.rec_weight[rslot] = 0.0f;
-        }
-        dst_rec[slot] = rec;
-        dst_ids[slot] = path_id;
-        dst[0 * cap + slot] = nx_o.x; dst[1 * cap + slot] = nx_o.y; dst[2 * cap + slot] = nx_o.z;
-        dst[3 * cap + slot] = 0.001f;
-        dst[4 * cap + slot] = nx_d.x; dst[5 * cap + slot] = nx_d.y; dst[6 * cap + slot] = nx_d.z;
-        dst[7 * cap + slot] = FLT_MAX;
-        dst[8 * cap + slot] = nx_t.x; dst[9 * cap + slot] = nx_t.y; dst[10 * cap + slot] = nx_t.z;
-        dst[11 * cap + slot] = nx_pdf;
-      } else {
-        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
-      }
-    }
-  }
-}
-
 // first record of the chunk = records appended so far (capped)
 __global__ void records_begin_chunk_kernel(uint32_t* hdr, uint32_t cap) { hdr[1] = min(hdr[0], cap); }
 
 // Records of the chunk: weight = mean_rgb((R_end - R_before) / T_after) *
 // cos / pdf, the radiance gathered after the vertex per unit throughput.
-__global__ void __launch_bounds__(kBlock) records_finish_chunk_kernel(GuideCtx gc, const float* __restrict__ radiance,
+__global__ void __launch_bounds__(kBlock) records_finish_chunk_kernel(ShadeCtx gc, const float* __restrict__ radiance,
                                                                       uint32_t cap) {
   const uint32_t start = gc.rec_hdr[1], end = min(gc.rec_hdr[0], gc.rec_cap);
   for (uint32_t i = start + blockIdx.x * kBlock + threadIdx.x; i < end; i += gridDim.x * kBlock) {
@@ -779,7 +672,8 @@ constexpr uint32_t kDefaultChunk = 1u << 22;
 struct Layout {
   uint32_t cap, pixels_per_chunk, n_counters;
   size_t off_counters, off_ids[2], off_fields[2], off_shadow_ids, off_shadow_fields, off_radiance;
-  size_t off_rec[2], off_vtx_ids, off_vtx;  // guided tracing only
+  size_t off_vtx_ids, off_vtx;  // vertex queue between the trace and shade kernels
+  size_t off_rec[2];            // guided tracing only
   size_t total;
 };
 
@@ -797,9 +691,9 @@ bool make_layout(const BajoRenderSettings* s, Layout* L) {
   const bool guided = s->algorithm == BAJO_RENDER_GUIDED;
   L->pixels_per_chunk = ppc;
   L->cap = ppc * s->spp;
-  // [2b] paths of bounce b, [2b+1] its shadow rays; guided: then the
-  // Lambertian vertices of every bounce
-  L->n_counters = 2 * s->max_depth + 2 + (guided ? s->max_depth : 0);
+  // [2b] paths of bounce b, [2b+1] its shadow rays, then [2 max_depth + 2 +
+  // b] the Lambertian vertices of bounce b
+  L->n_counters = 3 * s->max_depth + 2;
   const size_t cap = L->cap;
   size_t o = 256;  // status word, then two 64-bit ray totals at offset 8
   L->off_counters = o;
@@ -816,16 +710,16 @@ bool make_layout(const BajoRenderSettings* s, Layout* L) {
   o = a256(o + cap * 4 * kShadowPlanes);
   L->off_radiance = o;
   o = a256(o + cap * 4 * 3);
-  L->off_rec[0] = L->off_rec[1] = L->off_vtx_ids = L->off_vtx = 0;
+  L->off_vtx_ids = o;
+  o = a256(o + cap * 4);
+  L->off_vtx = o;
+  o = a256(o + cap * 4 * kVtxPlanes);
+  L->off_rec[0] = L->off_rec[1] = 0;
   if (guided) {
     for (int k = 0; k < 2; ++k) {
       L->off_rec[k] = o;
       o = a256(o + cap * 4);
     }
-    L->off_vtx_ids = o;
-    o = a256(o + cap * 4);
-    L->off_vtx = o;
-    o = a256(o + cap * 4 * kVtxPlanes);
   }
   L->total = o;
   return true;
@@ -862,12 +756,22 @@ bool make_views(const BajoRtScene* scene, unsigned char* w, const Layout& L, Sce
   return true;
 }
 
+ShadeCtx shade_ctx(unsigned char* w, const Layout& L, const Queues& q, uint32_t max_depth) {
+  ShadeCtx c{};
+  c.vtx_ids = (uint32_t*)(w + L.off_vtx_ids);
+  c.vtx = (float*)(w + L.off_vtx);
+  c.vcount = q.counters + 2 * max_depth + 2;
+  return c;
+}
+
 template <int ALGO>
-cudaError_t launch_bounce(const SceneView& sc, const Queues& q, uint32_t grid, uint32_t b, uint32_t max_depth,
-                          uint32_t sample_base, uint64_t seed, cudaStream_t st) {
-  trace_shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, b, max_depth, sample_base, seed);
+cudaError_t launch_bounce(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t grid, uint32_t b,
+                          uint32_t max_depth, uint32_t sample_base, uint64_t seed, cudaStream_t st) {
+  trace_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, sample_base);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
+  shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
+  if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (ALGO != BAJO_RENDER_PATH) {
     shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
     e = cudaGetLastError();
@@ -937,12 +841,13 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
   cudaStream_t st = (cudaStream_t)stream;
   const uint32_t grid = bounce_grid(L.cap);
   const int algo = s->algorithm;
+  const ShadeCtx c = shade_ctx(w, L, q, s->max_depth);
   auto bounce = [&](uint32_t b, uint32_t sample_base) {
     if (algo == BAJO_RENDER_PATH)
-      return launch_bounce<BAJO_RENDER_PATH>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
+      return launch_bounce<BAJO_RENDER_PATH>(sc, q, c, grid, b, s->max_depth, sample_base, s->seed, st);
     if (algo == BAJO_RENDER_NEE)
-      return launch_bounce<BAJO_RENDER_NEE>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
-    return launch_bounce<BAJO_RENDER_MIS>(sc, q, grid, b, s->max_depth, sample_base, s->seed, st);
+      return launch_bounce<BAJO_RENDER_NEE>(sc, q, c, grid, b, s->max_depth, sample_base, s->seed, st);
+    return launch_bounce<BAJO_RENDER_MIS>(sc, q, c, grid, b, s->max_depth, sample_base, s->seed, st);
   };
   auto none = []() { return cudaSuccess; };
   const cudaError_t e = render_chunks(s, L, q, d_camera, d_pixels, d_pixels64, (unsigned long long*)(w + 8), st,
@@ -967,7 +872,7 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   unsigned char* w = (unsigned char*)d_ws;
   if (!make_views(scene, w, L, sc, q)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
-  GuideCtx gc;
+  ShadeCtx gc = shade_ctx(w, L, q, s->max_depth);
   gc.params16 = (const __half*)guide->params16;
   gc.box = guide->box6;
   gc.frac = guide->guide_fraction;
@@ -987,9 +892,6 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   gc.rec_snap = rb ? (float*)(rb + RL.snap) : nullptr;
   gc.rec_wpre = rb ? (float*)(rb + RL.wpre) : nullptr;
   if (!rb) gc.rec_cap = 0;
-  gc.vtx_ids = (uint32_t*)(w + L.off_vtx_ids);
-  gc.vtx = (float*)(w + L.off_vtx);
-  gc.vcount = q.counters + 2 * s->max_depth + 2;
   const size_t smem = sizeof(ShadeSmem);
   if (cudaFuncSetAttribute(guided_shade_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
@@ -999,13 +901,13 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
           cudaSuccess ||
       per_sm < 1)
     return BAJO_ERR_CUDA;
-  uint32_t shade_grid = (L.cap + kShadeRows - 1) / kShadeRows;
+  uint32_t shade_grid = (L.cap + kShadeThreads - 1) / kShadeThreads;
   const uint32_t shade_max = (uint32_t)(sm_count() * per_sm);
   if (shade_grid > shade_max) shade_grid = shade_max;
   const uint32_t grid = bounce_grid(L.cap);
   if (!rb && cudaMemsetAsync(gc.rec_hdr, 0, 8, st) != cudaSuccess) return BAJO_ERR_CUDA;
   auto bounce = [&](uint32_t b, uint32_t sample_base) {
-    guided_trace_kernel<<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
+    trace_kernel<BAJO_RENDER_GUIDED><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     guided_shade_kernel<<<shade_grid, kShadeThreads, smem, st>>>(sc, q, gc, b, s->max_depth, sample_base, s->seed);

@@ -54,12 +54,20 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
-    p.add_argument("--case", default=None, choices=["sort", "build", "trace", "tune", "render", "batched"],
+    p.add_argument("--case", default=None,
+                   choices=["sort", "build", "trace", "tune", "render", "batched", "guided", "guided_pass"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
     p.add_argument("--end-bit", type=int, default=None, help="--case sort: sort bits [0, end-bit)")
     p.add_argument("--keys-only", action="store_true", help="--case sort without payload")
+    p.add_argument("--scene", default="spheres", choices=["spheres", "indirect"], help="--case guided scene")
+    p.add_argument("--width", type=int, default=1280, help="--case guided image width")
+    p.add_argument("--height", type=int, default=720, help="--case guided image height")
+    p.add_argument("--ref-spp", type=int, default=4096, help="--case guided reference samples per pixel")
+    p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
+    p.add_argument("--train-passes", type=int, default=8, help="--case guided passes followed by training")
+    p.add_argument("--train-steps", type=int, default=8, help="--case guided Adam steps per training pass")
     return p.parse_args()
 
 
@@ -546,6 +554,130 @@ def run_batched(steps, warmup, n_scenes=4096):
             "rays": rays, "status": g.status()}
 
 
+def run_guided(args):
+    """Learned guiding against plain MIS at equal wall time.
+
+    Scene: the path-tracing workload (64 icospheres in the lit box; or
+    ``--scene indirect``, the box lit only by a panel facing the ceiling),
+    1280x720, depth 8.  Error = MSE against a ``--ref-spp`` plain MIS render
+    accumulated in FP64.  Plain: one 64-spp MIS render, device-timed.
+    Guided: progressive passes of ``--spp-per-pass`` with the network trained
+    after each of the first ``--train-passes`` passes (training time counted);
+    after each pass the cumulative device time and the MSE (computed outside
+    the timed region) are logged until the guided image is at least as good
+    as the plain one or twice the plain time has passed."""
+    import torch
+    from bajo_b200 import guide, rt, scenes
+    stream = torch.cuda.current_stream()
+    w, h = args.width, args.height
+    sc = scenes.indirect_box_scene() if args.scene == "indirect" else scenes.spheres_in_box()
+    gsc = rt.GpuRtTriangleScene(sc)
+
+    def ev_time(fn):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        r = fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b), r
+
+    chunk = 64
+    st = rt.RenderSettings(w, h, chunk, max_depth=8)
+    ws = rt.RenderWorkspace(st, rt.MIS)
+    ref64 = torch.zeros((h, w, 3), dtype=torch.float64, device="cuda")
+    t_ref = 0.0
+    for k in range(args.ref_spp // chunk):
+        st.rng_seed = 900001 + k
+        t, _ = ev_time(lambda: rt.render_gpu_triangles(st, sc.camera, gsc, rt.MIS, workspace=ws, pixels64=ref64))
+        t_ref += t
+    ref = ref64 / (args.ref_spp // chunk * chunk)
+    # plain MIS, 64 spp (first call warms up)
+    st_plain = rt.RenderSettings(w, h, 64, rng_seed=2026, max_depth=8)
+    rt.render_gpu_triangles(st_plain, sc.camera, gsc, rt.MIS, workspace=ws)
+    t_plain, img = ev_time(lambda: rt.render_gpu_triangles(st_plain, sc.camera, gsc, rt.MIS, workspace=ws))
+    mse_plain = float(((img.double() - ref) ** 2).mean())
+    # guided, progressive
+    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=args.spp_per_pass, record_capacity=1 << 18,
+                              batch=1 << 14, steps=args.train_steps, lr=1e-2)
+    gr.render_pass(1, train=False)  # warm-up: kernel attributes, tuning table
+    torch.cuda.synchronize()
+    gr.reset_image()
+    gr.net = guide.GuideNetwork("cuda", seed=0)
+    log, t_g, reached = [], 0.0, None
+    k = 0
+    while t_g < 2.0 * t_plain and k < 4096:
+        train = k < args.train_passes
+        t, _ = ev_time(lambda: gr.render_pass(70001 + 7919 * k, train=train))
+        t_g += t
+        k += 1
+        mse = float(((gr.image() - ref) ** 2).mean())
+        log.append((round(t_g, 2), gr.samples, mse))
+        if reached is None and mse <= mse_plain:
+            reached = t_g
+            break
+    # MSE at equal time: last logged point not past t_plain
+    eq = [m for (t, _, m) in log if t <= t_plain]
+    # guided throughput with a trained network and no training
+    t_pass, _ = ev_time(lambda: gr.render_pass(5, train=False))
+    samples = w * h * args.spp_per_pass
+    rays, shadows = gr.workspace.ray_counts()
+    out = {"case": "guided", "scene": args.scene, "width": w, "height": h, "ref_spp": args.ref_spp,
+           "ref_ms": round(t_ref, 1), "plain_ms": round(t_plain, 2), "plain_mse": mse_plain,
+           "guided_ms_to_plain_mse": None if reached is None else round(reached, 2),
+           "time_ratio": None if reached is None else round(reached / t_plain, 3),
+           "guided_mse_at_plain_time": eq[-1] if eq else None,
+           "guided_spp_at_plain_time": max([s for (t, s, _) in log if t <= t_plain], default=0),
+           "guided_samples_s": round(samples / t_pass * 1e3, 1),
+           "plain_samples_s": round(w * h * 64 / t_plain * 1e3, 1),
+           "guided_mrays_s": round((rays + shadows) / t_pass / 1e3, 1),
+           "train_passes": args.train_passes, "spp_per_pass": args.spp_per_pass, "train_steps": args.train_steps,
+           "log": log[:: max(1, len(log) // 40)], "status": gr.workspace.status()}
+    return out
+
+
+def run_guided_pass(args):
+    """Throughput of guided passes with a network trained for
+    --train-passes passes first (no training in the timed passes), next to
+    plain MIS passes of the same size."""
+    import torch
+    from bajo_b200 import guide, rt, scenes
+    stream = torch.cuda.current_stream()
+    w, h, spp = args.width, args.height, args.spp_per_pass
+    sc = scenes.indirect_box_scene() if args.scene == "indirect" else scenes.spheres_in_box()
+    gsc = rt.GpuRtTriangleScene(sc)
+    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=spp, record_capacity=1 << 18, batch=1 << 14,
+                              steps=args.train_steps)
+    for k in range(args.train_passes):
+        gr.render_pass(11 + k, train=True)
+    st = rt.RenderSettings(w, h, spp, max_depth=8)
+    ws = rt.RenderWorkspace(st, rt.MIS)
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        ms = []
+        for _ in range(args.steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        return statistics.median(ms)
+
+    t_g = timed(lambda: gr.render_pass(5, train=False))
+    g_rays = sum(gr.workspace.ray_counts())
+    t_p = timed(lambda: rt.render_gpu_triangles(st, sc.camera, gsc, rt.MIS, workspace=ws))
+    p_rays = sum(ws.ray_counts())
+    n = w * h * spp
+    return {"case": "guided_pass", "scene": args.scene, "width": w, "height": h, "spp": spp,
+            "guided_ms": round(t_g, 3), "guided_samples_s": round(n / t_g * 1e3, 1),
+            "guided_mrays_s": round(g_rays / t_g / 1e3, 1), "plain_ms": round(t_p, 3),
+            "plain_samples_s": round(n / t_p * 1e3, 1), "plain_mrays_s": round(p_rays / t_p / 1e3, 1),
+            "status": gr.workspace.status() | ws.status()}
+
+
 def run_case(args):
     """One piece of the path alone, for ncu captures and tuning runs."""
     import torch
@@ -585,6 +717,10 @@ def run_case(args):
                     "triangles": sc.n_tris, "status": ws.status()})
     elif args.case == "batched":
         out.update(run_batched(args.steps, args.warmup))
+    elif args.case == "guided":
+        out = run_guided(args)
+    elif args.case == "guided_pass":
+        out = run_guided_pass(args)
     elif args.case == "tune":
         out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
         out["device"] = autotune.device_key()
