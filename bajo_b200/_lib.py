@@ -68,6 +68,19 @@ class BajoLbvhSizesC(ctypes.Structure):
     _fields_ = [(name, _SZ) for name in LBVH_ARRAYS] + [("workspace", _SZ)]
 
 
+class BajoWideBvhC(ctypes.Structure):
+    """Mirror of ``struct BajoWideBvh`` (include/bajo_b200.h)."""
+    _fields_ = [("width", _U32), ("n_segments", _U32), ("node_offsets", _P), ("leaf_offsets", _P), ("nodes", _P),
+                ("leaf_indices", _P), ("leaf_tris", _P), ("leaf_sorted", _P), ("bvh2_leaf_tris", _P)]
+
+
+WIDE_ARRAYS = ("node_offsets", "leaf_offsets", "nodes", "leaf_indices", "leaf_tris", "leaf_sorted")
+
+
+class BajoWideSizesC(ctypes.Structure):
+    _fields_ = [(name, _SZ) for name in WIDE_ARRAYS] + [("workspace", _SZ)]
+
+
 # every symbol the header declares, with its ctypes signature
 SIGNATURES = {
     "bajo_workspace_status": (_I32, [_P, _P, ctypes.POINTER(_U32)]),
@@ -94,6 +107,13 @@ SIGNATURES = {
     "bajo_render_workspace_size": (_I32, [_P, ctypes.POINTER(_SZ)]),
     "bajo_render": (_I32, [_P, _P, _P, _P, _P, _P, _SZ, _P]),
     "bajo_render_stats": (_I32, [_P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]),
+    "bajo_wide_sizes": (_I32, [_U32, _U32, _U32, ctypes.POINTER(BajoWideSizesC)]),
+    "bajo_wide_build": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoWideBvhC), _P, _SZ, _P]),
+    "bajo_wide_counts": (_I32, [ctypes.POINTER(BajoWideBvhC), _P, ctypes.POINTER(_U32), ctypes.POINTER(_U32)]),
+    "bajo_trace_wide_rays": (_I32, [ctypes.POINTER(BajoWideBvhC), _U32, _U32, _P, _U32, _I32, _P, _P, _P, _P,
+                                    _P]),
+    "bajo_trace_wide_camera": (_I32, [ctypes.POINTER(BajoWideBvhC), _U32, _U32, _P, _U32, _U32, _U32, _I32, _P, _P,
+                                      _P, _P, _P, _P]),
     "bajo_mlp_param_count": (_I32, [ctypes.POINTER(_U32)]),
     "bajo_mlp_forward": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
     "bajo_mlp_grad": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),

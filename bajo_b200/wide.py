@@ -1,0 +1,118 @@
+"""Wide BVH (W = 4 or 8) collapsed from a built binary LBVH.
+
+Mirrors the reference's ordinary wide layout (``GpuWideBoundsBvh``,
+bajo/bvh/gpu/wide_layout.mojo:119; collapse ``hploc_literature_to_wide_kernel``,
+bajo/bvh/gpu/builder/wide_collapse.mojo:148; triangle leaf packing
+``pack_segmented_triangle_leaf_lanes_kernel``, bajo/bvh/gpu/triangle_bvh.mojo:81)
+with deterministic pre-order node and leaf ids.  Device work is
+``bajo_wide_build`` / ``bajo_trace_wide_*`` in the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import torch
+
+from . import _lib
+from ._lib import BajoWideBvhC, BajoWideSizesC, WIDE_ARRAYS
+
+_DTYPES = {"node_offsets": torch.int32, "leaf_offsets": torch.int32, "nodes": torch.float32,
+           "leaf_indices": torch.int32, "leaf_tris": torch.float32, "leaf_sorted": torch.int32}
+
+
+def wide_sizes(n_tris: int, n_segments: int, width: int) -> dict:
+    s = BajoWideSizesC()
+    _lib.check(_lib.load().bajo_wide_sizes(n_tris, n_segments, width, ctypes.byref(s)), "bajo_wide_sizes")
+    return {name: getattr(s, name) for name in WIDE_ARRAYS + ("workspace",)}
+
+
+class GpuWideBvh:
+    """Wide tree of a ``GpuTriangleBvh``; ``n_nodes`` / ``n_leaf_blocks``
+    are read back after the build (one synchronisation)."""
+
+    def __init__(self, tree, width: int = 4):
+        if width not in (4, 8):
+            raise ValueError("width must be 4 or 8")
+        dev = tree.node_meta.device
+        sizes = wide_sizes(tree.n_leaves, tree.n_segments, width)
+        self.width = width
+        self.tree = tree
+        for name in WIDE_ARRAYS:
+            dt = _DTYPES[name]
+            item = torch.empty(0, dtype=dt).element_size()
+            setattr(self, name, torch.empty(max(sizes[name] // item, 1), dtype=dt, device=dev))
+        self.workspace = torch.zeros(sizes["workspace"], dtype=torch.uint8, device=dev)
+        self._c = None
+        self.n_nodes = 0
+        self.n_leaf_blocks = 0
+
+    def c_struct(self) -> BajoWideBvhC:
+        c = BajoWideBvhC()
+        c.width = self.width
+        c.n_segments = self.tree.n_segments
+        for name in WIDE_ARRAYS:
+            setattr(c, name, getattr(self, name).data_ptr())
+        c.bvh2_leaf_tris = self.tree.leaf_tris.data_ptr()
+        self._c = c
+        return c
+
+    def build(self, stream=None, read_counts: bool = True) -> "GpuWideBvh":
+        t = self.tree.c_struct()
+        c = self.c_struct()
+        _lib.check(_lib.load().bajo_wide_build(ctypes.byref(t), ctypes.byref(c), self.workspace.data_ptr(),
+                                               self.workspace.numel(), _lib.stream_handle(stream)),
+                   "bajo_wide_build")
+        self._c = c
+        if read_counts:
+            self.read_counts(stream)
+        return self
+
+    def read_counts(self, stream=None):
+        a, b = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        _lib.check(_lib.load().bajo_wide_counts(ctypes.byref(self._c), _lib.stream_handle(stream), ctypes.byref(a),
+                                                ctypes.byref(b)), "bajo_wide_counts")
+        self.n_nodes, self.n_leaf_blocks = a.value, b.value
+        return self.n_nodes, self.n_leaf_blocks
+
+    def status(self, stream=None) -> int:
+        st = ctypes.c_uint32(0)
+        _lib.check(_lib.load().bajo_workspace_status(self.workspace.data_ptr(), _lib.stream_handle(stream),
+                                                     ctypes.byref(st)), "bajo_workspace_status")
+        return st.value
+
+    def seg0_counts(self):
+        """(wide nodes, leaf blocks) of segment 0, the tree the traversal
+        entry points trace."""
+        if self.tree.n_segments == 1:
+            return self.n_nodes, self.n_leaf_blocks
+        return int(self.node_offsets[1].item()), int(self.leaf_offsets[1].item())
+
+    def launch_rays(self, d_rays, d_hits, ray_count, tri_mode=_lib.TRI_WATERTIGHT, d_t=None, d_prim=None,
+                    d_status=None, stream=None):
+        _lib.require_cuda(d_rays)
+        st = d_status if d_status is not None else torch.zeros(1, dtype=torch.int32, device=d_rays.device)
+        rc = _lib.load().bajo_trace_wide_rays(ctypes.byref(self._c), *self.seg0_counts(), d_rays.data_ptr(),
+                                              ray_count, tri_mode, _ptr(d_hits), _ptr(d_t), _ptr(d_prim),
+                                              st.data_ptr(), _lib.stream_handle(stream))
+        _lib.check(rc, "bajo_trace_wide_rays")
+        return st
+
+    def launch_camera(self, d_camera, d_hits, ray_count, width, height, tri_mode=_lib.TRI_WATERTIGHT, d_t=None,
+                      d_prim=None, d_status=None, d_stats=None, stream=None):
+        _lib.require_cuda(d_camera)
+        st = d_status if d_status is not None else torch.zeros(1, dtype=torch.int32, device=d_camera.device)
+        rc = _lib.load().bajo_trace_wide_camera(ctypes.byref(self._c), *self.seg0_counts(), d_camera.data_ptr(),
+                                                ray_count, width, height, tri_mode, _ptr(d_hits), _ptr(d_t),
+                                                _ptr(d_prim), st.data_ptr(), _ptr(d_stats),
+                                                _lib.stream_handle(stream))
+        _lib.check(rc, "bajo_trace_wide_camera")
+        return st
+
+
+def _ptr(t):
+    return None if t is None else t.data_ptr()
+
+
+def build_wide_bvh(tree, width: int = 4, stream=None) -> GpuWideBvh:
+    """Collapse a built ``GpuTriangleBvh`` into a ``GpuWideBvh``."""
+    return GpuWideBvh(tree, width).build(stream)

@@ -55,12 +55,13 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--case", default=None,
-                   choices=["sort", "build", "trace", "tune", "render", "batched", "guided", "guided_pass"],
+                   choices=["sort", "build", "trace", "wide", "tune", "render", "batched", "guided", "guided_pass"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
     p.add_argument("--end-bit", type=int, default=None, help="--case sort: sort bits [0, end-bit)")
     p.add_argument("--keys-only", action="store_true", help="--case sort without payload")
+    p.add_argument("--node-width", type=int, default=4, choices=[4, 8], help="--case wide node width")
     p.add_argument("--scene", default="spheres", choices=["spheres", "indirect"], help="--case guided scene")
     p.add_argument("--width", type=int, default=1280, help="--case guided image width")
     p.add_argument("--height", type=int, default=720, help="--case guided image height")
@@ -741,6 +742,25 @@ def run_case(args):
         _lib.load().bajo_sort_tuning_get(kb, int(vals is not None), n, ctypes.byref(v))
         out.update({"bits": args.bits, "end_bit": end_bit, "pairs": vals is not None, "ms": round(ms, 5),
                     "gkeys_s": round(n / ms / 1e6, 3), "variant": v.value, "status": ws.status()})
+    elif args.case == "wide":
+        from bajo_b200 import scenes, wide
+        verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
+        tree = bvh.build_triangle_bvh(verts)
+        w = wide.build_wide_bvh(tree, args.node_width)
+        ms_build = timed(lambda: w.build(read_counts=False))
+        cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+        hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
+        ms_wide = timed(lambda: w.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
+        ms_bin = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
+        stats = torch.zeros(2 * WIDTH * HEIGHT, dtype=torch.int32, device="cuda")
+        w.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, d_stats=stats)
+        s = stats.view(-1, 2).double().mean(0).tolist()
+        out.update({"node_width": args.node_width, "wide_nodes": w.n_nodes, "leaf_blocks": w.n_leaf_blocks,
+                    "collapse_ms": round(ms_build, 5), "collapse_mtri_s": round(n / ms_build / 1e3, 2),
+                    "wide_trace_ms": round(ms_wide, 4), "wide_mrays_s": round(WIDTH * HEIGHT / ms_wide / 1e3, 2),
+                    "binary_trace_ms": round(ms_bin, 4),
+                    "binary_mrays_s": round(WIDTH * HEIGHT / ms_bin / 1e3, 2),
+                    "wide_nodes_per_ray": round(s[0], 3), "tris_per_ray": round(s[1], 3), "status": w.status()})
     elif args.case in ("build", "trace"):
         from bajo_b200 import scenes
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()

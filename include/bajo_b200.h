@@ -41,6 +41,7 @@ extern "C" {
 #define BAJO_STATUS_LOOKBACK_TIMEOUT 0x1u /* sort look-back gave up waiting    */
 #define BAJO_STATUS_STACK_OVERFLOW 0x2u   /* traversal stack would overflow    */
 #define BAJO_STATUS_BAD_TOPOLOGY 0x4u     /* refit met an inconsistent parent  */
+#define BAJO_STATUS_WIDE_TIMEOUT 0x40u    /* wide collapse gave up on a task   */
 
 /* triangle tests */
 #define BAJO_TRI_MT 0         /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
@@ -204,6 +205,66 @@ int32_t bajo_trace_batch(const BajoLbvh* bvh, const float* d_cameras, uint32_t c
 int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cameras, uint32_t n_rays, uint32_t width,
                                 uint32_t height, int32_t tri_mode, float* d_hits8, uint32_t* d_stats,
                                 void* stream);
+
+/* ======================================================================== */
+/* Wide BVH (W = 4 or 8) collapsed from the binary LBVH                      */
+/* ======================================================================== */
+/* Layouts of the reference (bajo/bvh/constants.mojo:26,47-55,
+ * bajo/bvh/wide_meta.mojo:7-47): node i = 7 x W f32 field-major
+ * [min x][min y][min z][max x][max y][max z][meta] (meta as u32 bits:
+ * count << 26 | segment-local index; count 0 = internal child, 1..4 = leaf
+ * block of that many triangles; 0xFFFFFFFF = empty lane with an invalid
+ * box); leaf block b = W payloads (item ids) and W packed triangles
+ * [v0 xyz][prim][e1 xyz][0][e2 xyz][0] x W (triangle_bvh.mojo:81-148).
+ * leaf_sorted (this library's addition) holds each lane's sorted binary leaf,
+ * which the watertight test uses to read the original vertices.  Node and
+ * leaf ids are pre-order and deterministic (the reference allocates them with
+ * atomics, wide_collapse.mojo:551-559). */
+typedef struct BajoWideBvh {
+  uint32_t width;              /* 4 or 8 (leaf blocks hold `width` lanes)          */
+  uint32_t n_segments;         /* set by bajo_wide_build                           */
+  uint32_t* node_offsets;      /* [S+1] first wide node of each segment            */
+  uint32_t* leaf_offsets;      /* [S+1] first leaf block of each segment           */
+  float* nodes;                /* [node][7][W]                                     */
+  uint32_t* leaf_indices;      /* [block][W], 0xFFFFFFFF padding                   */
+  float* leaf_tris;            /* [block][12][W]                                   */
+  uint32_t* leaf_sorted;       /* [block][W], 0xFFFFFFFF padding                   */
+  const float* bvh2_leaf_tris; /* set by bajo_wide_build: the binary tree's records */
+} BajoWideBvh;
+
+typedef struct BajoWideSizes {
+  size_t node_offsets, leaf_offsets, nodes, leaf_indices, leaf_tris, leaf_sorted, workspace;
+} BajoWideSizes;
+
+int32_t bajo_wide_sizes(uint32_t n_tris, uint32_t n_segments, uint32_t width, BajoWideSizes* sizes);
+
+/* Replaces the collapse step of enqueue_segmented_wide_build
+ * (bajo/bvh/gpu/builder/segmented_build.mojo:89; hploc_literature_to_wide_kernel,
+ * wide_collapse.mojo:148) and the leaf packing
+ * (pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81) with fat
+ * leaves of up to 4 triangles, for every segment of a built binary tree. */
+int32_t bajo_wide_build(const BajoLbvh* bvh, BajoWideBvh* out, void* d_workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Synchronises `stream` and reads the total wide nodes and leaf blocks. */
+int32_t bajo_wide_counts(const BajoWideBvh* wide, void* stream, uint32_t* n_nodes, uint32_t* n_leaf_blocks);
+
+/* Closest hits over segment 0's wide tree (GpuTriangleBvh.launch_rays /
+ * launch_camera on the wide layout, triangle_bvh.mojo:520-614; loop
+ * trace_bounds_bvh_state, bajo/bvh/gpu/trace.mojo:431-552).  Same
+ * arguments and outputs as bajo_trace_rays / bajo_trace_camera plus segment
+ * 0's node and leaf-block counts (bajo_wide_counts; the node count bounds the
+ * visits, the block count the leaf references); d_stats (may be NULL)
+ * receives [nodes visited, triangles tested] per ray.  Hits equal the binary
+ * tree's bit for bit. */
+int32_t bajo_trace_wide_rays(const BajoWideBvh* wide, uint32_t n_nodes, uint32_t n_leaf_blocks, const float* d_rays,
+                             uint32_t n_rays,
+                             int32_t tri_mode, float* d_hits8, float* d_t, uint32_t* d_prim, uint32_t* d_status,
+                             void* stream);
+int32_t bajo_trace_wide_camera(const BajoWideBvh* wide, uint32_t n_nodes, uint32_t n_leaf_blocks,
+                               const float* d_cameras, uint32_t n_rays,
+                               uint32_t width, uint32_t height, int32_t tri_mode, float* d_hits8, float* d_t,
+                               uint32_t* d_prim, uint32_t* d_status, uint32_t* d_stats, void* stream);
 
 /* ======================================================================== */
 /* Wavefront path tracing over one triangle LBVH                             */

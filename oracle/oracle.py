@@ -93,6 +93,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
         "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
+        "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_mlp_param_count": (_U32, []),
         "bo_mlp_encode": (None, [_P, _P, _P, _P]),
         "bo_mlp_forward_f64": (None, [_P, _P, _P, _P, _U32, _P]),
@@ -457,3 +458,32 @@ def mlp_grad(params, pos, nrm, dirs, w, box):
     loss = lib().bo_mlp_grad_f64(_ptr(params), _ptr(pos), _ptr(nrm), _ptr(dirs), _ptr(w), w.size, _ptr(box),
                                  _ptr(g))
     return g, float(loss)
+
+
+# ---- wide BVH collapse ------------------------------------------------------
+@dataclass
+class OracleWide:
+    width: int
+    nodes: np.ndarray         # [n_nodes * 7 * W] f32 (meta as bits)
+    leaf_indices: np.ndarray  # [n_blocks * W] u32
+    leaf_tris: np.ndarray     # [n_blocks * 12 * W] f32
+    leaf_sorted: np.ndarray   # [n_blocks * W] u32
+    node_offsets: np.ndarray  # [S+1]
+    leaf_offsets: np.ndarray  # [S+1]
+
+
+def wide_build(bvh: OracleLbvh, width: int) -> OracleWide:
+    """Sequential BVH2 -> W-wide collapse with fat leaves, pre-order ids."""
+    n = max(bvh.n_leaves, 1)
+    S = bvh.seg_offsets.size - 1
+    nodes = np.zeros(n * 7 * width, np.float32)
+    li = np.zeros(n * width, np.uint32)
+    lt = np.zeros(n * 12 * width, np.float32)
+    ls = np.zeros(n * width, np.uint32)
+    no = np.zeros(S + 1, np.uint32)
+    lo = np.zeros(S + 1, np.uint32)
+    s = bvh.struct()
+    lib().bo_wide_build(ctypes.byref(s), _ptr(bvh.verts), width, _ptr(nodes), _ptr(li), _ptr(lt), _ptr(ls),
+                        _ptr(no), _ptr(lo))
+    nn, nb = int(no[-1]), int(lo[-1])
+    return OracleWide(width, nodes[:nn * 7 * width], li[:nb * width], lt[:nb * 12 * width], ls[:nb * width], no, lo)
