@@ -123,6 +123,23 @@ __device__ __forceinline__ uint32_t atomic_add_acq_rel_gpu(uint32_t* p, uint32_t
   return old;
 }
 
+__device__ __forceinline__ uint32_t atomic_add_acquire_gpu(uint32_t* p, uint32_t v) {
+  uint32_t old;
+  asm volatile("atom.add.acquire.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+  return old;
+}
+__device__ __forceinline__ void red_add_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 // Device status word bits (read back by bajo_workspace_status).
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bit) {
   if (status) atomicOr(status, bit);

@@ -272,19 +272,54 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 //    (refit_lbvh_bounds_from_leaves_kernel, lbvh.mojo:116-161;
 //     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
 //    One thread per sorted leaf climbs towards the root; the first arrival at
-//    a node stops, the second merges both child boxes and continues.  The
-//    arrival counter is an acquire-release atomic, which makes the sibling's
-//    box visible (the reference uses relaxed atomics with no fence).
+//    a node stops, the second merges both child boxes and continues.
+//    A CTA owns 1024 consecutive sorted leaves.  Nodes whose leaf range lies
+//    inside the CTA's leaves (almost all of them: a Karras node's range is
+//    contiguous) meet in shared memory: arrival counter and the first
+//    arrival's box in shared slots, no L2 round trip.  Only the nodes whose
+//    range crosses a CTA boundary meet in global memory, with the arrival
+//    counted first (acquire) and the first arrival then publishing its box
+//    with a release flag bit (kBoxReady), so the arrival that continues waits
+//    for one atomic and one box load per level rather than also for its own
+//    box stores.  node_flags ends at 2 for every internal node either way.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__ verts,
-                                                       const uint32_t* __restrict__ leaf_ids, uint32_t n,
-                                                       const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
-                                                       const uint32_t* __restrict__ node_meta,
-                                                       const uint32_t* __restrict__ leaf_parent,
-                                                       float* __restrict__ node_bounds,
-                                                       uint32_t* __restrict__ node_flags,
-                                                       float* __restrict__ leaf_tris, uint32_t* __restrict__ status) {
-  const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
+constexpr int kRefitBlock = 1024;
+constexpr uint32_t kBoxReady = 0x100u;
+constexpr uint64_t kRefitWaitNs = 200000000ull;
+
+__global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restrict__ verts,
+                                                            const uint32_t* __restrict__ leaf_ids, uint32_t n,
+                                                            const uint32_t* __restrict__ seg_offsets, uint32_t n_seg,
+                                                            const uint32_t* __restrict__ internal_offsets,
+                                                            const uint32_t* __restrict__ node_meta,
+                                                            const uint32_t* __restrict__ node_leaf_counts,
+                                                            const uint32_t* __restrict__ leaf_parent,
+                                                            float* __restrict__ node_bounds,
+                                                            uint32_t* __restrict__ node_flags,
+                                                            float* __restrict__ leaf_tris, uint32_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char refit_smem[];
+  uint4* s_meta = reinterpret_cast<uint4*>(refit_smem);                             // [kRefitBlock]
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(refit_smem + kRefitBlock * 16);     // [kRefitBlock]
+  uint32_t* s_flag = reinterpret_cast<uint32_t*>(refit_smem + kRefitBlock * 20);    // [kRefitBlock]
+  float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(refit_smem + kRefitBlock * 24);
+  s_flag[threadIdx.x] = 0;
+  const uint32_t c0 = blockIdx.x * kRefitBlock;  // first sorted leaf of this CTA
+  const uint32_t s = c0 + threadIdx.x;
+  uint32_t seg = 0, lb = 0, ib = 0;
+  if (s < n) {
+    if (n_seg > 1) seg = segment_for_item(seg_offsets, n_seg + 1, s);
+    lb = seg_offsets[seg];
+    ib = internal_offsets[seg];
+    // the internal node whose own index sits at this leaf position (one end
+    // of every Karras node's range is its index): its record is read from
+    // shared memory while the climb stays inside this CTA's leaves
+    const uint32_t li = s - lb, len = seg_offsets[seg + 1] - lb;
+    if (li + 1 < len) {
+      s_meta[threadIdx.x] = *reinterpret_cast<const uint4*>(node_meta + (size_t)(ib + li) * 4);
+      s_cnt[threadIdx.x] = node_leaf_counts[ib + li];
+    }
+  }
+  __syncthreads();
   if (s >= n) return;
   const uint32_t item = leaf_ids[s];
   if (item >= n) {  // only after a failed sort
@@ -295,8 +330,7 @@ __global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__
   f3 a = mk(__ldg(v + 0), __ldg(v + 1), __ldg(v + 2));
   f3 b = mk(__ldg(v + 3), __ldg(v + 4), __ldg(v + 5));
   f3 c = mk(__ldg(v + 6), __ldg(v + 7), __ldg(v + 8));
-  uint32_t prim = item;
-  if (n_seg > 1) prim = item - seg_offsets[segment_for_item(seg_offsets, n_seg + 1, s)];
+  const uint32_t prim = item - lb;
   float4* rec = reinterpret_cast<float4*>(leaf_tris + (size_t)s * 12);
   rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(prim));
   rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
@@ -310,22 +344,64 @@ __global__ void __launch_bounds__(kBlock) refit_kernel(const float* __restrict__
   for (int depth = 0; parent != kSentinel; ++depth) {
     if (depth > 128 || parent >= n) {
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-      break;
+      return;
     }
-    const uint4 m = *reinterpret_cast<const uint4*>(node_meta + (size_t)parent * 4);
+    const uint32_t pos = lb + (parent - ib);  // leaf position of the parent's own index
+    uint4 m;
+    uint32_t cnt;
+    if (pos >= c0 && pos < c0 + kRefitBlock) {
+      m = s_meta[pos - c0];
+      cnt = s_cnt[pos - c0];
+    } else {
+      m = *reinterpret_cast<const uint4*>(node_meta + (size_t)parent * 4);
+      cnt = __ldg(node_leaf_counts + parent);
+    }
     const bool is_left = m.y == cur;
     if (!is_left && m.z != cur) {
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-      break;
+      return;
     }
-    float* slot = node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6);
-    slot[0] = mn.x; slot[1] = mn.y; slot[2] = mn.z; slot[3] = mx.x; slot[4] = mx.y; slot[5] = mx.z;
-    // release our slot, acquire the sibling's (the second arrival reads the
-    // first arrival's release)
-    if (atomic_add_acq_rel_gpu(&node_flags[parent], 1u) == 0) break;
-    const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
-    mn = vmin(mn, mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2)));
-    mx = vmax(mx, mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5)));
+    float2* slot = reinterpret_cast<float2*>(node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6));
+    slot[0] = make_float2(mn.x, mn.y);
+    slot[1] = make_float2(mn.z, mx.x);
+    slot[2] = make_float2(mx.y, mx.z);
+    const uint32_t last = m.w, first = last + 1 - cnt;
+    f3 smn, smx;
+    if (first >= c0 && last < c0 + kRefitBlock) {
+      // both children live in this CTA; one end of a Karras node's range is
+      // its own local index, so lb + (parent - ib) - c0 is a unique slot
+      const uint32_t k = lb + (parent - ib) - c0;
+      float* mine = s_box[k][is_left ? 0 : 1];
+      mine[0] = mn.x; mine[1] = mn.y; mine[2] = mn.z; mine[3] = mx.x; mine[4] = mx.y; mine[5] = mx.z;
+      __threadfence_block();
+      if (atomicAdd(&s_flag[k], 1u) == 0) return;
+      __threadfence_block();
+      const float* sib = s_box[k][is_left ? 1 : 0];
+      smn = mk(sib[0], sib[1], sib[2]);
+      smx = mk(sib[3], sib[4], sib[5]);
+      node_flags[parent] = 2u;
+    } else {
+      const uint32_t old = atomic_add_acquire_gpu(&node_flags[parent], 1u);
+      if ((old & 0xFFu) == 0) {  // first: publish the box stored above
+        red_add_release_gpu(&node_flags[parent], kBoxReady);
+        return;
+      }
+      if (!(old & kBoxReady)) {
+        const uint64_t t0 = global_timer_ns();
+        while (!(ld_acquire_gpu(&node_flags[parent]) & kBoxReady)) {
+          if (global_timer_ns() - t0 > kRefitWaitNs) {
+            raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+            return;
+          }
+        }
+      }
+      const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
+      smn = mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2));
+      smx = mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5));
+      node_flags[parent] = 2u;
+    }
+    mn = vmin(mn, smn);
+    mx = vmax(mx, smx);
     cur = parent;
     parent = m.x;
   }
@@ -456,9 +532,13 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
       bvh->node_leaf_counts, bvh->node_flags, bvh->roots);
   if (cudaGetLastError() != cudaSuccess || !mark(3 + passes)) return BAJO_ERR_CUDA;
   if (n > 0) {
-    refit_kernel<<<blocks, kBlock, 0, st>>>(d_verts, bvh->leaf_ids, n, bvh->seg_offsets, S, bvh->node_meta,
-                                            bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris,
-                                            status);
+    constexpr size_t refit_smem = kRefitBlock * (16 + 4 + 4 + 2 * 6 * 4);
+    if (cudaFuncSetAttribute(refit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)refit_smem) !=
+        cudaSuccess)
+      return BAJO_ERR_CUDA;
+    refit_kernel<<<(n + kRefitBlock - 1) / kRefitBlock, kRefitBlock, refit_smem, st>>>(
+        d_verts, bvh->leaf_ids, n, bvh->seg_offsets, S, bvh->internal_offsets, bvh->node_meta, bvh->node_leaf_counts,
+        bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris, status);
     if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
   }
   if (!mark(4 + passes)) return BAJO_ERR_CUDA;

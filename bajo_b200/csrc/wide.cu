@@ -33,15 +33,6 @@ namespace wide {
 constexpr int kBlock = 128;
 constexpr uint64_t kWaitNs = 200000000ull;  // 200 ms bound on one task wait
 
-__device__ __forceinline__ uint32_t ld_acquire_gpu(const uint32_t* p) {
-  uint32_t v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
-  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
 struct Work {
   uint32_t* flags;      // [internal] arrival counters
   uint32_t* cands;      // [internal][W] children of the wide node rooted there
