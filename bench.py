@@ -171,34 +171,20 @@ class ClockSampler:
 
 # ----------------------------------------------------------------- distributed
 def dist_setup(args):
-    import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
-    elif torch.cuda.is_available():
-        torch.cuda.set_device(0)
-    return world, rank, local
+    """One process per GPU over NCCL (torchrun sets RANK / WORLD_SIZE /
+    LOCAL_RANK / MASTER_*); see bajo_b200/dist.py."""
+    from bajo_b200 import dist
+    return dist.init()
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from bajo_b200 import dist
+    dist.barrier(world)
 
 
 def max_over_ranks(world, x: float) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from bajo_b200 import dist
+    return dist.max_over_ranks(world, x)
 
 
 # ----------------------------------------------------------------- CPU baseline
@@ -808,9 +794,8 @@ def main():
         run_reference(args)
         return
     run_bajo(args)
-    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
-        import torch.distributed as dist
-        dist.destroy_process_group()
+    from bajo_b200 import dist
+    dist.finish(int(os.environ.get("WORLD_SIZE", "1")))
 
 
 if __name__ == "__main__":
