@@ -82,19 +82,30 @@ __device__ __forceinline__ bool better(float t, uint32_t prim, const Hit& h) {
 // lies in [bmin, bmax], empty otherwise).  With the reference's +-1e9
 // reciprocal (ray.mojo:86-111) a ray running exactly along a box face gets an
 // empty slab; containment keeps such rays inside the closed box.
+// PAR = false compiles the slab for rays with no parallel axis (the common
+// case: no selects); the result is the same as with PAR = true for them.
+template <bool PAR>
 __device__ __forceinline__ void slab(float bmin, float bmax, float o, float rcp, bool par, float& t0, float& t1) {
   const float a = (bmin - o) * rcp, b = (bmax - o) * rcp;
-  t0 = par ? (bmin <= o ? -INFINITY : INFINITY) : a;
-  t1 = par ? (bmax >= o ? INFINITY : -INFINITY) : b;
+  if constexpr (PAR) {
+    t0 = par ? (bmin <= o ? -INFINITY : INFINITY) : a;
+    t1 = par ? (bmax >= o ? INFINITY : -INFINITY) : b;
+  } else {
+    t0 = a;
+    t1 = b;
+  }
 }
 
+__device__ __forceinline__ bool has_parallel_axis(const Ray& r) { return r.px || r.py || r.pz; }
+
 // intersect.mojo:193-215, far bound scaled by kSlack
+template <bool PAR = true>
 __device__ __forceinline__ bool box_hit(const Ray& r, float4 a, float2 b, float tlimit, float& tnear) {
   // a = (min x, min y, min z, max x), b = (max y, max z)
   float t0x, t1x, t0y, t1y, t0z, t1z;
-  slab(a.x, a.w, r.o.x, r.rcp.x, r.px, t0x, t1x);
-  slab(a.y, b.x, r.o.y, r.rcp.y, r.py, t0y, t1y);
-  slab(a.z, b.y, r.o.z, r.rcp.z, r.pz, t0z, t1z);
+  slab<PAR>(a.x, a.w, r.o.x, r.rcp.x, r.px, t0x, t1x);
+  slab<PAR>(a.y, b.x, r.o.y, r.rcp.y, r.py, t0y, t1y);
+  slab<PAR>(a.z, b.y, r.o.z, r.rcp.z, r.pz, t0z, t1z);
   float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
   float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlimit));
   tnear = tn;
@@ -169,11 +180,11 @@ __device__ __forceinline__ void test_tri(const Ray& r, const float4* __restrict_
 
 // max_nodes: node visits allowed (the node count): a tree is never visited
 // twice per node, so more visits means a corrupt tree.
-template <int MODE, bool STATS = false, bool ANY = false>
-__device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const float4* __restrict__ nb,
-                                          const uint4* __restrict__ meta, const float4* __restrict__ tris,
-                                          uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes = nullptr,
-                                          uint32_t* n_tris = nullptr) {
+template <int MODE, bool STATS, bool ANY, bool PAR>
+__device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, const float4* __restrict__ nb,
+                                               const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                                               uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes,
+                                               uint32_t* n_tris) {
   Hit h;
   h.t = r.tmax;
   h.u = h.v = 0.0f;
@@ -202,8 +213,8 @@ __device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const flo
     const uint4 m = __ldg(meta + cur);
     float tl, tr;
     const float limit0 = ANY ? r.tmax : h.t;
-    const bool hl = box_hit(r, b0, make_float2(b1.x, b1.y), limit0, tl);
-    const bool hr = box_hit(r, make_float4(b1.z, b1.w, b2.x, b2.y), make_float2(b2.z, b2.w), limit0, tr);
+    const bool hl = box_hit<PAR>(r, b0, make_float2(b1.x, b1.y), limit0, tl);
+    const bool hr = box_hit<PAR>(r, make_float4(b1.z, b1.w, b2.x, b2.y), make_float2(b2.z, b2.w), limit0, tr);
     bool vl = false, vr = false;
     if (hl) {
       if (m.y & kLeafFlag) {
@@ -240,6 +251,18 @@ __device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const flo
     cur = stack[--sp];
   }
   return h;
+}
+
+// Rays with an axis parallel to the boxes (|d| <= 1e-9) take the containment
+// slab; every other ray takes the select-free one.
+template <int MODE, bool STATS = false, bool ANY = false>
+__device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const float4* __restrict__ nb,
+                                          const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                                          uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes = nullptr,
+                                          uint32_t* n_tris = nullptr) {
+  if (has_parallel_axis(r))
+    return trace_bvh2_impl<MODE, STATS, ANY, true>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
+  return trace_bvh2_impl<MODE, STATS, ANY, false>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
 }
 
 }  // namespace trav

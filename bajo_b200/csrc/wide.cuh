@@ -133,9 +133,9 @@ struct View {
 // pop once the hit is nearer.  The same order-independent rules as the
 // binary traversal (lowest prim on ties, conservative slabs) make the result
 // equal to the binary tree's bit for bit.
-template <int W, int MODE, bool STATS = false, bool ANY = false>
-__device__ __forceinline__ trav::Hit trace_wide(const trav::Ray& r, const View& v, uint32_t* status,
-                                                uint32_t* n_nodes = nullptr, uint32_t* n_tris = nullptr) {
+template <int W, int MODE, bool STATS, bool ANY, bool PAR>
+__device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const View& v, uint32_t* status,
+                                                     uint32_t* n_nodes, uint32_t* n_tris) {
   trav::Hit h;
   h.t = r.tmax;
   h.u = h.v = 0.0f;
@@ -170,7 +170,7 @@ __device__ __forceinline__ trav::Hit trace_wide(const trav::Ray& r, const View& 
       if (meta == kEmpty) continue;
       float tn;
       const float limit = ANY ? r.tmax : h.t;
-      if (!trav::box_hit(r, make_float4(f[0][j], f[1][j], f[2][j], f[3][j]), make_float2(f[4][j], f[5][j]),
+      if (!trav::box_hit<PAR>(r, make_float4(f[0][j], f[1][j], f[2][j], f[3][j]), make_float2(f[4][j], f[5][j]),
                          limit, tn))
         continue;
       const uint32_t count = meta >> kCountShift, data = meta & kDataMask;
@@ -252,6 +252,13 @@ __device__ __forceinline__ trav::Hit trace_wide(const trav::Ray& r, const View& 
     if (!found) break;
   }
   return h;
+}
+
+template <int W, int MODE, bool STATS = false, bool ANY = false>
+__device__ __forceinline__ trav::Hit trace_wide(const trav::Ray& r, const View& v, uint32_t* status,
+                                                uint32_t* n_nodes = nullptr, uint32_t* n_tris = nullptr) {
+  if (trav::has_parallel_axis(r)) return trace_wide_impl<W, MODE, STATS, ANY, true>(r, v, status, n_nodes, n_tris);
+  return trace_wide_impl<W, MODE, STATS, ANY, false>(r, v, status, n_nodes, n_tris);
 }
 
 }  // namespace wide
