@@ -70,8 +70,8 @@ class BajoLbvhSizesC(ctypes.Structure):
 
 class BajoWideBvhC(ctypes.Structure):
     """Mirror of ``struct BajoWideBvh`` (include/bajo_b200.h)."""
-    _fields_ = [("width", _U32), ("n_segments", _U32), ("node_offsets", _P), ("leaf_offsets", _P), ("nodes", _P),
-                ("leaf_indices", _P), ("leaf_tris", _P), ("leaf_sorted", _P), ("bvh2_leaf_tris", _P)]
+    _fields_ = [("width", _U32), ("max_leaf", _U32), ("n_segments", _U32), ("node_offsets", _P), ("leaf_offsets", _P),
+                ("nodes", _P), ("leaf_indices", _P), ("leaf_tris", _P), ("leaf_sorted", _P), ("bvh2_leaf_tris", _P)]
 
 
 WIDE_ARRAYS = ("node_offsets", "leaf_offsets", "nodes", "leaf_indices", "leaf_tris", "leaf_sorted")

@@ -52,7 +52,8 @@ __global__ void __launch_bounds__(kBlock) count_kernel(uint32_t n, const uint32_
                                                        const uint32_t* __restrict__ node_leaf_counts,
                                                        const float* __restrict__ leaf_bounds,
                                                        const uint32_t* __restrict__ leaf_ids,
-                                                       const float* __restrict__ node_bounds, Work wk) {
+                                                       const float* __restrict__ node_bounds, uint32_t max_leaf,
+                                                       Work wk) {
   const uint32_t s = blockIdx.x * kBlock + threadIdx.x;
   if (s >= n) return;
   uint32_t parent = leaf_parent[s];
@@ -65,10 +66,11 @@ __global__ void __launch_bounds__(kBlock) count_kernel(uint32_t n, const uint32_
     if (atomic_add_acq_rel_gpu(&wk.flags[parent], 1u) == 0) return;
     const uint32_t x = parent;
     uint32_t cand[W], cnt[W];
-    const int nc = open_children<W>(x, node_meta, node_leaf_counts, leaf_bounds, leaf_ids, node_bounds, cand, cnt);
+    const int nc =
+        open_children<W>(x, node_meta, node_leaf_counts, leaf_bounds, leaf_ids, node_bounds, max_leaf, cand, cnt);
     uint32_t nodes = 1, leaves = 0, mask = 0;
     for (int k = 0; k < nc; ++k) {
-      if (terminal(cand[k], cnt[k])) {
+      if (terminal(cand[k], cnt[k], max_leaf)) {
         ++leaves;
         mask |= 1u << k;
       } else {
@@ -88,12 +90,12 @@ __global__ void __launch_bounds__(kBlock) count_kernel(uint32_t n, const uint32_
 // node / leaf-block counts of a segment's root
 __device__ __forceinline__ void root_counts(uint32_t s, const uint32_t* __restrict__ seg_offsets,
                                             const uint32_t* __restrict__ roots,
-                                            const uint32_t* __restrict__ node_leaf_counts, const Work& wk,
-                                            uint32_t& nodes, uint32_t& leaves) {
+                                            const uint32_t* __restrict__ node_leaf_counts, uint32_t max_leaf,
+                                            const Work& wk, uint32_t& nodes, uint32_t& leaves) {
   nodes = leaves = 0;
   if (seg_offsets[s + 1] == seg_offsets[s]) return;
   const uint32_t r = roots[s];
-  if (terminal(r, ref_count(r, node_leaf_counts))) {
+  if (terminal(r, ref_count(r, node_leaf_counts), max_leaf)) {
     nodes = leaves = 1;
   } else {
     nodes = wk.nw[r & kIndexMask];
@@ -104,8 +106,9 @@ __device__ __forceinline__ void root_counts(uint32_t s, const uint32_t* __restri
 // one block: exclusive scans of the per-segment counts, then the roots' tasks
 __global__ void __launch_bounds__(1024) offsets_kernel(uint32_t n_seg, const uint32_t* __restrict__ seg_offsets,
                                                        const uint32_t* __restrict__ roots,
-                                                       const uint32_t* __restrict__ node_leaf_counts, Work wk,
-                                                       uint32_t cap, uint32_t* __restrict__ node_offsets,
+                                                       const uint32_t* __restrict__ node_leaf_counts,
+                                                       uint32_t max_leaf, Work wk, uint32_t cap,
+                                                       uint32_t* __restrict__ node_offsets,
                                                        uint32_t* __restrict__ leaf_offsets) {
   __shared__ uint32_t sn[1024], sl[1024];
   const uint32_t t = threadIdx.x;
@@ -114,7 +117,7 @@ __global__ void __launch_bounds__(1024) offsets_kernel(uint32_t n_seg, const uin
   uint32_t an = 0, al = 0;
   for (uint32_t s = b; s < e; ++s) {
     uint32_t cn, cl;
-    root_counts(s, seg_offsets, roots, node_leaf_counts, wk, cn, cl);
+    root_counts(s, seg_offsets, roots, node_leaf_counts, max_leaf, wk, cn, cl);
     an += cn;
     al += cl;
   }
@@ -131,7 +134,7 @@ __global__ void __launch_bounds__(1024) offsets_kernel(uint32_t n_seg, const uin
   uint32_t pn = sn[t] - an, pl = sl[t] - al;
   for (uint32_t s = b; s < e; ++s) {
     uint32_t cn, cl;
-    root_counts(s, seg_offsets, roots, node_leaf_counts, wk, cn, cl);
+    root_counts(s, seg_offsets, roots, node_leaf_counts, max_leaf, wk, cn, cl);
     node_offsets[s] = pn;
     leaf_offsets[s] = pl;
     if (cn && pn < cap) {
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
                                                         const float4* __restrict__ tris,
                                                         const uint32_t* __restrict__ node_offsets,
                                                         const uint32_t* __restrict__ leaf_offsets, uint32_t cap,
-                                                        Work wk, Out o) {
+                                                        uint32_t max_leaf, Work wk, Out o) {
   // node and leaf-block totals never exceed the triangle count; more means
   // the binary tree is corrupt
   uint32_t total = node_offsets[n_seg];
@@ -251,7 +254,7 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
     const uint32_t nb = node_offsets[s], lb = leaf_offsets[s];
     float* node = o.nodes + (size_t)I * kFields * W;
     const uint32_t xc = ref_count(x, node_leaf_counts);
-    if (terminal(x, xc)) {  // a segment of at most four triangles: one node, one leaf block
+    if (terminal(x, xc, max_leaf)) {  // a segment of at most max_leaf triangles: one node, one leaf block
       if (B >= cap) {
         raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
         continue;
@@ -406,7 +409,8 @@ inline Plan make_plan(uint32_t n, uint32_t width) {
 }
 
 template <int W>
-cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const Plan& p, cudaStream_t st) {
+cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const Plan& p, uint32_t max_leaf,
+                  cudaStream_t st) {
   Work wk;
   wk.status = (uint32_t*)ws;
   wk.flags = (uint32_t*)(ws + p.flags);
@@ -424,10 +428,10 @@ cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const 
   if (n > 0) {
     count_kernel<W><<<(n + kBlock - 1) / kBlock, kBlock, 0, st>>>(n, b->node_meta, b->leaf_parent,
                                                                  b->node_leaf_counts, b->leaf_bounds, b->leaf_ids,
-                                                                 b->node_bounds, wk);
+                                                                 b->node_bounds, max_leaf, wk);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  offsets_kernel<<<1, 1024, 0, st>>>(b->n_segments, b->seg_offsets, b->roots, b->node_leaf_counts, wk,
+  offsets_kernel<<<1, 1024, 0, st>>>(b->n_segments, b->seg_offsets, b->roots, b->node_leaf_counts, max_leaf, wk,
                                      std::max<uint32_t>(n, 1), out->node_offsets, out->leaf_offsets);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (n == 0) return cudaSuccess;
@@ -442,7 +446,7 @@ cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const 
   assign_kernel<W><<<grid, kBlock, 0, st>>>(b->n_segments, b->node_meta, b->node_leaf_counts, b->leaf_bounds,
                                            b->leaf_ids, b->node_bounds,
                                            reinterpret_cast<const float4*>(b->leaf_tris), out->node_offsets,
-                                           out->leaf_offsets, std::max<uint32_t>(n, 1), wk, o);
+                                           out->leaf_offsets, std::max<uint32_t>(n, 1), max_leaf, wk, o);
   return cudaGetLastError();
 }
 
@@ -504,8 +508,10 @@ int32_t bajo_wide_build(const BajoLbvh* b, BajoWideBvh* out, void* ws, size_t ws
   out->n_segments = b->n_segments;
   out->bvh2_leaf_tris = b->leaf_tris;
   cudaStream_t st = (cudaStream_t)stream;
-  const cudaError_t e = out->width == 4 ? build<4>(b, out, (unsigned char*)ws, p, st)
-                                        : build<8>(b, out, (unsigned char*)ws, p, st);
+  const uint32_t max_leaf = out->max_leaf ? out->max_leaf : kFatLeaf;
+  if (max_leaf > kFatLeaf) return BAJO_ERR_INVALID_ARGUMENT;
+  const cudaError_t e = out->width == 4 ? build<4>(b, out, (unsigned char*)ws, p, max_leaf, st)
+                                        : build<8>(b, out, (unsigned char*)ws, p, max_leaf, st);
   return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 

@@ -23,7 +23,7 @@ namespace bajo {
 namespace wide {
 
 constexpr int kFields = 7;
-constexpr uint32_t kFatLeaf = 4;  // HIPRT fat leaves: binary subtrees of <= 4 triangles
+constexpr uint32_t kFatLeaf = 4;  // HIPRT fat leaves: binary subtrees of <= 4 triangles (the largest leaf)
 constexpr uint32_t kCountShift = 26, kDataMask = 0x03FFFFFFu;
 constexpr int kLeafStride = 12;   // TRI_LEAF_PACKED_STRIDE
 
@@ -62,15 +62,18 @@ __device__ __forceinline__ uint32_t ref_count(uint32_t ref, const uint32_t* __re
   return (ref & kLeafFlag) ? 1u : __ldg(node_leaf_counts + (ref & kIndexMask));
 }
 
-__device__ __forceinline__ bool terminal(uint32_t ref, uint32_t count) {
-  return (ref & kLeafFlag) || count <= kFatLeaf;
+// max_leaf: triangles a leaf block may hold (1 = every triangle its own
+// leaf, the reference's fat_leaves = false; 4 = HIPRT fat leaves)
+__device__ __forceinline__ bool terminal(uint32_t ref, uint32_t count, uint32_t max_leaf) {
+  return (ref & kLeafFlag) || count <= max_leaf;
 }
 
 // Children of the wide node rooted at binary internal node x
 // (hploc_literature_to_wide_kernel, wide_collapse.mojo:318-444): start from
-// x's two children; first open the non-fat internal candidate of largest
-// surface area until W candidates or none is left, then open the largest
-// fat-leaf-sized internal candidates until full.  An opened candidate is
+// x's two children; first open the internal candidate of largest surface
+// area among those with more than max_leaf triangles until W candidates or
+// none is left, then open the largest remaining internal candidates until
+// full.  An opened candidate is
 // replaced by its left child and its right child is appended.  Ties keep the
 // first candidate.  Returns the candidate count.
 template <int W>
@@ -78,8 +81,8 @@ __device__ __forceinline__ int open_children(uint32_t x, const uint32_t* __restr
                                              const uint32_t* __restrict__ node_leaf_counts,
                                              const float* __restrict__ leaf_bounds,
                                              const uint32_t* __restrict__ leaf_ids,
-                                             const float* __restrict__ node_bounds, uint32_t cand[W],
-                                             uint32_t cnt[W]) {
+                                             const float* __restrict__ node_bounds, uint32_t max_leaf,
+                                             uint32_t cand[W], uint32_t cnt[W]) {
   float ar[W];
   cand[0] = __ldg(node_meta + (size_t)x * 4 + 1);
   cand[1] = __ldg(node_meta + (size_t)x * 4 + 2);
@@ -95,7 +98,7 @@ __device__ __forceinline__ int open_children(uint32_t x, const uint32_t* __restr
       float best = -1.0f;
       for (int k = 0; k < n; ++k) {
         if (cand[k] & kLeafFlag) continue;
-        if (phase == 0 && cnt[k] <= kFatLeaf) continue;
+        if (phase == 0 && cnt[k] <= max_leaf) continue;
         if (ar[k] > best) {
           best = ar[k];
           pos = k;

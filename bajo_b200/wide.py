@@ -30,9 +30,12 @@ class GpuWideBvh:
     """Wide tree of a ``GpuTriangleBvh``; ``n_nodes`` / ``n_leaf_blocks``
     are read back after the build (one synchronisation)."""
 
-    def __init__(self, tree, width: int = 4):
+    def __init__(self, tree, width: int = 4, max_leaf: int = 4):
         if width not in (4, 8):
             raise ValueError("width must be 4 or 8")
+        if not 1 <= max_leaf <= 4:
+            raise ValueError("max_leaf must be 1..4")
+        self.max_leaf = max_leaf
         dev = tree.node_meta.device
         sizes = wide_sizes(tree.n_leaves, tree.n_segments, width)
         self.width = width
@@ -49,6 +52,7 @@ class GpuWideBvh:
     def c_struct(self) -> BajoWideBvhC:
         c = BajoWideBvhC()
         c.width = self.width
+        c.max_leaf = self.max_leaf
         c.n_segments = self.tree.n_segments
         for name in WIDE_ARRAYS:
             setattr(c, name, getattr(self, name).data_ptr())
@@ -113,6 +117,7 @@ def _ptr(t):
     return None if t is None else t.data_ptr()
 
 
-def build_wide_bvh(tree, width: int = 4, stream=None) -> GpuWideBvh:
-    """Collapse a built ``GpuTriangleBvh`` into a ``GpuWideBvh``."""
-    return GpuWideBvh(tree, width).build(stream)
+def build_wide_bvh(tree, width: int = 4, max_leaf: int = 4, stream=None) -> GpuWideBvh:
+    """Collapse a built ``GpuTriangleBvh`` into a ``GpuWideBvh`` (leaf blocks
+    of up to ``max_leaf`` triangles; 4 = the reference's fat leaves)."""
+    return GpuWideBvh(tree, width, max_leaf).build(stream)

@@ -62,6 +62,7 @@ def parse():
     p.add_argument("--end-bit", type=int, default=None, help="--case sort: sort bits [0, end-bit)")
     p.add_argument("--keys-only", action="store_true", help="--case sort without payload")
     p.add_argument("--node-width", type=int, default=4, choices=[4, 8], help="--case wide node width")
+    p.add_argument("--max-leaf", type=int, default=4, choices=[1, 2, 3, 4], help="--case wide leaf block size")
     p.add_argument("--scene", default="spheres", choices=["spheres", "indirect"], help="--case guided scene")
     p.add_argument("--width", type=int, default=1280, help="--case guided image width")
     p.add_argument("--height", type=int, default=720, help="--case guided image height")
@@ -753,7 +754,7 @@ def run_case(args):
         from bajo_b200 import scenes, wide
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
         tree = bvh.build_triangle_bvh(verts)
-        w = wide.build_wide_bvh(tree, args.node_width)
+        w = wide.build_wide_bvh(tree, args.node_width, args.max_leaf)
         ms_build = timed(lambda: w.build(read_counts=False))
         cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
         hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
@@ -762,7 +763,7 @@ def run_case(args):
         stats = torch.zeros(2 * WIDTH * HEIGHT, dtype=torch.int32, device="cuda")
         w.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, d_stats=stats)
         s = stats.view(-1, 2).double().mean(0).tolist()
-        out.update({"node_width": args.node_width, "wide_nodes": w.n_nodes, "leaf_blocks": w.n_leaf_blocks,
+        out.update({"node_width": args.node_width, "max_leaf": args.max_leaf, "wide_nodes": w.n_nodes, "leaf_blocks": w.n_leaf_blocks,
                     "collapse_ms": round(ms_build, 5), "collapse_mtri_s": round(n / ms_build / 1e3, 2),
                     "wide_trace_ms": round(ms_wide, 4), "wide_mrays_s": round(WIDTH * HEIGHT / ms_wide / 1e3, 2),
                     "binary_trace_ms": round(ms_bin, 4),

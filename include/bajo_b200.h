@@ -222,6 +222,9 @@ int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cameras, uin
  * atomics, wide_collapse.mojo:551-559). */
 typedef struct BajoWideBvh {
   uint32_t width;              /* 4 or 8 (leaf blocks hold `width` lanes)          */
+  uint32_t max_leaf;           /* triangles per leaf block, 1..4; 0 = 4 (the
+                                  reference's fat leaves for triangles; 1 is its
+                                  fat_leaves = false)                              */
   uint32_t n_segments;         /* set by bajo_wide_build                           */
   uint32_t* node_offsets;      /* [S+1] first wide node of each segment            */
   uint32_t* leaf_offsets;      /* [S+1] first leaf block of each segment           */

@@ -171,9 +171,11 @@ void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, ui
                     uint32_t n_threads);
 
 /* ---- a10: BVH2 -> W-wide collapse (bajo_oracle_wide.c) ------------------- */
-/* Outputs sized for n_leaves nodes and leaf blocks; offsets [S+1]. */
-void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, float* nodes, uint32_t* leaf_indices,
-                   float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets, uint32_t* leaf_offsets);
+/* Outputs sized for n_leaves nodes and leaf blocks; offsets [S+1];
+ * max_leaf = triangles per leaf block (1..4, 0 = 4). */
+void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, uint32_t max_leaf, float* nodes,
+                   uint32_t* leaf_indices, float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets,
+                   uint32_t* leaf_offsets);
 
 /* ---- path-guiding network (bajo_oracle_mlp.c), FP64 ---------------------- */
 /* Parameters as doubles in the library's layout: W1[64x64] b1[64] W2 b2 W3 b3

@@ -38,6 +38,7 @@ typedef struct {
   float* leaf_tris;
   uint32_t* leaf_sorted;
   uint32_t seg_item0;
+  uint32_t max_leaf; /* triangles per leaf block (1..4) */
 } wctx;
 
 static void ref_box(const wctx* c, uint32_t ref, float out[6]) {
@@ -64,7 +65,9 @@ static uint32_t ref_count(const wctx* c, uint32_t ref) {
   return (ref & LEAF_FLAG) ? 1u : c->b->node_leaf_counts[ref & IDX_MASK];
 }
 
-static int is_terminal(uint32_t ref, uint32_t count) { return (ref & LEAF_FLAG) || count <= FAT; }
+static int is_terminal(const wctx* c, uint32_t ref, uint32_t count) {
+  return (ref & LEAF_FLAG) || count <= c->max_leaf;
+}
 
 static int open_children(const wctx* c, uint32_t x, uint32_t* cand, uint32_t* cnt) {
   const uint32_t* m = c->b->node_meta;
@@ -82,7 +85,7 @@ static int open_children(const wctx* c, uint32_t x, uint32_t* cand, uint32_t* cn
       float best = -1.0f;
       for (int k = 0; k < n; ++k) {
         if (cand[k] & LEAF_FLAG) continue;
-        if (phase == 0 && cnt[k] <= FAT) continue;
+        if (phase == 0 && cnt[k] <= c->max_leaf) continue;
         if (ar[k] > best) {
           best = ar[k];
           pos = k;
@@ -108,7 +111,7 @@ static void counts(wctx* c, uint32_t x) {
   int n = open_children(c, x, cand, cnt);
   uint32_t nodes = 1, leaves = 0;
   for (int k = 0; k < n; ++k) {
-    if (is_terminal(cand[k], cnt[k])) {
+    if (is_terminal(c, cand[k], cnt[k])) {
       ++leaves;
     } else {
       uint32_t ci = cand[k] & IDX_MASK;
@@ -181,7 +184,7 @@ static void emit(wctx* c, uint32_t x, uint32_t I, uint32_t B, uint32_t nb, uint3
   float* node = c->nodes + (size_t)I * 7 * W;
   float bx[6];
   uint32_t xc = ref_count(c, x);
-  if (is_terminal(x, xc)) {
+  if (is_terminal(c, x, xc)) {
     write_block(c, x, B);
     ref_box(c, x, bx);
     store_lane(node, W, 0, bx, pack_meta(B - lb, xc));
@@ -192,7 +195,7 @@ static void emit(wctx* c, uint32_t x, uint32_t I, uint32_t B, uint32_t nb, uint3
   int n = open_children(c, x & IDX_MASK, cand, cnt);
   uint32_t leaf_next = B;
   for (int k = 0; k < n; ++k)
-    if (is_terminal(cand[k], cnt[k])) write_block(c, cand[k], leaf_next++);
+    if (is_terminal(c, cand[k], cnt[k])) write_block(c, cand[k], leaf_next++);
   uint32_t own = B, child = I + 1, child_leaf = leaf_next;
   uint32_t child_id[8], child_lb[8];
   for (uint32_t k = 0; k < W; ++k) {
@@ -201,7 +204,7 @@ static void emit(wctx* c, uint32_t x, uint32_t I, uint32_t B, uint32_t nb, uint3
       continue;
     }
     ref_box(c, cand[k], bx);
-    if (is_terminal(cand[k], cnt[k])) {
+    if (is_terminal(c, cand[k], cnt[k])) {
       store_lane(node, W, k, bx, pack_meta(own - lb, cnt[k]));
       ++own;
     } else {
@@ -214,13 +217,15 @@ static void emit(wctx* c, uint32_t x, uint32_t I, uint32_t B, uint32_t nb, uint3
     }
   }
   for (int k = 0; k < n; ++k)
-    if (!is_terminal(cand[k], cnt[k])) emit(c, cand[k], child_id[k], child_lb[k], nb, lb);
+    if (!is_terminal(c, cand[k], cnt[k])) emit(c, cand[k], child_id[k], child_lb[k], nb, lb);
 }
 
-void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, float* nodes, uint32_t* leaf_indices,
-                   float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets, uint32_t* leaf_offsets) {
+void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, uint32_t max_leaf, float* nodes,
+                   uint32_t* leaf_indices, float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets,
+                   uint32_t* leaf_offsets) {
   wctx c;
   memset(&c, 0, sizeof(c));
+  c.max_leaf = max_leaf ? max_leaf : FAT;
   c.b = b;
   c.verts = verts;
   c.W = width;
@@ -240,7 +245,7 @@ void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, float* n
     uint32_t r = b->roots[s];
     c.seg_item0 = b->seg_offsets[s];
     uint32_t rn, rl;
-    if (is_terminal(r, ref_count(&c, r))) {
+    if (is_terminal(&c, r, ref_count(&c, r))) {
       rn = rl = 1;
     } else {
       counts(&c, r & IDX_MASK);

@@ -93,7 +93,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
         "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
-        "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _P, _P, _P, _P, _P, _P]),
+        "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_mlp_param_count": (_U32, []),
         "bo_mlp_encode": (None, [_P, _P, _P, _P]),
         "bo_mlp_forward_f64": (None, [_P, _P, _P, _P, _U32, _P]),
@@ -472,7 +472,7 @@ class OracleWide:
     leaf_offsets: np.ndarray  # [S+1]
 
 
-def wide_build(bvh: OracleLbvh, width: int) -> OracleWide:
+def wide_build(bvh: OracleLbvh, width: int, max_leaf: int = 4) -> OracleWide:
     """Sequential BVH2 -> W-wide collapse with fat leaves, pre-order ids."""
     n = max(bvh.n_leaves, 1)
     S = bvh.seg_offsets.size - 1
@@ -483,7 +483,7 @@ def wide_build(bvh: OracleLbvh, width: int) -> OracleWide:
     no = np.zeros(S + 1, np.uint32)
     lo = np.zeros(S + 1, np.uint32)
     s = bvh.struct()
-    lib().bo_wide_build(ctypes.byref(s), _ptr(bvh.verts), width, _ptr(nodes), _ptr(li), _ptr(lt), _ptr(ls),
+    lib().bo_wide_build(ctypes.byref(s), _ptr(bvh.verts), width, max_leaf, _ptr(nodes), _ptr(li), _ptr(lt), _ptr(ls),
                         _ptr(no), _ptr(lo))
     nn, nb = int(no[-1]), int(lo[-1])
     return OracleWide(width, nodes[:nn * 7 * width], li[:nb * width], lt[:nb * 12 * width], ls[:nb * width], no, lo)

@@ -18,9 +18,9 @@ def dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def gpu_wide(verts, W, seg=None):
+def gpu_wide(verts, W, seg=None, max_leaf=4):
     tree = bvh.build_triangle_bvh(dev(np.asarray(verts, np.float32)), seg)
-    w = wide.build_wide_bvh(tree, W)
+    w = wide.build_wide_bvh(tree, W, max_leaf)
     assert w.status() == 0
     return tree, w
 
@@ -57,6 +57,14 @@ def test_random_layouts_match_oracle(oracle, n, W):
     compare_layout(w, oracle.wide_build(oracle.lbvh_build(verts), W), W)
 
 
+@pytest.mark.parametrize("W,max_leaf", [(4, 1), (4, 2), (8, 1)])
+def test_small_leaf_layouts_match_oracle(oracle, W, max_leaf):
+    for n in (1, 5, 3000):
+        verts = scenes.random_triangles(n, seed=n + 11)
+        _, w = gpu_wide(verts, W, max_leaf=max_leaf)
+        compare_layout(w, oracle.wide_build(oracle.lbvh_build(verts), W, max_leaf), W)
+
+
 @pytest.mark.parametrize("W", [4, 8])
 def test_segmented_layout_matches_oracle(oracle, W):
     verts = scenes.random_triangles(5000, seed=3)
@@ -85,14 +93,14 @@ def _trace(w, rays, mode):
     return hits.cpu().numpy()
 
 
-@pytest.mark.parametrize("W", [4, 8])
+@pytest.mark.parametrize("W,max_leaf", [(4, 4), (8, 4), (4, 1)])
 @pytest.mark.parametrize("mode", [0, 1])
-def test_wide_hits_equal_binary_hits(oracle, golden_dir, mode, W):
+def test_wide_hits_equal_binary_hits(oracle, golden_dir, mode, W, max_leaf):
     g = np.load(os.path.join(golden_dir, "lbvh_fixtures.npz"))
     tg = np.load(os.path.join(golden_dir, "trace_fixtures.npz"))
     for name in FIXTURES:
         verts, rays = g[name + "__verts"], tg[name + "__rays"]
-        _, w = gpu_wide(verts, W)
+        _, w = gpu_wide(verts, W, max_leaf=max_leaf)
         got = _trace(w, rays, mode)
         ref = oracle.trace_bvh2(oracle.lbvh_build(verts), rays, mode)
         assert np.array_equal(got.view(np.uint32), ref.view(np.uint32)), name
@@ -121,12 +129,12 @@ def test_wide_random_rays(oracle, mode, W):
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
 
 
-@pytest.mark.parametrize("W", [4, 8])
-def test_wide_camera_plain_workload(oracle, W):
+@pytest.mark.parametrize("W,max_leaf", [(4, 4), (8, 4), (4, 1)])
+def test_wide_camera_plain_workload(oracle, W, max_leaf):
     """65,536 triangles, 1024x1024 camera rays: wide hits = binary hits, and
     the instrumented counts show fewer node visits than the binary tree."""
     v = scenes.random_triangles(65536, seed=0)
-    tree, w = gpu_wide(v, W)
+    tree, w = gpu_wide(v, W, max_leaf=max_leaf)
     cam = dev(camera.plain_lbvh_camera())
     n = 1024 * 1024
     hw = torch.empty(8 * n, dtype=torch.float32, device="cuda")
@@ -141,5 +149,5 @@ def test_wide_camera_plain_workload(oracle, W):
                             oracle.TRI_WATERTIGHT)
     assert np.array_equal(hw.cpu().numpy().view(np.uint32), ref.view(np.uint32))
     s = stats.view(-1, 2).double().mean(0).cpu().numpy()
-    print(f"W={W}: {s[0]:.2f} wide nodes, {s[1]:.2f} triangles per ray")
+    print(f"W={W} max_leaf={max_leaf}: {s[0]:.2f} wide nodes, {s[1]:.2f} triangles per ray")
     assert s[0] < 24.0  # the binary tree visits ~24 nodes per ray here

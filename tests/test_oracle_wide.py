@@ -1,5 +1,5 @@
 """CPU checks of the wide-BVH oracle (no GPU): the collapsed tree covers every
-triangle exactly once in blocks of at most four, lane boxes are the unions of
+triangle exactly once in blocks of at most max_leaf (1..4), lane boxes are the unions of
 what they hold, child ids follow pre-order, and leaf lanes pack the
 reference's [v0][prim][e1][0][e2][0] record."""
 import numpy as np
@@ -24,7 +24,7 @@ def _scenes():
     yield "segmented", v, np.array([0, 1, 4, 4, 37, 300, 700], np.uint32)
 
 
-def _check_segment(ow, bvh, verts, s, W):
+def _check_segment(ow, bvh, verts, s, W, max_leaf=4):
     nb, ne = int(ow.node_offsets[s]), int(ow.node_offsets[s + 1])
     lb, le = int(ow.leaf_offsets[s]), int(ow.leaf_offsets[s + 1])
     i0, i1 = int(bvh.seg_offsets[s]), int(bvh.seg_offsets[s + 1])
@@ -59,7 +59,7 @@ def _check_segment(ow, bvh, verts, s, W):
                 assert np.array_equal(mn, nodes[c, 0:3][:, ok].min(axis=1))
                 assert np.array_equal(mx, nodes[c, 3:6][:, ok].max(axis=1))
             else:
-                assert 1 <= cnt <= 4
+                assert 1 <= cnt <= max_leaf
                 blk = lb + data
                 assert lb <= blk < le
                 referenced_blocks.append(blk)
@@ -82,13 +82,13 @@ def _check_segment(ow, bvh, verts, s, W):
     assert ne - nb <= max(1, i1 - i0 - 1) and le - lb <= i1 - i0
 
 
-@pytest.mark.parametrize("W", [4, 8])
-def test_oracle_wide_structure(W):
+@pytest.mark.parametrize("W,max_leaf", [(4, 4), (8, 4), (4, 1), (8, 2)])
+def test_oracle_wide_structure(W, max_leaf):
     for name, verts, seg in _scenes():
         bvh = oracle.lbvh_build(verts, seg)
-        ow = oracle.wide_build(bvh, W)
+        ow = oracle.wide_build(bvh, W, max_leaf)
         for s in range(bvh.seg_offsets.size - 1):
-            _check_segment(ow, bvh, np.asarray(verts, np.float32), s, W)
+            _check_segment(ow, bvh, np.asarray(verts, np.float32), s, W, max_leaf)
 
 
 def test_wide_nodes_use_the_width():
