@@ -22,6 +22,8 @@ ERR_DEVICE = 5
 STATUS_LOOKBACK_TIMEOUT = 0x1
 STATUS_STACK_OVERFLOW = 0x2
 STATUS_BAD_TOPOLOGY = 0x4
+STATUS_WIDE_TIMEOUT = 0x40
+STATUS_STAGE_TIMEOUT = 0x80
 TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
@@ -56,7 +58,7 @@ class BajoLbvhC(ctypes.Structure):
         ("n_leaves", _U32), ("n_segments", _U32), ("seg_offsets", _P), ("internal_offsets", _P),
         ("leaf_bounds", _P), ("seg_bounds", _P), ("sort_keys", _P), ("leaf_ids", _P), ("morton_codes", _P),
         ("node_meta", _P), ("node_bounds", _P), ("node_leaf_counts", _P), ("node_flags", _P),
-        ("leaf_parent", _P), ("roots", _P), ("leaf_tris", _P),
+        ("leaf_parent", _P), ("roots", _P), ("leaf_tris", _P), ("top_nodes", _P),
     ]
 
 
@@ -65,7 +67,12 @@ LBVH_ARRAYS = ("internal_offsets", "leaf_bounds", "seg_bounds", "sort_keys", "le
 
 
 class BajoLbvhSizesC(ctypes.Structure):
-    _fields_ = [(name, _SZ) for name in LBVH_ARRAYS] + [("workspace", _SZ)]
+    _fields_ = [(name, _SZ) for name in LBVH_ARRAYS] + [("workspace", _SZ), ("top_nodes", _SZ)]
+
+
+TOP_NODES = 256          # BAJO_TOP_NODES
+TOP_FLAG = 0x40000000    # BAJO_TOP_FLAG
+TOP_BYTES = 16 + 64 * TOP_NODES
 
 
 class BajoWideBvhC(ctypes.Structure):
@@ -97,6 +104,7 @@ SIGNATURES = {
     "bajo_lbvh_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
+    "bajo_lbvh_stage_top": (_I32, [ctypes.POINTER(BajoLbvhC), _P]),
     "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_batch": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, ctypes.c_uint64, _I32, _P, _P,

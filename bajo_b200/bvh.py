@@ -63,9 +63,13 @@ class GpuBvhBuildWorkspace:
 
 
 class GpuTriangleBvh:
-    """Binary LBVH over triangles plus its traversal entry points."""
+    """Binary LBVH over triangles plus its traversal entry points.
 
-    def __init__(self, n_tris: int, seg_offsets: torch.Tensor, device="cuda"):
+    With ``stage_top`` the tree also carries ``top_nodes``, the first
+    BAJO_TOP_NODES nodes of segment 0 in breadth-first order, which the build
+    writes and the closest-hit kernels read from shared memory."""
+
+    def __init__(self, n_tris: int, seg_offsets: torch.Tensor, device="cuda", stage_top: bool = False):
         self.n_leaves = n_tris
         self.n_segments = seg_offsets.numel() - 1
         self.seg_offsets = seg_offsets
@@ -74,17 +78,35 @@ class GpuTriangleBvh:
             dt = _DTYPES[name]
             itemsize = torch.empty(0, dtype=dt).element_size()
             setattr(self, name, torch.empty(sizes[name] // itemsize, dtype=dt, device=device))
+        self.top_nodes = torch.zeros(_lib.TOP_BYTES // 4, dtype=torch.float32, device=device) if stage_top else None
         self.vertices = None
         self._c = None
 
-    def c_struct(self) -> BajoLbvhC:
+    def c_struct(self, stage_top: bool = True) -> BajoLbvhC:
+        """The C record of this tree; ``stage_top=False`` leaves top_nodes
+        NULL (builds through it do not stage, traces through it read the
+        whole tree from global memory)."""
         c = BajoLbvhC()
         c.n_leaves, c.n_segments = self.n_leaves, self.n_segments
         c.seg_offsets = self.seg_offsets.data_ptr()
         for name in LBVH_ARRAYS:
             setattr(c, name, getattr(self, name).data_ptr())
+        c.top_nodes = self.top_nodes.data_ptr() if stage_top and self.top_nodes is not None else None
         self._c = c
         return c
+
+    def restage_top(self, stream=None) -> None:
+        """Rewrite top_nodes from the current nodes (bajo_lbvh_stage_top)."""
+        if self.top_nodes is None:
+            raise ValueError("this tree was created without stage_top")
+        c = self.c_struct()
+        _lib.check(_lib.load().bajo_lbvh_stage_top(ctypes.byref(c), _lib.stream_handle(stream)),
+                   "bajo_lbvh_stage_top")
+
+    def top_header(self) -> tuple[int, int]:
+        """(staged node count, root ref) of top_nodes."""
+        h = self.top_nodes[:2].view(torch.int32).cpu().numpy().view(np.uint32)
+        return int(h[0]), int(h[1])
 
     @property
     def internal_count(self) -> int:
@@ -146,12 +168,15 @@ def _ptr(t):
 
 
 def build_triangle_bvh(vertices: torch.Tensor, seg_offsets=None, workspace: GpuBvhBuildWorkspace | None = None,
-                       out: GpuTriangleBvh | None = None, stream=None) -> GpuTriangleBvh:
+                       out: GpuTriangleBvh | None = None, stream=None,
+                       stage_top: bool | None = None) -> GpuTriangleBvh:
     """Build the binary LBVH of `vertices` (9 floats per triangle, CUDA).
 
     `seg_offsets` (optional, S+1 item offsets) builds one independent tree per
     segment in the same launches (the batched BLAS path,
-    bajo/bvh/gpu/triangle_bvh.mojo:469)."""
+    bajo/bvh/gpu/triangle_bvh.mojo:469).  `stage_top` also writes the staged
+    top levels for the traversal (off by default: on B200 the top of the tree
+    stays in L1 and the staged kernels were measured no faster)."""
     _lib.require_cuda(vertices)
     if vertices.dtype != torch.float32 or not vertices.is_contiguous() or vertices.numel() % 9:
         raise ValueError("triangle vertex buffer must be contiguous float32 with 9 floats per triangle")
@@ -170,14 +195,16 @@ def build_triangle_bvh(vertices: torch.Tensor, seg_offsets=None, workspace: GpuB
     S = seg.numel() - 1
     if S < 1:
         raise ValueError("at least one segment is required")
+    if stage_top is None:
+        stage_top = False
     if workspace is None or workspace.n_tris != n or workspace.n_segments != S:
         workspace = GpuBvhBuildWorkspace(n, S, device=vertices.device)
-    bvh = out if out is not None and out.n_leaves == n and out.n_segments == S else GpuTriangleBvh(n, seg,
-                                                                                                 vertices.device)
+    reuse = out is not None and out.n_leaves == n and out.n_segments == S and (out.top_nodes is not None or not stage_top)
+    bvh = out if reuse else GpuTriangleBvh(n, seg, vertices.device, stage_top=stage_top)
     bvh.seg_offsets = seg
     bvh.vertices = vertices
     bvh.workspace = workspace
-    c = bvh.c_struct()
+    c = bvh.c_struct(stage_top)
     rc = _lib.load().bajo_lbvh_build(vertices.data_ptr(), ctypes.byref(c), workspace.buffer.data_ptr(),
                                      workspace.buffer.numel(), _lib.stream_handle(stream))
     _lib.check(rc, "bajo_lbvh_build")

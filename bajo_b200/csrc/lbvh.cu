@@ -408,6 +408,103 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 }
 
 // ---------------------------------------------------------------------------
+// staged top levels
+// ---------------------------------------------------------------------------
+// The first BAJO_TOP_NODES internal nodes of segment 0's tree in breadth-first
+// order (left before right), one level per round: every frontier node counts
+// its internal children, a block scan gives them consecutive slots, and the
+// children that fit become the next frontier.  Nodes whose children fall past
+// the last slot keep their global refs, so any prefix of levels is a valid
+// tree top.  Output layout: header [count, root ref, 0, 0] then 64-byte
+// records [left AABB | right AABB | left ref, right ref, 0, 0].
+constexpr uint32_t kTop = BAJO_TOP_NODES;
+static_assert(kTop % 32 == 0 && kTop <= 1024, "one thread per slot");
+
+__global__ void __launch_bounds__(kTop) stage_top_kernel(const uint32_t* __restrict__ roots,
+                                                         const uint4* __restrict__ meta,
+                                                         const float4* __restrict__ nb, uint32_t n_leaves,
+                                                         float4* __restrict__ out) {
+  __shared__ uint32_t s_ref[kTop];
+  __shared__ uint2 s_child[kTop];
+  __shared__ uint32_t s_warp[kTop / 32];
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint32_t root = __ldg(roots);
+  const bool stage = root != kSentinel && !(root & kLeafFlag) && n_leaves < BAJO_TOP_FLAG;
+  if (t == 0) s_ref[0] = root;
+  __syncthreads();
+  uint32_t lo = 0, hi = stage ? 1u : 0u;
+  while (lo < hi) {  // block-uniform
+    const bool mine = t >= lo && t < hi;
+    uint32_t cl = 0, cr = 0, cnt = 0;
+    if (mine) {
+      const uint4 m = __ldg(meta + s_ref[t]);
+      cl = m.y;
+      cr = m.z;
+      cnt = (uint32_t)!(cl & kLeafFlag) + (uint32_t)!(cr & kLeafFlag);
+    }
+    // exclusive block scan of cnt
+    uint32_t incl = cnt;
+    for (int d = 1; d < 32; d <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+      if ((int)lane >= d) incl += y;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+    for (uint32_t w = 0; w < kTop / 32; ++w) {
+      const uint32_t c = s_warp[w];
+      before += w < warp ? c : 0u;
+      total += c;
+    }
+    if (mine) {
+      uint32_t k = hi + before + incl - cnt;
+      uint32_t rl = cl, rr = cr;
+      if (!(cl & kLeafFlag)) {
+        if (k < kTop) {
+          s_ref[k] = cl;
+          rl = BAJO_TOP_FLAG | k;
+        }
+        ++k;
+      }
+      if (!(cr & kLeafFlag)) {
+        if (k < kTop) {
+          s_ref[k] = cr;
+          rr = BAJO_TOP_FLAG | k;
+        }
+      }
+      s_child[t] = make_uint2(rl, rr);
+    }
+    __syncthreads();
+    lo = hi;
+    hi = min(kTop, hi + total);
+  }
+  const uint32_t n_staged = hi;
+  float4* rec = out + 1 + (size_t)t * 4;
+  if (t < n_staged) {
+    const uint32_t r = s_ref[t];
+    rec[0] = __ldg(nb + (size_t)r * 3 + 0);
+    rec[1] = __ldg(nb + (size_t)r * 3 + 1);
+    rec[2] = __ldg(nb + (size_t)r * 3 + 2);
+    const uint2 c = s_child[t];
+    rec[3] = make_float4(__uint_as_float(c.x), __uint_as_float(c.y), 0.0f, 0.0f);
+  } else {
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    rec[0] = z;
+    rec[1] = z;
+    rec[2] = z;
+    rec[3] = z;
+  }
+  if (t == 0) out[0] = make_float4(__uint_as_float(n_staged), __uint_as_float(root), 0.0f, 0.0f);
+}
+
+cudaError_t launch_stage_top(const BajoLbvh* bvh, cudaStream_t st) {
+  stage_top_kernel<<<1, kTop, 0, st>>>(bvh->roots, reinterpret_cast<const uint4*>(bvh->node_meta),
+                                       reinterpret_cast<const float4*>(bvh->node_bounds), bvh->n_leaves,
+                                       reinterpret_cast<float4*>(bvh->top_nodes));
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // host plan
 // ---------------------------------------------------------------------------
 // Build workspace: the sort plan of the u64 keys, with the per-segment
@@ -455,6 +552,7 @@ int32_t bajo_lbvh_sizes(uint32_t n, uint32_t n_seg, BajoLbvhSizes* s) {
   s->roots = (size_t)n_seg * 4;
   s->leaf_tris = N * 48;
   s->workspace = bajo::make_build_plan(n, n_seg).total;
+  s->top_nodes = BAJO_TOP_BYTES;
   return BAJO_OK;
 }
 
@@ -468,6 +566,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
                 !bvh->leaf_ids || !bvh->morton_codes || !bvh->node_meta || !bvh->node_bounds ||
                 !bvh->node_leaf_counts || !bvh->node_flags || !bvh->leaf_parent || !bvh->roots || !bvh->leaf_tris))
     return BAJO_ERR_INVALID_ARGUMENT;
+  if (bvh->top_nodes && ((uintptr_t)bvh->top_nodes & 15)) return BAJO_ERR_INVALID_ARGUMENT;
   BuildPlan plan = make_build_plan(n, S);
   if (ws_bytes < plan.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
   if (ev && n_ev < (int32_t)(5 + plan.sort.passes)) return BAJO_ERR_INVALID_ARGUMENT;
@@ -542,6 +641,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
     if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
   }
   if (!mark(4 + passes)) return BAJO_ERR_CUDA;
+  if (bvh->top_nodes && launch_stage_top(bvh, st) != cudaSuccess) return BAJO_ERR_CUDA;
   return BAJO_OK;
 }
 
@@ -553,6 +653,13 @@ int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* ws, siz
                               void* const* events, int32_t n_events) {
   if (!events) return BAJO_ERR_INVALID_ARGUMENT;
   return lbvh_build_impl(d_verts, bvh, ws, ws_bytes, stream, (cudaEvent_t*)events, n_events);
+}
+
+int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream) {
+  if (!bvh || !bvh->top_nodes || !bvh->roots || !bvh->node_meta || !bvh->node_bounds ||
+      ((uintptr_t)bvh->top_nodes & 15))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  return bajo::launch_stage_top(bvh, (cudaStream_t)stream) == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {

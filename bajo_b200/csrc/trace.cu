@@ -30,46 +30,73 @@ __device__ __forceinline__ void store_hit(const Hit& h, const float4* __restrict
   if (out_prim) out_prim[i] = h.prim;
 }
 
-template <int MODE>
-__global__ void __launch_bounds__(kTraceBlock) trace_rays_kernel(const float* __restrict__ rays, uint32_t n,
-                                                                 uint32_t n_nodes,
-                                                                 const uint32_t* __restrict__ roots,
-                                                                 const float4* __restrict__ nb,
-                                                                 const uint4* __restrict__ meta,
-                                                                 const float4* __restrict__ tris,
-                                                                 float* __restrict__ hits8, float* __restrict__ out_t,
-                                                                 uint32_t* __restrict__ out_prim,
-                                                                 uint32_t* __restrict__ status) {
-  const uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x;
-  if (i >= n) return;
+// Kernels with TOP read the staged top levels from shared memory; they run
+// one persistent block per resident slot (kTopBlock threads, grid-stride over
+// the rays) so that each block copies the records once.
+constexpr int kTopBlock = 512;
+constexpr int kTopMinBlocks = 2;  // 64 registers: as many warps per SM as the 128-thread kernels
+
+template <bool TOP>
+struct StageSmem {
+  using type = char;
+};
+template <>
+struct StageSmem<true> {
+  using type = TopSmem;
+};
+
+template <int MODE, bool TOP>
+__device__ __forceinline__ void ray_query(uint32_t i, const float* __restrict__ rays, uint32_t n, uint32_t n_nodes,
+                                          uint32_t root, const float4* __restrict__ nb,
+                                          const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                                          const float4* top, float* __restrict__ hits8, float* __restrict__ out_t,
+                                          uint32_t* __restrict__ out_prim, uint32_t* __restrict__ status) {
   // field-major ray planes (ray_launch.mojo:95-112)
   f3 o = mk(rays[i], rays[(size_t)n + i], rays[2 * (size_t)n + i]);
   float tmin = rays[3 * (size_t)n + i];
   f3 d = mk(rays[4 * (size_t)n + i], rays[5 * (size_t)n + i], rays[6 * (size_t)n + i]);
   float tmax = rays[7 * (size_t)n + i];
   Ray r = make_ray(o, d, tmin, tmax);
-  Hit h = trace_bvh2<MODE>(r, __ldg(roots), nb, meta, tris, n_nodes, status);
+  Hit h;
+  if constexpr (TOP) h = trace_bvh2_top<MODE>(r, root, nb, meta, tris, n_nodes, status, top);
+  else h = trace_bvh2<MODE>(r, root, nb, meta, tris, n_nodes, status);
   store_hit(h, tris, i, hits8, out_t, out_prim);
+}
+
+// Unstaged: 10 blocks of 128 per SM (48 registers): general rays are mostly
+// incoherent and latency bound, and the extra warps outweigh the spills
+// (+5% to +8% on random rays against 64 registers).
+template <int MODE, bool TOP>
+__global__ void __launch_bounds__(TOP ? kTopBlock : kTraceBlock, TOP ? kTopMinBlocks : 10)
+    trace_rays_kernel(const float* __restrict__ rays, uint32_t n, uint32_t n_nodes, const uint32_t* __restrict__ roots,
+                      const float4* __restrict__ nb, const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                      const float4* __restrict__ top_g, float* __restrict__ hits8, float* __restrict__ out_t,
+                      uint32_t* __restrict__ out_prim, uint32_t* __restrict__ status) {
+  __shared__ typename StageSmem<TOP>::type sm;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (TOP) {
+    const uint32_t root = __ldg(roots);
+    const float4* top = stage_top(sm, top_g, root, status);
+    for (uint32_t i = i0; i < n; i += gridDim.x * blockDim.x)
+      ray_query<MODE, TOP>(i, rays, n, n_nodes, root, nb, meta, tris, top, hits8, out_t, out_prim, status);
+    stage_top_drain(sm, top);
+  } else if (i0 < n) {
+    ray_query<MODE, TOP>(i0, rays, n, n_nodes, __ldg(roots), nb, meta, tris, nullptr, hits8, out_t, out_prim,
+                         status);
+  }
 }
 
 // camera.mojo:137-154 make_ray_raster; camera_launch.mojo:34-55.  With STATS
 // it also writes per-ray [node visits, triangle tests] like the reference's
 // instrumented kernel (triangle_bvh.mojo:813, GpuTraversalStats trace.mojo:62).
-template <int MODE, bool STATS = false>
-__global__ void __launch_bounds__(kTraceBlock) trace_camera_kernel(const float* __restrict__ cams, uint32_t n,
-                                                                   uint32_t n_nodes, uint32_t width,
-                                                                   uint32_t height, float inv_h,
-                                                                   const uint32_t* __restrict__ roots,
-                                                                   const float4* __restrict__ nb,
-                                                                   const uint4* __restrict__ meta,
-                                                                   const float4* __restrict__ tris,
-                                                                   float* __restrict__ hits8,
-                                                                   float* __restrict__ out_t,
-                                                                   uint32_t* __restrict__ out_prim,
-                                                                   uint32_t* __restrict__ status,
-                                                                   uint32_t* __restrict__ stats = nullptr) {
-  const uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x;
-  if (i >= n) return;
+template <int MODE, bool STATS, bool TOP>
+__device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__ cams, uint32_t n_nodes,
+                                           uint32_t width, uint32_t height, float inv_h, uint32_t root,
+                                           const float4* __restrict__ nb, const uint4* __restrict__ meta,
+                                           const float4* __restrict__ tris, const float4* top,
+                                           float* __restrict__ hits8, float* __restrict__ out_t,
+                                           uint32_t* __restrict__ out_prim, uint32_t* __restrict__ status,
+                                           uint32_t* __restrict__ stats) {
   const uint32_t ppv = width * height;
   const uint32_t view = i / ppv, local = i - view * ppv;
   const float* c = cams + (size_t)view * 20;
@@ -83,9 +110,34 @@ __global__ void __launch_bounds__(kTraceBlock) trace_camera_kernel(const float* 
   f3 dir = normalize((fwd + right * (sx * fs)) + up * (sy * fs));
   Ray r = make_ray(mk(__ldg(c + 0), __ldg(c + 1), __ldg(c + 2)), dir, 0.0f, FLT_MAX);
   uint32_t nn = 0, nt = 0;
-  Hit h = trace_bvh2<MODE, STATS>(r, __ldg(roots), nb, meta, tris, n_nodes, status, &nn, &nt);
+  Hit h;
+  if constexpr (TOP) h = trace_bvh2_top<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, top, &nn, &nt);
+  else h = trace_bvh2<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, &nn, &nt);
   store_hit(h, tris, i, hits8, out_t, out_prim);
   if constexpr (STATS) reinterpret_cast<uint2*>(stats)[i] = make_uint2(nn, nt);
+}
+
+template <int MODE, bool STATS, bool TOP>
+__global__ void __launch_bounds__(TOP ? kTopBlock : kTraceBlock, TOP ? kTopMinBlocks : 0)
+    trace_camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t n_nodes, uint32_t width, uint32_t height,
+                        float inv_h, const uint32_t* __restrict__ roots, const float4* __restrict__ nb,
+                        const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                        const float4* __restrict__ top_g, float* __restrict__ hits8, float* __restrict__ out_t,
+                        uint32_t* __restrict__ out_prim, uint32_t* __restrict__ status,
+                        uint32_t* __restrict__ stats) {
+  __shared__ typename StageSmem<TOP>::type sm;
+  const uint32_t i0 = blockIdx.x * blockDim.x + threadIdx.x;
+  if constexpr (TOP) {
+    const uint32_t root = __ldg(roots);
+    const float4* top = stage_top(sm, top_g, root, status);
+    for (uint32_t i = i0; i < n; i += gridDim.x * blockDim.x)
+      camera_ray<MODE, STATS, TOP>(i, cams, n_nodes, width, height, inv_h, root, nb, meta, tris, top, hits8, out_t,
+                                   out_prim, status, stats);
+    stage_top_drain(sm, top);
+  } else if (i0 < n) {
+    camera_ray<MODE, STATS, TOP>(i0, cams, n_nodes, width, height, inv_h, __ldg(roots), nb, meta, tris, nullptr,
+                                 hits8, out_t, out_prim, status, stats);
+  }
 }
 
 // Batched closest hits over a segmented LBVH: ray i belongs to scene
@@ -139,7 +191,63 @@ __global__ void __launch_bounds__(kTraceBlock) batch_trace_kernel(
 }
 
 bool bvh_ok(const BajoLbvh* b) {
-  return b && b->roots && b->node_bounds && b->node_meta && b->leaf_tris && b->n_segments >= 1;
+  return b && b->roots && b->node_bounds && b->node_meta && b->leaf_tris && b->n_segments >= 1 &&
+         !((uintptr_t)b->top_nodes & 15);
+}
+
+// Grid of a TOP kernel: every resident block slot once, at most one ray per
+// thread.
+template <typename Kernel>
+uint32_t top_grid(Kernel kernel, uint32_t n) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kTopBlock, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  const uint32_t cap = (uint32_t)per_sm * (uint32_t)sm_count();
+  const uint32_t need = (n + kTopBlock - 1) / kTopBlock;
+  return need < cap ? need : cap;
+}
+
+template <int MODE, bool TOP>
+void launch_rays(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
+                 uint32_t* status, cudaStream_t st) {
+  const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
+  const uint4* meta = reinterpret_cast<const uint4*>(b->node_meta);
+  const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
+  const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
+  const uint32_t grid = TOP ? top_grid(trace_rays_kernel<MODE, TOP>, n) : (n + kTraceBlock - 1) / kTraceBlock;
+  trace_rays_kernel<MODE, TOP><<<grid, TOP ? kTopBlock : kTraceBlock, 0, st>>>(rays, n, b->n_leaves, b->roots, nb,
+                                                                               meta, tris, top, hits8, t, prim,
+                                                                               status);
+}
+
+template <int MODE, bool STATS, bool TOP>
+void launch_camera(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height, float* hits8,
+                   float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
+  const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
+  const uint4* meta = reinterpret_cast<const uint4*>(b->node_meta);
+  const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
+  const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
+  const float inv_h = 1.0f / (float)height;
+  const uint32_t grid =
+      TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (n + kTraceBlock - 1) / kTraceBlock;
+  trace_camera_kernel<MODE, STATS, TOP><<<grid, TOP ? kTopBlock : kTraceBlock, 0, st>>>(
+      cams, n, b->n_leaves, width, height, inv_h, b->roots, nb, meta, tris, top, hits8, t, prim, status, stats);
+}
+
+template <bool STATS>
+void launch_camera_any(const BajoLbvh* b, int32_t mode, const float* cams, uint32_t n, uint32_t width,
+                       uint32_t height, float* hits8, float* t, uint32_t* prim, uint32_t* status, uint32_t* stats,
+                       cudaStream_t st) {
+  const bool top = b->top_nodes != nullptr;
+  if (mode == BAJO_TRI_MT) {
+    if (top) launch_camera<BAJO_TRI_MT, STATS, true>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+    else launch_camera<BAJO_TRI_MT, STATS, false>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+  } else {
+    if (top)
+      launch_camera<BAJO_TRI_WATERTIGHT, STATS, true>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+    else
+      launch_camera<BAJO_TRI_WATERTIGHT, STATS, false>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+  }
 }
 
 }  // namespace
@@ -153,17 +261,15 @@ int32_t bajo_trace_rays(const BajoLbvh* bvh, const float* d_rays, uint32_t n, in
   if (!bvh_ok(bvh) || (n && !d_rays) || (mode != BAJO_TRI_MT && mode != BAJO_TRI_WATERTIGHT))
     return BAJO_ERR_INVALID_ARGUMENT;
   if (n == 0) return BAJO_OK;
-  const uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
-  const float4* nb = reinterpret_cast<const float4*>(bvh->node_bounds);
-  const uint4* meta = reinterpret_cast<const uint4*>(bvh->node_meta);
-  const float4* tris = reinterpret_cast<const float4*>(bvh->leaf_tris);
   cudaStream_t st = (cudaStream_t)stream;
-  if (mode == BAJO_TRI_MT)
-    trace_rays_kernel<BAJO_TRI_MT><<<grid, kTraceBlock, 0, st>>>(d_rays, n, bvh->n_leaves, bvh->roots, nb, meta, tris, d_hits8, d_t,
-                                                                 d_prim, d_status);
-  else
-    trace_rays_kernel<BAJO_TRI_WATERTIGHT><<<grid, kTraceBlock, 0, st>>>(d_rays, n, bvh->n_leaves, bvh->roots, nb, meta, tris,
-                                                                         d_hits8, d_t, d_prim, d_status);
+  const bool top = bvh->top_nodes != nullptr;
+  if (mode == BAJO_TRI_MT) {
+    if (top) launch_rays<BAJO_TRI_MT, true>(bvh, d_rays, n, d_hits8, d_t, d_prim, d_status, st);
+    else launch_rays<BAJO_TRI_MT, false>(bvh, d_rays, n, d_hits8, d_t, d_prim, d_status, st);
+  } else {
+    if (top) launch_rays<BAJO_TRI_WATERTIGHT, true>(bvh, d_rays, n, d_hits8, d_t, d_prim, d_status, st);
+    else launch_rays<BAJO_TRI_WATERTIGHT, false>(bvh, d_rays, n, d_hits8, d_t, d_prim, d_status, st);
+  }
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
@@ -176,18 +282,8 @@ int32_t bajo_trace_camera(const BajoLbvh* bvh, const float* d_cams, uint32_t n, 
     return BAJO_ERR_INVALID_ARGUMENT;
   if ((uint64_t)width * height > 0xFFFFFFFFull) return BAJO_ERR_TOO_LARGE;
   if (n == 0) return BAJO_OK;
-  const uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
-  const float inv_h = 1.0f / (float)height;
-  const float4* nb = reinterpret_cast<const float4*>(bvh->node_bounds);
-  const uint4* meta = reinterpret_cast<const uint4*>(bvh->node_meta);
-  const float4* tris = reinterpret_cast<const float4*>(bvh->leaf_tris);
-  cudaStream_t st = (cudaStream_t)stream;
-  if (mode == BAJO_TRI_MT)
-    trace_camera_kernel<BAJO_TRI_MT><<<grid, kTraceBlock, 0, st>>>(d_cams, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb,
-                                                                   meta, tris, d_hits8, d_t, d_prim, d_status);
-  else
-    trace_camera_kernel<BAJO_TRI_WATERTIGHT><<<grid, kTraceBlock, 0, st>>>(
-        d_cams, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb, meta, tris, d_hits8, d_t, d_prim, d_status);
+  launch_camera_any<false>(bvh, mode, d_cams, n, width, height, d_hits8, d_t, d_prim, d_status, nullptr,
+                           (cudaStream_t)stream);
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
@@ -229,18 +325,8 @@ int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cams, uint32
     return BAJO_ERR_INVALID_ARGUMENT;
   if ((uint64_t)width * height > 0xFFFFFFFFull) return BAJO_ERR_TOO_LARGE;
   if (n == 0) return BAJO_OK;
-  const uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
-  const float inv_h = 1.0f / (float)height;
-  const float4* nb = reinterpret_cast<const float4*>(bvh->node_bounds);
-  const uint4* meta = reinterpret_cast<const uint4*>(bvh->node_meta);
-  const float4* tris = reinterpret_cast<const float4*>(bvh->leaf_tris);
-  cudaStream_t st = (cudaStream_t)stream;
-  if (mode == BAJO_TRI_MT)
-    trace_camera_kernel<BAJO_TRI_MT, true><<<grid, kTraceBlock, 0, st>>>(
-        d_cams, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb, meta, tris, d_hits8, nullptr, nullptr, nullptr, d_stats);
-  else
-    trace_camera_kernel<BAJO_TRI_WATERTIGHT, true><<<grid, kTraceBlock, 0, st>>>(
-        d_cams, n, bvh->n_leaves, width, height, inv_h, bvh->roots, nb, meta, tris, d_hits8, nullptr, nullptr, nullptr, d_stats);
+  launch_camera_any<true>(bvh, mode, d_cams, n, width, height, d_hits8, nullptr, nullptr, nullptr, d_stats,
+                          (cudaStream_t)stream);
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 

@@ -17,6 +17,12 @@
 //  - BAJO_TRI_WATERTIGHT selects the watertight test of Woop, Benthin and
 //    Wald (JCGT 2013); BAJO_TRI_MT is the reference's Moller-Trumbore
 //    (bajo/core/intersect.mojo:415-459).
+//
+// With TOP, the first BAJO_TOP_NODES nodes of the tree (breadth first, built
+// by the LBVH build into BajoLbvh::top_nodes) are read from shared memory:
+// each block copies them once with a bulk asynchronous copy (TMA) completing
+// on an mbarrier.  Refs tagged BAJO_TOP_FLAG name a staged slot; the boxes and
+// child order are the same, so the hits are the same.
 #pragma once
 
 #include "bajo_common.cuh"
@@ -178,13 +184,84 @@ __device__ __forceinline__ void test_tri(const Ray& r, const float4* __restrict_
   }
 }
 
+// ---- staged top levels -----------------------------------------------------
+constexpr uint32_t kTopMask = BAJO_TOP_FLAG - 1u;
+constexpr uint32_t kTopFloat4 = 1u + 4u * BAJO_TOP_NODES;  // header + records
+constexpr uint64_t kStageWaitNs = 200000000ull;            // 200 ms
+
+struct TopSmem {
+  float4 rec[kTopFloat4];
+  unsigned long long bar;
+};
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_timer_ns();
+  while (!mbar_try_wait(bar, parity))
+    if (global_timer_ns() - t0 > kStageWaitNs) return false;
+  return true;
+}
+
+// Copies the staged top levels (g, BAJO_TOP_BYTES, 16-byte aligned) into
+// shared memory: thread 0 arms the mbarrier with the byte count and issues
+// one cp.async.bulk (no multicast); every thread waits, at most 200 ms.
+// Returns the records when the copy arrived and belongs to `root`, else
+// nullptr (the caller traverses from global memory; a timeout also raises
+// BAJO_STATUS_STAGE_TIMEOUT).  Must be called by every thread of the block.
+__device__ __forceinline__ const float4* stage_top(TopSmem& sm, const float4* __restrict__ g, uint32_t root,
+                                                   uint32_t* status) {
+  const uint32_t bar = smem_addr(&sm.bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(BAJO_TOP_BYTES)
+                 : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(sm.rec)),
+                 "l"(g), "r"(BAJO_TOP_BYTES), "r"(bar)
+                 : "memory");
+  }
+  if (!mbar_wait_bounded(bar, 0)) {
+    raise_status(status, BAJO_STATUS_STAGE_TIMEOUT);
+    return nullptr;
+  }
+  const float4 h = sm.rec[0];
+  const uint32_t count = __float_as_uint(h.x);
+  if (count == 0 || count > BAJO_TOP_NODES || __float_as_uint(h.y) != root) return nullptr;
+  return sm.rec + 1;
+}
+
+// A block that gave up waiting must not leave while the copy may still land
+// in its shared memory: wait once more (bounded) before returning.
+__device__ __forceinline__ void stage_top_drain(TopSmem& sm, const float4* staged) {
+  if (staged == nullptr && threadIdx.x == 0) mbar_wait_bounded(smem_addr(&sm.bar), 0);
+}
+
 // max_nodes: node visits allowed (the node count): a tree is never visited
-// twice per node, so more visits means a corrupt tree.
-template <int MODE, bool STATS, bool ANY, bool PAR>
+// twice per node, so more visits means a corrupt tree.  With TOP, `top` holds
+// the staged records and refs tagged BAJO_TOP_FLAG are read from it.
+template <int MODE, bool STATS, bool ANY, bool PAR, bool TOP = false>
 __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                                const uint4* __restrict__ meta, const float4* __restrict__ tris,
                                                uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes,
-                                               uint32_t* n_tris) {
+                                               uint32_t* n_tris, const float4* top = nullptr) {
   Hit h;
   h.t = r.tmax;
   h.u = h.v = 0.0f;
@@ -202,30 +279,43 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
   int sp = 0;
   uint32_t cur = root;
   for (uint32_t visits = 0;; ++visits) {
-    if (visits >= max_nodes || cur >= max_nodes) {
+    const bool staged = TOP && (cur & BAJO_TOP_FLAG);
+    if (visits >= max_nodes || (staged ? (cur & kTopMask) >= BAJO_TOP_NODES : cur >= max_nodes)) {
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
       break;
     }
     if constexpr (STATS) ++*n_nodes;
-    const float4 b0 = __ldg(nb + (size_t)cur * 3 + 0);  // L: min xyz, max x
-    const float4 b1 = __ldg(nb + (size_t)cur * 3 + 1);  // L: max yz | R: min xy
-    const float4 b2 = __ldg(nb + (size_t)cur * 3 + 2);  // R: min z, max xyz
-    const uint4 m = __ldg(meta + cur);
+    float4 b0, b1, b2;  // b0 L: min xyz, max x | b1 L: max yz, R: min xy | b2 R: min z, max xyz
+    uint2 m;            // left, right child refs
+    if (staged) {
+      const float4* p = top + (size_t)(cur & kTopMask) * 4;
+      b0 = p[0];
+      b1 = p[1];
+      b2 = p[2];
+      const float4 c = p[3];
+      m = make_uint2(__float_as_uint(c.x), __float_as_uint(c.y));
+    } else {
+      b0 = __ldg(nb + (size_t)cur * 3 + 0);
+      b1 = __ldg(nb + (size_t)cur * 3 + 1);
+      b2 = __ldg(nb + (size_t)cur * 3 + 2);
+      const uint4 g = __ldg(meta + cur);
+      m = make_uint2(g.y, g.z);
+    }
     float tl, tr;
     const float limit0 = ANY ? r.tmax : h.t;
     const bool hl = box_hit<PAR>(r, b0, make_float2(b1.x, b1.y), limit0, tl);
     const bool hr = box_hit<PAR>(r, make_float4(b1.z, b1.w, b2.x, b2.y), make_float2(b2.z, b2.w), limit0, tr);
     bool vl = false, vr = false;
     if (hl) {
-      if (m.y & kLeafFlag) {
-        test_tri<MODE>(r, tris, m.y & kIndexMask, h);
+      if (m.x & kLeafFlag) {
+        test_tri<MODE>(r, tris, m.x & kIndexMask, h);
         if constexpr (STATS) ++*n_tris;
         if (ANY && h.leaf != kEmpty) return h;
       } else vl = true;
     }
     if (hr) {
-      if (m.z & kLeafFlag) {
-        test_tri<MODE>(r, tris, m.z & kIndexMask, h);
+      if (m.y & kLeafFlag) {
+        test_tri<MODE>(r, tris, m.y & kIndexMask, h);
         if constexpr (STATS) ++*n_tris;
         if (ANY && h.leaf != kEmpty) return h;
       } else vr = true;
@@ -239,11 +329,11 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
       const float far_t = near == 0 ? tr : tl;
       const float near_t = near == 0 ? tl : tr;
       if (far_valid && far_t <= limit) {
-        if (sp < kStack) stack[sp++] = near == 0 ? m.z : m.y;
+        if (sp < kStack) stack[sp++] = near == 0 ? m.y : m.x;
         else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
       }
       if (near_t <= limit) {
-        cur = near == 0 ? m.y : m.z;
+        cur = near == 0 ? m.x : m.y;
         continue;
       }
     }
@@ -263,6 +353,23 @@ __device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const flo
   if (has_parallel_axis(r))
     return trace_bvh2_impl<MODE, STATS, ANY, true>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
   return trace_bvh2_impl<MODE, STATS, ANY, false>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
+}
+
+// Same, starting from the staged top (slot 0 is `root`) when `top` is set.
+// Trees of 2^30 or more nodes are never staged (the build leaves the count 0).
+template <int MODE, bool STATS = false, bool ANY = false>
+__device__ __forceinline__ Hit trace_bvh2_top(const Ray& r, uint32_t root, const float4* __restrict__ nb,
+                                              const uint4* __restrict__ meta, const float4* __restrict__ tris,
+                                              uint32_t max_nodes, uint32_t* status, const float4* top,
+                                              uint32_t* n_nodes = nullptr, uint32_t* n_tris = nullptr) {
+  // without staged records no ref carries BAJO_TOP_FLAG (node indices stay
+  // below 2^30), so the same loop runs from the global root
+  const uint32_t start = top ? BAJO_TOP_FLAG : root;
+  if (has_parallel_axis(r))
+    return trace_bvh2_impl<MODE, STATS, ANY, true, true>(r, start, nb, meta, tris, max_nodes, status, n_nodes,
+                                                         n_tris, top);
+  return trace_bvh2_impl<MODE, STATS, ANY, false, true>(r, start, nb, meta, tris, max_nodes, status, n_nodes,
+                                                        n_tris, top);
 }
 
 }  // namespace trav

@@ -68,6 +68,7 @@ def parse():
     p.add_argument("--height", type=int, default=720, help="--case guided image height")
     p.add_argument("--ref-spp", type=int, default=4096, help="--case guided reference samples per pixel")
     p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
+    p.add_argument("--spp", type=int, default=64, help="--case render samples per pixel")
     p.add_argument("--train-passes", type=int, default=8, help="--case guided passes followed by training")
     p.add_argument("--train-steps", type=int, default=8, help="--case guided Adam steps per training pass")
     return p.parse_args()
@@ -285,7 +286,10 @@ def run_bajo(args):
     verts = torch.from_numpy(verts_h).to(dev)
     ws = bvh.GpuBvhBuildWorkspace(N_TRIS, 1, device=dev)
     tree = bvh.build_triangle_bvh(verts, workspace=ws)
-    c = tree.c_struct()
+    # builds go through a record without top_nodes (the reference's build);
+    # traces through one with the staged top levels the first build wrote
+    c = tree.c_struct(stage_top=False)
+    c_trace = tree.c_struct()
     cam = torch.from_numpy(camera.plain_lbvh_camera()).to(dev)
     n_rays = WIDTH * HEIGHT
     hits = torch.empty(8 * n_rays, dtype=torch.float32, device=dev)
@@ -313,8 +317,8 @@ def run_bajo(args):
         return evs
 
     def trace(h=None):
-        _lib.check(L.bajo_trace_camera(ctypes.byref(c), cam.data_ptr(), n_rays, WIDTH, HEIGHT, _lib.TRI_WATERTIGHT,
-                                       h.data_ptr(), None, None, None, sh), "bajo_trace_camera")
+        _lib.check(L.bajo_trace_camera(ctypes.byref(c_trace), cam.data_ptr(), n_rays, WIDTH, HEIGHT,
+                                       _lib.TRI_WATERTIGHT, h.data_ptr(), None, None, None, sh), "bajo_trace_camera")
 
     # ---- warm-up
     evs = new_events(n_ev)
@@ -375,7 +379,7 @@ def run_bajo(args):
 
     # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
     stats = torch.empty(2 * n_rays, dtype=torch.int32, device=dev)
-    _lib.check(L.bajo_trace_camera_stats(ctypes.byref(c), cam.data_ptr(), n_rays, WIDTH, HEIGHT,
+    _lib.check(L.bajo_trace_camera_stats(ctypes.byref(c_trace), cam.data_ptr(), n_rays, WIDTH, HEIGHT,
                                          _lib.TRI_WATERTIGHT, None, stats.data_ptr(), sh), "bajo_trace_camera_stats")
     torch.cuda.synchronize()
     st = stats.view(-1, 2).double()
@@ -388,7 +392,7 @@ def run_bajo(args):
     out_h = torch.empty(12, dtype=torch.float32).pin_memory()
     st_h = torch.empty(1, dtype=torch.int32).pin_memory()
     e2e_v = torch.empty_like(verts)
-    c_e2e = tree.c_struct()  # the C-ABI call a host makes, with its tree record prepared once
+    c_e2e = tree.c_struct(stage_top=False)  # the C-ABI call a host makes, with its tree record prepared once
     root_box = tree.node_bounds[:12]
     status_word = ws.buffer[:4].view(torch.int32)
 
@@ -716,11 +720,11 @@ def run_case(args):
         from bajo_b200 import rt, scenes
         sc = scenes.spheres_in_box()
         gsc = rt.GpuRtTriangleScene(sc)
-        settings = rt.RenderSettings(1280, 720, 64, rng_seed=2026, max_depth=8)
+        settings = rt.RenderSettings(1280, 720, args.spp, rng_seed=2026, max_depth=8)
         ws = rt.RenderWorkspace(settings, rt.MIS)
         ms = timed(lambda: rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws))
         rays, shadows = ws.ray_counts()
-        paths = 1280 * 720 * 64
+        paths = 1280 * 720 * args.spp
         out.update({"ms": round(ms, 3), "samples_s": round(paths / ms * 1e3, 1),
                     "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
                     "triangles": sc.n_tris, "status": ws.status()})
@@ -776,12 +780,32 @@ def run_case(args):
         tree = bvh.build_triangle_bvh(verts, workspace=ws)
         if args.case == "build":
             ms = timed(lambda: bvh.build_triangle_bvh(verts, workspace=ws, out=tree))
-            out.update({"ms": round(ms, 5), "mtri_s": round(n / ms / 1e3, 2)})
+            staged = bvh.build_triangle_bvh(verts, stage_top=True)
+            ms_stage = timed(lambda: staged.restage_top())
+            out.update({"ms": round(ms, 5), "mtri_s": round(n / ms / 1e3, 2), "stage_top_ms": round(ms_stage, 5)})
         else:
             cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
             hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
             ms = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
-            out.update({"ms": round(ms, 5), "mrays_s": round(WIDTH * HEIGHT / ms / 1e3, 2)})
+            staged = bvh.build_triangle_bvh(verts, stage_top=True)  # same tree plus the staged top levels
+            ms_staged = timed(lambda: staged.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
+            # incoherent rays: origins uniform in the unit cube, directions uniform on the sphere
+            nr = WIDTH * HEIGHT
+            g = torch.Generator(device="cuda").manual_seed(1)
+            rays = torch.empty(8, nr, dtype=torch.float32, device="cuda")
+            rays[0:3].uniform_(0.0, 1.0, generator=g)
+            rays[3].zero_()
+            d = torch.randn(3, nr, device="cuda", generator=g)
+            rays[4:7] = d / d.norm(dim=0, keepdim=True)
+            rays[7].fill_(3.0e38)
+            rays = rays.reshape(-1)
+            ms_inc = timed(lambda: tree.launch_rays(rays, hits, nr))
+            ms_inc_staged = timed(lambda: staged.launch_rays(rays, hits, nr))
+            out.update({"ms": round(ms, 5), "mrays_s": round(WIDTH * HEIGHT / ms / 1e3, 2),
+                        "staged_ms": round(ms_staged, 5),
+                        "staged_mrays_s": round(WIDTH * HEIGHT / ms_staged / 1e3, 2),
+                        "incoherent_mrays_s": round(nr / ms_inc / 1e3, 2),
+                        "incoherent_staged_mrays_s": round(nr / ms_inc_staged / 1e3, 2)})
         out["status"] = ws.status()
     print(json.dumps(out), flush=True)
 

@@ -42,6 +42,7 @@ extern "C" {
 #define BAJO_STATUS_STACK_OVERFLOW 0x2u   /* traversal stack would overflow    */
 #define BAJO_STATUS_BAD_TOPOLOGY 0x4u     /* refit met an inconsistent parent  */
 #define BAJO_STATUS_WIDE_TIMEOUT 0x40u    /* wide collapse gave up on a task   */
+#define BAJO_STATUS_STAGE_TIMEOUT 0x80u   /* staged top levels did not arrive  */
 
 /* triangle tests */
 #define BAJO_TRI_MT 0         /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
@@ -130,7 +131,21 @@ typedef struct BajoLbvh {
   uint32_t* leaf_parent;       /* N     parent internal node of each sorted leaf          */
   uint32_t* roots;             /* S     tagged root ref per segment (SENTINEL if empty)   */
   float* leaf_tris;            /* 12*N  sorted triangle records [v0,prim | v1,0 | v2,0]   */
+  float* top_nodes;            /* optional (NULL = none): BAJO_TOP_BYTES, the top levels  */
+                               /* of segment 0's tree for the traversal (see below)       */
 } BajoLbvh;
+
+/* Staged top levels.  When bvh->top_nodes is set (16-byte aligned), the build
+ * also writes the first BAJO_TOP_NODES internal nodes of segment 0's tree in
+ * breadth-first order (left before right): a 16-byte header [staged count,
+ * root ref, 0, 0] then one 64-byte record per slot [left-child AABB |
+ * right-child AABB | left ref, right ref, 0, 0], where a child that is itself
+ * staged is referenced as BAJO_TOP_FLAG | slot.  The closest-hit kernels copy
+ * the records into shared memory once per block with one bulk asynchronous
+ * copy and read the top of the tree from there; the hits do not change. */
+#define BAJO_TOP_NODES 256u
+#define BAJO_TOP_FLAG 0x40000000u
+#define BAJO_TOP_BYTES (16u + 64u * BAJO_TOP_NODES)
 
 /* Byte size of every BajoLbvh array for N triangles in S segments (in field
  * order: internal_offsets, leaf_bounds, seg_bounds, sort_keys, leaf_ids,
@@ -140,6 +155,7 @@ typedef struct BajoLbvhSizes {
   size_t internal_offsets, leaf_bounds, seg_bounds, sort_keys, leaf_ids, morton_codes, node_meta, node_bounds,
       node_leaf_counts, node_flags, leaf_parent, roots, leaf_tris;
   size_t workspace;
+  size_t top_nodes; /* BAJO_TOP_BYTES */
 } BajoLbvhSizes;
 int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* sizes);
 
@@ -162,6 +178,11 @@ int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, 
 int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                               void* stream, void* const* events, int32_t n_events);
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);
+
+/* Rewrites bvh->top_nodes from the tree's current nodes (the build does this
+ * itself when top_nodes is set).  Trees of 2^30 or more triangles are not
+ * staged (the header's count stays 0). */
+int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream);
 
 /* ======================================================================== */
 /* Closest-hit traversal                                                     */

@@ -487,3 +487,43 @@ def wide_build(bvh: OracleLbvh, width: int, max_leaf: int = 4) -> OracleWide:
                         _ptr(no), _ptr(lo))
     nn, nb = int(no[-1]), int(lo[-1])
     return OracleWide(width, nodes[:nn * 7 * width], li[:nb * width], lt[:nb * 12 * width], ls[:nb * width], no, lo)
+
+
+# ---- staged top levels --------------------------------------------------------
+TOP_NODES = 256
+TOP_FLAG = 0x40000000
+
+
+def stage_top(bvh: OracleLbvh, k: int = TOP_NODES) -> np.ndarray:
+    """The staged top levels of segment 0's tree as u32 words: header
+    [count, root ref, 0, 0] then k records of 16 words [left AABB (6) |
+    right AABB (6) | left ref, right ref, 0, 0].  Slots follow breadth-first
+    order, left child before right; a staged child is referenced as
+    TOP_FLAG | slot, every other child keeps its tagged global ref.  This
+    layout is the library's own (the reference reads the whole tree from
+    global memory), restated here to check it word for word."""
+    out = np.zeros(4 + 16 * k, np.uint32)
+    root = int(bvh.roots[0])
+    out[1] = root
+    if root == SENTINEL or root & LEAF_FLAG:
+        return out
+    meta = bvh.node_meta.reshape(-1, 4)
+    nb = bvh.node_bounds.view(np.uint32).reshape(-1, 12)
+    refs = [root]
+    slot_of = {root: 0}
+    i = 0
+    while i < len(refs):  # breadth first: refs grows level by level
+        m = meta[refs[i]]
+        for c in (int(m[1]), int(m[2])):
+            if not (c & LEAF_FLAG) and len(refs) < k:
+                slot_of[c] = len(refs)
+                refs.append(c)
+        i += 1
+    for s, r in enumerate(refs):
+        rec = out[4 + 16 * s: 4 + 16 * (s + 1)]
+        rec[0:12] = nb[r]
+        m = meta[r]
+        for j, c in enumerate((int(m[1]), int(m[2]))):
+            rec[12 + j] = TOP_FLAG | slot_of[c] if c in slot_of else c
+    out[0] = len(refs)
+    return out
