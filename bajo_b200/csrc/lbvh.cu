@@ -11,6 +11,9 @@ int sm_count();
 namespace {
 
 constexpr int kBlock = 256;
+// refit CTA: leaves per CTA (also the unit that decides which nodes meet in
+// global memory, see section 4)
+constexpr int kRefitBlock = 512;
 
 // Per segment, 12 ordered words: [min bounds xyz, max bounds xyz,
 // min centroid xyz, max centroid xyz].  Minima are stored complemented so
@@ -203,6 +206,7 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
                                                           uint32_t* __restrict__ leaf_parent,
                                                           uint32_t* __restrict__ node_leaf_counts,
                                                           uint32_t* __restrict__ node_flags,
+                                                          float* __restrict__ node_bounds,
                                                           uint32_t* __restrict__ roots) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i < n_seg) {
@@ -248,6 +252,18 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 
   node_leaf_counts[i] = (uint32_t)(last - first + 1);
   node_flags[i] = 0;
+  // nodes whose children meet in global memory during the refit start from
+  // the invalid box (AABB.invalid, bajo/core/aabb.mojo:28), which lets the
+  // refit read a sibling's slot before its arrival atomic returns
+  if ((lb + (uint32_t)first) / kRefitBlock != (lb + (uint32_t)last) / kRefitBlock) {
+    float4* nb4 = reinterpret_cast<float4*>(node_bounds + (size_t)i * 12);
+    const float4 lo = make_float4(FLT_MAX, FLT_MAX, FLT_MAX, -FLT_MAX);
+    const float4 mid = make_float4(-FLT_MAX, -FLT_MAX, FLT_MAX, FLT_MAX);
+    const float4 hi = make_float4(FLT_MAX, -FLT_MAX, -FLT_MAX, -FLT_MAX);
+    nb4[0] = lo;
+    nb4[1] = mid;
+    nb4[2] = hi;
+  }
   if (first == 0 && last == len - 1) node_meta[(size_t)i * 4 + 0] = kSentinel;
   uint32_t left = ib + (uint32_t)split, right = ib + (uint32_t)split + 1;
   if (split == first) {
@@ -273,17 +289,21 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 //     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
 //    One thread per sorted leaf climbs towards the root; the first arrival at
 //    a node stops, the second merges both child boxes and continues.
-//    A CTA owns 1024 consecutive sorted leaves.  Nodes whose leaf range lies
-//    inside the CTA's leaves (almost all of them: a Karras node's range is
-//    contiguous) meet in shared memory: arrival counter and the first
-//    arrival's box in shared slots, no L2 round trip.  Only the nodes whose
-//    range crosses a CTA boundary meet in global memory, with the arrival
-//    counted first (acquire) and the first arrival then publishing its box
-//    with a release flag bit (kBoxReady), so the arrival that continues waits
-//    for one atomic and one box load per level rather than also for its own
-//    box stores.  node_flags ends at 2 for every internal node either way.
+//    A CTA owns kRefitBlock consecutive sorted leaves.  Nodes whose leaf
+//    range lies inside the CTA's leaves (almost all of them: a Karras node's
+//    range is contiguous) meet in shared memory: arrival counter and the
+//    first arrival's box in shared slots, no L2 round trip.  Only the nodes
+//    whose range crosses a CTA boundary meet in global memory, with the
+//    arrival counted first (acquire) and the first arrival then publishing
+//    its box with a release flag bit (kBoxReady), so the arrival that
+//    continues does not wait for its own box stores.  The continuing arrival
+//    reads the sibling's slot while its atomic is in flight (the slot starts
+//    invalid, so a complete box is a final one): one L2 round trip per level
+//    instead of two in the common case.  node_flags ends at 2 for every
+//    internal node either way.  512 leaves per CTA (128 CTAs at 65,536
+//    triangles) measured faster than 1,024 (64 CTAs): the local climbs are
+//    spread over twice the SMs for one more global level.
 // ---------------------------------------------------------------------------
-constexpr int kRefitBlock = 1024;
 constexpr uint32_t kBoxReady = 0x100u;
 constexpr uint64_t kRefitWaitNs = 200000000ull;
 
@@ -361,13 +381,21 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
       return;
     }
-    float2* slot = reinterpret_cast<float2*>(node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6));
-    slot[0] = make_float2(mn.x, mn.y);
-    slot[1] = make_float2(mn.z, mx.x);
-    slot[2] = make_float2(mx.y, mx.z);
     const uint32_t last = m.w, first = last + 1 - cnt;
+    const bool local = first >= c0 && last < c0 + kRefitBlock;
+    float* slot = node_bounds + (size_t)parent * 12 + (is_left ? 0 : 6);
+    if (local) {
+      float2* s2 = reinterpret_cast<float2*>(slot);
+      s2[0] = make_float2(mn.x, mn.y);
+      s2[1] = make_float2(mn.z, mx.x);
+      s2[2] = make_float2(mx.y, mx.z);
+    } else {  // read early by the sibling's arrival (below): strong stores
+      st_relaxed_gpu_f2(slot + 0, mn.x, mn.y);
+      st_relaxed_gpu_f2(slot + 2, mn.z, mx.x);
+      st_relaxed_gpu_f2(slot + 4, mx.y, mx.z);
+    }
     f3 smn, smx;
-    if (first >= c0 && last < c0 + kRefitBlock) {
+    if (local) {
       // both children live in this CTA; one end of a Karras node's range is
       // its own local index, so lb + (parent - ib) - c0 is a unique slot
       const uint32_t k = lb + (parent - ib) - c0;
@@ -381,24 +409,42 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
       smx = mk(sib[3], sib[4], sib[5]);
       node_flags[parent] = 2u;
     } else {
+      // The sibling's slot is read before the arrival atomic returns, so the
+      // continuing arrival usually pays one L2 round trip per level.  The
+      // slot is written once per build and starts invalid (topology_kernel),
+      // so six values that all differ from the invalid box are final; any
+      // invalid value is read again after the handshake.
+      const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
+      const float2 q0 = ld_relaxed_gpu_f2(sib), q1 = ld_relaxed_gpu_f2(sib + 2), q2 = ld_relaxed_gpu_f2(sib + 4);
       const uint32_t old = atomic_add_acquire_gpu(&node_flags[parent], 1u);
       if ((old & 0xFFu) == 0) {  // first: publish the box stored above
         red_add_release_gpu(&node_flags[parent], kBoxReady);
         return;
       }
-      if (!(old & kBoxReady)) {
-        const uint64_t t0 = global_timer_ns();
-        while (!(ld_acquire_gpu(&node_flags[parent]) & kBoxReady)) {
-          if (global_timer_ns() - t0 > kRefitWaitNs) {
-            raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-            return;
+      smn = mk(q0.x, q0.y, q1.x);
+      smx = mk(q1.y, q2.x, q2.y);
+      const bool ready = smn.x != FLT_MAX && smn.y != FLT_MAX && smn.z != FLT_MAX && smx.x != -FLT_MAX &&
+                         smx.y != -FLT_MAX && smx.z != -FLT_MAX;
+      if (ready && !(old & kBoxReady)) {
+        // the first arrival's kBoxReady add may still be in flight: cancel
+        // it arithmetically so the counter ends at 2 in either order
+        atomicSub(&node_flags[parent], kBoxReady);
+      } else {
+        if (!ready) {
+          if (!(old & kBoxReady)) {
+            const uint64_t t0 = global_timer_ns();
+            while (!(ld_acquire_gpu(&node_flags[parent]) & kBoxReady)) {
+              if (global_timer_ns() - t0 > kRefitWaitNs) {
+                raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+                return;
+              }
+            }
           }
+          smn = mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2));
+          smx = mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5));
         }
+        node_flags[parent] = 2u;
       }
-      const float* sib = node_bounds + (size_t)parent * 12 + (is_left ? 6 : 0);
-      smn = mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2));
-      smx = mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5));
-      node_flags[parent] = 2u;
     }
     mn = vmin(mn, smn);
     mx = vmax(mx, smx);
@@ -628,7 +674,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   }
   topology_kernel<<<(max(n, S) + kBlock - 1) / kBlock, kBlock, 0, st>>>(
       bvh->morton_codes, bvh->seg_offsets, S, bvh->internal_offsets, n, bvh->node_meta, bvh->leaf_parent,
-      bvh->node_leaf_counts, bvh->node_flags, bvh->roots);
+      bvh->node_leaf_counts, bvh->node_flags, bvh->node_bounds, bvh->roots);
   if (cudaGetLastError() != cudaSuccess || !mark(3 + passes)) return BAJO_ERR_CUDA;
   if (n > 0) {
     constexpr size_t refit_smem = kRefitBlock * (16 + 4 + 4 + 2 * 6 * 4);

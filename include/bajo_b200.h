@@ -180,8 +180,9 @@ int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_works
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);
 
 /* Rewrites bvh->top_nodes from the tree's current nodes (the build does this
- * itself when top_nodes is set).  Trees of 2^30 or more triangles are not
- * staged (the header's count stays 0). */
+ * itself when top_nodes is set).  Needed after a build through a record whose
+ * top_nodes was NULL: the staged copy is not checked against the tree beyond
+ * its root ref. */
 int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream);
 
 /* ======================================================================== */
