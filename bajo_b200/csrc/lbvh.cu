@@ -11,9 +11,16 @@ int sm_count();
 namespace {
 
 constexpr int kBlock = 256;
-// refit CTA: leaves per CTA (also the unit that decides which nodes meet in
-// global memory, see section 4)
+// hierarchy CTA: sorted leaves per CTA (also the unit that decides which
+// splits meet in global memory, section 3).  512 measured faster than 1,024:
+// the local climbs spread over twice the SMs for one more global level.
 constexpr int kRefitBlock = 512;
+// Builds of up to this many triangles emit the hierarchy bottom-up in the
+// refit pass (section 3); larger ones run the top-down topology kernel and
+// the refit separately (section 4), which keeps more warps resident per SM.
+// Measured crossover on B200: 2^17 triangles (101 vs 108 us; 2^18: 144 vs
+// 141 us).
+constexpr uint32_t kMergedMaxLeaves = 1u << 17;
 
 // Per segment, 12 ordered words: [min bounds xyz, max bounds xyz,
 // min centroid xyz, max centroid xyz].  Minima are stored complemented so
@@ -133,7 +140,8 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
                                                         float* __restrict__ seg_bounds_out,
                                                         uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
                                                         uint32_t passes, uint32_t end_bit,
-                                                        uint32_t* __restrict__ ghist) {
+                                                        uint32_t* __restrict__ ghist,
+                                                        uint32_t* __restrict__ node_flags) {
   extern __shared__ uint32_t s_hist[];  // passes * copies * 256
   const uint32_t copies = passes <= 4 ? 8 : 4;
   const uint32_t words = passes * copies * 256;
@@ -170,6 +178,7 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
     uint64_t key = ((uint64_t)seg << 32) | code;
     keys[i] = key;
     vals[i] = i;
+    node_flags[i] = 0;  // arrival counters of the hierarchy kernel
     for (uint32_t p = 0; p < passes; ++p) {
       uint32_t sh = 8 * p;
       uint32_t bits = min(8u, end_bit - sh);
@@ -186,7 +195,288 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
 }
 
 // ---------------------------------------------------------------------------
-// 3. Karras topology (init_segmented_lbvh_roots_kernel, lbvh.mojo:235;
+// 3. Karras hierarchy, refit and sorted triangle records in one bottom-up pass
+//    (builds of up to kMergedMaxLeaves triangles)
+//    (init_segmented_lbvh_roots_kernel, lbvh.mojo:235;
+//     build_lbvh_topology_kernel, lbvh.mojo:257-329;
+//     refit_lbvh_bounds_from_leaves_kernel, lbvh.mojo:116-161;
+//     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
+//
+//    The reference finds every internal node's range and split top-down
+//    (one thread per node, two binary searches over the codes), then refits
+//    the boxes bottom-up.  Here one thread per sorted leaf climbs and builds
+//    the same binary radix tree bottom-up (Apetrei, "Fast and simple
+//    agglomerative LBVH construction", 2014): a node [f, l] is the left child
+//    of its parent iff delta(l, l+1) > delta(f-1, f), so its parent splits at
+//    l (left child) or f-1 (right child).  The two children of a split meet
+//    there; the second to arrive knows the parent's whole range, writes the
+//    parent in Karras numbering and continues upwards.  Karras numbering: a
+//    non-root internal node is indexed by its last position when it is a left
+//    child and by its first when it is a right child; the root is 0.  The
+//    arrays are bit-identical to the top-down construction (same ranges,
+//    splits, numbering, boxes).
+//
+//    A CTA owns kRefitBlock consecutive sorted leaves.  Splits whose
+//    sibling starts inside the CTA meet in shared memory (arrival counter,
+//    child boxes, far range ends and their deltas in shared slots).  A split
+//    whose sibling lies (partly) outside meets in global memory after the
+//    CTA's local climbs are done: node_flags of the split counts the
+//    arrivals (acquire), the first arrival publishes its subtree (already
+//    written to the node arrays) with a release flag bit, and passes its far
+//    end's delta in the counter word; the second reads the sibling's box
+//    from its node record or triangle record.  node_flags ends at 2 for
+//    every internal node.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kArrive = 1u;
+constexpr uint32_t kLeafArrive = 0x10u;   // the arrival is a leaf
+constexpr uint32_t kBoxReady = 0x100u;    // first arrival published
+constexpr uint64_t kRefitWaitNs = 200000000ull;
+
+// lbvh.mojo:221-232 + core/morton.mojo:22: clz64 of the (code, local index)
+// keys of two positions of one segment.
+__device__ __forceinline__ int delta_codes(uint32_t ci, uint32_t li, uint32_t cj, uint32_t lj) {
+  const uint64_t x = (((uint64_t)ci << 32) | li) ^ (((uint64_t)cj << 32) | lj);
+  return x ? __clzll((long long)x) : 64;
+}
+
+struct SegInfo {
+  uint32_t lb, len, ib;
+};
+
+// Writes internal node k = the parent [F, L] (global positions) split at
+// gamma, and its children's parent links.
+__device__ __forceinline__ void write_parent(const SegInfo& g, uint32_t k, uint32_t F, uint32_t L, uint32_t gamma,
+                                             f3 lmn, f3 lmx, f3 rmn, f3 rmx, uint32_t* __restrict__ node_meta,
+                                             uint32_t* __restrict__ node_leaf_counts,
+                                             uint32_t* __restrict__ leaf_parent, float* __restrict__ node_bounds) {
+  const uint32_t lg = gamma - g.lb;
+  const bool left_leaf = gamma == F, right_leaf = gamma + 1 == L;
+  const uint32_t left = left_leaf ? (kLeafFlag | gamma) : g.ib + lg;
+  const uint32_t right = right_leaf ? (kLeafFlag | (gamma + 1)) : g.ib + lg + 1;
+  uint32_t* m = node_meta + (size_t)k * 4;
+  if (F == g.lb && L == g.lb + g.len - 1) m[0] = kSentinel;  // the root
+  m[1] = left;
+  m[2] = right;
+  m[3] = L;  // fence = leaf_begin + last
+  node_leaf_counts[k] = L - F + 1;
+  float2* b = reinterpret_cast<float2*>(node_bounds + (size_t)k * 12);
+  b[0] = make_float2(lmn.x, lmn.y);
+  b[1] = make_float2(lmn.z, lmx.x);
+  b[2] = make_float2(lmx.y, lmx.z);
+  b[3] = make_float2(rmn.x, rmn.y);
+  b[4] = make_float2(rmn.z, rmx.x);
+  b[5] = make_float2(rmx.y, rmx.z);
+  if (left_leaf) leaf_parent[gamma] = k;
+  else node_meta[(size_t)(g.ib + lg) * 4] = k;
+  if (right_leaf) leaf_parent[gamma + 1] = k;
+  else node_meta[(size_t)(g.ib + lg + 1) * 4] = k;
+}
+
+__device__ __forceinline__ void tri_box(const float4* __restrict__ rec, f3& mn, f3& mx) {
+  const float4 a = __ldcg(rec + 0), b = __ldcg(rec + 1), c = __ldcg(rec + 2);
+  const f3 va = mk(a.x, a.y, a.z), vb = mk(b.x, b.y, b.z), vc = mk(c.x, c.y, c.z);
+  mn = vmin(vmin(va, vb), vc);
+  mx = vmax(vmax(va, vb), vc);
+}
+
+__global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
+    const float* __restrict__ verts, const uint32_t* __restrict__ leaf_ids, const uint32_t* __restrict__ codes,
+    uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
+    uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
+    float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
+    uint32_t* __restrict__ roots, uint32_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char hier_smem[];
+  float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(hier_smem);                      // [B][side]
+  uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(hier_smem + kRefitBlock * 48);   // far end
+  int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(hier_smem + kRefitBlock * 56);            // its delta
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(hier_smem + kRefitBlock * 64);            // arrivals
+  uint32_t* s_code = reinterpret_cast<uint32_t*>(hier_smem + kRefitBlock * 68);           // [B + 2]
+  const uint32_t tid = threadIdx.x;
+  const uint32_t c0 = blockIdx.x * kRefitBlock;  // first sorted leaf of this CTA
+  const uint32_t s = c0 + tid;
+
+  // roots (init_segmented_lbvh_roots_kernel)
+  for (uint32_t i = blockIdx.x * kRefitBlock + tid; i < n_seg; i += gridDim.x * kRefitBlock) {
+    const uint32_t lb = seg_offsets[i], le = seg_offsets[i + 1];
+    if (le == lb) roots[i] = kSentinel;
+    else if (le - lb == 1) {
+      roots[i] = kLeafFlag | lb;
+      leaf_parent[lb] = kSentinel;
+    } else roots[i] = internal_offsets[i];
+  }
+
+  s_cnt[tid] = 0;
+  s_code[tid + 1] = s < n ? codes[s] : 0u;
+  if (tid == 0) s_code[0] = (c0 > 0 && c0 - 1 < n) ? codes[c0 - 1] : 0u;
+  if (tid == kRefitBlock - 1) s_code[kRefitBlock + 1] = (s + 1 < n) ? codes[s + 1] : 0u;
+
+  SegInfo g{0, 0, 0};
+  bool active = s < n;
+  f3 mn, mx;
+  if (active) {
+    const uint32_t seg = n_seg > 1 ? segment_for_item(seg_offsets, n_seg + 1, s) : 0;
+    g.lb = seg_offsets[seg];
+    g.len = seg_offsets[seg + 1] - g.lb;
+    g.ib = internal_offsets[seg];
+    const uint32_t item = leaf_ids[s];
+    if (item >= n) {  // only after a failed sort
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      active = false;
+    } else {
+      const float* v = verts + (size_t)item * 9;
+      const f3 a = mk(__ldg(v + 0), __ldg(v + 1), __ldg(v + 2));
+      const f3 b = mk(__ldg(v + 3), __ldg(v + 4), __ldg(v + 5));
+      const f3 c = mk(__ldg(v + 6), __ldg(v + 7), __ldg(v + 8));
+      float4* rec = reinterpret_cast<float4*>(leaf_tris + (size_t)s * 12);
+      rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(item - g.lb));
+      rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
+      rec[2] = make_float4(c.x, c.y, c.z, 0.0f);
+      mn = vmin(vmin(a, b), c);
+      mx = vmax(vmax(a, b), c);
+      if (g.len < 2) active = false;  // a one-leaf segment: the leaf is the root
+    }
+  }
+  __syncthreads();  // codes staged
+
+  // the climbing subtree [f, l] and the deltas at its two ends
+  uint32_t f = s, l = s;
+  bool leaf = true;
+  int dl = -1, dr = -1;
+  if (active) {
+    const uint32_t li = s - g.lb;
+    if (li > 0) dl = delta_codes(s_code[tid], li - 1, s_code[tid + 1], li);
+    if (li + 1 < g.len) dr = delta_codes(s_code[tid + 1], li, s_code[tid + 2], li + 1);
+  }
+  // phase 1: splits whose sibling starts inside this CTA, in shared memory
+  bool global = false;
+  int pending = -1;  // shared slot where this subtree arrived first
+  for (int depth = 0; active; ++depth) {
+    if (depth > 128) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      active = false;
+      break;
+    }
+    const bool is_left = dr > dl;
+    const uint32_t gamma = is_left ? l : f - 1;
+    if (is_left ? (l + 1 >= c0 + kRefitBlock) : (f < c0 + 1)) {
+      global = true;
+      break;
+    }
+    const uint32_t slot = gamma - c0, side = is_left ? 0 : 1;
+    float* mine = s_box[slot][side];
+    mine[0] = mn.x; mine[1] = mn.y; mine[2] = mn.z; mine[3] = mx.x; mine[4] = mx.y; mine[5] = mx.z;
+    s_far[slot][side] = is_left ? f : l;
+    s_dfar[slot][side] = is_left ? dl : dr;
+    __threadfence_block();
+    if (atomicAdd(&s_cnt[slot], 1u) == 0) {
+      pending = (int)slot;
+      break;
+    }
+    __threadfence_block();
+    const float* sib = s_box[slot][side ^ 1];
+    const f3 smn = mk(sib[0], sib[1], sib[2]), smx = mk(sib[3], sib[4], sib[5]);
+    const uint32_t sfar = s_far[slot][side ^ 1];
+    const int sd = s_dfar[slot][side ^ 1];
+    const uint32_t F = is_left ? f : sfar, L = is_left ? sfar : l;
+    const int dL = is_left ? dl : sd, dR = is_left ? sd : dr;
+    const bool root = F == g.lb && L == g.lb + g.len - 1;
+    const uint32_t k = g.ib + (root ? 0u : (dR > dL ? L - g.lb : F - g.lb));
+    if (is_left) write_parent(g, k, F, L, gamma, mn, mx, smn, smx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
+    else write_parent(g, k, F, L, gamma, smn, smx, mn, mx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
+    node_flags[g.ib + (gamma - g.lb)] = 2u;
+    mn = vmin(mn, smn);
+    mx = vmax(mx, smx);
+    f = F;
+    l = L;
+    dl = dL;
+    dr = dR;
+    leaf = false;
+    if (root) active = false;
+  }
+  __syncthreads();  // every local climb of this CTA has ended
+  if (pending >= 0 && s_cnt[pending] == 1) global = true;  // the sibling comes from outside
+  if (!global) return;
+
+  // phase 2: the splits that cross a CTA boundary, in global memory
+  for (int depth = 0;; ++depth) {
+    if (depth > 128) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      return;
+    }
+    const bool is_left = dr > dl;
+    const uint32_t gamma = is_left ? l : f - 1;
+    const uint32_t lg = gamma - g.lb;
+    uint32_t* flag = node_flags + g.ib + lg;
+    const int dfar = is_left ? dl : dr;
+    const uint32_t inc = kArrive | (leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
+    const uint32_t old = atomic_add_acquire_gpu(flag, inc);
+    if ((old & 0xFu) == 0) {  // first: publish the subtree written above
+      red_add_release_gpu(flag, kBoxReady);
+      return;
+    }
+    if (!(old & kBoxReady)) {
+      const uint64_t t0 = global_timer_ns();
+      while (!(ld_acquire_gpu(flag) & kBoxReady)) {
+        if (global_timer_ns() - t0 > kRefitWaitNs) {
+          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+          return;
+        }
+      }
+    }
+    const bool sib_leaf = (old & kLeafArrive) != 0;
+    const int sd = (int)((old >> 16) & 0x7Fu) - 1;
+    f3 smn, smx;
+    uint32_t sfar;
+    if (is_left) {  // sibling = right child, starts at gamma + 1
+      if (sib_leaf) {
+        sfar = gamma + 1;
+        tri_box(reinterpret_cast<const float4*>(leaf_tris) + (size_t)(gamma + 1) * 3, smn, smx);
+      } else {
+        const uint32_t ks = g.ib + lg + 1;
+        sfar = __ldcg(node_meta + (size_t)ks * 4 + 3);
+        const float4* nb = reinterpret_cast<const float4*>(node_bounds) + (size_t)ks * 3;
+        const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
+        smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
+        smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
+      }
+    } else {  // sibling = left child, ends at gamma
+      if (sib_leaf) {
+        sfar = gamma;
+        tri_box(reinterpret_cast<const float4*>(leaf_tris) + (size_t)gamma * 3, smn, smx);
+      } else {
+        const uint32_t ks = g.ib + lg;
+        sfar = gamma + 1 - __ldcg(node_leaf_counts + ks);
+        const float4* nb = reinterpret_cast<const float4*>(node_bounds) + (size_t)ks * 3;
+        const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
+        smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
+        smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
+      }
+    }
+    *flag = 2u;
+    const uint32_t F = is_left ? f : sfar, L = is_left ? sfar : l;
+    if (F > L || L >= g.lb + g.len || F < g.lb) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      return;
+    }
+    const int dL = is_left ? dl : sd, dR = is_left ? sd : dr;
+    const bool root = F == g.lb && L == g.lb + g.len - 1;
+    const uint32_t k = g.ib + (root ? 0u : (dR > dL ? L - g.lb : F - g.lb));
+    if (is_left) write_parent(g, k, F, L, gamma, mn, mx, smn, smx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
+    else write_parent(g, k, F, L, gamma, smn, smx, mn, mx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
+    if (root) return;
+    mn = vmin(mn, smn);
+    mx = vmax(mx, smx);
+    f = F;
+    l = L;
+    dl = dL;
+    dr = dR;
+    leaf = false;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// 4. Large builds: Karras topology top-down, then the refit
+//    (init_segmented_lbvh_roots_kernel, lbvh.mojo:235;
 //    build_lbvh_topology_kernel, lbvh.mojo:257-329).
 // ---------------------------------------------------------------------------
 // lbvh.mojo:221-232 + core/morton.mojo:22: clz64 of the (code, local index)
@@ -284,7 +574,7 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 }
 
 // ---------------------------------------------------------------------------
-// 4. refit + sorted triangle records
+// 4b. refit + sorted triangle records
 //    (refit_lbvh_bounds_from_leaves_kernel, lbvh.mojo:116-161;
 //     pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:81).
 //    One thread per sorted leaf climbs towards the root; the first arrival at
@@ -300,12 +590,9 @@ __global__ void __launch_bounds__(kBlock) topology_kernel(const uint32_t* __rest
 //    reads the sibling's slot while its atomic is in flight (the slot starts
 //    invalid, so a complete box is a final one): one L2 round trip per level
 //    instead of two in the common case.  node_flags ends at 2 for every
-//    internal node either way.  512 leaves per CTA (128 CTAs at 65,536
-//    triangles) measured faster than 1,024 (64 CTAs): the local climbs are
-//    spread over twice the SMs for one more global level.
+//    internal node either way.  512 leaves per CTA measured faster than
+//    1,024 (16M-triangle build 15% faster): more CTAs resident per SM.
 // ---------------------------------------------------------------------------
-constexpr uint32_t kBoxReady = 0x100u;
-constexpr uint64_t kRefitWaitNs = 200000000ull;
 
 __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restrict__ verts,
                                                             const uint32_t* __restrict__ leaf_ids, uint32_t n,
@@ -655,7 +942,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
         return BAJO_ERR_CUDA;
     }
     morton_kernel<<<grid, kBlock, smem, st>>>(bvh->leaf_bounds, n, bvh->seg_offsets, S, seg_ord, bvh->seg_bounds, k0,
-                                              v0, passes, (uint32_t)plan.end_bit, ghist);
+                                              v0, passes, (uint32_t)plan.end_bit, ghist, bvh->node_flags);
     if (cudaGetLastError() != cudaSuccess || !mark(2)) return BAJO_ERR_CUDA;
   }
   if (n > 1) {
@@ -672,11 +959,25 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
     for (uint32_t p = 0; p < passes; ++p)
       if (!mark(3 + p)) return BAJO_ERR_CUDA;
   }
-  topology_kernel<<<(max(n, S) + kBlock - 1) / kBlock, kBlock, 0, st>>>(
-      bvh->morton_codes, bvh->seg_offsets, S, bvh->internal_offsets, n, bvh->node_meta, bvh->leaf_parent,
-      bvh->node_leaf_counts, bvh->node_flags, bvh->node_bounds, bvh->roots);
-  if (cudaGetLastError() != cudaSuccess || !mark(3 + passes)) return BAJO_ERR_CUDA;
-  if (n > 0) {
+  if (n <= kMergedMaxLeaves) {
+    // one bottom-up pass builds the hierarchy and refits it: the topology
+    // stage event is recorded right before it
+    if (!mark(3 + passes)) return BAJO_ERR_CUDA;
+    constexpr size_t hier_smem = (size_t)kRefitBlock * 72 + 8;
+    if (cudaFuncSetAttribute(hierarchy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hier_smem) !=
+        cudaSuccess)
+      return BAJO_ERR_CUDA;
+    const uint32_t grid = (max(max(n, S), 1u) + kRefitBlock - 1) / kRefitBlock;
+    hierarchy_kernel<<<grid, kRefitBlock, hier_smem, st>>>(
+        d_verts, bvh->leaf_ids, bvh->morton_codes, n, bvh->seg_offsets, S, bvh->internal_offsets, bvh->node_meta,
+        bvh->node_leaf_counts, bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris, bvh->roots,
+        status);
+    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
+  } else {
+    topology_kernel<<<(max(n, S) + kBlock - 1) / kBlock, kBlock, 0, st>>>(
+        bvh->morton_codes, bvh->seg_offsets, S, bvh->internal_offsets, n, bvh->node_meta, bvh->leaf_parent,
+        bvh->node_leaf_counts, bvh->node_flags, bvh->node_bounds, bvh->roots);
+    if (cudaGetLastError() != cudaSuccess || !mark(3 + passes)) return BAJO_ERR_CUDA;
     constexpr size_t refit_smem = kRefitBlock * (16 + 4 + 4 + 2 * 6 * 4);
     if (cudaFuncSetAttribute(refit_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)refit_smem) !=
         cudaSuccess)

@@ -69,6 +69,7 @@ def parse():
     p.add_argument("--ref-spp", type=int, default=4096, help="--case guided reference samples per pixel")
     p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
     p.add_argument("--spp", type=int, default=64, help="--case render samples per pixel")
+    p.add_argument("--scenes", type=int, default=4096, help="--case batched scene count")
     p.add_argument("--train-passes", type=int, default=8, help="--case guided passes followed by training")
     p.add_argument("--train-steps", type=int, default=8, help="--case guided Adam steps per training pass")
     return p.parse_args()
@@ -729,7 +730,7 @@ def run_case(args):
                     "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
                     "triangles": sc.n_tris, "status": ws.status()})
     elif args.case == "batched":
-        out.update(run_batched(args.steps, args.warmup))
+        out.update(run_batched(args.steps, args.warmup, args.scenes))
     elif args.case == "guided":
         out = run_guided(args)
     elif args.case == "guided_pass":

@@ -68,7 +68,7 @@ def test_fixture_scenes_match_oracle_and_golden(oracle, golden_dir, name):
         assert np.array_equal(h(b.node_meta, np.uint32)[: 4 * (n - 1)], g[name + "__node_meta"][: 4 * (n - 1)])
 
 
-@pytest.mark.parametrize("n", [2, 3, 255, 256, 257, 5632, 65536, 1 << 20])
+@pytest.mark.parametrize("n", [2, 3, 255, 256, 257, 5632, 65536, 1 << 17, (1 << 17) + 1, 1 << 20])
 def test_random_scenes_match_oracle(oracle, n):
     v = scenes.random_triangles(n, seed=n)
     assert_same_build(build_gpu(v), oracle.lbvh_build(v))
@@ -87,7 +87,9 @@ def test_plain_lbvh_workload_validators(oracle):
     assert r.ok and r.diff == 0.0
 
 
-@pytest.mark.parametrize("counts", [[5, 1, 0, 300, 2, 77], [1000] * 7, [0, 0, 3], [1], [70000, 3, 9000]])
+# totals below and above the bottom-up hierarchy size limit (2^17 triangles)
+@pytest.mark.parametrize("counts", [[5, 1, 0, 300, 2, 77], [1000] * 7, [0, 0, 3], [1], [70000, 3, 9000],
+                                    [70000, 1, 0, 70000, 513]])
 def test_segmented_build_matches_oracle(oracle, counts):
     parts = [scenes.random_triangles(c, seed=100 + i) for i, c in enumerate(counts)]
     so = np.concatenate([[0], np.cumsum(counts)]).astype(np.uint32)
