@@ -28,7 +28,7 @@ TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
 SORT_NOALLOC_MAX_KEYS = 1 << 20
-SORT_VARIANTS = 4
+SORT_VARIANTS = 5  # tile shapes / digit widths of the 64-bit keys; 32-bit keys have 4
 
 _ERRORS = {
     ERR_INVALID_ARGUMENT: "invalid argument",

@@ -1,7 +1,7 @@
-"""Project autotuner for the sort tile shapes.
+"""Project autotuner for the sort tile shapes and digit widths.
 
 The sort kernels are compiled in several tile shapes (threads x keys per
-thread).  For each (key width, values, size bucket) the tuner times every
+thread) and, for 64-bit keys, two digit widths (8 and 10 bits).  For each (key width, values, size bucket) the tuner times every
 shape the library allows on the current GPU with CUDA events and writes the
 fastest into the library's tuning table (``bajo_sort_tuning_set``).  Results
 are cached as JSON keyed by (kernel, size bucket, GPU name and SM count) so a
@@ -117,8 +117,12 @@ def load(path: str = CACHE) -> int:
 
 def tune_all(reps: int = 5, save_cache: bool = True) -> dict:
     """The shapes the LBVH build and the sort sweep use."""
+    # 64-bit keys: up to 2^18 with the 30 live bits of single-scene LBVH keys
+    # (where 10-bit digits compete), above with 44 bits (segmented builds)
+    u64 = tune_sort(8, True, range(10, 19), end_bit=30, reps=reps)
+    u64.update(tune_sort(8, True, range(19, 27), end_bit=44, reps=reps))
     res = {
-        _kernel_key(8, True): tune_sort(8, True, range(10, 27), end_bit=44, reps=reps),
+        _kernel_key(8, True): u64,
         _kernel_key(4, True): tune_sort(4, True, range(10, 27), reps=reps),
     }
     if save_cache:

@@ -128,6 +128,11 @@ __global__ void __launch_bounds__(kBlock) bounds_kernel(const float* __restrict_
   }
 }
 
+// shared histogram copies per pass of the Morton kernel
+__host__ __device__ constexpr uint32_t morton_hist_copies(uint32_t passes, uint32_t digit_bits) {
+  return digit_bits > 8 ? 2u : (passes <= 4 ? 8u : 4u);
+}
+
 // ---------------------------------------------------------------------------
 // 2. Morton keys + every live digit histogram of the sort
 //    (compute_bounds_morton_codes_kernel, lbvh.mojo:30-62, fused with
@@ -139,12 +144,12 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
                                                         const uint32_t* __restrict__ seg_ord,
                                                         float* __restrict__ seg_bounds_out,
                                                         uint64_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                                                        uint32_t passes, uint32_t end_bit,
+                                                        uint32_t passes, uint32_t end_bit, uint32_t digit_bits,
                                                         uint32_t* __restrict__ ghist,
                                                         uint32_t* __restrict__ node_flags) {
-  extern __shared__ uint32_t s_hist[];  // passes * copies * 256
-  const uint32_t copies = passes <= 4 ? 8 : 4;
-  const uint32_t words = passes * copies * 256;
+  extern __shared__ uint32_t s_hist[];  // passes * copies * radix
+  const uint32_t radix = 1u << digit_bits, copies = morton_hist_copies(passes, digit_bits);
+  const uint32_t words = passes * copies * radix;
   for (uint32_t i = threadIdx.x; i < words; i += kBlock) s_hist[i] = 0;
   if (blockIdx.x == 0) {
     for (uint32_t k = threadIdx.x; k < n_seg * 12; k += kBlock) {
@@ -180,16 +185,16 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
     vals[i] = i;
     node_flags[i] = 0;  // arrival counters of the hierarchy kernel
     for (uint32_t p = 0; p < passes; ++p) {
-      uint32_t sh = 8 * p;
-      uint32_t bits = min(8u, end_bit - sh);
+      uint32_t sh = digit_bits * p;
+      uint32_t bits = min(digit_bits, end_bit - sh);
       uint32_t dg = (uint32_t)(key >> sh) & ((1u << bits) - 1u);
-      atomicAdd(&s_hist[(p * copies + copy) * 256 + dg], 1u);
+      atomicAdd(&s_hist[(p * copies + copy) * radix + dg], 1u);
     }
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < passes * 256; i += kBlock) {
-    uint32_t p = i >> 8, dg = i & 255, s = 0;
-    for (uint32_t c = 0; c < copies; ++c) s += s_hist[(p * copies + c) * 256 + dg];
+  for (uint32_t i = threadIdx.x; i < passes * radix; i += kBlock) {
+    uint32_t p = i >> digit_bits, dg = i & (radix - 1u), s = 0;
+    for (uint32_t c = 0; c < copies; ++c) s += s_hist[(p * copies + c) * radix + dg];
     if (s) atomicAdd(&ghist[i], s);
   }
 }
@@ -842,9 +847,15 @@ cudaError_t launch_stage_top(const BajoLbvh* bvh, cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // Build workspace: the sort plan of the u64 keys, with the per-segment
 // ordered bounds as the extra zeroed region.
+// The keys' live bits: the 30 Morton bits, and above bit 32 the segment
+// index when there are several segments.  variant / passes / digit_bits:
+// the sort's tile shape and digit width from the tuning table; the
+// workspace fits every variant the size allows.
 struct BuildPlan {
   onesweep::Plan sort;
   int end_bit;
+  int variant;
+  uint32_t passes, digit_bits;
   size_t off_seg_ord, off_keys_alt, off_vals_alt, total;
 };
 
@@ -852,9 +863,11 @@ BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
   BuildPlan b{};
   int seg_bits = 0;
   while (seg_bits < 32 && ((n_seg - 1) >> seg_bits)) ++seg_bits;
-  b.end_bit = 32 + seg_bits;
-  const uint32_t passes = onesweep::num_passes(0, b.end_bit);
-  b.sort = onesweep::make_plan<uint64_t>(n, true, passes, (size_t)n_seg * 12 * 4);
+  b.end_bit = n_seg > 1 ? 32 + seg_bits : 30;
+  b.variant = onesweep::choose_variant<uint64_t, true>(n, sm_count());
+  b.digit_bits = onesweep::variant_bits<uint64_t>(b.variant);
+  b.passes = onesweep::passes_for(0, b.end_bit, b.digit_bits);
+  b.sort = onesweep::make_plan<uint64_t>(n, true, onesweep::num_passes(0, b.end_bit), (size_t)n_seg * 12 * 4);
   b.off_seg_ord = b.sort.off_extra;
   b.off_keys_alt = b.sort.off_keys_alt;
   b.off_vals_alt = b.sort.off_vals_alt;
@@ -902,7 +915,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   if (bvh->top_nodes && ((uintptr_t)bvh->top_nodes & 15)) return BAJO_ERR_INVALID_ARGUMENT;
   BuildPlan plan = make_build_plan(n, S);
   if (ws_bytes < plan.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
-  if (ev && n_ev < (int32_t)(5 + plan.sort.passes)) return BAJO_ERR_INVALID_ARGUMENT;
+  if (ev && n_ev < (int32_t)(5 + plan.passes)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream_;
   // stage events: [start, bounds, morton, pass 0..P-1, topology, refit]
   auto mark = [&](int i) { return !ev || cudaEventRecord(ev[i], st) == cudaSuccess; };
@@ -919,7 +932,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
 
   // sort buffers: the Morton kernel writes where an even/odd pass count lands
   // the result in bvh->sort_keys / bvh->leaf_ids
-  const uint32_t passes = plan.sort.passes;
+  const uint32_t passes = plan.passes;
   uint64_t* kalt = (uint64_t*)(ws + plan.off_keys_alt);
   uint32_t* valt = (uint32_t*)(ws + plan.off_vals_alt);
   // (with n <= 1 nothing is sorted and the keys stay where they are written)
@@ -930,8 +943,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   uint32_t* v1 = even ? valt : bvh->leaf_ids;
   uint32_t* ghist = (uint32_t*)(ws + plan.sort.off_ghist);
   {
-    const uint32_t copies = passes <= 4 ? 8 : 4;
-    const size_t smem = (size_t)passes * copies * 256 * 4;
+    const size_t smem = (size_t)passes * morton_hist_copies(passes, plan.digit_bits) * (4u << plan.digit_bits);
     uint32_t grid = blocks;
     const uint32_t cap = (uint32_t)sm_count() * 8;
     if (grid > cap) grid = cap;
@@ -942,14 +954,14 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
         return BAJO_ERR_CUDA;
     }
     morton_kernel<<<grid, kBlock, smem, st>>>(bvh->leaf_bounds, n, bvh->seg_offsets, S, seg_ord, bvh->seg_bounds, k0,
-                                              v0, passes, (uint32_t)plan.end_bit, ghist, bvh->node_flags);
+                                              v0, passes, (uint32_t)plan.end_bit, plan.digit_bits, ghist,
+                                              bvh->node_flags);
     if (cudaGetLastError() != cudaSuccess || !mark(2)) return BAJO_ERR_CUDA;
   }
   if (n > 1) {
     bool in_first = true;
-    const int variant = onesweep::choose_variant<uint64_t, true>(n, sm_count());
     if (onesweep::run_passes<uint64_t, true>(k0, v0, k1, v1, bvh->morton_codes, plan.sort, ws, 0, plan.end_bit, st,
-                                             &in_first, variant, ev ? ev + 3 : nullptr) != cudaSuccess)
+                                             &in_first, plan.variant, ev ? ev + 3 : nullptr) != cudaSuccess)
       return BAJO_ERR_CUDA;
   } else {
     // nothing to sort; keep the low word in step with the key
@@ -1011,7 +1023,7 @@ int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream) {
 
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {
   if (!n_events || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
-  *n_events = (int32_t)(5 + bajo::make_build_plan(n_tris, n_segments).sort.passes);
+  *n_events = (int32_t)(5 + bajo::make_build_plan(n_tris, n_segments).passes);
   return BAJO_OK;
 }
 

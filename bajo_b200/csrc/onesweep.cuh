@@ -1,5 +1,6 @@
-// onesweep.cuh -- stable LSD radix sort, one scatter kernel per 8-bit digit
-// with decoupled look-back (Merrill & Garland / Adinets & Merrill "Onesweep").
+// onesweep.cuh -- stable LSD radix sort, one scatter kernel per digit (8
+// bits, or 10 bits for small 64-bit-key sorts) with decoupled look-back
+// (Merrill & Garland / Adinets & Merrill "Onesweep").
 //
 // Restates the reference's onesweep (bajo/sort/gpu/onesweep.mojo:31-328) for
 // sm_100a, with these changes:
@@ -15,10 +16,13 @@
 //    (one fewer launch than scan_global, onesweep.mojo:102);
 //  - two look-back regions alternate between passes and every pass clears the
 //    other region's slots, so only the first region needs a memset;
-//  - several tile shapes are compiled and chosen at run time (tuning table);
+//  - several tile shapes and two digit widths are compiled and chosen at run
+//    time (tuning table);
 //  - any digit range [begin_bit, end_bit) can be sorted, so constant key bits
 //    cost no pass.
 #pragma once
+
+#include <type_traits>
 
 #include "bajo_common.cuh"
 
@@ -45,23 +49,32 @@ struct KeyTraits<uint64_t> {
 };
 
 // ---------------------------------------------------------------------------
-// Tile shapes.  Variant 0 is the large default; smaller tiles give small
-// sorts more CTAs.  max_log2n: the largest sort (log2 of n) a variant may
-// serve, which bounds the look-back memory a workspace must hold.
+// Tile shapes and digit widths.  Variant 0 is the large default; smaller
+// tiles give small sorts more CTAs.  max_log2n: the largest sort (log2 of n)
+// a variant may serve, which bounds the look-back memory a workspace must
+// hold.  bits: digit width.  Variant 4 of the 64-bit keys sorts 10-bit
+// digits, so the 30 live bits of single-scene LBVH keys take three passes
+// instead of four, but each pass does 1,024 digits of per-tile work.
+// Measured on B200 (30-bit keys + 32-bit values): 2^14 keys 54.8 vs 60.2 us
+// (best 8-bit variant), 2^16 68.3 vs 59.3, 2^18 87.8 vs 71.3; inside the
+// LBVH build 2^15 triangles 78.8 vs 80.9 us, 2^16 85-87 vs 85.0.
 // ---------------------------------------------------------------------------
-constexpr int kNumVariants = 4;
+constexpr int kNumVariants = 5;  // the largest variant count of any key type
 struct Shape {
-  int block, kpt, max_log2n;
+  int block, kpt, max_log2n, bits;
 };
 template <typename K>
 struct Shapes;
 template <>
 struct Shapes<uint32_t> {
-  static constexpr Shape v[kNumVariants] = {{512, 12, 30}, {256, 12, 30}, {256, 8, 24}, {256, 4, 20}};
+  static constexpr int count = 4;
+  static constexpr Shape v[count] = {{512, 12, 30, 8}, {256, 12, 30, 8}, {256, 8, 24, 8}, {256, 4, 20, 8}};
 };
 template <>
 struct Shapes<uint64_t> {
-  static constexpr Shape v[kNumVariants] = {{512, 8, 30}, {256, 8, 30}, {256, 5, 24}, {256, 3, 20}};
+  static constexpr int count = 5;
+  static constexpr Shape v[count] = {{512, 8, 30, 8}, {256, 8, 30, 8}, {256, 5, 24, 8}, {256, 3, 20, 8},
+                                     {256, 4, 18, 10}};
 };
 
 constexpr uint32_t ceil_log2(uint32_t n) {
@@ -71,19 +84,39 @@ constexpr uint32_t ceil_log2(uint32_t n) {
 }
 template <typename K>
 constexpr bool variant_allowed(int v, uint32_t n) {
-  return v >= 0 && v < kNumVariants && ceil_log2(n) <= (uint32_t)Shapes<K>::v[v].max_log2n;
+  return v >= 0 && v < Shapes<K>::count && ceil_log2(n) <= (uint32_t)Shapes<K>::v[v].max_log2n;
 }
 template <typename K>
 constexpr uint32_t variant_tile(int v) {
   return (uint32_t)(Shapes<K>::v[v].block * Shapes<K>::v[v].kpt);
 }
-// smallest tile any allowed variant uses for n keys (sizes the look-back)
 template <typename K>
-constexpr uint32_t min_tile(uint32_t n) {
-  uint32_t t = variant_tile<K>(0);
-  for (int v = 1; v < kNumVariants; ++v)
-    if (variant_allowed<K>(v, n) && variant_tile<K>(v) < t) t = variant_tile<K>(v);
-  return t;
+constexpr uint32_t variant_bits(int v) {
+  return (uint32_t)Shapes<K>::v[v].bits;
+}
+constexpr uint32_t passes_for(int begin_bit, int end_bit, uint32_t bits) {
+  return (uint32_t)((end_bit - begin_bit + (int)bits - 1) / (int)bits);
+}
+// look-back words one region needs for n keys: the largest tiles x digits of
+// any allowed variant
+template <typename K>
+constexpr size_t lookback_words(uint32_t n) {
+  size_t w = 0;
+  for (int v = 0; v < Shapes<K>::count; ++v) {
+    if (!variant_allowed<K>(v, n)) continue;
+    const size_t t = ((size_t)n + variant_tile<K>(v) - 1) / variant_tile<K>(v);
+    const size_t x = (t ? t : 1) * ((size_t)1 << variant_bits<K>(v));
+    if (x > w) w = x;
+  }
+  return w;
+}
+// digits per pass of the widest allowed variant (sizes the histograms)
+template <typename K>
+constexpr uint32_t max_radix(uint32_t n) {
+  uint32_t r = 256;
+  for (int v = 0; v < Shapes<K>::count; ++v)
+    if (variant_allowed<K>(v, n) && (1u << variant_bits<K>(v)) > r) r = 1u << variant_bits<K>(v);
+  return r;
 }
 
 // Process-wide tuning table: variant per (key bytes, values, log2 n).  A
@@ -95,12 +128,16 @@ inline int choose_variant(uint32_t n, int sm_count) {
   int v = tuned_variant((int)sizeof(K), HAS_V, n);
   if (variant_allowed<K>(v, n)) return v;
   // built-in: the largest tile that still gives every SM two tiles
-  for (int c = 0; c < kNumVariants; ++c) {
-    if (!variant_allowed<K>(c, n)) continue;
+  // built-in: 10-bit digits for small 64-bit-key sorts (measured faster up
+  // to 2^15 keys), else the largest 8-bit tile that still gives every SM two
+  // tiles
+  if (sizeof(K) == 8 && HAS_V && n <= (1u << 15) && variant_allowed<K>(4, n)) return 4;
+  for (int c = 0; c < Shapes<K>::count; ++c) {
+    if (!variant_allowed<K>(c, n) || variant_bits<K>(c) != 8) continue;
     if ((n + variant_tile<K>(c) - 1) / variant_tile<K>(c) >= (uint32_t)(2 * sm_count)) return c;
   }
-  for (int c = kNumVariants - 1; c >= 0; --c)
-    if (variant_allowed<K>(c, n)) return c;
+  for (int c = Shapes<K>::count - 1; c >= 0; --c)
+    if (variant_allowed<K>(c, n) && variant_bits<K>(c) == 8) return c;
   return 0;
 }
 
@@ -145,32 +182,38 @@ __device__ __forceinline__ uint32_t scan256_exclusive(uint32_t v, uint32_t* tmp8
 constexpr int kHistBlock = 256;
 constexpr int kHistCopies = 4;  // copies per pass inside a CTA
 
+// Shared copies per pass of a histogram of 2^digit_bits digits.
+__host__ __device__ constexpr uint32_t hist_copies(uint32_t digit_bits) { return digit_bits > 8 ? 2u : (uint32_t)kHistCopies; }
+constexpr size_t hist_smem(uint32_t passes, uint32_t digit_bits) {
+  return (size_t)passes * hist_copies(digit_bits) * (1u << digit_bits) * 4;
+}
+
 template <typename K>
 __global__ void __launch_bounds__(kHistBlock) global_histogram_kernel(const K* __restrict__ keys, uint32_t n,
                                                                       uint32_t begin_bit, uint32_t n_passes,
-                                                                      uint32_t end_bit,
+                                                                      uint32_t end_bit, uint32_t digit_bits,
                                                                       uint32_t* __restrict__ ghist) {
-  extern __shared__ uint32_t s_hist[];  // n_passes * kHistCopies * 256
-  const uint32_t words = n_passes * kHistCopies * kRadix;
+  extern __shared__ uint32_t s_hist[];  // n_passes * copies * 2^digit_bits
+  const uint32_t radix = 1u << digit_bits, copies = hist_copies(digit_bits);
+  const uint32_t words = n_passes * copies * radix;
   for (uint32_t i = threadIdx.x; i < words; i += kHistBlock) s_hist[i] = 0;
   __syncthreads();
-  const uint32_t copy = (threadIdx.x >> 5) % kHistCopies;
+  const uint32_t copy = (threadIdx.x >> 5) % copies;
   const uint32_t stride = gridDim.x * kHistBlock;
   for (uint32_t i = blockIdx.x * kHistBlock + threadIdx.x; i < n; i += stride) {
     K k = keys[i];
     for (uint32_t p = 0; p < n_passes; ++p) {
-      uint32_t sh = begin_bit + 8 * p;
-      uint32_t bits = min(8u, end_bit - sh);
+      uint32_t sh = begin_bit + digit_bits * p;
+      uint32_t bits = min(digit_bits, end_bit - sh);
       uint32_t d = (uint32_t)(k >> sh) & ((1u << bits) - 1u);
-      atomicAdd(&s_hist[(p * kHistCopies + copy) * kRadix + d], 1u);
+      atomicAdd(&s_hist[(p * copies + copy) * radix + d], 1u);
     }
   }
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n_passes * kRadix; i += kHistBlock) {
-    uint32_t p = i / kRadix, d = i % kRadix, s = 0;
-#pragma unroll
-    for (int c = 0; c < kHistCopies; ++c) s += s_hist[(p * kHistCopies + c) * kRadix + d];
-    if (s) atomicAdd(&ghist[p * kRadix + d], s);
+  for (uint32_t i = threadIdx.x; i < n_passes * radix; i += kHistBlock) {
+    uint32_t p = i / radix, d = i % radix, s = 0;
+    for (uint32_t c = 0; c < copies; ++c) s += s_hist[(p * copies + c) * radix + d];
+    if (s) atomicAdd(&ghist[p * radix + d], s);
   }
 }
 
@@ -408,41 +451,313 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
 }
 
 // ---------------------------------------------------------------------------
+// One pass over wide digits (2^RBITS = 1,024 digits): the same steps as
+// onesweep_pass_kernel, reorganised for many digits per thread.
+//  - per-(warp, digit) counters are 16-bit (a tile holds fewer than 65,536
+//    keys) and warp private, so the run leader updates them without an
+//    atomic;
+//  - each thread owns DPT consecutive digits: it publishes and reads their
+//    look-back flags with 16-byte loads and stores, and walks the
+//    predecessors of all of them in one loop;
+//  - the tile scans of the digit totals are one block scan of per-thread
+//    sums.
+// ---------------------------------------------------------------------------
+template <typename K, bool HAS_V, int BLOCK, int KPT, int RBITS>
+struct WideBinSmem {
+  using T = typename Staged<K, HAS_V>::T;
+  static constexpr int kWarps = BLOCK / 32;
+  static constexpr int kTile = BLOCK * KPT;
+  static constexpr int R = 1 << RBITS;
+  static_assert(kTile < 65536, "16-bit per-warp counters");
+  union {
+    T staged[kTile];
+    uint16_t warp_hist[kWarps * R];  // per (warp, digit): count, then start
+  } u;
+  uint32_t digit_offset[R];
+  uint32_t scan_tmp[2][kWarps];
+  uint32_t tile;
+  uint32_t abort;
+};
+
+__device__ __forceinline__ void st_relaxed_gpu_v4(uint32_t* p, uint4 v) {
+  asm volatile("st.relaxed.gpu.global.v4.u32 [%0], {%1, %2, %3, %4};" ::"l"(p), "r"(v.x), "r"(v.y), "r"(v.z),
+               "r"(v.w)
+               : "memory");
+}
+__device__ __forceinline__ uint4 ld_relaxed_gpu_v4(const uint32_t* p) {
+  uint4 v;
+  asm volatile("ld.relaxed.gpu.global.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "l"(p)
+               : "memory");
+  return v;
+}
+
+// exclusive block scans of two values per thread
+template <int BLOCK>
+__device__ __forceinline__ void scan2_exclusive(uint32_t a, uint32_t b, uint32_t* tmpa, uint32_t* tmpb,
+                                                uint32_t& ea, uint32_t& eb) {
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t ia = warp_inclusive_scan(a), ib = warp_inclusive_scan(b);
+  if (lane == 31) {
+    tmpa[warp] = ia;
+    tmpb[warp] = ib;
+  }
+  __syncthreads();
+  uint32_t sa = 0, sb = 0;
+#pragma unroll
+  for (int w = 0; w < BLOCK / 32; ++w)
+    if (w < (int)warp) {
+      sa += tmpa[w];
+      sb += tmpb[w];
+    }
+  ea = sa + ia - a;
+  eb = sb + ib - b;
+  __syncthreads();
+}
+
+template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT, int RBITS>
+__global__ void __launch_bounds__(BLOCK) onesweep_wide_pass_kernel(
+    const K* __restrict__ keys_in, K* __restrict__ keys_out, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
+    uint32_t* __restrict__ lookback, uint32_t* __restrict__ lookback_next, uint32_t* __restrict__ tile_counter,
+    uint32_t* __restrict__ status, uint32_t n, uint32_t shift, uint32_t digit_mask) {
+  using S = WideBinSmem<K, HAS_V, BLOCK, KPT, RBITS>;
+  using ST = Staged<K, HAS_V>;
+  constexpr int R = S::R, kWarps = S::kWarps;
+  constexpr uint32_t kTile = S::kTile;
+  constexpr int DPT = R / BLOCK;  // consecutive digits per thread
+  static_assert(DPT % 4 == 0, "digits are handled in groups of four");
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  {
+    uint4* z = reinterpret_cast<uint4*>(s.u.warp_hist);
+    for (uint32_t i = tid; i < kWarps * R * 2 / 16; i += BLOCK) z[i] = make_uint4(0, 0, 0, 0);
+  }
+  if (tid == 0) {
+    s.tile = atomicAdd(tile_counter, 1u);  // tiles in launch order
+    s.abort = 0;
+  }
+  __syncthreads();
+  const uint32_t tile = s.tile;
+  const uint32_t tile_base = tile * kTile;
+  const uint32_t valid = min(kTile, n - tile_base);
+  const uint32_t d0 = tid * DPT;
+  if (lookback_next) {
+#pragma unroll
+    for (int g = 0; g < DPT / 4; ++g)
+      reinterpret_cast<uint4*>(lookback_next + (size_t)tile * R + d0)[g] = make_uint4(0, 0, 0, 0);
+  }
+
+  K key[KPT];
+  const uint32_t pos0 = tile_base + warp * 32 * KPT + lane;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t p = pos0 + 32 * i;
+    key[i] = (p < n) ? keys_in[p] : KeyTraits<K>::kMax;
+  }
+  // rank among equal digits of the warp, in position order
+  uint16_t* wh = s.u.warp_hist + warp * R;
+  const uint32_t lt = lanemask_lt();
+  uint32_t rank[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t leader = __ffs(peers) - 1;
+    uint32_t before = 0;
+    if (lane == leader) {  // one leader per digit value: no two lanes share a counter
+      before = wh[d];
+      wh[d] = (uint16_t)(before + __popc(peers));
+    }
+    __syncwarp();
+    before = __shfl_sync(0xFFFFFFFFu, before, leader);
+    rank[i] = before + __popc(peers & lt);
+  }
+  __syncthreads();
+
+  // this thread's digits: tile totals, published aggregates, global counts
+  uint32_t total[DPT], agg[DPT], gc[DPT];
+  uint32_t tsum = 0, gsum = 0;
+#pragma unroll
+  for (int j = 0; j < DPT; ++j) {
+    const uint32_t d = d0 + j;
+    uint32_t t = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) t += s.u.warp_hist[w * R + d];
+    total[j] = t;
+    agg[j] = t - ((d == digit_mask) ? (kTile - valid) : 0u);  // padding keys carry the top digit
+    gc[j] = ghist[d];
+    tsum += t;
+    gsum += gc[j];
+  }
+  {
+    const uint32_t f = tile == 0 ? kFlagInc : kFlagAgg;
+#pragma unroll
+    for (int g = 0; g < DPT / 4; ++g)
+      st_relaxed_gpu_v4(lookback + (size_t)tile * R + d0 + 4 * g,
+                        make_uint4(agg[4 * g] | f, agg[4 * g + 1] | f, agg[4 * g + 2] | f, agg[4 * g + 3] | f));
+  }
+  uint32_t tbase, gbase;
+  scan2_exclusive<BLOCK>(tsum, gsum, s.scan_tmp[0], s.scan_tmp[1], tbase, gbase);
+  uint32_t tstart[DPT], gstart[DPT];
+#pragma unroll
+  for (int j = 0; j < DPT; ++j) {
+    tstart[j] = tbase;
+    gstart[j] = gbase;
+    tbase += total[j];
+    gbase += gc[j];
+  }
+  // per (warp, digit) start inside the tile
+#pragma unroll
+  for (int j = 0; j < DPT; ++j) {
+    const uint32_t d = d0 + j;
+    uint32_t run = tstart[j];
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      const uint32_t c = s.u.warp_hist[w * R + d];
+      s.u.warp_hist[w * R + d] = (uint16_t)run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    rank[i] += s.u.warp_hist[warp * R + d];
+  }
+
+  // decoupled look-back over the predecessors, all DPT digits together:
+  // a step consumes one predecessor once every pending digit's flag there
+  // is published
+  uint32_t excl[DPT];
+#pragma unroll
+  for (int j = 0; j < DPT; ++j) excl[j] = 0;
+  if (tile > 0) {
+    constexpr uint32_t kAll = (DPT >= 32) ? 0xFFFFFFFFu : ((1u << DPT) - 1u);
+    uint32_t done = 0;  // bit j: digit j has reached an inclusive prefix
+    int32_t k = (int32_t)tile - 1;
+    uint32_t spins = 0;
+    uint64_t t0 = 0;
+    while (done != kAll && k >= 0) {
+      uint32_t f[DPT];
+#pragma unroll
+      for (int g = 0; g < DPT / 4; ++g) {
+        const uint4 v = ld_relaxed_gpu_v4(lookback + (size_t)k * R + d0 + 4 * g);
+        f[4 * g] = v.x;
+        f[4 * g + 1] = v.y;
+        f[4 * g + 2] = v.z;
+        f[4 * g + 3] = v.w;
+      }
+      bool ready = true;
+#pragma unroll
+      for (int j = 0; j < DPT; ++j)
+        if (!((done >> j) & 1u) && !(f[j] & kFlagMask)) ready = false;
+      if (ready) {
+#pragma unroll
+        for (int j = 0; j < DPT; ++j) {
+          if ((done >> j) & 1u) continue;
+          excl[j] += f[j] & kValueMask;
+          if ((f[j] & kFlagMask) == kFlagInc) done |= 1u << j;
+        }
+        --k;
+        spins = 0;
+        continue;
+      }
+      // not ready: back off, give up after kLookbackTimeoutNs
+      if (spins == 0) t0 = global_timer_ns();
+      ++spins;
+      if ((spins & 63u) == 0 && global_timer_ns() - t0 > kLookbackTimeoutNs) {
+        raise_status(status, BAJO_STATUS_LOOKBACK_TIMEOUT);
+        s.abort = 1;
+        break;
+      }
+      __nanosleep(spins < 64 ? 32 : 256);
+    }
+#pragma unroll
+    for (int g = 0; g < DPT / 4; ++g)
+      st_relaxed_gpu_v4(lookback + (size_t)tile * R + d0 + 4 * g,
+                        make_uint4(((excl[4 * g] + agg[4 * g]) & kValueMask) | kFlagInc,
+                                   ((excl[4 * g + 1] + agg[4 * g + 1]) & kValueMask) | kFlagInc,
+                                   ((excl[4 * g + 2] + agg[4 * g + 2]) & kValueMask) | kFlagInc,
+                                   ((excl[4 * g + 3] + agg[4 * g + 3]) & kValueMask) | kFlagInc));
+  }
+#pragma unroll
+  for (int j = 0; j < DPT; ++j) s.digit_offset[d0 + j] = gstart[j] + excl[j] - tstart[j];
+  __syncthreads();
+  // without a complete prefix the scatter addresses are unknown: write nothing
+  if (s.abort) return;
+
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t v = 0;
+    if constexpr (HAS_V) {
+      const uint32_t p = pos0 + 32 * i;
+      v = (p < n) ? vals_in[p] : 0u;
+    }
+    s.u.staged[rank[i]] = ST::pack(key[i], v);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t j = tid + i * BLOCK;
+    if (j < valid) {
+      const auto e = s.u.staged[j];
+      const K k = ST::key(e);
+      const uint32_t d = (uint32_t)(k >> shift) & digit_mask;
+      const uint32_t dst = s.digit_offset[d] + j;
+      if (dst < n) {  // holds whenever the digit counts are consistent
+        keys_out[dst] = k;
+        if constexpr (HAS_V) vals_out[dst] = ST::val(e);
+        if constexpr (EMIT_LOW32) low32_out[dst] = (uint32_t)k;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // host-side plan
 // ---------------------------------------------------------------------------
 inline uint32_t num_passes(int begin_bit, int end_bit) { return (uint32_t)((end_bit - begin_bit + 7) / 8); }
 
 constexpr size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
-// Workspace of one sort: [status | ghist (P*256) | tile counters (P) |
-// look-back region 0 | look-back region 1 | keys_alt | vals_alt].  ghist,
-// the counters and region 0 must start zeroed (one memset of zero_bytes from
+// Workspace of one sort: [status | ghist | tile counters (P) | look-back
+// region 0 | look-back region 1 | keys_alt | vals_alt].  ghist holds P
+// histograms of up to max_radix digits, a look-back region lookback_words
+// flags (both sized for every variant the size allows).  ghist, the
+// counters and region 0 must start zeroed (one memset of zero_bytes from
 // off_ghist); region 1 is cleared by the first pass.
 // An optional `extra` region (caller data that must also start zeroed) sits
 // between the status word and ghist, inside the zeroed range.
 struct Plan {
-  uint32_t n, passes, tiles_cap;
+  uint32_t n, passes, radix;
+  size_t lb_words;
   size_t off_extra, off_zero, off_ghist, off_counters, off_lookback, zero_bytes, off_keys_alt, off_vals_alt, total;
 };
 
-constexpr Plan make_plan_tiles(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t passes,
-                               uint32_t tiles_cap, size_t extra_zero_bytes = 0) {
+// passes: the 8-bit digit passes of the sorted bit range (every allowed
+// variant needs at most as many).
+constexpr Plan make_plan_words(uint32_t n, uint32_t key_bytes, bool has_values, uint32_t passes, uint32_t radix,
+                               size_t lb_words, size_t extra_zero_bytes = 0) {
   Plan p{};
   p.n = n;
   p.passes = passes;
-  p.tiles_cap = tiles_cap;
+  p.radix = radix;
+  p.lb_words = lb_words;
   size_t o = 256;  // status word
   p.off_extra = o;
   p.off_zero = o;
   o += (extra_zero_bytes + 15) & ~(size_t)15;
   p.off_ghist = o;
-  o += (size_t)passes * kRadix * 4;
+  o += (size_t)passes * radix * 4;
   p.off_counters = o;
   o += (size_t)passes * 4;
   o = (o + 15) & ~(size_t)15;
   p.off_lookback = o;
-  p.zero_bytes = o + (size_t)tiles_cap * kRadix * 4 - p.off_zero;
-  o += 2 * (size_t)tiles_cap * kRadix * 4;
+  p.zero_bytes = o + lb_words * 4 - p.off_zero;
+  o += 2 * lb_words * 4;
   o = align256(o);
   p.off_keys_alt = o;
   o = align256(o + (size_t)n * key_bytes);
@@ -454,8 +769,8 @@ constexpr Plan make_plan_tiles(uint32_t n, uint32_t key_bytes, bool has_values, 
 
 template <typename K>
 constexpr Plan make_plan(uint32_t n, bool has_values, uint32_t passes, size_t extra_zero_bytes = 0) {
-  const uint32_t t = min_tile<K>(n);
-  return make_plan_tiles(n, (uint32_t)sizeof(K), has_values, passes, (n + t - 1) / t, extra_zero_bytes);
+  return make_plan_words(n, (uint32_t)sizeof(K), has_values, passes, max_radix<K>(n), lookback_words<K>(n),
+                         extra_zero_bytes);
 }
 
 template <typename K, bool HAS_V, bool EMIT_LOW32, int V>
@@ -465,8 +780,14 @@ inline cudaError_t launch_variant(const K* kin, K* kout, const uint32_t* vin, ui
                                   cudaStream_t stream) {
   constexpr int B = Shapes<K>::v[V].block;
   constexpr int KPT = Shapes<K>::v[V].kpt;
-  auto kern = onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
-  const size_t smem = sizeof(BinSmem<K, HAS_V, B, KPT>);
+  constexpr int BITS = Shapes<K>::v[V].bits;
+  using Smem = typename std::conditional<BITS == 8, BinSmem<K, HAS_V, B, KPT>,
+                                         WideBinSmem<K, HAS_V, B, KPT, (BITS == 8 ? 10 : BITS)>>::type;
+  auto kern = [] {
+    if constexpr (BITS == 8) return onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
+    else return onesweep_wide_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT, BITS>;
+  }();
+  const size_t smem = sizeof(Smem);
   static bool configured[64] = {};  // per template instance and device
   int dev = 0;
   cudaGetDevice(&dev);
@@ -496,6 +817,11 @@ inline cudaError_t launch_pass(int variant, const K* kin, K* kout, const uint32_
     case 3:
       return launch_variant<K, HAS_V, EMIT_LOW32, 3>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
                                                      status, n, shift, digit_mask, stream);
+    case 4:
+      if constexpr (Shapes<K>::count > 4)
+        return launch_variant<K, HAS_V, EMIT_LOW32, 4>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                       status, n, shift, digit_mask, stream);
+      return cudaErrorInvalidValue;
     default:
       return launch_variant<K, HAS_V, EMIT_LOW32, 0>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
                                                      status, n, shift, digit_mask, stream);
@@ -504,8 +830,9 @@ inline cudaError_t launch_pass(int variant, const K* kin, K* kout, const uint32_
 
 // Runs every digit pass of [begin_bit, end_bit) over keys that start in
 // (k0, v0); the workspace gives the other buffer (k1, v1).  The histograms in
-// the workspace must already hold the counts of every pass, and ghist, the
-// counters and look-back region 0 must be zero.  Returns through
+// the workspace must already hold the counts of every pass in the variant's
+// digit width (pass p at ghist + p * 2^bits), and ghist, the counters and
+// look-back region 0 must be zero.  Returns through
 // *result_in_first whether the sorted keys ended in (k0, v0).  `variant`
 // selects the tile shape (it must be allowed for p.n); pass_events, when
 // given, receive one record after each pass.
@@ -513,31 +840,33 @@ template <typename K, bool HAS_V>
 inline cudaError_t run_passes(K* k0, uint32_t* v0, K* k1, uint32_t* v1, uint32_t* low32_last, const Plan& p,
                               unsigned char* ws, int begin_bit, int end_bit, cudaStream_t stream,
                               bool* result_in_first, int variant, cudaEvent_t* pass_events = nullptr) {
+  if (!variant_allowed<K>(variant, p.n)) return cudaErrorInvalidValue;
+  const uint32_t bits_v = variant_bits<K>(variant), radix = 1u << bits_v;
+  const uint32_t passes = passes_for(begin_bit, end_bit, bits_v);
+  const size_t tiles = ((size_t)p.n + variant_tile<K>(variant) - 1) / variant_tile<K>(variant);
+  if (passes > p.passes || radix > p.radix || tiles * radix > p.lb_words) return cudaErrorInvalidValue;
   uint32_t* status = reinterpret_cast<uint32_t*>(ws);
   uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + p.off_ghist);
   uint32_t* counters = reinterpret_cast<uint32_t*>(ws + p.off_counters);
   uint32_t* region[2] = {reinterpret_cast<uint32_t*>(ws + p.off_lookback),
-                         reinterpret_cast<uint32_t*>(ws + p.off_lookback) + (size_t)p.tiles_cap * kRadix};
-  if (!variant_allowed<K>(variant, p.n) ||
-      (p.n + variant_tile<K>(variant) - 1) / variant_tile<K>(variant) > p.tiles_cap)
-    return cudaErrorInvalidValue;
+                         reinterpret_cast<uint32_t*>(ws + p.off_lookback) + p.lb_words};
   K* src = k0;
   K* dst = k1;
   uint32_t* vs = v0;
   uint32_t* vd = v1;
-  for (uint32_t pass = 0; pass < p.passes; ++pass) {
-    uint32_t sh = (uint32_t)begin_bit + 8 * pass;
-    uint32_t bits = min(8u, (uint32_t)end_bit - sh);
+  for (uint32_t pass = 0; pass < passes; ++pass) {
+    uint32_t sh = (uint32_t)begin_bit + bits_v * pass;
+    uint32_t bits = min(bits_v, (uint32_t)end_bit - sh);
     uint32_t mask = (1u << bits) - 1u;
     uint32_t* lb = region[pass & 1];
-    uint32_t* lb_next = (pass + 1 < p.passes) ? region[(pass + 1) & 1] : nullptr;
+    uint32_t* lb_next = (pass + 1 < passes) ? region[(pass + 1) & 1] : nullptr;
     cudaError_t e;
-    bool last = pass + 1 == p.passes;
+    bool last = pass + 1 == passes;
     if (last && low32_last)
-      e = launch_pass<K, HAS_V, true>(variant, src, dst, vs, vd, low32_last, ghist + pass * kRadix, lb, lb_next,
+      e = launch_pass<K, HAS_V, true>(variant, src, dst, vs, vd, low32_last, ghist + pass * radix, lb, lb_next,
                                       counters + pass, status, p.n, sh, mask, stream);
     else
-      e = launch_pass<K, HAS_V, false>(variant, src, dst, vs, vd, nullptr, ghist + pass * kRadix, lb, lb_next,
+      e = launch_pass<K, HAS_V, false>(variant, src, dst, vs, vd, nullptr, ghist + pass * radix, lb, lb_next,
                                        counters + pass, status, p.n, sh, mask, stream);
     if (e != cudaSuccess) return e;
     if (pass_events && (e = cudaEventRecord(pass_events[pass], stream)) != cudaSuccess) return e;

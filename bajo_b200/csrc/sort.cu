@@ -58,19 +58,25 @@ int32_t sort_impl(K* keys, uint32_t* vals, uint32_t n, int32_t begin_bit, int32_
   cudaStream_t stream = (cudaStream_t)stream_;
   unsigned char* w = (unsigned char*)ws;
   if (cudaMemsetAsync(w + p.off_zero, 0, p.zero_bytes, stream) != cudaSuccess) return BAJO_ERR_CUDA;
+  const int variant = onesweep::choose_variant<K, HAS_V>(n, sm_count());
+  const uint32_t bits = onesweep::variant_bits<K>(variant);
+  const uint32_t vpasses = onesweep::passes_for(begin_bit, end_bit, bits);
   uint32_t* ghist = (uint32_t*)(w + p.off_ghist);
-  const size_t hsmem = (size_t)passes * onesweep::kHistCopies * onesweep::kRadix * 4;
+  const size_t hsmem = onesweep::hist_smem(vpasses, bits);
   uint32_t grid = (n + onesweep::kHistBlock * 16 - 1) / (onesweep::kHistBlock * 16);
   uint32_t max_grid = (uint32_t)sm_count() * 4;
   if (grid > max_grid) grid = max_grid;
   if (grid == 0) grid = 1;
+  if (hsmem > 48 * 1024 &&
+      cudaFuncSetAttribute(onesweep::global_histogram_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)hsmem) != cudaSuccess)
+    return BAJO_ERR_CUDA;
   onesweep::global_histogram_kernel<K><<<grid, onesweep::kHistBlock, hsmem, stream>>>(
-      keys, n, (uint32_t)begin_bit, passes, (uint32_t)end_bit, ghist);
+      keys, n, (uint32_t)begin_bit, vpasses, (uint32_t)end_bit, bits, ghist);
   if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
   K* kalt = (K*)(w + p.off_keys_alt);
   uint32_t* valt = HAS_V ? (uint32_t*)(w + p.off_vals_alt) : nullptr;
   bool in_first = true;
-  const int variant = onesweep::choose_variant<K, HAS_V>(n, sm_count());
   if (onesweep::run_passes<K, HAS_V>(keys, vals, kalt, valt, nullptr, p, w, begin_bit, end_bit, stream,
                                      &in_first, variant) != cudaSuccess)
     return BAJO_ERR_CUDA;
@@ -115,7 +121,8 @@ int32_t bajo_sort_workspace_size(uint32_t n, uint32_t key_bytes, int32_t has_val
 
 int32_t bajo_sort_tuning_set(uint32_t key_bytes, int32_t has_values, uint32_t log2n, int32_t variant) {
   using namespace bajo::onesweep;
-  if ((key_bytes != 4 && key_bytes != 8) || log2n > 32 || variant < -1 || variant >= kNumVariants)
+  if ((key_bytes != 4 && key_bytes != 8) || log2n > 32 || variant < -1 ||
+      variant >= (key_bytes == 4 ? Shapes<uint32_t>::count : Shapes<uint64_t>::count))
     return BAJO_ERR_INVALID_ARGUMENT;
   if (variant >= 0) {
     const uint32_t n = log2n >= 32 ? 0xFFFFFFFFu : (1u << log2n);

@@ -86,13 +86,13 @@ extern "C" int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_val
   if (n > 1 && passes > 0) {
     if (cudaMemsetAsync(w + p.off_zero, 0, p.zero_bytes, stream) != cudaSuccess) return BAJO_ERR_CUDA;
     uint32_t* ghist = (uint32_t*)(w + p.off_ghist);
-    const size_t hsmem = (size_t)passes * onesweep::kHistCopies * onesweep::kRadix * 4;
+    const size_t hsmem = onesweep::hist_smem(passes, 8);  // 32-bit keys: 8-bit digits only
     uint32_t grid = (n + onesweep::kHistBlock * 16 - 1) / (onesweep::kHistBlock * 16);
     const uint32_t max_grid = (uint32_t)sm_count() * 4;
     if (grid > max_grid) grid = max_grid;
     if (grid == 0) grid = 1;
     onesweep::global_histogram_kernel<uint32_t><<<grid, onesweep::kHistBlock, hsmem, stream>>>(
-        d_keys, n, (uint32_t)begin_bit, passes, (uint32_t)end_bit, ghist);
+        d_keys, n, (uint32_t)begin_bit, passes, (uint32_t)end_bit, 8u, ghist);
     if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
     uint32_t* kalt = (uint32_t*)(w + p.off_keys_alt);
     uint32_t* valt = (uint32_t*)(w + p.off_vals_alt);

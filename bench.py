@@ -300,7 +300,9 @@ def run_bajo(args):
     L.bajo_lbvh_stage_count(N_TRIS, 1, ctypes.byref(n_ev))
     n_ev = n_ev.value
     passes = n_ev - 5
-    kernels_per_build = 4 + passes  # bounds, morton, passes, topology, refit
+    # bounds, Morton, the sort passes, then one bottom-up hierarchy kernel (up
+    # to 2^17 triangles) or topology + refit
+    kernels_per_build = (3 if N_TRIS <= 1 << 17 else 4) + passes
 
     def build_timed(events):
         arr = (ctypes.c_void_p * n_ev)(*[e.cuda_event for e in events])

@@ -174,7 +174,44 @@ def test_every_tile_variant_matches_oracle(oracle, variant, kind):
             L.bajo_sort_tuning_set(kb, 0, lg, -1)
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("bits", [(0, 30), (0, 44), (0, 64), (5, 37), (32, 40)])
+def test_wide_digit_variant_matches_oracle(oracle, bits):
+    """Variant 4 of the 64-bit keys sorts 10-bit digits (passes of
+    [begin, begin + 10), ... with a shorter last pass); any bit range, pairs
+    and keys only, bit-exact with the oracle and stable."""
+    from bajo_b200 import _lib
+    L = _lib.load()
+    begin, end = bits
+    rng = np.random.default_rng(begin * 100 + end)
+    try:
+        for n in (1, 2, 1000, 1025, 70_001, 262_144):
+            lg = int(np.ceil(np.log2(max(n, 2))))
+            assert L.bajo_sort_tuning_set(8, 1, lg, 4) == _lib.OK
+            assert L.bajo_sort_tuning_set(8, 0, lg, 4) == _lib.OK
+            keys = rng.integers(0, 2**63, size=n, dtype=np.uint64) * np.uint64(2) + rng.integers(0, 2, size=n).astype(np.uint64)
+            keys[: n // 4] = keys[0]  # long runs of equal keys
+            vals = np.arange(n, dtype=np.uint32)
+            k, v = gpu_sort(keys, vals, begin, end)
+            ok, ov = oracle.sort_pairs(keys, vals, begin, end)
+            assert np.array_equal(k, ok) and np.array_equal(v, ov)
+            k2, _ = gpu_sort(keys, None, begin, end)
+            assert np.array_equal(k2, ok)
+    finally:
+        for lg in range(33):
+            L.bajo_sort_tuning_set(8, 1, lg, -1)
+            L.bajo_sort_tuning_set(8, 0, lg, -1)
+
+
+def test_wide_digit_variant_limits():
+    from bajo_b200 import _lib
+    L = _lib.load()
+    assert L.bajo_sort_tuning_set(4, 1, 16, 4) == _lib.ERR_INVALID_ARGUMENT   # 32-bit keys: 8-bit digits only
+    assert L.bajo_sort_tuning_set(8, 1, 19, 4) == _lib.ERR_INVALID_ARGUMENT   # up to 2^18 keys
+    assert L.bajo_sort_tuning_set(8, 1, 18, 4) == _lib.OK
+    assert L.bajo_sort_tuning_set(8, 1, 18, -1) == _lib.OK
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 def test_lbvh_build_with_every_variant(oracle, variant):
     from bajo_b200 import _lib, bvh, scenes
     L = _lib.load()
