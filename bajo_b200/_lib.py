@@ -24,6 +24,7 @@ STATUS_STACK_OVERFLOW = 0x2
 STATUS_BAD_TOPOLOGY = 0x4
 STATUS_WIDE_TIMEOUT = 0x40
 STATUS_STAGE_TIMEOUT = 0x80
+STATUS_WAIT_TIMEOUT = 0x100
 TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
@@ -105,6 +106,7 @@ SIGNATURES = {
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_stage_top": (_I32, [ctypes.POINTER(BajoLbvhC), _P]),
+    "bajo_wait_selftest": (_I32, [_P, _U32, _U32, _P, _P]),
     "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_batch": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, ctypes.c_uint64, _I32, _P, _P,

@@ -148,6 +148,19 @@ __device__ __forceinline__ void st_release_gpu(uint32_t* p, uint32_t v) {
   asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Bounded wait for a flag another thread publishes: spins with acquire loads
+// until any of `bits` is set in *p, for at most limit_ns (global timer).
+// Returns false when the limit ran out; the caller then reports a status and
+// returns instead of waiting further.  Every wait on another thread's flag in
+// this library goes through a bound like this one.
+__device__ __forceinline__ bool wait_bits_acquire(const uint32_t* p, uint32_t bits, uint64_t limit_ns) {
+  if (ld_acquire_gpu(p) & bits) return true;
+  const uint64_t t0 = global_timer_ns();
+  while (!(ld_acquire_gpu(p) & bits))
+    if (global_timer_ns() - t0 > limit_ns) return false;
+  return true;
+}
+
 // Device status word bits (read back by bajo_workspace_status).
 __device__ __forceinline__ void raise_status(uint32_t* status, uint32_t bit) {
   if (status) atomicOr(status, bit);

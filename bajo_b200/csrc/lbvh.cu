@@ -419,14 +419,9 @@ __global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
       red_add_release_gpu(flag, kBoxReady);
       return;
     }
-    if (!(old & kBoxReady)) {
-      const uint64_t t0 = global_timer_ns();
-      while (!(ld_acquire_gpu(flag) & kBoxReady)) {
-        if (global_timer_ns() - t0 > kRefitWaitNs) {
-          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-          return;
-        }
-      }
+    if (!(old & kBoxReady) && !wait_bits_acquire(flag, kBoxReady, kRefitWaitNs)) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      return;
     }
     const bool sib_leaf = (old & kLeafArrive) != 0;
     const int sd = (int)((old >> 16) & 0x7Fu) - 1;
@@ -723,14 +718,9 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
         atomicSub(&node_flags[parent], kBoxReady);
       } else {
         if (!ready) {
-          if (!(old & kBoxReady)) {
-            const uint64_t t0 = global_timer_ns();
-            while (!(ld_acquire_gpu(&node_flags[parent]) & kBoxReady)) {
-              if (global_timer_ns() - t0 > kRefitWaitNs) {
-                raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-                return;
-              }
-            }
+          if (!(old & kBoxReady) && !wait_bits_acquire(&node_flags[parent], kBoxReady, kRefitWaitNs)) {
+            raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+            return;
           }
           smn = mk(__ldcg(sib + 0), __ldcg(sib + 1), __ldcg(sib + 2));
           smx = mk(__ldcg(sib + 3), __ldcg(sib + 4), __ldcg(sib + 5));
@@ -1028,3 +1018,22 @@ int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_e
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// bounded-wait self-test
+// ---------------------------------------------------------------------------
+namespace bajo {
+namespace {
+__global__ void wait_selftest_kernel(const uint32_t* flag, uint32_t bits, uint64_t limit_ns, uint32_t* status) {
+  if (!wait_bits_acquire(flag, bits, limit_ns)) raise_status(status, BAJO_STATUS_WAIT_TIMEOUT);
+}
+}  // namespace
+}  // namespace bajo
+
+extern "C" int32_t bajo_wait_selftest(const uint32_t* d_flag, uint32_t bits, uint32_t limit_us, uint32_t* d_status,
+                                      void* stream) {
+  if (!d_flag || !d_status || bits == 0 || limit_us == 0 || limit_us > 1000000u) return BAJO_ERR_INVALID_ARGUMENT;
+  bajo::wait_selftest_kernel<<<1, 1, 0, (cudaStream_t)stream>>>(d_flag, bits, (uint64_t)limit_us * 1000ull,
+                                                                d_status);
+  return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}

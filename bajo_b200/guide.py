@@ -118,6 +118,31 @@ class GuideNetwork:
                                              self.adam_v.data_ptr(), self.step, lr, beta1, beta2, eps, grad_scale,
                                              _lib.stream_handle(stream)), "bajo_mlp_adam")
 
+    # ---- checkpoint ---------------------------------------------------------
+    # A plain dump of the training state: FP32 master weights, their FP16
+    # copy, both Adam moments and the step count, so that training resumes
+    # exactly where it stopped (the next Adam step sees the same state).
+    def state(self) -> dict:
+        torch.cuda.synchronize()
+        return {"params32": self.params32.cpu().numpy(), "params16": self.params16.cpu().numpy(),
+                "adam_m": self.adam_m.cpu().numpy(), "adam_v": self.adam_v.cpu().numpy(),
+                "step": np.int64(self.step), "n_params": np.int64(N_PARAMS)}
+
+    def save(self, path: str) -> None:
+        np.savez(path, **self.state())
+
+    @classmethod
+    def load(cls, path: str, device="cuda") -> "GuideNetwork":
+        with np.load(path) as z:
+            if int(z["n_params"]) != N_PARAMS:
+                raise ValueError(f"checkpoint holds {int(z['n_params'])} parameters, the network has {N_PARAMS}")
+            net = cls(device, params=z["params32"])
+            net.params16.copy_(torch.from_numpy(z["params16"]).to(device))
+            net.adam_m.copy_(torch.from_numpy(z["adam_m"]).to(device))
+            net.adam_v.copy_(torch.from_numpy(z["adam_v"]).to(device))
+            net.step = int(z["step"])
+        return net
+
     def train_records(self, records: "GuideRecords", box: torch.Tensor, batch: int, steps: int, lr: float = 1e-2,
                       stream=None):
         """`steps` Adam steps on `batch` records each (count read on device)."""

@@ -43,6 +43,7 @@ extern "C" {
 #define BAJO_STATUS_BAD_TOPOLOGY 0x4u     /* refit met an inconsistent parent  */
 #define BAJO_STATUS_WIDE_TIMEOUT 0x40u    /* wide collapse gave up on a task   */
 #define BAJO_STATUS_STAGE_TIMEOUT 0x80u   /* staged top levels did not arrive  */
+#define BAJO_STATUS_WAIT_TIMEOUT 0x100u   /* bajo_wait_selftest gave up        */
 
 /* triangle tests */
 #define BAJO_TRI_MT 0         /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
@@ -184,6 +185,17 @@ int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_e
  * top_nodes was NULL: the staged copy is not checked against the tree beyond
  * its root ref. */
 int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream);
+
+/* Diagnostic for the library's failure detection (the reference spins
+ * without a bound, onesweep.mojo:246-270; its wide collapse bounds its spin
+ * and reports a timeout, wide_collapse.mojo:236-253): one device thread waits
+ * through the same bounded-wait helper the kernels use until any of `bits`
+ * is set in *d_flag, for at most limit_us microseconds (1..1,000,000), and
+ * on timeout ORs BAJO_STATUS_WAIT_TIMEOUT into *d_status and returns.  A
+ * flag that nothing sets shows the wait ending with a status instead of
+ * hanging the GPU. */
+int32_t bajo_wait_selftest(const uint32_t* d_flag, uint32_t bits, uint32_t limit_us, uint32_t* d_status,
+                           void* stream);
 
 /* ======================================================================== */
 /* Closest-hit traversal                                                     */

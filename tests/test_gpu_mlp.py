@@ -151,3 +151,38 @@ def test_training_learns_a_direction_field():
                           d[:2000], w[:2000], BOX) / 2000
     _, l2 = net.gradient(P[:2000], N[:2000], D[:2000], W[:2000], box)
     assert float(l2.item()) / 2000 == pytest.approx(ref, abs=2e-2)
+
+
+def test_checkpoint_resumes_training_exactly(tmp_path):
+    """save() / load() keep the whole training state: after reloading, the
+    same gradient gives the same Adam step, bit for bit."""
+    rng = np.random.default_rng(5)
+    n = 4096
+    pos, nrm, d, w = _batch(rng, n)
+    P, N, D, W = _dev(pos, nrm, d, w)
+    box = torch.from_numpy(BOX).cuda()
+    a = guide.GuideNetwork("cuda", seed=3)
+    for _ in range(25):
+        a.gradient(P, N, D, W, box)
+        a.adam(lr=1e-2, grad_scale=1.0 / n)
+    path = str(tmp_path / "guide.npz")
+    a.save(path)
+    b = guide.GuideNetwork.load(path)
+    assert b.step == a.step == 25
+    for name in ("params32", "params16", "adam_m", "adam_v"):
+        assert torch.equal(getattr(a, name), getattr(b, name)), name
+    a.gradient(P, N, D, W, box)
+    b.grad_buf.copy_(a.grad_buf)  # one gradient for both (its atomics may sum in any order)
+    a.adam(lr=1e-2, grad_scale=1.0 / n)
+    b.adam(lr=1e-2, grad_scale=1.0 / n)
+    torch.cuda.synchronize()
+    assert torch.equal(a.params32, b.params32) and torch.equal(a.params16, b.params16)
+    assert torch.equal(a.adam_m, b.adam_m) and torch.equal(a.adam_v, b.adam_v)
+
+
+def test_checkpoint_of_another_network_is_refused(tmp_path):
+    path = str(tmp_path / "bad.npz")
+    np.savez(path, params32=np.zeros(10, np.float32), params16=np.zeros(10, np.float16),
+             adam_m=np.zeros(10, np.float32), adam_v=np.zeros(10, np.float32), step=np.int64(0), n_params=np.int64(10))
+    with pytest.raises(ValueError):
+        guide.GuideNetwork.load(path)
