@@ -31,6 +31,7 @@ SENTINEL = 0xFFFFFFFF
 LEAF_FLAG = 0x80000000
 HIT_STRIDE = 8   # Hit.STRIDE, bajo/bvh/types.mojo:23
 RAY_STRIDE = 8   # Ray.STRIDE, bajo/core/ray.mojo:10
+STATS_WORDS = 5  # GpuTraversalStats.STRIDE, bajo/bvh/gpu/trace.mojo:68
 
 _DTYPES = {
     "internal_offsets": torch.int32, "leaf_bounds": torch.float32, "seg_bounds": torch.float32,
@@ -151,10 +152,12 @@ class GpuTriangleBvh:
     def launch_camera_instrumented(self, d_camera_params: torch.Tensor, d_hits: torch.Tensor | None,
                                    d_stats: torch.Tensor, ray_count: int, width: int, height: int,
                                    tri_mode: int = TRI_WATERTIGHT, stream=None) -> None:
-        """launch_camera plus per-ray [node visits, triangle tests]
+        """launch_camera plus STATS_WORDS counters per ray in the layout of
+        GpuTraversalStats (bajo/bvh/gpu/trace.mojo:62-90): node visits,
+        internal child hits, leaf blocks, triangle tests, deepest stack
         (launch_camera_instrumented, triangle_bvh.mojo:550)."""
         _lib.require_cuda(d_stats)
-        if d_stats.numel() < 2 * ray_count or d_stats.element_size() != 4:
+        if d_stats.numel() < STATS_WORDS * ray_count or d_stats.element_size() != 4:
             raise ValueError("traversal stats output buffer is too short")
         c = self.c_struct()
         rc = _lib.load().bajo_trace_camera_stats(ctypes.byref(c), d_camera_params.data_ptr(), ray_count, width,

@@ -109,12 +109,15 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   f3 up = mk(__ldg(c + 9), __ldg(c + 10), __ldg(c + 11));
   f3 dir = normalize((fwd + right * (sx * fs)) + up * (sy * fs));
   Ray r = make_ray(mk(__ldg(c + 0), __ldg(c + 1), __ldg(c + 2)), dir, 0.0f, FLT_MAX);
-  uint32_t nn = 0, nt = 0;
+  uint32_t st[kStatWords] = {0, 0, 0, 0, 0};
   Hit h;
-  if constexpr (TOP) h = trace_bvh2_top<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, top, &nn, &nt);
-  else h = trace_bvh2<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, &nn, &nt);
+  if constexpr (TOP) h = trace_bvh2_top<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, top, st);
+  else h = trace_bvh2<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, st);
   store_hit(h, tris, i, hits8, out_t, out_prim);
-  if constexpr (STATS) reinterpret_cast<uint2*>(stats)[i] = make_uint2(nn, nt);
+  if constexpr (STATS) {
+#pragma unroll
+    for (int k = 0; k < kStatWords; ++k) stats[(size_t)i * kStatWords + k] = st[k];
+  }
 }
 
 template <int MODE, bool STATS, bool TOP>

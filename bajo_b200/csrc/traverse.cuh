@@ -79,6 +79,13 @@ struct Hit {
   uint32_t prim, leaf;
 };
 
+// Per-ray traversal counters, in the order of the reference's
+// GpuTraversalStats (bajo/bvh/gpu/trace.mojo:62-90): internal nodes visited,
+// internal children whose box was hit, leaf blocks entered, triangles
+// tested, deepest stack.
+constexpr int kStatNodeVisits = 0, kStatChildHits = 1, kStatLeafBlocks = 2, kStatPrimTests = 3, kStatMaxStack = 4;
+constexpr int kStatWords = BAJO_TRACE_STATS_WORDS;
+
 __device__ __forceinline__ bool better(float t, uint32_t prim, const Hit& h) {
   return t < h.t || (t == h.t && prim < h.prim);
 }
@@ -260,8 +267,8 @@ __device__ __forceinline__ void stage_top_drain(TopSmem& sm, const float4* stage
 template <int MODE, bool STATS, bool ANY, bool PAR, bool TOP = false>
 __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                                const uint4* __restrict__ meta, const float4* __restrict__ tris,
-                                               uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes,
-                                               uint32_t* n_tris, const float4* top = nullptr) {
+                                               uint32_t max_nodes, uint32_t* status, uint32_t* stats,
+                                               const float4* top = nullptr) {
   Hit h;
   h.t = r.tmax;
   h.u = h.v = 0.0f;
@@ -270,7 +277,10 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
   if (root == kSentinel) return h;
   if (root & kLeafFlag) {
     test_tri<MODE>(r, tris, root & kIndexMask, h);
-    if constexpr (STATS) ++*n_tris;
+    if constexpr (STATS) {
+      ++stats[kStatLeafBlocks];
+      ++stats[kStatPrimTests];
+    }
     return h;
   }
   // any-hit queries stop at the first accepted triangle; boxes are culled
@@ -284,7 +294,7 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
       break;
     }
-    if constexpr (STATS) ++*n_nodes;
+    if constexpr (STATS) ++stats[kStatNodeVisits];
     float4 b0, b1, b2;  // b0 L: min xyz, max x | b1 L: max yz, R: min xy | b2 R: min z, max xyz
     uint2 m;            // left, right child refs
     if (staged) {
@@ -309,17 +319,24 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
     if (hl) {
       if (m.x & kLeafFlag) {
         test_tri<MODE>(r, tris, m.x & kIndexMask, h);
-        if constexpr (STATS) ++*n_tris;
+        if constexpr (STATS) {
+          ++stats[kStatLeafBlocks];
+          ++stats[kStatPrimTests];
+        }
         if (ANY && h.leaf != kEmpty) return h;
       } else vl = true;
     }
     if (hr) {
       if (m.y & kLeafFlag) {
         test_tri<MODE>(r, tris, m.y & kIndexMask, h);
-        if constexpr (STATS) ++*n_tris;
+        if constexpr (STATS) {
+          ++stats[kStatLeafBlocks];
+          ++stats[kStatPrimTests];
+        }
         if (ANY && h.leaf != kEmpty) return h;
       } else vr = true;
     }
+    if constexpr (STATS) stats[kStatChildHits] += (uint32_t)vl + (uint32_t)vr;
     int near = -1;
     if (vl) near = 0;
     if (vr && (near == -1 || tr < tl)) near = 1;
@@ -331,6 +348,7 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
       if (far_valid && far_t <= limit) {
         if (sp < kStack) stack[sp++] = near == 0 ? m.y : m.x;
         else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+        if constexpr (STATS) stats[kStatMaxStack] = max(stats[kStatMaxStack], (uint32_t)sp);
       }
       if (near_t <= limit) {
         cur = near == 0 ? m.x : m.y;
@@ -348,11 +366,10 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
 template <int MODE, bool STATS = false, bool ANY = false>
 __device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                           const uint4* __restrict__ meta, const float4* __restrict__ tris,
-                                          uint32_t max_nodes, uint32_t* status, uint32_t* n_nodes = nullptr,
-                                          uint32_t* n_tris = nullptr) {
+                                          uint32_t max_nodes, uint32_t* status, uint32_t* stats = nullptr) {
   if (has_parallel_axis(r))
-    return trace_bvh2_impl<MODE, STATS, ANY, true>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
-  return trace_bvh2_impl<MODE, STATS, ANY, false>(r, root, nb, meta, tris, max_nodes, status, n_nodes, n_tris);
+    return trace_bvh2_impl<MODE, STATS, ANY, true>(r, root, nb, meta, tris, max_nodes, status, stats);
+  return trace_bvh2_impl<MODE, STATS, ANY, false>(r, root, nb, meta, tris, max_nodes, status, stats);
 }
 
 // Same, starting from the staged top (slot 0 is `root`) when `top` is set.
@@ -361,15 +378,13 @@ template <int MODE, bool STATS = false, bool ANY = false>
 __device__ __forceinline__ Hit trace_bvh2_top(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                               const uint4* __restrict__ meta, const float4* __restrict__ tris,
                                               uint32_t max_nodes, uint32_t* status, const float4* top,
-                                              uint32_t* n_nodes = nullptr, uint32_t* n_tris = nullptr) {
+                                              uint32_t* stats = nullptr) {
   // without staged records no ref carries BAJO_TOP_FLAG (node indices stay
   // below 2^30), so the same loop runs from the global root
   const uint32_t start = top ? BAJO_TOP_FLAG : root;
   if (has_parallel_axis(r))
-    return trace_bvh2_impl<MODE, STATS, ANY, true, true>(r, start, nb, meta, tris, max_nodes, status, n_nodes,
-                                                         n_tris, top);
-  return trace_bvh2_impl<MODE, STATS, ANY, false, true>(r, start, nb, meta, tris, max_nodes, status, n_nodes,
-                                                        n_tris, top);
+    return trace_bvh2_impl<MODE, STATS, ANY, true, true>(r, start, nb, meta, tris, max_nodes, status, stats, top);
+  return trace_bvh2_impl<MODE, STATS, ANY, false, true>(r, start, nb, meta, tris, max_nodes, status, stats, top);
 }
 
 }  // namespace trav

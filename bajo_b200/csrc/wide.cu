@@ -364,12 +364,15 @@ __global__ void __launch_bounds__(trav::kTraceBlock) wide_camera_kernel(
   const f3 right = mk(__ldg(c + 6), __ldg(c + 7), __ldg(c + 8));
   const f3 up = mk(__ldg(c + 9), __ldg(c + 10), __ldg(c + 11));
   const f3 dir = normalize((fwd + right * (sx * fs)) + up * (sy * fs));
-  uint32_t nn = 0, nt = 0;
+  uint32_t st[trav::kStatWords] = {0, 0, 0, 0, 0};
   const trav::Hit h =
       trace_wide<W, MODE, STATS>(trav::make_ray(mk(__ldg(c + 0), __ldg(c + 1), __ldg(c + 2)), dir, 0.0f, FLT_MAX),
-                                 v, status, &nn, &nt);
+                                 v, status, st);
   store_hit(h, v.bvh2_tris, i, hits8, out_t, out_prim);
-  if constexpr (STATS) reinterpret_cast<uint2*>(stats)[i] = make_uint2(nn, nt);
+  if constexpr (STATS) {
+#pragma unroll
+    for (int k = 0; k < trav::kStatWords; ++k) stats[(size_t)i * trav::kStatWords + k] = st[k];
+  }
 }
 
 // ---------------------------------------------------------------------------

@@ -138,7 +138,7 @@ struct View {
 // equal to the binary tree's bit for bit.
 template <int W, int MODE, bool STATS, bool ANY, bool PAR>
 __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const View& v, uint32_t* status,
-                                                     uint32_t* n_nodes, uint32_t* n_tris) {
+                                                     uint32_t* stats) {
   trav::Hit h;
   h.t = r.tmax;
   h.u = h.v = 0.0f;
@@ -153,7 +153,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
       break;
     }
-    if constexpr (STATS) ++*n_nodes;
+    if constexpr (STATS) ++stats[trav::kStatNodeVisits];
     const float4* node = reinterpret_cast<const float4*>(v.nodes + (size_t)cur * kFields * W);
     float f[kFields][W];
 #pragma unroll
@@ -178,6 +178,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
         continue;
       const uint32_t count = meta >> kCountShift, data = meta & kDataMask;
       if (count == 0) {
+        if constexpr (STATS) ++stats[trav::kStatChildHits];
         ci[nc] = data;
         ct[nc] = tn;
         ++nc;
@@ -187,9 +188,10 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
         raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
         continue;
       }
+      if constexpr (STATS) ++stats[trav::kStatLeafBlocks];
       const size_t base = (size_t)data * kLeafStride * W;
       for (uint32_t k = 0; k < count; ++k) {
-        if constexpr (STATS) ++*n_tris;
+        if constexpr (STATS) ++stats[trav::kStatPrimTests];
         float t, u, vv;
         bool ok;
         uint32_t prim;
@@ -238,6 +240,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
       if (ct[k] > limit) continue;
       if (sp < trav::kStack) stack[sp++] = make_uint2(ci[k], __float_as_uint(ct[k]));
       else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+      if constexpr (STATS) stats[trav::kStatMaxStack] = max(stats[trav::kStatMaxStack], (uint32_t)sp);
     }
     if (nc > 0 && ct[0] <= limit) {
       cur = ci[0];
@@ -259,9 +262,9 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
 
 template <int W, int MODE, bool STATS = false, bool ANY = false>
 __device__ __forceinline__ trav::Hit trace_wide(const trav::Ray& r, const View& v, uint32_t* status,
-                                                uint32_t* n_nodes = nullptr, uint32_t* n_tris = nullptr) {
-  if (trav::has_parallel_axis(r)) return trace_wide_impl<W, MODE, STATS, ANY, true>(r, v, status, n_nodes, n_tris);
-  return trace_wide_impl<W, MODE, STATS, ANY, false>(r, v, status, n_nodes, n_tris);
+                                                uint32_t* stats = nullptr) {
+  if (trav::has_parallel_axis(r)) return trace_wide_impl<W, MODE, STATS, ANY, true>(r, v, status, stats);
+  return trace_wide_impl<W, MODE, STATS, ANY, false>(r, v, status, stats);
 }
 
 }  // namespace wide

@@ -381,12 +381,12 @@ def run_bajo(args):
     traffic = committed_traffic().get("onesweep_pass_65536")
 
     # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
-    stats = torch.empty(2 * n_rays, dtype=torch.int32, device=dev)
+    stats = torch.empty(5 * n_rays, dtype=torch.int32, device=dev)
     _lib.check(L.bajo_trace_camera_stats(ctypes.byref(c_trace), cam.data_ptr(), n_rays, WIDTH, HEIGHT,
                                          _lib.TRI_WATERTIGHT, None, stats.data_ptr(), sh), "bajo_trace_camera_stats")
     torch.cuda.synchronize()
-    st = stats.view(-1, 2).double()
-    nodes_per_ray, tris_per_ray = float(st[:, 0].mean()), float(st[:, 1].mean())
+    st = stats.view(-1, 5).double()  # GpuTraversalStats: visits, child hits, leaf blocks, tri tests, max stack
+    nodes_per_ray, tris_per_ray = float(st[:, 0].mean()), float(st[:, 3].mean())
     trace_bytes = n_rays * (nodes_per_ray * NODE_BYTES + tris_per_ray * TRI_BYTES + HIT_BYTES)
     trace_achieved = trace_bytes / (statistics.mean(trace_ms) / 1e3) / 1e9
 
@@ -767,9 +767,9 @@ def run_case(args):
         hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
         ms_wide = timed(lambda: w.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
         ms_bin = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
-        stats = torch.zeros(2 * WIDTH * HEIGHT, dtype=torch.int32, device="cuda")
+        stats = torch.zeros(5 * WIDTH * HEIGHT, dtype=torch.int32, device="cuda")
         w.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, d_stats=stats)
-        s = stats.view(-1, 2).double().mean(0).tolist()
+        s = stats.view(-1, 5).double().mean(0)[[0, 3]].tolist()
         out.update({"node_width": args.node_width, "max_leaf": args.max_leaf, "wide_nodes": w.n_nodes, "leaf_blocks": w.n_leaf_blocks,
                     "collapse_ms": round(ms_build, 5), "collapse_mtri_s": round(n / ms_build / 1e3, 2),
                     "wide_trace_ms": round(ms_wide, 4), "wide_mrays_s": round(WIDTH * HEIGHT / ms_wide / 1e3, 2),

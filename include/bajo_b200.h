@@ -233,9 +233,12 @@ int32_t bajo_trace_batch(const BajoLbvh* bvh, const float* d_cameras, uint32_t c
                          float* d_t1, uint32_t* d_prim1, uint32_t* d_status, void* stream);
 
 /* Instrumented camera trace (trace_triangle_bvh_camera_instrumented_kernel,
- * bajo/bvh/gpu/triangle_bvh.mojo:813; GpuTraversalStats,
- * bajo/bvh/gpu/trace.mojo:62): same hits as bajo_trace_camera plus, per ray,
- * d_stats[2i] = internal nodes visited, d_stats[2i+1] = triangles tested. */
+ * bajo/bvh/gpu/triangle_bvh.mojo:813): same hits as bajo_trace_camera plus,
+ * per ray, BAJO_TRACE_STATS_WORDS counters in the layout of
+ * GpuTraversalStats (bajo/bvh/gpu/trace.mojo:62-90): d_stats[5i + 0]
+ * internal nodes visited, + 1 internal children whose box was hit, + 2 leaf
+ * blocks entered, + 3 triangles tested, + 4 deepest traversal stack. */
+#define BAJO_TRACE_STATS_WORDS 5
 int32_t bajo_trace_camera_stats(const BajoLbvh* bvh, const float* d_cameras, uint32_t n_rays, uint32_t width,
                                 uint32_t height, int32_t tri_mode, float* d_hits8, uint32_t* d_stats,
                                 void* stream);
@@ -292,8 +295,8 @@ int32_t bajo_wide_counts(const BajoWideBvh* wide, void* stream, uint32_t* n_node
  * arguments and outputs as bajo_trace_rays / bajo_trace_camera plus segment
  * 0's node and leaf-block counts (bajo_wide_counts; the node count bounds the
  * visits, the block count the leaf references); d_stats (may be NULL)
- * receives [nodes visited, triangles tested] per ray.  Hits equal the binary
- * tree's bit for bit. */
+ * receives BAJO_TRACE_STATS_WORDS counters per ray, as
+ * bajo_trace_camera_stats.  Hits equal the binary tree's bit for bit. */
 int32_t bajo_trace_wide_rays(const BajoWideBvh* wide, uint32_t n_nodes, uint32_t n_leaf_blocks, const float* d_rays,
                              uint32_t n_rays,
                              int32_t tri_mode, float* d_hits8, float* d_t, uint32_t* d_prim, uint32_t* d_status,

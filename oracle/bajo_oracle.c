@@ -677,14 +677,18 @@ static bo_hit miss_hit(float tmax) {
  * bajo/bvh/gpu/trace.mojo:340-428: test both child boxes against the current
  * hit distance, intersect leaf children immediately, continue with the nearer
  * internal child and push the other one if it is still within reach. */
+/* st (may be NULL): the five per-ray counters of GpuTraversalStats
+ * (bajo/bvh/gpu/trace.mojo:62-90): internal nodes visited, internal children
+ * whose box was hit, leaf blocks entered (one triangle each here), triangles
+ * tested, deepest stack. */
 static bo_hit trace_one(const BoLbvh* bvh, const float* verts, const bo_ray* r, uint32_t seg, int mode,
-                        uint32_t* nodes_visited, uint32_t* tris_tested) {
+                        uint32_t* st) {
   bo_hit h = miss_hit(r->tmax);
   uint32_t root = bvh->roots[seg];
   /* prim ids are reported relative to the segment's first item
    * (pack_segmented_triangle_leaf_lanes_kernel, triangle_bvh.mojo:117-120) */
   uint32_t first_item = bvh->seg_offsets ? bvh->seg_offsets[seg] : 0;
-  uint32_t nv = 0, nt = 0;
+  uint32_t nv = 0, nt = 0, nc = 0, ms = 0;
   if (root == BO_SENTINEL) goto done;
   if (root & BO_LEAF_FLAG) {
     uint32_t item = bvh->leaf_ids[root & 0x7FFFFFFFu];
@@ -715,6 +719,7 @@ static bo_hit trace_one(const BoLbvh* bvh, const float* verts, const bo_ray* r, 
       } else {
         valid[k] = 1;
         ct[k] = tn;
+        nc++;
       }
     }
     int near = -1;
@@ -722,15 +727,23 @@ static bo_hit trace_one(const BoLbvh* bvh, const float* verts, const bo_ray* r, 
     if (valid[1] && (near == -1 || ct[1] < ct[0])) near = 1;
     if (near >= 0) {
       int far = 1 - near;
-      if (valid[far] && ct[far] <= h.t * BO_SLACK) stack[sp++] = c[far];
+      if (valid[far] && ct[far] <= h.t * BO_SLACK) {
+        stack[sp++] = c[far];
+        if (sp > ms) ms = sp;
+      }
       if (ct[near] <= h.t * BO_SLACK) { cur = c[near]; continue; }
     }
     if (sp == 0) break;
     cur = stack[--sp];
   }
 done:
-  if (nodes_visited) *nodes_visited = nv;
-  if (tris_tested) *tris_tested = nt;
+  if (st) {
+    st[0] = nv;
+    st[1] = nc;
+    st[2] = nt;
+    st[3] = nt;
+    st[4] = ms;
+  }
   return h;
 }
 
@@ -748,7 +761,7 @@ static void trace_range(void* p, uint32_t b, uint32_t e) {
   trace_ctx* c = (trace_ctx*)p;
   for (uint32_t i = b; i < e; ++i) {
     bo_ray r = make_ray(c->rays, c->n, i);
-    bo_hit h = trace_one(c->bvh, c->verts, &r, 0, c->mode, NULL, NULL);
+    bo_hit h = trace_one(c->bvh, c->verts, &r, 0, c->mode, NULL);
     store_hit(c->hits, i, &h);
   }
 }
@@ -763,7 +776,7 @@ void bo_trace_bvh2_stats(const BoLbvh* bvh, const float* verts, const float* ray
                          uint32_t* stats) {
   for (uint32_t i = 0; i < n; ++i) {
     bo_ray r = make_ray(rays, n, i);
-    trace_one(bvh, verts, &r, 0, mode, &stats[2 * (size_t)i], &stats[2 * (size_t)i + 1]);
+    trace_one(bvh, verts, &r, 0, mode, &stats[5 * (size_t)i]);
   }
 }
 
@@ -1284,7 +1297,7 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
   float rad[3] = {0.0f, 0.0f, 0.0f};
   for (uint32_t b = 0; b < c->max_depth; ++b) {
     bo_ray ray = make_ray_od(o, d, tmin, tmax);
-    bo_hit hit = trace_one(c->bvh, c->verts, &ray, 0, BO_TRI_WATERTIGHT, NULL, NULL);
+    bo_hit hit = trace_one(c->bvh, c->verts, &ray, 0, BO_TRI_WATERTIGHT, NULL);
     if (hit.prim == BO_EMPTY) {
       v3 un = v3normalize(d);
       float a = 0.5f * (un.y + 1.0f);
@@ -1481,7 +1494,7 @@ static void batch_range(void* p, uint32_t b, uint32_t e) {
     v3 d = v3normalize(v3add(v3add(load3(cam + 3), v3muls(load3(cam + 6), sx * fs)), v3muls(load3(cam + 9), sy * fs)));
     v3 o = load3(cam);
     bo_ray r = make_ray_od(o, d, 0.0f, BO_FLT_MAX);
-    bo_hit h = trace_one(c->bvh, c->verts, &r, view, c->mode, NULL, NULL);
+    bo_hit h = trace_one(c->bvh, c->verts, &r, view, c->mode, NULL);
     c->t0[i] = h.t;
     c->p0[i] = h.prim;
     float bt = BO_FLT_MAX;
@@ -1493,7 +1506,7 @@ static void batch_range(void* p, uint32_t b, uint32_t e) {
       v3 dir = lambertian_dir(normal, u[0], u[1]);
       v3 p = v3make(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
       bo_ray r2 = make_ray_od(p, dir, 0.001f, BO_FLT_MAX);
-      bo_hit h2 = trace_one(c->bvh, c->verts, &r2, view, c->mode, NULL, NULL);
+      bo_hit h2 = trace_one(c->bvh, c->verts, &r2, view, c->mode, NULL);
       bt = h2.t;
       bp = h2.prim;
     }

@@ -131,8 +131,10 @@ void bo_trace_bvh2(const BoLbvh* bvh, const float* verts, const float* rays_soa,
 void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays_soa,
                     uint32_t n_rays, int tri_mode, float* hits8,
                     uint32_t n_threads);
-/* per-ray node visits / triangle tests on the BVH2 (GpuTraversalStats,
- * bajo/bvh/gpu/trace.mojo:62) -> stats[2*i] = nodes, stats[2*i+1] = tris */
+/* per-ray traversal counters on the BVH2 in the layout of GpuTraversalStats
+ * (bajo/bvh/gpu/trace.mojo:62-90): stats[5*i + 0..4] = internal nodes
+ * visited, internal children hit, leaf blocks entered, triangles tested,
+ * deepest stack */
 void bo_trace_bvh2_stats(const BoLbvh* bvh, const float* verts,
                          const float* rays_soa, uint32_t n_rays, int tri_mode,
                          uint32_t* stats);

@@ -296,7 +296,7 @@ def trace_bvh2(bvh: OracleLbvh, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT, t
 def trace_bvh2_stats(bvh: OracleLbvh, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT) -> np.ndarray:
     rays = np.ascontiguousarray(rays_soa, np.float32)
     n = rays.size // 8
-    stats = np.empty(2 * n, np.uint32)
+    stats = np.empty(5 * n, np.uint32)  # GpuTraversalStats per ray (trace.mojo:62-90)
     s = bvh.struct()
     lib().bo_trace_bvh2_stats(ctypes.byref(s), _ptr(bvh.verts), _ptr(rays), n, tri_mode, _ptr(stats))
     return stats

@@ -127,7 +127,7 @@ def test_staged_camera_and_counts_equal_unstaged():
     for staged in (True, False):
         c = tree.c_struct(stage_top=staged)
         hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
-        stats = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+        stats = torch.zeros(5 * n, dtype=torch.int32, device="cuda")
         _lib.check(_lib.load().bajo_trace_camera(ctypes.byref(c), cam.data_ptr(), n, 1024, 1024, 1, hits.data_ptr(),
                                                  None, None, None, None), "bajo_trace_camera")
         h2 = torch.empty_like(hits)

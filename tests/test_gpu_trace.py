@@ -125,3 +125,31 @@ def test_large_scene_camera_property(oracle):
     torch.cuda.synchronize()
     ref = oracle.trace_bvh2(oracle.lbvh_build(v), oracle.camera_rays(cam, n, 256, 256), oracle.TRI_WATERTIGHT)
     assert np.array_equal(hits.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+@pytest.mark.parametrize("n_tris", [1, 2, 1000, 65536])
+def test_instrumented_counts_match_oracle(oracle, mode, n_tris):
+    """bajo_trace_camera_stats writes the reference's five GpuTraversalStats
+    counters per ray (node visits, internal child hits, leaf blocks, triangle
+    tests, deepest stack); the walk is the oracle's, so every counter of
+    every ray is equal."""
+    from bajo_b200 import camera
+    v = scenes.random_triangles(n_tris, seed=n_tris)
+    b = build(v)
+    cam = camera.plain_lbvh_camera()
+    w = h = 256
+    n = w * h
+    hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+    stats = torch.zeros(5 * n, dtype=torch.int32, device="cuda")
+    b.launch_camera_instrumented(dev(cam), hits, stats, n, w, h, tri_mode=mode)
+    torch.cuda.synchronize()
+    o = oracle.lbvh_build(v)
+    rays = oracle.camera_rays(cam, n, w, h)
+    want = oracle.trace_bvh2_stats(o, rays, mode)
+    got = stats.cpu().numpy().view(np.uint32)
+    assert np.array_equal(got, want)
+    s = got.reshape(-1, 5)
+    assert np.array_equal(s[:, 2], s[:, 3])  # one triangle per binary leaf
+    if n_tris > 2:
+        assert s[:, 4].max() > 0

@@ -138,7 +138,7 @@ def test_wide_camera_plain_workload(oracle, W, max_leaf):
     cam = dev(camera.plain_lbvh_camera())
     n = 1024 * 1024
     hw = torch.empty(8 * n, dtype=torch.float32, device="cuda")
-    stats = torch.zeros(2 * n, dtype=torch.int32, device="cuda")
+    stats = torch.zeros(5 * n, dtype=torch.int32, device="cuda")
     st = w.launch_camera(cam, hw, n, 1024, 1024, d_stats=stats)
     hb = torch.empty(8 * n, dtype=torch.float32, device="cuda")
     tree.launch_camera(cam, hb, n, 1024, 1024)
@@ -148,6 +148,8 @@ def test_wide_camera_plain_workload(oracle, W, max_leaf):
     ref = oracle.trace_bvh2(oracle.lbvh_build(v), oracle.camera_rays(camera.plain_lbvh_camera(), n, 1024, 1024),
                             oracle.TRI_WATERTIGHT)
     assert np.array_equal(hw.cpu().numpy().view(np.uint32), ref.view(np.uint32))
-    s = stats.view(-1, 2).double().mean(0).cpu().numpy()
-    print(f"W={W} max_leaf={max_leaf}: {s[0]:.2f} wide nodes, {s[1]:.2f} triangles per ray")
+    s = stats.view(-1, 5).double().mean(0).cpu().numpy()
+    print(f"W={W} max_leaf={max_leaf}: {s[0]:.2f} wide nodes, {s[3]:.2f} triangles per ray")
     assert s[0] < 24.0  # the binary tree visits ~24 nodes per ray here
+    st = stats.view(-1, 5).cpu().numpy()
+    assert np.all(st[:, 2] <= st[:, 3]) and np.all(st[:, 3] <= max_leaf * st[:, 2])  # blocks hold 1..max_leaf
