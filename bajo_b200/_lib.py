@@ -107,6 +107,12 @@ SIGNATURES = {
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_stage_top": (_I32, [ctypes.POINTER(BajoLbvhC), _P]),
     "bajo_wait_selftest": (_I32, [_P, _U32, _U32, _P, _P]),
+    "bajo_render_create": (_I32, [_P, _P, _SZ, ctypes.POINTER(_P)]),
+    "bajo_render_enqueue": (_I32, [_P, _P, _P, _P, _P, _P, _P]),
+    "bajo_render_download": (_I32, [_P, _P, _P, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64),
+                                    ctypes.POINTER(_U32), _P]),
+    "bajo_render_graph_launches": (_I32, [_P, ctypes.POINTER(_U32)]),
+    "bajo_render_destroy": (_I32, [_P]),
     "bajo_trace_rays": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_camera": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, _I32, _P, _P, _P, _P, _P]),
     "bajo_trace_batch": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _U32, _U32, _U32, ctypes.c_uint64, _I32, _P, _P,

@@ -133,3 +133,55 @@ def render_gpu_triangles(settings: RenderSettings, camera, scene: GpuRtTriangleS
                                  workspace.buffer.numel(), _lib.stream_handle(stream))
     _lib.check(rc, "bajo_render")
     return pixels
+
+
+class Renderer:
+    """Handle-based rendering (bajo_render_create / enqueue / download /
+    destroy): the settings and workspace are fixed at creation; the first
+    enqueue on a non-default stream records the render into a CUDA graph,
+    later enqueues with the same buffers replay it with one launch."""
+
+    def __init__(self, settings: RenderSettings, algorithm: int = MIS, device="cuda"):
+        self.settings, self.algorithm = settings, algorithm
+        self.workspace = RenderWorkspace(settings, algorithm, device)
+        self._c = settings.c(algorithm)
+        h = ctypes.c_void_p()
+        _lib.check(_lib.load().bajo_render_create(ctypes.byref(self._c), self.workspace.buffer.data_ptr(),
+                                                  self.workspace.buffer.numel(), ctypes.byref(h)),
+                   "bajo_render_create")
+        self._h = h
+        self._scene_c = None
+
+    def enqueue(self, scene: GpuRtTriangleScene, camera: torch.Tensor, pixels: torch.Tensor,
+                pixels64: torch.Tensor | None = None, guide=None, stream=None) -> None:
+        self._scene_c = scene.c()  # kept alive: the graph was recorded with its pointers
+        rc = _lib.load().bajo_render_enqueue(self._h, ctypes.byref(self._scene_c), camera.data_ptr(),
+                                             None if guide is None else ctypes.byref(guide), pixels.data_ptr(),
+                                             None if pixels64 is None else pixels64.data_ptr(),
+                                             _lib.stream_handle(stream))
+        _lib.check(rc, "bajo_render_enqueue")
+
+    def download(self, pixels: torch.Tensor, stream=None):
+        """(host float32 image, closest-hit rays, shadow rays, status)."""
+        out = np.empty((self.settings.height, self.settings.width, 3), np.float32)
+        a, b, st = ctypes.c_uint64(0), ctypes.c_uint64(0), ctypes.c_uint32(0)
+        _lib.check(_lib.load().bajo_render_download(self._h, pixels.data_ptr(), out.ctypes.data, ctypes.byref(a),
+                                                    ctypes.byref(b), ctypes.byref(st), _lib.stream_handle(stream)),
+                   "bajo_render_download")
+        return out, a.value, b.value, st.value
+
+    def graph_launches(self) -> int:
+        n = ctypes.c_uint32(0)
+        _lib.check(_lib.load().bajo_render_graph_launches(self._h, ctypes.byref(n)), "bajo_render_graph_launches")
+        return n.value
+
+    def close(self) -> None:
+        if self._h:
+            _lib.load().bajo_render_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # pragma: no cover
+            pass

@@ -728,9 +728,29 @@ def run_case(args):
         ms = timed(lambda: rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws))
         rays, shadows = ws.ray_counts()
         paths = 1280 * 720 * args.spp
+        # the same render through the handle API on a side stream: recorded
+        # once into a CUDA graph, then one graph launch per render
+        renderer = rt.Renderer(settings, rt.MIS)
+        side = torch.cuda.Stream()
+        cam = torch.from_numpy(sc.camera.astype("float32")).cuda()
+        px = torch.empty((720, 1280, 3), dtype=torch.float32, device="cuda")
+        ms_graph = []
+        with torch.cuda.stream(side):
+            for _ in range(max(1, args.warmup)):
+                renderer.enqueue(gsc, cam, px, stream=side)
+            side.synchronize()
+            for _ in range(args.steps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(side)
+                renderer.enqueue(gsc, cam, px, stream=side)
+                b.record(side)
+                b.synchronize()
+                ms_graph.append(a.elapsed_time(b))
+        renderer.close()
         out.update({"ms": round(ms, 3), "samples_s": round(paths / ms * 1e3, 1),
                     "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
-                    "triangles": sc.n_tris, "status": ws.status()})
+                    "triangles": sc.n_tris, "graph_ms": round(statistics.median(ms_graph), 3),
+                    "status": ws.status()})
     elif args.case == "batched":
         out.update(run_batched(args.steps, args.warmup, args.scenes))
     elif args.case == "guided":

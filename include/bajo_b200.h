@@ -375,6 +375,7 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
  * the last bajo_render call on this workspace. */
 int32_t bajo_render_stats(const void* d_workspace, void* stream, uint64_t* rays, uint64_t* shadow_rays);
 
+
 /* ======================================================================== */
 /* Path guiding: a small MLP proposal trained online (new on this path; the  */
 /* reference has no guiding)                                                 */
@@ -439,6 +440,31 @@ int32_t bajo_guide_records_size(uint32_t capacity, size_t* bytes);
 int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, const BajoRenderSettings* settings,
                            const BajoGuide* guide, float* d_pixels, double* d_pixels64, void* d_workspace,
                            size_t workspace_bytes, void* stream);
+
+/* Handle-based rendering (render_gpu_triangles / enqueue_render_gpu_triangles,
+ * bajo/rt/gpu/triangle_path.mojo:143,172; GpuRtRenderTarget download,
+ * bajo/rt/gpu/resources.mojo:275).  The caller owns the workspace (at least
+ * bajo_render_workspace_size bytes), the scene and the pixel buffers; the
+ * handle is host memory holding the settings and a CUDA graph of the last
+ * enqueued render.  bajo_render_enqueue renders like bajo_render (guide =
+ * NULL) or bajo_render_guided (settings->algorithm BAJO_RENDER_GUIDED).  On a
+ * stream other than the legacy default stream the first enqueue records the
+ * render into a graph and launches it; later enqueues with the same
+ * pointers, scene, guide and settings replay the graph with one launch (it
+ * reads buffer contents at replay, so new camera or scene data in the same
+ * buffers is picked up).  Inside a capture the caller started, the render is
+ * recorded into that capture.  bajo_render_download synchronises `stream`,
+ * copies the pixels (3 f32 each) to host memory when h_pixels is set and
+ * reads the status word and the ray totals. */
+typedef struct BajoRenderer BajoRenderer;
+int32_t bajo_render_create(const BajoRenderSettings* settings, void* d_workspace, size_t workspace_bytes,
+                           BajoRenderer** renderer);
+int32_t bajo_render_enqueue(BajoRenderer* renderer, const BajoRtScene* scene, const float* d_camera,
+                            const BajoGuide* guide, float* d_pixels, double* d_pixels64, void* stream);
+int32_t bajo_render_download(BajoRenderer* renderer, const float* d_pixels, float* h_pixels, uint64_t* rays,
+                             uint64_t* shadow_rays, uint32_t* status, void* stream);
+int32_t bajo_render_graph_launches(const BajoRenderer* renderer, uint32_t* launches);
+int32_t bajo_render_destroy(BajoRenderer* renderer);
 
 /* Online training state (device arrays of bajo_mlp_param_count elements). */
 typedef struct BajoGuideNet {
