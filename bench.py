@@ -70,8 +70,8 @@ def parse():
     p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
     p.add_argument("--spp", type=int, default=64, help="--case render samples per pixel")
     p.add_argument("--scenes", type=int, default=4096, help="--case batched scene count")
-    p.add_argument("--train-passes", type=int, default=8, help="--case guided passes followed by training")
-    p.add_argument("--train-steps", type=int, default=8, help="--case guided Adam steps per training pass")
+    p.add_argument("--train-passes", type=int, default=16, help="--case guided passes followed by training")
+    p.add_argument("--train-steps", type=int, default=32, help="--case guided Adam steps per training pass")
     return p.parse_args()
 
 

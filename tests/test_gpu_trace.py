@@ -153,3 +153,28 @@ def test_instrumented_counts_match_oracle(oracle, mode, n_tris):
     assert np.array_equal(s[:, 2], s[:, 3])  # one triangle per binary leaf
     if n_tris > 2:
         assert s[:, 4].max() > 0
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_three_camera_views_match_oracle(oracle, mode):
+    """One launch over three 64x48 views (camera record of view i at 20 * i,
+    camera_launch.mojo:34-55), as the reference's camera fixtures do
+    (test/bvh/fixtures.mojo:141): hits equal the oracle's per ray."""
+    from bajo_b200 import camera
+    v = scenes.random_triangles(5000, seed=21, spread=0.03)
+    b = build(v)
+    cams = np.concatenate([
+        camera.camera_from_vfov([0.5, 0.5, -1.5], [0.5, 0.5, 0.5], [0.0, 1.0, 0.0], 60.0),
+        camera.camera_from_vfov([2.0, 0.7, 0.5], [0.5, 0.5, 0.5], [0.0, 1.0, 0.0], 45.0),
+        camera.camera_from_vfov([0.4, 2.5, 0.6], [0.5, 0.5, 0.5], [0.0, 0.0, 1.0], 75.0),
+    ]).astype(np.float32)
+    w, h = 64, 48
+    n = 3 * w * h
+    hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+    b.launch_camera(dev(cams), hits, n, w, h, tri_mode=mode)
+    torch.cuda.synchronize()
+    ref = oracle.trace_bvh2(oracle.lbvh_build(v), oracle.camera_rays(cams, n, w, h), mode)
+    got = hits.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    per_view = (oracle.hits_prim(got).reshape(3, -1) != oracle.EMPTY).mean(axis=1)
+    assert np.all(per_view > 0.02)  # every view sees geometry
