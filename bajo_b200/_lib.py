@@ -89,6 +89,20 @@ class BajoWideSizesC(ctypes.Structure):
     _fields_ = [(name, _SZ) for name in WIDE_ARRAYS] + [("workspace", _SZ)]
 
 
+class BajoCwbvh8C(ctypes.Structure):
+    """Mirror of ``struct BajoCwbvh8`` (include/bajo_b200.h)."""
+    _fields_ = [("n_segments", _U32), ("n_tris", _U32), ("node_offsets", _P), ("nodes", _P), ("triangles", _P)]
+
+
+CWBVH8_ARRAYS = ("node_offsets", "nodes", "triangles")
+CWBVH8_NODE_WORDS = 20  # BAJO_CWBVH8_NODE_WORDS
+CWBVH8_TRI_WORDS = 12   # BAJO_CWBVH8_TRI_WORDS
+
+
+class BajoCwbvh8SizesC(ctypes.Structure):
+    _fields_ = [(name, _SZ) for name in CWBVH8_ARRAYS] + [("workspace", _SZ)]
+
+
 # every symbol the header declares, with its ctypes signature
 SIGNATURES = {
     "bajo_workspace_status": (_I32, [_P, _P, ctypes.POINTER(_U32)]),
@@ -130,6 +144,12 @@ SIGNATURES = {
                                     _P]),
     "bajo_trace_wide_camera": (_I32, [ctypes.POINTER(BajoWideBvhC), _U32, _U32, _P, _U32, _U32, _U32, _I32, _P, _P,
                                       _P, _P, _P, _P]),
+    "bajo_cwbvh8_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoCwbvh8SizesC)]),
+    "bajo_cwbvh8_build": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoCwbvh8C), _P, _SZ, _P]),
+    "bajo_cwbvh8_count": (_I32, [ctypes.POINTER(BajoCwbvh8C), _P, ctypes.POINTER(_U32)]),
+    "bajo_trace_cwbvh8_rays": (_I32, [ctypes.POINTER(BajoCwbvh8C), _U32, _P, _U32, _I32, _P, _P, _P, _P, _P]),
+    "bajo_trace_cwbvh8_camera": (_I32, [ctypes.POINTER(BajoCwbvh8C), _U32, _P, _U32, _U32, _U32, _I32, _P, _P, _P,
+                                        _P, _P]),
     "bajo_mlp_param_count": (_I32, [ctypes.POINTER(_U32)]),
     "bajo_mlp_forward": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
     "bajo_mlp_grad": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),

@@ -6,8 +6,10 @@
 // pack_segmented_triangle_leaf_lanes_kernel (bajo/bvh/gpu/triangle_bvh.mojo:
 // 81-148), driven by enqueue_segmented_wide_build (segmented_build.mojo:89)
 // with max_leaf_size = leaf width and fat leaves on.  The reference hands out
-// node and leaf ids with atomics while its work queue runs, so its layout
-// differs from run to run; here ids are pre-order and fixed:
+// node and leaf ids with atomics while its work queue runs -- a node takes its
+// internal children's ids as one contiguous range and its leaf blocks as
+// another (wide_collapse.mojo:551-559) -- so its layout differs from run to
+// run; here ids have the same shape and are fixed:
 //   1. count_kernel climbs the binary tree bottom-up (refit-style arrival
 //      flags) and, at every internal node x, applies the opening rule to
 //      find the children the wide node rooted at x would have, and the
@@ -16,11 +18,24 @@
 //   2. offsets_kernel turns the roots' counts into per-segment node and leaf
 //      offsets and publishes each root's task;
 //   3. assign_kernel walks wide node ids in increasing order: node I's task
-//      (binary node, first leaf block) is published by its parent, which has
-//      a smaller id, so every wait points backwards and a resident grid
-//      always makes progress.  Node I writes its own leaf blocks first, then
-//      gives child c the id I + 1 + (wide nodes of the children before it)
-//      and the matching leaf base, and publishes c's task.
+//      (binary node, first descendant id D, first leaf block, first
+//      triangle) is published by its parent, which has a smaller id, so every
+//      wait points backwards and a resident grid always makes progress.  Node
+//      I writes its own leaf blocks first, gives its internal children the
+//      ids D, D + 1, ... in lane order, and hands child c the descendant range
+//      after its siblings' (D + internal children + the NW - 1 of the children
+//      before it) with the matching leaf base, then publishes c's task.
+//
+// The CWBVH8 build (W = 8, leaves of at most 3 triangles) runs the same three
+// kernels with octant slots (spatial_slots, wide_collapse.mojo:457-521: the
+// candidates go to the eight lanes by a greedy centroid-octant assignment) and
+// encodes each node straight from its lane boxes into the 80-byte compressed
+// node of _encode_cwbvh8_node (compressed_bounds_bvh.mojo:84-325), packing its
+// triangles as 48-byte records (pack_segmented_cwbvh_triangles_kernel,
+// :372-404).  The reference reserves a node's triangle range with an atomic
+// counter; here node I's range starts at the first triangle of I's subtree in
+// depth-first lane order (own leaf lanes, then each internal child's subtree),
+// one of the orders that atomic can produce.
 #include <algorithm>
 
 #include "wide.cuh"
@@ -42,6 +57,8 @@ struct Work {
   uint32_t* task_ref;   // [wide node] binary ref
   uint32_t* task_leaf;  // [wide node] first leaf block (global)
   uint32_t* task_seg;   // [wide node] segment
+  uint32_t* task_desc;  // [wide node] id of its first internal child (global)
+  uint32_t* task_tri;   // [wide node] first triangle of its subtree (global; CWBVH8)
   uint32_t* ready;      // [wide node] task published
   uint32_t* status;
 };
@@ -141,6 +158,8 @@ __global__ void __launch_bounds__(1024) offsets_kernel(uint32_t n_seg, const uin
       wk.task_ref[pn] = roots[s];
       wk.task_leaf[pn] = pl;
       wk.task_seg[pn] = s;
+      wk.task_desc[pn] = pn + 1u;
+      wk.task_tri[pn] = seg_offsets[s];
       wk.ready[pn] = 1u;
     }
     pn += cn;
@@ -157,6 +176,8 @@ struct Out {
   uint32_t* leaf_indices;
   float* leaf_tris;
   uint32_t* leaf_sorted;
+  float4* cw_nodes;  // CWBVH8: [node][5] (80 B)
+  float4* cw_tris;   // CWBVH8: [triangle][3] (48 B)
 };
 
 // leaf block `blk` (global) from the binary subtree `ref` (<= 4 leaves),
@@ -205,6 +226,181 @@ __device__ void write_leaf_block(uint32_t ref, uint32_t blk, const uint32_t* __r
   }
 }
 
+// CWBVH8 triangle records of the binary subtree `ref` (<= 3 leaves), left to
+// right, from global position `pos` (pack_segmented_cwbvh_triangles_kernel,
+// compressed_bounds_bvh.mojo:372-404): [e1][0][e2][0][v0][segment-local prim].
+// Returns the position after the last record.
+__device__ uint32_t write_cw_tris(uint32_t ref, uint32_t pos, uint32_t cap, const uint32_t* __restrict__ node_meta,
+                                  const float4* __restrict__ tris, const Out& o, uint32_t* status) {
+  uint32_t stack[kFatLeaf + 1];
+  int sp = 0;
+  stack[sp++] = ref;
+  while (sp > 0) {
+    const uint32_t cur = stack[--sp];
+    if (cur & kLeafFlag) {
+      if (pos >= cap) {
+        raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+        return pos;
+      }
+      const uint32_t sl = cur & kIndexMask;
+      const float4 a = __ldg(tris + (size_t)sl * 3 + 0);
+      const float4 b = __ldg(tris + (size_t)sl * 3 + 1);
+      const float4 c = __ldg(tris + (size_t)sl * 3 + 2);
+      float4* r = o.cw_tris + (size_t)pos * 3;
+      r[0] = make_float4(b.x - a.x, b.y - a.y, b.z - a.z, 0.0f);
+      r[1] = make_float4(c.x - a.x, c.y - a.y, c.z - a.z, 0.0f);
+      r[2] = a;  // v0 and the prim bits
+      ++pos;
+    } else {
+      if (sp + 2 > (int)kFatLeaf + 1) {
+        raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+        return pos;
+      }
+      const uint32_t y = cur & kIndexMask;
+      stack[sp++] = __ldg(node_meta + (size_t)y * 4 + 2);
+      stack[sp++] = __ldg(node_meta + (size_t)y * 4 + 1);
+    }
+  }
+  return pos;
+}
+
+// _power_of_two_scale_exponent (compressed_bounds_bvh.mojo:43-53): the
+// smallest 2^(e - 127) with 255 * 2^(e - 127) >= extent, e in [1, 254]
+__device__ __forceinline__ uint32_t cw_exponent(float extent) {
+  if (extent <= 0.0f) return 127u;
+  const uint32_t bits = __float_as_uint(extent / 255.0f);
+  uint32_t e = (bits >> 23) & 0xFFu;
+  if (bits & 0x007FFFFFu) e += 1u;
+  return e < 1u ? 1u : (e > 254u ? 254u : e);
+}
+
+__device__ __forceinline__ int cw_clamp255(float f) { return f >= 0.0f ? (f <= 255.0f ? (int)f : 255) : 0; }
+
+// _quantize_lower / _quantize_upper (:61-76)
+__device__ __forceinline__ uint32_t cw_qlo(float value, float start, float scale) {
+  int q = cw_clamp255(floorf((value - start) / scale));
+  if (__fmaf_rn((float)q, scale, start) > value && q > 0) q -= 1;
+  return (uint32_t)q;
+}
+
+__device__ __forceinline__ uint32_t cw_qhi(float value, float start, float scale) {
+  int q = cw_clamp255(ceilf((value - start) / scale));
+  if (__fmaf_rn((float)q, scale, start) < value && q < 255) q += 1;
+  return (uint32_t)q;
+}
+
+// _encode_cwbvh8_node (:84-325) from the eight lanes' boxes and metas
+// (internal data = segment-local child id, leaf count 1..3): node bounds are
+// the lanes' minimum / maximum in lane order (fmin / fmax as a < b ? a : b),
+// then p, per-axis exponents | imask << 24, child base, triangle base, the
+// lane bytes (internal: 001 | slot + 24; leaf: unary count | triangle offset;
+// empty: 0) and the 8-bit planes of every lane.
+__device__ void write_cw_node(float4* __restrict__ out, const Box (&bx)[8], const uint32_t (&meta)[8],
+                              uint32_t tri_base) {
+  float lx = FLT_MAX, ly = FLT_MAX, lz = FLT_MAX, hx = -FLT_MAX, hy = -FLT_MAX, hz = -FLT_MAX;
+  uint32_t child_base = 0, n_int = 0, imask = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    if (meta[j] == kEmpty) continue;
+    lx = lx < bx[j].mn.x ? lx : bx[j].mn.x;
+    ly = ly < bx[j].mn.y ? ly : bx[j].mn.y;
+    lz = lz < bx[j].mn.z ? lz : bx[j].mn.z;
+    hx = hx > bx[j].mx.x ? hx : bx[j].mx.x;
+    hy = hy > bx[j].mx.y ? hy : bx[j].mx.y;
+    hz = hz > bx[j].mx.z ? hz : bx[j].mx.z;
+    if ((meta[j] >> kCountShift) == 0) {
+      if (n_int == 0) child_base = meta[j] & kDataMask;
+      ++n_int;
+      imask |= 1u << j;
+    }
+  }
+  uint32_t ex = cw_exponent(hx - lx), ey = cw_exponent(hy - ly), ez = cw_exponent(hz - lz);
+  if (__fmaf_rn(255.0f, __uint_as_float(ex << 23), lx) < hx && ex < 254u) ++ex;
+  if (__fmaf_rn(255.0f, __uint_as_float(ey << 23), ly) < hy && ey < 254u) ++ey;
+  if (__fmaf_rn(255.0f, __uint_as_float(ez << 23), lz) < hz && ez < 254u) ++ez;
+  const float sx = __uint_as_float(ex << 23), sy = __uint_as_float(ey << 23), sz = __uint_as_float(ez << 23);
+  uint32_t m[2] = {0u, 0u}, q[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) q[k] = 0u;
+  uint32_t leaf_off = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int g = j >> 2, sh = (j & 3) * 8;
+    if (meta[j] == kEmpty) continue;
+    const uint32_t count = meta[j] >> kCountShift;
+    uint32_t byte;
+    if (count == 0) {
+      byte = 0x20u | (24u + (uint32_t)j);
+    } else {
+      byte = (((1u << count) - 1u) << 5) | leaf_off;
+      leaf_off += count;
+    }
+    m[g] |= byte << sh;
+    q[0 + g] |= cw_qlo(bx[j].mn.x, lx, sx) << sh;
+    q[2 + g] |= cw_qlo(bx[j].mn.y, ly, sy) << sh;
+    q[4 + g] |= cw_qlo(bx[j].mn.z, lz, sz) << sh;
+    q[6 + g] |= cw_qhi(bx[j].mx.x, lx, sx) << sh;
+    q[8 + g] |= cw_qhi(bx[j].mx.y, ly, sy) << sh;
+    q[10 + g] |= cw_qhi(bx[j].mx.z, lz, sz) << sh;
+  }
+  out[0] = make_float4(lx, ly, lz, __uint_as_float(ex | (ey << 8) | (ez << 16) | (imask << 24)));
+  out[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(m[0]),
+                       __uint_as_float(m[1]));
+  out[2] = make_float4(__uint_as_float(q[0]), __uint_as_float(q[1]), __uint_as_float(q[2]), __uint_as_float(q[3]));
+  out[3] = make_float4(__uint_as_float(q[4]), __uint_as_float(q[5]), __uint_as_float(q[6]), __uint_as_float(q[7]));
+  out[4] = make_float4(__uint_as_float(q[8]), __uint_as_float(q[9]), __uint_as_float(q[10]), __uint_as_float(q[11]));
+}
+
+// octant slots (spatial_slots, wide_collapse.mojo:457-521): perm[slot] =
+// candidate placed in that lane (-1 = empty).  Repeatedly the unassigned
+// candidate and free slot of lowest cost (centroid(candidate) -
+// centroid(parent)) . s(slot), s(slot) = (bit 2 ? -1 : 1, bit 1 ? -1 : 1,
+// bit 0 ? -1 : 1), are paired; candidates, then slots, are scanned in
+// ascending order and the first minimum below FLT_MAX is kept; with none
+// (NaN boxes) the first unassigned candidate takes the first free slot.
+__device__ void octant_slots(const Box& parent, const uint32_t* __restrict__ cands, int nc,
+                             const float* __restrict__ leaf_bounds, const uint32_t* __restrict__ leaf_ids,
+                             const float* __restrict__ node_bounds, int (&perm)[8]) {
+  const f3 pc = (parent.mn + parent.mx) * 0.5f;
+  f3 d[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    perm[k] = -1;
+    if (k < nc) {
+      const Box b = ref_bounds(cands[k], leaf_bounds, leaf_ids, node_bounds);
+      d[k] = (b.mn + b.mx) * 0.5f - pc;
+    }
+  }
+  uint32_t assigned = 0, occupied = 0;
+  for (int it = 0; it < nc; ++it) {
+    float best = FLT_MAX;
+    int bc = -1, bs = -1;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k >= nc || (assigned >> k & 1u)) continue;
+#pragma unroll
+      for (int sl = 0; sl < 8; ++sl) {
+        if (occupied >> sl & 1u) continue;
+        const float cost = (((sl & 4) ? -d[k].x : d[k].x) + ((sl & 2) ? -d[k].y : d[k].y)) + ((sl & 1) ? -d[k].z : d[k].z);
+        if (cost < best) {
+          best = cost;
+          bc = k;
+          bs = sl;
+        }
+      }
+    }
+    if (bc < 0) {
+      bc = __ffs(~assigned) - 1;
+      bs = __ffs(~occupied) - 1;
+    }
+    assigned |= 1u << bc;
+    occupied |= 1u << bs;
+#pragma unroll
+    for (int sl = 0; sl < 8; ++sl)
+      if (sl == bs) perm[sl] = bc;
+  }
+}
+
 template <int W>
 __device__ __forceinline__ void store_lane(float* node, int lane, const Box& b, uint32_t meta) {
   node[0 * W + lane] = b.mn.x;
@@ -216,24 +412,27 @@ __device__ __forceinline__ void store_lane(float* node, int lane, const Box& b, 
   node[6 * W + lane] = __uint_as_float(meta);
 }
 
-template <int W>
-__device__ __forceinline__ void store_empty(float* node, int lane) {
+__device__ __forceinline__ Box empty_box() {
   Box b;
   b.mn = mk(FLT_MAX, FLT_MAX, FLT_MAX);
   b.mx = mk(-FLT_MAX, -FLT_MAX, -FLT_MAX);
-  store_lane<W>(node, lane, b, kEmpty);
+  return b;
 }
 
-template <int W>
+// CW = the CWBVH8 build (W = 8, octant slots, compressed nodes and triangle
+// records instead of wide nodes and leaf blocks)
+template <int W, bool CW>
 __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const uint32_t* __restrict__ node_meta,
                                                         const uint32_t* __restrict__ node_leaf_counts,
                                                         const float* __restrict__ leaf_bounds,
                                                         const uint32_t* __restrict__ leaf_ids,
                                                         const float* __restrict__ node_bounds,
                                                         const float4* __restrict__ tris,
+                                                        const uint32_t* __restrict__ seg_offsets,
                                                         const uint32_t* __restrict__ node_offsets,
                                                         const uint32_t* __restrict__ leaf_offsets, uint32_t cap,
                                                         uint32_t max_leaf, Work wk, Out o) {
+  static_assert(!CW || W == 8, "CWBVH8 nodes are 8 wide");
   // node and leaf-block totals never exceed the triangle count; more means
   // the binary tree is corrupt
   uint32_t total = node_offsets[n_seg];
@@ -250,59 +449,93 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
         return;
       }
     }
-    const uint32_t x = wk.task_ref[I], B = wk.task_leaf[I], s = wk.task_seg[I];
+    const uint32_t x = wk.task_ref[I], B = wk.task_leaf[I], s = wk.task_seg[I], D = wk.task_desc[I];
+    const uint32_t T = CW ? wk.task_tri[I] : 0u;
     const uint32_t nb = node_offsets[s], lb = leaf_offsets[s];
-    float* node = o.nodes + (size_t)I * kFields * W;
+    const uint32_t t_seg = CW ? seg_offsets[s] : 0u;
+    float* node = CW ? nullptr : o.nodes + (size_t)I * kFields * W;
+    Box lane_box[W];
+    uint32_t lane_meta[W];
     const uint32_t xc = ref_count(x, node_leaf_counts);
     if (terminal(x, xc, max_leaf)) {  // a segment of at most max_leaf triangles: one node, one leaf block
       if (B >= cap) {
         raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
         continue;
       }
-      write_leaf_block<W>(x, B, node_meta, leaf_ids, tris, o, wk.status);
-      store_lane<W>(node, 0, ref_bounds(x, leaf_bounds, leaf_ids, node_bounds), pack_meta(B - lb, xc));
-      for (int j = 1; j < W; ++j) store_empty<W>(node, j);
-      continue;
-    }
-    const uint32_t xi = x & kIndexMask;
-    const uint32_t info = wk.cinfo[xi];
-    const int nc = (int)(info & 0xFF);
-    const uint32_t mask = info >> 8;
-    uint32_t leaf_next = B;
-    for (int k = 0; k < nc; ++k) {
-      if (!(mask & (1u << k))) continue;
-      if (leaf_next >= cap) {
-        raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
-        break;
+      if constexpr (CW) write_cw_tris(x, T, cap, node_meta, tris, o, wk.status);
+      else write_leaf_block<W>(x, B, node_meta, leaf_ids, tris, o, wk.status);
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        lane_box[j] = j == 0 ? ref_bounds(x, leaf_bounds, leaf_ids, node_bounds) : empty_box();
+        lane_meta[j] = j == 0 ? pack_meta(B - lb, xc) : kEmpty;
       }
-      write_leaf_block<W>(wk.cands[(size_t)xi * W + k], leaf_next, node_meta, leaf_ids, tris, o, wk.status);
-      ++leaf_next;
-    }
-    uint32_t own = B, child = I + 1, child_leaf = leaf_next;
-    for (int k = 0; k < W; ++k) {
-      if (k >= nc) {
-        store_empty<W>(node, k);
-        continue;
-      }
-      const uint32_t c = wk.cands[(size_t)xi * W + k];
-      const Box bx = ref_bounds(c, leaf_bounds, leaf_ids, node_bounds);
-      if (mask & (1u << k)) {
-        store_lane<W>(node, k, bx, pack_meta(own - lb, ref_count(c, node_leaf_counts)));
-        ++own;
+    } else {
+      const uint32_t xi = x & kIndexMask;
+      const uint32_t info = wk.cinfo[xi];
+      const int nc = (int)(info & 0xFF);
+      const uint32_t mask = info >> 8;
+      const uint32_t* cands = wk.cands + (size_t)xi * W;
+      int perm[W];
+      if constexpr (CW) {
+        octant_slots(ref_bounds(x, leaf_bounds, leaf_ids, node_bounds), cands, nc, leaf_bounds, leaf_ids,
+                     node_bounds, reinterpret_cast<int(&)[8]>(perm));
       } else {
-        const uint32_t ci = c & kIndexMask;
-        store_lane<W>(node, k, bx, pack_meta(child - nb, 0));
-        if (child < total) {
-          wk.task_ref[child] = c;
-          wk.task_leaf[child] = child_leaf;
-          wk.task_seg[child] = s;
-          st_release_gpu(wk.ready + child, 1u);
-        } else {
-          raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
-        }
-        child += wk.nw[ci];
-        child_leaf += wk.nl[ci];
+#pragma unroll
+        for (int j = 0; j < W; ++j) perm[j] = j < nc ? j : -1;
       }
+      const uint32_t n_leaf = __popc(mask & ((1u << nc) - 1u)), n_int = (uint32_t)nc - n_leaf;
+      uint32_t own_tris = 0;
+      if constexpr (CW) {
+        for (int k = 0; k < nc; ++k)
+          if (mask & (1u << k)) own_tris += ref_count(cands[k], node_leaf_counts);
+      }
+      uint32_t own = B, own_t = T, child = D, desc = D + n_int, child_leaf = B + n_leaf, child_t = T + own_tris;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const int k = perm[j];
+        if (k < 0) {
+          lane_box[j] = empty_box();
+          lane_meta[j] = kEmpty;
+          continue;
+        }
+        const uint32_t c = cands[k];
+        lane_box[j] = ref_bounds(c, leaf_bounds, leaf_ids, node_bounds);
+        const uint32_t cnt = ref_count(c, node_leaf_counts);
+        if (mask & (1u << k)) {
+          if (own >= cap) {
+            raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
+            lane_meta[j] = kEmpty;
+            continue;
+          }
+          if constexpr (CW) own_t = write_cw_tris(c, own_t, cap, node_meta, tris, o, wk.status);
+          else write_leaf_block<W>(c, own, node_meta, leaf_ids, tris, o, wk.status);
+          lane_meta[j] = pack_meta(own - lb, cnt);
+          ++own;
+        } else {
+          const uint32_t ci = c & kIndexMask;
+          lane_meta[j] = pack_meta(child - nb, 0);
+          if (child < total && desc <= total) {
+            wk.task_ref[child] = c;
+            wk.task_leaf[child] = child_leaf;
+            wk.task_seg[child] = s;
+            wk.task_desc[child] = desc;
+            if constexpr (CW) wk.task_tri[child] = child_t;
+            st_release_gpu(wk.ready + child, 1u);
+          } else {
+            raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
+          }
+          ++child;
+          desc += wk.nw[ci] - 1u;
+          child_leaf += wk.nl[ci];
+          child_t += cnt;
+        }
+      }
+    }
+    if constexpr (CW) {
+      if constexpr (W == 8) write_cw_node(o.cw_nodes + (size_t)I * 5, lane_box, lane_meta, T - t_seg);
+    } else {
+#pragma unroll
+      for (int j = 0; j < W; ++j) store_lane<W>(node, j, lane_box[j], lane_meta[j]);
     }
   }
 }
@@ -381,10 +614,13 @@ __global__ void __launch_bounds__(trav::kTraceBlock) wide_camera_kernel(
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Plan {
-  size_t flags, ready, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, zero_bytes, total;
+  size_t flags, ready, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, task_desc, task_tri, leaf_offsets,
+      zero_bytes, total;
 };
 
-inline Plan make_plan(uint32_t n, uint32_t width) {
+// cw_segments > 0: the CWBVH8 build, which also keeps the per-segment leaf
+// offsets ([S+1]) in the workspace
+inline Plan make_plan(uint32_t n, uint32_t width, uint32_t cw_segments = 0) {
   Plan p;
   const size_t cap = std::max<uint32_t>(n, 1);
   size_t o = 256;  // status word
@@ -407,13 +643,19 @@ inline Plan make_plan(uint32_t n, uint32_t width) {
   o = a256(o + cap * 4);
   p.task_seg = o;
   o = a256(o + cap * 4);
+  p.task_desc = o;
+  o = a256(o + cap * 4);
+  p.task_tri = o;
+  if (cw_segments) o = a256(o + cap * 4);
+  p.leaf_offsets = o;
+  if (cw_segments) o = a256(o + ((size_t)cw_segments + 1) * 4);
   p.total = o;
   return p;
 }
 
-template <int W>
-cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const Plan& p, uint32_t max_leaf,
-                  cudaStream_t st) {
+template <int W, bool CW>
+cudaError_t build(const BajoLbvh* b, uint32_t* node_offsets, uint32_t* leaf_offsets, const Out& o,
+                  unsigned char* ws, const Plan& p, uint32_t max_leaf, cudaStream_t st) {
   Work wk;
   wk.status = (uint32_t*)ws;
   wk.flags = (uint32_t*)(ws + p.flags);
@@ -425,6 +667,8 @@ cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const 
   wk.task_ref = (uint32_t*)(ws + p.task_ref);
   wk.task_leaf = (uint32_t*)(ws + p.task_leaf);
   wk.task_seg = (uint32_t*)(ws + p.task_seg);
+  wk.task_desc = (uint32_t*)(ws + p.task_desc);
+  wk.task_tri = (uint32_t*)(ws + p.task_tri);
   cudaError_t e = cudaMemsetAsync(ws, 0, p.zero_bytes, st);
   if (e != cudaSuccess) return e;
   const uint32_t n = b->n_leaves;
@@ -435,21 +679,20 @@ cudaError_t build(const BajoLbvh* b, BajoWideBvh* out, unsigned char* ws, const 
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   offsets_kernel<<<1, 1024, 0, st>>>(b->n_segments, b->seg_offsets, b->roots, b->node_leaf_counts, max_leaf, wk,
-                                     std::max<uint32_t>(n, 1), out->node_offsets, out->leaf_offsets);
+                                     std::max<uint32_t>(n, 1), node_offsets, leaf_offsets);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (n == 0) return cudaSuccess;
   // every block resident, so a task's producer always runs
   int per_sm = 0;
-  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assign_kernel<W>, kBlock, 0)) != cudaSuccess)
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, assign_kernel<W, CW>, kBlock, 0)) != cudaSuccess)
     return e;
   uint32_t grid = (uint32_t)std::max(1, per_sm) * (uint32_t)sm_count();
   const uint32_t need = (n + kBlock - 1) / kBlock;
   if (grid > need) grid = need;
-  Out o{out->nodes, out->leaf_indices, out->leaf_tris, out->leaf_sorted};
-  assign_kernel<W><<<grid, kBlock, 0, st>>>(b->n_segments, b->node_meta, b->node_leaf_counts, b->leaf_bounds,
-                                           b->leaf_ids, b->node_bounds,
-                                           reinterpret_cast<const float4*>(b->leaf_tris), out->node_offsets,
-                                           out->leaf_offsets, std::max<uint32_t>(n, 1), max_leaf, wk, o);
+  assign_kernel<W, CW><<<grid, kBlock, 0, st>>>(b->n_segments, b->node_meta, b->node_leaf_counts, b->leaf_bounds,
+                                               b->leaf_ids, b->node_bounds,
+                                               reinterpret_cast<const float4*>(b->leaf_tris), b->seg_offsets,
+                                               node_offsets, leaf_offsets, std::max<uint32_t>(n, 1), max_leaf, wk, o);
   return cudaGetLastError();
 }
 
@@ -513,9 +756,50 @@ int32_t bajo_wide_build(const BajoLbvh* b, BajoWideBvh* out, void* ws, size_t ws
   cudaStream_t st = (cudaStream_t)stream;
   const uint32_t max_leaf = out->max_leaf ? out->max_leaf : kFatLeaf;
   if (max_leaf > kFatLeaf) return BAJO_ERR_INVALID_ARGUMENT;
-  const cudaError_t e = out->width == 4 ? build<4>(b, out, (unsigned char*)ws, p, max_leaf, st)
-                                        : build<8>(b, out, (unsigned char*)ws, p, max_leaf, st);
+  const Out o{out->nodes, out->leaf_indices, out->leaf_tris, out->leaf_sorted, nullptr, nullptr};
+  unsigned char* w = (unsigned char*)ws;
+  const cudaError_t e = out->width == 4
+                            ? build<4, false>(b, out->node_offsets, out->leaf_offsets, o, w, p, max_leaf, st)
+                            : build<8, false>(b, out->node_offsets, out->leaf_offsets, o, w, p, max_leaf, st);
   return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_cwbvh8_sizes(uint32_t n_tris, uint32_t n_segments, BajoCwbvh8Sizes* s) {
+  if (!s || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  const size_t cap = std::max<uint32_t>(n_tris, 1);
+  s->node_offsets = (size_t)(n_segments + 1) * 4;
+  s->nodes = cap * BAJO_CWBVH8_NODE_WORDS * 4;
+  s->triangles = cap * BAJO_CWBVH8_TRI_WORDS * 4;
+  s->workspace = bajo::wide::make_plan(n_tris, 8, n_segments).total;
+  return BAJO_OK;
+}
+
+int32_t bajo_cwbvh8_build(const BajoLbvh* b, BajoCwbvh8* out, void* ws, size_t ws_bytes, void* stream) {
+  using namespace bajo::wide;
+  if (!b || !out || !ws || b->n_segments == 0 || !out->node_offsets || !out->nodes || !out->triangles ||
+      !b->seg_offsets || !b->roots || !b->node_meta || !b->node_leaf_counts || !b->leaf_parent || !b->leaf_bounds ||
+      !b->leaf_ids || !b->node_bounds || !b->leaf_tris)
+    return BAJO_ERR_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(out->nodes) | reinterpret_cast<uintptr_t>(out->triangles)) & 15u)
+    return BAJO_ERR_INVALID_ARGUMENT;
+  const Plan p = make_plan(b->n_leaves, 8, b->n_segments);
+  if (ws_bytes < p.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
+  out->n_segments = b->n_segments;
+  out->n_tris = b->n_leaves;
+  unsigned char* w = (unsigned char*)ws;
+  const Out o{nullptr, nullptr, nullptr, nullptr, reinterpret_cast<float4*>(out->nodes),
+              reinterpret_cast<float4*>(out->triangles)};
+  const cudaError_t e = build<8, true>(b, out->node_offsets, (uint32_t*)(w + p.leaf_offsets), o, w, p,
+                                       BAJO_CWBVH8_MAX_LEAF, (cudaStream_t)stream);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_cwbvh8_count(const BajoCwbvh8* c, void* stream, uint32_t* n_nodes) {
+  if (!c || !c->node_offsets || !n_nodes || c->n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  if (cudaStreamSynchronize((cudaStream_t)stream) != cudaSuccess) return BAJO_ERR_CUDA;
+  if (cudaMemcpy(n_nodes, c->node_offsets + c->n_segments, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return BAJO_ERR_CUDA;
+  return BAJO_OK;
 }
 
 int32_t bajo_wide_counts(const BajoWideBvh* w, void* stream, uint32_t* n_nodes, uint32_t* n_leaf_blocks) {

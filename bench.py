@@ -55,7 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--case", default=None,
-                   choices=["sort", "build", "trace", "wide", "tune", "render", "batched", "guided", "guided_pass"],
+                   choices=["sort", "build", "trace", "wide", "cwbvh8", "tune", "render", "batched", "guided",
+                            "guided_pass"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -796,6 +797,23 @@ def run_case(args):
                     "binary_trace_ms": round(ms_bin, 4),
                     "binary_mrays_s": round(WIDTH * HEIGHT / ms_bin / 1e3, 2),
                     "wide_nodes_per_ray": round(s[0], 3), "tris_per_ray": round(s[1], 3), "status": w.status()})
+    elif args.case == "cwbvh8":
+        from bajo_b200 import scenes, wide
+        verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
+        tree = bvh.build_triangle_bvh(verts)
+        cw = wide.build_cwbvh8(tree)
+        ms_build = timed(lambda: cw.build(read_count=False))
+        cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+        hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
+        ms_cw = timed(lambda: cw.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
+        ms_any = timed(lambda: cw.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, any_hit=True))
+        ms_bin = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, tri_mode=0))
+        out.update({"cwbvh8_nodes": cw.n_nodes, "build_ms": round(ms_build, 5),
+                    "build_mtri_s": round(n / ms_build / 1e3, 2),
+                    "closest_ms": round(ms_cw, 4), "closest_mrays_s": round(WIDTH * HEIGHT / ms_cw / 1e3, 2),
+                    "any_ms": round(ms_any, 4), "any_mrays_s": round(WIDTH * HEIGHT / ms_any / 1e3, 2),
+                    "binary_mt_ms": round(ms_bin, 4), "binary_mt_mrays_s": round(WIDTH * HEIGHT / ms_bin / 1e3, 2),
+                    "status": cw.status()})
     elif args.case in ("build", "trace"):
         from bajo_b200 import scenes
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()

@@ -307,6 +307,73 @@ int32_t bajo_trace_wide_camera(const BajoWideBvh* wide, uint32_t n_nodes, uint32
                                uint32_t* d_prim, uint32_t* d_status, uint32_t* d_stats, void* stream);
 
 /* ======================================================================== */
+/* CWBVH8: compressed 8-wide BVH (Ylitie, Karras, Laine, HPG 2017)           */
+/* ======================================================================== */
+/* Layouts of the reference (bajo/bvh/gpu/compressed_bounds_bvh.mojo:25-39):
+ * node = 20 words (80 B): [0..2] p = the node's minimum corner (f32),
+ * [3] exponents x | y << 8 | z << 16 | imask << 24 (a lane's box is
+ * p + q * 2^(e - 127)), [4] first internal child and [5] first triangle
+ * (segment-local), [6..7] one byte per lane (internal child: 001 | slot + 24,
+ * leaf: unary triangle count << 5 | triangle offset, empty: 0), [8 + 2 * plane
+ * + group] the lanes' 8-bit planes (plane lo x, lo y, lo z, hi x, hi y, hi z;
+ * group = lanes 0..3 / 4..7).  A node's internal children are consecutive
+ * nodes in lane order.  Triangle = 12 words (48 B): e1 xyz, 0, e2 xyz, 0,
+ * v0 xyz, segment-local prim (u32 bits); segment s's triangles start at the
+ * binary tree's seg_offsets[s]. */
+#define BAJO_CWBVH8_NODE_WORDS 20
+#define BAJO_CWBVH8_TRI_WORDS 12
+#define BAJO_CWBVH8_MAX_LEAF 3u /* triangles per leaf lane (CWBVH_MAX_LEAF_SIZE) */
+
+typedef struct BajoCwbvh8 {
+  uint32_t n_segments;    /* set by bajo_cwbvh8_build                      */
+  uint32_t n_tris;        /* set by bajo_cwbvh8_build: triangle records   */
+  uint32_t* node_offsets; /* [S+1] first node of each segment              */
+  float* nodes;           /* [node][20], 16-byte aligned                   */
+  float* triangles;       /* [triangle][12], 16-byte aligned               */
+} BajoCwbvh8;
+
+typedef struct BajoCwbvh8Sizes {
+  size_t node_offsets, nodes, triangles, workspace;
+} BajoCwbvh8Sizes;
+
+int32_t bajo_cwbvh8_sizes(uint32_t n_tris, uint32_t n_segments, BajoCwbvh8Sizes* sizes);
+
+/* Replaces build_triangle_blas_set[8, 4, layout = CWBVH8]
+ * (bajo/bvh/gpu/triangle_bvh.mojo:366-485): the W = 8 collapse with leaves of
+ * at most three triangles and octant slots (enqueue_segmented_wide_build with
+ * fat_leaves and spatial_slots, segmented_build.mojo:89;
+ * wide_collapse.mojo:457-521), encoded (encode_segmented_cwbvh8_nodes_kernel,
+ * compressed_bounds_bvh.mojo:328) and packed
+ * (pack_segmented_cwbvh_triangles_kernel, :372) for every segment of a built
+ * binary tree, in one pass over the wide nodes.  Node ids and triangle ranges
+ * are deterministic (the reference takes both from atomic counters).  The
+ * build status (bajo_workspace_status) is BAJO_STATUS_BAD_TOPOLOGY for a
+ * corrupt binary tree and BAJO_STATUS_WIDE_TIMEOUT for a task wait that gave
+ * up. */
+int32_t bajo_cwbvh8_build(const BajoLbvh* bvh, BajoCwbvh8* out, void* d_workspace, size_t workspace_bytes,
+                          void* stream);
+
+/* Synchronises `stream` and reads the total compressed nodes. */
+int32_t bajo_cwbvh8_count(const BajoCwbvh8* cwbvh, void* stream, uint32_t* n_nodes);
+
+/* Closest hits (any_hit = 0) or occlusion (any_hit = 1) over segment 0's tree
+ * (trace_cwbvh8_triangles, triangle_bvh.mojo:1010-1104; node decode
+ * _intersect_cwbvh8_node_tasks, compressed_bounds_bvh.mojo:469-576; record
+ * test _intersect_cwbvh_triangle, triangle_bvh.mojo:962-1007, the
+ * determinant-scaled Moller-Trumbore of intersect.mojo:462-505).  Rays and
+ * outputs as bajo_trace_rays / bajo_trace_camera; an occluded ray reports
+ * t = 0 and prim 0xFFFFFFFF (Hit.shadow_hit, bajo/bvh/types.mojo:46).
+ * n_nodes (bajo_cwbvh8_count) bounds node references and visits;
+ * *d_status gets BAJO_STATUS_BAD_TOPOLOGY for an out-of-range node or
+ * triangle and BAJO_STATUS_STACK_OVERFLOW past 64 stacked node groups. */
+int32_t bajo_trace_cwbvh8_rays(const BajoCwbvh8* cwbvh, uint32_t n_nodes, const float* d_rays, uint32_t n_rays,
+                               int32_t any_hit, float* d_hits8, float* d_t, uint32_t* d_prim, uint32_t* d_status,
+                               void* stream);
+int32_t bajo_trace_cwbvh8_camera(const BajoCwbvh8* cwbvh, uint32_t n_nodes, const float* d_cameras,
+                                 uint32_t n_rays, uint32_t width, uint32_t height, int32_t any_hit, float* d_hits8,
+                                 float* d_t, uint32_t* d_prim, uint32_t* d_status, void* stream);
+
+/* ======================================================================== */
 /* Wavefront path tracing over one triangle LBVH                             */
 /* ======================================================================== */
 /* Render algorithms (RENDER, bajo/rt/types.mojo:53-59). */

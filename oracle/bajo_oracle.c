@@ -797,6 +797,168 @@ void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays, uint
 }
 
 /* ------------------------------------------------------------------------- */
+/* CWBVH8 traversal                                                           */
+/* ------------------------------------------------------------------------- */
+/* fmax / fmin of bajo/core/utils.mojo:60-70: a > b ? a : b, a < b ? a : b */
+static inline float sel_max(float a, float b) { return a > b ? a : b; }
+static inline float sel_min(float a, float b) { return a < b ? a : b; }
+
+/* intersect_ray_tri_edges_scaled (bajo/core/intersect.mojo:462-505):
+ * determinant-scaled Moller-Trumbore; the candidate passes when
+ * |det| > 1e-8, 0 <= u', v', u' + v' <= |det| and t_min|det| < t' < t_max|det| */
+static inline int tri_scaled(v3 o, v3 d, v3 v0, v3 e1, v3 e2, float tmax, float tmin, float* ad, float* ts,
+                             float* us, float* vs) {
+  v3 p = v3cross(d, e2);
+  float det = v3dot(e1, p);
+  int pos = det >= 0.0f;
+  float a = pos ? det : -det;
+  v3 tv = v3sub(o, v0);
+  float un = v3dot(tv, p);
+  v3 q = v3cross(tv, e1);
+  float vn = v3dot(d, q), tn = v3dot(e2, q);
+  float u = pos ? un : -un, v = pos ? vn : -vn, t = pos ? tn : -tn;
+  *ad = a; *ts = t; *us = u; *vs = v;
+  return a > 1e-8f && u >= 0.0f && u <= a && v >= 0.0f && (u + v) <= a && t > tmin * a && t < tmax * a;
+}
+
+static inline float cw_exp_scale(uint32_t e) {
+  uint32_t bits = (e & 0xFFu) << 23;
+  float f;
+  memcpy(&f, &bits, 4);
+  return f;
+}
+
+/* trace_cwbvh8_triangles (bajo/bvh/gpu/triangle_bvh.mojo:1010-1104) with the
+ * node decode of _intersect_cwbvh8_node_tasks (compressed_bounds_bvh.mojo:
+ * 469-576) and the record test of _intersect_cwbvh_triangle
+ * (triangle_bvh.mojo:962-1007).  Node groups hold hit internal children in
+ * bits 24..31 (slot + 24, slot XOR the inverted ray octant) and the node's
+ * imask in bits 0..7; triangle groups hold hit triangles in bits 0..23,
+ * relative to the node's triangle base; both are consumed highest bit first.
+ * Any-hit returns t = 0 and prim = EMPTY on the first triangle hit.  *err
+ * records an out-of-range node or triangle, a revisit beyond n_nodes or a full
+ * stack (64 groups); the ray then stops. */
+static bo_hit cwbvh8_one(const float* nodes, const float* tris, uint32_t n_nodes, uint32_t n_tris,
+                         const bo_ray* r, int any, uint32_t* err) {
+  bo_hit h = miss_hit(r->tmax);
+  if (n_nodes == 0) return h;
+  uint32_t sb[64], sm[64];
+  int sp = 0;
+  uint32_t sign = (r->d.x < 0.0f ? 4u : 0u) | (r->d.y < 0.0f ? 2u : 0u) | (r->d.z < 0.0f ? 1u : 0u);
+  uint32_t oi = 7u - sign;
+  uint32_t nbase = 0, nmask = 1u << 31, tbase = 0, tmask = 0, visits = 0;
+  for (;;) {
+    if (nmask > 0x00FFFFFFu) {
+      uint32_t gm = nmask;
+      int bit = 31 - __builtin_clz(nmask);
+      nmask &= ~(1u << bit);
+      if (nmask > 0x00FFFFFFu) {
+        if (sp >= 64) { *err |= 2u; break; }
+        sb[sp] = nbase;
+        sm[sp] = nmask;
+        ++sp;
+      }
+      uint32_t slot = ((uint32_t)bit - 24u) ^ oi;
+      uint32_t rel = (uint32_t)__builtin_popcount(gm & ((1u << slot) - 1u));
+      uint32_t ni = nbase + rel;
+      if (ni >= n_nodes || ++visits > n_nodes) { *err |= 1u; break; }
+      const float* nd = nodes + (size_t)ni * 20;
+      const uint32_t* w = (const uint32_t*)nd;
+      float px = nd[0], py = nd[1], pz = nd[2];
+      uint32_t ei = w[3];
+      float sx = cw_exp_scale(ei), sy = cw_exp_scale(ei >> 8), sz = cw_exp_scale(ei >> 16);
+      uint32_t imask = ei >> 24;
+      float tlim = any ? r->tmax : h.t;
+      float idx = sx * r->rcp.x, idy = sy * r->rcp.y, idz = sz * r->rcp.z;
+      float ox = (px - r->o.x) * r->rcp.x, oy = (py - r->o.y) * r->rcp.y, oz = (pz - r->o.z) * r->rcp.z;
+      uint32_t hm = 0;
+      for (int j = 0; j < 8; ++j) {
+        int g = j >> 2, sh = (j & 3) * 8;
+        float qlx = (float)((w[8 + 0 + g] >> sh) & 0xFFu), qly = (float)((w[8 + 2 + g] >> sh) & 0xFFu);
+        float qlz = (float)((w[8 + 4 + g] >> sh) & 0xFFu), qhx = (float)((w[8 + 6 + g] >> sh) & 0xFFu);
+        float qhy = (float)((w[8 + 8 + g] >> sh) & 0xFFu), qhz = (float)((w[8 + 10 + g] >> sh) & 0xFFu);
+        float nx = r->d.x < 0.0f ? qhx : qlx, fx = r->d.x < 0.0f ? qlx : qhx;
+        float ny = r->d.y < 0.0f ? qhy : qly, fy = r->d.y < 0.0f ? qly : qhy;
+        float nz = r->d.z < 0.0f ? qhz : qlz, fz = r->d.z < 0.0f ? qlz : qhz;
+        float tnx = fmaf(nx, idx, ox), tny = fmaf(ny, idy, oy), tnz = fmaf(nz, idz, oz);
+        float tfx = fmaf(fx, idx, ox), tfy = fmaf(fy, idy, oy), tfz = fmaf(fz, idz, oz);
+        float tn = sel_max(sel_max(tnx, tny), sel_max(tnz, 0.0f));
+        float tf = sel_min(sel_min(tfx, tfy), sel_min(tfz, tlim));
+        uint32_t byte = (w[6 + g] >> sh) & 0xFFu;
+        if (byte != 0 && tn <= tf) {
+          uint32_t bi = byte & 0x1Fu;
+          if (imask >> j & 1u) bi ^= oi;
+          hm |= (byte >> 5) << bi;
+        }
+      }
+      nbase = w[4];
+      nmask = (hm & 0xFF000000u) | imask;
+      tbase = w[5];
+      tmask = hm & 0x00FFFFFFu;
+    } else {
+      tbase = nbase;
+      tmask = nmask;
+      nmask = 0;
+    }
+    while (tmask != 0) {
+      int bit = 31 - __builtin_clz(tmask);
+      tmask &= ~(1u << bit);
+      uint32_t ti = tbase + (uint32_t)bit;
+      if (ti >= n_tris) { *err |= 1u; return h; }
+      const float* tr = tris + (size_t)ti * 12;
+      v3 e1 = load3(tr), e2 = load3(tr + 4), v0 = load3(tr + 8);
+      float ad, ts, us, vs;
+      if (!tri_scaled(r->o, r->d, v0, e1, e2, h.t, r->tmin, &ad, &ts, &us, &vs)) continue;
+      if (any) {
+        h = miss_hit(0.0f);
+        return h;
+      }
+      float inv = 1.0f / ad;
+      h.t = ts * inv;
+      h.u = us * inv;
+      h.v = vs * inv;
+      memcpy(&h.prim, &tr[11], 4);
+      h.n = v3normalize(v3cross(e1, e2));
+    }
+    if (nmask <= 0x00FFFFFFu) {
+      if (sp == 0) break;
+      --sp;
+      nbase = sb[sp];
+      nmask = sm[sp];
+    }
+  }
+  return h;
+}
+
+typedef struct {
+  const float* nodes;
+  const float* tris;
+  uint32_t n_nodes, n_tris;
+  const float* rays;
+  uint32_t n;
+  int any;
+  float* hits;
+  uint32_t* err;
+} cw_ctx;
+
+static void cw_range(void* p, uint32_t b, uint32_t e) {
+  cw_ctx* c = (cw_ctx*)p;
+  for (uint32_t i = b; i < e; ++i) {
+    bo_ray r = make_ray(c->rays, c->n, i);
+    uint32_t err = 0;
+    bo_hit h = cwbvh8_one(c->nodes, c->tris, c->n_nodes, c->n_tris, &r, c->any, &err);
+    store_hit(c->hits, i, &h);
+    if (c->err) c->err[i] = err;
+  }
+}
+
+void bo_trace_cwbvh8(const float* nodes, uint32_t n_nodes, const float* tris, uint32_t n_tris, const float* rays,
+                     uint32_t n, int any_hit, float* hits8, uint32_t* err, uint32_t n_threads) {
+  cw_ctx c = {nodes, tris, n_nodes, n_tris, rays, n, any_hit, hits8, err};
+  bo_parallel_for(n, n_threads, 1024, cw_range, &c);
+}
+
+/* ------------------------------------------------------------------------- */
 /* reference CPU builder (timed CPU baseline)                                 */
 /* ------------------------------------------------------------------------- */
 typedef struct { uint32_t code, item; } bo_mitem;

@@ -179,6 +179,19 @@ void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, uint32_t
                    uint32_t* leaf_indices, float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets,
                    uint32_t* leaf_offsets);
 
+/* ---- CWBVH8 (bajo_oracle_wide.c, bajo_oracle.c) -------------------------- */
+/* W = 8 collapse with octant slots and leaves of <= 3 triangles, encoded as
+ * 80-byte nodes (20 words, `cw_nodes` sized for n_leaves nodes) and 48-byte
+ * triangle records (12 words, n_leaves records); `wide_nodes` (n_leaves x 56
+ * words) receives the uncompressed wide nodes; node_offsets [S+1]. */
+void bo_cwbvh8_build(const BoLbvh* b, const float* verts, float* wide_nodes, float* cw_nodes, float* cw_tris,
+                     uint32_t* node_offsets);
+/* closest (any_hit = 0) or any hit of SoA rays over one CWBVH8 tree rooted at
+ * node 0; hits8 as bo_trace_bvh2; err (may be NULL) per ray: bit 0 = node or
+ * triangle out of range / too many visits, bit 1 = stack overflow */
+void bo_trace_cwbvh8(const float* nodes, uint32_t n_nodes, const float* tris, uint32_t n_tris, const float* rays,
+                     uint32_t n, int any_hit, float* hits8, uint32_t* err, uint32_t n_threads);
+
 /* ---- path-guiding network (bajo_oracle_mlp.c), FP64 ---------------------- */
 /* Parameters as doubles in the library's layout: W1[64x64] b1[64] W2 b2 W3 b3
  * W4[32x64] b4[32] (rows 20..31 of the output layer unused). */

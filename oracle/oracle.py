@@ -94,6 +94,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
         "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
+        "bo_cwbvh8_build": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P]),
+        "bo_trace_cwbvh8": (None, [_P, _U32, _P, _U32, _P, _U32, ctypes.c_int, _P, _P, _U32]),
         "bo_mlp_param_count": (_U32, []),
         "bo_mlp_encode": (None, [_P, _P, _P, _P]),
         "bo_mlp_forward_f64": (None, [_P, _P, _P, _P, _U32, _P]),
@@ -473,7 +475,8 @@ class OracleWide:
 
 
 def wide_build(bvh: OracleLbvh, width: int, max_leaf: int = 4) -> OracleWide:
-    """Sequential BVH2 -> W-wide collapse with fat leaves, pre-order ids."""
+    """Sequential BVH2 -> W-wide collapse with fat leaves; a node's internal
+    children take consecutive ids, its leaf blocks consecutive blocks."""
     n = max(bvh.n_leaves, 1)
     S = bvh.seg_offsets.size - 1
     nodes = np.zeros(n * 7 * width, np.float32)
@@ -487,6 +490,49 @@ def wide_build(bvh: OracleLbvh, width: int, max_leaf: int = 4) -> OracleWide:
                         _ptr(no), _ptr(lo))
     nn, nb = int(no[-1]), int(lo[-1])
     return OracleWide(width, nodes[:nn * 7 * width], li[:nb * width], lt[:nb * 12 * width], ls[:nb * width], no, lo)
+
+
+# ---- CWBVH8 -------------------------------------------------------------------
+CW_NODE_WORDS = 20
+CW_TRI_WORDS = 12
+
+
+@dataclass
+class OracleCwbvh8:
+    wide_nodes: np.ndarray    # [n_nodes * 56] f32: the W = 8 octant-slot collapse (meta as bits)
+    nodes: np.ndarray         # [n_nodes * 20] f32: 80-byte compressed nodes
+    triangles: np.ndarray     # [n_tris * 12] f32: e1, 0, e2, 0, v0, prim bits
+    node_offsets: np.ndarray  # [S+1]
+
+
+def cwbvh8_build(bvh: OracleLbvh) -> OracleCwbvh8:
+    """W = 8 collapse with octant slots and leaves of at most 3 triangles,
+    encoded as CWBVH8 nodes and triangle records."""
+    n = max(bvh.n_leaves, 1)
+    S = bvh.seg_offsets.size - 1
+    wide = np.zeros(n * 56, np.float32)
+    nodes = np.zeros(n * CW_NODE_WORDS, np.float32)
+    tris = np.zeros(n * CW_TRI_WORDS, np.float32)
+    no = np.zeros(S + 1, np.uint32)
+    s = bvh.struct()
+    lib().bo_cwbvh8_build(ctypes.byref(s), _ptr(bvh.verts), _ptr(wide), _ptr(nodes), _ptr(tris), _ptr(no))
+    nn = int(no[-1])
+    return OracleCwbvh8(wide[:nn * 56], nodes[:nn * CW_NODE_WORDS], tris[:bvh.n_leaves * CW_TRI_WORDS], no)
+
+
+def trace_cwbvh8(cw: OracleCwbvh8, rays: np.ndarray, any_hit: bool = False, threads: int = 0,
+                 with_errors: bool = False):
+    """Closest or any hit of SoA rays [8][n] over segment 0's CWBVH8 tree:
+    hits8 [n * 8] f32 (u, v, prim bits, inst bits, normal, t)."""
+    rays = np.ascontiguousarray(rays, np.float32).reshape(-1)
+    n = rays.size // 8
+    hits = np.zeros(n * 8, np.float32)
+    err = np.zeros(max(n, 1), np.uint32)
+    n0 = int(cw.node_offsets[1]) - int(cw.node_offsets[0])
+    nt = cw.triangles.size // CW_TRI_WORDS
+    lib().bo_trace_cwbvh8(_ptr(cw.nodes), n0, _ptr(cw.triangles), nt, _ptr(rays), n, int(any_hit), _ptr(hits),
+                          _ptr(err), threads or os.cpu_count() or 1)
+    return (hits, err[:n]) if with_errors else hits
 
 
 # ---- staged top levels --------------------------------------------------------

@@ -1,7 +1,8 @@
 """CPU checks of the wide-BVH oracle (no GPU): the collapsed tree covers every
 triangle exactly once in blocks of at most max_leaf (1..4), lane boxes are the unions of
-what they hold, child ids follow pre-order, and leaf lanes pack the
-reference's [v0][prim][e1][0][e2][0] record."""
+what they hold, a node's internal children are consecutive nodes after it and
+its leaf blocks consecutive blocks (both in lane order), and leaf lanes pack
+the reference's [v0][prim][e1][0][e2][0] record."""
 import numpy as np
 import pytest
 
@@ -43,6 +44,10 @@ def _check_segment(ow, bvh, verts, s, W, max_leaf=4):
         return nodes[i, 0:3, j], nodes[i, 3:6, j]
 
     for i in range(nb, ne):
+        kids = [nb + (int(m) & 0x03FFFFFF) for m in meta[i] if int(m) != EMPTY and int(m) >> 26 == 0]
+        blocks = [lb + (int(m) & 0x03FFFFFF) for m in meta[i] if int(m) != EMPTY and int(m) >> 26 != 0]
+        assert kids == list(range(kids[0], kids[0] + len(kids))) if kids else True
+        assert blocks == list(range(blocks[0], blocks[0] + len(blocks))) if blocks else True
         for j in range(W):
             m = int(meta[i, j])
             if m == EMPTY:
@@ -52,7 +57,7 @@ def _check_segment(ow, bvh, verts, s, W, max_leaf=4):
             mn, mx = lane_box(i, j)
             if cnt == 0:
                 c = nb + data
-                assert nb < c < ne and c > i  # pre-order: children after their parent
+                assert nb < c < ne and c > i  # children after their parent
                 referenced_nodes.append(c)
                 cm = meta[c]
                 ok = cm != EMPTY
