@@ -15,8 +15,11 @@
 //    tested as soon as the node is decoded;
 //  - a lane's box is p + q * 2^(e - 127) per axis, tested with fma against
 //    the ray's reciprocal (rcp_direction: +-1e9 where |d| <= 1e-9) over
-//    [max(t near, 0), min(t far, t)] with the reference's select-based
-//    max / min (bajo/core/utils.mojo:60-70);
+//    [max(t near, 0), min(t far, t)]; max / min are fmaxf / fminf, which
+//    agree with the reference's select form (bajo/core/utils.mojo:60-70)
+//    unless an operand is NaN;
+//  - the lane bytes are split four at a time into bit positions and child
+//    bits (the node's hit mask is the reference's, bit for bit);
 //  - triangles use the determinant-scaled Moller-Trumbore test
 //    (intersect_ray_tri_edges_scaled, bajo/core/intersect.mojo:462-505) with
 //    the current hit distance as t_max, so the first of equal-distance
@@ -43,12 +46,9 @@ struct Hit {
   uint32_t prim, tri;
 };
 
-__device__ __forceinline__ float smax(float a, float b) { return a > b ? a : b; }
-__device__ __forceinline__ float smin(float a, float b) { return a < b ? a : b; }
-
-// byte `sh / 8` of w as an exact float
-__device__ __forceinline__ float qbyte(uint32_t w, int sh) {
-  return __uint_as_float(0x4B000000u | ((w >> sh) & 0xFFu)) - 8388608.0f;
+// byte b of w as an exact float: 2^23 + q (one byte permute) minus 2^23
+__device__ __forceinline__ float qbyte(uint32_t w, int b) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7540u + b)) - 8388608.0f;
 }
 
 template <bool ANY>
@@ -101,21 +101,22 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       const uint32_t meta[2] = {__float_as_uint(n1.z), __float_as_uint(n1.w)};
       uint32_t hm = 0;
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int g = j >> 2, sh = (j & 3) * 8;
+      for (int g = 0; g < 2; ++g) {
+        // four lanes at once: bit position (low 5 bits, XOR the inverted
+        // octant on internal lanes) and child bits (top 3 bits) of each byte
+        const uint32_t inner = ((((imask >> (4 * g)) & 0xFu) * 0x00204081u) & 0x01010101u) * oi;
+        const uint32_t bit4 = (meta[g] ^ inner) & 0x1F1F1F1Fu, kids4 = (meta[g] >> 5) & 0x07070707u;
         const uint32_t nxw = negx ? q[6 + g] : q[0 + g], fxw = negx ? q[0 + g] : q[6 + g];
         const uint32_t nyw = negy ? q[8 + g] : q[2 + g], fyw = negy ? q[2 + g] : q[8 + g];
         const uint32_t nzw = negz ? q[10 + g] : q[4 + g], fzw = negz ? q[4 + g] : q[10 + g];
-        const float tnx = __fmaf_rn(qbyte(nxw, sh), idx, ox), tfx = __fmaf_rn(qbyte(fxw, sh), idx, ox);
-        const float tny = __fmaf_rn(qbyte(nyw, sh), idy, oy), tfy = __fmaf_rn(qbyte(fyw, sh), idy, oy);
-        const float tnz = __fmaf_rn(qbyte(nzw, sh), idz, oz), tfz = __fmaf_rn(qbyte(fzw, sh), idz, oz);
-        const float tn = smax(smax(tnx, tny), smax(tnz, 0.0f));
-        const float tf = smin(smin(tfx, tfy), smin(tfz, tlim));
-        const uint32_t byte = (meta[g] >> sh) & 0xFFu;
-        if (byte != 0u && tn <= tf) {
-          uint32_t bi = byte & 0x1Fu;
-          if (imask & (1u << j)) bi ^= oi;
-          hm |= (byte >> 5) << bi;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const float tnx = __fmaf_rn(qbyte(nxw, b), idx, ox), tfx = __fmaf_rn(qbyte(fxw, b), idx, ox);
+          const float tny = __fmaf_rn(qbyte(nyw, b), idy, oy), tfy = __fmaf_rn(qbyte(fyw, b), idy, oy);
+          const float tnz = __fmaf_rn(qbyte(nzw, b), idz, oz), tfz = __fmaf_rn(qbyte(fzw, b), idz, oz);
+          const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+          const float tf = fminf(fminf(tfx, tfy), fminf(tfz, tlim));
+          if (tn <= tf) hm |= __byte_perm(kids4, 0u, 0x4440u + b) << __byte_perm(bit4, 0u, 0x4440u + b);
         }
       }
       nbase = __float_as_uint(n1.x);

@@ -59,6 +59,7 @@ struct Work {
   uint32_t* task_seg;   // [wide node] segment
   uint32_t* task_desc;  // [wide node] id of its first internal child (global)
   uint32_t* task_tri;   // [wide node] first triangle of its subtree (global; CWBVH8)
+  float* area;          // [internal] box area of each binary node
   uint32_t* ready;      // [wide node] task published
   uint32_t* status;
 };
@@ -82,9 +83,9 @@ __global__ void __launch_bounds__(kBlock) count_kernel(uint32_t n, const uint32_
     // the second arrival sees every result of the subtree (acq_rel chain)
     if (atomic_add_acq_rel_gpu(&wk.flags[parent], 1u) == 0) return;
     const uint32_t x = parent;
+    wk.area[x] = area(ref_bounds(x, leaf_bounds, leaf_ids, node_bounds));
     uint32_t cand[W], cnt[W];
-    const int nc =
-        open_children<W>(x, node_meta, node_leaf_counts, leaf_bounds, leaf_ids, node_bounds, max_leaf, cand, cnt);
+    const int nc = open_children<W>(x, node_meta, node_leaf_counts, wk.area, max_leaf, cand, cnt);
     uint32_t nodes = 1, leaves = 0, mask = 0;
     for (int k = 0; k < nc; ++k) {
       if (terminal(cand[k], cnt[k], max_leaf)) {
@@ -614,8 +615,8 @@ __global__ void __launch_bounds__(trav::kTraceBlock) wide_camera_kernel(
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Plan {
-  size_t flags, ready, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, task_desc, task_tri, leaf_offsets,
-      zero_bytes, total;
+  size_t flags, ready, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, task_desc, task_tri, area,
+      leaf_offsets, zero_bytes, total;
 };
 
 // cw_segments > 0: the CWBVH8 build, which also keeps the per-segment leaf
@@ -647,6 +648,8 @@ inline Plan make_plan(uint32_t n, uint32_t width, uint32_t cw_segments = 0) {
   o = a256(o + cap * 4);
   p.task_tri = o;
   if (cw_segments) o = a256(o + cap * 4);
+  p.area = o;
+  o = a256(o + cap * 4);
   p.leaf_offsets = o;
   if (cw_segments) o = a256(o + ((size_t)cw_segments + 1) * 4);
   p.total = o;
@@ -669,6 +672,7 @@ cudaError_t build(const BajoLbvh* b, uint32_t* node_offsets, uint32_t* leaf_offs
   wk.task_seg = (uint32_t*)(ws + p.task_seg);
   wk.task_desc = (uint32_t*)(ws + p.task_desc);
   wk.task_tri = (uint32_t*)(ws + p.task_tri);
+  wk.area = (float*)(ws + p.area);
   cudaError_t e = cudaMemsetAsync(ws, 0, p.zero_bytes, st);
   if (e != cudaSuccess) return e;
   const uint32_t n = b->n_leaves;

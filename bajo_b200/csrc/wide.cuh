@@ -73,23 +73,24 @@ __device__ __forceinline__ bool terminal(uint32_t ref, uint32_t count, uint32_t 
 // x's two children; first open the internal candidate of largest surface
 // area among those with more than max_leaf triangles until W candidates or
 // none is left, then open the largest remaining internal candidates until
-// full.  An opened candidate is
-// replaced by its left child and its right child is appended.  Ties keep the
-// first candidate.  Returns the candidate count.
+// full.  An opened candidate is replaced by its left child and its right child
+// is appended.  Ties keep the first candidate.  Only internal candidates are
+// ever opened, so only their areas are read: `area` holds each internal
+// node's box area (area(), computed once per node by the bottom-up pass; L2
+// loads, as the values were written by other threads during that pass).
+// Returns the candidate count.
 template <int W>
 __device__ __forceinline__ int open_children(uint32_t x, const uint32_t* __restrict__ node_meta,
                                              const uint32_t* __restrict__ node_leaf_counts,
-                                             const float* __restrict__ leaf_bounds,
-                                             const uint32_t* __restrict__ leaf_ids,
-                                             const float* __restrict__ node_bounds, uint32_t max_leaf,
-                                             uint32_t cand[W], uint32_t cnt[W]) {
+                                             const float* area, uint32_t max_leaf, uint32_t cand[W],
+                                             uint32_t cnt[W]) {
   float ar[W];
   cand[0] = __ldg(node_meta + (size_t)x * 4 + 1);
   cand[1] = __ldg(node_meta + (size_t)x * 4 + 2);
 #pragma unroll
   for (int k = 0; k < 2; ++k) {
     cnt[k] = ref_count(cand[k], node_leaf_counts);
-    ar[k] = area(ref_bounds(cand[k], leaf_bounds, leaf_ids, node_bounds));
+    ar[k] = (cand[k] & kLeafFlag) ? 0.0f : __ldcg(area + (cand[k] & kIndexMask));
   }
   int n = 2;
   for (int phase = 0; phase < 2; ++phase) {
@@ -110,8 +111,8 @@ __device__ __forceinline__ int open_children(uint32_t x, const uint32_t* __restr
       cand[n] = __ldg(node_meta + (size_t)y * 4 + 2);
       cnt[pos] = ref_count(cand[pos], node_leaf_counts);
       cnt[n] = ref_count(cand[n], node_leaf_counts);
-      ar[pos] = area(ref_bounds(cand[pos], leaf_bounds, leaf_ids, node_bounds));
-      ar[n] = area(ref_bounds(cand[n], leaf_bounds, leaf_ids, node_bounds));
+      ar[pos] = (cand[pos] & kLeafFlag) ? 0.0f : __ldcg(area + (cand[pos] & kIndexMask));
+      ar[n] = (cand[n] & kLeafFlag) ? 0.0f : __ldcg(area + (cand[n] & kIndexMask));
       ++n;
     }
   }

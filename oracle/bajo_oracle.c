@@ -799,9 +799,6 @@ void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays, uint
 /* ------------------------------------------------------------------------- */
 /* CWBVH8 traversal                                                           */
 /* ------------------------------------------------------------------------- */
-/* fmax / fmin of bajo/core/utils.mojo:60-70: a > b ? a : b, a < b ? a : b */
-static inline float sel_max(float a, float b) { return a > b ? a : b; }
-static inline float sel_min(float a, float b) { return a < b ? a : b; }
 
 /* intersect_ray_tri_edges_scaled (bajo/core/intersect.mojo:462-505):
  * determinant-scaled Moller-Trumbore; the candidate passes when
@@ -882,8 +879,11 @@ static bo_hit cwbvh8_one(const float* nodes, const float* tris, uint32_t n_nodes
         float nz = r->d.z < 0.0f ? qhz : qlz, fz = r->d.z < 0.0f ? qlz : qhz;
         float tnx = fmaf(nx, idx, ox), tny = fmaf(ny, idy, oy), tnz = fmaf(nz, idz, oz);
         float tfx = fmaf(fx, idx, ox), tfy = fmaf(fy, idy, oy), tfz = fmaf(fz, idz, oz);
-        float tn = sel_max(sel_max(tnx, tny), sel_max(tnz, 0.0f));
-        float tf = sel_min(sel_min(tfx, tfy), sel_min(tfz, tlim));
+        /* fmaxf / fminf: the reference's select-based fmax / fmin
+         * (bajo/core/utils.mojo:60-70) give the same comparison unless an
+         * operand is NaN */
+        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
+        float tf = fminf(fminf(tfx, tfy), fminf(tfz, tlim));
         uint32_t byte = (w[6 + g] >> sh) & 0xFFu;
         if (byte != 0 && tn <= tf) {
           uint32_t bi = byte & 0x1Fu;
