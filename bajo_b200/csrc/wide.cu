@@ -17,14 +17,19 @@
 //      subtree;
 //   2. offsets_kernel turns the roots' counts into per-segment node and leaf
 //      offsets and publishes each root's task;
-//   3. assign_kernel walks wide node ids in increasing order: node I's task
-//      (binary node, first descendant id D, first leaf block, first
-//      triangle) is published by its parent, which has a smaller id, so every
-//      wait points backwards and a resident grid always makes progress.  Node
-//      I writes its own leaf blocks first, gives its internal children the
-//      ids D, D + 1, ... in lane order, and hands child c the descendant range
-//      after its siblings' (D + internal children + the NW - 1 of the children
-//      before it) with the matching leaf base, then publishes c's task.
+//   3. assign_kernel processes the wide nodes through a FIFO queue: a node's
+//      task (binary node, first descendant id D, first leaf block, first
+//      triangle) is written by its parent, which then appends the node's id
+//      to the queue; every thread takes queue slots in turn and waits (with a
+//      bound) until its slot is filled.  The set of processed nodes is closed
+//      under children, so while a slot is empty some resident thread holds an
+//      earlier slot and will fill it: a resident grid always progresses.
+//      Node I gives its internal children the ids D, D + 1, ... in lane
+//      order, hands child c the descendant range after its siblings' (D +
+//      internal children + the NW - 1 of the children before it) with the
+//      matching leaf base, publishes the children's tasks, and only then
+//      writes its own lane boxes and leaf blocks.  Ids depend only on the
+//      tree, never on the processing order.
 //
 // The CWBVH8 build (W = 8, leaves of at most 3 triangles) runs the same three
 // kernels with octant slots (spatial_slots, wide_collapse.mojo:457-521: the
@@ -60,7 +65,9 @@ struct Work {
   uint32_t* task_desc;  // [wide node] id of its first internal child (global)
   uint32_t* task_tri;   // [wide node] first triangle of its subtree (global; CWBVH8)
   float* area;          // [internal] box area of each binary node
-  uint32_t* ready;      // [wide node] task published
+  uint32_t* queue;      // [slot] 1 + id of a wide node whose task is published (0 = not yet)
+  uint32_t* head;       // next queue slot to take
+  uint32_t* tail;       // next queue slot to fill
   uint32_t* status;
 };
 
@@ -161,7 +168,7 @@ __global__ void __launch_bounds__(1024) offsets_kernel(uint32_t n_seg, const uin
       wk.task_seg[pn] = s;
       wk.task_desc[pn] = pn + 1u;
       wk.task_tri[pn] = seg_offsets[s];
-      wk.ready[pn] = 1u;
+      wk.queue[atomicAdd(wk.tail, 1u)] = pn + 1u;
     }
     pn += cn;
     pl += cl;
@@ -277,15 +284,22 @@ __device__ __forceinline__ uint32_t cw_exponent(float extent) {
 
 __device__ __forceinline__ int cw_clamp255(float f) { return f >= 0.0f ? (f <= 255.0f ? (int)f : 255) : 0; }
 
-// _quantize_lower / _quantize_upper (:61-76)
-__device__ __forceinline__ uint32_t cw_qlo(float value, float start, float scale) {
-  int q = cw_clamp255(floorf((value - start) / scale));
+// _quantize_lower / _quantize_upper (:61-76).  (value - start) / scale is
+// computed as (value - start) * 2^(127 - e): the reciprocal of a power of two
+// is exact (2^-127 as a subnormal for e = 254), so both round the same exact
+// value once.
+__device__ __forceinline__ float cw_inv_scale(uint32_t e) {
+  return e < 254u ? __uint_as_float((254u - e) << 23) : __uint_as_float(0x00400000u);
+}
+
+__device__ __forceinline__ uint32_t cw_qlo(float value, float start, float scale, float inv) {
+  int q = cw_clamp255(floorf((value - start) * inv));
   if (__fmaf_rn((float)q, scale, start) > value && q > 0) q -= 1;
   return (uint32_t)q;
 }
 
-__device__ __forceinline__ uint32_t cw_qhi(float value, float start, float scale) {
-  int q = cw_clamp255(ceilf((value - start) / scale));
+__device__ __forceinline__ uint32_t cw_qhi(float value, float start, float scale, float inv) {
+  int q = cw_clamp255(ceilf((value - start) * inv));
   if (__fmaf_rn((float)q, scale, start) < value && q < 255) q += 1;
   return (uint32_t)q;
 }
@@ -320,6 +334,7 @@ __device__ void write_cw_node(float4* __restrict__ out, const Box (&bx)[8], cons
   if (__fmaf_rn(255.0f, __uint_as_float(ey << 23), ly) < hy && ey < 254u) ++ey;
   if (__fmaf_rn(255.0f, __uint_as_float(ez << 23), lz) < hz && ez < 254u) ++ez;
   const float sx = __uint_as_float(ex << 23), sy = __uint_as_float(ey << 23), sz = __uint_as_float(ez << 23);
+  const float ix = cw_inv_scale(ex), iy = cw_inv_scale(ey), iz = cw_inv_scale(ez);
   uint32_t m[2] = {0u, 0u}, q[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) q[k] = 0u;
@@ -337,12 +352,12 @@ __device__ void write_cw_node(float4* __restrict__ out, const Box (&bx)[8], cons
       leaf_off += count;
     }
     m[g] |= byte << sh;
-    q[0 + g] |= cw_qlo(bx[j].mn.x, lx, sx) << sh;
-    q[2 + g] |= cw_qlo(bx[j].mn.y, ly, sy) << sh;
-    q[4 + g] |= cw_qlo(bx[j].mn.z, lz, sz) << sh;
-    q[6 + g] |= cw_qhi(bx[j].mx.x, lx, sx) << sh;
-    q[8 + g] |= cw_qhi(bx[j].mx.y, ly, sy) << sh;
-    q[10 + g] |= cw_qhi(bx[j].mx.z, lz, sz) << sh;
+    q[0 + g] |= cw_qlo(bx[j].mn.x, lx, sx, ix) << sh;
+    q[2 + g] |= cw_qlo(bx[j].mn.y, ly, sy, iy) << sh;
+    q[4 + g] |= cw_qlo(bx[j].mn.z, lz, sz, iz) << sh;
+    q[6 + g] |= cw_qhi(bx[j].mx.x, lx, sx, ix) << sh;
+    q[8 + g] |= cw_qhi(bx[j].mx.y, ly, sy, iy) << sh;
+    q[10 + g] |= cw_qhi(bx[j].mx.z, lz, sz, iz) << sh;
   }
   out[0] = make_float4(lx, ly, lz, __uint_as_float(ex | (ey << 8) | (ez << 16) | (imask << 24)));
   out[1] = make_float4(__uint_as_float(child_base), __uint_as_float(tri_base), __uint_as_float(m[0]),
@@ -372,22 +387,40 @@ __device__ void octant_slots(const Box& parent, const uint32_t* __restrict__ can
       d[k] = (b.mn + b.mx) * 0.5f - pc;
     }
   }
+  // Each candidate's cheapest free slot (lowest slot on ties; -1 when no
+  // cost is below FLT_MAX).  The cheapest candidate (lowest index on ties)
+  // then takes its slot, and only the candidates that wanted that slot look
+  // again -- the same pairs, in the same order, as a full rescan.
+  auto cost = [&](int k, int sl) {
+    return (((sl & 4) ? -d[k].x : d[k].x) + ((sl & 2) ? -d[k].y : d[k].y)) + ((sl & 1) ? -d[k].z : d[k].z);
+  };
+  float bc_cost[8];
+  int bc_slot[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    bc_cost[k] = FLT_MAX;
+    bc_slot[k] = -1;
+    if (k < nc) {
+#pragma unroll
+      for (int sl = 0; sl < 8; ++sl) {
+        const float c = cost(k, sl);
+        if (c < bc_cost[k]) {
+          bc_cost[k] = c;
+          bc_slot[k] = sl;
+        }
+      }
+    }
+  }
   uint32_t assigned = 0, occupied = 0;
   for (int it = 0; it < nc; ++it) {
     float best = FLT_MAX;
     int bc = -1, bs = -1;
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      if (k >= nc || (assigned >> k & 1u)) continue;
-#pragma unroll
-      for (int sl = 0; sl < 8; ++sl) {
-        if (occupied >> sl & 1u) continue;
-        const float cost = (((sl & 4) ? -d[k].x : d[k].x) + ((sl & 2) ? -d[k].y : d[k].y)) + ((sl & 1) ? -d[k].z : d[k].z);
-        if (cost < best) {
-          best = cost;
-          bc = k;
-          bs = sl;
-        }
+      if (k < nc && !(assigned >> k & 1u) && bc_slot[k] >= 0 && bc_cost[k] < best) {
+        best = bc_cost[k];
+        bc = k;
+        bs = bc_slot[k];
       }
     }
     if (bc < 0) {
@@ -399,6 +432,22 @@ __device__ void octant_slots(const Box& parent, const uint32_t* __restrict__ can
 #pragma unroll
     for (int sl = 0; sl < 8; ++sl)
       if (sl == bs) perm[sl] = bc;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      if (k < nc && !(assigned >> k & 1u) && bc_slot[k] == bs) {
+        bc_cost[k] = FLT_MAX;
+        bc_slot[k] = -1;
+#pragma unroll
+        for (int sl = 0; sl < 8; ++sl) {
+          if (occupied >> sl & 1u) continue;
+          const float c = cost(k, sl);
+          if (c < bc_cost[k]) {
+            bc_cost[k] = c;
+            bc_slot[k] = sl;
+          }
+        }
+      }
+    }
   }
 }
 
@@ -441,14 +490,29 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
     if (blockIdx.x == 0 && threadIdx.x == 0) raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
     return;
   }
-  const uint32_t stride = gridDim.x * kBlock;
-  for (uint32_t I = blockIdx.x * kBlock + threadIdx.x; I < total; I += stride) {
-    const uint64_t t0 = global_timer_ns();
-    while (ld_acquire_gpu(wk.ready + I) == 0) {
-      if (global_timer_ns() - t0 > kWaitNs) {
-        raise_status(wk.status, BAJO_STATUS_WIDE_TIMEOUT);
-        return;
+  for (;;) {
+    // take the next queue slots, one atomic per converged group of lanes
+    const unsigned active = __activemask();
+    const int lane = (int)(threadIdx.x & 31u), leader = __ffs(active) - 1;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(wk.head, (uint32_t)__popc(active));
+    base = __shfl_sync(active, base, leader);
+    const uint32_t slot = base + (uint32_t)__popc(active & ((1u << lane) - 1u));
+    if (slot >= total) break;
+    uint32_t qv = ld_acquire_gpu(wk.queue + slot);
+    if (qv == 0) {
+      const uint64_t t0 = global_timer_ns();
+      while ((qv = ld_acquire_gpu(wk.queue + slot)) == 0) {
+        if (global_timer_ns() - t0 > kWaitNs) {
+          raise_status(wk.status, BAJO_STATUS_WIDE_TIMEOUT);
+          return;
+        }
       }
+    }
+    const uint32_t I = qv - 1u;
+    if (I >= total) {
+      raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
+      continue;
     }
     const uint32_t x = wk.task_ref[I], B = wk.task_leaf[I], s = wk.task_seg[I], D = wk.task_desc[I];
     const uint32_t T = CW ? wk.task_tri[I] : 0u;
@@ -490,38 +554,33 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
         for (int k = 0; k < nc; ++k)
           if (mask & (1u << k)) own_tris += ref_count(cands[k], node_leaf_counts);
       }
-      uint32_t own = B, own_t = T, child = D, desc = D + n_int, child_leaf = B + n_leaf, child_t = T + own_tris;
+      // first the children's tasks, so the next level starts while this
+      // node writes its leaf payloads
+      uint32_t own = B, child = D, desc = D + n_int, child_leaf = B + n_leaf, child_t = T + own_tris;
+      uint32_t qs = n_int ? atomicAdd(wk.tail, n_int) : 0u;
 #pragma unroll
       for (int j = 0; j < W; ++j) {
         const int k = perm[j];
         if (k < 0) {
-          lane_box[j] = empty_box();
           lane_meta[j] = kEmpty;
           continue;
         }
         const uint32_t c = cands[k];
-        lane_box[j] = ref_bounds(c, leaf_bounds, leaf_ids, node_bounds);
         const uint32_t cnt = ref_count(c, node_leaf_counts);
         if (mask & (1u << k)) {
-          if (own >= cap) {
-            raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
-            lane_meta[j] = kEmpty;
-            continue;
-          }
-          if constexpr (CW) own_t = write_cw_tris(c, own_t, cap, node_meta, tris, o, wk.status);
-          else write_leaf_block<W>(c, own, node_meta, leaf_ids, tris, o, wk.status);
           lane_meta[j] = pack_meta(own - lb, cnt);
           ++own;
         } else {
           const uint32_t ci = c & kIndexMask;
           lane_meta[j] = pack_meta(child - nb, 0);
-          if (child < total && desc <= total) {
+          if (child < total && desc <= total && qs < total) {
             wk.task_ref[child] = c;
             wk.task_leaf[child] = child_leaf;
             wk.task_seg[child] = s;
             wk.task_desc[child] = desc;
             if constexpr (CW) wk.task_tri[child] = child_t;
-            st_release_gpu(wk.ready + child, 1u);
+            st_release_gpu(wk.queue + qs, child + 1u);
+            ++qs;
           } else {
             raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
           }
@@ -530,6 +589,28 @@ __global__ void __launch_bounds__(kBlock) assign_kernel(uint32_t n_seg, const ui
           child_leaf += wk.nl[ci];
           child_t += cnt;
         }
+      }
+      // then the lane boxes and the leaf payloads
+      uint32_t own_t = T;
+      own = B;
+#pragma unroll
+      for (int j = 0; j < W; ++j) {
+        const int k = perm[j];
+        if (k < 0) {
+          lane_box[j] = empty_box();
+          continue;
+        }
+        const uint32_t c = cands[k];
+        lane_box[j] = ref_bounds(c, leaf_bounds, leaf_ids, node_bounds);
+        if (!(mask & (1u << k))) continue;
+        if (own >= cap) {
+          raise_status(wk.status, BAJO_STATUS_BAD_TOPOLOGY);
+          lane_meta[j] = kEmpty;
+          continue;
+        }
+        if constexpr (CW) own_t = write_cw_tris(c, own_t, cap, node_meta, tris, o, wk.status);
+        else write_leaf_block<W>(c, own, node_meta, leaf_ids, tris, o, wk.status);
+        ++own;
       }
     }
     if constexpr (CW) {
@@ -615,7 +696,7 @@ __global__ void __launch_bounds__(trav::kTraceBlock) wide_camera_kernel(
 inline size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 
 struct Plan {
-  size_t flags, ready, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, task_desc, task_tri, area,
+  size_t flags, queue, cands, cinfo, nw, nl, task_ref, task_leaf, task_seg, task_desc, task_tri, area,
       leaf_offsets, zero_bytes, total;
 };
 
@@ -627,9 +708,9 @@ inline Plan make_plan(uint32_t n, uint32_t width, uint32_t cw_segments = 0) {
   size_t o = 256;  // status word
   p.flags = o;
   o = a256(o + cap * 4);
-  p.ready = o;
+  p.queue = o;
   o = a256(o + cap * 4);
-  p.zero_bytes = o;  // status, flags and ready are cleared per build
+  p.zero_bytes = o;  // status, queue counters, flags and queue are cleared per build
   p.cands = o;
   o = a256(o + cap * width * 4);
   p.cinfo = o;
@@ -662,7 +743,9 @@ cudaError_t build(const BajoLbvh* b, uint32_t* node_offsets, uint32_t* leaf_offs
   Work wk;
   wk.status = (uint32_t*)ws;
   wk.flags = (uint32_t*)(ws + p.flags);
-  wk.ready = (uint32_t*)(ws + p.ready);
+  wk.queue = (uint32_t*)(ws + p.queue);
+  wk.head = wk.status + 1;
+  wk.tail = wk.status + 2;
   wk.cands = (uint32_t*)(ws + p.cands);
   wk.cinfo = (uint32_t*)(ws + p.cinfo);
   wk.nw = (uint32_t*)(ws + p.nw);
