@@ -144,6 +144,8 @@ SIGNATURES = {
                                     _P]),
     "bajo_trace_wide_camera": (_I32, [ctypes.POINTER(BajoWideBvhC), _U32, _U32, _P, _U32, _U32, _U32, _I32, _P, _P,
                                       _P, _P, _P, _P]),
+    "bajo_hploc_workspace_size": (_I32, [_U32, _U32, ctypes.POINTER(_SZ)]),
+    "bajo_hploc_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
     "bajo_cwbvh8_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoCwbvh8SizesC)]),
     "bajo_cwbvh8_build": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoCwbvh8C), _P, _SZ, _P]),
     "bajo_cwbvh8_count": (_I32, [ctypes.POINTER(BajoCwbvh8C), _P, ctypes.POINTER(_U32)]),

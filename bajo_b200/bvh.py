@@ -47,13 +47,26 @@ def lbvh_sizes(n_tris: int, n_segments: int = 1) -> dict:
     return {name: getattr(s, name) for name in LBVH_ARRAYS + ("workspace",)}
 
 
+# GpuBvhBuildMethod (bajo/bvh/gpu/builder): LBVH (Karras topology + refit) or
+# HPLOC (hierarchical PLOC clustering over the same sorted keys)
+BUILD_METHODS = ("lbvh", "hploc")
+
+
 class GpuBvhBuildWorkspace:
     """Reusable build scratch for one (N, S) shape (GpuBinaryBuildWorkspace,
     bajo/bvh/gpu/builder/binary_layout.mojo:252)."""
 
-    def __init__(self, n_tris: int, n_segments: int = 1, device="cuda"):
-        self.n_tris, self.n_segments = n_tris, n_segments
-        nbytes = lbvh_sizes(n_tris, n_segments)["workspace"]
+    def __init__(self, n_tris: int, n_segments: int = 1, device="cuda", method: str = "lbvh"):
+        if method not in BUILD_METHODS:
+            raise ValueError(f"method must be one of {BUILD_METHODS}")
+        self.n_tris, self.n_segments, self.method = n_tris, n_segments, method
+        if method == "hploc":
+            b = ctypes.c_size_t(0)
+            _lib.check(_lib.load().bajo_hploc_workspace_size(n_tris, n_segments, ctypes.byref(b)),
+                       "bajo_hploc_workspace_size")
+            nbytes = b.value
+        else:
+            nbytes = lbvh_sizes(n_tris, n_segments)["workspace"]
         self.buffer = torch.zeros(max(nbytes, 256), dtype=torch.uint8, device=device)
 
     def status(self, stream=None) -> int:
@@ -172,14 +185,16 @@ def _ptr(t):
 
 def build_triangle_bvh(vertices: torch.Tensor, seg_offsets=None, workspace: GpuBvhBuildWorkspace | None = None,
                        out: GpuTriangleBvh | None = None, stream=None,
-                       stage_top: bool | None = None) -> GpuTriangleBvh:
+                       stage_top: bool | None = None, method: str = "lbvh") -> GpuTriangleBvh:
     """Build the binary LBVH of `vertices` (9 floats per triangle, CUDA).
 
     `seg_offsets` (optional, S+1 item offsets) builds one independent tree per
     segment in the same launches (the batched BLAS path,
     bajo/bvh/gpu/triangle_bvh.mojo:469).  `stage_top` also writes the staged
     top levels for the traversal (off by default: on B200 the top of the tree
-    stays in L1 and the staged kernels were measured no faster)."""
+    stays in L1 and the staged kernels were measured no faster).  `method`
+    "hploc" builds the tree by H-PLOC (the reference's default builder,
+    GpuBvhBuildMethod.HPLOC) instead of the LBVH topology and refit."""
     _lib.require_cuda(vertices)
     if vertices.dtype != torch.float32 or not vertices.is_contiguous() or vertices.numel() % 9:
         raise ValueError("triangle vertex buffer must be contiguous float32 with 9 floats per triangle")
@@ -200,17 +215,19 @@ def build_triangle_bvh(vertices: torch.Tensor, seg_offsets=None, workspace: GpuB
         raise ValueError("at least one segment is required")
     if stage_top is None:
         stage_top = False
-    if workspace is None or workspace.n_tris != n or workspace.n_segments != S:
-        workspace = GpuBvhBuildWorkspace(n, S, device=vertices.device)
+    if (workspace is None or workspace.n_tris != n or workspace.n_segments != S or
+            getattr(workspace, "method", "lbvh") != method):
+        workspace = GpuBvhBuildWorkspace(n, S, device=vertices.device, method=method)
     reuse = out is not None and out.n_leaves == n and out.n_segments == S and (out.top_nodes is not None or not stage_top)
     bvh = out if reuse else GpuTriangleBvh(n, seg, vertices.device, stage_top=stage_top)
     bvh.seg_offsets = seg
     bvh.vertices = vertices
     bvh.workspace = workspace
     c = bvh.c_struct(stage_top)
-    rc = _lib.load().bajo_lbvh_build(vertices.data_ptr(), ctypes.byref(c), workspace.buffer.data_ptr(),
+    entry = "bajo_hploc_build" if method == "hploc" else "bajo_lbvh_build"
+    rc = getattr(_lib.load(), entry)(vertices.data_ptr(), ctypes.byref(c), workspace.buffer.data_ptr(),
                                      workspace.buffer.numel(), _lib.stream_handle(stream))
-    _lib.check(rc, "bajo_lbvh_build")
+    _lib.check(rc, entry)
     return bvh
 
 

@@ -866,6 +866,10 @@ BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
 }
 
 }  // namespace
+
+size_t hploc_workspace_bytes(uint32_t n, uint32_t n_seg);  // hploc.cu
+cudaError_t launch_hploc(const float* d_verts, BajoLbvh* bvh, unsigned char* extra, uint32_t* status,
+                         cudaStream_t st);
 }  // namespace bajo
 
 extern "C" {
@@ -892,8 +896,14 @@ int32_t bajo_lbvh_sizes(uint32_t n, uint32_t n_seg, BajoLbvhSizes* s) {
   return BAJO_OK;
 }
 
+// hploc: the tree comes from H-PLOC (hploc.cu) instead of the LBVH topology
+// and refit; its workspace is the LBVH build's plus hploc_workspace_bytes
+static size_t hploc_extra_offset(uint32_t n, uint32_t n_seg) {
+  return (bajo::make_build_plan(n, n_seg).total + 255) & ~(size_t)255;
+}
+
 static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, size_t ws_bytes, void* stream_,
-                               cudaEvent_t* ev, int32_t n_ev) {
+                               cudaEvent_t* ev, int32_t n_ev, bool hploc = false) {
   using namespace bajo;
   if (!bvh || !ws_ || bvh->n_segments == 0 || !bvh->seg_offsets) return BAJO_ERR_INVALID_ARGUMENT;
   const uint32_t n = bvh->n_leaves, S = bvh->n_segments;
@@ -904,7 +914,8 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
     return BAJO_ERR_INVALID_ARGUMENT;
   if (bvh->top_nodes && ((uintptr_t)bvh->top_nodes & 15)) return BAJO_ERR_INVALID_ARGUMENT;
   BuildPlan plan = make_build_plan(n, S);
-  if (ws_bytes < plan.total) return BAJO_ERR_WORKSPACE_TOO_SMALL;
+  const size_t need = hploc ? hploc_extra_offset(n, S) + hploc_workspace_bytes(n, S) : plan.total;
+  if (ws_bytes < need) return BAJO_ERR_WORKSPACE_TOO_SMALL;
   if (ev && n_ev < (int32_t)(5 + plan.passes)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream_;
   // stage events: [start, bounds, morton, pass 0..P-1, topology, refit]
@@ -961,7 +972,10 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
     for (uint32_t p = 0; p < passes; ++p)
       if (!mark(3 + p)) return BAJO_ERR_CUDA;
   }
-  if (n <= kMergedMaxLeaves) {
+  if (hploc) {
+    if (!mark(3 + passes)) return BAJO_ERR_CUDA;
+    if (launch_hploc(d_verts, bvh, ws + hploc_extra_offset(n, S), status, st) != cudaSuccess) return BAJO_ERR_CUDA;
+  } else if (n <= kMergedMaxLeaves) {
     // one bottom-up pass builds the hierarchy and refits it: the topology
     // stage event is recorded right before it
     if (!mark(3 + passes)) return BAJO_ERR_CUDA;
@@ -996,6 +1010,17 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
 
 int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* ws, size_t ws_bytes, void* stream) {
   return lbvh_build_impl(d_verts, bvh, ws, ws_bytes, stream, nullptr, 0);
+}
+
+int32_t bajo_hploc_workspace_size(uint32_t n, uint32_t n_seg, size_t* bytes) {
+  if (!bytes || n_seg == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  if (n > BAJO_SORT_MAX_KEYS) return BAJO_ERR_TOO_LARGE;
+  *bytes = hploc_extra_offset(n, n_seg) + bajo::hploc_workspace_bytes(n, n_seg);
+  return BAJO_OK;
+}
+
+int32_t bajo_hploc_build(const float* d_verts, BajoLbvh* bvh, void* ws, size_t ws_bytes, void* stream) {
+  return lbvh_build_impl(d_verts, bvh, ws, ws_bytes, stream, nullptr, 0, true);
 }
 
 int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* ws, size_t ws_bytes, void* stream,

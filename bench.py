@@ -55,8 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--case", default=None,
-                   choices=["sort", "build", "trace", "wide", "cwbvh8", "tune", "render", "batched", "guided",
-                            "guided_pass"],
+                   choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tune", "render", "batched",
+                            "guided", "guided_pass"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -814,6 +814,32 @@ def run_case(args):
                     "any_ms": round(ms_any, 4), "any_mrays_s": round(WIDTH * HEIGHT / ms_any / 1e3, 2),
                     "binary_mt_ms": round(ms_bin, 4), "binary_mt_mrays_s": round(WIDTH * HEIGHT / ms_bin / 1e3, 2),
                     "status": cw.status()})
+    elif args.case == "hploc":
+        # H-PLOC against LBVH on the same triangles: build time, then closest
+        # hits of the camera and of incoherent rays through each tree
+        from bajo_b200 import scenes
+        verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
+        cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+        hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
+        nr = WIDTH * HEIGHT
+        g = torch.Generator(device="cuda").manual_seed(1)
+        rays = torch.empty(8, nr, dtype=torch.float32, device="cuda")
+        rays[0:3].uniform_(0.0, 1.0, generator=g)
+        rays[3].zero_()
+        d = torch.randn(3, nr, device="cuda", generator=g)
+        rays[4:7] = d / d.norm(dim=0, keepdim=True)
+        rays[7].fill_(3.0e38)
+        rays = rays.reshape(-1)
+        for method in ("lbvh", "hploc"):
+            ws = bvh.GpuBvhBuildWorkspace(n, 1, method=method)
+            tree = bvh.build_triangle_bvh(verts, workspace=ws, method=method)
+            ms_b = timed(lambda: bvh.build_triangle_bvh(verts, workspace=ws, out=tree, method=method))
+            ms_c = timed(lambda: tree.launch_camera(cam, hits, nr, WIDTH, HEIGHT))
+            ms_i = timed(lambda: tree.launch_rays(rays, hits, nr))
+            out.update({f"{method}_build_ms": round(ms_b, 5), f"{method}_build_mtri_s": round(n / ms_b / 1e3, 2),
+                        f"{method}_camera_mrays_s": round(nr / ms_c / 1e3, 2),
+                        f"{method}_incoherent_mrays_s": round(nr / ms_i / 1e3, 2),
+                        f"{method}_status": ws.status()})
     elif args.case in ("build", "trace"):
         from bajo_b200 import scenes
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()

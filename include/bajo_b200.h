@@ -171,6 +171,22 @@ int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* siz
 int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
+/* H-PLOC build (GpuBvhBuildMethod.HPLOC, the reference's default builder,
+ * triangle_bvh.mojo:472; build_hploc_multi_wave_kernel,
+ * bajo/bvh/gpu/builder/hploc_multi_wave.mojo:187-545): the same bounds,
+ * Morton keys and sort as bajo_lbvh_build, then Hierarchical PLOC
+ * clustering (Benthin et al., HPG 2024) instead of the Karras topology and
+ * refit.  Fills the same BajoLbvh arrays (node layout, sorted leaves and
+ * triangle records, roots), so every traversal, the wide collapse and the
+ * CWBVH8 build take its tree unchanged.  Internal node ids come from atomic
+ * counters and vary from run to run, as in the reference; children, boxes
+ * and leaf counts do not.  The workspace is larger than the LBVH build's
+ * (bajo_hploc_workspace_size); the build status (bajo_workspace_status) gets
+ * BAJO_STATUS_BAD_TOPOLOGY if a segment's node count or root is off. */
+int32_t bajo_hploc_workspace_size(uint32_t n_tris, uint32_t n_segments, size_t* bytes);
+int32_t bajo_hploc_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
+                         void* stream);
+
 /* Stage-timed build, the sync-free counterpart of the reference's
  * measure_stages / GpuBuildTimings (bajo/bvh/gpu/builder/lbvh.mojo:347-422):
  * `events` holds n_events cudaEvent_t handles created by the caller; the

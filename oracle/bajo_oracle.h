@@ -179,6 +179,14 @@ void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, uint32_t
                    uint32_t* leaf_indices, float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets,
                    uint32_t* leaf_offsets);
 
+/* ---- H-PLOC (bajo_oracle_hploc.c) ---------------------------------------- */
+/* The H-PLOC tree of the sorted leaves of `karras` (an LBVH built by
+ * bo_lbvh_build: its leaf bounds, sorted ids, codes and offsets), written to
+ * out's node_meta / node_bounds / node_leaf_counts / node_flags /
+ * leaf_parent / roots (arrays distinct from karras's).  Returns 0, or bit 0 =
+ * a PLOC round found no mutual pair, bit 1 = a segment's node count is off. */
+uint32_t bo_hploc_build(const BoLbvh* karras, BoLbvh* out);
+
 /* ---- CWBVH8 (bajo_oracle_wide.c, bajo_oracle.c) -------------------------- */
 /* W = 8 collapse with octant slots and leaves of <= 3 triangles, encoded as
  * 80-byte nodes (20 words, `cw_nodes` sized for n_leaves nodes) and 48-byte

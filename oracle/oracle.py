@@ -95,6 +95,7 @@ def _declare(L: ctypes.CDLL) -> None:
                              ctypes.c_uint64, _I, _P, _P, _U32]),
         "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_cwbvh8_build": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P]),
+        "bo_hploc_build": (ctypes.c_uint32, [ctypes.POINTER(_BoLbvh), ctypes.POINTER(_BoLbvh)]),
         "bo_trace_cwbvh8": (None, [_P, _U32, _P, _U32, _P, _U32, ctypes.c_int, _P, _P, _U32]),
         "bo_mlp_param_count": (_U32, []),
         "bo_mlp_encode": (None, [_P, _P, _P, _P]),
@@ -261,6 +262,47 @@ def lbvh_build(verts: np.ndarray, seg_offsets=None) -> OracleLbvh:
     lib().bo_lbvh_build(_ptr(v), _ptr(so), ns, ctypes.byref(s))
     o._struct = s
     return o
+
+
+def hploc_build(verts: np.ndarray, seg_offsets=None) -> OracleLbvh:
+    """The H-PLOC tree over the same sorted leaves as lbvh_build (same leaf
+    bounds, keys and ids; its own node arrays, ids in task post order)."""
+    k = lbvh_build(verts, seg_offsets)
+    m = max(k.n_internal, 1)
+    o = OracleLbvh(
+        verts=k.verts, seg_offsets=k.seg_offsets, n_leaves=k.n_leaves, n_internal=k.n_internal,
+        leaf_bounds=k.leaf_bounds, seg_bounds=k.seg_bounds, sort_keys=k.sort_keys, leaf_ids=k.leaf_ids,
+        morton_codes=k.morton_codes, node_meta=np.full(m * 4, SENTINEL, np.uint32),
+        node_bounds=np.zeros(m * 12, np.float32), node_leaf_counts=np.zeros(m, np.uint32),
+        node_flags=np.zeros(m, np.uint32), leaf_parent=np.full(max(k.n_leaves, 1), SENTINEL, np.uint32),
+        roots=np.full(k.roots.size, SENTINEL, np.uint32), internal_offsets=k.internal_offsets,
+    )
+    ks, os_ = k.struct(), o.struct()
+    err = lib().bo_hploc_build(ctypes.byref(ks), ctypes.byref(os_))
+    if err:
+        raise RuntimeError(f"oracle H-PLOC failed ({err})")
+    o._struct = os_
+    return o
+
+
+def canonical_tree(bvh, seg: int = 0) -> list:
+    """Segment seg's tree as a list of words, independent of internal node
+    ids: pre-order, one entry per node, leaf = ("L", sorted index), internal
+    = ("N", leaf count, both child boxes as u32 bits)."""
+    meta = np.asarray(bvh.node_meta).reshape(-1, 4)
+    nb = np.asarray(bvh.node_bounds).view(np.uint32).reshape(-1, 12)
+    lc = np.asarray(bvh.node_leaf_counts)
+    out, stack = [], [int(np.asarray(bvh.roots)[seg])]
+    while stack:
+        r = stack.pop()
+        if r == SENTINEL:
+            out.append(("E",))
+        elif r & LEAF_FLAG:
+            out.append(("L", r & 0x7FFFFFFF))
+        else:
+            out.append(("N", int(lc[r]), tuple(int(x) for x in nb[r])))
+            stack += [int(meta[r, 2]), int(meta[r, 1])]
+    return out
 
 
 # ---------------------------------------------------------------- camera/trace
