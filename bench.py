@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--end-bit", type=int, default=None, help="--case sort: sort bits [0, end-bit)")
     p.add_argument("--keys-only", action="store_true", help="--case sort without payload")
     p.add_argument("--node-width", type=int, default=4, choices=[4, 8], help="--case wide node width")
+    p.add_argument("--method", default="lbvh", choices=["lbvh", "hploc"],
+                   help="--case wide / cwbvh8: binary builder under the wide tree")
     p.add_argument("--max-leaf", type=int, default=4, choices=[1, 2, 3, 4], help="--case wide leaf block size")
     p.add_argument("--scene", default="spheres", choices=["spheres", "indirect"], help="--case guided scene")
     p.add_argument("--width", type=int, default=1280, help="--case guided image width")
@@ -800,7 +802,7 @@ def run_case(args):
     elif args.case == "cwbvh8":
         from bajo_b200 import scenes, wide
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
-        tree = bvh.build_triangle_bvh(verts)
+        tree = bvh.build_triangle_bvh(verts, method=args.method)
         cw = wide.build_cwbvh8(tree)
         ms_build = timed(lambda: cw.build(read_count=False))
         cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
@@ -808,6 +810,19 @@ def run_case(args):
         ms_cw = timed(lambda: cw.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT))
         ms_any = timed(lambda: cw.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, any_hit=True))
         ms_bin = timed(lambda: tree.launch_camera(cam, hits, WIDTH * HEIGHT, WIDTH, HEIGHT, tri_mode=0))
+        nr = WIDTH * HEIGHT
+        g = torch.Generator(device="cuda").manual_seed(1)
+        rays = torch.empty(8, nr, dtype=torch.float32, device="cuda")
+        rays[0:3].uniform_(0.0, 1.0, generator=g)
+        rays[3].zero_()
+        d = torch.randn(3, nr, device="cuda", generator=g)
+        rays[4:7] = d / d.norm(dim=0, keepdim=True)
+        rays[7].fill_(3.0e38)
+        rays = rays.reshape(-1)
+        ms_inc = timed(lambda: cw.launch_rays(rays, hits, nr))
+        ms_inc_bin = timed(lambda: tree.launch_rays(rays, hits, nr, tri_mode=0))
+        out.update({"method": args.method, "incoherent_mrays_s": round(nr / ms_inc / 1e3, 2),
+                    "binary_mt_incoherent_mrays_s": round(nr / ms_inc_bin / 1e3, 2)})
         out.update({"cwbvh8_nodes": cw.n_nodes, "build_ms": round(ms_build, 5),
                     "build_mtri_s": round(n / ms_build / 1e3, 2),
                     "closest_ms": round(ms_cw, 4), "closest_mrays_s": round(WIDTH * HEIGHT / ms_cw / 1e3, 2),
