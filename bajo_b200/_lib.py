@@ -146,6 +146,11 @@ SIGNATURES = {
                                       _P, _P, _P, _P]),
     "bajo_hploc_workspace_size": (_I32, [_U32, _U32, ctypes.POINTER(_SZ)]),
     "bajo_hploc_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
+    "bajo_tlas_instance_boxes": (_I32, [ctypes.POINTER(BajoLbvhC), _P, _P, _U32, _P, _P, _P]),
+    "bajo_trace_tlas_rays": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoLbvhC), _P, _P, _U32, _P, _U32,
+                                    _I32, _I32, _P, _P, _P]),
+    "bajo_trace_tlas_camera": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoLbvhC), _P, _P, _U32, _P, _U32,
+                                      _U32, _U32, _I32, _I32, _P, _P, _P]),
     "bajo_cwbvh8_sizes": (_I32, [_U32, _U32, ctypes.POINTER(BajoCwbvh8SizesC)]),
     "bajo_cwbvh8_build": (_I32, [ctypes.POINTER(BajoLbvhC), ctypes.POINTER(BajoCwbvh8C), _P, _SZ, _P]),
     "bajo_cwbvh8_count": (_I32, [ctypes.POINTER(BajoCwbvh8C), _P, ctypes.POINTER(_U32)]),

@@ -390,6 +390,44 @@ int32_t bajo_trace_cwbvh8_camera(const BajoCwbvh8* cwbvh, uint32_t n_nodes, cons
                                  float* d_t, uint32_t* d_prim, uint32_t* d_status, void* stream);
 
 /* ======================================================================== */
+/* Two-level trees: instances of the BLASes of a segmented build             */
+/* ======================================================================== */
+/* A BLAS set is a segmented BajoLbvh (bajo_lbvh_build or bajo_hploc_build),
+ * segment b = BLAS b (build_triangle_blas_set, triangle_bvh.mojo:466).  An
+ * instance i is d_blas[i] and an affine transform from BLAS space to world
+ * space, 12 f32 row-major [m00 m01 m02 tx | m10 m11 m12 ty | m20 m21 m22 tz]
+ * (Affine3, bajo/core/transform.mojo:22-47; Instance, bajo/bvh/types.mojo:
+ * 153-190), 16-byte aligned; the traversal takes the inverse transforms
+ * (world to BLAS space) in the same layout.
+ *
+ * bajo_tlas_instance_boxes writes, per instance, its BLAS root box under the
+ * transform (AABB.apply_transform, bajo/core/aabb.mojo:101-139) as 9 floats
+ * [min xyz, max xyz, min xyz]: a triangle record whose bounds are the box.
+ * bajo_lbvh_build over those records (one segment, n_instances leaves) is
+ * the top-level tree (build_triangle_tlas, bajo/bvh/gpu/tlas.mojo:618).
+ * d_status (may be NULL) gets BAJO_STATUS_BAD_TOPOLOGY for a BLAS index out
+ * of range. */
+int32_t bajo_tlas_instance_boxes(const BajoLbvh* blas_set, const float* d_transforms, const uint32_t* d_blas,
+                                 uint32_t n_instances, float* d_boxes9, uint32_t* d_status, void* stream);
+
+/* Closest hits (any_hit = 0) or occlusion (any_hit = 1) through the
+ * top-level tree (_trace_tlas_ray, bajo/bvh/gpu/tlas.mojo:176-232;
+ * trace_triangle_tlas_camera_kernel :235): each instance leaf takes the ray
+ * to BLAS space (Affine3.ray), traverses its BLAS with the current hit
+ * distance as t_max and keeps a closer hit with its instance id; the winning
+ * normal goes to world space through the inverse's transpose.  Rays, cameras
+ * and hits as bajo_trace_rays / bajo_trace_camera; the hit's inst word is
+ * the instance (0xFFFFFFFF on a miss), prim is BLAS-local.  An occluded ray
+ * reports t = 0, prim 0xFFFFFFFF and the occluding instance. */
+int32_t bajo_trace_tlas_rays(const BajoLbvh* tlas, const BajoLbvh* blas_set, const float* d_inv_transforms,
+                             const uint32_t* d_blas, uint32_t n_instances, const float* d_rays, uint32_t n_rays,
+                             int32_t any_hit, int32_t tri_mode, float* d_hits8, uint32_t* d_status, void* stream);
+int32_t bajo_trace_tlas_camera(const BajoLbvh* tlas, const BajoLbvh* blas_set, const float* d_inv_transforms,
+                               const uint32_t* d_blas, uint32_t n_instances, const float* d_cameras, uint32_t n_rays,
+                               uint32_t width, uint32_t height, int32_t any_hit, int32_t tri_mode, float* d_hits8,
+                               uint32_t* d_status, void* stream);
+
+/* ======================================================================== */
 /* Wavefront path tracing over one triangle LBVH                             */
 /* ======================================================================== */
 /* Render algorithms (RENDER, bajo/rt/types.mojo:53-59). */

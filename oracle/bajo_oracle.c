@@ -797,6 +797,157 @@ void bo_trace_brute(const float* verts, uint32_t n_tris, const float* rays, uint
 }
 
 /* ------------------------------------------------------------------------- */
+/* two-level trees                                                            */
+/* ------------------------------------------------------------------------- */
+/* AABB.apply_transform (bajo/core/aabb.mojo:101-139) of each instance's BLAS
+ * root box (seg_bounds[12 b .. 12 b + 6)), written as [min, max, min]; an
+ * empty box (min > max) stays empty */
+void bo_tlas_instance_boxes(const float* seg_bounds, uint32_t n_blas, const float* xf, const uint32_t* blas,
+                            uint32_t n, float* out9) {
+  for (uint32_t i = 0; i < n; ++i) {
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    uint32_t b = blas[i];
+    if (b < n_blas) {
+      const float* lb = seg_bounds + (size_t)b * 12;
+      const float* r = xf + (size_t)i * 12;
+      if (lb[0] <= lb[3]) {
+        for (int k = 0; k < 3; ++k) mn[k] = mx[k] = r[4 * k + 3];
+        for (int col = 0; col < 3; ++col)
+          for (int k = 0; k < 3; ++k) {
+            float m = r[4 * k + col], a = m * lb[col], c = m * lb[3 + col];
+            mn[k] = mn[k] + fminf(a, c);
+            mx[k] = mx[k] + fmaxf(a, c);
+          }
+      }
+    }
+    float* o = out9 + (size_t)i * 9;
+    o[0] = mn[0]; o[1] = mn[1]; o[2] = mn[2];
+    o[3] = mx[0]; o[4] = mx[1]; o[5] = mx[2];
+    o[6] = mn[0]; o[7] = mn[1]; o[8] = mn[2];
+  }
+}
+
+typedef struct {
+  const BoLbvh* top;
+  const BoLbvh* blas;
+  const float* blas_verts;
+  const float* inv;
+  const uint32_t* blas_idx;
+  uint32_t n_inst;
+  int mode, any;
+} tlas_ctx;
+
+typedef struct { bo_hit h; uint32_t inst; int hit; } tl_hit;
+
+/* one instance leaf (tlas.mojo:54-136): the ray in BLAS space (Affine3.ray,
+ * transform.mojo:155-211), the BLAS walk with the current hit distance as
+ * t_max, a closer hit promoted with its instance */
+static int tlas_leaf(const tlas_ctx* c, const bo_ray* r, uint32_t sorted, tl_hit* th) {
+  uint32_t inst = c->top->leaf_ids[sorted];
+  uint32_t b = c->blas_idx[inst];
+  const float* m = c->inv + (size_t)inst * 12;
+  v3 o = v3make(fmaf(m[0], r->o.x, fmaf(m[1], r->o.y, fmaf(m[2], r->o.z, m[3]))),
+                fmaf(m[4], r->o.x, fmaf(m[5], r->o.y, fmaf(m[6], r->o.z, m[7]))),
+                fmaf(m[8], r->o.x, fmaf(m[9], r->o.y, fmaf(m[10], r->o.z, m[11]))));
+  v3 d = v3make(fmaf(m[0], r->d.x, fmaf(m[1], r->d.y, m[2] * r->d.z)),
+                fmaf(m[4], r->d.x, fmaf(m[5], r->d.y, m[6] * r->d.z)),
+                fmaf(m[8], r->d.x, fmaf(m[9], r->d.y, m[10] * r->d.z)));
+  bo_ray lr = make_ray_od(o, d, r->tmin, c->any ? r->tmax : th->h.t);
+  bo_hit lh = trace_one(c->blas, c->blas_verts, &lr, b, c->mode, NULL);
+  if (lh.prim == BO_EMPTY) return 0;
+  th->h = lh;
+  th->inst = inst;
+  th->hit = 1;
+  return 1;
+}
+
+/* the binary near-first loop of trace_one over the top-level tree */
+static tl_hit tlas_one(const tlas_ctx* c, const bo_ray* r) {
+  tl_hit th;
+  th.h = miss_hit(r->tmax);
+  th.inst = BO_EMPTY;
+  th.hit = 0;
+  const BoLbvh* t = c->top;
+  uint32_t root = t->roots[0];
+  if (root == BO_SENTINEL) return th;
+  if (root & BO_LEAF_FLAG) {
+    tlas_leaf(c, r, root & 0x7FFFFFFFu, &th);
+    return th;
+  }
+  uint32_t stack[128];
+  uint32_t sp = 0, cur = root;
+  for (;;) {
+    const float* b = t->node_bounds + (size_t)12 * cur;
+    uint32_t ch[2] = {t->node_meta[4 * (size_t)cur + 1], t->node_meta[4 * (size_t)cur + 2]};
+    float lim0 = c->any ? r->tmax : th.h.t;
+    int bh[2];
+    float tn[2];
+    for (int k = 0; k < 2; ++k) bh[k] = box_hit(r, b + 6 * k, lim0, &tn[k]);
+    int valid[2] = {0, 0};
+    for (int k = 0; k < 2; ++k) {
+      if (!bh[k]) continue;
+      if (ch[k] & BO_LEAF_FLAG) {
+        if (tlas_leaf(c, r, ch[k] & 0x7FFFFFFFu, &th) && c->any) return th;
+      } else {
+        valid[k] = 1;
+      }
+    }
+    int near = -1;
+    if (valid[0]) near = 0;
+    if (valid[1] && (near == -1 || tn[1] < tn[0])) near = 1;
+    if (near >= 0) {
+      float lim = (c->any ? r->tmax : th.h.t) * BO_SLACK;
+      int far = 1 - near;
+      if (valid[far] && tn[far] <= lim) stack[sp++] = ch[far];
+      if (tn[near] <= lim) {
+        cur = ch[near];
+        continue;
+      }
+    }
+    if (sp == 0) break;
+    cur = stack[--sp];
+  }
+  return th;
+}
+
+static void tlas_store(const tlas_ctx* c, float* hits8, uint32_t i, const tl_hit* th) {
+  float* o = hits8 + (size_t)8 * i;
+  memset(o, 0, 8 * sizeof(float));
+  uint32_t prim = th->hit ? th->h.prim : BO_EMPTY;
+  float t = th->h.t;
+  v3 n = v3make(0, 0, 0);
+  if (c->any) {
+    if (th->hit) {
+      t = 0.0f;
+      prim = BO_EMPTY;
+    }
+  } else if (th->hit) {
+    o[0] = th->h.u;
+    o[1] = th->h.v;
+    const float* m = c->inv + (size_t)th->inst * 12;
+    v3 ln = th->h.n; /* normalize(cross(e1, e2)) of the BLAS triangle */
+    /* normal_from_inverse (transform.mojo:224-257) */
+    n = v3normalize(v3make(fmaf(m[0], ln.x, fmaf(m[4], ln.y, m[8] * ln.z)),
+                           fmaf(m[1], ln.x, fmaf(m[5], ln.y, m[9] * ln.z)),
+                           fmaf(m[2], ln.x, fmaf(m[6], ln.y, m[10] * ln.z))));
+  }
+  memcpy(&o[2], &prim, 4);
+  memcpy(&o[3], &th->inst, 4);
+  o[4] = n.x; o[5] = n.y; o[6] = n.z; o[7] = t;
+}
+
+void bo_trace_tlas(const BoLbvh* top, const BoLbvh* blas, const float* blas_verts, const float* inv,
+                   const uint32_t* blas_idx, uint32_t n_inst, const float* rays, uint32_t n, int any, int mode,
+                   float* hits8) {
+  tlas_ctx c = {top, blas, blas_verts, inv, blas_idx, n_inst, mode, any};
+  for (uint32_t i = 0; i < n; ++i) {
+    bo_ray r = make_ray(rays, n, i);
+    tl_hit th = tlas_one(&c, &r);
+    tlas_store(&c, hits8, i, &th);
+  }
+}
+
+/* ------------------------------------------------------------------------- */
 /* CWBVH8 traversal                                                           */
 /* ------------------------------------------------------------------------- */
 

@@ -179,6 +179,17 @@ void bo_wide_build(const BoLbvh* b, const float* verts, uint32_t width, uint32_t
                    uint32_t* leaf_indices, float* leaf_tris, uint32_t* leaf_sorted, uint32_t* node_offsets,
                    uint32_t* leaf_offsets);
 
+/* ---- two-level trees (bajo_oracle.c) ------------------------------------- */
+/* instance boxes as [min, max, min] records (see bajo_tlas_instance_boxes) */
+void bo_tlas_instance_boxes(const float* seg_bounds, uint32_t n_blas, const float* transforms12,
+                            const uint32_t* blas, uint32_t n, float* out9);
+/* closest (any = 0) or any hit of SoA rays through `top` (an LBVH over the
+ * instance boxes) and the segmented BLAS set `blas` (vertices blas_verts);
+ * inv = world -> BLAS transforms (12 f32 each); hits8 with inst set */
+void bo_trace_tlas(const BoLbvh* top, const BoLbvh* blas, const float* blas_verts, const float* inv,
+                   const uint32_t* blas_idx, uint32_t n_inst, const float* rays, uint32_t n, int any, int mode,
+                   float* hits8);
+
 /* ---- H-PLOC (bajo_oracle_hploc.c) ---------------------------------------- */
 /* The H-PLOC tree of the sorted leaves of `karras` (an LBVH built by
  * bo_lbvh_build: its leaf bounds, sorted ids, codes and offsets), written to

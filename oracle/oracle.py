@@ -96,6 +96,9 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_cwbvh8_build": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P]),
         "bo_hploc_build": (ctypes.c_uint32, [ctypes.POINTER(_BoLbvh), ctypes.POINTER(_BoLbvh)]),
+        "bo_tlas_instance_boxes": (None, [_P, _U32, _P, _P, _U32, _P]),
+        "bo_trace_tlas": (None, [ctypes.POINTER(_BoLbvh), ctypes.POINTER(_BoLbvh), _P, _P, _P, _U32, _P, _U32,
+                                 ctypes.c_int, ctypes.c_int, _P]),
         "bo_trace_cwbvh8": (None, [_P, _U32, _P, _U32, _P, _U32, ctypes.c_int, _P, _P, _U32]),
         "bo_mlp_param_count": (_U32, []),
         "bo_mlp_encode": (None, [_P, _P, _P, _P]),
@@ -283,6 +286,31 @@ def hploc_build(verts: np.ndarray, seg_offsets=None) -> OracleLbvh:
         raise RuntimeError(f"oracle H-PLOC failed ({err})")
     o._struct = os_
     return o
+
+
+def tlas_instance_boxes(blas: OracleLbvh, transforms: np.ndarray, blas_idx: np.ndarray) -> np.ndarray:
+    """Each instance's world box as a [min, max, min] triangle record (n, 9)."""
+    xf = np.ascontiguousarray(transforms, np.float32).reshape(-1)
+    bi = np.ascontiguousarray(blas_idx, np.uint32)
+    out = np.zeros(bi.size * 9, np.float32)
+    lib().bo_tlas_instance_boxes(_ptr(blas.seg_bounds), blas.seg_offsets.size - 1, _ptr(xf), _ptr(bi), bi.size,
+                                 _ptr(out))
+    return out.reshape(-1, 9)
+
+
+def trace_tlas(top: OracleLbvh, blas: OracleLbvh, inv_transforms: np.ndarray, blas_idx: np.ndarray,
+               rays_soa: np.ndarray, any_hit: bool = False, tri_mode=TRI_WATERTIGHT) -> np.ndarray:
+    """Closest or any hit of SoA rays through a top-level tree over instances
+    of a segmented BLAS set; hits8 with the instance in word 3."""
+    rays = np.ascontiguousarray(rays_soa, np.float32).reshape(-1)
+    n = rays.size // 8
+    inv = np.ascontiguousarray(inv_transforms, np.float32).reshape(-1)
+    bi = np.ascontiguousarray(blas_idx, np.uint32)
+    hits = np.zeros(n * 8, np.float32)
+    ts, bs = top.struct(), blas.struct()
+    lib().bo_trace_tlas(ctypes.byref(ts), ctypes.byref(bs), _ptr(blas.verts), _ptr(inv), _ptr(bi), bi.size,
+                        _ptr(rays), n, int(any_hit), int(tri_mode), _ptr(hits))
+    return hits
 
 
 def canonical_tree(bvh, seg: int = 0) -> list:
