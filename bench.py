@@ -55,8 +55,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--case", default=None,
-                   choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tune", "render", "batched",
-                            "guided", "guided_pass"],
+                   choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tlas", "tune", "render",
+                            "batched", "guided", "guided_pass"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -855,6 +855,52 @@ def run_case(args):
                         f"{method}_camera_mrays_s": round(nr / ms_c / 1e3, 2),
                         f"{method}_incoherent_mrays_s": round(nr / ms_i / 1e3, 2),
                         f"{method}_status": ws.status()})
+    elif args.case == "tlas":
+        # 8 BLASes of n / 8 triangles each, 512 randomly rotated, scaled and
+        # placed instances (the shape of the reference's TLAS stress test,
+        # test/bvh/gpu/test_blas_tlas.mojo:320); camera and incoherent rays
+        import numpy as np
+        from bajo_b200 import scenes, tlas
+        rng = np.random.default_rng(0)
+        per = max(n // 8, 1)
+        verts = torch.from_numpy(np.concatenate(
+            [scenes.random_triangles(per, seed=b, spread=0.02).reshape(-1) for b in range(8)])).cuda()
+        seg = np.arange(9, dtype=np.int64) * per
+        xf = []
+        for _ in range(512):
+            q = rng.normal(size=4)
+            q /= np.linalg.norm(q)
+            w, x, y, z = q
+            rot = np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - w * z), 2 * (x * z + w * y)],
+                            [2 * (x * y + w * z), 1 - 2 * (x * x + z * z), 2 * (y * z - w * x)],
+                            [2 * (x * z - w * y), 2 * (y * z + w * x), 1 - 2 * (x * x + y * y)]])
+            xf.append(np.concatenate([rot * rng.uniform(0.5, 1.5), rng.uniform(-6, 6, (3, 1))], axis=1).reshape(-1))
+        xf = np.array(xf, np.float32)
+        bi = rng.integers(0, 8, 512).astype(np.uint32)
+        blas_ws = bvh.GpuBvhBuildWorkspace(per * 8, 8)
+        blas_set = bvh.build_triangle_bvh(verts, seg, workspace=blas_ws)
+        t = tlas.build_triangle_tlas(blas_set, xf, bi)
+        ms_blas = timed(lambda: bvh.build_triangle_bvh(verts, seg, workspace=blas_ws, out=blas_set))
+        ms_tlas = timed(lambda: t.build())
+        cam = torch.from_numpy(camera.camera([0.0, 2.0, -20.0], [0, 0, 0], [0, 1, 0], 0.5)).cuda()
+        hits = torch.empty(8 * WIDTH * HEIGHT, dtype=torch.float32, device="cuda")
+        nr = WIDTH * HEIGHT
+        ms_cam = timed(lambda: t.launch_camera(cam, hits, nr, WIDTH, HEIGHT))
+        ms_any = timed(lambda: t.launch_camera(cam, hits, nr, WIDTH, HEIGHT, any_hit=True))
+        hit_frac = (hits.view(-1, 8)[:, 3].view(torch.int32) != -1).float().mean().item()
+        g = torch.Generator(device="cuda").manual_seed(1)
+        rays = torch.empty(8, nr, dtype=torch.float32, device="cuda")
+        rays[0:3].uniform_(-6.0, 6.0, generator=g)
+        rays[3].zero_()
+        d = torch.randn(3, nr, device="cuda", generator=g)
+        rays[4:7] = d / d.norm(dim=0, keepdim=True)
+        rays[7].fill_(3.0e38)
+        rays = rays.reshape(-1)
+        ms_inc = timed(lambda: t.launch_rays(rays, hits, nr))
+        out.update({"blas": 8, "instances": 512, "triangles_per_blas": per, "blas_build_ms": round(ms_blas, 5),
+                    "tlas_build_ms": round(ms_tlas, 5), "camera_mrays_s": round(nr / ms_cam / 1e3, 2),
+                    "camera_any_mrays_s": round(nr / ms_any / 1e3, 2), "camera_hit_fraction": round(hit_frac, 3),
+                    "incoherent_mrays_s": round(nr / ms_inc / 1e3, 2), "status": int(t.status.item())})
     elif args.case in ("build", "trace"):
         from bajo_b200 import scenes
         verts = torch.from_numpy(scenes.random_triangles(n, seed=0, spread=0.01 if n <= 65536 else 0.004)).cuda()
