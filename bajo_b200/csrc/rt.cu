@@ -1,6 +1,6 @@
 // rt.cu -- wavefront path tracing (PATH / NEE / MIS, and GUIDED with the
-// learned proposal of mlp.cuh) of Lambertian + emissive triangle scenes over
-// the binary LBVH, on sm_100a.
+// learned proposal of mlp.cuh) of Lambertian, emissive, metal and dielectric
+// triangle scenes over the binary LBVH, on sm_100a.
 //
 // Restates the reference's GPU wavefront renderer for triangle scenes:
 //  - primary rays: gpu_rt_primary_kernel (bajo/rt/gpu/common_kernels.mojo:22),
@@ -94,6 +94,9 @@ struct SceneView {
   const float* lights;
   uint32_t n_lights;
   float total_light_weight;
+  const float* metals;       // 4 per metal: albedo rgb, fuzz
+  const float* dielectrics;  // 1 per dielectric: refraction index
+  bool has_materials;
 };
 
 // warp-aggregated queue append: one atomic per warp; every lane of the warp
@@ -184,7 +187,8 @@ constexpr int kShadeThreads = 256;
 struct ShadeCtx {
   uint32_t* vtx_ids;
   float* vtx;
-  uint32_t* vcount;     // [b] = Lambertian vertices of bounce b
+  uint32_t* vcount;     // [b] = Lambertian vertices of bounce b (from the front of the vertex queue)
+  uint32_t* mcount;     // [b] = metal / dielectric hits of bounce b (from the back)
   // guided tracing only
   const __half* params16;
   const float* box;
@@ -247,8 +251,9 @@ __global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q
   const uint32_t stride = gridDim.x * kBlock;
   for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
     const uint32_t idx = base + threadIdx.x;
-    bool want_vtx = false;
-    uint32_t path_id = 0;
+    bool want_vtx = false, want_mat = false;
+    uint32_t path_id = 0, mat_leaf = 0;
+    float mat_t = 0.0f;
     f3 vp, vn, va, vt;
     if (idx < count) {
       const uint32_t idw = src_ids[idx];
@@ -309,6 +314,27 @@ __global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q
           vn = normal;
           va = mk(sc.lambertians[3 * midx], sc.lambertians[3 * midx + 1], sc.lambertians[3 * midx + 2]);
           vt = T;
+        } else if (kind == BAJO_MAT_METAL || kind == BAJO_MAT_DIELECTRIC) {
+          want_mat = true;
+          mat_leaf = h.leaf;
+          mat_t = t;
+        }
+      }
+    }
+    if (sc.has_materials) {
+      // metal / dielectric hits go to the back of the vertex queue: the
+      // source slot, the hit's sorted leaf and distance (material_kernel
+      // recomputes the rest exactly as above)
+      const uint32_t k = warp_append(&c.mcount[bounce], want_mat);
+      if (want_mat) {
+        // every path yields at most one vertex, so the two ends never meet
+        const uint32_t slot = cap - 1u - k;
+        if (k < cap) {
+          c.vtx_ids[slot] = idx;
+          c.vtx[0 * cap + slot] = __uint_as_float(mat_leaf);
+          c.vtx[1 * cap + slot] = mat_t;
+        } else {
+          raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
         }
       }
     }
@@ -528,6 +554,93 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(SceneView sc, Queues q, S
   }
 }
 
+// Metal and dielectric hits of bounce `bounce` (gpu_rt_shade_dispatch_kernel
+// and _gpu_rt_shade_one, bajo/rt/gpu/path_shading.mojo:690-786): the hit is
+// rebuilt from the source path and triangle as trace_kernel built it, the
+// material sample (smp::sample_metal / sample_dielectric) draws u, v from the
+// bounce's BSDF stream, and the continued path (Russian roulette as for
+// Lambertian bounces) carries the sample's pdf and delta flag.  No light
+// sample is taken at these vertices, as in the reference.
+template <int ALGO>
+__global__ void __launch_bounds__(kBlock) material_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
+                                                          uint32_t max_depth, uint64_t seed) {
+  const uint32_t cap = q.capacity;
+  const uint32_t count = min(c.mcount[bounce], cap);
+  const uint32_t* src_ids = q.ids[bounce & 1];
+  const float* src = q.fields[bounce & 1];
+  for (uint32_t base = blockIdx.x * kBlock; base < count; base += gridDim.x * kBlock) {
+    const uint32_t k = base + threadIdx.x;
+    bool want = false;
+    uint32_t path_id = 0;
+    f3 p, dir, Tn;
+    float pdf = 0.0f;
+    bool delta = false;
+    if (k < count && bounce + 1 < max_depth) {
+      const uint32_t slot = cap - 1u - k;
+      const uint32_t idx = c.vtx_ids[slot];
+      const uint32_t leaf = __float_as_uint(c.vtx[0 * cap + slot]);
+      const float t = c.vtx[1 * cap + slot];
+      path_id = src_ids[idx] & kIdMask;
+      const f3 o = mk(src[0 * cap + idx], src[1 * cap + idx], src[2 * cap + idx]);
+      const f3 d = mk(src[4 * cap + idx], src[5 * cap + idx], src[6 * cap + idx]);
+      const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
+      const float4 a = __ldg(sc.tris + (size_t)leaf * 3 + 0);
+      const float4 b = __ldg(sc.tris + (size_t)leaf * 3 + 1);
+      const float4 cc = __ldg(sc.tris + (size_t)leaf * 3 + 2);
+      const f3 v0 = mk(a.x, a.y, a.z);
+      const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(cc.x, cc.y, cc.z) - v0));
+      const bool front = dot(d, outward) < 0.0f;
+      const f3 normal = front ? outward : neg(outward);
+      const uint32_t surface = __ldg(sc.surfaces + __float_as_uint(a.w));
+      const uint32_t midx = surface & kIndexMask28;
+      p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+      const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
+      smp::BsdfSample smpl;
+      if ((surface >> 28) == BAJO_MAT_METAL) {
+        const float* m = sc.metals + 4 * (size_t)midx;
+        smpl = smp::sample_metal(d, normal, mk(m[0], m[1], m[2]), m[3], u.x, u.y);
+      } else {
+        smpl = smp::sample_dielectric(d, normal, sc.dielectrics[midx], front, u.x);
+      }
+      if (smpl.ok) {
+        Tn = mul(T, smpl.weight);
+        bool alive = true;
+        if (bounce + 1 >= 5u) {
+          const float mx = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+          if (mx <= 0.0f) alive = false;
+          else {
+            const float survival = fminf(fmaxf(mx, 0.05f), 0.95f);
+            const float4 rr = uniform4(seed, path_id, stage_roulette(bounce));
+            if (rr.x >= survival) alive = false;
+            else Tn = divs(Tn, survival);
+          }
+        }
+        want = alive;
+        dir = smpl.dir;
+        pdf = smpl.pdf;
+        delta = smpl.delta;
+      }
+    }
+    const uint32_t slot = warp_append(&q.counters[2 * (bounce + 1)], want);
+    if (want) {
+      if (slot < cap) {
+        uint32_t* dst_ids = q.ids[(bounce + 1) & 1];
+        float* dst = q.fields[(bounce + 1) & 1];
+        if (ALGO == BAJO_RENDER_GUIDED) q.rec[(bounce + 1) & 1][slot] = kNoRecord;
+        dst_ids[slot] = path_id | (delta ? kDeltaBit : 0u);
+        dst[0 * cap + slot] = p.x; dst[1 * cap + slot] = p.y; dst[2 * cap + slot] = p.z;
+        dst[3 * cap + slot] = 0.001f;
+        dst[4 * cap + slot] = dir.x; dst[5 * cap + slot] = dir.y; dst[6 * cap + slot] = dir.z;
+        dst[7 * cap + slot] = FLT_MAX;
+        dst[8 * cap + slot] = Tn.x; dst[9 * cap + slot] = Tn.y; dst[10 * cap + slot] = Tn.z;
+        dst[11 * cap + slot] = pdf;
+      } else {
+        raise_status(q.status, BAJO_WAVE_PATH_OVERFLOW);
+      }
+    }
+  }
+}
+
 struct ShadeSmem {
   mlp::Net net;
   mlp::WarpTile tile[kShadeThreads / 32];
@@ -696,7 +809,7 @@ bool make_layout(const BajoRenderSettings* s, Layout* L) {
   L->cap = ppc * s->spp;
   // [2b] paths of bounce b, [2b+1] its shadow rays, then [2 max_depth + 2 +
   // b] the Lambertian vertices of bounce b
-  L->n_counters = 3 * s->max_depth + 2;
+  L->n_counters = 4 * s->max_depth + 2;
   const size_t cap = L->cap;
   size_t o = 256;  // status word, then two 64-bit ray totals at offset 8
   L->off_counters = o;
@@ -745,6 +858,9 @@ bool make_views(const BajoRtScene* scene, unsigned char* w, const Layout& L, Sce
   sc.lights = scene->lights;
   sc.n_lights = scene->n_lights;
   sc.total_light_weight = scene->total_light_weight;
+  sc.metals = scene->metals;
+  sc.dielectrics = scene->dielectrics;
+  sc.has_materials = scene->metals || scene->dielectrics;
   for (int k = 0; k < 2; ++k) {
     q.ids[k] = (uint32_t*)(w + L.off_ids[k]);
     q.fields[k] = (float*)(w + L.off_fields[k]);
@@ -764,6 +880,7 @@ ShadeCtx shade_ctx(unsigned char* w, const Layout& L, const Queues& q, uint32_t 
   c.vtx_ids = (uint32_t*)(w + L.off_vtx_ids);
   c.vtx = (float*)(w + L.off_vtx);
   c.vcount = q.counters + 2 * max_depth + 2;
+  c.mcount = c.vcount + max_depth;
   return c;
 }
 
@@ -775,6 +892,10 @@ cudaError_t launch_bounce(const SceneView& sc, const Queues& q, const ShadeCtx& 
   if (e != cudaSuccess) return e;
   shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if (sc.has_materials) {
+    material_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, seed);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  }
   if (ALGO != BAJO_RENDER_PATH) {
     shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
     e = cudaGetLastError();
@@ -915,6 +1036,10 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
     if (e != cudaSuccess) return e;
     guided_shade_kernel<<<shade_grid, kShadeThreads, smem, st>>>(sc, q, gc, b, s->max_depth, sample_base, s->seed);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if (sc.has_materials) {
+      material_kernel<BAJO_RENDER_GUIDED><<<grid, kBlock, 0, st>>>(sc, q, gc, b, s->max_depth, s->seed);
+      if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    }
     shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
     return cudaGetLastError();
   };

@@ -3,8 +3,8 @@
 Reference entry points (jgsimard/bajo): ``render_gpu_triangles`` /
 ``enqueue_render_gpu_triangles`` (bajo/rt/gpu/triangle_path.mojo:143,172)
 with ``RenderSettings`` and the PATH / NEE / MIS algorithms
-(``RENDER``, bajo/rt/types.mojo:53).  Scenes are Lambertian + emissive
-triangles (metal / dielectric shading is outside this path).  Device work is
+(``RENDER``, bajo/rt/types.mojo:53).  Scenes are Lambertian, emissive,
+metal and dielectric triangles.  Device work is
 ``bajo_render`` in the C ABI; the light table is built by the library's host
 code (``bajo_rt_build_lights``).
 """
@@ -27,7 +27,8 @@ LIGHT_STRIDE = 16
 class BajoRtSceneC(ctypes.Structure):
     _fields_ = [("bvh", ctypes.POINTER(_lib.BajoLbvhC)), ("surfaces", ctypes.c_void_p),
                 ("lambertians", ctypes.c_void_p), ("emissives", ctypes.c_void_p), ("lights", ctypes.c_void_p),
-                ("n_lights", ctypes.c_uint32), ("total_light_weight", ctypes.c_float)]
+                ("n_lights", ctypes.c_uint32), ("total_light_weight", ctypes.c_float),
+                ("metals", ctypes.c_void_p), ("dielectrics", ctypes.c_void_p)]
 
 
 class BajoRenderSettingsC(ctypes.Structure):
@@ -76,6 +77,10 @@ class GpuRtTriangleScene:
         self.surfaces = torch.from_numpy(scene.surfaces.view(np.int32)).to(device)
         self.lambertians = torch.from_numpy(scene.lambertians).to(device)
         self.emissives = torch.from_numpy(scene.emissives).to(device)
+        metals, dielectrics = getattr(scene, "metals", None), getattr(scene, "dielectrics", None)
+        self.metals = None if metals is None or metals.size == 0 else torch.from_numpy(metals).to(device)
+        self.dielectrics = (None if dielectrics is None or dielectrics.size == 0
+                            else torch.from_numpy(dielectrics).to(device))
         lights, self.n_lights, self.total_light_weight = build_lights(scene)
         self.lights_host = lights
         self.lights = torch.from_numpy(lights).to(device)
@@ -90,6 +95,8 @@ class GpuRtTriangleScene:
         s.lights = self.lights.data_ptr()
         s.n_lights = self.n_lights
         s.total_light_weight = self.total_light_weight
+        s.metals = None if self.metals is None else self.metals.data_ptr()
+        s.dielectrics = None if self.dielectrics is None else self.dielectrics.data_ptr()
         return s
 
 

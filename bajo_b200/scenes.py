@@ -105,6 +105,8 @@ def bounds_of(verts: np.ndarray):
 
 # --- path-tracing scenes ------------------------------------------------------
 MAT_LAMBERTIAN = 0
+MAT_METAL = 1
+MAT_DIELECTRIC = 2
 MAT_EMISSIVE = 3
 
 
@@ -164,11 +166,15 @@ class RtScene:
     per-triangle surface ids and material tables (SceneData,
     bajo/rt/types.mojo:382)."""
 
-    def __init__(self, vertices, surfaces, lambertians, emissives, camera=None, description=""):
+    def __init__(self, vertices, surfaces, lambertians, emissives, camera=None, description="", metals=None,
+                 dielectrics=None):
         self.vertices = np.ascontiguousarray(vertices, np.float32).reshape(-1)
         self.surfaces = np.ascontiguousarray(surfaces, np.uint32)
         self.lambertians = np.ascontiguousarray(lambertians, np.float32).reshape(-1)
         self.emissives = np.ascontiguousarray(emissives, np.float32).reshape(-1)
+        # metals: 4 f32 each (albedo rgb, fuzz); dielectrics: 1 f32 each (refraction index)
+        self.metals = None if metals is None else np.ascontiguousarray(metals, np.float32).reshape(-1)
+        self.dielectrics = None if dielectrics is None else np.ascontiguousarray(dielectrics, np.float32).reshape(-1)
         self.camera = camera
         self.description = description
 
@@ -230,6 +236,38 @@ def indirect_box_scene(emission: float = 40.0, size: float = 0.2, y: float = 0.8
     return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
                    np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
                    f"unit box lit by an upward-facing {size} x {size} panel + {n_spheres} icospheres")
+
+
+def materials_in_box(n_spheres: int = 12, subdivisions: int = 3, seed: int = 3, kinds=(0, 1, 2, 3)) -> RtScene:
+    """The lit unit box with icospheres of every material the renderer
+    shades, taking `kinds` in turn: 0 Lambertian, 1 mirror metal (fuzz 0),
+    2 glossy metal (fuzz 0.05 to 0.4), 3 glass (refraction index 1.5)."""
+    rng = np.random.default_rng(seed)
+    unit = icosphere(subdivisions)
+    parts, surf = [unit_box_inward(), ceiling_light()], [[surface_id(MAT_LAMBERTIAN, 0)] * 12,
+                                                        [surface_id(MAT_EMISSIVE, 0)] * 2]
+    albedo, metals, dielectrics = [[0.75, 0.75, 0.75]], [], []
+    for s in range(n_spheres):
+        r = rng.uniform(0.06, 0.12)
+        lo = np.array([r + 0.01, r + 0.01, r + 0.25])
+        hi = np.array([1 - r - 0.01, 1 - r - 0.06, 1 - r - 0.01])
+        parts.append(unit * r + (lo + rng.random(3) * (hi - lo)))
+        kind = kinds[s % len(kinds)]
+        if kind == 0:
+            surf.append([surface_id(MAT_LAMBERTIAN, len(albedo))] * unit.shape[0])
+            albedo.append(list(rng.uniform(0.2, 0.8, 3)))
+        elif kind in (1, 2):
+            surf.append([surface_id(MAT_METAL, len(metals))] * unit.shape[0])
+            metals.append(list(rng.uniform(0.5, 0.95, 3)) + [0.0 if kind == 1 else float(rng.uniform(0.05, 0.4))])
+        else:
+            surf.append([surface_id(MAT_DIELECTRIC, len(dielectrics))] * unit.shape[0])
+            dielectrics.append(1.5)
+    from .camera import camera_from_vfov
+    cam = camera_from_vfov([0.5, 0.5, 0.02], [0.5, 0.5, 1.0], [0.0, 1.0, 0.0], 60.0)
+    return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
+                   np.array(albedo, np.float32), np.array([[15.0] * 3], np.float32), cam,
+                   f"unit box + {n_spheres} icospheres: Lambertian, mirror, glossy metal, glass",
+                   metals=np.array(metals, np.float32), dielectrics=np.array(dielectrics, np.float32))
 
 
 def small_rt_scene(seed: int = 1) -> RtScene:

@@ -438,6 +438,8 @@ int32_t bajo_trace_tlas_camera(const BajoLbvh* tlas, const BajoLbvh* blas_set, c
 /* Surface ids: kind in the top 4 bits, table index below
  * (SurfaceId, bajo/rt/types.mojo:24-34). */
 #define BAJO_MAT_LAMBERTIAN 0u
+#define BAJO_MAT_METAL 1u
+#define BAJO_MAT_DIELECTRIC 2u
 #define BAJO_MAT_EMISSIVE 3u
 #define BAJO_SURFACE(kind, index) (((uint32_t)(kind) << 28) | ((uint32_t)(index) & 0x0FFFFFFFu))
 
@@ -458,7 +460,16 @@ typedef struct BajoRtScene {
   const float* lights;       /* BAJO_LIGHT_STRIDE f32 per emissive triangle        */
   uint32_t n_lights;
   float total_light_weight;  /* sum of area * mean(radiance) over the lights        */
+  const float* metals;       /* 4 f32 per metal: albedo rgb, fuzz (NULL: none)     */
+  const float* dielectrics;  /* 1 f32 refraction index per dielectric (NULL: none) */
 } BajoRtScene;
+/* Metal and dielectric surfaces (_sample_metal / _sample_dielectric,
+ * bajo/rt/shading.mojo:122-198; gpu_rt_shade_dispatch_kernel,
+ * bajo/rt/gpu/path_shading.mojo:786): mirror (fuzz <= 1e-4) or glossy
+ * reflection, and Schlick-weighted reflection / refraction.  They take no
+ * light sample; the continued path carries the sample's pdf and the delta
+ * flag (mirror and dielectric).  With both tables NULL the renderer runs no
+ * material pass. */
 
 typedef struct BajoRenderSettings {
   uint32_t width, height, spp, max_depth;

@@ -1457,6 +1457,8 @@ void bo_rt_sincos_turns(float u, float* s_out, float* c_out) {
 }
 
 #define BO_MAT_LAMBERTIAN 0u
+#define BO_MAT_METAL 1u
+#define BO_MAT_DIELECTRIC 2u
 #define BO_MAT_EMISSIVE 3u
 #define BO_LIGHT_STRIDE 16
 static const float BO_INV_PI = 0.3183098861837907f;
@@ -1467,6 +1469,126 @@ static inline v3 vdivs(v3 a, float s) { return v3make(a.x / s, a.y / s, a.z / s)
 static inline float power_heuristic(float a, float b) {
   float a2 = a * a, b2 = b * b, den = a2 + b2;
   return den > 0.0f ? a2 / den : 0.0f;
+}
+
+/* series_log2 / series_exp2 / series_pow: the CUDA sampling.cuh functions,
+ * operation for operation (atanh series of log2 on [sqrt(1/2), sqrt(2)),
+ * Taylor series of 2^f on |f| <= 1/2) */
+static float series_log2(float x) {
+  uint32_t bits;
+  memcpy(&bits, &x, 4);
+  int e = (int)((bits >> 23) & 0xFFu) - 127;
+  uint32_t mb = (bits & 0x007FFFFFu) | 0x3F800000u;
+  float m;
+  memcpy(&m, &mb, 4);
+  if (m > 1.41421356f) {
+    m = m * 0.5f;
+    e += 1;
+  }
+  float s = (m - 1.0f) / (m + 1.0f);
+  float s2 = s * s;
+  float poly = 1.0f + s2 * (0.333333333f + s2 * (0.2f + s2 * (0.142857143f + s2 * 0.111111111f)));
+  return (float)e + ((2.0f * s) * poly) * 1.44269504f;
+}
+
+static float series_exp2(float z) {
+  if (z < -126.0f) return 0.0f;
+  if (z > 127.0f) z = 127.0f;
+  float k = rintf(z);
+  float y = (z - k) * 0.693147181f;
+  float p = 1.0f + y * (1.0f + y * (0.5f + y * (0.166666667f + y * (0.0416666667f + y * (0.00833333333f +
+                                                                     y * (0.00138888889f + y * 0.000198412698f))))));
+  uint32_t sb = (uint32_t)((int)k + 127) << 23;
+  float sc;
+  memcpy(&sc, &sb, 4);
+  return p * sc;
+}
+
+static float series_pow(float x, float y) {
+  if (y == 0.0f) return 1.0f;
+  if (!(x >= 1.17549435e-38f)) return 0.0f;
+  return series_exp2(y * series_log2(x));
+}
+
+float bo_rt_series_pow(float x, float y) { return series_pow(x, y); }
+
+static v3 v3reflect(v3 v, v3 n) {
+  float k = 2.0f * v3dot(v, n);
+  return v3make(v.x - k * n.x, v.y - k * n.y, v.z - k * n.z);
+}
+
+typedef struct { v3 dir, weight; float pdf; int delta, ok; } bo_bsdf;
+
+/* _sample_metal / _evaluate_metal (bajo/rt/shading.mojo:29-56,122-161) */
+static bo_bsdf sample_metal(v3 d, v3 normal, v3 albedo, float fuzz, float u, float v) {
+  bo_bsdf r;
+  v3 reflected = v3normalize(v3reflect(v3normalize(d), normal));
+  int smooth = fuzz <= 1.0e-4f;
+  r.delta = smooth;
+  if (smooth) {
+    r.dir = reflected;
+    r.weight = albedo;
+    r.pdf = 1.0f;
+    r.ok = v3dot(reflected, normal) > 0.0f;
+    return r;
+  }
+  float exponent = fmaxf(2.0f / (fuzz * fuzz) - 2.0f, 0.0f);
+  float cos_t = series_pow(u, 1.0f / (exponent + 1.0f));
+  float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+  float sp, cp;
+  bo_rt_sincos_turns(v, &sp, &cp);
+  v3 helper = fabsf(reflected.y) > 0.99f ? v3make(1.0f, 0.0f, 0.0f) : v3make(0.0f, 1.0f, 0.0f);
+  v3 tangent = v3normalize(v3cross(helper, reflected));
+  v3 bitangent = v3cross(reflected, tangent);
+  v3 dir = v3normalize(v3add(v3add(v3muls(tangent, cp * sin_t), v3muls(bitangent, sp * sin_t)),
+                             v3muls(reflected, cos_t)));
+  v3 dn = v3normalize(dir);
+  int surface_valid = v3dot(normal, dn) > 0.0f;
+  float lobe_cos = fmaxf(v3dot(reflected, dn), 0.0f);
+  float lobe = series_pow(lobe_cos, exponent);
+  int valid = surface_valid && lobe_cos > 0.0f;
+  float value_scale = valid ? ((exponent + 2.0f) * lobe) / 6.28318531f : 0.0f;
+  float pdf = valid ? ((exponent + 1.0f) * lobe) / 6.28318531f : 0.0f;
+  float scos = fmaxf(v3dot(normal, dir), 0.0f);
+  r.ok = pdf > 0.0f && scos > 0.0f;
+  float scale = scos / (r.ok ? pdf : 1.0f);
+  r.dir = dir;
+  r.weight = v3muls(v3muls(albedo, value_scale), scale);
+  r.pdf = pdf;
+  return r;
+}
+
+/* _sample_dielectric (bajo/rt/shading.mojo:165-198), refract and the
+ * Schlick reflectance (:235-258) */
+static bo_bsdf sample_dielectric(v3 d, v3 normal, float ior, int front, float u) {
+  bo_bsdf r;
+  float ri = front ? 1.0f / ior : ior;
+  v3 ud = v3normalize(d);
+  float cos_t = fminf(v3dot(vneg(ud), normal), 1.0f);
+  float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+  int cannot = ri * sin_t > 1.0f;
+  float root = (1.0f - ri) / (1.0f + ri);
+  float r2 = root * root;
+  float x = 1.0f - cos_t;
+  float x2 = x * x;
+  float x5 = (x2 * x2) * x;
+  float refl = fmaf(1.0f - r2, x5, r2);
+  int rs = cannot || refl > u;
+  v3 out;
+  if (rs) {
+    out = v3reflect(ud, normal);
+  } else {
+    float ct = fminf(v3dot(vneg(ud), normal), 1.0f);
+    v3 perp = v3make(ri * (ud.x + ct * normal.x), ri * (ud.y + ct * normal.y), ri * (ud.z + ct * normal.z));
+    float par = -sqrtf(fabsf(1.0f - v3dot(perp, perp)));
+    out = v3make(perp.x + par * normal.x, perp.y + par * normal.y, perp.z + par * normal.z);
+  }
+  r.dir = v3normalize(out);
+  r.weight = v3make(1.0f, 1.0f, 1.0f);
+  r.pdf = rs ? (cannot ? 1.0f : refl) : 1.0f - refl;
+  r.delta = 1;
+  r.ok = 1;
+  return r;
 }
 
 /* LightStore (bajo/rt/types.mojo:190-247, 490-525) */
@@ -1570,6 +1692,8 @@ typedef struct {
   const float* lights;
   uint32_t n_lights;
   float total_weight;
+  const float* metals;      /* 4 per metal (may be NULL) */
+  const float* dielectrics; /* 1 per dielectric (may be NULL) */
   const float* cam;
   uint32_t width, height, spp, max_depth;
   uint64_t seed;
@@ -1644,6 +1768,33 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
         rad[0] += TL.x * wgt; rad[1] += TL.y * wgt; rad[2] += TL.z * wgt;
       }
       break;
+    }
+    if (kind == BO_MAT_METAL || kind == BO_MAT_DIELECTRIC) {
+      /* _gpu_rt_shade_one for METAL / DIELECTRIC (path_shading.mojo:690-786):
+       * no light sample; the continuation carries the sample's pdf and delta */
+      if (b + 1 >= c->max_depth) break;
+      float u[4];
+      bo_rt_uniform4(c->seed, path_id, st_bsdf(b), u);
+      bo_bsdf sm;
+      if (kind == BO_MAT_METAL) {
+        const float* m = c->metals + 4 * (size_t)midx;
+        sm = sample_metal(d, normal, load3(m), m[3], u[0], u[1]);
+      } else {
+        sm = sample_dielectric(d, normal, c->dielectrics[midx], front, u[0]);
+      }
+      if (!sm.ok) break;
+      v3 Tm = vmul(T, sm.weight);
+      if (b + 1 >= 5u) {
+        float mm = fmaxf(Tm.x, fmaxf(Tm.y, Tm.z));
+        if (mm <= 0.0f) break;
+        float survival = fminf(fmaxf(mm, 0.05f), 0.95f);
+        float rr[4];
+        bo_rt_uniform4(c->seed, path_id, st_roulette(b), rr);
+        if (rr[0] >= survival) break;
+        Tm = vdivs(Tm, survival);
+      }
+      o = p; d = sm.dir; tmin = 0.001f; tmax = BO_FLT_MAX; T = Tm; prev_pdf = sm.pdf; delta = sm.delta;
+      continue;
     }
     if (kind != BO_MAT_LAMBERTIAN) break;
     v3 albedo = load3(c->lambertians + 3 * (size_t)midx);
@@ -1742,12 +1893,13 @@ static void rt_range(void* p, uint32_t b, uint32_t e) {
 /* bo_render: pixels (3 f32, mean over samples in sample order) and optional
  * per-sample radiance.  Scene arrays as in BajoRtScene. */
 void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, const float* lambertians,
-               const float* emissives, const float* lights, uint32_t n_lights, float total_weight,
+               const float* emissives, const float* metals, const float* dielectrics, const float* lights,
+               uint32_t n_lights, float total_weight,
                const float* cam, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth, uint64_t seed,
                int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads) {
   uint64_t n_paths = (uint64_t)width * height * spp;
   float* rad = sample_radiance ? sample_radiance : (float*)malloc(sizeof(float) * 3 * n_paths);
-  rt_ctx c = {bvh, verts, surfaces, lambertians, emissives, lights, n_lights, total_weight, cam,
+  rt_ctx c = {bvh, verts, surfaces, lambertians, emissives, lights, n_lights, total_weight, metals, dielectrics, cam,
               width, height, spp, max_depth, seed, algorithm, rad};
   rt_job job = {&c};
   bo_parallel_for((uint32_t)n_paths, n_threads, 256, rt_range, &job);

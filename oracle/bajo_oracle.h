@@ -162,8 +162,11 @@ void bo_rt_uniform4(uint64_t seed, uint32_t path_id, uint32_t stage, float out[4
 void bo_rt_sincos_turns(float u, float* s, float* c);
 int bo_rt_build_lights(const float* verts, const uint32_t* surfaces, uint32_t n_tris, const float* emissives,
                        float* out_lights, uint32_t max_lights, uint32_t* n_lights, float* total_weight);
+/* x^y by the series the metal lobe uses (see sampling.cuh) */
+float bo_rt_series_pow(float x, float y);
 void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, const float* lambertians,
-               const float* emissives, const float* lights, uint32_t n_lights, float total_weight,
+               const float* emissives, const float* metals, const float* dielectrics, const float* lights,
+               uint32_t n_lights, float total_weight,
                const float* camera20, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth,
                uint64_t seed, int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads);
 

@@ -91,10 +91,11 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_uniform4": (None, [ctypes.c_uint64, _U32, _U32, _P]),
         "bo_rt_sincos_turns": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
-        "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
+        "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
         "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_cwbvh8_build": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P]),
+        "bo_rt_series_pow": (ctypes.c_float, [ctypes.c_float, ctypes.c_float]),
         "bo_hploc_build": (ctypes.c_uint32, [ctypes.POINTER(_BoLbvh), ctypes.POINTER(_BoLbvh)]),
         "bo_tlas_instance_boxes": (None, [_P, _U32, _P, _P, _U32, _P]),
         "bo_trace_tlas": (None, [ctypes.POINTER(_BoLbvh), ctypes.POINTER(_BoLbvh), _P, _P, _P, _U32, _P, _U32,
@@ -467,8 +468,14 @@ def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=
     pixels = np.zeros(3 * width * height, np.float32)
     samples = np.zeros(3 * width * height * spp, np.float32) if return_samples else None
     s = bvh.struct()
+    metals = getattr(scene, "metals", None)
+    dielectrics = getattr(scene, "dielectrics", None)
+    metals = None if metals is None else np.ascontiguousarray(metals, np.float32).reshape(-1)
+    dielectrics = None if dielectrics is None else np.ascontiguousarray(dielectrics, np.float32).reshape(-1)
     lib().bo_render(ctypes.byref(s), _ptr(bvh.verts), _ptr(scene.surfaces), _ptr(scene.lambertians),
-                    _ptr(scene.emissives), _ptr(lights), n_lights, total, _ptr(cam), width, height, spp, max_depth,
+                    _ptr(scene.emissives), None if metals is None else _ptr(metals),
+                    None if dielectrics is None else _ptr(dielectrics), _ptr(lights), n_lights, total, _ptr(cam),
+                    width, height, spp, max_depth,
                     seed, algorithm, _ptr(pixels), None if samples is None else _ptr(samples), threads or n_threads())
     img = pixels.reshape(height, width, 3)
     return (img, samples.reshape(height, width, spp, 3)) if return_samples else img

@@ -71,3 +71,36 @@ def test_large_scene_render_matches_oracle(oracle):
     torch.cuda.synchronize()
     ref = oracle.render(sc, sc.camera, w, h, spp, algorithm=4)
     assert np.array_equal(img.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+
+
+@pytest.fixture(scope="module")
+def materials():
+    from bajo_b200 import rt
+    sc = scenes.materials_in_box(n_spheres=8, subdivisions=2)
+    return sc, rt.GpuRtTriangleScene(sc)
+
+
+@pytest.mark.parametrize("algorithm", [0, 3, 4])
+def test_materials_render_matches_oracle(oracle, materials, algorithm):
+    """Lambertian, mirror, glossy metal and glass spheres: the material pass
+    and the delta flag give the oracle's image bit for bit."""
+    from bajo_b200 import rt
+    sc, gsc = materials
+    w, h, spp = 40, 24, 8
+    settings = rt.RenderSettings(w, h, spp, rng_seed=404, max_depth=12)
+    ws = rt.RenderWorkspace(settings, algorithm)
+    img = rt.render_gpu_triangles(settings, sc.camera, gsc, algorithm, workspace=ws)
+    torch.cuda.synchronize()
+    assert ws.status() == 0
+    ref = oracle.render(sc, sc.camera, w, h, spp, max_depth=12, seed=404, algorithm=algorithm)
+    got = img.cpu().numpy()
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+    assert got.mean() > 0.05
+
+
+def test_guided_render_runs_with_materials(materials):
+    from bajo_b200 import guide
+    sc, gsc = materials
+    gr = guide.GuidedRenderer(gsc, sc.camera, 32, 20, max_depth=8, record_capacity=1 << 14, steps=2, batch=1 << 10)
+    img = gr.render(passes=3, train_passes=2).cpu().numpy()
+    assert gr.workspace.status() == 0 and np.all(np.isfinite(img)) and img.mean() > 0.05
