@@ -26,7 +26,7 @@ pack.mojo:5-23):
   came first; texture maps are deduplicated by path and resolved against the
   MTL file's directory, option flags (``-bm 0.5``) skipped.
 
-The PBRT reader (``bajo/parser/pbrt``) is not restated.
+The PBRT reader (``bajo/parser/pbrt``) is restated in ``bajo_b200.pbrt``.
 
 ``write_ppm_from_colors`` restates bajo/rt/cpu/depth_first.mojo:287-315:
 binary P6 with each channel stored as ``uint8(256 * clamp(sqrt(x), 0,
