@@ -301,3 +301,21 @@ def test_parsed_scene_renders_with_oracle(oracle):
     img = oracle.render(rs, rs.camera, s.width, s.height, s.samples_per_pixel, max_depth=s.max_depth,
                         seed=s.rng_seed, algorithm=4)
     assert img.shape == (10, 12, 3) and np.all(np.isfinite(img)) and img.sum() > 0.0
+
+
+@pytest.mark.parametrize("text,value", [("1e-3", 0.001), ("+2", 2.0), (".5", 0.5), ("-0", 0.0), ("3.", 3.0),
+                                        ("12.5E+1", 125.0), ("", 0.0)])
+def test_number_tokens(text, value):
+    assert pbrt.parse_f32(text) == np.float32(value)
+
+
+@pytest.mark.parametrize("text", ["1.5x", "0x10", "nan", "inf", "1e", "--1", "1e400"])
+def test_bad_number_tokens(text):
+    with pytest.raises(pbrt.PbrtParseError):
+        pbrt.parse_f32(text)
+
+
+def test_integer_tokens():
+    assert pbrt.parse_int("3.0") == 3 and pbrt.parse_int("-7") == -7
+    with pytest.raises(pbrt.PbrtParseError):
+        pbrt.parse_int("3.25")
