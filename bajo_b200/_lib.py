@@ -29,6 +29,7 @@ TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
 SORT_NOALLOC_MAX_KEYS = 1 << 20
+SORT_NOALLOC_SCRATCH_BYTES = 10490368  # BAJO_SORT_NOALLOC_SCRATCH_BYTES
 SORT_VARIANTS = 5  # tile shapes / digit widths of the 64-bit keys; 32-bit keys have 4
 
 _ERRORS = {

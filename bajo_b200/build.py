@@ -44,21 +44,42 @@ def up_to_date() -> bool:
     return all(os.path.getmtime(p) <= t for p in _inputs())
 
 
+def _stale(obj: str, src: str) -> bool:
+    """An object is rebuilt when it is missing or older than its source, any
+    shared header, the C-ABI header or this script."""
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    deps = [src, __file__, os.path.join(ROOT, "include", "bajo_b200.h")] + [os.path.join(CSRC, h) for h in HEADERS]
+    return any(os.path.getmtime(p) > t for p in deps)
+
+
 def build(verbose: bool = False, ptxas_verbose: bool = False, force: bool = False) -> str:
     if not force and up_to_date():
         return LIB
+    from concurrent.futures import ThreadPoolExecutor
     build_dir = os.path.join(HERE, "_build")
     os.makedirs(build_dir, exist_ok=True)
-    objs = []
+    objs, jobs = [], []
     for src in _sources():
         obj = os.path.join(build_dir, os.path.basename(src) + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj]
-        if ptxas_verbose:
-            cmd += ["-Xptxas", "-v"]
+        objs.append(obj)
+        if force or ptxas_verbose or _stale(obj, src):
+            cmd = [NVCC, *ARCH, *FLAGS, "-c", src, "-o", obj + ".tmp"]
+            if ptxas_verbose:
+                cmd += ["-Xptxas", "-v"]
+            jobs.append((cmd, obj))
+
+    def compile_one(job):
+        cmd, obj = job
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
-        objs.append(obj)
+        os.replace(obj + ".tmp", obj)
+
+    workers = max(1, min(len(jobs), os.cpu_count() or 1))
+    with ThreadPoolExecutor(max_workers=workers) as ex:
+        list(ex.map(compile_one, jobs))
     tmp = LIB + ".tmp"
     cmd = [NVCC, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     if verbose:

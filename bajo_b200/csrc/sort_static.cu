@@ -19,7 +19,10 @@
 //    must be serialised by the caller;
 //  - the first call on a device looks up the array's device address
 //    (cudaGetSymbolAddress) with that device current; make that first call
-//    before any stream capture.
+//    before any stream capture.  Calls made outside a capture look the
+//    address up again (a host-side table lookup), so a device reset, after
+//    which the module and its array may be loaded elsewhere, is picked up by
+//    the next uncaptured call; captured calls use the address cached last.
 #include <mutex>
 
 #include "onesweep.cuh"
@@ -39,6 +42,8 @@ constexpr uint32_t kNoAllocPasses = 4;  // 32-bit keys, 8-bit digits
 // array has a fixed size; smaller sorts use a prefix-compatible, smaller plan.
 constexpr size_t kNoAllocScratchBytes =
     onesweep::make_plan<uint32_t>(kNoAllocMaxKeys, true, kNoAllocPasses).total;
+static_assert(kNoAllocScratchBytes == BAJO_SORT_NOALLOC_SCRATCH_BYTES,
+              "the header's scratch size must follow the sort plan");
 
 __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
@@ -48,13 +53,16 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 std::mutex g_noalloc_mu;
 void* g_noalloc_ptr[64] = {};
 
-cudaError_t noalloc_scratch(void** out) {
+cudaError_t noalloc_scratch(cudaStream_t stream, void** out) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= 64) return cudaErrorInvalidDevice;
+  cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+  e = cudaStreamIsCapturing(stream, &capture);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev] || capture == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess) return e;
@@ -78,7 +86,7 @@ extern "C" int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_val
   if (p.total > kNoAllocScratchBytes) return BAJO_ERR_TOO_LARGE;
   cudaStream_t stream = (cudaStream_t)stream_;
   void* base = nullptr;
-  if (noalloc_scratch(&base) != cudaSuccess) return BAJO_ERR_CUDA;
+  if (noalloc_scratch(stream, &base) != cudaSuccess) return BAJO_ERR_CUDA;
   unsigned char* w = (unsigned char*)base;
   // the array keeps the previous call's contents: clear the status word and
   // every counter / flag that must start at zero

@@ -40,12 +40,46 @@ WORKLOAD = "plain LBVH build of 65,536 random triangles (seed 0) + 1024x1024 clo
 # Algorithmic bytes of one onesweep digit pass over the LBVH sort: read and
 # write one u64 key and one u32 payload per triangle.
 PASS_BYTES_PER_KEY = 24
+# digit passes of the single-scene LBVH sort: 8-bit digits over the 30-bit
+# Morton code, bits [0, 32) (the reference CPU builder's four byte passes,
+# bajo/bvh/cpu/builder/lbvh.mojo:56-62)
+CPU_SORT_PASSES = 4
 HIT_BYTES = 32      # 8-word hit written per ray
 NODE_BYTES = 64     # 48 B child boxes + 16 B child refs per visited node
 TRI_BYTES = 48      # packed triangle record per triangle test
 
 
-def parse():
+def workload_triangles(n: int = N_TRIS, seed: int = 0, spread: float = 0.01):
+    """The plain LBVH workload's triangles: centroids uniform in [0,1]^3 plus
+    three vertex offsets uniform in +-spread per axis, FP32, seeded.  The same
+    numpy calls as bajo_b200.scenes.random_triangles, repeated here so the
+    reference arm imports nothing from bajo_b200."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    c = rng.random((n, 1, 3), dtype=np.float32)
+    off = rng.uniform(-spread, spread, size=(n, 3, 3)).astype(np.float32)
+    return np.ascontiguousarray((c + off).reshape(n * 9), dtype=np.float32)
+
+
+def workload_camera():
+    """The workload's pinhole camera through the oracle's restatement of
+    Camera.from_vfov (bajo/bvh/camera.mojo): eye (0.5, 0.5, -1.5) looking +z,
+    60 degree vertical field of view."""
+    from oracle import oracle as O
+    return O.camera_from_vfov([0.5, 0.5, -1.5], [0.5, 0.5, -0.5], [0.0, 1.0, 0.0], 60.0)
+
+
+def workload_config() -> dict:
+    """The `config` both arms print (identical dicts)."""
+    return {"workload": WORKLOAD, "triangles": N_TRIS, "rays": WIDTH * HEIGHT, "seed": 0, "morton_bits": 30,
+            "l2": "GPU arm: 256 MiB device write before every timed build and trace; CPU arm: host caches as they are"}
+
+
+def parse(argv=None):
+    return parse_args(argv)
+
+
+def parse_args(argv=None):
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=50)
@@ -75,7 +109,7 @@ def parse():
     p.add_argument("--scenes", type=int, default=4096, help="--case batched scene count")
     p.add_argument("--train-passes", type=int, default=16, help="--case guided passes followed by training")
     p.add_argument("--train-steps", type=int, default=32, help="--case guided Adam steps per training pass")
-    return p.parse_args()
+    return p.parse_args(argv)
 
 
 def measured_peaks():
@@ -214,19 +248,19 @@ def cpu_baseline(verts, seconds):
 
 def cpu_trace_sample(verts, stride=16):
     from oracle import oracle as O
-    from bajo_b200 import camera
     cb = O.CpuLbvh(verts)
     cb.build()
-    rays = O.camera_rays(camera.plain_lbvh_camera(), WIDTH * HEIGHT, WIDTH, HEIGHT).reshape(8, -1)
+    rays = O.camera_rays(workload_camera(), WIDTH * HEIGHT, WIDTH, HEIGHT).reshape(8, -1)
     sub = rays[:, ::stride].copy().reshape(-1)
     n = sub.size // 8
     cb.trace(sub)
+    seconds = float(os.environ.get("BENCH_CPU_TRACE_SECONDS", "2.0"))
     t0 = time.perf_counter()
     reps = 0
     while True:
         cb.trace(sub)
         reps += 1
-        if time.perf_counter() - t0 > 2.0:
+        if time.perf_counter() - t0 > seconds:
             break
     dt = (time.perf_counter() - t0) / reps
     return n / dt / 1e6, cb.threads, n
@@ -238,10 +272,9 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    from bajo_b200 import scenes
     from oracle import oracle as O
     O.build()
-    verts = scenes.random_triangles(N_TRIS, seed=0)
+    verts = workload_triangles()
     cb = O.CpuLbvh(verts)
     for _ in range(max(args.warmup, 1)):
         cb.build()
@@ -257,8 +290,7 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(total / args.steps * 1e3, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays": WIDTH * HEIGHT, "seed": 0,
-                   "parallelism": "host threads"},
+        "config": workload_config(), "parallelism": f"{cb.threads} host threads", "sort_passes": CPU_SORT_PASSES,
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": cb.threads, "kind": "port",
                          "sample": f"{args.steps} full builds of the 65,536-triangle scene (C restatement of the "
                                    "reference CPU LBVH builder; Mojo is unavailable here)"},
@@ -286,12 +318,12 @@ def run_bajo(args):
     stream = torch.cuda.current_stream()
     sh = stream.cuda_stream
 
-    verts_h = scenes.random_triangles(N_TRIS, seed=0)
+    verts_h = workload_triangles()
     verts = torch.from_numpy(verts_h).to(dev)
     ws = bvh.GpuBvhBuildWorkspace(N_TRIS, 1, device=dev)
     tree = bvh.build_triangle_bvh(verts, workspace=ws)
-    # builds go through a record without top_nodes (the reference's build);
-    # traces through one with the staged top levels the first build wrote
+    # builds and traces go through the tree record as built (no staged top
+    # levels: the tree was created without them, the reference's layout)
     c = tree.c_struct(stage_top=False)
     c_trace = tree.c_struct()
     cam = torch.from_numpy(camera.plain_lbvh_camera()).to(dev)
@@ -444,9 +476,8 @@ def run_bajo(args):
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(build_total / args.steps * 1e3, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "triangles": N_TRIS, "rays": n_rays, "seed": 0,
-                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-                   "l2": "flushed (256 MiB write) before every timed build and trace", "sort_passes": passes},
+        "config": workload_config(), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+        "sort_passes": passes,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
                 "d2h_bytes_per_step": 12 * 4,
                 "what": "pinned H2D of the vertices + build + D2H of the root child boxes (device status read once after the timed steps)"},

@@ -3,7 +3,7 @@
  *
  * Drop-in boundary for the GPU path of jgsimard/bajo (Mojo).  The reference
  * exposes this path as Mojo generics over a DeviceContext; a Mojo host binds
- * these symbols with `external_call` / `DLHandle` instead (INTEGRATION.md).
+ * these symbols with `external_call` / `DLHandle` instead.
  *
  * Conventions
  *  - Every pointer named d_* is DEVICE memory allocated by the caller.  The
@@ -97,14 +97,17 @@ int32_t bajo_sort_tuning_get(uint32_t key_bytes, int32_t has_values, uint32_t n,
  * memory and pass only the buffers they compute on, or frame loops where an
  * allocation would stall the device.  No counterpart in the reference.  Same
  * result as bajo_sort_pairs_u32 (stable, in place).  Its scratch is one fixed
- * device array inside the library (about 8.6 MB, held on every GPU that loads
- * the library until exit), so n <= BAJO_SORT_NOALLOC_MAX_KEYS; larger n
- * returns BAJO_ERR_TOO_LARGE.  All calls on a device share that array: calls
- * whose device work overlaps race and must be serialised by the caller.  The
- * first call on a device looks up the array's address; make it before any
- * stream capture.  d_status (may be NULL) receives the BAJO_STATUS_* bits of
- * this call. */
+ * device array inside the library (BAJO_SORT_NOALLOC_SCRATCH_BYTES, about
+ * 10.5 MB, held on every GPU that loads the library until exit), so
+ * n <= BAJO_SORT_NOALLOC_MAX_KEYS; larger n returns BAJO_ERR_TOO_LARGE.  All
+ * calls on a device share that array: calls whose device work overlaps race
+ * and must be serialised by the caller.  The first call on a device looks up
+ * the array's address; make it before any stream capture.  Every call made
+ * outside a capture looks the address up again, so after a device reset the
+ * next uncaptured call uses the reloaded array.  d_status (may be NULL)
+ * receives the BAJO_STATUS_* bits of this call. */
 #define BAJO_SORT_NOALLOC_MAX_KEYS (1u << 20)
+#define BAJO_SORT_NOALLOC_SCRATCH_BYTES 10490368u
 int32_t bajo_sort_pairs_u32_noalloc(uint32_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit,
                                     int32_t end_bit, uint32_t* d_status, void* stream);
 

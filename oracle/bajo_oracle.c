@@ -22,33 +22,82 @@
 #define BO_SLACK 1.00000095367431640625f
 
 /* ------------------------------------------------------------------------- */
-/* tiny thread pool                                                           */
+/* persistent worker pool                                                     */
 /* ------------------------------------------------------------------------- */
+/* The reference's CPU builders run their parallel loops on the Mojo runtime's
+ * persistent worker pool (max.algorithm.parallelize,
+ * bajo/bvh/cpu/builder/lbvh.mojo:87,112,199,354).  This pool is the same
+ * kind of object: worker threads are started once (grown on demand), spin
+ * briefly and then sleep between jobs, and a job hands out [0, n) in chunks
+ * through an atomic counter.  One job runs at a time; a nested call, or a
+ * call from a second host thread while a job runs, executes inline. */
 typedef void (*bo_range_fn)(void* ctx, uint32_t begin, uint32_t end);
 
 typedef struct {
   bo_range_fn fn;
   void* ctx;
-  uint32_t n, chunk;
-  uint32_t next;
-  pthread_mutex_t mu;
+  uint64_t n, chunk;
+  uint64_t next; /* atomic */
 } bo_job;
 
-typedef struct {
-  bo_job* job;
-} bo_worker_arg;
+#define BO_POOL_MAX 256
+#define BO_POOL_SPIN 20000
 
-static void* bo_worker(void* p) {
-  bo_job* job = ((bo_worker_arg*)p)->job;
+static struct {
+  pthread_mutex_t mu;     /* sleeping workers and the submitter's wait */
+  pthread_cond_t wake, done;
+  pthread_mutex_t submit; /* one job at a time */
+  uint32_t started;       /* worker threads running (indices 1..started) */
+  uint64_t state;         /* (generation << 16) | workers taking part; atomic */
+  uint32_t running;       /* workers still inside the current job; atomic */
+  bo_job job;
+  uint64_t start_state[BO_POOL_MAX + 1];
+} g_pool = {PTHREAD_MUTEX_INITIALIZER, PTHREAD_COND_INITIALIZER, PTHREAD_COND_INITIALIZER,
+            PTHREAD_MUTEX_INITIALIZER, 0, 0, 0, {0}, {0}};
+static __thread int bo_in_pool;
+
+static inline void bo_relax(void) {
+#if defined(__x86_64__) || defined(__i386__)
+  __builtin_ia32_pause();
+#endif
+}
+
+static void bo_run_chunks(bo_job* j) {
   for (;;) {
-    uint32_t b;
-    pthread_mutex_lock(&job->mu);
-    b = job->next;
-    if (b < job->n) job->next = (job->n - b > job->chunk) ? b + job->chunk : job->n;
-    pthread_mutex_unlock(&job->mu);
-    if (b >= job->n) break;
-    uint32_t e = (job->n - b > job->chunk) ? b + job->chunk : job->n;
-    job->fn(job->ctx, b, e);
+    uint64_t b = __atomic_fetch_add(&j->next, j->chunk, __ATOMIC_RELAXED);
+    if (b >= j->n) break;
+    uint64_t e = (j->n - b > j->chunk) ? b + j->chunk : j->n;
+    j->fn(j->ctx, (uint32_t)b, (uint32_t)e);
+  }
+}
+
+static void* bo_pool_worker(void* arg) {
+  const uint32_t idx = (uint32_t)(uintptr_t)arg;
+  uint64_t seen = g_pool.start_state[idx];
+  bo_in_pool = 1;
+  for (;;) {
+    uint64_t st;
+    int spins = 0;
+    while ((st = __atomic_load_n(&g_pool.state, __ATOMIC_ACQUIRE)) == seen && spins < BO_POOL_SPIN) {
+      bo_relax();
+      ++spins;
+    }
+    if (st == seen) {
+      pthread_mutex_lock(&g_pool.mu);
+      while ((st = __atomic_load_n(&g_pool.state, __ATOMIC_ACQUIRE)) == seen)
+        pthread_cond_wait(&g_pool.wake, &g_pool.mu);
+      pthread_mutex_unlock(&g_pool.mu);
+    }
+    seen = st;
+    /* generation and participant count are read as one word, so a worker
+     * that slept through a job cannot join the next one twice */
+    if (idx > (uint32_t)(st & 0xFFFFu)) continue;
+    bo_run_chunks(&g_pool.job);
+    if (__atomic_sub_fetch(&g_pool.running, 1u, __ATOMIC_ACQ_REL) == 0) {
+      pthread_mutex_lock(&g_pool.mu);
+      pthread_cond_signal(&g_pool.done);
+      pthread_mutex_unlock(&g_pool.mu);
+    }
   }
   return NULL;
 }
@@ -58,24 +107,75 @@ static void bo_parallel_for(uint32_t n, uint32_t n_threads, uint32_t chunk,
                             bo_range_fn fn, void* ctx) {
   if (n == 0) return;
   if (chunk == 0) chunk = 1;
-  if (n_threads <= 1 || n <= chunk) {
+  if (n_threads > BO_POOL_MAX + 1) n_threads = BO_POOL_MAX + 1;
+  const uint64_t chunks = ((uint64_t)n + chunk - 1) / chunk;
+  uint32_t helpers = (uint32_t)((chunks < n_threads ? chunks : n_threads) - 1);
+  if (helpers == 0 || bo_in_pool || pthread_mutex_trylock(&g_pool.submit) != 0) {
     fn(ctx, 0, n);
     return;
   }
-  if (n_threads > 256) n_threads = 256;
-  bo_job job;
-  job.fn = fn;
-  job.ctx = ctx;
-  job.n = n;
-  job.chunk = chunk;
-  job.next = 0;
-  pthread_mutex_init(&job.mu, NULL);
-  pthread_t th[256];
-  bo_worker_arg arg = {&job};
-  for (uint32_t i = 1; i < n_threads; ++i) pthread_create(&th[i], NULL, bo_worker, &arg);
-  bo_worker(&arg);
-  for (uint32_t i = 1; i < n_threads; ++i) pthread_join(th[i], NULL);
-  pthread_mutex_destroy(&job.mu);
+  const uint64_t cur = __atomic_load_n(&g_pool.state, __ATOMIC_RELAXED);
+  while (g_pool.started < helpers) {
+    pthread_t th;
+    const uint32_t idx = g_pool.started + 1;
+    g_pool.start_state[idx] = cur;
+    if (pthread_create(&th, NULL, bo_pool_worker, (void*)(uintptr_t)idx) != 0) break;
+    pthread_detach(th);
+    g_pool.started = idx;
+  }
+  if (helpers > g_pool.started) helpers = g_pool.started;
+  g_pool.job.fn = fn;
+  g_pool.job.ctx = ctx;
+  g_pool.job.n = n;
+  g_pool.job.chunk = chunk;
+  g_pool.job.next = 0;
+  __atomic_store_n(&g_pool.running, helpers, __ATOMIC_RELAXED);
+  const uint64_t next_state = (((cur >> 16) + 1) << 16) | helpers;
+  pthread_mutex_lock(&g_pool.mu);
+  __atomic_store_n(&g_pool.state, next_state, __ATOMIC_RELEASE);
+  pthread_cond_broadcast(&g_pool.wake);
+  pthread_mutex_unlock(&g_pool.mu);
+  bo_in_pool = 1;
+  bo_run_chunks(&g_pool.job);
+  bo_in_pool = 0;
+  int spins = 0;
+  while (__atomic_load_n(&g_pool.running, __ATOMIC_ACQUIRE) != 0 && spins < BO_POOL_SPIN) {
+    bo_relax();
+    ++spins;
+  }
+  pthread_mutex_lock(&g_pool.mu);
+  while (__atomic_load_n(&g_pool.running, __ATOMIC_ACQUIRE) != 0) pthread_cond_wait(&g_pool.done, &g_pool.mu);
+  pthread_mutex_unlock(&g_pool.mu);
+  pthread_mutex_unlock(&g_pool.submit);
+}
+
+uint32_t bo_minmax_selftest(uint32_t n_random, uint64_t seed) {
+  static const float special[] = {0.0f, -0.0f, 1.0f, -1.0f, INFINITY, -INFINITY, NAN, -NAN,
+                                  FLT_MIN, -FLT_MIN, FLT_MAX, -FLT_MAX, 1.0e-45f, -1.0e-45f};
+  const uint32_t ns = sizeof special / sizeof special[0];
+  uint32_t bad = 0;
+  uint64_t x = seed * 2862933555777941757ull + 3037000493ull;
+  for (uint32_t i = 0; i < ns * ns + n_random; ++i) {
+    float a, b;
+    if (i < ns * ns) {
+      a = special[i / ns];
+      b = special[i % ns];
+    } else {
+      uint32_t ua, ub;
+      x = x * 6364136223846793005ull + 1442695040888963407ull;
+      ua = (uint32_t)(x >> 32);
+      ub = (uint32_t)x;
+      if (i & 1) ub = ua ^ (ub & 0x80000000u); /* equal magnitudes, signs vary */
+      if ((ua & 0x7F800000u) == 0x7F800000u && (ua & 0x007FFFFFu)) ua |= 0x00400000u; /* quiet NaNs only */
+      if ((ub & 0x7F800000u) == 0x7F800000u && (ub & 0x007FFFFFu)) ub |= 0x00400000u;
+      memcpy(&a, &ua, 4);
+      memcpy(&b, &ub, 4);
+    }
+    float r[4] = {bo_fminf(a, b), fminf(a, b), bo_fmaxf(a, b), fmaxf(a, b)};
+    if (memcmp(&r[0], &r[1], 4) != 0 && !(r[0] != r[0] && r[1] != r[1])) ++bad;
+    if (memcmp(&r[2], &r[3], 4) != 0 && !(r[2] != r[2] && r[3] != r[3])) ++bad;
+  }
+  return bad;
 }
 
 /* ------------------------------------------------------------------------- */
@@ -87,8 +187,8 @@ static inline v3 v3make(float x, float y, float z) { v3 r = {x, y, z}; return r;
 static inline v3 v3sub(v3 a, v3 b) { return v3make(a.x - b.x, a.y - b.y, a.z - b.z); }
 static inline v3 v3add(v3 a, v3 b) { return v3make(a.x + b.x, a.y + b.y, a.z + b.z); }
 static inline v3 v3muls(v3 a, float s) { return v3make(a.x * s, a.y * s, a.z * s); }
-static inline v3 v3min(v3 a, v3 b) { return v3make(fminf(a.x, b.x), fminf(a.y, b.y), fminf(a.z, b.z)); }
-static inline v3 v3max(v3 a, v3 b) { return v3make(fmaxf(a.x, b.x), fmaxf(a.y, b.y), fmaxf(a.z, b.z)); }
+static inline v3 v3min(v3 a, v3 b) { return v3make(bo_fminf(a.x, b.x), bo_fminf(a.y, b.y), bo_fminf(a.z, b.z)); }
+static inline v3 v3max(v3 a, v3 b) { return v3make(bo_fmaxf(a.x, b.x), bo_fmaxf(a.y, b.y), bo_fmaxf(a.z, b.z)); }
 /* dot = fma(a.x, b.x, fma(a.y, b.y, a.z * b.z))  -- vec.mojo:440 */
 static inline float v3dot(v3 a, v3 b) { return fmaf(a.x, b.x, fmaf(a.y, b.y, a.z * b.z)); }
 /* cross -- vec.mojo:522-526 */
@@ -392,8 +492,8 @@ static void child_box(uint32_t ref, const float* lb6, const uint32_t* ids, const
   } else {
     const float* b = nb + (size_t)12 * ref;
     for (int k = 0; k < 3; ++k) {
-      out[k] = fminf(b[k], b[6 + k]);
-      out[3 + k] = fmaxf(b[3 + k], b[9 + k]);
+      out[k] = bo_fminf(b[k], b[6 + k]);
+      out[3 + k] = bo_fmaxf(b[3 + k], b[9 + k]);
     }
   }
 }
@@ -583,8 +683,8 @@ static inline int box_hit(const bo_ray* r, const float* b, float tlimit, float* 
   slab(b[0], b[3], r->o.x, r->rcp.x, r->par[0], &t0x, &t1x);
   slab(b[1], b[4], r->o.y, r->rcp.y, r->par[1], &t0y, &t1y);
   slab(b[2], b[5], r->o.z, r->rcp.z, r->par[2], &t0z, &t1z);
-  float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.0f));
-  float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tlimit));
+  float tn = bo_fmaxf(bo_fmaxf(bo_fminf(t0x, t1x), bo_fminf(t0y, t1y)), bo_fmaxf(bo_fminf(t0z, t1z), 0.0f));
+  float tf = bo_fminf(bo_fminf(bo_fmaxf(t0x, t1x), bo_fmaxf(t0y, t1y)), bo_fminf(bo_fmaxf(t0z, t1z), tlimit));
   *tnear = tn;
   return tn <= tf * BO_SLACK;
 }
@@ -815,8 +915,8 @@ void bo_tlas_instance_boxes(const float* seg_bounds, uint32_t n_blas, const floa
         for (int col = 0; col < 3; ++col)
           for (int k = 0; k < 3; ++k) {
             float m = r[4 * k + col], a = m * lb[col], c = m * lb[3 + col];
-            mn[k] = mn[k] + fminf(a, c);
-            mx[k] = mx[k] + fmaxf(a, c);
+            mn[k] = mn[k] + bo_fminf(a, c);
+            mx[k] = mx[k] + bo_fmaxf(a, c);
           }
       }
     }
@@ -1033,8 +1133,8 @@ static bo_hit cwbvh8_one(const float* nodes, const float* tris, uint32_t n_nodes
         /* fmaxf / fminf: the reference's select-based fmax / fmin
          * (bajo/core/utils.mojo:60-70) give the same comparison unless an
          * operand is NaN */
-        float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, 0.0f));
-        float tf = fminf(fminf(tfx, tfy), fminf(tfz, tlim));
+        float tn = bo_fmaxf(bo_fmaxf(tnx, tny), bo_fmaxf(tnz, 0.0f));
+        float tf = bo_fminf(bo_fminf(tfx, tfy), bo_fminf(tfz, tlim));
         uint32_t byte = (w[6 + g] >> sh) & 0xFFu;
         if (byte != 0 && tn <= tf) {
           uint32_t bi = byte & 0x1Fu;
@@ -1173,7 +1273,7 @@ typedef struct {
   BoCpuNode* nodes;
   uint32_t* item_indices;
   const float* bounds6;
-  uint32_t next; /* atomic node allocator */
+  uint32_t next; /* next free node id (frontier collection, then task bases) */
 } cpu_tree_ctx;
 
 static int cp_pairs(const bo_mitem* p, int64_t len, int64_t i, int64_t j) {
@@ -1197,7 +1297,12 @@ static void node_set_box(BoCpuNode* nd, const float* mn, const float* mx) {
 }
 
 /* bajo/bvh/cpu/builder/lbvh.mojo:252-267 (leaf, leaf_size 1) and 401-437 */
-static void cpu_build_rec(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t count) {
+/* Node ids: the reference takes each child pair from one shared atomic
+ * counter (lbvh.mojo:414).  A frontier task over c leaves allocates exactly
+ * 2 (c - 1) nodes, so each task here draws from its own contiguous range
+ * (`next`), assigned in task order: the layout the shared counter produces
+ * when the tasks run one after another, without its cache-line traffic. */
+static void cpu_build_rec(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t count, uint32_t* next) {
   BoCpuNode* nd = &c->nodes[node];
   if (count <= 1) {
     const float* b = c->bounds6 + (size_t)6 * c->item_indices[first];
@@ -1209,25 +1314,26 @@ static void cpu_build_rec(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t
   int64_t last = first + count - 1;
   int64_t split = split_pairs(c->pairs, c->len, first, last);
   int64_t lc = split - first + 1;
-  uint32_t left = __atomic_fetch_add(&c->next, 2u, __ATOMIC_RELAXED);
-  cpu_build_rec(c, left, first, lc);
-  cpu_build_rec(c, left + 1, split + 1, count - lc);
+  uint32_t left = *next;
+  *next += 2u;
+  cpu_build_rec(c, left, first, lc, next);
+  cpu_build_rec(c, left + 1, split + 1, count - lc, next);
   BoCpuNode* L = &c->nodes[left];
   BoCpuNode* R = &c->nodes[left + 1];
   float mn[3], mx[3];
-  for (int k = 0; k < 3; ++k) { mn[k] = fminf(L->bmin[k], R->bmin[k]); mx[k] = fmaxf(L->bmax[k], R->bmax[k]); }
+  for (int k = 0; k < 3; ++k) { mn[k] = bo_fminf(L->bmin[k], R->bmin[k]); mx[k] = bo_fmaxf(L->bmax[k], R->bmax[k]); }
   node_set_box(nd, mn, mx);
   nd->left_or_first = left;
   nd->count = 0;
 }
 
-typedef struct { uint32_t node; int64_t first, count; } frontier_task;
+typedef struct { uint32_t node; int64_t first, count; uint32_t base; } frontier_task;
 typedef struct { cpu_tree_ctx* t; frontier_task* tasks; } frontier_ctx;
 
 static void cpu_collect(cpu_tree_ctx* c, uint32_t node, int64_t first, int64_t count, int depth,
                         frontier_task* out, uint32_t* n_out) {
   if (count <= 1 || depth == 0) {
-    out[(*n_out)++] = (frontier_task){node, first, count};
+    out[(*n_out)++] = (frontier_task){node, first, count, 0};
     return;
   }
   int64_t last = first + count - 1;
@@ -1246,7 +1352,8 @@ static void frontier_worker(void* p, uint32_t b, uint32_t e) {
   for (uint32_t k = b; k < e; ++k) {
     frontier_task t = f->tasks[k];
     for (int64_t i = t.first; i < t.first + t.count; ++i) f->t->item_indices[i] = f->t->pairs[i].item;
-    cpu_build_rec(f->t, t.node, t.first, t.count);
+    uint32_t next = t.base;
+    cpu_build_rec(f->t, t.node, t.first, t.count, &next);
   }
 }
 
@@ -1257,46 +1364,70 @@ static void refit_frontier(BoCpuNode* nodes, uint32_t node, int depth) {
   refit_frontier(nodes, l, depth - 1);
   refit_frontier(nodes, l + 1, depth - 1);
   for (int k = 0; k < 3; ++k) {
-    nd->bmin[k] = fminf(nodes[l].bmin[k], nodes[l + 1].bmin[k]);
-    nd->bmax[k] = fmaxf(nodes[l].bmax[k], nodes[l + 1].bmax[k]);
+    nd->bmin[k] = bo_fminf(nodes[l].bmin[k], nodes[l + 1].bmin[k]);
+    nd->bmax[k] = bo_fmaxf(nodes[l].bmax[k], nodes[l + 1].bmax[k]);
   }
 }
 
-typedef struct { const float* b6; uint32_t n; float* part; } cbounds_ctx;
+/* Scratch of one build: leaf bounds, Morton pairs and their sort buffer, and
+ * the per-worker radix histograms and offsets (256 each). */
+static size_t cpu_scratch_layout(uint32_t n, uint32_t workers, size_t* off_pairs, size_t* off_scratch,
+                                 size_t* off_counts, size_t* off_offsets) {
+  size_t o = ((sizeof(float) * 6 * (size_t)n) + 63) & ~(size_t)63;
+  *off_pairs = o;
+  o += (sizeof(bo_mitem) * (size_t)n + 63) & ~(size_t)63;
+  *off_scratch = o;
+  o += (sizeof(bo_mitem) * (size_t)n + 63) & ~(size_t)63;
+  *off_counts = o;
+  o += sizeof(uint32_t) * 256 * (size_t)workers;
+  *off_offsets = o;
+  o += sizeof(uint32_t) * 256 * (size_t)workers;
+  return o;
+}
+
+size_t bo_cpu_lbvh_scratch_bytes(uint32_t n, uint32_t n_threads) {
+  size_t a, b, c, d;
+  if (n_threads == 0) n_threads = 1;
+  return cpu_scratch_layout(n, n_threads < n ? n_threads : (n ? n : 1), &a, &b, &c, &d);
+}
 
 /* bajo/bvh/cpu/builder/lbvh.mojo:166-216 + 318-359 */
-uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads, BoCpuNode* nodes,
-                           uint32_t* item_indices) {
+uint32_t bo_cpu_build_lbvh_scratch(const float* verts, uint32_t n, uint32_t n_threads, BoCpuNode* nodes,
+                                   uint32_t* item_indices, void* scratch) {
   if (n == 0) return 0;
   if (n_threads == 0) n_threads = 1;
+  uint32_t workers = n_threads < n ? n_threads : n;
+  size_t off_pairs, off_scratch, off_counts, off_offsets;
+  cpu_scratch_layout(n, workers, &off_pairs, &off_scratch, &off_counts, &off_offsets);
+  unsigned char* sb = (unsigned char*)scratch;
   cpu_build_ctx c;
   memset(&c, 0, sizeof c);
   c.verts = verts;
   c.n = n;
-  c.bounds6 = (float*)malloc(sizeof(float) * 6 * (size_t)n);
+  c.bounds6 = (float*)sb;
   bo_parallel_for(n, n_threads, 8192, cb_bounds, &c);
-  /* centroid bounds (grown serially, as _sorted_morton_pairs does) */
+  /* centroid bounds grown serially over the items, as
+   * update_node_bounds_and_centroid_bounds does (builder.mojo:133-147) */
   float cmn[3] = {BO_FLT_MAX, BO_FLT_MAX, BO_FLT_MAX}, cmx[3] = {-BO_FLT_MAX, -BO_FLT_MAX, -BO_FLT_MAX};
   for (uint32_t i = 0; i < n; ++i) {
     const float* b = c.bounds6 + (size_t)6 * i;
     for (int k = 0; k < 3; ++k) {
       float cc = (b[k] + b[3 + k]) * 0.5f;
-      cmn[k] = fminf(cmn[k], cc);
-      cmx[k] = fmaxf(cmx[k], cc);
+      cmn[k] = bo_fminf(cmn[k], cc);
+      cmx[k] = bo_fmaxf(cmx[k], cc);
     }
   }
   for (int k = 0; k < 3; ++k) { c.cmin[k] = cmn[k]; c.inv[k] = safe_inv1(cmx[k] - cmn[k]); }
-  bo_mitem* pairs = (bo_mitem*)malloc(sizeof(bo_mitem) * n);
-  bo_mitem* scratch = (bo_mitem*)malloc(sizeof(bo_mitem) * n);
+  bo_mitem* pairs = (bo_mitem*)(sb + off_pairs);
+  bo_mitem* scratch_pairs = (bo_mitem*)(sb + off_scratch);
   c.pairs = pairs;
   bo_parallel_for(n, n_threads, 8192, cb_morton, &c);
   /* stable LSD radix over the 32-bit code, workers over contiguous chunks */
-  uint32_t workers = n_threads < n ? n_threads : n;
   c.workers = workers;
-  c.counts = (uint32_t*)malloc(sizeof(uint32_t) * 256 * workers);
-  c.offsets = (uint32_t*)malloc(sizeof(uint32_t) * 256 * workers);
+  c.counts = (uint32_t*)(sb + off_counts);
+  c.offsets = (uint32_t*)(sb + off_offsets);
   bo_mitem* src = pairs;
-  bo_mitem* dst = scratch;
+  bo_mitem* dst = scratch_pairs;
   for (int sh = 0; sh < 32; sh += 8) {
     c.src = src;
     c.dst = dst;
@@ -1319,15 +1450,23 @@ uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads, B
   frontier_task tasks[16];
   uint32_t nt = 0;
   cpu_collect(&t, 0, 0, n, 3, tasks, &nt);
+  for (uint32_t k = 0; k < nt; ++k) {
+    tasks[k].base = t.next;
+    t.next += tasks[k].count > 1 ? 2u * (uint32_t)(tasks[k].count - 1) : 0u;
+  }
   frontier_ctx f = {&t, tasks};
   bo_parallel_for(nt, n_threads, 1, frontier_worker, &f);
   refit_frontier(nodes, 0, 3);
-  uint32_t used = t.next;
-  free(c.counts);
-  free(c.offsets);
-  free(pairs);
+  return t.next;
+}
+
+uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads, BoCpuNode* nodes,
+                           uint32_t* item_indices) {
+  if (n == 0) return 0;
+  void* scratch = malloc(bo_cpu_lbvh_scratch_bytes(n, n_threads));
+  if (!scratch) return 0;
+  uint32_t used = bo_cpu_build_lbvh_scratch(verts, n, n_threads, nodes, item_indices, scratch);
   free(scratch);
-  free(c.bounds6);
   return used;
 }
 
@@ -1532,9 +1671,9 @@ static bo_bsdf sample_metal(v3 d, v3 normal, v3 albedo, float fuzz, float u, flo
     r.ok = v3dot(reflected, normal) > 0.0f;
     return r;
   }
-  float exponent = fmaxf(2.0f / (fuzz * fuzz) - 2.0f, 0.0f);
+  float exponent = bo_fmaxf(2.0f / (fuzz * fuzz) - 2.0f, 0.0f);
   float cos_t = series_pow(u, 1.0f / (exponent + 1.0f));
-  float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+  float sin_t = sqrtf(bo_fmaxf(1.0f - cos_t * cos_t, 0.0f));
   float sp, cp;
   bo_rt_sincos_turns(v, &sp, &cp);
   v3 helper = fabsf(reflected.y) > 0.99f ? v3make(1.0f, 0.0f, 0.0f) : v3make(0.0f, 1.0f, 0.0f);
@@ -1544,12 +1683,12 @@ static bo_bsdf sample_metal(v3 d, v3 normal, v3 albedo, float fuzz, float u, flo
                              v3muls(reflected, cos_t)));
   v3 dn = v3normalize(dir);
   int surface_valid = v3dot(normal, dn) > 0.0f;
-  float lobe_cos = fmaxf(v3dot(reflected, dn), 0.0f);
+  float lobe_cos = bo_fmaxf(v3dot(reflected, dn), 0.0f);
   float lobe = series_pow(lobe_cos, exponent);
   int valid = surface_valid && lobe_cos > 0.0f;
   float value_scale = valid ? ((exponent + 2.0f) * lobe) / 6.28318531f : 0.0f;
   float pdf = valid ? ((exponent + 1.0f) * lobe) / 6.28318531f : 0.0f;
-  float scos = fmaxf(v3dot(normal, dir), 0.0f);
+  float scos = bo_fmaxf(v3dot(normal, dir), 0.0f);
   r.ok = pdf > 0.0f && scos > 0.0f;
   float scale = scos / (r.ok ? pdf : 1.0f);
   r.dir = dir;
@@ -1564,8 +1703,8 @@ static bo_bsdf sample_dielectric(v3 d, v3 normal, float ior, int front, float u)
   bo_bsdf r;
   float ri = front ? 1.0f / ior : ior;
   v3 ud = v3normalize(d);
-  float cos_t = fminf(v3dot(vneg(ud), normal), 1.0f);
-  float sin_t = sqrtf(fmaxf(1.0f - cos_t * cos_t, 0.0f));
+  float cos_t = bo_fminf(v3dot(vneg(ud), normal), 1.0f);
+  float sin_t = sqrtf(bo_fmaxf(1.0f - cos_t * cos_t, 0.0f));
   int cannot = ri * sin_t > 1.0f;
   float root = (1.0f - ri) / (1.0f + ri);
   float r2 = root * root;
@@ -1578,7 +1717,7 @@ static bo_bsdf sample_dielectric(v3 d, v3 normal, float ior, int front, float u)
   if (rs) {
     out = v3reflect(ud, normal);
   } else {
-    float ct = fminf(v3dot(vneg(ud), normal), 1.0f);
+    float ct = bo_fminf(v3dot(vneg(ud), normal), 1.0f);
     v3 perp = v3make(ri * (ud.x + ct * normal.x), ri * (ud.y + ct * normal.y), ri * (ud.z + ct * normal.z));
     float par = -sqrtf(fabsf(1.0f - v3dot(perp, perp)));
     out = v3make(perp.x + par * normal.x, perp.y + par * normal.y, perp.z + par * normal.z);
@@ -1605,7 +1744,7 @@ int bo_rt_build_lights(const float* v, const uint32_t* surf, uint32_t n, const f
     v3 c = v3cross(e1, e2);
     float area = 0.5f * sqrtf(v3dot(c, c));
     const float* L = em + 3 * (size_t)(surf[i] & 0x0FFFFFFFu);
-    float imp = fmaxf(((L[0] + L[1]) + L[2]) / 3.0f, 0.0f);
+    float imp = bo_fmaxf(((L[0] + L[1]) + L[2]) / 3.0f, 0.0f);
     float wt = area * imp;
     if (wt > 0.0f) {
       total += wt;
@@ -1756,7 +1895,7 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
         float wgt = 1.0f;
         if (c->algorithm == 3 && b > 0 && !delta) wgt = 0.0f;
         if (c->algorithm == 4 && b > 0 && !delta) {
-          float lc = fmaxf(v3dot(normal, vneg(v3normalize(d))), 0.0f);
+          float lc = bo_fmaxf(v3dot(normal, vneg(v3normalize(d))), 0.0f);
           float lpdf = 0.0f;
           if (lc > 0.0f && c->total_weight > 0.0f) {
             float d2 = (t * t) * v3dot(d, d);
@@ -1785,9 +1924,9 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
       if (!sm.ok) break;
       v3 Tm = vmul(T, sm.weight);
       if (b + 1 >= 5u) {
-        float mm = fmaxf(Tm.x, fmaxf(Tm.y, Tm.z));
+        float mm = bo_fmaxf(Tm.x, bo_fmaxf(Tm.y, Tm.z));
         if (mm <= 0.0f) break;
-        float survival = fminf(fmaxf(mm, 0.05f), 0.95f);
+        float survival = bo_fminf(bo_fmaxf(mm, 0.05f), 0.95f);
         float rr[4];
         bo_rt_uniform4(c->seed, path_id, st_roulette(b), rr);
         if (rr[0] >= survival) break;
@@ -1824,13 +1963,13 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
         if (d2 > 1.0e-8f) {
           float dist = sqrtf(d2);
           v3 dir = vdivs(tl, dist);
-          float scos = fmaxf(v3dot(normal, dir), 0.0f);
-          float lcos = fmaxf(v3dot(ln, vneg(dir)), 0.0f);
+          float scos = bo_fmaxf(v3dot(normal, dir), 0.0f);
+          float lcos = bo_fmaxf(v3dot(ln, vneg(dir)), 0.0f);
           float smax = dist - 0.002f;
           if (scos > 0.0f && lcos > 0.0f && smax > 0.001f) {
             v3 E = load3(lrec + 9);
             float lpdf = (d2 * ((E.x + E.y) + E.z)) / ((3.0f * lcos) * c->total_weight);
-            float bpdf = fmaxf(v3dot(normal, v3normalize(dir)), 0.0f) * BO_INV_PI;
+            float bpdf = bo_fmaxf(v3dot(normal, v3normalize(dir)), 0.0f) * BO_INV_PI;
             if (lpdf > 0.0f && bpdf > 0.0f) {
               float wgt = c->algorithm == 4 ? power_heuristic(lpdf, bpdf) : 1.0f;
               float scale = (scos * wgt) / lpdf;
@@ -1855,18 +1994,18 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
       float s2, c2;
       bo_rt_sincos_turns(u[0], &s2, &c2);
       float z = 1.0f - 2.0f * u[1];
-      float radius = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+      float radius = sqrtf(bo_fmaxf(1.0f - z * z, 0.0f));
       v3 sd = v3add(normal, v3make(radius * c2, radius * s2, z));
       if (fabsf(sd.x) < 1.0e-8f && fabsf(sd.y) < 1.0e-8f && fabsf(sd.z) < 1.0e-8f) sd = normal;
       nd = v3normalize(sd);
-      pdf = fmaxf(v3dot(normal, v3normalize(nd)), 0.0f) * BO_INV_PI;
+      pdf = bo_fmaxf(v3dot(normal, v3normalize(nd)), 0.0f) * BO_INV_PI;
       Tn = vmul(T, albedo);
       alive = 1;
       if (b + 1 >= 5u) {
-        float m = fmaxf(Tn.x, fmaxf(Tn.y, Tn.z));
+        float m = bo_fmaxf(Tn.x, bo_fmaxf(Tn.y, Tn.z));
         if (m <= 0.0f) alive = 0;
         else {
-          float survival = fminf(fmaxf(m, 0.05f), 0.95f);
+          float survival = bo_fminf(bo_fmaxf(m, 0.05f), 0.95f);
           float rr[4];
           bo_rt_uniform4(c->seed, path_id, st_roulette(b), rr);
           if (rr[0] >= survival) alive = 0;
@@ -1928,7 +2067,7 @@ static v3 lambertian_dir(v3 normal, float u, float v) {
   float st, ct;
   bo_rt_sincos_turns(u, &st, &ct);
   float z = 1.0f - 2.0f * v;
-  float rad = sqrtf(fmaxf(1.0f - z * z, 0.0f));
+  float rad = sqrtf(bo_fmaxf(1.0f - z * z, 0.0f));
   v3 sd = v3add(normal, v3make(rad * ct, rad * st, z));
   if (fabsf(sd.x) < 1.0e-8f && fabsf(sd.y) < 1.0e-8f && fabsf(sd.z) < 1.0e-8f) sd = normal;
   return v3normalize(sd);

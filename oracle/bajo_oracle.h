@@ -25,6 +25,35 @@
 extern "C" {
 #endif
 
+/* Inline min / max.  bo_fminf / bo_fmaxf give C99 fminf / fmaxf results for
+ * every quiet operand: the smaller (larger) of two numbers as `a < b ? a : b`
+ * (`a > b ? a : b`), which is the reference's fmin / fmax
+ * (bajo/core/utils.mojo:60-70), and the other operand when one is NaN.  On
+ * x86-64 they are branch free (SSE minss / maxss, whose unordered and equal
+ * cases return the second operand, plus a NaN mask on b); without
+ * -ffast-math the compiler would otherwise call libm or branch per compare,
+ * which cost the CPU builder most of its time. */
+#if defined(__x86_64__) || defined(__SSE2__)
+#include <emmintrin.h>
+static inline float bo_fminf(float a, float b) {
+  const __m128 va = _mm_set_ss(a), vb = _mm_set_ss(b);
+  const __m128 nan_b = _mm_cmpunord_ss(vb, vb);
+  return _mm_cvtss_f32(_mm_or_ps(_mm_and_ps(nan_b, va), _mm_andnot_ps(nan_b, _mm_min_ss(va, vb))));
+}
+static inline float bo_fmaxf(float a, float b) {
+  const __m128 va = _mm_set_ss(a), vb = _mm_set_ss(b);
+  const __m128 nan_b = _mm_cmpunord_ss(vb, vb);
+  return _mm_cvtss_f32(_mm_or_ps(_mm_and_ps(nan_b, va), _mm_andnot_ps(nan_b, _mm_max_ss(va, vb))));
+}
+#else
+static inline float bo_fminf(float a, float b) { return b != b ? a : (a < b ? a : b); }
+static inline float bo_fmaxf(float a, float b) { return b != b ? a : (a > b ? a : b); }
+#endif
+/* Number of (a, b) pairs over special and random values (signalling NaNs
+ * excluded: libm quiets them) where bo_fminf / bo_fmaxf differ from libm's
+ * fminf / fmaxf bit for bit (0 = identical). */
+uint32_t bo_minmax_selftest(uint32_t n_random, uint64_t seed);
+
 #define BO_SENTINEL 0xFFFFFFFFu   /* LBVH_SENTINEL, bajo/bvh/constants.mojo:6 */
 #define BO_LEAF_FLAG 0x80000000u  /* _BVH_LEAF_FLAG, bajo/bvh/tagged_ref.mojo:3 */
 #define BO_EMPTY 0xFFFFFFFFu      /* EMPTY_LANE / MISS_PRIM, constants.mojo:19-20 */
@@ -151,6 +180,12 @@ typedef struct BoCpuNode {
 uint32_t bo_cpu_build_lbvh(const float* verts, uint32_t n, uint32_t n_threads,
                            BoCpuNode* nodes /* 2n-1 */,
                            uint32_t* item_indices /* n */);
+/* The same build into caller-owned scratch of bo_cpu_lbvh_scratch_bytes(n,
+ * n_threads) bytes (no allocation inside the build, as the reference keeps
+ * its builder's buffers across rebuilds). */
+size_t bo_cpu_lbvh_scratch_bytes(uint32_t n, uint32_t n_threads);
+uint32_t bo_cpu_build_lbvh_scratch(const float* verts, uint32_t n, uint32_t n_threads,
+                                   BoCpuNode* nodes, uint32_t* item_indices, void* scratch);
 void bo_cpu_trace(const BoCpuNode* nodes, const uint32_t* item_indices,
                   const float* verts, const float* rays_soa, uint32_t n_rays,
                   int tri_mode, float* hits8, uint32_t n_threads);

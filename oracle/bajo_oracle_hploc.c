@@ -58,8 +58,8 @@ static uint32_t cluster_leaves(const hctx* c, uint32_t ref) {
 
 static void unite(const float a[6], const float b[6], float out[6]) {
   for (int k = 0; k < 3; ++k) {
-    out[k] = fminf(a[k], b[k]);
-    out[3 + k] = fmaxf(a[3 + k], b[3 + k]);
+    out[k] = bo_fminf(a[k], b[k]);
+    out[3 + k] = bo_fmaxf(a[3 + k], b[3 + k]);
   }
 }
 

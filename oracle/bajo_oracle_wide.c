@@ -67,8 +67,8 @@ static void ref_box(const wctx* c, uint32_t ref, float out[6]) {
   } else {
     const float* p = c->b->node_bounds + (size_t)(ref & IDX_MASK) * 12;
     for (int k = 0; k < 3; ++k) {
-      out[k] = fminf(p[k], p[6 + k]);
-      out[3 + k] = fmaxf(p[3 + k], p[9 + k]);
+      out[k] = bo_fminf(p[k], p[6 + k]);
+      out[3 + k] = bo_fmaxf(p[3 + k], p[9 + k]);
     }
   }
 }

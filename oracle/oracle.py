@@ -84,6 +84,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_trace_brute": (None, [_P, _U32, _P, _U32, _I, _P, _U32]),
         "bo_trace_bvh2_stats": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _I, _P]),
         "bo_cpu_build_lbvh": (_U32, [_P, _U32, _U32, _P, _P]),
+        "bo_cpu_lbvh_scratch_bytes": (ctypes.c_size_t, [_U32, _U32]),
+        "bo_cpu_build_lbvh_scratch": (_U32, [_P, _U32, _U32, _P, _P, _P]),
         "bo_cpu_trace": (None, [_P, _P, _P, _P, _U32, _I, _P, _U32]),
         "bo_rt_philox4x32_10": (None, [_P, _P, _P]),
         "bo_trace_batch": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _U32, _U32, ctypes.c_uint64, _I, _P, _P, _P,
@@ -398,11 +400,13 @@ class CpuLbvh:
         self.threads = threads or n_threads()
         self.nodes = np.zeros(max(2 * self.n - 1, 1), self.NODE_DTYPE)
         self.items = np.zeros(max(self.n, 1), np.uint32)
+        # the builder's buffers live as long as the builder (no allocation per build)
+        self.scratch = np.zeros(max(int(lib().bo_cpu_lbvh_scratch_bytes(self.n, self.threads)), 1), np.uint8)
         self.node_count = 0
 
     def build(self) -> int:
-        self.node_count = lib().bo_cpu_build_lbvh(_ptr(self.verts), self.n, self.threads, _ptr(self.nodes),
-                                                  _ptr(self.items))
+        self.node_count = lib().bo_cpu_build_lbvh_scratch(_ptr(self.verts), self.n, self.threads, _ptr(self.nodes),
+                                                          _ptr(self.items), _ptr(self.scratch))
         return self.node_count
 
     def trace(self, rays_soa: np.ndarray, tri_mode=TRI_WATERTIGHT, hits=None) -> np.ndarray:

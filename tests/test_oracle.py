@@ -244,3 +244,28 @@ def test_cpu_baseline_builder_traces_like_oracle(oracle):
         a, c = oracle.trace_bvh2(b, rays, mode), cb.trace(rays, mode)
         assert np.array_equal(oracle.hits_prim(a), oracle.hits_prim(c))
         assert np.array_equal(oracle.hits_t(a).view(np.uint32), oracle.hits_t(c).view(np.uint32))
+
+
+def test_cpu_baseline_builder_same_tree_on_any_thread_count(oracle):
+    """The timed CPU builder's node ids come from per-task ranges assigned in
+    frontier order, so the whole node array is the same at every thread count
+    (and equal to the serial run of the reference's shared-counter order)."""
+    v = scenes.random_triangles(50000, seed=3)
+    ref = oracle.CpuLbvh(v, threads=1)
+    ref.build()
+    for threads in (2, 3, 8, 16):
+        cb = oracle.CpuLbvh(v, threads=threads)
+        for _ in range(3):  # repeated builds reuse the builder's scratch
+            assert cb.build() == 2 * 50000 - 1
+            assert cb.nodes.tobytes() == ref.nodes.tobytes()
+            assert np.array_equal(cb.items, ref.items)
+
+
+def test_inline_min_max_match_libm(oracle):
+    """bo_fminf / bo_fmaxf (branch-free min / max used across the oracle)
+    return libm's fminf / fmaxf bits on signed zeros, infinities, quiet NaNs,
+    subnormals and random pairs."""
+    import ctypes
+    f = oracle.lib().bo_minmax_selftest
+    f.restype, f.argtypes = ctypes.c_uint32, [ctypes.c_uint32, ctypes.c_uint64]
+    assert f(1 << 20, 11) == 0
