@@ -27,6 +27,44 @@ def clustered_points(n: int, seed: int = 0, clusters: int = 32, sigma: float = 0
     return np.clip(p, 0.0, 1.0).astype(np.float32)
 
 
+def clustered_points_torch(n: int, seed: int = 0, clusters: int = 32, sigma: float = 0.02, device="cuda"):
+    """Points in `clusters` Gaussian clusters (sigma) clipped to the unit cube,
+    generated on `device` with a seeded torch generator (the sort workload's
+    points at up to 2^28 keys, too many for a host generator)."""
+    import torch
+    g = torch.Generator(device=device).manual_seed(seed)
+    centers = torch.rand((clusters, 3), generator=g, device=device)
+    which = torch.randint(0, clusters, (n,), generator=g, device=device)
+    p = centers[which]
+    del which
+    p += torch.randn((n, 3), generator=g, device=device) * sigma
+    return p.clamp_(0.0, 1.0)
+
+
+def _expand_bits_21_torch(v):
+    v = v & 0x1FFFFF
+    v = (v | (v << 32)) & 0x001F00000000FFFF
+    v = (v | (v << 16)) & 0x001F0000FF0000FF
+    v = (v | (v << 8)) & 0x100F00F00F00F00F
+    v = (v | (v << 4)) & 0x10C30C30C30C30C3
+    v = (v | (v << 2)) & 0x1249249249249249
+    return v
+
+
+def morton63_torch(points):
+    """63-bit Morton codes (21 bits per axis, e(z) << 2 | e(y) << 1 | e(x)) of
+    points in the unit cube, as int64 holding the unsigned code: per axis
+    u = clamp(trunc(c * 2^21), 0, 2^21 - 1)."""
+    import torch
+    code = None
+    for axis, shift in ((2, 2), (1, 1), (0, 0)):
+        q = (points[:, axis] * 2097152.0).clamp_(0.0, 2097151.0).to(torch.int64)
+        e = _expand_bits_21_torch(q) << shift
+        code = e if code is None else code.bitwise_or_(e)
+        del q, e
+    return code
+
+
 def uniform_u32(n: int, seed: int = 0) -> np.ndarray:
     rng = np.random.default_rng(seed)
     return rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)

@@ -88,6 +88,7 @@ def parse_args(argv=None):
     p.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU baseline sample length")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--no-extras", action="store_true", help="skip the render, batched and guided workloads")
     p.add_argument("--case", default=None,
                    choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tlas", "tune", "render",
                             "batched", "guided", "guided_pass"],
@@ -414,6 +415,7 @@ def run_bajo(args):
     pass_bytes = PASS_BYTES_PER_KEY * N_TRIS
     achieved = pass_bytes / pass_avg_s / 1e9
     traffic = committed_traffic().get("onesweep_pass_65536")
+    trace_dram = committed_traffic().get("trace_camera_65536")
 
     # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
     stats = torch.empty(5 * n_rays, dtype=torch.int32, device=dev)
@@ -425,46 +427,86 @@ def run_bajo(args):
     trace_bytes = n_rays * (nodes_per_ray * NODE_BYTES + tris_per_ray * TRI_BYTES + HIT_BYTES)
     trace_achieved = trace_bytes / (statistics.mean(trace_ms) / 1e3) / 1e9
 
-    # ---- e2e through the public API: upload, build, read back root bounds + status
-    pinned_v = torch.from_numpy(verts_h).pin_memory()
-    out_h = torch.empty(12, dtype=torch.float32).pin_memory()
+    # ---- e2e through the public API: every step uploads its vertices from
+    # pinned host memory, builds through bajo_lbvh_build and reads the root
+    # child boxes back.  Pipelined as a host would drive the C ABI: the upload
+    # of step k+1 runs on a copy stream into the other of two device vertex
+    # buffers while step k builds; the read-back follows each build on the
+    # build stream.  The serialised form (one stream, step after step) is
+    # reported beside it.
+    pinned_v = [torch.from_numpy(verts_h).pin_memory() for _ in range(2)]
+    out_h = [torch.empty(12, dtype=torch.float32).pin_memory() for _ in range(2)]
     st_h = torch.empty(1, dtype=torch.int32).pin_memory()
-    e2e_v = torch.empty_like(verts)
+    dev_v = [torch.empty_like(verts) for _ in range(2)]
     c_e2e = tree.c_struct(stage_top=False)  # the C-ABI call a host makes, with its tree record prepared once
     root_box = tree.node_bounds[:12]
     status_word = ws.buffer[:4].view(torch.int32)
+    copy_stream = torch.cuda.Stream()
+    uploaded = [torch.cuda.Event() for _ in range(2)]
+    consumed = [torch.cuda.Event() for _ in range(2)]
 
-    def e2e_step():
-        e2e_v.copy_(pinned_v, non_blocking=True)
-        _lib.check(L.bajo_lbvh_build(e2e_v.data_ptr(), ctypes.byref(c_e2e), ws.buffer.data_ptr(), ws.buffer.numel(),
-                                     sh), "bajo_lbvh_build")
-        out_h.copy_(root_box, non_blocking=True)
+    def e2e_build(k):
+        _lib.check(L.bajo_lbvh_build(dev_v[k % 2].data_ptr(), ctypes.byref(c_e2e), ws.buffer.data_ptr(),
+                                     ws.buffer.numel(), sh), "bajo_lbvh_build")
+        out_h[k % 2].copy_(root_box, non_blocking=True)
 
-    for _ in range(2):
-        e2e_step()
+    def e2e_pipelined(steps):
+        for k in range(steps):
+            b = k % 2
+            with torch.cuda.stream(copy_stream):
+                copy_stream.wait_event(consumed[b])  # the build that read this buffer is done
+                dev_v[b].copy_(pinned_v[b], non_blocking=True)
+                uploaded[b].record(copy_stream)
+            stream.wait_event(uploaded[b])
+            e2e_build(k)
+            consumed[b].record(stream)
+
+    def e2e_serial(k):
+        dev_v[0].copy_(pinned_v[0], non_blocking=True)
+        e2e_build(0)
+
+    for b in range(2):
+        consumed[b].record(stream)
+    e2e_pipelined(4)
+    for k in range(2):
+        e2e_serial(k)
     torch.cuda.synchronize()
     barrier(world)
+    flush.zero_()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e2e_ms = []
-    for _ in range(args.steps):
+    e_start.record(stream)
+    copy_stream.wait_stream(stream)
+    e2e_pipelined(args.steps)
+    e_end.record(stream)
+    e_end.synchronize()
+    e2e_total = max_over_ranks(world, e_start.elapsed_time(e_end) / 1e3)
+    serial_ms = []
+    for k in range(args.steps):
         flush.zero_()
         e_start.record(stream)
-        e2e_step()
+        e2e_serial(k)
         e_end.record(stream)
         e_end.synchronize()
-        e2e_ms.append(e_start.elapsed_time(e_end))
+        serial_ms.append(e_start.elapsed_time(e_end))
     # the device status word is sticky (every error sets a bit and nothing
     # clears it between builds), so one read after the timed steps checks them all
     st_h.copy_(status_word)
     if int(st_h.item()) != 0:
         raise RuntimeError(f"device status {int(st_h.item())}")
-    e2e_total = max_over_ranks(world, sum(e2e_ms) / 1e3)
     e2e_value = world * N_TRIS * args.steps / e2e_total / 1e6
+    serial_total = max_over_ranks(world, sum(serial_ms) / 1e3)
+    e2e_serial_value = world * N_TRIS * args.steps / serial_total / 1e6
 
     # ---- sweep (sort and build at larger sizes), rank 0 only
     sweep = None
-    if rank == 0 and not args.no_sweep:
+    if rank == 0 and world == 1 and not args.no_sweep:
         sweep = run_sweep(torch, bvh, _lib, L, dev, stream, peak)
+        if not args.no_cpu_baseline:
+            sweep["cpu_baseline"] = cpu_sort_baseline(torch, dev)
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = run_extras(args, local)
 
     if rank != 0:
         barrier(world)
@@ -480,7 +522,11 @@ def run_bajo(args):
         "sort_passes": passes,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
                 "d2h_bytes_per_step": 12 * 4,
-                "what": "pinned H2D of the vertices + build + D2H of the root child boxes (device status read once after the timed steps)"},
+                "what": "every step: pinned H2D of its vertices + bajo_lbvh_build + D2H of the root child boxes; "
+                        "uploads on a copy stream into two device buffers overlap the previous step's build; "
+                        "one event pair around all steps (device status read once after them)",
+                "serial_value": round(e2e_serial_value, 3),
+                "serial_what": "the same steps on one stream, one after another, each timed alone"},
         "roofline": {"kernel": "onesweep digit pass (u64 key + u32 id)", "bound": "hbm",
                      "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
@@ -492,7 +538,14 @@ def run_bajo(args):
                         "nodes_per_ray": round(nodes_per_ray, 3), "tris_per_ray": round(tris_per_ray, 3),
                         "roofline": {"bound": "hbm (instrumented bytes: node + triangle loads, mostly L2)",
                                      "achieved": round(trace_achieved, 2), "peak": peak, "unit": "GB/s",
-                                     "frac": round(trace_achieved / peak, 4)}},
+                                     "frac": round(trace_achieved / peak, 4),
+                                     "dram_bytes_per_launch": trace_dram,
+                                     "dram_frac": None if trace_dram is None else round(
+                                         trace_dram / (statistics.mean(trace_ms) / 1e3) / 1e9 / peak, 4),
+                                     "target_basis": "frac (instrumented node + triangle bytes served from "
+                                                     "L1/L2/DRAM) is the figure compared with the 40% target; "
+                                                     "dram_frac (ncu DRAM bytes of one launch) shows the tree "
+                                                     "is cache resident"}},
         "gpu_launches": args.steps * (kernels_per_build + 1),
         "clocks": clocks.summary(),
     }
@@ -506,22 +559,51 @@ def run_bajo(args):
             line["closest_hit"]["cpu_baseline"] = {"error": str(e)}
     if sweep:
         line["sweep"] = sweep
+    line.update(extras)
     print(json.dumps(line), flush=True)
     barrier(world)
 
 
-def run_sweep(torch, bvh, _lib, L, dev, stream, peak):
-    """Throughput at larger sizes: sort (u32 pairs, u64/u32 pairs) and build."""
+# Radix sort sweep workload: N = 2^16 ... 2^28 in powers of 4; uniform u32
+# keys (keys only, and with u32 payloads) and 63-bit Morton keys of points in
+# 32 Gaussian clusters (sigma 0.02) with u32 payloads.  Algorithmic bytes per
+# key (read + write of every live pass, plus one histogram read of the keys):
+# u32 keys 4 x 8 + 4 = 36; u32 pairs 4 x 16 + 4 = 68; u64 keys + u32 payload
+# over 63 live bits 8 x 24 + 8 = 200.
+SWEEP_LOG2 = (16, 18, 20, 22, 24, 26, 28)
+SWEEP_KINDS = {"sort_u32_keys": (36, False), "sort_u32_pairs": (68, True), "sort_u64_morton_pairs": (200, True)}
+CPU_SORT_LOG2 = 22
+
+
+def sweep_keys(torch, kind, n, seed, dev):
+    """(keys, begin_bit, end_bit) of one sweep point, generated on the device."""
+    from bajo_b200 import scenes
+    if kind == "sort_u64_morton_pairs":
+        p = scenes.clustered_points_torch(n, seed=seed, device=dev)
+        k = scenes.morton63_torch(p)
+        del p
+        return k, 0, 63
+    g = torch.Generator(device=dev).manual_seed(seed)
+    return torch.randint(-2**31, 2**31, (n,), dtype=torch.int32, device=dev, generator=g), 0, 32
+
+
+def run_sweep(torch, bvh, _lib, L, dev, stream, peak, reps=7):
+    """Throughput of the sort sweep workload at every stated size and key
+    kind, and of the LBVH build at larger sizes.  Each timed sample restores
+    the unsorted keys and flushes L2 outside the event pair, so the events
+    bracket the sort alone."""
     from bajo_b200 import sort
-    out = {"sort_u32_pairs": {}, "sort_u64_pairs": {}, "build": {}}
-    g = torch.Generator(device=dev).manual_seed(0)
+    out = {k: {} for k in SWEEP_KINDS}
+    out["build"] = {}
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
 
-    def timeit(fn, reps=5):
+    def timeit(prepare, fn):
+        prepare()
         fn()
         torch.cuda.synchronize()
         ms = []
         for _ in range(reps):
+            prepare()
             flush.zero_()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
@@ -529,51 +611,183 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak):
             b.record(stream)
             b.synchronize()
             ms.append(a.elapsed_time(b))
-        return statistics.median(ms)
+        return statistics.median(ms), min(ms)
 
-    for lg in (20, 22, 24, 26):
+    for lg in SWEEP_LOG2:
         n = 1 << lg
-        k32 = torch.randint(-2**31, 2**31, (n,), dtype=torch.int32, device=dev, generator=g)
-        v32 = torch.arange(n, dtype=torch.int32, device=dev)
-        src_k, src_v = k32.clone(), v32.clone()
-        ws = sort.RadixSortWorkspace(n, 4, True, device=dev)
+        for kind, (bytes_per_key, pairs) in SWEEP_KINDS.items():
+            src_k, b, e = sweep_keys(torch, kind, n, seed=lg, dev=dev)
+            keys = torch.empty_like(src_k)
+            vals = torch.empty(n, dtype=torch.int32, device=dev) if pairs else None
+            src_v = torch.arange(n, dtype=torch.int32, device=dev) if pairs else None
+            ws = sort.RadixSortWorkspace(n, src_k.element_size(), pairs, b, e, device=dev)
 
-        def f32():
-            k32.copy_(src_k)
-            v32.copy_(src_v)
-            sort.onesweep_radix_sort_pairs(k32, v32, workspace=ws)
-        copy_ms = timeit(lambda: (k32.copy_(src_k), v32.copy_(src_v)))
-        ms = timeit(f32) - copy_ms
-        out["sort_u32_pairs"][f"2^{lg}"] = {"gkeys_s": round(n / ms / 1e6, 2),
-                                           "hbm_frac": round(68 * n / (ms / 1e3) / 1e9 / peak, 3)}
-        del k32, v32, src_k, src_v, ws
-        k64 = torch.randint(0, 2**62, (n,), dtype=torch.int64, device=dev, generator=g) & 0x00000FFF3FFFFFFF
-        v32 = torch.arange(n, dtype=torch.int32, device=dev)
-        src_k, src_v = k64.clone(), v32.clone()
-        ws = sort.RadixSortWorkspace(n, 8, True, 0, 44, device=dev)
+            def prepare():
+                keys.copy_(src_k)
+                if pairs:
+                    vals.copy_(src_v)
 
-        def f64():
-            k64.copy_(src_k)
-            v32.copy_(src_v)
-            sort.onesweep_radix_sort_pairs(k64, v32, workspace=ws, begin_bit=0, end_bit=44)
-        copy_ms = timeit(lambda: (k64.copy_(src_k), v32.copy_(src_v)))
-        ms = timeit(f64) - copy_ms
-        out["sort_u64_pairs"][f"2^{lg}"] = {"bits": 44, "gkeys_s": round(n / ms / 1e6, 2),
-                                           "hbm_frac": round((6 * 24 + 8) * n / (ms / 1e3) / 1e9 / peak, 3)}
-        del k64, v32, src_k, src_v, ws
+            if pairs:
+                fn = lambda: sort.onesweep_radix_sort_pairs(keys, vals, workspace=ws, begin_bit=b, end_bit=e)  # noqa
+            else:
+                fn = lambda: sort.onesweep_radix_sort_keys(keys, workspace=ws, begin_bit=b, end_bit=e)  # noqa
+            med, best = timeit(prepare, fn)
+            uk = (keys.to(torch.int64) & 0xFFFFFFFF) if keys.dtype == torch.int32 else keys
+            ok = bool((uk[1:] >= uk[:-1]).all())
+            del uk
+            if ws.status() != 0 or not ok:
+                raise RuntimeError(f"sweep {kind} 2^{lg}: status {ws.status()}, sorted {ok}")
+            out[kind][f"2^{lg}"] = {"gkeys_s": round(n / med / 1e6, 3), "ms": round(med, 5),
+                                    "hbm_frac": round(bytes_per_key * n / (med / 1e3) / 1e9 / peak, 4),
+                                    "best_gkeys_s": round(n / best / 1e6, 3)}
+            del src_k, keys, vals, src_v, ws
     for lg in (20, 22, 24):
         n = 1 << lg
+        g = torch.Generator(device=dev).manual_seed(0)
         c = torch.rand((n, 1, 3), generator=g, device=dev)
         off = (torch.rand((n, 3, 3), generator=g, device=dev) * 2 - 1) * 0.004
         v = (c + off).reshape(-1).contiguous()
         ws = bvh.GpuBvhBuildWorkspace(n, 1, device=dev)
         tree = bvh.build_triangle_bvh(v, workspace=ws)
-        ms = timeit(lambda: bvh.build_triangle_bvh(v, workspace=ws, out=tree))
+        med, _ = timeit(lambda: None, lambda: bvh.build_triangle_bvh(v, workspace=ws, out=tree))
         # bytes per triangle: bounds 36+24, Morton 24+12, 4 passes x 24, topology ~24, refit 36+48+48
-        out["build"][f"2^{lg}"] = {"mtri_s": round(n / ms / 1e3, 1), "ms": round(ms, 4),
-                                   "hbm_frac": round(348 * n / (ms / 1e3) / 1e9 / peak, 3)}
+        out["build"][f"2^{lg}"] = {"mtri_s": round(n / med / 1e3, 1), "ms": round(med, 4),
+                                   "hbm_frac": round(348 * n / (med / 1e3) / 1e9 / peak, 3)}
         del c, off, v, ws, tree
+    out["bytes_per_key"] = {k: v[0] for k, v in SWEEP_KINDS.items()}
+    out["timing"] = f"median of {reps} event-timed sorts; unsorted keys restored and L2 flushed before each"
     return out
+
+
+def cpu_sort_baseline(torch, dev, seconds=2.0):
+    """The oracle's multithreaded stable LSD radix sort (the reference CPU
+    builder's parallel pass) on every host thread: 2^22 keys of each sweep
+    kind, repeated for about `seconds` each."""
+    import numpy as np
+    from oracle import oracle as O
+    n = 1 << CPU_SORT_LOG2
+    out = {}
+    for kind, (_, pairs) in SWEEP_KINDS.items():
+        k_dev, b, e = sweep_keys(torch, kind, n, seed=CPU_SORT_LOG2, dev=dev)
+        src = k_dev.cpu().numpy().view(np.uint32 if k_dev.dtype == torch.int32 else np.uint64).copy()
+        del k_dev
+        cs = O.CpuSort(n, src.dtype.itemsize, pairs)
+        keys = src.copy()
+        vals = np.arange(n, dtype=np.uint32) if pairs else None
+        times = []
+        t_end = time.perf_counter() + seconds
+        while time.perf_counter() < t_end or len(times) < 2:
+            keys[:] = src
+            if pairs:
+                vals[:] = np.arange(n, dtype=np.uint32)
+            t0 = time.perf_counter()
+            cs.sort(keys, vals, b, e)
+            times.append(time.perf_counter() - t0)
+        t = statistics.median(times)
+        out[kind] = {"value": round(n / t / 1e9, 4), "unit": "Gkeys/s", "cores": cs.threads, "kind": "port",
+                     "sample": f"{len(times)} sorts of 2^{CPU_SORT_LOG2} keys (bits [{b}, {e})), median"}
+    return out
+
+
+def run_render(steps, warmup, spp=64, graph=True):
+    """Path-tracing workload: 64 icospheres (subdivision 5) + box + quad
+    light, 1280x720, `spp` samples per pixel, MIS, depth 8, FP32.  Device
+    time of the render through render_gpu_triangles (median), and of the same
+    render replayed as one CUDA graph through the handle API."""
+    import torch
+    from bajo_b200 import rt, scenes
+    stream = torch.cuda.current_stream()
+    sc = scenes.spheres_in_box()
+    gsc = rt.GpuRtTriangleScene(sc)
+    settings = rt.RenderSettings(1280, 720, spp, rng_seed=2026, max_depth=8)
+    ws = rt.RenderWorkspace(settings, rt.MIS)
+    for _ in range(max(1, warmup)):
+        rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws)
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    t = statistics.median(ms)
+    rays, shadows = ws.ray_counts()
+    paths = 1280 * 720 * spp
+    out = {"workload": "64 icospheres (subdivision 5) + box + 0.25x0.25 light (emission 15), 1280x720, "
+                       f"{spp} spp, MIS, depth 8", "triangles": sc.n_tris, "ms": round(t, 3),
+           "samples_s": round(paths / t * 1e3, 1), "mrays_s": round((rays + shadows) / t / 1e3, 2),
+           "rays": rays, "shadow_rays": shadows, "status": ws.status()}
+    if graph:
+        renderer = rt.Renderer(settings, rt.MIS)
+        side = torch.cuda.Stream()
+        cam = torch.from_numpy(sc.camera.astype("float32")).cuda()
+        px = torch.empty((720, 1280, 3), dtype=torch.float32, device="cuda")
+        ms_graph = []
+        with torch.cuda.stream(side):
+            for _ in range(max(1, warmup)):
+                renderer.enqueue(gsc, cam, px, stream=side)
+            side.synchronize()
+            for _ in range(steps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(side)
+                renderer.enqueue(gsc, cam, px, stream=side)
+                b.record(side)
+                b.synchronize()
+                ms_graph.append(a.elapsed_time(b))
+        renderer.close()
+        out["graph_ms"] = round(statistics.median(ms_graph), 3)
+    out["_scene"] = sc
+    return out
+
+
+def cpu_render_sample(sc, seconds=10.0):
+    """The oracle's restatement of the reference CPU path tracer (MIS, depth
+    8) on every host thread over the path-tracing scene: 1280x720 at 1 sample
+    per pixel, repeated for about `seconds`."""
+    from oracle import oracle as O
+    bvh = O.lbvh_build(sc.vertices)
+    lights = O.rt_build_lights(sc)
+    threads = O.n_threads()
+    t_end = time.perf_counter() + seconds
+    times = []
+    while time.perf_counter() < t_end or not times:
+        t0 = time.perf_counter()
+        O.render(sc, sc.camera, 1280, 720, 1, max_depth=8, seed=2026 + len(times), algorithm=4, lights=lights,
+                 bvh=bvh, threads=threads)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    return {"value": round(1280 * 720 / t / 1e6, 3), "unit": "Msamples/s", "cores": threads, "kind": "port",
+            "sample": f"{len(times)} renders of 1280x720 at 1 spp (MIS, depth 8), median"}
+
+
+def cpu_batched_sample(verts, so, n_scenes=32, width=256, height=256):
+    """CPU build + trace of the first `n_scenes` scenes of the batched
+    workload: the restated reference CPU builder per scene and the oracle's
+    primary + cosine-bounce trace of its 256x256 rays, on every host thread."""
+    from oracle import oracle as O
+    import numpy as np
+    cam = workload_camera()
+    tris = rays = 0
+    t_build = t_trace = 0.0
+    for s in range(n_scenes):
+        sub = verts[9 * int(so[s]): 9 * int(so[s + 1])]
+        cb = O.CpuLbvh(sub)
+        t0 = time.perf_counter()
+        cb.build()
+        t_build += time.perf_counter() - t0
+        o = O.lbvh_build(sub)
+        t0 = time.perf_counter()
+        _, p0, _, _ = O.trace_batch(o, cam, 0, width, height, seed=7, view_base=s)
+        t_trace += time.perf_counter() - t0
+        tris += int(so[s + 1] - so[s])
+        rays += width * height + int(np.count_nonzero(p0 != O.EMPTY))
+    t = t_build + t_trace
+    return {"value": round(tris / t / 1e6, 3), "unit": "Mtri/s (build + trace)", "mrays_s": round(rays / t / 1e6, 3),
+            "cores": O.n_threads(), "kind": "port",
+            "sample": f"first {n_scenes} scenes ({tris} triangles, {rays} rays): CPU LBVH build + 256x256 primary "
+                      "and bounce rays each"}
 
 
 def run_batched(steps, warmup, n_scenes=4096):
@@ -601,9 +815,39 @@ def run_batched(steps, warmup, n_scenes=4096):
     p0 = g.result.p0
     bounce = int((p0 != -1).sum().item())
     rays = n_scenes * 256 * 256 + bounce
-    return {"scenes": n_scenes, "triangles": int(so[-1]), "ms": round(t, 3),
+    return {"workload": f"{n_scenes} scenes, 256..65,536 triangles (log-uniform), 256x256 primary + one "
+                        "cosine bounce per pixel, one CUDA-graph launch", "scenes": n_scenes,
+            "triangles": int(so[-1]), "ms": round(t, 3),
             "build_trace_mtri_s": round(int(so[-1]) / t / 1e3, 1), "mrays_s": round(rays / t / 1e3, 1),
-            "rays": rays, "status": g.status()}
+            "rays": rays, "status": g.status(), "_verts": verts, "_so": so}
+
+
+def run_extras(args, local):
+    """The other stated workloads, one GPU, each with its clock record and a
+    CPU baseline: `render` (path tracing), `batched` (4,096 scenes) and
+    `guided` (learned guiding vs plain MIS at equal time)."""
+    out = {}
+    with ClockSampler(local) as ck:
+        r = run_render(3, 1, 64)
+    sc = r.pop("_scene")
+    r["clocks"] = ck.summary()
+    if not args.no_cpu_baseline:
+        r["cpu_baseline"] = cpu_render_sample(sc)
+    out["render"] = r
+    with ClockSampler(local) as ck:
+        r = run_batched(5, 2)
+    verts, so = r.pop("_verts"), r.pop("_so")
+    r["clocks"] = ck.summary()
+    if not args.no_cpu_baseline:
+        r["cpu_baseline"] = cpu_batched_sample(verts, so)
+    del verts, so
+    out["batched"] = r
+    gargs = parse_args([])
+    with ClockSampler(local) as ck:
+        r = run_guided(gargs)
+    r["clocks"] = ck.summary()
+    out["guided"] = r
+    return out
 
 
 def run_guided(args):
@@ -756,39 +1000,11 @@ def run_case(args):
         return statistics.median(ms)
 
     if args.case == "render":
-        from bajo_b200 import rt, scenes
-        sc = scenes.spheres_in_box()
-        gsc = rt.GpuRtTriangleScene(sc)
-        settings = rt.RenderSettings(1280, 720, args.spp, rng_seed=2026, max_depth=8)
-        ws = rt.RenderWorkspace(settings, rt.MIS)
-        ms = timed(lambda: rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws))
-        rays, shadows = ws.ray_counts()
-        paths = 1280 * 720 * args.spp
-        # the same render through the handle API on a side stream: recorded
-        # once into a CUDA graph, then one graph launch per render
-        renderer = rt.Renderer(settings, rt.MIS)
-        side = torch.cuda.Stream()
-        cam = torch.from_numpy(sc.camera.astype("float32")).cuda()
-        px = torch.empty((720, 1280, 3), dtype=torch.float32, device="cuda")
-        ms_graph = []
-        with torch.cuda.stream(side):
-            for _ in range(max(1, args.warmup)):
-                renderer.enqueue(gsc, cam, px, stream=side)
-            side.synchronize()
-            for _ in range(args.steps):
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(side)
-                renderer.enqueue(gsc, cam, px, stream=side)
-                b.record(side)
-                b.synchronize()
-                ms_graph.append(a.elapsed_time(b))
-        renderer.close()
-        out.update({"ms": round(ms, 3), "samples_s": round(paths / ms * 1e3, 1),
-                    "mrays_s": round((rays + shadows) / ms / 1e3, 2), "rays": rays, "shadow_rays": shadows,
-                    "triangles": sc.n_tris, "graph_ms": round(statistics.median(ms_graph), 3),
-                    "status": ws.status()})
+        out.update(run_render(args.steps, args.warmup, args.spp))
     elif args.case == "batched":
-        out.update(run_batched(args.steps, args.warmup, args.scenes))
+        r = run_batched(args.steps, args.warmup, args.scenes)
+        r.pop("_verts"), r.pop("_so")
+        out.update(r)
     elif args.case == "guided":
         out = run_guided(args)
     elif args.case == "guided_pass":

@@ -356,6 +356,139 @@ static BO_SORT_IMPL(bo_sort_keys_u64_impl, uint64_t, 0)
 void bo_sort_keys_u32(uint32_t* k, uint32_t n, int b, int e) { bo_sort_keys_u32_impl(k, NULL, n, b, e); }
 void bo_sort_keys_u64(uint64_t* k, uint32_t n, int b, int e) { bo_sort_keys_u64_impl(k, NULL, n, b, e); }
 
+/* Multithreaded stable LSD radix sort, the CPU sort baseline.  Each pass is
+ * the reference CPU builder's parallel pass (bajo/bvh/cpu/builder/
+ * lbvh.mojo:65-110): per-worker digit histograms over contiguous chunks,
+ * destinations assigned digit-major then worker-major (which keeps the pass
+ * stable), then a parallel scatter.  8-bit digits over [begin_bit, end_bit);
+ * scratch from bo_cpu_sort_scratch_bytes (alternate buffers and histograms),
+ * so nothing is allocated per call. */
+typedef struct {
+  const void* ks;
+  void* kd;
+  const uint32_t* vs;
+  uint32_t* vd;
+  uint32_t n, workers, shift, mask, key_bytes;
+  uint32_t* counts;  /* [workers][256] */
+} cpu_sort_ctx;
+
+static inline uint32_t cs_digit(const cpu_sort_ctx* c, uint32_t i) {
+  return c->key_bytes == 8 ? (uint32_t)((((const uint64_t*)c->ks)[i] >> c->shift) & c->mask)
+                           : (((const uint32_t*)c->ks)[i] >> c->shift) & c->mask;
+}
+static void cs_hist(void* p, uint32_t b, uint32_t e) {
+  cpu_sort_ctx* c = (cpu_sort_ctx*)p;
+  for (uint32_t w = b; w < e; ++w) {
+    uint32_t* cnt = c->counts + 256 * (size_t)w;
+    memset(cnt, 0, 256 * sizeof(uint32_t));
+    uint32_t first = (uint32_t)((uint64_t)c->n * w / c->workers), end = (uint32_t)((uint64_t)c->n * (w + 1) / c->workers);
+    for (uint32_t i = first; i < end; ++i) cnt[cs_digit(c, i)]++;
+  }
+}
+static void cs_scatter(void* p, uint32_t b, uint32_t e) {
+  cpu_sort_ctx* c = (cpu_sort_ctx*)p;
+  for (uint32_t w = b; w < e; ++w) {
+    uint32_t off[256];
+    memcpy(off, c->counts + 256 * (size_t)w, sizeof off);  /* offsets by now */
+    uint32_t first = (uint32_t)((uint64_t)c->n * w / c->workers), end = (uint32_t)((uint64_t)c->n * (w + 1) / c->workers);
+    if (c->key_bytes == 8) {
+      const uint64_t* ks = (const uint64_t*)c->ks;
+      uint64_t* kd = (uint64_t*)c->kd;
+      for (uint32_t i = first; i < end; ++i) {
+        uint32_t o = off[(uint32_t)((ks[i] >> c->shift) & c->mask)]++;
+        kd[o] = ks[i];
+        if (c->vs) c->vd[o] = c->vs[i];
+      }
+    } else {
+      const uint32_t* ks = (const uint32_t*)c->ks;
+      uint32_t* kd = (uint32_t*)c->kd;
+      for (uint32_t i = first; i < end; ++i) {
+        uint32_t o = off[(ks[i] >> c->shift) & c->mask]++;
+        kd[o] = ks[i];
+        if (c->vs) c->vd[o] = c->vs[i];
+      }
+    }
+  }
+}
+
+size_t bo_cpu_sort_scratch_bytes(uint32_t n, uint32_t key_bytes, int has_values, uint32_t n_threads) {
+  if (n_threads == 0) n_threads = 1;
+  size_t o = ((size_t)n * key_bytes + 63) & ~(size_t)63;
+  if (has_values) o += ((size_t)n * 4 + 63) & ~(size_t)63;
+  return o + sizeof(uint32_t) * 256 * (size_t)n_threads;
+}
+
+void bo_cpu_sort(void* keys, uint32_t* vals, uint32_t n, uint32_t key_bytes, int begin_bit, int end_bit,
+                 uint32_t n_threads, void* scratch) {
+  if (n <= 1 || begin_bit >= end_bit) return;
+  if (n_threads == 0) n_threads = 1;
+  const uint32_t workers = n_threads < n ? n_threads : n;
+  unsigned char* sb = (unsigned char*)scratch;
+  void* kalt = sb;
+  size_t o = ((size_t)n * key_bytes + 63) & ~(size_t)63;
+  uint32_t* valt = vals ? (uint32_t*)(sb + o) : NULL;
+  if (vals) o += ((size_t)n * 4 + 63) & ~(size_t)63;
+  cpu_sort_ctx c;
+  c.n = n;
+  c.workers = workers;
+  c.key_bytes = key_bytes;
+  c.counts = (uint32_t*)(sb + o);
+  void* ks = keys;
+  void* kd = kalt;
+  uint32_t* vs = vals;
+  uint32_t* vd = valt;
+  for (int sh = begin_bit; sh < end_bit; sh += 8) {
+    int bits = end_bit - sh < 8 ? end_bit - sh : 8;
+    c.ks = ks;
+    c.kd = kd;
+    c.vs = vs;
+    c.vd = vd;
+    c.shift = (uint32_t)sh;
+    c.mask = (1u << bits) - 1u;
+    bo_parallel_for(workers, workers, 1, cs_hist, &c);
+    uint32_t acc = 0;
+    for (uint32_t b = 0; b <= c.mask; ++b)
+      for (uint32_t w = 0; w < workers; ++w) {
+        uint32_t cnt = c.counts[256 * (size_t)w + b];
+        c.counts[256 * (size_t)w + b] = acc;
+        acc += cnt;
+      }
+    bo_parallel_for(workers, workers, 1, cs_scatter, &c);
+    void* tk = ks; ks = kd; kd = tk;
+    uint32_t* tv = vs; vs = vd; vd = tv;
+  }
+  if (ks != keys) {
+    memcpy(keys, ks, (size_t)n * key_bytes);
+    if (vals) memcpy(vals, vs, (size_t)n * 4);
+  }
+}
+
+/* 63-bit 3D Morton code, 21 bits per axis (the sort workload's 64-bit keys):
+ * u = clamp(u32(c * 2^21), 0, 2^21 - 1) per axis as quantize1024 does with
+ * 10 bits (core/morton.mojo:78), code = e(z) << 2 | e(y) << 1 | e(x). */
+static inline uint64_t expand_bits_21(uint64_t v) {
+  v &= 0x1FFFFFull;
+  v = (v | (v << 32)) & 0x001F00000000FFFFull;
+  v = (v | (v << 16)) & 0x001F0000FF0000FFull;
+  v = (v | (v << 8)) & 0x100F00F00F00F00Full;
+  v = (v | (v << 4)) & 0x10C30C30C30C30C3ull;
+  v = (v | (v << 2)) & 0x1249249249249249ull;
+  return v;
+}
+static inline uint64_t quantize21(float c) {
+  float s = c * 2097152.0f;
+  if (!(s > 0.0f)) return 0;
+  if (s >= 2097151.0f) return 2097151ull;
+  return (uint64_t)s;
+}
+void bo_morton63(const float* xyz, uint32_t n, uint64_t* out) {
+  for (uint32_t i = 0; i < n; ++i) {
+    const float* p = xyz + (size_t)3 * i;
+    out[i] = (expand_bits_21(quantize21(p[2])) << 2) | (expand_bits_21(quantize21(p[1])) << 1) |
+             expand_bits_21(quantize21(p[0]));
+  }
+}
+
 /* ------------------------------------------------------------------------- */
 /* a7/a8: Karras topology                                                     */
 /* ------------------------------------------------------------------------- */
@@ -2082,6 +2215,7 @@ typedef struct {
   int mode;
   float *t0, *t1;
   uint32_t *p0, *p1;
+  uint32_t view_base; /* global view of segment 0 (random streams, camera) */
 } batch_ctx;
 
 static void batch_range(void* p, uint32_t b, uint32_t e) {
@@ -2090,7 +2224,9 @@ static void batch_range(void* p, uint32_t b, uint32_t e) {
   const float inv_h = 1.0f / (float)c->height;
   for (uint32_t i = b; i < e; ++i) {
     uint32_t view = i / ppv, local = i - view * ppv;
-    const float* cam = c->cams + (size_t)view * c->cam_stride;
+    const uint32_t gview = c->view_base + view;
+    const uint32_t gi = gview * ppv + local; /* the ray's index in the whole batch */
+    const float* cam = c->cams + (size_t)gview * c->cam_stride;
     uint32_t px = local % c->width, py = local / c->width;
     float sx = (2.0f * ((float)px + 0.5f) - (float)c->width) * inv_h;
     float sy = 1.0f - 2.0f * ((float)py + 0.5f) * inv_h;
@@ -2106,7 +2242,7 @@ static void batch_range(void* p, uint32_t b, uint32_t e) {
     if (h.prim != BO_EMPTY) {
       v3 normal = v3dot(d, h.n) < 0.0f ? h.n : vneg(h.n);
       float u[4];
-      bo_rt_uniform4(c->seed, i, st_bsdf0(), u);
+      bo_rt_uniform4(c->seed, gi, st_bsdf0(), u);
       v3 dir = lambertian_dir(normal, u[0], u[1]);
       v3 p = v3make(o.x + h.t * d.x, o.y + h.t * d.y, o.z + h.t * d.z);
       bo_ray r2 = make_ray_od(p, dir, 0.001f, BO_FLT_MAX);
@@ -2122,7 +2258,13 @@ static void batch_range(void* p, uint32_t b, uint32_t e) {
 void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride, uint32_t width,
                     uint32_t height, uint64_t seed, int mode, float* t0, uint32_t* p0, float* t1, uint32_t* p1,
                     uint32_t n_threads) {
-  batch_ctx c = {bvh, verts, cams, cam_stride, width, height, seed, mode, t0, t1, p0, p1};
+  bo_trace_batch_views(bvh, verts, cams, cam_stride, width, height, seed, mode, 0, t0, p0, t1, p1, n_threads);
+}
+
+void bo_trace_batch_views(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride,
+                          uint32_t width, uint32_t height, uint64_t seed, int mode, uint32_t view_base, float* t0,
+                          uint32_t* p0, float* t1, uint32_t* p1, uint32_t n_threads) {
+  batch_ctx c = {bvh, verts, cams, cam_stride, width, height, seed, mode, t0, t1, p0, p1, view_base};
   uint32_t n = bvh->n_segments * width * height;
   bo_parallel_for(n, n_threads, 512, batch_range, &c);
 }

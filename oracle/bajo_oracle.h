@@ -85,6 +85,16 @@ void bo_sort_pairs_u64(uint64_t* keys, uint32_t* vals, uint32_t n,
 void bo_sort_pairs_u32(uint32_t* keys, uint32_t* vals, uint32_t n,
                        int begin_bit, int end_bit);
 void bo_sort_keys_u32(uint32_t* keys, uint32_t n, int begin_bit, int end_bit);
+/* Multithreaded stable LSD radix sort (the CPU sort baseline; the reference
+ * CPU builder's parallel pass, bajo/bvh/cpu/builder/lbvh.mojo:65-110), keys
+ * of key_bytes (4 or 8) with optional u32 values (vals may be NULL), into
+ * caller-owned scratch of bo_cpu_sort_scratch_bytes bytes. */
+size_t bo_cpu_sort_scratch_bytes(uint32_t n, uint32_t key_bytes, int has_values, uint32_t n_threads);
+void bo_cpu_sort(void* keys, uint32_t* vals, uint32_t n, uint32_t key_bytes, int begin_bit, int end_bit,
+                 uint32_t n_threads, void* scratch);
+/* 63-bit Morton codes of points (3 floats each) in the unit cube, 21 bits per
+ * axis: the sort workload's 64-bit keys. */
+void bo_morton63(const float* xyz, uint32_t n, uint64_t* out);
 void bo_sort_keys_u64(uint64_t* keys, uint32_t n, int begin_bit, int end_bit);
 
 /* ---- a8: internal segment offsets (binary_layout.mojo:219) --------------- */
@@ -209,6 +219,12 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
 void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride, uint32_t width,
                     uint32_t height, uint64_t seed, int mode, float* t0, uint32_t* p0, float* t1, uint32_t* p1,
                     uint32_t n_threads);
+/* The same over the segments of `bvh` taken as views view_base, view_base+1,
+ * ... of a larger batch: the bounce rays draw the random streams of their
+ * index in that batch, so a scene built alone reproduces its rays there. */
+void bo_trace_batch_views(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride,
+                          uint32_t width, uint32_t height, uint64_t seed, int mode, uint32_t view_base, float* t0,
+                          uint32_t* p0, float* t1, uint32_t* p1, uint32_t n_threads);
 
 /* ---- a10: BVH2 -> W-wide collapse (bajo_oracle_wide.c) ------------------- */
 /* Outputs sized for n_leaves nodes and leaf blocks; offsets [S+1];

@@ -71,6 +71,9 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_sort_pairs_u64": (None, [_P, _P, _U32, _I, _I]),
         "bo_sort_pairs_u32": (None, [_P, _P, _U32, _I, _I]),
         "bo_sort_keys_u32": (None, [_P, _U32, _I, _I]),
+        "bo_cpu_sort_scratch_bytes": (ctypes.c_size_t, [_U32, _U32, _I, _U32]),
+        "bo_cpu_sort": (None, [_P, _P, _U32, _U32, _I, _I, _U32, _P]),
+        "bo_morton63": (None, [_P, _U32, _P]),
         "bo_sort_keys_u64": (None, [_P, _U32, _I, _I]),
         "bo_internal_offsets": (None, [_P, _U32, _P]),
         "bo_lbvh_topology": (None, [_P, _P, _P, _U32, _P, _P, _P, _P, _P]),
@@ -90,6 +93,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_philox4x32_10": (None, [_P, _P, _P]),
         "bo_trace_batch": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _U32, _U32, ctypes.c_uint64, _I, _P, _P, _P,
                                   _P, _U32]),
+        "bo_trace_batch_views": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _U32, _U32, _U32, ctypes.c_uint64, _I,
+                                         _U32, _P, _P, _P, _P, _U32]),
         "bo_rt_uniform4": (None, [ctypes.c_uint64, _U32, _U32, _P]),
         "bo_rt_sincos_turns": (None, [_F, ctypes.POINTER(_F), ctypes.POINTER(_F)]),
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
@@ -175,6 +180,33 @@ def sort_pairs(keys: np.ndarray, vals: np.ndarray, begin_bit=0, end_bit=None):
     else:
         raise TypeError(k.dtype)
     return k, v
+
+
+class CpuSort:
+    """Multithreaded stable LSD radix sort (the CPU sort baseline), in place,
+    with its scratch allocated once for up to ``n`` keys."""
+
+    def __init__(self, n: int, key_bytes: int, has_values: bool, threads=None):
+        self.n, self.key_bytes, self.has_values = n, key_bytes, has_values
+        self.threads = threads or n_threads()
+        self.scratch = np.zeros(max(int(lib().bo_cpu_sort_scratch_bytes(n, key_bytes, int(has_values),
+                                                                       self.threads)), 1), np.uint8)
+
+    def sort(self, keys: np.ndarray, vals=None, begin_bit=0, end_bit=None):
+        assert keys.flags.c_contiguous and keys.dtype.itemsize == self.key_bytes and keys.size <= self.n
+        assert (vals is not None) == self.has_values
+        if end_bit is None:
+            end_bit = self.key_bytes * 8
+        lib().bo_cpu_sort(_ptr(keys), _ptr(vals) if vals is not None else None, keys.size, self.key_bytes,
+                          begin_bit, end_bit, self.threads, _ptr(self.scratch))
+
+
+def morton63(points: np.ndarray) -> np.ndarray:
+    """63-bit Morton codes (21 bits per axis) of points in the unit cube."""
+    p = np.ascontiguousarray(points, np.float32).reshape(-1)
+    out = np.empty(p.size // 3, np.uint64)
+    lib().bo_morton63(_ptr(p), out.size, _ptr(out))
+    return out
 
 
 def sort_keys(keys: np.ndarray, begin_bit=0, end_bit=None):
@@ -485,14 +517,17 @@ def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=
     return (img, samples.reshape(height, width, spp, 3)) if return_samples else img
 
 
-def trace_batch(bvh: OracleLbvh, cams, cam_stride, width, height, seed=7, tri_mode=TRI_WATERTIGHT, threads=None):
+def trace_batch(bvh: OracleLbvh, cams, cam_stride, width, height, seed=7, tri_mode=TRI_WATERTIGHT, threads=None,
+                view_base=0):
+    """Primary + cosine bounce rays of every segment; `view_base` > 0 treats
+    segment k as view view_base + k of a larger batch (its random streams)."""
     n = (bvh.seg_offsets.size - 1) * width * height
     t0, t1 = np.zeros(n, np.float32), np.zeros(n, np.float32)
     p0, p1 = np.zeros(n, np.uint32), np.zeros(n, np.uint32)
     c = np.ascontiguousarray(cams, np.float32)
     s = bvh.struct()
-    lib().bo_trace_batch(ctypes.byref(s), _ptr(bvh.verts), _ptr(c), cam_stride, width, height, seed, tri_mode,
-                         _ptr(t0), _ptr(p0), _ptr(t1), _ptr(p1), threads or n_threads())
+    lib().bo_trace_batch_views(ctypes.byref(s), _ptr(bvh.verts), _ptr(c), cam_stride, width, height, seed, tri_mode,
+                               view_base, _ptr(t0), _ptr(p0), _ptr(t1), _ptr(p1), threads or n_threads())
     return t0, p0, t1, p1
 
 
