@@ -25,6 +25,8 @@ STATUS_BAD_TOPOLOGY = 0x4
 STATUS_WIDE_TIMEOUT = 0x40
 STATUS_STAGE_TIMEOUT = 0x80
 STATUS_WAIT_TIMEOUT = 0x100
+STATUS_GRID_TIMEOUT = 0x200
+FUSED_MAX_LEAVES = 1 << 17  # largest scene the one-launch build takes
 TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
@@ -120,6 +122,8 @@ SIGNATURES = {
     "bajo_lbvh_build": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P]),
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
+    "bajo_lbvh_fused_max_set": (_I32, [_U32]),
+    "bajo_lbvh_build_launches": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_stage_top": (_I32, [ctypes.POINTER(BajoLbvhC), _P]),
     "bajo_wait_selftest": (_I32, [_P, _U32, _U32, _P, _P]),
     "bajo_render_create": (_I32, [_P, _P, _SZ, ctypes.POINTER(_P)]),

@@ -20,7 +20,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libbajo_b200.so")
 SOURCES = ["sort.cu", "sort_static.cu", "lbvh.cu", "trace.cu", "camera.cu", "rt.cu", "render_handle.cu", "mlp.cu",
            "wide.cu", "cwbvh.cu", "hploc.cu", "tlas.cu"]
-HEADERS = ["bajo_common.cuh", "onesweep.cuh", "traverse.cuh", "sampling.cuh", "mlp.cuh", "wide.cuh"]
+HEADERS = ["bajo_common.cuh", "onesweep.cuh", "traverse.cuh", "sampling.cuh", "mlp.cuh", "wide.cuh", "cwbvh.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

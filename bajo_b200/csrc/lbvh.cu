@@ -2,6 +2,8 @@
 // keys, onesweep sort, Karras topology, atomic-flag refit.  Restates
 // bajo/bvh/gpu/builder/lbvh.mojo (GPU driver) and binary_layout.mojo with the
 // reference's buffer layouts; see include/bajo_b200.h for the boundary.
+#include <atomic>
+
 #include "onesweep.cuh"
 
 namespace bajo {
@@ -736,6 +738,576 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 }
 
 // ---------------------------------------------------------------------------
+// 5. One-launch build of one scene of up to fused::kMaxLeaves triangles
+//    (the whole of sections 1-3 for a single segment, in one cooperative
+//    launch).
+//
+//    At 65,536 triangles every kernel of the multi-launch build is latency
+//    bound: a few microseconds of work each, behind a chain of dependent
+//    global round trips.  Here one CTA per kTile sorted leaves runs every
+//    phase, and phases meet at grid-wide barriers (bounded waits,
+//    BAJO_STATUS_GRID_TIMEOUT):
+//      A  triangle bounds, root and centroid bounds    -> barrier 1
+//      B  Morton codes (kept in registers), the digit histograms of every
+//         pass, and tile 0's digit counts of pass 0    -> barrier 2
+//      P0..P3  LSD radix passes over the 30-bit code, 8-bit digits: each
+//         tile ranks its keys (stable, in position order) and scatters them
+//         to  base(digit) + counts of the digit in earlier tiles + rank.
+//         While it scatters, it counts the next pass's digits per
+//         destination tile with global atomics, so the next pass finds its
+//         per-tile counts complete after a single barrier -> barriers 3-6
+//      H  the bottom-up hierarchy + refit of hierarchy_kernel with kTile
+//         leaves per CTA: more of the climb stays in shared memory, and the
+//         splits that cross tiles meet through one acq_rel atomic per level
+//         (the first arrival's subtree is written before its atomic, so the
+//         second reads it right after its own).
+//    Every output array is bit-identical to the multi-launch build's (same
+//    stable sort, same tree, same numbering).
+// ---------------------------------------------------------------------------
+namespace fused {
+constexpr int kThreads = 512;
+constexpr int kKpt = 4;                              // keys (and leaves) per thread
+constexpr uint32_t kTile = kThreads * kKpt;          // sorted leaves per CTA
+constexpr uint32_t kMaxLeaves = 1u << 17;
+constexpr uint32_t kMaxTiles = kMaxLeaves / kTile;  // 64
+constexpr int kPasses = 4;                           // digits [0,8) [8,16) [16,24) [24,30)
+constexpr int kWarps = kThreads / 32;
+constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
+
+// Workspace (bytes from the start of the build workspace; word 0 is the
+// status word): barrier counter, ordered segment bounds and the digit
+// histograms (zeroed before the launch), per-(pass, tile) digit counts, and
+// two key / payload buffers for the passes.
+struct Layout {
+  size_t off_bar, off_seg_ord, off_ghist, zero_end, off_counts, off_ka, off_va, off_kb, off_vb, total;
+};
+__host__ __device__ constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
+__host__ __device__ constexpr Layout layout(uint32_t n) {
+  Layout l{};
+  l.off_bar = 256;
+  l.off_seg_ord = 320;
+  l.off_ghist = 384;
+  l.zero_end = l.off_ghist + (size_t)kPasses * 256 * 4;
+  l.off_counts = a256(l.zero_end);
+  l.off_ka = a256(l.off_counts + (size_t)kPasses * kMaxTiles * 256 * 4);
+  l.off_va = a256(l.off_ka + (size_t)n * 4);
+  l.off_kb = a256(l.off_va + (size_t)n * 4);
+  l.off_vb = a256(l.off_kb + (size_t)n * 4);
+  l.total = a256(l.off_vb + (size_t)n * 4);
+  return l;
+}
+
+// Shared memory, one buffer reused by the phases.
+constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;  // phase A
+constexpr size_t kSmemHier = (size_t)kTile * 48 + (size_t)kTile * 8 + (size_t)kTile * 8 + (size_t)kTile * 4 +
+                             (size_t)(kTile + 2) * 4;  // phase H
+constexpr size_t kSmemSort = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
+constexpr size_t kSmem = ((kSmemHier > kSmemVerts ? (kSmemHier > kSmemSort ? kSmemHier : kSmemSort)
+                                                  : (kSmemVerts > kSmemSort ? kSmemVerts : kSmemSort)) + 15) & ~(size_t)15;
+
+// Grid-wide barrier number k (1, 2, ...) of a cooperative launch: every CTA
+// adds one to *bar (released) and waits until all of them have, for at most
+// kWaitNs.  Returns false when the wait ran out (status bit raised); the CTA
+// then leaves the kernel, and the others run out at their next barrier.
+__device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t k, uint32_t* status, uint32_t* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    red_add_release_gpu(bar, 1u);
+    const uint32_t target = k * gridDim.x;
+    uint32_t ok = 1;
+    if (ld_acquire_gpu(bar) < target) {
+      const uint64_t t0 = global_timer_ns();
+      while (ld_acquire_gpu(bar) < target) {
+        if (global_timer_ns() - t0 > kWaitNs) {
+          raise_status(status, BAJO_STATUS_GRID_TIMEOUT);
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();
+    *s_flag = ok;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
+// One climb of the bottom-up hierarchy (see hierarchy_kernel).
+struct Climb {
+  uint32_t f, l;
+  int dl, dr;
+  f3 mn, mx;
+  bool leaf;
+  int pending;    // shared slot where it arrived first
+  uint32_t mode;  // 0 done, 1 continues through global memory
+};
+
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __restrict__ verts, uint32_t n,
+                                                                 BajoLbvh t, unsigned char* __restrict__ ws,
+                                                                 uint32_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ uint32_t s_red[kWarps][12];
+  __shared__ uint32_t s_flag;
+  constexpr Layout kL0 = layout(0);
+  const Layout L = layout(n);
+  uint32_t* bar = reinterpret_cast<uint32_t*>(ws + kL0.off_bar);
+  uint32_t* seg_ord = reinterpret_cast<uint32_t*>(ws + kL0.off_seg_ord);
+  uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + kL0.off_ghist);
+  uint32_t* counts = reinterpret_cast<uint32_t*>(ws + kL0.off_counts);  // [pass][tile][digit]
+  uint32_t* const ka = reinterpret_cast<uint32_t*>(ws + L.off_ka);
+  uint32_t* const va = reinterpret_cast<uint32_t*>(ws + L.off_va);
+  uint32_t* const kb = reinterpret_cast<uint32_t*>(ws + L.off_kb);
+  uint32_t* const vb = reinterpret_cast<uint32_t*>(ws + L.off_vb);
+
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t c = blockIdx.x;
+  const uint32_t base = c * kTile;
+  const uint32_t cnt = min(kTile, n - base);
+  // key k of this thread sits at tile position warp*32*kKpt + 32*k + lane,
+  // so (warp, k, lane) order is position order
+  const uint32_t pos0 = warp * 32 * kKpt + lane;
+
+  // ---------------- phase A: triangle bounds, root and centroid bounds
+  {
+    float* s_v = reinterpret_cast<float*>(smem);
+    const float* src = verts + (size_t)base * 9;
+    const uint32_t nf = cnt * 9;
+    if (VEC) {
+      const float4* s4 = reinterpret_cast<const float4*>(src);
+      float4* d4 = reinterpret_cast<float4*>(s_v);
+      for (uint32_t q = tid; q < nf / 4; q += kThreads) d4[q] = __ldg(s4 + q);
+      for (uint32_t q = (nf & ~3u) + tid; q < nf; q += kThreads) s_v[q] = __ldg(src + q);
+    } else {
+      for (uint32_t q = tid; q < nf; q += kThreads) s_v[q] = __ldg(src + q);
+    }
+    // arrival counters of the hierarchy's crossing splits start at zero; the
+    // next passes' digit counts of this tile are accumulated by atomics
+    for (uint32_t q = base + tid; q < min(base + kTile, n - 1); q += kThreads) t.node_flags[q] = 0u;
+    for (uint32_t q = tid; q < (kPasses - 1) * 256; q += kThreads)
+      counts[((q >> 8) + 1) * kMaxTiles * 256 + c * 256 + (q & 255)] = 0u;
+    if (c == 0 && tid == 0) {
+      t.internal_offsets[0] = 0;
+      t.internal_offsets[1] = n - 1;
+      t.roots[0] = 0;
+    }
+    __syncthreads();
+  }
+  float cx[kKpt], cy[kKpt], cz[kKpt];
+  {
+    const float* s_v = reinterpret_cast<const float*>(smem);
+    uint32_t w[12];
+#pragma unroll
+    for (int q = 0; q < 12; ++q) w[q] = 0;
+#pragma unroll
+    for (int k = 0; k < kKpt; ++k) {
+      const uint32_t p = pos0 + 32 * k;
+      cx[k] = cy[k] = cz[k] = 0.0f;
+      if (p < cnt) {
+        const float* v = s_v + p * 9;
+        const f3 a = mk(v[0], v[1], v[2]), b = mk(v[3], v[4], v[5]), cc = mk(v[6], v[7], v[8]);
+        const f3 mn = vmin(vmin(a, b), cc), mx = vmax(vmax(a, b), cc);
+        float2* o = reinterpret_cast<float2*>(t.leaf_bounds + (size_t)(base + p) * 6);
+        o[0] = make_float2(mn.x, mn.y);
+        o[1] = make_float2(mn.z, mx.x);
+        o[2] = make_float2(mx.y, mx.z);
+        const f3 ce = (mn + mx) * 0.5f;  // core/aabb.mojo:53
+        cx[k] = ce.x;
+        cy[k] = ce.y;
+        cz[k] = ce.z;
+        w[0] = max(w[0], enc_min(mn.x)); w[1] = max(w[1], enc_min(mn.y)); w[2] = max(w[2], enc_min(mn.z));
+        w[3] = max(w[3], enc_max(mx.x)); w[4] = max(w[4], enc_max(mx.y)); w[5] = max(w[5], enc_max(mx.z));
+        w[6] = max(w[6], enc_min(ce.x)); w[7] = max(w[7], enc_min(ce.y)); w[8] = max(w[8], enc_min(ce.z));
+        w[9] = max(w[9], enc_max(ce.x)); w[10] = max(w[10], enc_max(ce.y)); w[11] = max(w[11], enc_max(ce.z));
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 12; ++q) {
+      const uint32_t r = __reduce_max_sync(0xFFFFFFFFu, w[q]);
+      if (lane == 0) s_red[warp][q] = r;
+    }
+    __syncthreads();
+    if (tid < 12) {
+      uint32_t r = 0;
+#pragma unroll
+      for (int q = 0; q < kWarps; ++q) r = max(r, s_red[q][tid]);
+      if (r) atomicMax(&seg_ord[tid], r);
+    }
+  }
+  if (!grid_sync(bar, 1, status, &s_flag)) return;
+
+  // ---------------- phase B: Morton codes and every pass's digit histogram
+  uint32_t key[kKpt], val[kKpt];
+  uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem);  // [kPasses][256]
+  {
+    const f3 cmin = mk(dec_min(__ldcg(seg_ord + 6)), dec_min(__ldcg(seg_ord + 7)), dec_min(__ldcg(seg_ord + 8)));
+    const f3 cmax = mk(dec_max(__ldcg(seg_ord + 9)), dec_max(__ldcg(seg_ord + 10)), dec_max(__ldcg(seg_ord + 11)));
+    const f3 ext = cmax - cmin;
+    const f3 inv = mk(safe_inv1(ext.x), safe_inv1(ext.y), safe_inv1(ext.z));
+    if (c == 0 && tid < 12) {
+      const uint32_t u = __ldcg(seg_ord + tid);
+      const bool is_min = tid < 3 || (tid >= 6 && tid < 9);
+      t.seg_bounds[tid] = is_min ? dec_min(u) : dec_max(u);
+    }
+    for (uint32_t q = tid; q < kPasses * 256; q += kThreads) s_hist[q] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kKpt; ++k) {
+      const uint32_t p = pos0 + 32 * k;
+      if (p < cnt) {
+        const f3 d = mk(cx[k], cy[k], cz[k]) - cmin;
+        key[k] = morton3(d.x * inv.x, d.y * inv.y, d.z * inv.z);
+        val[k] = base + p;
+#pragma unroll
+        for (int ps = 0; ps < kPasses; ++ps) atomicAdd(&s_hist[ps * 256 + ((key[k] >> (8 * ps)) & 255u)], 1u);
+      } else {
+        key[k] = 0xFFFFFFFFu;  // padding: the top digit in every pass, after every real key
+        val[k] = 0;
+      }
+    }
+    __syncthreads();
+    for (uint32_t q = tid; q < kPasses * 256; q += kThreads) {
+      const uint32_t h = s_hist[q];
+      if (h) atomicAdd(&ghist[q], h);
+      if (q < 256) counts[c * 256 + q] = h;  // pass 0: this tile's digit counts
+    }
+  }
+  if (!grid_sync(bar, 2, status, &s_flag)) return;
+
+  // ---------------- radix passes
+  {
+    uint32_t* s_wh = reinterpret_cast<uint32_t*>(smem);           // [kWarps][256]: counts, then starts
+    uint32_t* s_off = s_wh + kWarps * 256;                         // [256] global position - tile position
+    uint32_t* s_pre = s_off + 256;                                 // [2][256] counts of the earlier tiles
+    uint32_t* s_tmp = s_pre + 512;                                 // scan scratch
+    const uint32_t d_own = tid & 255u, half = tid >> 8;
+    for (int ps = 0; ps < kPasses; ++ps) {
+      const uint32_t sh = 8u * ps;
+      // counts of this pass's digit d_own in the earlier tiles (half of them per thread)
+      uint32_t pre = 0;
+      const uint32_t* cp = counts + (size_t)ps * kMaxTiles * 256 + d_own;
+      for (uint32_t q = half; q < c; q += 2) pre += __ldcg(cp + q * 256);
+      const uint32_t gcount = __ldcg(ghist + ps * 256 + d_own);
+      if (ps > 0) {
+        const uint32_t* ks = (ps & 1) ? ka : kb;  // written by the previous pass
+        const uint32_t* vs = (ps & 1) ? va : vb;
+#pragma unroll
+        for (int k = 0; k < kKpt; ++k) {
+          const uint32_t p = pos0 + 32 * k;
+          key[k] = p < cnt ? __ldcg(ks + base + p) : 0xFFFFFFFFu;
+          val[k] = p < cnt ? __ldcg(vs + base + p) : 0u;
+        }
+      }
+      for (uint32_t q = tid; q < kWarps * 256; q += kThreads) s_wh[q] = 0;
+      s_pre[half * 256 + d_own] = pre;
+      __syncthreads();
+      // rank among equal digits of the warp, in position order
+      uint32_t* wh = s_wh + warp * 256;
+      const uint32_t lt = lanemask_lt();
+      uint32_t rank[kKpt];
+#pragma unroll
+      for (int k = 0; k < kKpt; ++k) {
+        const uint32_t d = (key[k] >> sh) & 255u;
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t leader = __ffs(peers) - 1;
+        uint32_t before = 0;
+        if (lane == leader) before = atomicAdd(&wh[d], (uint32_t)__popc(peers));
+        before = __shfl_sync(0xFFFFFFFFu, before, leader);
+        rank[k] = before + __popc(peers & lt);
+      }
+      __syncthreads();
+      uint32_t total = 0;
+      if (tid < 256) {
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) total += s_wh[w * 256 + tid];
+      }
+      const uint32_t tstart = onesweep::scan256_exclusive<kThreads>(total, s_tmp);
+      const uint32_t gbase = onesweep::scan256_exclusive<kThreads>(tid < 256 ? gcount : 0u, s_tmp);
+      if (tid < 256) {
+        uint32_t run = tstart;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+          const uint32_t cw = s_wh[w * 256 + tid];
+          s_wh[w * 256 + tid] = run;
+          run += cw;
+        }
+        s_off[tid] = gbase + s_pre[tid] + s_pre[256 + tid] - tstart;
+      }
+      __syncthreads();
+      const bool last = ps == kPasses - 1;
+      uint32_t* kd = (ps & 1) ? kb : ka;
+      uint32_t* vd = (ps & 1) ? vb : va;
+      uint32_t* next_counts = counts + (size_t)(ps + 1) * kMaxTiles * 256;
+#pragma unroll
+      for (int k = 0; k < kKpt; ++k) {
+        const uint32_t p = pos0 + 32 * k;
+        const bool ok = p < cnt;
+        const uint32_t d = (key[k] >> sh) & 255u;
+        const uint32_t dst = s_off[d] + rank[k] + s_wh[warp * 256 + d];
+        if (last) {
+          if (ok && dst < n) {
+            t.morton_codes[dst] = key[k];
+            t.leaf_ids[dst] = val[k];
+            t.sort_keys[dst] = (uint64_t)key[k];
+          }
+        } else {
+          if (ok && dst < n) {
+            kd[dst] = key[k];
+            vd[dst] = val[k];
+          }
+          // the next pass's digit counts of the destination tile, one atomic
+          // per (tile, digit) run of the warp
+          const uint32_t tag = ok ? (((dst / kTile) << 8) | ((key[k] >> (sh + 8)) & 255u)) : 0xFFFFFFFFu;
+          const uint32_t same = __match_any_sync(0xFFFFFFFFu, tag);
+          if (ok && lane == (uint32_t)(__ffs(same) - 1) && dst < n)
+            atomicAdd(next_counts + tag, (uint32_t)__popc(same));
+        }
+      }
+      if (!grid_sync(bar, 3 + ps, status, &s_flag)) return;
+    }
+  }
+
+  // ---------------- phase H: hierarchy, refit and triangle records
+  {
+    float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(smem);
+    uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(smem + (size_t)kTile * 48);
+    int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(smem + (size_t)kTile * 56);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 64);
+    uint32_t* s_code = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 68);  // [kTile + 2]
+    const SegInfo g{0, n, 0};
+    for (uint32_t q = tid; q < kTile; q += kThreads) {
+      s_cnt[q] = 0;
+      s_code[q + 1] = base + q < n ? __ldcg(t.morton_codes + base + q) : 0u;
+    }
+    if (tid == 0) s_code[0] = base > 0 ? __ldcg(t.morton_codes + base - 1) : 0u;
+    if (tid == 1) s_code[kTile + 1] = base + kTile < n ? __ldcg(t.morton_codes + base + kTile) : 0u;
+    Climb cl[kKpt];
+#pragma unroll
+    for (int j = 0; j < kKpt; ++j) {
+      const uint32_t s = base + tid + j * kThreads;
+      cl[j].mode = 0;
+      cl[j].pending = -1;
+      cl[j].leaf = true;
+      cl[j].f = cl[j].l = s;
+      cl[j].dl = cl[j].dr = -1;
+      if (s < n) {
+        const uint32_t item = __ldcg(t.leaf_ids + s);
+        if (item >= n) {  // only after a failed sort
+          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+          continue;
+        }
+        const float* v = verts + (size_t)item * 9;
+        const f3 a = mk(__ldg(v + 0), __ldg(v + 1), __ldg(v + 2));
+        const f3 b = mk(__ldg(v + 3), __ldg(v + 4), __ldg(v + 5));
+        const f3 cc = mk(__ldg(v + 6), __ldg(v + 7), __ldg(v + 8));
+        float4* rec = reinterpret_cast<float4*>(t.leaf_tris + (size_t)s * 12);
+        rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(item));
+        rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
+        rec[2] = make_float4(cc.x, cc.y, cc.z, 0.0f);
+        cl[j].mn = vmin(vmin(a, b), cc);
+        cl[j].mx = vmax(vmax(a, b), cc);
+        cl[j].mode = 1;
+      }
+    }
+    __syncthreads();  // codes staged
+    // phase H1: splits whose sibling starts inside this tile, in shared memory
+#pragma unroll
+    for (int j = 0; j < kKpt; ++j) {
+      Climb& q = cl[j];
+      if (!q.mode) continue;
+      const uint32_t s = q.f, li = s;
+      if (li > 0) q.dl = delta_codes(s_code[s - base], li - 1, s_code[s - base + 1], li);
+      if (li + 1 < n) q.dr = delta_codes(s_code[s - base + 1], li, s_code[s - base + 2], li + 1);
+      for (int depth = 0;; ++depth) {
+        if (depth > 128) {
+          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+          q.mode = 0;
+          break;
+        }
+        const bool is_left = q.dr > q.dl;
+        const uint32_t gamma = is_left ? q.l : q.f - 1;
+        if (is_left ? (q.l + 1 >= base + kTile) : (q.f < base + 1)) break;  // crossing split: global
+        const uint32_t slot = gamma - base, side = is_left ? 0 : 1;
+        float* mine = s_box[slot][side];
+        mine[0] = q.mn.x; mine[1] = q.mn.y; mine[2] = q.mn.z; mine[3] = q.mx.x; mine[4] = q.mx.y; mine[5] = q.mx.z;
+        s_far[slot][side] = is_left ? q.f : q.l;
+        s_dfar[slot][side] = is_left ? q.dl : q.dr;
+        __threadfence_block();
+        if (atomicAdd(&s_cnt[slot], 1u) == 0) {
+          q.pending = (int)slot;
+          break;
+        }
+        __threadfence_block();
+        const float* sib = s_box[slot][side ^ 1];
+        const f3 smn = mk(sib[0], sib[1], sib[2]), smx = mk(sib[3], sib[4], sib[5]);
+        const uint32_t sfar = s_far[slot][side ^ 1];
+        const int sd = s_dfar[slot][side ^ 1];
+        const uint32_t F = is_left ? q.f : sfar, Lr = is_left ? sfar : q.l;
+        const int dL = is_left ? q.dl : sd, dR = is_left ? sd : q.dr;
+        const bool root = F == 0 && Lr == n - 1;
+        const uint32_t kn = root ? 0u : (dR > dL ? Lr : F);
+        if (is_left)
+          write_parent(g, kn, F, Lr, gamma, q.mn, q.mx, smn, smx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
+                       t.node_bounds);
+        else
+          write_parent(g, kn, F, Lr, gamma, smn, smx, q.mn, q.mx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
+                       t.node_bounds);
+        t.node_flags[gamma] = 2u;
+        q.mn = vmin(q.mn, smn);
+        q.mx = vmax(q.mx, smx);
+        q.f = F;
+        q.l = Lr;
+        q.dl = dL;
+        q.dr = dR;
+        q.leaf = false;
+        if (root) {
+          q.mode = 0;
+          break;
+        }
+      }
+    }
+    __syncthreads();  // every local climb of this tile has ended
+#pragma unroll
+    for (int j = 0; j < kKpt; ++j)
+      if (cl[j].mode && cl[j].pending >= 0 && s_cnt[cl[j].pending] != 1) cl[j].mode = 0;  // sibling came, went on
+    // phase H2: the splits that cross a tile boundary, in global memory.  The
+    // arrival word of split gamma (node_flags[gamma]) counts arrivals and
+    // carries the first arrival's leaf bit and far-end delta; its acq_rel
+    // add releases the first arrival's subtree, which the second reads.
+#pragma unroll
+    for (int j = 0; j < kKpt; ++j) {
+      Climb& q = cl[j];
+      for (int depth = 0; q.mode; ++depth) {
+        if (depth > 128) {
+          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+          break;
+        }
+        const bool is_left = q.dr > q.dl;
+        const uint32_t gamma = is_left ? q.l : q.f - 1;
+        uint32_t* flag = t.node_flags + gamma;
+        const int dfar = is_left ? q.dl : q.dr;
+        const uint32_t inc = kArrive | (q.leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
+        const uint32_t old = atomic_add_acq_rel_gpu(flag, inc);
+        if ((old & 0xFu) == 0) break;  // first: the sibling continues
+        const bool sib_leaf = (old & kLeafArrive) != 0;
+        const int sd = (int)((old >> 16) & 0x7Fu) - 1;
+        f3 smn, smx;
+        uint32_t sfar;
+        if (is_left) {  // sibling = right child, starts at gamma + 1
+          if (sib_leaf) {
+            sfar = gamma + 1;
+            tri_box(reinterpret_cast<const float4*>(t.leaf_tris) + (size_t)(gamma + 1) * 3, smn, smx);
+          } else {
+            const uint32_t ks = gamma + 1;
+            sfar = __ldcg(t.node_meta + (size_t)ks * 4 + 3);
+            const float4* nb = reinterpret_cast<const float4*>(t.node_bounds) + (size_t)ks * 3;
+            const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
+            smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
+            smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
+          }
+        } else {  // sibling = left child, ends at gamma
+          if (sib_leaf) {
+            sfar = gamma;
+            tri_box(reinterpret_cast<const float4*>(t.leaf_tris) + (size_t)gamma * 3, smn, smx);
+          } else {
+            const uint32_t ks = gamma;
+            sfar = gamma + 1 - __ldcg(t.node_leaf_counts + ks);
+            const float4* nb = reinterpret_cast<const float4*>(t.node_bounds) + (size_t)ks * 3;
+            const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
+            smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
+            smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
+          }
+        }
+        *flag = 2u;
+        const uint32_t F = is_left ? q.f : sfar, Lr = is_left ? sfar : q.l;
+        if (F > Lr || Lr >= n) {
+          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+          break;
+        }
+        const int dL = is_left ? q.dl : sd, dR = is_left ? sd : q.dr;
+        const bool root = F == 0 && Lr == n - 1;
+        const uint32_t kn = root ? 0u : (dR > dL ? Lr : F);
+        if (is_left)
+          write_parent(g, kn, F, Lr, gamma, q.mn, q.mx, smn, smx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
+                       t.node_bounds);
+        else
+          write_parent(g, kn, F, Lr, gamma, smn, smx, q.mn, q.mx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
+                       t.node_bounds);
+        if (root) break;
+        q.mn = vmin(q.mn, smn);
+        q.mx = vmax(q.mx, smx);
+        q.f = F;
+        q.l = Lr;
+        q.dl = dL;
+        q.dr = dR;
+        q.leaf = false;
+      }
+    }
+  }
+}
+
+// Launch state per device: the kernel attributes are set and the co-resident
+// CTA count is known.
+struct DeviceState {
+  bool ready = false;
+  int max_ctas = 0;
+};
+DeviceState g_fused_state[64];
+std::atomic<uint32_t> g_fused_max_leaves{kMaxLeaves};
+
+bool can_run(uint32_t n, uint32_t n_seg) {
+  return n_seg == 1 && n >= 2 && n <= g_fused_max_leaves.load(std::memory_order_relaxed) && n <= kMaxLeaves;
+}
+
+cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws, uint32_t* status, cudaStream_t st,
+                   bool* launched) {
+  *launched = false;
+  const uint32_t n = bvh->n_leaves;
+  const uint32_t G = (n + kTile - 1) / kTile;
+  const bool vec = ((uintptr_t)d_verts & 15) == 0;
+  auto kern = vec ? lbvh_fused_kernel<true> : lbvh_fused_kernel<false>;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64) return cudaSuccess;  // use the multi-launch build
+  DeviceState& ds = g_fused_state[dev];
+  if (!ds.ready) {
+    int per_sm_t = 0, per_sm_f = 0;
+    if ((e = cudaFuncSetAttribute(lbvh_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmem)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(lbvh_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmem)) != cudaSuccess)
+      return e;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, lbvh_fused_kernel<true>, kThreads, kSmem)) !=
+            cudaSuccess ||
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, lbvh_fused_kernel<false>, kThreads, kSmem)) !=
+            cudaSuccess)
+      return e;
+    ds.max_ctas = min(per_sm_t, per_sm_f) * sm_count();
+    ds.ready = true;
+  }
+  if ((int)G > ds.max_ctas) return cudaSuccess;  // not co-resident: use the multi-launch build
+  constexpr Layout kL0 = layout(0);
+  if ((e = cudaMemsetAsync(ws + kL0.off_bar, 0, kL0.zero_end - kL0.off_bar, st)) != cudaSuccess) return e;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(G);
+  cfg.blockDim = dim3(kThreads);
+  cfg.dynamicSmemBytes = kSmem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  BajoLbvh tcopy = *bvh;
+  e = cudaLaunchKernelEx(&cfg, kern, d_verts, n, tcopy, ws, status);
+  if (e == cudaSuccess) *launched = true;
+  return e;
+}
+}  // namespace fused
+
+// ---------------------------------------------------------------------------
 // staged top levels
 // ---------------------------------------------------------------------------
 // The first BAJO_TOP_NODES internal nodes of segment 0's tree in breadth-first
@@ -862,6 +1434,8 @@ BuildPlan make_build_plan(uint32_t n, uint32_t n_seg) {
   b.off_keys_alt = b.sort.off_keys_alt;
   b.off_vals_alt = b.sort.off_vals_alt;
   b.total = b.sort.total;
+  // room for the one-launch build as well (section 5)
+  if (n_seg == 1 && n <= fused::kMaxLeaves && fused::layout(n).total > b.total) b.total = fused::layout(n).total;
   return b;
 }
 
@@ -918,11 +1492,21 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   if (ws_bytes < need) return BAJO_ERR_WORKSPACE_TOO_SMALL;
   if (ev && n_ev < (int32_t)(5 + plan.passes)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream_;
+  unsigned char* ws = (unsigned char*)ws_;
+  uint32_t* status = (uint32_t*)ws;
+  // one scene of up to fused::kMaxLeaves triangles: the one-launch build
+  // (stage-timed builds keep the multi-launch kernels, whose stages they time)
+  if (!hploc && !ev && fused::can_run(n, S)) {
+    bool launched = false;
+    if (fused::launch(d_verts, bvh, ws, status, st, &launched) != cudaSuccess) return BAJO_ERR_CUDA;
+    if (launched) {
+      if (bvh->top_nodes && launch_stage_top(bvh, st) != cudaSuccess) return BAJO_ERR_CUDA;
+      return BAJO_OK;
+    }
+  }
   // stage events: [start, bounds, morton, pass 0..P-1, topology, refit]
   auto mark = [&](int i) { return !ev || cudaEventRecord(ev[i], st) == cudaSuccess; };
   if (!mark(0)) return BAJO_ERR_CUDA;
-  unsigned char* ws = (unsigned char*)ws_;
-  uint32_t* status = (uint32_t*)ws;
   if (cudaMemsetAsync(ws + plan.sort.off_zero, 0, plan.sort.zero_bytes, st) != cudaSuccess) return BAJO_ERR_CUDA;
   uint32_t* seg_ord = (uint32_t*)(ws + plan.off_seg_ord);
   const uint32_t blocks = (n + kBlock - 1) / kBlock;
@@ -1034,6 +1618,31 @@ int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream) {
       ((uintptr_t)bvh->top_nodes & 15))
     return BAJO_ERR_INVALID_ARGUMENT;
   return bajo::launch_stage_top(bvh, (cudaStream_t)stream) == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves) {
+  if (max_leaves > bajo::fused::kMaxLeaves) return BAJO_ERR_TOO_LARGE;
+  bajo::fused::g_fused_max_leaves.store(max_leaves, std::memory_order_relaxed);
+  return BAJO_OK;
+}
+
+int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* launches) {
+  using namespace bajo;
+  if (!launches || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  if (n_tris > BAJO_SORT_MAX_KEYS) return BAJO_ERR_TOO_LARGE;
+  if (fused::can_run(n_tris, n_segments)) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
+      const fused::DeviceState& ds = fused::g_fused_state[dev];
+      if (!ds.ready || (int)((n_tris + fused::kTile - 1) / fused::kTile) <= ds.max_ctas) {
+        *launches = 1;
+        return BAJO_OK;
+      }
+    }
+  }
+  const BuildPlan plan = make_build_plan(n_tris, n_segments);
+  *launches = (int32_t)(2 + (n_tris > 1 ? plan.passes : 0) + (n_tris <= kMergedMaxLeaves ? 1 : 2));
+  return BAJO_OK;
 }
 
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {

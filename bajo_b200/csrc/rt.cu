@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "mlp.cuh"
+#include "cwbvh.cuh"
 #include "sampling.cuh"
 #include "traverse.cuh"
 
@@ -97,7 +98,67 @@ struct SceneView {
   const float* metals;       // 4 per metal: albedo rgb, fuzz
   const float* dielectrics;  // 1 per dielectric: refraction index
   bool has_materials;
+  bool use_cw;  // trace through the compressed 8-wide tree (BajoRtScene::cwbvh8)
+  cw::Tree cw;
 };
+
+// The hit triangle's first vertex, outward normal and item index from its
+// record: a sorted BVH2 leaf record [v0, prim | v1, 0 | v2, 0] (the normal
+// from v1 - v0 and v2 - v0), or a CWBVH8 record [e1, 0 | e2, 0 | v0, prim]
+// whose edges were computed the same way at its build.  Both give the same
+// bits for the same triangle.
+struct TriFrame {
+  f3 v0, outward;
+  uint32_t prim;
+};
+template <bool CW>
+__device__ __forceinline__ TriFrame tri_frame(const SceneView& sc, uint32_t rec) {
+  TriFrame fr;
+  if constexpr (CW) {
+    const float4 a = __ldg(sc.cw.tris + (size_t)rec * 3 + 0);
+    const float4 b = __ldg(sc.cw.tris + (size_t)rec * 3 + 1);
+    const float4 cc = __ldg(sc.cw.tris + (size_t)rec * 3 + 2);
+    fr.v0 = mk(cc.x, cc.y, cc.z);
+    fr.outward = normalize(cross(mk(a.x, a.y, a.z), mk(b.x, b.y, b.z)));
+    fr.prim = __float_as_uint(cc.w);
+  } else {
+    const float4 a = __ldg(sc.tris + (size_t)rec * 3 + 0);
+    const float4 b = __ldg(sc.tris + (size_t)rec * 3 + 1);
+    const float4 cc = __ldg(sc.tris + (size_t)rec * 3 + 2);
+    fr.v0 = mk(a.x, a.y, a.z);
+    fr.outward = normalize(cross(mk(b.x, b.y, b.z) - fr.v0, mk(cc.x, cc.y, cc.z) - fr.v0));
+    fr.prim = __float_as_uint(a.w);
+  }
+  return fr;
+}
+
+// Closest hit of one path ray: (distance, record, item); record = kEmpty on
+// a miss.  BVH2: the watertight test, ties to the lowest item id; CWBVH8:
+// the reference's own walk and Moller-Trumbore test, first of equal-distance
+// hits in visiting order.
+struct PathHit {
+  float t;
+  uint32_t rec, prim;
+};
+template <bool CW>
+__device__ __forceinline__ PathHit trace_path(const SceneView& sc, f3 o, f3 d, float tmin, float tmax,
+                                              uint32_t* status) {
+  PathHit ph;
+  if constexpr (CW) {
+    const cw::Hit h = cw::trace<false>(o, d, tmin, tmax, sc.cw, status);
+    ph.t = h.t;
+    ph.rec = h.tri;
+    ph.prim = h.prim;
+  } else {
+    const Ray r = trav::make_ray(o, d, tmin, tmax);
+    const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
+                                                        status);
+    ph.t = h.t;
+    ph.rec = h.leaf;
+    ph.prim = h.prim;
+  }
+  return ph;
+}
 
 // warp-aggregated queue append: one atomic per warp; every lane of the warp
 // must call it (want = false for lanes with nothing to append)
@@ -239,7 +300,7 @@ __device__ __forceinline__ f3 vmf_sample(const float* mu, float kappa, float u, 
 // 8 blocks of 128 per SM (64 registers, a few bytes spilled): the traversal is
 // latency bound and 32 resident warps hide more of it than 24 unspilled ones
 // (C2 render 142 ms against 159 ms at 80 registers).
-template <int ALGO>
+template <int ALGO, bool CW>
 __global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
                                                        uint32_t sample_base) {
   constexpr bool kMisWeights = ALGO == BAJO_RENDER_MIS || ALGO == BAJO_RENDER_GUIDED;
@@ -274,18 +335,12 @@ __global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q
           c.rec_snap[3 * (size_t)rec + 2] = q.radiance[2 * cap + sidx];
         }
       }
-      const Ray r = trav::make_ray(o, d, tmin, tmax);
-      const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris, sc.n_nodes,
-                                                          q.status);
-      if (h.leaf == kEmpty) {
+      const PathHit h = trace_path<CW>(sc, o, d, tmin, tmax, q.status);
+      if (h.rec == kEmpty) {
         accumulate(q, sidx, mul(T, sky(d)));
       } else {
         const float t = h.t;
-        const float4 a = __ldg(sc.tris + (size_t)h.leaf * 3 + 0);
-        const float4 b = __ldg(sc.tris + (size_t)h.leaf * 3 + 1);
-        const float4 cc = __ldg(sc.tris + (size_t)h.leaf * 3 + 2);
-        const f3 v0 = mk(a.x, a.y, a.z);
-        const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(cc.x, cc.y, cc.z) - v0));
+        const f3 outward = tri_frame<CW>(sc, h.rec).outward;
         const bool front = dot(d, outward) < 0.0f;
         const f3 normal = front ? outward : neg(outward);
         const uint32_t surface = __ldg(sc.surfaces + h.prim);
@@ -316,7 +371,7 @@ __global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q
           vt = T;
         } else if (kind == BAJO_MAT_METAL || kind == BAJO_MAT_DIELECTRIC) {
           want_mat = true;
-          mat_leaf = h.leaf;
+          mat_leaf = h.rec;
           mat_t = t;
         }
       }
@@ -561,7 +616,7 @@ __global__ void __launch_bounds__(kBlock) shade_kernel(SceneView sc, Queues q, S
 // bounce's BSDF stream, and the continued path (Russian roulette as for
 // Lambertian bounces) carries the sample's pdf and delta flag.  No light
 // sample is taken at these vertices, as in the reference.
-template <int ALGO>
+template <int ALGO, bool CW>
 __global__ void __launch_bounds__(kBlock) material_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
                                                           uint32_t max_depth, uint64_t seed) {
   const uint32_t cap = q.capacity;
@@ -584,14 +639,11 @@ __global__ void __launch_bounds__(kBlock) material_kernel(SceneView sc, Queues q
       const f3 o = mk(src[0 * cap + idx], src[1 * cap + idx], src[2 * cap + idx]);
       const f3 d = mk(src[4 * cap + idx], src[5 * cap + idx], src[6 * cap + idx]);
       const f3 T = mk(src[8 * cap + idx], src[9 * cap + idx], src[10 * cap + idx]);
-      const float4 a = __ldg(sc.tris + (size_t)leaf * 3 + 0);
-      const float4 b = __ldg(sc.tris + (size_t)leaf * 3 + 1);
-      const float4 cc = __ldg(sc.tris + (size_t)leaf * 3 + 2);
-      const f3 v0 = mk(a.x, a.y, a.z);
-      const f3 outward = normalize(cross(mk(b.x, b.y, b.z) - v0, mk(cc.x, cc.y, cc.z) - v0));
+      const TriFrame fr = tri_frame<CW>(sc, leaf);
+      const f3 outward = fr.outward;
       const bool front = dot(d, outward) < 0.0f;
       const f3 normal = front ? outward : neg(outward);
-      const uint32_t surface = __ldg(sc.surfaces + __float_as_uint(a.w));
+      const uint32_t surface = __ldg(sc.surfaces + fr.prim);
       const uint32_t midx = surface & kIndexMask28;
       p = mk(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
       const float4 u = uniform4(seed, path_id, stage_bsdf(bounce));
@@ -693,6 +745,7 @@ __global__ void __launch_bounds__(kShadeThreads, 2) guided_shade_kernel(SceneVie
 // ---------------------------------------------------------------------------
 // any-hit shadow rays (gpu_rt_shadow_kernel, scene_trace.mojo:586)
 // ---------------------------------------------------------------------------
+template <bool CW>
 __global__ void __launch_bounds__(kBlock) shadow_kernel(SceneView sc, Queues q, uint32_t bounce,
                                                         uint32_t sample_base) {
   const uint32_t count = q.counters[2 * bounce + 1];
@@ -701,10 +754,16 @@ __global__ void __launch_bounds__(kBlock) shadow_kernel(SceneView sc, Queues q, 
   for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < count; i += gridDim.x * kBlock) {
     const f3 o = mk(f[0 * cap + i], f[1 * cap + i], f[2 * cap + i]);
     const f3 d = mk(f[4 * cap + i], f[5 * cap + i], f[6 * cap + i]);
-    const Ray r = trav::make_ray(o, d, f[3 * cap + i], f[7 * cap + i]);
-    const Hit h = trav::trace_bvh2<BAJO_TRI_WATERTIGHT, false, true>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris,
-                                                                     sc.n_nodes, q.status);
-    if (h.leaf == kEmpty) {
+    bool open;
+    if constexpr (CW) {
+      open = cw::trace<true>(o, d, f[3 * cap + i], f[7 * cap + i], sc.cw, q.status).t != 0.0f;  // t = 0: occluded
+    } else {
+      const Ray r = trav::make_ray(o, d, f[3 * cap + i], f[7 * cap + i]);
+      open = trav::trace_bvh2<BAJO_TRI_WATERTIGHT, false, true>(r, __ldg(sc.roots), sc.nb, sc.meta, sc.tris,
+                                                                sc.n_nodes, q.status)
+                 .leaf == kEmpty;
+    }
+    if (open) {
       const uint32_t sidx = q.shadow_ids[i] - sample_base;
       accumulate(q, sidx, mk(f[8 * cap + i], f[9 * cap + i], f[10 * cap + i]));
     }
@@ -861,6 +920,20 @@ bool make_views(const BajoRtScene* scene, unsigned char* w, const Layout& L, Sce
   sc.metals = scene->metals;
   sc.dielectrics = scene->dielectrics;
   sc.has_materials = scene->metals || scene->dielectrics;
+  // the compressed 8-wide tree, when the scene names one: a single-segment
+  // build over the same triangles (bajo_cwbvh8_build of scene->bvh)
+  sc.use_cw = scene->cwbvh8 != nullptr;
+  sc.cw = cw::Tree{};
+  if (sc.use_cw) {
+    const BajoCwbvh8* c = scene->cwbvh8;
+    if (c->n_segments != 1 || !c->nodes || !c->triangles || scene->cwbvh8_nodes == 0 ||
+        ((uintptr_t)c->nodes & 15) || ((uintptr_t)c->triangles & 15))
+      return false;
+    sc.cw.nodes = reinterpret_cast<const float4*>(c->nodes);
+    sc.cw.tris = reinterpret_cast<const float4*>(c->triangles);
+    sc.cw.n_nodes = scene->cwbvh8_nodes;
+    sc.cw.n_tris = c->n_tris;
+  }
   for (int k = 0; k < 2; ++k) {
     q.ids[k] = (uint32_t*)(w + L.off_ids[k]);
     q.fields[k] = (float*)(w + L.off_fields[k]);
@@ -884,23 +957,30 @@ ShadeCtx shade_ctx(unsigned char* w, const Layout& L, const Queues& q, uint32_t 
   return c;
 }
 
-template <int ALGO>
-cudaError_t launch_bounce(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t grid, uint32_t b,
-                          uint32_t max_depth, uint32_t sample_base, uint64_t seed, cudaStream_t st) {
-  trace_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, sample_base);
+template <int ALGO, bool CW>
+cudaError_t launch_bounce_tree(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t grid, uint32_t b,
+                               uint32_t max_depth, uint32_t sample_base, uint64_t seed, cudaStream_t st) {
+  trace_kernel<ALGO, CW><<<grid, kBlock, 0, st>>>(sc, q, c, b, sample_base);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
   if ((e = cudaGetLastError()) != cudaSuccess) return e;
   if (sc.has_materials) {
-    material_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, seed);
+    material_kernel<ALGO, CW><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, seed);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
   if (ALGO != BAJO_RENDER_PATH) {
-    shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
+    shadow_kernel<CW><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
     e = cudaGetLastError();
   }
   return e;
+}
+
+template <int ALGO>
+cudaError_t launch_bounce(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t grid, uint32_t b,
+                          uint32_t max_depth, uint32_t sample_base, uint64_t seed, cudaStream_t st) {
+  return sc.use_cw ? launch_bounce_tree<ALGO, true>(sc, q, c, grid, b, max_depth, sample_base, seed, st)
+                   : launch_bounce_tree<ALGO, false>(sc, q, c, grid, b, max_depth, sample_base, seed, st);
 }
 
 // Chunks of whole pixels: primary rays, `bounce(chunk, b)` per bounce, an
@@ -1031,16 +1111,21 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   const uint32_t grid = bounce_grid(L.cap);
   if (!rb && cudaMemsetAsync(gc.rec_hdr, 0, 8, st) != cudaSuccess) return BAJO_ERR_CUDA;
   auto bounce = [&](uint32_t b, uint32_t sample_base) {
-    trace_kernel<BAJO_RENDER_GUIDED><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
+    if (sc.use_cw) trace_kernel<BAJO_RENDER_GUIDED, true><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
+    else trace_kernel<BAJO_RENDER_GUIDED, false><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     guided_shade_kernel<<<shade_grid, kShadeThreads, smem, st>>>(sc, q, gc, b, s->max_depth, sample_base, s->seed);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if (sc.has_materials) {
-      material_kernel<BAJO_RENDER_GUIDED><<<grid, kBlock, 0, st>>>(sc, q, gc, b, s->max_depth, s->seed);
+      if (sc.use_cw)
+        material_kernel<BAJO_RENDER_GUIDED, true><<<grid, kBlock, 0, st>>>(sc, q, gc, b, s->max_depth, s->seed);
+      else
+        material_kernel<BAJO_RENDER_GUIDED, false><<<grid, kBlock, 0, st>>>(sc, q, gc, b, s->max_depth, s->seed);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    shadow_kernel<<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
+    if (sc.use_cw) shadow_kernel<true><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
+    else shadow_kernel<false><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
     return cudaGetLastError();
   };
   auto before = [&]() {

@@ -16,7 +16,7 @@ from dataclasses import dataclass
 import numpy as np
 import torch
 
-from . import _lib, bvh
+from . import _lib, bvh, wide
 
 PATH = 0
 NEE = 3
@@ -28,7 +28,16 @@ class BajoRtSceneC(ctypes.Structure):
     _fields_ = [("bvh", ctypes.POINTER(_lib.BajoLbvhC)), ("surfaces", ctypes.c_void_p),
                 ("lambertians", ctypes.c_void_p), ("emissives", ctypes.c_void_p), ("lights", ctypes.c_void_p),
                 ("n_lights", ctypes.c_uint32), ("total_light_weight", ctypes.c_float),
-                ("metals", ctypes.c_void_p), ("dielectrics", ctypes.c_void_p)]
+                ("metals", ctypes.c_void_p), ("dielectrics", ctypes.c_void_p),
+                ("cwbvh8", ctypes.POINTER(_lib.BajoCwbvh8C)), ("cwbvh8_nodes", ctypes.c_uint32)]
+
+# Acceleration structure of the path tracer's rays (the reference's
+# GPU_RT_BVH_* policies, bajo/rt/gpu/prepared_scene.mojo:29-33):
+#  "lbvh"          the binary LBVH (watertight test, ties to the lowest id)
+#  "cwbvh8"        the compressed 8-wide tree collapsed from the LBVH
+#  "cwbvh8_hploc"  the compressed 8-wide tree collapsed from an H-PLOC tree
+#                  (the reference's default, GPU_RT_BVH_CWBVH8_HPLOC)
+BVH_POLICIES = ("lbvh", "cwbvh8", "cwbvh8_hploc")
 
 
 class BajoRenderSettingsC(ctypes.Structure):
@@ -70,10 +79,14 @@ class GpuRtTriangleScene:
     """A scene resident on the GPU: LBVH, surfaces, materials, lights
     (GpuRtTriangleScene, bajo/rt/gpu/triangle_path.mojo:57)."""
 
-    def __init__(self, scene, device="cuda"):
+    def __init__(self, scene, device="cuda", bvh_policy: str = "lbvh"):
+        if bvh_policy not in BVH_POLICIES:
+            raise ValueError(f"bvh_policy must be one of {BVH_POLICIES}")
         self.host = scene
+        self.bvh_policy = bvh_policy
         self.vertices = torch.from_numpy(scene.vertices).to(device)
-        self.tree = bvh.build_triangle_bvh(self.vertices)
+        self.tree = bvh.build_triangle_bvh(self.vertices, method="hploc" if bvh_policy == "cwbvh8_hploc" else "lbvh")
+        self.cwbvh8 = wide.build_cwbvh8(self.tree) if bvh_policy.startswith("cwbvh8") else None
         self.surfaces = torch.from_numpy(scene.surfaces.view(np.int32)).to(device)
         self.lambertians = torch.from_numpy(scene.lambertians).to(device)
         self.emissives = torch.from_numpy(scene.emissives).to(device)
@@ -97,6 +110,9 @@ class GpuRtTriangleScene:
         s.total_light_weight = self.total_light_weight
         s.metals = None if self.metals is None else self.metals.data_ptr()
         s.dielectrics = None if self.dielectrics is None else self.dielectrics.data_ptr()
+        if self.cwbvh8 is not None:
+            s.cwbvh8 = ctypes.pointer(self.cwbvh8._c)
+            s.cwbvh8_nodes = self.cwbvh8.n_nodes
         return s
 
 

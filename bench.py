@@ -37,9 +37,16 @@ WIDTH = HEIGHT = 1024
 METRIC = "LBVH build Mtri/s"
 UNIT = "Mtri/s"
 WORKLOAD = "plain LBVH build of 65,536 random triangles (seed 0) + 1024x1024 closest-hit camera rays"
-# Algorithmic bytes of one onesweep digit pass over the LBVH sort: read and
-# write one u64 key and one u32 payload per triangle.
+# Algorithmic bytes of one onesweep digit pass over the LBVH sort (the
+# per-stage build): read and write one u64 key and one u32 payload per key.
 PASS_BYTES_PER_KEY = 24
+# Algorithmic bytes per triangle of the one-launch build kernel: bounds
+# (vertices 36 read, leaf bounds 24 written, arrival counter 4 cleared), four
+# radix passes over u32 code + u32 id (8 written; 16 read and written twice;
+# 8 read + 16 written as codes, ids and u64 keys), hierarchy (codes 4, ids 4
+# and vertices 36 read; triangle record 48, node meta 16, node boxes 48, leaf
+# count 4, arrival counter 4 and parent link 4 written).
+FUSED_BYTES_PER_TRI = 36 + 24 + 4 + 8 + 2 * 16 + 24 + 44 + 124
 # digit passes of the single-scene LBVH sort: 8-bit digits over the 30-bit
 # Morton code, bits [0, 32) (the reference CPU builder's four byte passes,
 # bajo/bvh/cpu/builder/lbvh.mojo:56-62)
@@ -336,9 +343,9 @@ def run_bajo(args):
     L.bajo_lbvh_stage_count(N_TRIS, 1, ctypes.byref(n_ev))
     n_ev = n_ev.value
     passes = n_ev - 5
-    # bounds, Morton, the sort passes, then one bottom-up hierarchy kernel (up
-    # to 2^17 triangles) or topology + refit
-    kernels_per_build = (3 if N_TRIS <= 1 << 17 else 4) + passes
+    launches = ctypes.c_int32(0)
+    _lib.check(L.bajo_lbvh_build_launches(N_TRIS, 1, ctypes.byref(launches)), "bajo_lbvh_build_launches")
+    kernels_per_build = launches.value  # 1: the one-launch build
 
     def build_timed(events):
         arr = (ctypes.c_void_p * n_ev)(*[e.cuda_event for e in events])
@@ -409,12 +416,16 @@ def run_bajo(args):
     value = world * N_TRIS * args.steps / build_total / 1e6
     mrays = world * n_rays * args.steps / trace_total / 1e6
 
-    # ---- roofline: onesweep digit pass, the build's dominant kernel
+    # ---- roofline: the build's one kernel (lbvh_fused_kernel); its duration
+    # is the timed build's (the build is that launch plus a 4 KB memset)
     peak, peak_kind = measured_peaks()
+    build_avg_s = statistics.mean(build_ms) / 1e3
+    fused_bytes = FUSED_BYTES_PER_TRI * N_TRIS
+    achieved = fused_bytes / build_avg_s / 1e9
+    traffic = committed_traffic().get("lbvh_fused_65536")
+    # the per-stage build's onesweep pass, for comparison
     pass_avg_s = statistics.mean(pass_ms) / 1e3
     pass_bytes = PASS_BYTES_PER_KEY * N_TRIS
-    achieved = pass_bytes / pass_avg_s / 1e9
-    traffic = committed_traffic().get("onesweep_pass_65536")
     trace_dram = committed_traffic().get("trace_camera_65536")
 
     # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
@@ -476,10 +487,20 @@ def run_bajo(args):
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     copy_stream.wait_stream(stream)
+    h0 = time.perf_counter()
     e2e_pipelined(args.steps)
+    host_enqueue_us = (time.perf_counter() - h0) / args.steps * 1e6
     e_end.record(stream)
     e_end.synchronize()
     e2e_total = max_over_ranks(world, e_start.elapsed_time(e_end) / 1e3)
+    # the upload alone, to show what bounds the pipeline
+    h2d_ms = []
+    for _ in range(args.steps):
+        e_start.record(stream)
+        dev_v[0].copy_(pinned_v[0], non_blocking=True)
+        e_end.record(stream)
+        e_end.synchronize()
+        h2d_ms.append(e_start.elapsed_time(e_end))
     serial_ms = []
     for k in range(args.steps):
         flush.zero_()
@@ -519,21 +540,32 @@ def run_bajo(args):
         "warmup": args.warmup, "ms_per_step": round(build_total / args.steps * 1e3, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        "sort_passes": passes,
+        "sort_passes": 4 if kernels_per_build == 1 else passes,
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
                 "d2h_bytes_per_step": 12 * 4,
                 "what": "every step: pinned H2D of its vertices + bajo_lbvh_build + D2H of the root child boxes; "
                         "uploads on a copy stream into two device buffers overlap the previous step's build; "
                         "one event pair around all steps (device status read once after them)",
                 "serial_value": round(e2e_serial_value, 3),
-                "serial_what": "the same steps on one stream, one after another, each timed alone"},
-        "roofline": {"kernel": "onesweep digit pass (u64 key + u32 id)", "bound": "hbm",
+                "serial_what": "the same steps on one stream, one after another, each timed alone",
+                "h2d_us_median": round(statistics.median(h2d_ms) * 1e3, 1),
+                "h2d_gb_s": round(verts.numel() * 4 / (statistics.median(h2d_ms) / 1e3) / 1e9, 2),
+                "host_enqueue_us_per_step": round(host_enqueue_us, 1)},
+        "roofline": {"kernel": "lbvh_fused_kernel (the whole build in one cooperative launch)" if
+                     kernels_per_build == 1 else "per-stage build", "bound": "hbm",
                      "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "algorithmic_bytes_per_launch": pass_bytes, "avg_launch_us": round(pass_avg_s * 1e6, 3),
-                     "peak_kind": peak_kind},
-        "stages_ms": {k: round(v, 5) for k, v in stage.items()},
-        "stages_source": "separate instrumented builds with an event between every kernel",
+                     "algorithmic_bytes_per_launch": fused_bytes,
+                     "algorithmic_bytes_per_triangle": FUSED_BYTES_PER_TRI,
+                     "avg_launch_us": round(build_avg_s * 1e6, 3), "peak_kind": peak_kind},
+        "per_stage_build": {
+            "what": "the per-stage kernels (bajo_lbvh_build_timed: bounds, Morton, onesweep passes, hierarchy) with "
+                    "an event between every kernel",
+            "stages_ms": {k: round(v, 5) for k, v in stage.items()},
+            "onesweep_pass": {"achieved_gb_s": round(pass_bytes / pass_avg_s / 1e9, 2),
+                              "frac": round(pass_bytes / pass_avg_s / 1e9 / peak, 4),
+                              "avg_launch_us": round(pass_avg_s * 1e6, 3), "bytes_per_launch": pass_bytes,
+                              "traffic": committed_traffic().get("onesweep_pass_65536")}},
         "closest_hit": {"value": round(mrays, 3), "unit": "MRays/s", "ms": round(statistics.mean(trace_ms), 4),
                         "nodes_per_ray": round(nodes_per_ray, 3), "tris_per_ray": round(tris_per_ray, 3),
                         "roofline": {"bound": "hbm (instrumented bytes: node + triangle loads, mostly L2)",

@@ -44,6 +44,8 @@ extern "C" {
 #define BAJO_STATUS_WIDE_TIMEOUT 0x40u    /* wide collapse gave up on a task   */
 #define BAJO_STATUS_STAGE_TIMEOUT 0x80u   /* staged top levels did not arrive  */
 #define BAJO_STATUS_WAIT_TIMEOUT 0x100u   /* bajo_wait_selftest gave up        */
+#define BAJO_STATUS_GRID_TIMEOUT 0x200u   /* one-launch build: a grid barrier  */
+                                          /* wait gave up                      */
 
 /* triangle tests */
 #define BAJO_TRI_MT 0         /* Moller-Trumbore, bajo/core/intersect.mojo:415 */
@@ -170,9 +172,21 @@ int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* siz
  * triangle bounds, per-segment bounds, Morton keys, onesweep sort of the live
  * key bits, Karras topology, atomic-flag refit, sorted triangle packing.
  * d_verts: 9 floats per triangle [v0 xyz, v1 xyz, v2 xyz].  bvh->seg_offsets
- * and every output array must be set by the caller. */
+ * and every output array must be set by the caller.
+ * One scene (S = 1) of 2 .. 2^17 triangles is built by a single cooperative
+ * kernel launch (grid barriers between the phases; a barrier wait that runs
+ * out sets BAJO_STATUS_GRID_TIMEOUT); other builds launch one kernel per
+ * stage.  Both give the same arrays bit for bit. */
 int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                         void* stream);
+
+/* Largest scene (triangles) the one-launch build takes, at most 2^17 (the
+ * default); 0 sends every build through the per-stage kernels.  Process wide,
+ * like the sort tuning table: set it before building, not concurrently. */
+int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves);
+/* Kernel launches bajo_lbvh_build makes for n_tris triangles in n_segments
+ * segments on the current device (1 for the one-launch build). */
+int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* launches);
 
 /* H-PLOC build (GpuBvhBuildMethod.HPLOC, the reference's default builder,
  * triangle_bvh.mojo:472; build_hploc_multi_wave_kernel,
@@ -194,7 +208,9 @@ int32_t bajo_hploc_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace,
  * measure_stages / GpuBuildTimings (bajo/bvh/gpu/builder/lbvh.mojo:347-422):
  * `events` holds n_events cudaEvent_t handles created by the caller; the
  * build records them on `stream` at [start, bounds, morton, sort pass 0..P-1,
- * topology, refit].  bajo_lbvh_stage_count gives n_events = P + 5. */
+ * topology, refit].  bajo_lbvh_stage_count gives n_events = P + 5.  A
+ * stage-timed build always runs the per-stage kernels (whose stages it times),
+ * never the one-launch build. */
 int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                               void* stream, void* const* events, int32_t n_events);
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);
@@ -465,6 +481,15 @@ typedef struct BajoRtScene {
   float total_light_weight;  /* sum of area * mean(radiance) over the lights        */
   const float* metals;       /* 4 f32 per metal: albedo rgb, fuzz (NULL: none)     */
   const float* dielectrics;  /* 1 f32 refraction index per dielectric (NULL: none) */
+  /* Acceleration structure of the closest-hit and shadow rays: NULL traces
+   * bvh (the binary LBVH: watertight test, ties to the lowest triangle id);
+   * else this compressed 8-wide tree built from bvh by bajo_cwbvh8_build,
+   * with cwbvh8_nodes its node count (bajo_cwbvh8_count).  The CWBVH8 walk is
+   * the reference's default triangle path (GPU_RT_BVH_CWBVH8_*,
+   * bajo/rt/gpu/prepared_scene.mojo:29-33,52-53) with its own rules:
+   * Moller-Trumbore, first of equal-distance hits in visiting order. */
+  const struct BajoCwbvh8* cwbvh8;
+  uint32_t cwbvh8_nodes;
 } BajoRtScene;
 /* Metal and dielectric surfaces (_sample_metal / _sample_dielectric,
  * bajo/rt/shading.mojo:122-198; gpu_rt_shade_dispatch_kernel,

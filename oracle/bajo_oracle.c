@@ -1971,7 +1971,29 @@ typedef struct {
   uint64_t seed;
   int algorithm;
   float* sample_radiance; /* 3 per path, path_id order */
+  /* compressed 8-wide tree (NULL: trace bvh): bajo/rt/gpu/prepared_scene.mojo:29-33 */
+  const float* cw_nodes;
+  const float* cw_tris;
+  uint32_t cw_n_nodes, cw_n_tris;
 } rt_ctx;
+
+/* closest hit / occlusion of one path ray through the scene's tree: the
+ * binary LBVH (watertight, ties to the lowest id) or the CWBVH8 walk of
+ * trace_cwbvh8_triangles (its own visiting order and tie rule) */
+static bo_hit rt_closest(const rt_ctx* c, const bo_ray* r) {
+  if (c->cw_nodes) {
+    uint32_t err = 0;
+    return cwbvh8_one(c->cw_nodes, c->cw_tris, c->cw_n_nodes, c->cw_n_tris, r, 0, &err);
+  }
+  return trace_one(c->bvh, c->verts, r, 0, BO_TRI_WATERTIGHT, NULL);
+}
+static int rt_occluded(const rt_ctx* c, const bo_ray* r) {
+  if (c->cw_nodes) {
+    uint32_t err = 0;
+    return cwbvh8_one(c->cw_nodes, c->cw_tris, c->cw_n_nodes, c->cw_n_tris, r, 1, &err).t == 0.0f;
+  }
+  return any_hit(c->bvh, c->verts, r);
+}
 
 static inline uint32_t st_bsdf(uint32_t b) { return (0u << 30) | (b + 1); }
 static inline uint32_t st_roulette(uint32_t b) { return (1u << 30) | (b + 1); }
@@ -2006,7 +2028,7 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
   float rad[3] = {0.0f, 0.0f, 0.0f};
   for (uint32_t b = 0; b < c->max_depth; ++b) {
     bo_ray ray = make_ray_od(o, d, tmin, tmax);
-    bo_hit hit = trace_one(c->bvh, c->verts, &ray, 0, BO_TRI_WATERTIGHT, NULL);
+    bo_hit hit = rt_closest(c, &ray);
     if (hit.prim == BO_EMPTY) {
       v3 un = v3normalize(d);
       float a = 0.5f * (un.y + 1.0f);
@@ -2146,7 +2168,7 @@ static void rt_path(const rt_ctx* c, uint32_t path_id, float out[3]) {
         }
       }
     }
-    if (want_shadow && !any_hit(c->bvh, c->verts, &shadow)) {
+    if (want_shadow && !rt_occluded(c, &shadow)) {
       rad[0] += sh_c.x; rad[1] += sh_c.y; rad[2] += sh_c.z;
     }
     if (!alive) break;
@@ -2162,6 +2184,13 @@ static void rt_range(void* p, uint32_t b, uint32_t e) {
   for (uint32_t i = b; i < e; ++i) rt_path(c, i, c->sample_radiance + 3 * (size_t)i);
 }
 
+/* tree of the next bo_render call (set by bo_render_cwbvh8 around it) */
+static __thread struct {
+  const float* nodes;
+  const float* tris;
+  uint32_t n_nodes, n_tris;
+} g_render_cw;
+
 /* bo_render: pixels (3 f32, mean over samples in sample order) and optional
  * per-sample radiance.  Scene arrays as in BajoRtScene. */
 void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, const float* lambertians,
@@ -2172,7 +2201,8 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
   uint64_t n_paths = (uint64_t)width * height * spp;
   float* rad = sample_radiance ? sample_radiance : (float*)malloc(sizeof(float) * 3 * n_paths);
   rt_ctx c = {bvh, verts, surfaces, lambertians, emissives, lights, n_lights, total_weight, metals, dielectrics, cam,
-              width, height, spp, max_depth, seed, algorithm, rad};
+              width, height, spp, max_depth, seed, algorithm, rad, g_render_cw.nodes, g_render_cw.tris,
+              g_render_cw.n_nodes, g_render_cw.n_tris};
   rt_job job = {&c};
   bo_parallel_for((uint32_t)n_paths, n_threads, 256, rt_range, &job);
   float scale = 1.0f / (float)spp;
@@ -2187,6 +2217,26 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
     pixels[3 * px + 2] = b * scale;
   }
   if (!sample_radiance) free(rad);
+}
+
+/* bo_render through a compressed 8-wide tree (bajo_cwbvh8_build of the
+ * scene's single-segment tree): the reference's default triangle scene
+ * (prepared_scene.mojo:32-33,52-53). */
+void bo_render_cwbvh8(const float* cw_nodes, uint32_t cw_n_nodes, const float* cw_tris, uint32_t cw_n_tris,
+                      const float* verts, const uint32_t* surfaces, const float* lambertians, const float* emissives,
+                      const float* metals, const float* dielectrics, const float* lights, uint32_t n_lights,
+                      float total_weight, const float* cam, uint32_t width, uint32_t height, uint32_t spp,
+                      uint32_t max_depth, uint64_t seed, int algorithm, float* pixels, float* sample_radiance,
+                      uint32_t n_threads) {
+  g_render_cw.nodes = cw_nodes;
+  g_render_cw.tris = cw_tris;
+  g_render_cw.n_nodes = cw_n_nodes;
+  g_render_cw.n_tris = cw_n_tris;
+  bo_render(NULL, verts, surfaces, lambertians, emissives, metals, dielectrics, lights, n_lights, total_weight, cam,
+            width, height, spp, max_depth, seed, algorithm, pixels, sample_radiance, n_threads);
+  g_render_cw.nodes = NULL;
+  g_render_cw.tris = NULL;
+  g_render_cw.n_nodes = g_render_cw.n_tris = 0;
 }
 
 /* ========================================================================= */

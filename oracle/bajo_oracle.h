@@ -214,6 +214,14 @@ void bo_render(const BoLbvh* bvh, const float* verts, const uint32_t* surfaces, 
                uint32_t n_lights, float total_weight,
                const float* camera20, uint32_t width, uint32_t height, uint32_t spp, uint32_t max_depth,
                uint64_t seed, int algorithm, float* pixels, float* sample_radiance, uint32_t n_threads);
+/* bo_render through a compressed 8-wide tree (from bo_cwbvh8_build of the
+ * scene's single-segment tree) instead of the binary LBVH. */
+void bo_render_cwbvh8(const float* cw_nodes, uint32_t cw_n_nodes, const float* cw_tris, uint32_t cw_n_tris,
+                      const float* verts, const uint32_t* surfaces, const float* lambertians, const float* emissives,
+                      const float* metals, const float* dielectrics, const float* lights, uint32_t n_lights,
+                      float total_weight, const float* cam, uint32_t width, uint32_t height, uint32_t spp,
+                      uint32_t max_depth, uint64_t seed, int algorithm, float* pixels, float* sample_radiance,
+                      uint32_t n_threads);
 
 /* batched primary + one cosine bounce per pixel, segmented LBVH */
 void bo_trace_batch(const BoLbvh* bvh, const float* verts, const float* cams, uint32_t cam_stride, uint32_t width,

@@ -100,6 +100,8 @@ def _declare(L: ctypes.CDLL) -> None:
         "bo_rt_build_lights": (_I, [_P, _P, _U32, _P, _P, _U32, ctypes.POINTER(_U32), ctypes.POINTER(_F)]),
         "bo_render": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32, _U32,
                              ctypes.c_uint64, _I, _P, _P, _U32]),
+        "bo_render_cwbvh8": (None, [_P, _U32, _P, _U32, _P, _P, _P, _P, _P, _P, _P, _U32, _F, _P, _U32, _U32, _U32,
+                                    _U32, ctypes.c_uint64, _I, _P, _P, _U32]),
         "bo_wide_build": (None, [ctypes.POINTER(_BoLbvh), _P, _U32, _U32, _P, _P, _P, _P, _P, _P]),
         "bo_cwbvh8_build": (None, [ctypes.POINTER(_BoLbvh), _P, _P, _P, _P, _P]),
         "bo_rt_series_pow": (ctypes.c_float, [ctypes.c_float, ctypes.c_float]),
@@ -492,9 +494,11 @@ def rt_build_lights(scene):
 
 
 def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=4, lights=None, bvh=None,
-           threads=None, return_samples=False):
-    """CPU restatement of the wavefront tracer: (height, width, 3) pixels."""
-    if bvh is None:
+           threads=None, return_samples=False, cwbvh8=None):
+    """CPU restatement of the wavefront tracer: (height, width, 3) pixels.
+    ``cwbvh8`` (an OracleCwbvh8 of the scene's tree) traces through the
+    compressed 8-wide tree instead of the binary LBVH."""
+    if bvh is None and cwbvh8 is None:
         bvh = lbvh_build(scene.vertices)
     if lights is None:
         lights, n_lights, total = rt_build_lights(scene)
@@ -503,16 +507,22 @@ def render(scene, camera, width, height, spp, max_depth=8, seed=2026, algorithm=
     cam = np.ascontiguousarray(camera, np.float32)
     pixels = np.zeros(3 * width * height, np.float32)
     samples = np.zeros(3 * width * height * spp, np.float32) if return_samples else None
-    s = bvh.struct()
     metals = getattr(scene, "metals", None)
     dielectrics = getattr(scene, "dielectrics", None)
     metals = None if metals is None else np.ascontiguousarray(metals, np.float32).reshape(-1)
     dielectrics = None if dielectrics is None else np.ascontiguousarray(dielectrics, np.float32).reshape(-1)
-    lib().bo_render(ctypes.byref(s), _ptr(bvh.verts), _ptr(scene.surfaces), _ptr(scene.lambertians),
-                    _ptr(scene.emissives), None if metals is None else _ptr(metals),
-                    None if dielectrics is None else _ptr(dielectrics), _ptr(lights), n_lights, total, _ptr(cam),
-                    width, height, spp, max_depth,
-                    seed, algorithm, _ptr(pixels), None if samples is None else _ptr(samples), threads or n_threads())
+    tail = (_ptr(scene.surfaces), _ptr(scene.lambertians), _ptr(scene.emissives),
+            None if metals is None else _ptr(metals), None if dielectrics is None else _ptr(dielectrics),
+            _ptr(lights), n_lights, total, _ptr(cam), width, height, spp, max_depth, seed, algorithm, _ptr(pixels),
+            None if samples is None else _ptr(samples), threads or n_threads())
+    if cwbvh8 is not None:
+        verts = np.ascontiguousarray(scene.vertices, np.float32).reshape(-1)
+        n0 = int(cwbvh8.node_offsets[1]) - int(cwbvh8.node_offsets[0])
+        lib().bo_render_cwbvh8(_ptr(cwbvh8.nodes), n0, _ptr(cwbvh8.triangles), cwbvh8.triangles.size // CW_TRI_WORDS,
+                               _ptr(verts), *tail)
+    else:
+        s = bvh.struct()
+        lib().bo_render(ctypes.byref(s), _ptr(bvh.verts), *tail)
     img = pixels.reshape(height, width, 3)
     return (img, samples.reshape(height, width, spp, 3)) if return_samples else img
 
