@@ -1,11 +1,21 @@
-"""Project autotuner for the sort tile shapes and digit widths.
+"""Project autotuner: sort tile shapes and digit widths, closest-hit block
+sizes, and the size limit of the one-launch build front end.
 
-The sort kernels are compiled in several tile shapes (threads x keys per
-thread) and, for 64-bit keys, two digit widths (8 and 10 bits).  For each (key width, values, size bucket) the tuner times every
-shape the library allows on the current GPU with CUDA events and writes the
-fastest into the library's tuning table (``bajo_sort_tuning_set``).  Results
-are cached as JSON keyed by (kernel, size bucket, GPU name and SM count) so a
-process can load them instead of re-measuring.
+- The sort kernels are compiled in several tile shapes (threads x keys per
+  thread) and, for 64-bit keys, two digit widths (8 and 10 bits).  For each
+  (key width, values, size bucket) the tuner times every shape the library
+  allows on the current GPU with CUDA events and writes the fastest into the
+  library's table (``bajo_sort_tuning_set``).
+- The unstaged closest-hit kernels (camera and general rays) are compiled
+  for blocks of 64, 128 and 256 threads; the tuner times each per ray-count
+  bucket on a tree of the plain workload's kind, checks that the hits are
+  identical, and installs the fastest (``bajo_trace_tuning_set``).
+- The one-launch build front end is timed against the per-stage kernels at
+  every power of two up to its limit, and the largest size up to which it
+  wins is installed (``bajo_lbvh_fused_max_set``).
+
+Results are cached as JSON keyed by (kernel, size bucket, GPU name and SM
+count) so a process can load them instead of re-measuring.
 """
 from __future__ import annotations
 
@@ -85,6 +95,94 @@ def tune_sort(key_bytes: int, has_values: bool, log2ns, end_bit: int | None = No
     return out
 
 
+TRACE_BLOCKS = (128, 64, 256)
+_TRACE_KINDS = {"trace_camera": 0, "trace_rays": 1}
+
+
+def _events_ms(fn, reps):
+    stream = torch.cuda.current_stream()
+    fn()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    return statistics.median(ms)
+
+
+def tune_trace(kernel: str, log2rays, n_tris: int = 65536, reps: int = 5) -> dict:
+    """Time every block size of one closest-hit kernel ("trace_camera" or
+    "trace_rays") at 2^log2rays rays over n_tris random triangles, check that
+    every block size gives the same hits bit for bit, and install the
+    fastest.  Returns {log2rays: {"best": block, "ms": {...}}}."""
+    from . import bvh, camera, scenes
+    L = _lib.load()
+    kind = _TRACE_KINDS[kernel]
+    tree = bvh.build_triangle_bvh(torch.from_numpy(scenes.random_triangles(n_tris, seed=0)).cuda())
+    cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+    out = {}
+    for lg in log2rays:
+        n = 1 << lg
+        w = 1 << ((lg + 1) // 2)
+        h = n // w
+        hits = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+        if kind == 1:
+            g = torch.Generator(device="cuda").manual_seed(lg)
+            rays = torch.empty(8, n, dtype=torch.float32, device="cuda")
+            rays[0:3].uniform_(0.0, 1.0, generator=g)
+            rays[3].zero_()
+            d = torch.randn(3, n, device="cuda", generator=g)
+            rays[4:7] = d / d.norm(dim=0, keepdim=True)
+            rays[7].fill_(3.0e38)
+            rays = rays.reshape(-1)
+            fn = lambda: tree.launch_rays(rays, hits, n)  # noqa: E731
+        else:
+            fn = lambda: tree.launch_camera(cam, hits, n, w, h)  # noqa: E731
+        times, ref = {}, None
+        for blk in TRACE_BLOCKS:
+            _lib.check(L.bajo_trace_tuning_set(kind, lg, blk), "bajo_trace_tuning_set")
+            times[blk] = _events_ms(fn, reps)
+            got = hits.clone()
+            if ref is None:
+                ref = got
+            elif not torch.equal(got.view(torch.int32), ref.view(torch.int32)):
+                raise RuntimeError(f"{kernel}: block {blk} changed the hits")
+        best = min(times, key=times.get)
+        _lib.check(L.bajo_trace_tuning_set(kind, lg, best), "bajo_trace_tuning_set")
+        out[lg] = {"best": best, "ms": {str(k): round(t, 5) for k, t in times.items()}}
+    return out
+
+
+def tune_front_end(log2tris=range(11, 18), reps: int = 7) -> dict:
+    """Build time of one scene through the one-launch front end and through
+    the per-stage kernels at each size; installs the largest size up to
+    which the front end is faster.  Returns {log2n: {"best": limit, "ms": ...}}
+    with the same limit in every entry."""
+    from . import bvh, scenes
+    L = _lib.load()
+    out, limit = {}, 0
+    for lg in log2tris:
+        n = 1 << lg
+        v = torch.from_numpy(scenes.random_triangles(n, seed=lg)).cuda()
+        ws = bvh.GpuBvhBuildWorkspace(n, 1)
+        tree = bvh.build_triangle_bvh(v, workspace=ws)
+        t = {}
+        for name, lim in (("front_end", _lib.FUSED_MAX_LEAVES), ("per_stage", 0)):
+            _lib.check(L.bajo_lbvh_fused_max_set(lim), "bajo_lbvh_fused_max_set")
+            t[name] = _events_ms(lambda: bvh.build_triangle_bvh(v, workspace=ws, out=tree), reps)
+        if t["front_end"] < t["per_stage"] and limit == (n >> 1 if lg > min(log2tris) else 0):
+            limit = n
+        out[lg] = {"ms": {k: round(x, 5) for k, x in t.items()}}
+    _lib.check(L.bajo_lbvh_fused_max_set(limit), "bajo_lbvh_fused_max_set")
+    for lg in out:
+        out[lg]["best"] = limit
+    return out
+
+
 def save(results: dict, path: str = CACHE) -> None:
     data = {}
     if os.path.exists(path):
@@ -107,6 +205,15 @@ def load(path: str = CACHE) -> int:
     L = _lib.load()
     count = 0
     for kernel, entries in table.items():
+        if kernel in _TRACE_KINDS:
+            for lg, v in entries.items():
+                count += L.bajo_trace_tuning_set(_TRACE_KINDS[kernel], int(lg), int(v)) == _lib.OK
+            continue
+        if kernel == "lbvh_front_end":
+            limits = set(entries.values())
+            if len(limits) == 1:
+                count += L.bajo_lbvh_fused_max_set(int(limits.pop())) == _lib.OK
+            continue
         kb = 4 if "_u32_" in kernel else 8
         hv = kernel.endswith("pairs")
         for lg, v in entries.items():
@@ -124,6 +231,9 @@ def tune_all(reps: int = 5, save_cache: bool = True) -> dict:
     res = {
         _kernel_key(8, True): u64,
         _kernel_key(4, True): tune_sort(4, True, range(10, 27), reps=reps),
+        "trace_camera": tune_trace("trace_camera", range(16, 23, 2), reps=reps),
+        "trace_rays": tune_trace("trace_rays", range(16, 23, 2), reps=reps),
+        "lbvh_front_end": tune_front_end(reps=reps),
     }
     if save_cache:
         save(res)

@@ -228,11 +228,11 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
 //    child boxes, far range ends and their deltas in shared slots).  A split
 //    whose sibling lies (partly) outside meets in global memory after the
 //    CTA's local climbs are done: node_flags of the split counts the
-//    arrivals (acquire), the first arrival publishes its subtree (already
-//    written to the node arrays) with a release flag bit, and passes its far
-//    end's delta in the counter word; the second reads the sibling's box
-//    from its node record or triangle record.  node_flags ends at 2 for
-//    every internal node.
+//    arrivals with an acq_rel add, which releases the first arrival's subtree
+//    (already written to the node arrays) and passes its leaf bit and its far
+//    end's delta in the counter word; the second arrival's add acquires it,
+//    and it reads the sibling's box from its node record or triangle record.
+//    node_flags ends at 2 for every internal node.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kArrive = 1u;
 constexpr uint32_t kLeafArrive = 0x10u;   // the arrival is a leaf
@@ -416,15 +416,11 @@ __global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
     uint32_t* flag = node_flags + g.ib + lg;
     const int dfar = is_left ? dl : dr;
     const uint32_t inc = kArrive | (leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
-    const uint32_t old = atomic_add_acquire_gpu(flag, inc);
-    if ((old & 0xFu) == 0) {  // first: publish the subtree written above
-      red_add_release_gpu(flag, kBoxReady);
-      return;
-    }
-    if (!(old & kBoxReady) && !wait_bits_acquire(flag, kBoxReady, kRefitWaitNs)) {
-      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-      return;
-    }
+    // acq_rel: the first arrival's add releases the subtree it wrote (its
+    // node or triangle record); the second's add acquires it, so the second
+    // reads the sibling right after its own atomic
+    const uint32_t old = atomic_add_acq_rel_gpu(flag, inc);
+    if ((old & 0xFu) == 0) return;  // first: the sibling's climb continues
     const bool sib_leaf = (old & kLeafArrive) != 0;
     const int sd = (int)((old >> 16) & 0x7Fu) - 1;
     f3 smn, smx;
@@ -738,48 +734,56 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 }
 
 // ---------------------------------------------------------------------------
-// 5. One-launch build of one scene of up to fused::kMaxLeaves triangles
-//    (the whole of sections 1-3 for a single segment, in one cooperative
-//    launch).
+// 5. One-launch front end of the build of one scene of up to
+//    fused::kMaxLeaves triangles: bounds, Morton keys and the sort in one
+//    cooperative launch, followed by hierarchy_kernel (section 3).
 //
-//    At 65,536 triangles every kernel of the multi-launch build is latency
-//    bound: a few microseconds of work each, behind a chain of dependent
-//    global round trips.  Here one CTA per kTile sorted leaves runs every
-//    phase, and phases meet at grid-wide barriers (bounded waits,
-//    BAJO_STATUS_GRID_TIMEOUT):
-//      A  triangle bounds, root and centroid bounds    -> barrier 1
-//      B  Morton codes (kept in registers), the digit histograms of every
-//         pass, and tile 0's digit counts of pass 0    -> barrier 2
-//      P0..P3  LSD radix passes over the 30-bit code, 8-bit digits: each
-//         tile ranks its keys (stable, in position order) and scatters them
-//         to  base(digit) + counts of the digit in earlier tiles + rank.
-//         While it scatters, it counts the next pass's digits per
-//         destination tile with global atomics, so the next pass finds its
-//         per-tile counts complete after a single barrier -> barriers 3-6
-//      H  the bottom-up hierarchy + refit of hierarchy_kernel with kTile
-//         leaves per CTA: more of the climb stays in shared memory, and the
-//         splits that cross tiles meet through one acq_rel atomic per level
-//         (the first arrival's subtree is written before its atomic, so the
-//         second reads it right after its own).
-//    Every output array is bit-identical to the multi-launch build's (same
-//    stable sort, same tree, same numbering).
+//    At 65,536 triangles every kernel of the per-stage build is latency
+//    bound, and the sort is four onesweep passes of about 10 us each.  Here
+//    one CTA per kTile keys runs the phases, which meet at grid-wide barriers
+//    (bounded waits, BAJO_STATUS_GRID_TIMEOUT):
+//      A  triangle bounds, root and centroid bounds              -> barrier 1
+//      B  Morton codes (kept in registers), the histogram of the top
+//         kBucketBits code bits, and every LSD pass's digit histogram
+//                                                                 -> barrier 2
+//    Sort, fast path (every bucket holds at most kBucketMax keys, which
+//    every CTA reads off the same histogram):
+//      S1 each key goes to its bucket's range of a scratch buffer (slot from
+//         a per-bucket atomic counter, so the order inside a bucket is
+//         arbitrary)                                              -> barrier 3
+//      S2 each CTA takes the buckets that start inside its tile, loads them
+//         into shared memory and ranks every key inside its bucket by
+//         (code, item id).  Item ids are unique, so this is exactly the
+//         order of a stable sort by code: the multi-pass LSD sort's output.
+//    Sort, otherwise: LSD radix passes over the 30-bit code (8-bit digits):
+//    each tile ranks its keys (stable, in position order) and scatters them
+//    to base(digit) + counts of the digit in earlier tiles + rank, counting
+//    the next pass's digits per destination tile as it scatters, so a pass
+//    needs one barrier                                            -> barriers 3-6
+//    Every output array is bit-identical to the per-stage build's.
 // ---------------------------------------------------------------------------
 namespace fused {
 constexpr int kThreads = 512;
-constexpr int kKpt = 4;                              // keys (and leaves) per thread
-constexpr uint32_t kTile = kThreads * kKpt;          // sorted leaves per CTA
+constexpr int kKpt = 4;                              // keys per thread
+constexpr uint32_t kTile = kThreads * kKpt;          // keys per CTA
 constexpr uint32_t kMaxLeaves = 1u << 17;
 constexpr uint32_t kMaxTiles = kMaxLeaves / kTile;  // 64
-constexpr int kPasses = 4;                           // digits [0,8) [8,16) [16,24) [24,30)
+constexpr int kPasses = 4;                           // LSD digits [0,8) [8,16) [16,24) [24,30)
 constexpr int kWarps = kThreads / 32;
+constexpr int kBucketBits = 12;                      // buckets: the top 12 of the 30 code bits
+constexpr uint32_t kBuckets = 1u << kBucketBits;
+constexpr uint32_t kBucketShift = 30 - kBucketBits;
+constexpr uint32_t kBucketMax = 256;                 // fast path: no bucket larger than this
+constexpr uint32_t kOwnedMax = kTile + kBucketMax;   // keys a CTA owns on the fast path, at most
 constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
 
 // Workspace (bytes from the start of the build workspace; word 0 is the
-// status word): barrier counter, ordered segment bounds and the digit
-// histograms (zeroed before the launch), per-(pass, tile) digit counts, and
-// two key / payload buffers for the passes.
+// status word): barrier counter, ordered segment bounds and the LSD digit
+// histograms (zeroed before the launch); bucket histogram and fill counters
+// (zeroed by phase A); per-(pass, tile) digit counts; two key / item buffers.
 struct Layout {
-  size_t off_bar, off_seg_ord, off_ghist, zero_end, off_counts, off_ka, off_va, off_kb, off_vb, total;
+  size_t off_bar, off_seg_ord, off_ghist, zero_end, off_bhist, off_bfill, off_counts, off_ka, off_va, off_kb, off_vb,
+      total;
 };
 __host__ __device__ constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 __host__ __device__ constexpr Layout layout(uint32_t n) {
@@ -788,7 +792,9 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
   l.off_seg_ord = 320;
   l.off_ghist = 384;
   l.zero_end = l.off_ghist + (size_t)kPasses * 256 * 4;
-  l.off_counts = a256(l.zero_end);
+  l.off_bhist = a256(l.zero_end);
+  l.off_bfill = l.off_bhist + (size_t)kBuckets * 4;
+  l.off_counts = a256(l.off_bfill + (size_t)kBuckets * 4);
   l.off_ka = a256(l.off_counts + (size_t)kPasses * kMaxTiles * 256 * 4);
   l.off_va = a256(l.off_ka + (size_t)n * 4);
   l.off_kb = a256(l.off_va + (size_t)n * 4);
@@ -798,12 +804,11 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
 }
 
 // Shared memory, one buffer reused by the phases.
-constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;  // phase A
-constexpr size_t kSmemHier = (size_t)kTile * 48 + (size_t)kTile * 8 + (size_t)kTile * 8 + (size_t)kTile * 4 +
-                             (size_t)(kTile + 2) * 4;  // phase H
-constexpr size_t kSmemSort = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
-constexpr size_t kSmem = ((kSmemHier > kSmemVerts ? (kSmemHier > kSmemSort ? kSmemHier : kSmemSort)
-                                                  : (kSmemVerts > kSmemSort ? kSmemVerts : kSmemSort)) + 15) & ~(size_t)15;
+constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;                                 // phase A
+constexpr size_t kSmemFast = (size_t)kBuckets * 4 + 80 * 4 + (size_t)kOwnedMax * 8;  // fast sort
+constexpr size_t kSmemLsd = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
+constexpr size_t kSmemMax2 = kSmemFast > kSmemLsd ? kSmemFast : kSmemLsd;
+constexpr size_t kSmem = ((kSmemVerts > kSmemMax2 ? kSmemVerts : kSmemMax2) + 15) & ~(size_t)15;
 
 // Grid-wide barrier number k (1, 2, ...) of a cooperative launch: every CTA
 // adds one to *bar (released) and waits until all of them have, for at most
@@ -833,18 +838,47 @@ __device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t k, uint32_t* s
   return *s_flag != 0;
 }
 
-// One climb of the bottom-up hierarchy (see hierarchy_kernel).
-struct Climb {
-  uint32_t f, l;
-  int dl, dr;
-  f3 mn, mx;
-  bool leaf;
-  int pending;    // shared slot where it arrived first
-  uint32_t mode;  // 0 done, 1 continues through global memory
-};
+// Exclusive scan over kBuckets entries in shared memory (in place), kThreads
+// threads with kBuckets / kThreads consecutive entries each; returns the total
+// and the largest entry through *s_res (res[0] total, res[1] max).
+__device__ __forceinline__ void scan_buckets(uint32_t* s_b, uint32_t* s_tmp, uint32_t* s_res) {
+  constexpr uint32_t kPer = kBuckets / kThreads;
+  static_assert(kBuckets % kThreads == 0, "whole runs per thread");
+  const uint32_t tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint32_t v[kPer], sum = 0, mx = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    v[k] = s_b[tid * kPer + k];
+    sum += v[k];
+    mx = max(mx, v[k]);
+  }
+  uint32_t inc = onesweep::warp_inclusive_scan(sum);
+  mx = __reduce_max_sync(0xFFFFFFFFu, mx);
+  if (lane == 31) s_tmp[warp] = inc;
+  if (lane == 0) s_tmp[32 + warp] = mx;
+  __syncthreads();
+  uint32_t before = 0, total = 0, gmax = 0;
+#pragma unroll
+  for (int w = 0; w < kWarps; ++w) {
+    before += (w < (int)warp) ? s_tmp[w] : 0u;
+    total += s_tmp[w];
+    gmax = max(gmax, s_tmp[32 + w]);
+  }
+  uint32_t run = before + inc - sum;
+#pragma unroll
+  for (uint32_t k = 0; k < kPer; ++k) {
+    s_b[tid * kPer + k] = run;
+    run += v[k];
+  }
+  if (tid == 0) {
+    s_res[0] = total;
+    s_res[1] = gmax;
+  }
+  __syncthreads();
+}
 
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __restrict__ verts, uint32_t n,
+__global__ void __launch_bounds__(kThreads, 2) lbvh_front_kernel(const float* __restrict__ verts, uint32_t n,
                                                                  BajoLbvh t, unsigned char* __restrict__ ws,
                                                                  uint32_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -856,6 +890,8 @@ __global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __
   uint32_t* seg_ord = reinterpret_cast<uint32_t*>(ws + kL0.off_seg_ord);
   uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + kL0.off_ghist);
   uint32_t* counts = reinterpret_cast<uint32_t*>(ws + kL0.off_counts);  // [pass][tile][digit]
+  uint32_t* bhist = reinterpret_cast<uint32_t*>(ws + kL0.off_bhist);    // [bucket] keys
+  uint32_t* bfill = reinterpret_cast<uint32_t*>(ws + kL0.off_bfill);    // [bucket] slots handed out
   uint32_t* const ka = reinterpret_cast<uint32_t*>(ws + L.off_ka);
   uint32_t* const va = reinterpret_cast<uint32_t*>(ws + L.off_va);
   uint32_t* const kb = reinterpret_cast<uint32_t*>(ws + L.off_kb);
@@ -887,10 +923,10 @@ __global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __
     for (uint32_t q = base + tid; q < min(base + kTile, n - 1); q += kThreads) t.node_flags[q] = 0u;
     for (uint32_t q = tid; q < (kPasses - 1) * 256; q += kThreads)
       counts[((q >> 8) + 1) * kMaxTiles * 256 + c * 256 + (q & 255)] = 0u;
+    for (uint32_t q = c * kThreads + tid; q < 2 * kBuckets; q += gridDim.x * kThreads) bhist[q] = 0u;  // + bfill
     if (c == 0 && tid == 0) {
       t.internal_offsets[0] = 0;
       t.internal_offsets[1] = n - 1;
-      t.roots[0] = 0;
     }
     __syncthreads();
   }
@@ -959,6 +995,7 @@ __global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __
         const f3 d = mk(cx[k], cy[k], cz[k]) - cmin;
         key[k] = morton3(d.x * inv.x, d.y * inv.y, d.z * inv.z);
         val[k] = base + p;
+        atomicAdd(&bhist[key[k] >> kBucketShift], 1u);
 #pragma unroll
         for (int ps = 0; ps < kPasses; ++ps) atomicAdd(&s_hist[ps * 256 + ((key[k] >> (8 * ps)) & 255u)], 1u);
       } else {
@@ -975,7 +1012,74 @@ __global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __
   }
   if (!grid_sync(bar, 2, status, &s_flag)) return;
 
-  // ---------------- radix passes
+  // ---------------- sort, fast path: buckets of the top code bits
+  {
+    uint32_t* s_b = reinterpret_cast<uint32_t*>(smem);  // [kBuckets] bucket starts
+    uint32_t* s_tmp = s_b + kBuckets;                    // scan scratch [64] + results [2]
+    for (uint32_t q = tid; q < kBuckets; q += kThreads) s_b[q] = __ldcg(bhist + q);
+    __syncthreads();
+    scan_buckets(s_b, s_tmp, s_tmp + 64);
+    const bool fast = s_tmp[65] <= kBucketMax;  // every CTA reads the same histogram
+    if (fast) {
+      // S1: every key to a slot of its bucket's range
+#pragma unroll
+      for (int k = 0; k < kKpt; ++k) {
+        if (pos0 + 32 * k < cnt) {
+          const uint32_t b = key[k] >> kBucketShift;
+          const uint32_t slot = s_b[b] + atomicAdd(&bfill[b], 1u);
+          if (slot < n) {
+            ka[slot] = key[k];
+            va[slot] = val[k];
+          }
+        }
+      }
+      if (!grid_sync(bar, 3, status, &s_flag)) return;
+      // S2: the buckets that start inside this tile, ranked in shared memory
+      uint2* s_kv = reinterpret_cast<uint2*>(s_tmp + 64 + 16);  // [kOwnedMax] (code, item)
+      // owned positions [lo, hi): from the first bucket start >= base to the
+      // first bucket start >= base + kTile (n past the last one)
+      auto first_start_at_or_after = [&](uint32_t p) {
+        uint32_t a = 0, z = kBuckets;  // smallest b with s_b[b] >= p, kBuckets if none
+        while (a < z) {
+          const uint32_t m = (a + z) >> 1;
+          if (s_b[m] >= p) z = m;
+          else a = m + 1;
+        }
+        return a < kBuckets ? s_b[a] : n;
+      };
+      const uint32_t lo = base == 0 ? 0u : first_start_at_or_after(base);
+      const uint32_t hi = base + kTile >= n ? n : first_start_at_or_after(base + kTile);
+      const uint32_t m = hi > lo ? hi - lo : 0u;
+      if (m > kOwnedMax) {  // cannot happen when every bucket fits kBucketMax
+        if (tid == 0) raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+        return;
+      }
+      for (uint32_t q = tid; q < m; q += kThreads) s_kv[q] = make_uint2(__ldcg(ka + lo + q), __ldcg(va + lo + q));
+      __syncthreads();
+      for (uint32_t q = tid; q < m; q += kThreads) {
+        const uint2 me = s_kv[q];
+        const uint32_t b = me.x >> kBucketShift;
+        const uint32_t bs = s_b[b];
+        const uint32_t be = b + 1 < kBuckets ? s_b[b + 1] : n;
+        const uint64_t mine = ((uint64_t)me.x << 32) | me.y;
+        uint32_t rank = 0;
+        for (uint32_t j = bs - lo; j < be - lo; ++j) {
+          const uint2 o = s_kv[j];
+          rank += (((uint64_t)o.x << 32) | o.y) < mine ? 1u : 0u;
+        }
+        const uint32_t dst = bs + rank;
+        if (dst < n) {
+          t.morton_codes[dst] = me.x;
+          t.leaf_ids[dst] = me.y;
+          t.sort_keys[dst] = (uint64_t)me.x;
+        }
+      }
+      return;
+    }
+    __syncthreads();  // the bucket starts are no longer read: the passes reuse the buffer
+  }
+
+  // ---------------- sort, otherwise: LSD radix passes
   {
     uint32_t* s_wh = reinterpret_cast<uint32_t*>(smem);           // [kWarps][256]: counts, then starts
     uint32_t* s_off = s_wh + kWarps * 256;                         // [256] global position - tile position
@@ -1064,188 +1168,11 @@ __global__ void __launch_bounds__(kThreads, 1) lbvh_fused_kernel(const float* __
             atomicAdd(next_counts + tag, (uint32_t)__popc(same));
         }
       }
-      if (!grid_sync(bar, 3 + ps, status, &s_flag)) return;
-    }
-  }
-
-  // ---------------- phase H: hierarchy, refit and triangle records
-  {
-    float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(smem);
-    uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(smem + (size_t)kTile * 48);
-    int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(smem + (size_t)kTile * 56);
-    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 64);
-    uint32_t* s_code = reinterpret_cast<uint32_t*>(smem + (size_t)kTile * 68);  // [kTile + 2]
-    const SegInfo g{0, n, 0};
-    for (uint32_t q = tid; q < kTile; q += kThreads) {
-      s_cnt[q] = 0;
-      s_code[q + 1] = base + q < n ? __ldcg(t.morton_codes + base + q) : 0u;
-    }
-    if (tid == 0) s_code[0] = base > 0 ? __ldcg(t.morton_codes + base - 1) : 0u;
-    if (tid == 1) s_code[kTile + 1] = base + kTile < n ? __ldcg(t.morton_codes + base + kTile) : 0u;
-    Climb cl[kKpt];
-#pragma unroll
-    for (int j = 0; j < kKpt; ++j) {
-      const uint32_t s = base + tid + j * kThreads;
-      cl[j].mode = 0;
-      cl[j].pending = -1;
-      cl[j].leaf = true;
-      cl[j].f = cl[j].l = s;
-      cl[j].dl = cl[j].dr = -1;
-      if (s < n) {
-        const uint32_t item = __ldcg(t.leaf_ids + s);
-        if (item >= n) {  // only after a failed sort
-          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-          continue;
-        }
-        const float* v = verts + (size_t)item * 9;
-        const f3 a = mk(__ldg(v + 0), __ldg(v + 1), __ldg(v + 2));
-        const f3 b = mk(__ldg(v + 3), __ldg(v + 4), __ldg(v + 5));
-        const f3 cc = mk(__ldg(v + 6), __ldg(v + 7), __ldg(v + 8));
-        float4* rec = reinterpret_cast<float4*>(t.leaf_tris + (size_t)s * 12);
-        rec[0] = make_float4(a.x, a.y, a.z, __uint_as_float(item));
-        rec[1] = make_float4(b.x, b.y, b.z, 0.0f);
-        rec[2] = make_float4(cc.x, cc.y, cc.z, 0.0f);
-        cl[j].mn = vmin(vmin(a, b), cc);
-        cl[j].mx = vmax(vmax(a, b), cc);
-        cl[j].mode = 1;
-      }
-    }
-    __syncthreads();  // codes staged
-    // phase H1: splits whose sibling starts inside this tile, in shared memory
-#pragma unroll
-    for (int j = 0; j < kKpt; ++j) {
-      Climb& q = cl[j];
-      if (!q.mode) continue;
-      const uint32_t s = q.f, li = s;
-      if (li > 0) q.dl = delta_codes(s_code[s - base], li - 1, s_code[s - base + 1], li);
-      if (li + 1 < n) q.dr = delta_codes(s_code[s - base + 1], li, s_code[s - base + 2], li + 1);
-      for (int depth = 0;; ++depth) {
-        if (depth > 128) {
-          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-          q.mode = 0;
-          break;
-        }
-        const bool is_left = q.dr > q.dl;
-        const uint32_t gamma = is_left ? q.l : q.f - 1;
-        if (is_left ? (q.l + 1 >= base + kTile) : (q.f < base + 1)) break;  // crossing split: global
-        const uint32_t slot = gamma - base, side = is_left ? 0 : 1;
-        float* mine = s_box[slot][side];
-        mine[0] = q.mn.x; mine[1] = q.mn.y; mine[2] = q.mn.z; mine[3] = q.mx.x; mine[4] = q.mx.y; mine[5] = q.mx.z;
-        s_far[slot][side] = is_left ? q.f : q.l;
-        s_dfar[slot][side] = is_left ? q.dl : q.dr;
-        __threadfence_block();
-        if (atomicAdd(&s_cnt[slot], 1u) == 0) {
-          q.pending = (int)slot;
-          break;
-        }
-        __threadfence_block();
-        const float* sib = s_box[slot][side ^ 1];
-        const f3 smn = mk(sib[0], sib[1], sib[2]), smx = mk(sib[3], sib[4], sib[5]);
-        const uint32_t sfar = s_far[slot][side ^ 1];
-        const int sd = s_dfar[slot][side ^ 1];
-        const uint32_t F = is_left ? q.f : sfar, Lr = is_left ? sfar : q.l;
-        const int dL = is_left ? q.dl : sd, dR = is_left ? sd : q.dr;
-        const bool root = F == 0 && Lr == n - 1;
-        const uint32_t kn = root ? 0u : (dR > dL ? Lr : F);
-        if (is_left)
-          write_parent(g, kn, F, Lr, gamma, q.mn, q.mx, smn, smx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
-                       t.node_bounds);
-        else
-          write_parent(g, kn, F, Lr, gamma, smn, smx, q.mn, q.mx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
-                       t.node_bounds);
-        t.node_flags[gamma] = 2u;
-        q.mn = vmin(q.mn, smn);
-        q.mx = vmax(q.mx, smx);
-        q.f = F;
-        q.l = Lr;
-        q.dl = dL;
-        q.dr = dR;
-        q.leaf = false;
-        if (root) {
-          q.mode = 0;
-          break;
-        }
-      }
-    }
-    __syncthreads();  // every local climb of this tile has ended
-#pragma unroll
-    for (int j = 0; j < kKpt; ++j)
-      if (cl[j].mode && cl[j].pending >= 0 && s_cnt[cl[j].pending] != 1) cl[j].mode = 0;  // sibling came, went on
-    // phase H2: the splits that cross a tile boundary, in global memory.  The
-    // arrival word of split gamma (node_flags[gamma]) counts arrivals and
-    // carries the first arrival's leaf bit and far-end delta; its acq_rel
-    // add releases the first arrival's subtree, which the second reads.
-#pragma unroll
-    for (int j = 0; j < kKpt; ++j) {
-      Climb& q = cl[j];
-      for (int depth = 0; q.mode; ++depth) {
-        if (depth > 128) {
-          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-          break;
-        }
-        const bool is_left = q.dr > q.dl;
-        const uint32_t gamma = is_left ? q.l : q.f - 1;
-        uint32_t* flag = t.node_flags + gamma;
-        const int dfar = is_left ? q.dl : q.dr;
-        const uint32_t inc = kArrive | (q.leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
-        const uint32_t old = atomic_add_acq_rel_gpu(flag, inc);
-        if ((old & 0xFu) == 0) break;  // first: the sibling continues
-        const bool sib_leaf = (old & kLeafArrive) != 0;
-        const int sd = (int)((old >> 16) & 0x7Fu) - 1;
-        f3 smn, smx;
-        uint32_t sfar;
-        if (is_left) {  // sibling = right child, starts at gamma + 1
-          if (sib_leaf) {
-            sfar = gamma + 1;
-            tri_box(reinterpret_cast<const float4*>(t.leaf_tris) + (size_t)(gamma + 1) * 3, smn, smx);
-          } else {
-            const uint32_t ks = gamma + 1;
-            sfar = __ldcg(t.node_meta + (size_t)ks * 4 + 3);
-            const float4* nb = reinterpret_cast<const float4*>(t.node_bounds) + (size_t)ks * 3;
-            const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
-            smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
-            smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
-          }
-        } else {  // sibling = left child, ends at gamma
-          if (sib_leaf) {
-            sfar = gamma;
-            tri_box(reinterpret_cast<const float4*>(t.leaf_tris) + (size_t)gamma * 3, smn, smx);
-          } else {
-            const uint32_t ks = gamma;
-            sfar = gamma + 1 - __ldcg(t.node_leaf_counts + ks);
-            const float4* nb = reinterpret_cast<const float4*>(t.node_bounds) + (size_t)ks * 3;
-            const float4 b0 = __ldcg(nb + 0), b1 = __ldcg(nb + 1), b2 = __ldcg(nb + 2);
-            smn = vmin(mk(b0.x, b0.y, b0.z), mk(b1.z, b1.w, b2.x));
-            smx = vmax(mk(b0.w, b1.x, b1.y), mk(b2.y, b2.z, b2.w));
-          }
-        }
-        *flag = 2u;
-        const uint32_t F = is_left ? q.f : sfar, Lr = is_left ? sfar : q.l;
-        if (F > Lr || Lr >= n) {
-          raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-          break;
-        }
-        const int dL = is_left ? q.dl : sd, dR = is_left ? sd : q.dr;
-        const bool root = F == 0 && Lr == n - 1;
-        const uint32_t kn = root ? 0u : (dR > dL ? Lr : F);
-        if (is_left)
-          write_parent(g, kn, F, Lr, gamma, q.mn, q.mx, smn, smx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
-                       t.node_bounds);
-        else
-          write_parent(g, kn, F, Lr, gamma, smn, smx, q.mn, q.mx, t.node_meta, t.node_leaf_counts, t.leaf_parent,
-                       t.node_bounds);
-        if (root) break;
-        q.mn = vmin(q.mn, smn);
-        q.mx = vmax(q.mx, smx);
-        q.f = F;
-        q.l = Lr;
-        q.dl = dL;
-        q.dr = dR;
-        q.leaf = false;
-      }
+      if (ps + 1 < kPasses && !grid_sync(bar, 3 + ps, status, &s_flag)) return;
     }
   }
 }
+
 
 // Launch state per device: the kernel attributes are set and the co-resident
 // CTA count is known.
@@ -1260,34 +1187,37 @@ bool can_run(uint32_t n, uint32_t n_seg) {
   return n_seg == 1 && n >= 2 && n <= g_fused_max_leaves.load(std::memory_order_relaxed) && n <= kMaxLeaves;
 }
 
+// Enqueues the front end (one cooperative launch); *launched = false when the
+// grid cannot be co-resident on this device (the caller then runs the
+// per-stage kernels).
 cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws, uint32_t* status, cudaStream_t st,
                    bool* launched) {
   *launched = false;
   const uint32_t n = bvh->n_leaves;
   const uint32_t G = (n + kTile - 1) / kTile;
   const bool vec = ((uintptr_t)d_verts & 15) == 0;
-  auto kern = vec ? lbvh_fused_kernel<true> : lbvh_fused_kernel<false>;
+  auto kern = vec ? lbvh_front_kernel<true> : lbvh_front_kernel<false>;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 64) return cudaSuccess;  // use the multi-launch build
+  if (dev < 0 || dev >= 64) return cudaSuccess;
   DeviceState& ds = g_fused_state[dev];
   if (!ds.ready) {
     int per_sm_t = 0, per_sm_f = 0;
-    if ((e = cudaFuncSetAttribute(lbvh_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(lbvh_front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmem)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(lbvh_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (e = cudaFuncSetAttribute(lbvh_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmem)) != cudaSuccess)
       return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, lbvh_fused_kernel<true>, kThreads, kSmem)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, lbvh_front_kernel<true>, kThreads, kSmem)) !=
             cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, lbvh_fused_kernel<false>, kThreads, kSmem)) !=
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, lbvh_front_kernel<false>, kThreads, kSmem)) !=
             cudaSuccess)
       return e;
     ds.max_ctas = min(per_sm_t, per_sm_f) * sm_count();
     ds.ready = true;
   }
-  if ((int)G > ds.max_ctas) return cudaSuccess;  // not co-resident: use the multi-launch build
+  if ((int)G > ds.max_ctas) return cudaSuccess;
   constexpr Layout kL0 = layout(0);
   if ((e = cudaMemsetAsync(ws + kL0.off_bar, 0, kL0.zero_end - kL0.off_bar, st)) != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
@@ -1476,6 +1406,21 @@ static size_t hploc_extra_offset(uint32_t n, uint32_t n_seg) {
   return (bajo::make_build_plan(n, n_seg).total + 255) & ~(size_t)255;
 }
 
+// The bottom-up hierarchy + refit of builds of up to kMergedMaxLeaves
+// triangles (section 3); node_flags must be zero and the sorted leaves ready.
+static cudaError_t launch_hierarchy(const float* d_verts, BajoLbvh* bvh, uint32_t* status, cudaStream_t st) {
+  using namespace bajo;
+  const uint32_t n = bvh->n_leaves, S = bvh->n_segments;
+  constexpr size_t hier_smem = (size_t)kRefitBlock * 72 + 8;
+  cudaError_t e = cudaFuncSetAttribute(hierarchy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hier_smem);
+  if (e != cudaSuccess) return e;
+  const uint32_t grid = (max(max(n, S), 1u) + kRefitBlock - 1) / kRefitBlock;
+  hierarchy_kernel<<<grid, kRefitBlock, hier_smem, st>>>(
+      d_verts, bvh->leaf_ids, bvh->morton_codes, n, bvh->seg_offsets, S, bvh->internal_offsets, bvh->node_meta,
+      bvh->node_leaf_counts, bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris, bvh->roots, status);
+  return cudaGetLastError();
+}
+
 static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, size_t ws_bytes, void* stream_,
                                cudaEvent_t* ev, int32_t n_ev, bool hploc = false) {
   using namespace bajo;
@@ -1490,20 +1435,25 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   BuildPlan plan = make_build_plan(n, S);
   const size_t need = hploc ? hploc_extra_offset(n, S) + hploc_workspace_bytes(n, S) : plan.total;
   if (ws_bytes < need) return BAJO_ERR_WORKSPACE_TOO_SMALL;
-  if (ev && n_ev < (int32_t)(5 + plan.passes)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream_;
   unsigned char* ws = (unsigned char*)ws_;
   uint32_t* status = (uint32_t*)ws;
-  // one scene of up to fused::kMaxLeaves triangles: the one-launch build
-  // (stage-timed builds keep the multi-launch kernels, whose stages they time)
-  if (!hploc && !ev && fused::can_run(n, S)) {
+  // one scene of up to fused::kMaxLeaves triangles: the one-launch front end,
+  // then the hierarchy; its stage events are [start, front end, hierarchy]
+  if (!hploc && fused::can_run(n, S) && (!ev || n_ev == 3)) {
+    if (ev && cudaEventRecord(ev[0], st) != cudaSuccess) return BAJO_ERR_CUDA;
     bool launched = false;
     if (fused::launch(d_verts, bvh, ws, status, st, &launched) != cudaSuccess) return BAJO_ERR_CUDA;
     if (launched) {
+      if (ev && cudaEventRecord(ev[1], st) != cudaSuccess) return BAJO_ERR_CUDA;
+      if (launch_hierarchy(d_verts, bvh, status, st) != cudaSuccess) return BAJO_ERR_CUDA;
+      if (ev && cudaEventRecord(ev[2], st) != cudaSuccess) return BAJO_ERR_CUDA;
       if (bvh->top_nodes && launch_stage_top(bvh, st) != cudaSuccess) return BAJO_ERR_CUDA;
       return BAJO_OK;
     }
+    if (ev) return BAJO_ERR_INVALID_ARGUMENT;  // the per-stage kernels need their own events
   }
+  if (ev && n_ev < (int32_t)(5 + plan.passes)) return BAJO_ERR_INVALID_ARGUMENT;
   // stage events: [start, bounds, morton, pass 0..P-1, topology, refit]
   auto mark = [&](int i) { return !ev || cudaEventRecord(ev[i], st) == cudaSuccess; };
   if (!mark(0)) return BAJO_ERR_CUDA;
@@ -1563,16 +1513,7 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
     // one bottom-up pass builds the hierarchy and refits it: the topology
     // stage event is recorded right before it
     if (!mark(3 + passes)) return BAJO_ERR_CUDA;
-    constexpr size_t hier_smem = (size_t)kRefitBlock * 72 + 8;
-    if (cudaFuncSetAttribute(hierarchy_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hier_smem) !=
-        cudaSuccess)
-      return BAJO_ERR_CUDA;
-    const uint32_t grid = (max(max(n, S), 1u) + kRefitBlock - 1) / kRefitBlock;
-    hierarchy_kernel<<<grid, kRefitBlock, hier_smem, st>>>(
-        d_verts, bvh->leaf_ids, bvh->morton_codes, n, bvh->seg_offsets, S, bvh->internal_offsets, bvh->node_meta,
-        bvh->node_leaf_counts, bvh->leaf_parent, bvh->node_bounds, bvh->node_flags, bvh->leaf_tris, bvh->roots,
-        status);
-    if (cudaGetLastError() != cudaSuccess) return BAJO_ERR_CUDA;
+    if (launch_hierarchy(d_verts, bvh, status, st) != cudaSuccess) return BAJO_ERR_CUDA;
   } else {
     topology_kernel<<<(max(n, S) + kBlock - 1) / kBlock, kBlock, 0, st>>>(
         bvh->morton_codes, bvh->seg_offsets, S, bvh->internal_offsets, n, bvh->node_meta, bvh->leaf_parent,
@@ -1635,7 +1576,7 @@ int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* 
     if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
       const fused::DeviceState& ds = fused::g_fused_state[dev];
       if (!ds.ready || (int)((n_tris + fused::kTile - 1) / fused::kTile) <= ds.max_ctas) {
-        *launches = 1;
+        *launches = 2;  // the front end, then hierarchy_kernel
         return BAJO_OK;
       }
     }
@@ -1647,6 +1588,12 @@ int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* 
 
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {
   if (!n_events || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
+  int32_t launches = 0;
+  if (bajo_lbvh_build_launches(n_tris, n_segments, &launches) == BAJO_OK && launches == 2 &&
+      bajo::fused::can_run(n_tris, n_segments)) {
+    *n_events = 3;  // [start, front end, hierarchy]
+    return BAJO_OK;
+  }
   *n_events = (int32_t)(5 + bajo::make_build_plan(n_tris, n_segments).passes);
   return BAJO_OK;
 }

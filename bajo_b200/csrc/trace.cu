@@ -1,6 +1,9 @@
 // trace.cu -- closest-hit traversal entry points (GpuTriangleBvh.launch_rays /
 // launch_camera, bajo/bvh/gpu/triangle_bvh.mojo:520-614).  The traversal
 // itself is in traverse.cuh.
+#include <atomic>
+#include <mutex>
+
 #include "sampling.cuh"
 #include "traverse.cuh"
 
@@ -66,8 +69,8 @@ __device__ __forceinline__ void ray_query(uint32_t i, const float* __restrict__ 
 // Unstaged: 10 blocks of 128 per SM (48 registers): general rays are mostly
 // incoherent and latency bound, and the extra warps outweigh the spills
 // (+5% to +8% on random rays against 64 registers).
-template <int MODE, bool TOP>
-__global__ void __launch_bounds__(TOP ? kTopBlock : kTraceBlock, TOP ? kTopMinBlocks : 10)
+template <int MODE, bool TOP, int BLK = kTraceBlock>
+__global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 1280 / BLK)
     trace_rays_kernel(const float* __restrict__ rays, uint32_t n, uint32_t n_nodes, const uint32_t* __restrict__ roots,
                       const float4* __restrict__ nb, const uint4* __restrict__ meta, const float4* __restrict__ tris,
                       const float4* __restrict__ top_g, float* __restrict__ hits8, float* __restrict__ out_t,
@@ -120,8 +123,8 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   }
 }
 
-template <int MODE, bool STATS, bool TOP>
-__global__ void __launch_bounds__(TOP ? kTopBlock : kTraceBlock, TOP ? kTopMinBlocks : 0)
+template <int MODE, bool STATS, bool TOP, int BLK = kTraceBlock>
+__global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0)
     trace_camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t n_nodes, uint32_t width, uint32_t height,
                         float inv_h, const uint32_t* __restrict__ roots, const float4* __restrict__ nb,
                         const uint4* __restrict__ meta, const float4* __restrict__ tris,
@@ -210,31 +213,83 @@ uint32_t top_grid(Kernel kernel, uint32_t n) {
   return need < cap ? need : cap;
 }
 
-template <int MODE, bool TOP>
-void launch_rays(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
-                 uint32_t* status, cudaStream_t st) {
+// Block sizes of the unstaged closest-hit kernels, chosen per call from a
+// process-wide table indexed by (kind: 0 camera rays, 1 general rays,
+// ceil(log2 n)) that the autotuner fills (bajo_trace_tuning_set); -1 means
+// the built-in 128.  The block size changes only the launch shape: every
+// variant gives the same hits.
+constexpr int kTraceVariants = 3;
+constexpr int kTraceBlocks[kTraceVariants] = {128, 64, 256};
+std::atomic<int8_t> g_trace_tuning[2][33];
+std::once_flag g_trace_tuning_once;
+
+int trace_variant(int kind, uint32_t n) {
+  std::call_once(g_trace_tuning_once, [] {
+    for (auto& row : g_trace_tuning)
+      for (auto& v : row) v.store(-1);
+  });
+  uint32_t lg = 0;
+  while (lg < 32 && (1ull << lg) < n) ++lg;
+  const int v = g_trace_tuning[kind][lg].load(std::memory_order_relaxed);
+  return v >= 0 && v < kTraceVariants ? v : 0;
+}
+
+template <int MODE, bool TOP, int BLK>
+void launch_rays_blk(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
+                     uint32_t* status, cudaStream_t st) {
   const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
   const uint4* meta = reinterpret_cast<const uint4*>(b->node_meta);
   const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
-  const uint32_t grid = TOP ? top_grid(trace_rays_kernel<MODE, TOP>, n) : (n + kTraceBlock - 1) / kTraceBlock;
-  trace_rays_kernel<MODE, TOP><<<grid, TOP ? kTopBlock : kTraceBlock, 0, st>>>(rays, n, b->n_leaves, b->roots, nb,
-                                                                               meta, tris, top, hits8, t, prim,
-                                                                               status);
+  const uint32_t grid = TOP ? top_grid(trace_rays_kernel<MODE, TOP>, n) : (n + BLK - 1) / BLK;
+  trace_rays_kernel<MODE, TOP, BLK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(rays, n, b->n_leaves, b->roots, nb,
+                                                                            meta, tris, top, hits8, t, prim, status);
 }
 
-template <int MODE, bool STATS, bool TOP>
-void launch_camera(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height, float* hits8,
-                   float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
+template <int MODE, bool TOP>
+void launch_rays(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
+                 uint32_t* status, cudaStream_t st) {
+  if constexpr (TOP) {
+    launch_rays_blk<MODE, TOP, kTraceBlock>(b, rays, n, hits8, t, prim, status, st);
+  } else {
+    switch (trace_variant(1, n)) {
+      case 1: return launch_rays_blk<MODE, TOP, 64>(b, rays, n, hits8, t, prim, status, st);
+      case 2: return launch_rays_blk<MODE, TOP, 256>(b, rays, n, hits8, t, prim, status, st);
+      default: return launch_rays_blk<MODE, TOP, 128>(b, rays, n, hits8, t, prim, status, st);
+    }
+  }
+}
+
+template <int MODE, bool STATS, bool TOP, int BLK>
+void launch_camera_blk(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height,
+                       float* hits8, float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
   const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
   const uint4* meta = reinterpret_cast<const uint4*>(b->node_meta);
   const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
   const float inv_h = 1.0f / (float)height;
-  const uint32_t grid =
-      TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (n + kTraceBlock - 1) / kTraceBlock;
-  trace_camera_kernel<MODE, STATS, TOP><<<grid, TOP ? kTopBlock : kTraceBlock, 0, st>>>(
+  const uint32_t grid = TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (n + BLK - 1) / BLK;
+  trace_camera_kernel<MODE, STATS, TOP, BLK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
       cams, n, b->n_leaves, width, height, inv_h, b->roots, nb, meta, tris, top, hits8, t, prim, status, stats);
+}
+
+template <int MODE, bool STATS, bool TOP>
+void launch_camera(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height, float* hits8,
+                   float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
+  if constexpr (TOP || STATS) {
+    launch_camera_blk<MODE, STATS, TOP, kTraceBlock>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+  } else {
+    switch (trace_variant(0, n)) {
+      case 1:
+        return launch_camera_blk<MODE, STATS, TOP, 64>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
+      case 2:
+        return launch_camera_blk<MODE, STATS, TOP, 256>(b, cams, n, width, height, hits8, t, prim, status, stats,
+                                                        st);
+      default:
+        return launch_camera_blk<MODE, STATS, TOP, 128>(b, cams, n, width, height, hits8, t, prim, status, stats,
+                                                        st);
+    }
+  }
 }
 
 template <bool STATS>
@@ -274,6 +329,25 @@ int32_t bajo_trace_rays(const BajoLbvh* bvh, const float* d_rays, uint32_t n, in
     else launch_rays<BAJO_TRI_WATERTIGHT, false>(bvh, d_rays, n, d_hits8, d_t, d_prim, d_status, st);
   }
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_trace_tuning_set(int32_t kind, uint32_t log2n, int32_t block) {
+  using namespace bajo;
+  if ((kind != 0 && kind != 1) || log2n > 32) return BAJO_ERR_INVALID_ARGUMENT;
+  int v = -1;
+  for (int k = 0; k < kTraceVariants; ++k)
+    if (kTraceBlocks[k] == block) v = k;
+  if (block != 0 && v < 0) return BAJO_ERR_INVALID_ARGUMENT;
+  trace_variant(0, 1);  // initialise the table
+  g_trace_tuning[kind][log2n].store((int8_t)v);
+  return BAJO_OK;
+}
+
+int32_t bajo_trace_tuning_get(int32_t kind, uint32_t n, int32_t* block) {
+  using namespace bajo;
+  if ((kind != 0 && kind != 1) || !block) return BAJO_ERR_INVALID_ARGUMENT;
+  *block = kTraceBlocks[trace_variant(kind, n)];
+  return BAJO_OK;
 }
 
 int32_t bajo_trace_camera(const BajoLbvh* bvh, const float* d_cams, uint32_t n, uint32_t width, uint32_t height,

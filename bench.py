@@ -40,13 +40,15 @@ WORKLOAD = "plain LBVH build of 65,536 random triangles (seed 0) + 1024x1024 clo
 # Algorithmic bytes of one onesweep digit pass over the LBVH sort (the
 # per-stage build): read and write one u64 key and one u32 payload per key.
 PASS_BYTES_PER_KEY = 24
-# Algorithmic bytes per triangle of the one-launch build kernel: bounds
-# (vertices 36 read, leaf bounds 24 written, arrival counter 4 cleared), four
-# radix passes over u32 code + u32 id (8 written; 16 read and written twice;
-# 8 read + 16 written as codes, ids and u64 keys), hierarchy (codes 4, ids 4
-# and vertices 36 read; triangle record 48, node meta 16, node boxes 48, leaf
-# count 4, arrival counter 4 and parent link 4 written).
-FUSED_BYTES_PER_TRI = 36 + 24 + 4 + 8 + 2 * 16 + 24 + 44 + 124
+# Algorithmic bytes per triangle of the build's two kernels.
+#  lbvh_front_kernel: vertices 36 read, leaf bounds 24 written, arrival
+#    counter 4 cleared; bucket sort of u32 code + u32 id: 8 written to the
+#    buckets, 8 read back, 16 written as sorted codes, ids and u64 keys.
+#  hierarchy_kernel: codes 4, ids 4 and vertices 36 read; triangle record 48,
+#    node meta 16, node boxes 48, leaf count 4, arrival counter 4 and parent
+#    link 4 written.
+KERNEL_BYTES_PER_TRI = {"lbvh_front_kernel": 36 + 24 + 4 + 8 + 8 + 16,
+                        "hierarchy_kernel": 4 + 4 + 36 + 48 + 16 + 48 + 4 + 4 + 4}
 # digit passes of the single-scene LBVH sort: 8-bit digits over the 30-bit
 # Morton code, bits [0, 32) (the reference CPU builder's four byte passes,
 # bajo/bvh/cpu/builder/lbvh.mojo:56-62)
@@ -339,18 +341,20 @@ def run_bajo(args):
     hits = torch.empty(8 * n_rays, dtype=torch.float32, device=dev)
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)  # > 126 MB L2
 
-    n_ev = ctypes.c_int32(0)
-    L.bajo_lbvh_stage_count(N_TRIS, 1, ctypes.byref(n_ev))
-    n_ev = n_ev.value
-    passes = n_ev - 5
+    def stage_count():
+        x = ctypes.c_int32(0)
+        _lib.check(L.bajo_lbvh_stage_count(N_TRIS, 1, ctypes.byref(x)), "bajo_lbvh_stage_count")
+        return x.value
+
     launches = ctypes.c_int32(0)
     _lib.check(L.bajo_lbvh_build_launches(N_TRIS, 1, ctypes.byref(launches)), "bajo_lbvh_build_launches")
-    kernels_per_build = launches.value  # 1: the one-launch build
+    kernels_per_build = launches.value  # 2: the one-launch front end, then hierarchy_kernel
+    n_ev = stage_count()                # 3: [start, front end, hierarchy]
 
     def build_timed(events):
-        arr = (ctypes.c_void_p * n_ev)(*[e.cuda_event for e in events])
+        arr = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
         _lib.check(L.bajo_lbvh_build_timed(verts.data_ptr(), ctypes.byref(c), ws.buffer.data_ptr(),
-                                           ws.buffer.numel(), sh, arr, n_ev), "bajo_lbvh_build_timed")
+                                           ws.buffer.numel(), sh, arr, len(events)), "bajo_lbvh_build_timed")
 
     def build_plain():
         _lib.check(L.bajo_lbvh_build(verts.data_ptr(), ctypes.byref(c), ws.buffer.data_ptr(), ws.buffer.numel(), sh),
@@ -375,9 +379,8 @@ def run_bajo(args):
     torch.cuda.synchronize()
 
     # ---- device-timed region: K builds through the public entry point with
-    # events only around each build (events between the build's kernels cost
-    # several microseconds each), K traces, then K instrumented builds whose
-    # events split each build into its stages and digit passes
+    # events only around each build, K traces, then K builds with an event
+    # between their kernels (the per-kernel split of the roofline entry)
     step_events = [new_events(2) for _ in range(args.steps)]
     stage_events = [new_events(n_ev) for _ in range(args.steps)]
     trace_events = [new_events(2) for _ in range(args.steps)]
@@ -402,31 +405,49 @@ def run_bajo(args):
         build_timed(stage_events[k])
     torch.cuda.synchronize()
     build_ms = [e[0].elapsed_time(e[1]) for e in step_events]
-    pass_ms = [e[2 + p].elapsed_time(e[3 + p]) for e in stage_events for p in range(passes)]
-    stage = {
-        "bounds": statistics.mean(e[0].elapsed_time(e[1]) for e in stage_events),
-        "morton": statistics.mean(e[1].elapsed_time(e[2]) for e in stage_events),
-        "sort": statistics.mean(e[2].elapsed_time(e[2 + passes]) for e in stage_events),
-        "topology": statistics.mean(e[2 + passes].elapsed_time(e[3 + passes]) for e in stage_events),
-        "refit": statistics.mean(e[3 + passes].elapsed_time(e[4 + passes]) for e in stage_events),
-    }
     trace_ms = [e[0].elapsed_time(e[1]) for e in trace_events]
     build_total = max_over_ranks(world, sum(build_ms) / 1e3)
     trace_total = max_over_ranks(world, sum(trace_ms) / 1e3)
     value = world * N_TRIS * args.steps / build_total / 1e6
     mrays = world * n_rays * args.steps / trace_total / 1e6
 
-    # ---- roofline: the build's one kernel (lbvh_fused_kernel); its duration
-    # is the timed build's (the build is that launch plus a 4 KB memset)
+    # ---- the per-stage kernels of the same build (one scene takes them when
+    # the front end is switched off), with an event between every kernel
+    _lib.check(L.bajo_lbvh_fused_max_set(0), "bajo_lbvh_fused_max_set")
+    n_stage = stage_count()
+    passes = n_stage - 5
+    stage_ev = [new_events(n_stage) for _ in range(args.steps)]
+    build_timed(stage_ev[0])
+    torch.cuda.synchronize()
+    for k in range(args.steps):
+        flush.zero_()
+        build_timed(stage_ev[k])
+    torch.cuda.synchronize()
+    _lib.check(L.bajo_lbvh_fused_max_set(_lib.FUSED_MAX_LEAVES), "bajo_lbvh_fused_max_set")
+    pass_ms = [e[2 + p].elapsed_time(e[3 + p]) for e in stage_ev for p in range(passes)]
+    stage = {
+        "bounds": statistics.mean(e[0].elapsed_time(e[1]) for e in stage_ev),
+        "morton": statistics.mean(e[1].elapsed_time(e[2]) for e in stage_ev),
+        "sort": statistics.mean(e[2].elapsed_time(e[2 + passes]) for e in stage_ev),
+        "hierarchy": statistics.mean(e[2 + passes].elapsed_time(e[4 + passes]) for e in stage_ev),
+    }
+
+    # ---- roofline: the build's dominant kernel, from the events between its
+    # two kernels (front end: bounds + Morton + sort; hierarchy_kernel)
     peak, peak_kind = measured_peaks()
-    build_avg_s = statistics.mean(build_ms) / 1e3
-    fused_bytes = FUSED_BYTES_PER_TRI * N_TRIS
-    achieved = fused_bytes / build_avg_s / 1e9
-    traffic = committed_traffic().get("lbvh_fused_65536")
+    if n_ev == 3:
+        kern_us = {"lbvh_front_kernel": statistics.mean(e[0].elapsed_time(e[1]) for e in stage_events) * 1e3,
+                   "hierarchy_kernel": statistics.mean(e[1].elapsed_time(e[2]) for e in stage_events) * 1e3}
+    else:  # the per-stage kernels
+        kern_us = {"hierarchy_kernel": stage["hierarchy"] * 1e3}
+    top = max(kern_us, key=kern_us.get)
+    top_bytes = KERNEL_BYTES_PER_TRI[top] * N_TRIS
+    achieved = top_bytes / (kern_us[top] / 1e6) / 1e9
+    traffic = committed_traffic().get(f"{top}_65536")
+    trace_dram = committed_traffic().get("trace_camera_65536")
     # the per-stage build's onesweep pass, for comparison
     pass_avg_s = statistics.mean(pass_ms) / 1e3
     pass_bytes = PASS_BYTES_PER_KEY * N_TRIS
-    trace_dram = committed_traffic().get("trace_camera_65536")
 
     # ---- traversal instrumented bytes (per-ray node visits / triangle tests)
     stats = torch.empty(5 * n_rays, dtype=torch.int32, device=dev)
@@ -540,7 +561,8 @@ def run_bajo(args):
         "warmup": args.warmup, "ms_per_step": round(build_total / args.steps * 1e3, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
-        "sort_passes": 4 if kernels_per_build == 1 else passes,
+        "sort": "bucket sort over the top 12 code bits (LSD passes when a bucket holds more than 256 keys)"
+                if kernels_per_build == 2 else f"{passes} onesweep passes",
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
                 "d2h_bytes_per_step": 12 * 4,
                 "what": "every step: pinned H2D of its vertices + bajo_lbvh_build + D2H of the root child boxes; "
@@ -551,16 +573,15 @@ def run_bajo(args):
                 "h2d_us_median": round(statistics.median(h2d_ms) * 1e3, 1),
                 "h2d_gb_s": round(verts.numel() * 4 / (statistics.median(h2d_ms) / 1e3) / 1e9, 2),
                 "host_enqueue_us_per_step": round(host_enqueue_us, 1)},
-        "roofline": {"kernel": "lbvh_fused_kernel (the whole build in one cooperative launch)" if
-                     kernels_per_build == 1 else "per-stage build", "bound": "hbm",
-                     "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
+        "roofline": {"kernel": top, "bound": "hbm", "achieved": round(achieved, 2), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "algorithmic_bytes_per_launch": fused_bytes,
-                     "algorithmic_bytes_per_triangle": FUSED_BYTES_PER_TRI,
-                     "avg_launch_us": round(build_avg_s * 1e6, 3), "peak_kind": peak_kind},
+                     "algorithmic_bytes_per_launch": top_bytes,
+                     "algorithmic_bytes_per_triangle": KERNEL_BYTES_PER_TRI[top],
+                     "avg_launch_us": round(kern_us[top], 3), "peak_kind": peak_kind,
+                     "build_kernels_us": {k: round(v, 3) for k, v in kern_us.items()}},
         "per_stage_build": {
-            "what": "the per-stage kernels (bajo_lbvh_build_timed: bounds, Morton, onesweep passes, hierarchy) with "
-                    "an event between every kernel",
+            "what": "the same build through the per-stage kernels (bounds, Morton, onesweep passes, hierarchy; "
+                    "bajo_lbvh_fused_max_set(0)), an event between every kernel",
             "stages_ms": {k: round(v, 5) for k, v in stage.items()},
             "onesweep_pass": {"achieved_gb_s": round(pass_bytes / pass_avg_s / 1e9, 2),
                               "frac": round(pass_bytes / pass_avg_s / 1e9 / peak, 4),
@@ -770,6 +791,26 @@ def run_render(steps, warmup, spp=64, graph=True):
                 ms_graph.append(a.elapsed_time(b))
         renderer.close()
         out["graph_ms"] = round(statistics.median(ms_graph), 3)
+    # the same render under each acceleration-structure policy (the
+    # reference's GPU_RT_BVH_* choices, bajo/rt/gpu/prepared_scene.mojo:29-33)
+    by_policy = {}
+    for policy in rt.BVH_POLICIES:
+        g = gsc if policy == "lbvh" else rt.GpuRtTriangleScene(sc, bvh_policy=policy)
+        rt.render_gpu_triangles(settings, sc.camera, g, rt.MIS, workspace=ws)
+        pm = []
+        for _ in range(steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            rt.render_gpu_triangles(settings, sc.camera, g, rt.MIS, workspace=ws)
+            b.record(stream)
+            b.synchronize()
+            pm.append(a.elapsed_time(b))
+        r2, s2 = ws.ray_counts()
+        tp = statistics.median(pm)
+        by_policy[policy] = {"ms": round(tp, 3), "samples_s": round(paths / tp * 1e3, 1),
+                             "mrays_s": round((r2 + s2) / tp / 1e3, 2), "status": ws.status()}
+        del g
+    out["bvh_policies"] = by_policy
     out["_scene"] = sc
     return out
 
@@ -1032,7 +1073,9 @@ def run_case(args):
         return statistics.median(ms)
 
     if args.case == "render":
-        out.update(run_render(args.steps, args.warmup, args.spp))
+        r = run_render(args.steps, args.warmup, args.spp)
+        r.pop("_scene")
+        out.update(r)
     elif args.case == "batched":
         r = run_batched(args.steps, args.warmup, args.scenes)
         r.pop("_verts"), r.pop("_so")

@@ -173,19 +173,20 @@ int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* siz
  * key bits, Karras topology, atomic-flag refit, sorted triangle packing.
  * d_verts: 9 floats per triangle [v0 xyz, v1 xyz, v2 xyz].  bvh->seg_offsets
  * and every output array must be set by the caller.
- * One scene (S = 1) of 2 .. 2^17 triangles is built by a single cooperative
- * kernel launch (grid barriers between the phases; a barrier wait that runs
- * out sets BAJO_STATUS_GRID_TIMEOUT); other builds launch one kernel per
- * stage.  Both give the same arrays bit for bit. */
+ * One scene (S = 1) of 2 .. 2^17 triangles runs its bounds, Morton keys and
+ * sort in one cooperative kernel launch (grid barriers between the phases; a
+ * barrier wait that runs out sets BAJO_STATUS_GRID_TIMEOUT), then the
+ * hierarchy kernel; other builds launch one kernel per stage.  Both give the
+ * same arrays bit for bit. */
 int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
-/* Largest scene (triangles) the one-launch build takes, at most 2^17 (the
+/* Largest scene (triangles) the one-launch front end takes, at most 2^17 (the
  * default); 0 sends every build through the per-stage kernels.  Process wide,
  * like the sort tuning table: set it before building, not concurrently. */
 int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves);
 /* Kernel launches bajo_lbvh_build makes for n_tris triangles in n_segments
- * segments on the current device (1 for the one-launch build). */
+ * segments on the current device (2 with the one-launch front end). */
 int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* launches);
 
 /* H-PLOC build (GpuBvhBuildMethod.HPLOC, the reference's default builder,
@@ -208,9 +209,10 @@ int32_t bajo_hploc_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace,
  * measure_stages / GpuBuildTimings (bajo/bvh/gpu/builder/lbvh.mojo:347-422):
  * `events` holds n_events cudaEvent_t handles created by the caller; the
  * build records them on `stream` at [start, bounds, morton, sort pass 0..P-1,
- * topology, refit].  bajo_lbvh_stage_count gives n_events = P + 5.  A
- * stage-timed build always runs the per-stage kernels (whose stages it times),
- * never the one-launch build. */
+ * topology, refit]: bajo_lbvh_stage_count gives n_events = P + 5.  A build
+ * that takes the one-launch front end has three events instead, [start, front
+ * end, hierarchy] (bajo_lbvh_stage_count gives 3); with
+ * bajo_lbvh_fused_max_set(0) first, it times the per-stage kernels. */
 int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                               void* stream, void* const* events, int32_t n_events);
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);
@@ -245,6 +247,14 @@ int32_t bajo_wait_selftest(const uint32_t* d_flag, uint32_t bits, uint32_t limit
  * root is traced.  d_status (may be NULL) receives BAJO_STATUS_* bits. */
 int32_t bajo_trace_rays(const BajoLbvh* bvh, const float* d_rays, uint32_t n_rays, int32_t tri_mode,
                         float* d_hits8, float* d_t, uint32_t* d_prim, uint32_t* d_status, void* stream);
+
+/* Autotuner hook of the closest-hit kernels: block size (64, 128 or 256
+ * threads; 0 = the built-in 128) of the unstaged camera (kind 0) and general
+ * ray (kind 1) kernels per ceil(log2 n), process wide like the sort table.
+ * The hits do not depend on it.  bajo_trace_tuning_get reports the block size
+ * a call of n rays would use. */
+int32_t bajo_trace_tuning_set(int32_t kind, uint32_t log2n, int32_t block);
+int32_t bajo_trace_tuning_get(int32_t kind, uint32_t n, int32_t* block);
 
 /* Replaces GpuTriangleBvh.launch_camera (bajo/bvh/gpu/triangle_bvh.mojo:520):
  * primary rays generated in-kernel from 20-float camera records

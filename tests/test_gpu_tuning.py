@@ -1,0 +1,100 @@
+"""Every choice the autotuner can install gives the same results: the
+closest-hit kernels' block sizes (64 / 128 / 256 threads) leave the hits
+bit-identical, and the one-launch build front end on or off leaves the tree
+bit-identical (the front end's own parity is in test_gpu_lbvh_fused.py)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+from bajo_b200 import scenes  # noqa: E402
+
+
+def _rays(n, seed):
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    r = torch.empty(8, n, dtype=torch.float32, device="cuda")
+    r[0:3].uniform_(0.0, 1.0, generator=g)
+    r[3].zero_()
+    d = torch.randn(3, n, device="cuda", generator=g)
+    r[4:7] = d / d.norm(dim=0, keepdim=True)
+    r[7].fill_(3.0e38)
+    return r.reshape(-1)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_trace_block_sizes_give_identical_hits(oracle, mode):
+    from bajo_b200 import _lib, bvh, camera
+    L = _lib.load()
+    v = scenes.random_triangles(20000, seed=4)
+    tree = bvh.build_triangle_bvh(torch.from_numpy(v).cuda())
+    cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+    w, h = 96, 64
+    n = w * h
+    rays = _rays(5000, 3)
+    ref_cam = oracle.trace_bvh2(oracle.lbvh_build(v), oracle.camera_rays(camera.plain_lbvh_camera(), n, w, h), mode)
+    outs = {}
+    try:
+        for blk in (64, 128, 256):
+            for kind in (0, 1):
+                lg = int(np.ceil(np.log2(n if kind == 0 else 5000)))
+                assert L.bajo_trace_tuning_set(kind, lg, blk) == _lib.OK
+                got = ctypes.c_int32(0)
+                assert L.bajo_trace_tuning_get(kind, n if kind == 0 else 5000, ctypes.byref(got)) == _lib.OK
+                assert got.value == blk
+            hc = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+            tree.launch_camera(cam, hc, n, w, h, tri_mode=mode)
+            hr = torch.empty(8 * 5000, dtype=torch.float32, device="cuda")
+            tree.launch_rays(rays, hr, 5000, tri_mode=mode)
+            torch.cuda.synchronize()
+            outs[blk] = (hc.cpu().numpy().view(np.uint32), hr.cpu().numpy().view(np.uint32))
+    finally:
+        for kind in (0, 1):
+            for lg in range(33):
+                L.bajo_trace_tuning_set(kind, lg, 0)
+    for blk in (64, 256):
+        assert np.array_equal(outs[blk][0], outs[128][0])
+        assert np.array_equal(outs[blk][1], outs[128][1])
+    assert np.array_equal(outs[128][0], ref_cam.view(np.uint32))
+
+
+def test_trace_tuning_limits():
+    from bajo_b200 import _lib
+    L = _lib.load()
+    assert L.bajo_trace_tuning_set(0, 20, 96) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_tuning_set(2, 20, 64) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_tuning_set(1, 33, 64) == _lib.ERR_INVALID_ARGUMENT
+    got = ctypes.c_int32(0)
+    assert L.bajo_trace_tuning_set(1, 20, 0) == _lib.OK
+    assert L.bajo_trace_tuning_get(1, 1 << 20, ctypes.byref(got)) == _lib.OK and got.value == 128
+
+
+def test_tuner_runs_and_keeps_results(oracle):
+    """A short tuning run of the closest-hit blocks and the front-end limit
+    installs choices that reproduce the oracle's tree and hits."""
+    from bajo_b200 import _lib, autotune, bvh, camera
+    L = _lib.load()
+    try:
+        res = autotune.tune_trace("trace_camera", [16], reps=2)
+        assert res[16]["best"] in (64, 128, 256)
+        fe = autotune.tune_front_end(range(15, 17), reps=2)
+        assert set(v["best"] for v in fe.values()) <= {0, 1 << 15, 1 << 16}
+        v = scenes.random_triangles(1 << 16, seed=9)
+        t = bvh.build_triangle_bvh(torch.from_numpy(v).cuda())
+        torch.cuda.synchronize()
+        o = oracle.lbvh_build(v)
+        assert np.array_equal(t.node_meta.cpu().numpy().view(np.uint32)[: 4 * ((1 << 16) - 1)],
+                              o.node_meta[: 4 * ((1 << 16) - 1)])
+        cam = torch.from_numpy(camera.plain_lbvh_camera()).cuda()
+        hits = torch.empty(8 * 65536, dtype=torch.float32, device="cuda")
+        t.launch_camera(cam, hits, 65536, 256, 256)
+        torch.cuda.synchronize()
+        ref = oracle.trace_bvh2(o, oracle.camera_rays(camera.plain_lbvh_camera(), 65536, 256, 256))
+        assert np.array_equal(hits.cpu().numpy().view(np.uint32), ref.view(np.uint32))
+    finally:
+        for lg in range(33):
+            L.bajo_trace_tuning_set(0, lg, 0)
+        L.bajo_lbvh_fused_max_set(_lib.FUSED_MAX_LEAVES)
