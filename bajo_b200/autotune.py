@@ -1,5 +1,5 @@
 """Project autotuner: sort tile shapes and digit widths, closest-hit block
-sizes, and the size limit of the one-launch build front end.
+sizes, and the size limit of the one-launch build.
 
 - The sort kernels are compiled in several tile shapes (threads x keys per
   thread) and, for 64-bit keys, two digit widths (8 and 10 bits).  For each
@@ -10,9 +10,9 @@ sizes, and the size limit of the one-launch build front end.
   for blocks of 64, 128 and 256 threads; the tuner times each per ray-count
   bucket on a tree of the plain workload's kind, checks that the hits are
   identical, and installs the fastest (``bajo_trace_tuning_set``).
-- The one-launch build front end is timed against the per-stage kernels at
-  every power of two up to its limit, and the largest size up to which it
-  wins is installed (``bajo_lbvh_fused_max_set``).
+- The one-launch build is timed against the per-stage kernels at every
+  power of two up to its limit, and the largest size up to which it wins is
+  installed (``bajo_lbvh_fused_max_set``).
 
 Results are cached as JSON keyed by (kernel, size bucket, GPU name and SM
 count) so a process can load them instead of re-measuring.
@@ -157,10 +157,10 @@ def tune_trace(kernel: str, log2rays, n_tris: int = 65536, reps: int = 5) -> dic
     return out
 
 
-def tune_front_end(log2tris=range(11, 18), reps: int = 7) -> dict:
-    """Build time of one scene through the one-launch front end and through
-    the per-stage kernels at each size; installs the largest size up to
-    which the front end is faster.  Returns {log2n: {"best": limit, "ms": ...}}
+def tune_one_launch(log2tris=range(11, 18), reps: int = 7) -> dict:
+    """Build time of one scene through the one-launch build and through the
+    per-stage kernels at each size; installs the largest size up to which
+    the one-launch build is faster.  Returns {log2n: {"best": limit, "ms": ...}}
     with the same limit in every entry."""
     from . import bvh, scenes
     L = _lib.load()
@@ -171,10 +171,10 @@ def tune_front_end(log2tris=range(11, 18), reps: int = 7) -> dict:
         ws = bvh.GpuBvhBuildWorkspace(n, 1)
         tree = bvh.build_triangle_bvh(v, workspace=ws)
         t = {}
-        for name, lim in (("front_end", _lib.FUSED_MAX_LEAVES), ("per_stage", 0)):
+        for name, lim in (("one_launch", _lib.FUSED_MAX_LEAVES), ("per_stage", 0)):
             _lib.check(L.bajo_lbvh_fused_max_set(lim), "bajo_lbvh_fused_max_set")
             t[name] = _events_ms(lambda: bvh.build_triangle_bvh(v, workspace=ws, out=tree), reps)
-        if t["front_end"] < t["per_stage"] and limit == (n >> 1 if lg > min(log2tris) else 0):
+        if t["one_launch"] < t["per_stage"] and limit == (n >> 1 if lg > min(log2tris) else 0):
             limit = n
         out[lg] = {"ms": {k: round(x, 5) for k, x in t.items()}}
     _lib.check(L.bajo_lbvh_fused_max_set(limit), "bajo_lbvh_fused_max_set")
@@ -209,7 +209,7 @@ def load(path: str = CACHE) -> int:
             for lg, v in entries.items():
                 count += L.bajo_trace_tuning_set(_TRACE_KINDS[kernel], int(lg), int(v)) == _lib.OK
             continue
-        if kernel == "lbvh_front_end":
+        if kernel == "lbvh_one_launch":
             limits = set(entries.values())
             if len(limits) == 1:
                 count += L.bajo_lbvh_fused_max_set(int(limits.pop())) == _lib.OK
@@ -233,7 +233,7 @@ def tune_all(reps: int = 5, save_cache: bool = True) -> dict:
         _kernel_key(4, True): tune_sort(4, True, range(10, 27), reps=reps),
         "trace_camera": tune_trace("trace_camera", range(16, 23, 2), reps=reps),
         "trace_rays": tune_trace("trace_rays", range(16, 23, 2), reps=reps),
-        "lbvh_front_end": tune_front_end(reps=reps),
+        "lbvh_one_launch": tune_one_launch(reps=reps),
     }
     if save_cache:
         save(res)

@@ -228,11 +228,13 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
 //    child boxes, far range ends and their deltas in shared slots).  A split
 //    whose sibling lies (partly) outside meets in global memory after the
 //    CTA's local climbs are done: node_flags of the split counts the
-//    arrivals with an acq_rel add, which releases the first arrival's subtree
-//    (already written to the node arrays) and passes its leaf bit and its far
-//    end's delta in the counter word; the second arrival's add acquires it,
-//    and it reads the sibling's box from its node record or triangle record.
-//    node_flags ends at 2 for every internal node.
+//    arrivals (acquire), the first arrival publishes its subtree (already
+//    written to the node arrays) with a release flag bit, and passes its far
+//    end's delta in the counter word; the second reads the sibling's box
+//    from its node record or triangle record.  node_flags ends at 2 for
+//    every internal node.  (An acq_rel arrival add, which would spare the
+//    flag bit, was measured slower on B200: its release makes the second
+//    arrival, the one that climbs on, wait for its own stores first.)
 // ---------------------------------------------------------------------------
 constexpr uint32_t kArrive = 1u;
 constexpr uint32_t kLeafArrive = 0x10u;   // the arrival is a leaf
@@ -286,13 +288,15 @@ __device__ __forceinline__ void tri_box(const float4* __restrict__ rec, f3& mn, 
   mx = vmax(vmax(va, vb), vc);
 }
 
-__global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
+// One CTA's share: sorted leaves [blockIdx.x * kRefitBlock, +kRefitBlock) with
+// kRefitBlock threads and kRefitBlock * 72 + 8 bytes of shared memory.  Run
+// by hierarchy_kernel and as the last phase of the one-launch build.
+__device__ __forceinline__ void hierarchy_tile(
     const float* __restrict__ verts, const uint32_t* __restrict__ leaf_ids, const uint32_t* __restrict__ codes,
     uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
     uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
     float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
-    uint32_t* __restrict__ roots, uint32_t* __restrict__ status) {
-  extern __shared__ __align__(16) unsigned char hier_smem[];
+    uint32_t* __restrict__ roots, uint32_t* __restrict__ status, unsigned char* __restrict__ hier_smem) {
   float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(hier_smem);                      // [B][side]
   uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(hier_smem + kRefitBlock * 48);   // far end
   int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(hier_smem + kRefitBlock * 56);            // its delta
@@ -416,11 +420,16 @@ __global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
     uint32_t* flag = node_flags + g.ib + lg;
     const int dfar = is_left ? dl : dr;
     const uint32_t inc = kArrive | (leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
-    // acq_rel: the first arrival's add releases the subtree it wrote (its
-    // node or triangle record); the second's add acquires it, so the second
-    // reads the sibling right after its own atomic
-    const uint32_t old = atomic_add_acq_rel_gpu(flag, inc);
-    if ((old & 0xFu) == 0) return;  // first: the sibling's climb continues
+    const uint32_t old = atomic_add_acquire_gpu(flag, inc);
+    if ((old & 0xFu) == 0) {  // first: publish the subtree written above
+      red_add_release_gpu(flag, kBoxReady);
+      return;
+    }
+    // the first arrival's release may still be in flight
+    if (!(old & kBoxReady) && !wait_bits_acquire(flag, kBoxReady, kRefitWaitNs)) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      return;
+    }
     const bool sib_leaf = (old & kLeafArrive) != 0;
     const int sd = (int)((old >> 16) & 0x7Fu) - 1;
     f3 smn, smx;
@@ -470,6 +479,17 @@ __global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
     dr = dR;
     leaf = false;
   }
+}
+
+__global__ void __launch_bounds__(kRefitBlock) hierarchy_kernel(
+    const float* __restrict__ verts, const uint32_t* __restrict__ leaf_ids, const uint32_t* __restrict__ codes,
+    uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
+    uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
+    float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
+    uint32_t* __restrict__ roots, uint32_t* __restrict__ status) {
+  extern __shared__ __align__(16) unsigned char hier_smem[];
+  hierarchy_tile(verts, leaf_ids, codes, n, seg_offsets, n_seg, internal_offsets, node_meta, node_leaf_counts,
+                 leaf_parent, node_bounds, node_flags, leaf_tris, roots, status, hier_smem);
 }
 
 // ---------------------------------------------------------------------------
@@ -734,14 +754,15 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 }
 
 // ---------------------------------------------------------------------------
-// 5. One-launch front end of the build of one scene of up to
-//    fused::kMaxLeaves triangles: bounds, Morton keys and the sort in one
-//    cooperative launch, followed by hierarchy_kernel (section 3).
+// 5. One-launch build of one scene of up to fused::kMaxLeaves triangles:
+//    bounds, Morton keys, the sort and the hierarchy in one cooperative
+//    launch.
 //
 //    At 65,536 triangles every kernel of the per-stage build is latency
-//    bound, and the sort is four onesweep passes of about 10 us each.  Here
-//    one CTA per kTile keys runs the phases, which meet at grid-wide barriers
-//    (bounded waits, BAJO_STATUS_GRID_TIMEOUT):
+//    bound, and its sort is four onesweep passes of about 10 us each.  Here
+//    one CTA per kTile keys (= hierarchy_kernel's kRefitBlock sorted leaves)
+//    runs the phases, which meet at grid-wide barriers (bounded waits,
+//    BAJO_STATUS_GRID_TIMEOUT):
 //      A  triangle bounds, root and centroid bounds              -> barrier 1
 //      B  Morton codes (kept in registers), the histogram of the top
 //         kBucketBits code bits, and every LSD pass's digit histogram
@@ -755,19 +776,21 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 //         into shared memory and ranks every key inside its bucket by
 //         (code, item id).  Item ids are unique, so this is exactly the
 //         order of a stable sort by code: the multi-pass LSD sort's output.
+//                                                                 -> barrier 4
 //    Sort, otherwise: LSD radix passes over the 30-bit code (8-bit digits):
 //    each tile ranks its keys (stable, in position order) and scatters them
 //    to base(digit) + counts of the digit in earlier tiles + rank, counting
 //    the next pass's digits per destination tile as it scatters, so a pass
 //    needs one barrier                                            -> barriers 3-6
+//      H  hierarchy_tile (section 3) over the CTA's sorted leaves.
 //    Every output array is bit-identical to the per-stage build's.
 // ---------------------------------------------------------------------------
 namespace fused {
-constexpr int kThreads = 512;
-constexpr int kKpt = 4;                              // keys per thread
-constexpr uint32_t kTile = kThreads * kKpt;          // keys per CTA
+constexpr int kThreads = kRefitBlock;                // the hierarchy phase's CTA
+constexpr int kKpt = 1;                              // keys per thread
+constexpr uint32_t kTile = kThreads * kKpt;          // keys (and sorted leaves) per CTA
 constexpr uint32_t kMaxLeaves = 1u << 17;
-constexpr uint32_t kMaxTiles = kMaxLeaves / kTile;  // 64
+constexpr uint32_t kMaxTiles = kMaxLeaves / kTile;  // 256
 constexpr int kPasses = 4;                           // LSD digits [0,8) [8,16) [16,24) [24,30)
 constexpr int kWarps = kThreads / 32;
 constexpr int kBucketBits = 12;                      // buckets: the top 12 of the 30 code bits
@@ -807,8 +830,10 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
 constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;                                 // phase A
 constexpr size_t kSmemFast = (size_t)kBuckets * 4 + 80 * 4 + (size_t)kOwnedMax * 8;  // fast sort
 constexpr size_t kSmemLsd = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
+constexpr size_t kSmemHier = (size_t)kRefitBlock * 72 + 8;                          // phase H
 constexpr size_t kSmemMax2 = kSmemFast > kSmemLsd ? kSmemFast : kSmemLsd;
-constexpr size_t kSmem = ((kSmemVerts > kSmemMax2 ? kSmemVerts : kSmemMax2) + 15) & ~(size_t)15;
+constexpr size_t kSmemMax3 = kSmemHier > kSmemMax2 ? kSmemHier : kSmemMax2;
+constexpr size_t kSmem = ((kSmemVerts > kSmemMax3 ? kSmemVerts : kSmemMax3) + 15) & ~(size_t)15;
 
 // Grid-wide barrier number k (1, 2, ...) of a cooperative launch: every CTA
 // adds one to *bar (released) and waits until all of them have, for at most
@@ -878,7 +903,7 @@ __device__ __forceinline__ void scan_buckets(uint32_t* s_b, uint32_t* s_tmp, uin
 }
 
 template <bool VEC>
-__global__ void __launch_bounds__(kThreads, 2) lbvh_front_kernel(const float* __restrict__ verts, uint32_t n,
+__global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __restrict__ verts, uint32_t n,
                                                                  BajoLbvh t, unsigned char* __restrict__ ws,
                                                                  uint32_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -1013,6 +1038,7 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_front_kernel(const float* __
   if (!grid_sync(bar, 2, status, &s_flag)) return;
 
   // ---------------- sort, fast path: buckets of the top code bits
+  bool sorted = false;
   {
     uint32_t* s_b = reinterpret_cast<uint32_t*>(smem);  // [kBuckets] bucket starts
     uint32_t* s_tmp = s_b + kBuckets;                    // scan scratch [64] + results [2]
@@ -1074,13 +1100,14 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_front_kernel(const float* __
           t.sort_keys[dst] = (uint64_t)me.x;
         }
       }
-      return;
+      if (!grid_sync(bar, 4, status, &s_flag)) return;
     }
     __syncthreads();  // the bucket starts are no longer read: the passes reuse the buffer
+    sorted = fast;
   }
 
   // ---------------- sort, otherwise: LSD radix passes
-  {
+  if (!sorted) {
     uint32_t* s_wh = reinterpret_cast<uint32_t*>(smem);           // [kWarps][256]: counts, then starts
     uint32_t* s_off = s_wh + kWarps * 256;                         // [256] global position - tile position
     uint32_t* s_pre = s_off + 256;                                 // [2][256] counts of the earlier tiles
@@ -1168,9 +1195,14 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_front_kernel(const float* __
             atomicAdd(next_counts + tag, (uint32_t)__popc(same));
         }
       }
-      if (ps + 1 < kPasses && !grid_sync(bar, 3 + ps, status, &s_flag)) return;
+      if (!grid_sync(bar, 3 + ps, status, &s_flag)) return;
     }
   }
+
+  // ---------------- phase H: the bottom-up hierarchy, refit and triangle
+  // records over this CTA's kTile sorted leaves (section 3)
+  hierarchy_tile(verts, t.leaf_ids, t.morton_codes, n, t.seg_offsets, 1, t.internal_offsets, t.node_meta,
+                 t.node_leaf_counts, t.leaf_parent, t.node_bounds, t.node_flags, t.leaf_tris, t.roots, status, smem);
 }
 
 
@@ -1187,7 +1219,7 @@ bool can_run(uint32_t n, uint32_t n_seg) {
   return n_seg == 1 && n >= 2 && n <= g_fused_max_leaves.load(std::memory_order_relaxed) && n <= kMaxLeaves;
 }
 
-// Enqueues the front end (one cooperative launch); *launched = false when the
+// Enqueues the build (one cooperative launch); *launched = false when the
 // grid cannot be co-resident on this device (the caller then runs the
 // per-stage kernels).
 cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws, uint32_t* status, cudaStream_t st,
@@ -1196,7 +1228,7 @@ cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws,
   const uint32_t n = bvh->n_leaves;
   const uint32_t G = (n + kTile - 1) / kTile;
   const bool vec = ((uintptr_t)d_verts & 15) == 0;
-  auto kern = vec ? lbvh_front_kernel<true> : lbvh_front_kernel<false>;
+  auto kern = vec ? lbvh_fused_kernel<true> : lbvh_fused_kernel<false>;
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
@@ -1204,14 +1236,14 @@ cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws,
   DeviceState& ds = g_fused_state[dev];
   if (!ds.ready) {
     int per_sm_t = 0, per_sm_f = 0;
-    if ((e = cudaFuncSetAttribute(lbvh_front_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if ((e = cudaFuncSetAttribute(lbvh_fused_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmem)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(lbvh_front_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        (e = cudaFuncSetAttribute(lbvh_fused_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   (int)kSmem)) != cudaSuccess)
       return e;
-    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, lbvh_front_kernel<true>, kThreads, kSmem)) !=
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_t, lbvh_fused_kernel<true>, kThreads, kSmem)) !=
             cudaSuccess ||
-        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, lbvh_front_kernel<false>, kThreads, kSmem)) !=
+        (e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, lbvh_fused_kernel<false>, kThreads, kSmem)) !=
             cudaSuccess)
       return e;
     ds.max_ctas = min(per_sm_t, per_sm_f) * sm_count();
@@ -1438,16 +1470,14 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   cudaStream_t st = (cudaStream_t)stream_;
   unsigned char* ws = (unsigned char*)ws_;
   uint32_t* status = (uint32_t*)ws;
-  // one scene of up to fused::kMaxLeaves triangles: the one-launch front end,
-  // then the hierarchy; its stage events are [start, front end, hierarchy]
-  if (!hploc && fused::can_run(n, S) && (!ev || n_ev == 3)) {
+  // one scene of up to fused::kMaxLeaves triangles: the one-launch build;
+  // its stage events are [start, build]
+  if (!hploc && fused::can_run(n, S) && (!ev || n_ev == 2)) {
     if (ev && cudaEventRecord(ev[0], st) != cudaSuccess) return BAJO_ERR_CUDA;
     bool launched = false;
     if (fused::launch(d_verts, bvh, ws, status, st, &launched) != cudaSuccess) return BAJO_ERR_CUDA;
     if (launched) {
       if (ev && cudaEventRecord(ev[1], st) != cudaSuccess) return BAJO_ERR_CUDA;
-      if (launch_hierarchy(d_verts, bvh, status, st) != cudaSuccess) return BAJO_ERR_CUDA;
-      if (ev && cudaEventRecord(ev[2], st) != cudaSuccess) return BAJO_ERR_CUDA;
       if (bvh->top_nodes && launch_stage_top(bvh, st) != cudaSuccess) return BAJO_ERR_CUDA;
       return BAJO_OK;
     }
@@ -1576,7 +1606,7 @@ int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* 
     if (cudaGetDevice(&dev) == cudaSuccess && dev >= 0 && dev < 64) {
       const fused::DeviceState& ds = fused::g_fused_state[dev];
       if (!ds.ready || (int)((n_tris + fused::kTile - 1) / fused::kTile) <= ds.max_ctas) {
-        *launches = 2;  // the front end, then hierarchy_kernel
+        *launches = 1;  // the one-launch build
         return BAJO_OK;
       }
     }
@@ -1589,9 +1619,9 @@ int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* 
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events) {
   if (!n_events || n_segments == 0) return BAJO_ERR_INVALID_ARGUMENT;
   int32_t launches = 0;
-  if (bajo_lbvh_build_launches(n_tris, n_segments, &launches) == BAJO_OK && launches == 2 &&
+  if (bajo_lbvh_build_launches(n_tris, n_segments, &launches) == BAJO_OK && launches == 1 &&
       bajo::fused::can_run(n_tris, n_segments)) {
-    *n_events = 3;  // [start, front end, hierarchy]
+    *n_events = 2;  // [start, build]
     return BAJO_OK;
   }
   *n_events = (int32_t)(5 + bajo::make_build_plan(n_tris, n_segments).passes);

@@ -40,15 +40,17 @@ WORKLOAD = "plain LBVH build of 65,536 random triangles (seed 0) + 1024x1024 clo
 # Algorithmic bytes of one onesweep digit pass over the LBVH sort (the
 # per-stage build): read and write one u64 key and one u32 payload per key.
 PASS_BYTES_PER_KEY = 24
-# Algorithmic bytes per triangle of the build's two kernels.
-#  lbvh_front_kernel: vertices 36 read, leaf bounds 24 written, arrival
-#    counter 4 cleared; bucket sort of u32 code + u32 id: 8 written to the
-#    buckets, 8 read back, 16 written as sorted codes, ids and u64 keys.
-#  hierarchy_kernel: codes 4, ids 4 and vertices 36 read; triangle record 48,
-#    node meta 16, node boxes 48, leaf count 4, arrival counter 4 and parent
-#    link 4 written.
-KERNEL_BYTES_PER_TRI = {"lbvh_front_kernel": 36 + 24 + 4 + 8 + 8 + 16,
-                        "hierarchy_kernel": 4 + 4 + 36 + 48 + 16 + 48 + 4 + 4 + 4}
+# Algorithmic bytes per triangle of the build kernels.
+#  lbvh_fused_kernel (the one-launch build): bounds (vertices 36 read, leaf
+#    bounds 24 written, arrival counter 4 cleared), bucket sort of u32 code +
+#    u32 id (8 written to the buckets, 8 read back, 16 written as sorted
+#    codes, ids and u64 keys), hierarchy (codes 4, ids 4 and vertices 36
+#    read; triangle record 48, node meta 16, node boxes 48, leaf count 4,
+#    arrival counter 4 and parent link 4 written).
+#  hierarchy_kernel (per-stage build): the hierarchy part alone.
+_HIER_BYTES = 4 + 4 + 36 + 48 + 16 + 48 + 4 + 4 + 4
+KERNEL_BYTES_PER_TRI = {"lbvh_fused_kernel": 36 + 24 + 4 + 8 + 8 + 16 + _HIER_BYTES,
+                        "hierarchy_kernel": _HIER_BYTES}
 # digit passes of the single-scene LBVH sort: 8-bit digits over the 30-bit
 # Morton code, bits [0, 32) (the reference CPU builder's four byte passes,
 # bajo/bvh/cpu/builder/lbvh.mojo:56-62)
@@ -348,8 +350,8 @@ def run_bajo(args):
 
     launches = ctypes.c_int32(0)
     _lib.check(L.bajo_lbvh_build_launches(N_TRIS, 1, ctypes.byref(launches)), "bajo_lbvh_build_launches")
-    kernels_per_build = launches.value  # 2: the one-launch front end, then hierarchy_kernel
-    n_ev = stage_count()                # 3: [start, front end, hierarchy]
+    kernels_per_build = launches.value  # 1: the one-launch build
+    n_ev = stage_count()                # 2: [start, build]
 
     def build_timed(events):
         arr = (ctypes.c_void_p * len(events))(*[e.cuda_event for e in events])
@@ -412,7 +414,7 @@ def run_bajo(args):
     mrays = world * n_rays * args.steps / trace_total / 1e6
 
     # ---- the per-stage kernels of the same build (one scene takes them when
-    # the front end is switched off), with an event between every kernel
+    # the one-launch build is switched off), with an event between every kernel
     _lib.check(L.bajo_lbvh_fused_max_set(0), "bajo_lbvh_fused_max_set")
     n_stage = stage_count()
     passes = n_stage - 5
@@ -432,12 +434,11 @@ def run_bajo(args):
         "hierarchy": statistics.mean(e[2 + passes].elapsed_time(e[4 + passes]) for e in stage_ev),
     }
 
-    # ---- roofline: the build's dominant kernel, from the events between its
-    # two kernels (front end: bounds + Morton + sort; hierarchy_kernel)
+    # ---- roofline: the build's dominant kernel (with the one-launch build its
+    # only kernel; its events bracket that launch and a 4 KB memset)
     peak, peak_kind = measured_peaks()
-    if n_ev == 3:
-        kern_us = {"lbvh_front_kernel": statistics.mean(e[0].elapsed_time(e[1]) for e in stage_events) * 1e3,
-                   "hierarchy_kernel": statistics.mean(e[1].elapsed_time(e[2]) for e in stage_events) * 1e3}
+    if n_ev == 2:
+        kern_us = {"lbvh_fused_kernel": statistics.mean(e[0].elapsed_time(e[1]) for e in stage_events) * 1e3}
     else:  # the per-stage kernels
         kern_us = {"hierarchy_kernel": stage["hierarchy"] * 1e3}
     top = max(kern_us, key=kern_us.get)
@@ -562,7 +563,7 @@ def run_bajo(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": workload_config(), "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
         "sort": "bucket sort over the top 12 code bits (LSD passes when a bucket holds more than 256 keys)"
-                if kernels_per_build == 2 else f"{passes} onesweep passes",
+                if kernels_per_build == 1 else f"{passes} onesweep passes",
         "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": int(verts.numel() * 4),
                 "d2h_bytes_per_step": 12 * 4,
                 "what": "every step: pinned H2D of its vertices + bajo_lbvh_build + D2H of the root child boxes; "
@@ -769,7 +770,8 @@ def run_render(steps, warmup, spp=64, graph=True):
     rays, shadows = ws.ray_counts()
     paths = 1280 * 720 * spp
     out = {"workload": "64 icospheres (subdivision 5) + box + 0.25x0.25 light (emission 15), 1280x720, "
-                       f"{spp} spp, MIS, depth 8", "triangles": sc.n_tris, "ms": round(t, 3),
+                       f"{spp} spp, MIS, depth 8", "bvh_policy": rt.DEFAULT_BVH_POLICY, "triangles": sc.n_tris,
+           "ms": round(t, 3),
            "samples_s": round(paths / t * 1e3, 1), "mrays_s": round((rays + shadows) / t / 1e3, 2),
            "rays": rays, "shadow_rays": shadows, "status": ws.status()}
     if graph:
@@ -795,7 +797,7 @@ def run_render(steps, warmup, spp=64, graph=True):
     # reference's GPU_RT_BVH_* choices, bajo/rt/gpu/prepared_scene.mojo:29-33)
     by_policy = {}
     for policy in rt.BVH_POLICIES:
-        g = gsc if policy == "lbvh" else rt.GpuRtTriangleScene(sc, bvh_policy=policy)
+        g = gsc if policy == rt.DEFAULT_BVH_POLICY else rt.GpuRtTriangleScene(sc, bvh_policy=policy)
         rt.render_gpu_triangles(settings, sc.camera, g, rt.MIS, workspace=ws)
         pm = []
         for _ in range(steps):

@@ -173,20 +173,19 @@ int32_t bajo_lbvh_sizes(uint32_t n_tris, uint32_t n_segments, BajoLbvhSizes* siz
  * key bits, Karras topology, atomic-flag refit, sorted triangle packing.
  * d_verts: 9 floats per triangle [v0 xyz, v1 xyz, v2 xyz].  bvh->seg_offsets
  * and every output array must be set by the caller.
- * One scene (S = 1) of 2 .. 2^17 triangles runs its bounds, Morton keys and
- * sort in one cooperative kernel launch (grid barriers between the phases; a
- * barrier wait that runs out sets BAJO_STATUS_GRID_TIMEOUT), then the
- * hierarchy kernel; other builds launch one kernel per stage.  Both give the
- * same arrays bit for bit. */
+ * One scene (S = 1) of 2 .. 2^17 triangles is built by one cooperative
+ * kernel launch (grid barriers between the phases; a barrier wait that runs
+ * out sets BAJO_STATUS_GRID_TIMEOUT); other builds launch one kernel per
+ * stage.  Both give the same arrays bit for bit. */
 int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                         void* stream);
 
-/* Largest scene (triangles) the one-launch front end takes, at most 2^17 (the
+/* Largest scene (triangles) the one-launch build takes, at most 2^17 (the
  * default); 0 sends every build through the per-stage kernels.  Process wide,
  * like the sort tuning table: set it before building, not concurrently. */
 int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves);
 /* Kernel launches bajo_lbvh_build makes for n_tris triangles in n_segments
- * segments on the current device (2 with the one-launch front end). */
+ * segments on the current device (1 for the one-launch build). */
 int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* launches);
 
 /* H-PLOC build (GpuBvhBuildMethod.HPLOC, the reference's default builder,
@@ -210,9 +209,9 @@ int32_t bajo_hploc_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace,
  * `events` holds n_events cudaEvent_t handles created by the caller; the
  * build records them on `stream` at [start, bounds, morton, sort pass 0..P-1,
  * topology, refit]: bajo_lbvh_stage_count gives n_events = P + 5.  A build
- * that takes the one-launch front end has three events instead, [start, front
- * end, hierarchy] (bajo_lbvh_stage_count gives 3); with
- * bajo_lbvh_fused_max_set(0) first, it times the per-stage kernels. */
+ * that takes the one-launch build has two events instead, [start, build]
+ * (bajo_lbvh_stage_count gives 2); with bajo_lbvh_fused_max_set(0) first, it
+ * times the per-stage kernels. */
 int32_t bajo_lbvh_build_timed(const float* d_verts, BajoLbvh* bvh, void* d_workspace, size_t workspace_bytes,
                               void* stream, void* const* events, int32_t n_events);
 int32_t bajo_lbvh_stage_count(uint32_t n_tris, uint32_t n_segments, int32_t* n_events);

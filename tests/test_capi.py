@@ -57,7 +57,11 @@ def test_lbvh_sizes(lib):
     assert s["seg_bounds"] == 48 and s["internal_offsets"] == 8
     assert s["workspace"] > 65536 * 12
     s2 = lbvh_sizes(65536, 4096)
-    assert s2["roots"] == 4096 * 4 and s2["workspace"] > s["workspace"]
+    # segmented keys (u64, 44 live bits) and their alternate buffers
+    assert s2["roots"] == 4096 * 4 and s2["workspace"] > 65536 * 12 + 4096 * 48
+    # one scene of up to 2^17 triangles also has room for the one-launch
+    # build: two u32 key / id buffers and the per-(pass, tile) digit counts
+    assert s["workspace"] > 4 * 65536 * 4 + 4 * 256 * 256 * 4
     out = _lib.BajoLbvhSizesC()
     assert lib.bajo_lbvh_sizes(10, 0, ctypes.byref(out)) == _lib.ERR_INVALID_ARGUMENT
 

@@ -17,7 +17,7 @@ W, H = 48, 36
 @pytest.fixture(scope="module")
 def indirect():
     s = scenes.indirect_box_scene()
-    return s, rt.GpuRtTriangleScene(s)
+    return s, rt.GpuRtTriangleScene(s, bvh_policy="lbvh")
 
 
 def _mis(gs, cam, spp, seed, w=W, h=H):

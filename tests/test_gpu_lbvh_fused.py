@@ -1,9 +1,9 @@
-"""The one-launch front end of the LBVH build (bounds, Morton keys and sort
-in one cooperative kernel for a single scene of up to 2^17 triangles, then
-the hierarchy kernel) against the per-stage kernels and the oracle, bit for
-bit, on sizes around its 2,048-key tiles and on inputs that take the bucket
-sort (random triangles, a degenerate axis) or its LSD fallback (duplicate
-centroids, one far outlier: buckets past 256 keys)."""
+"""The one-launch LBVH build (bounds, Morton keys, sort and hierarchy in one
+cooperative kernel for a single scene of up to 2^17 triangles) against the
+per-stage kernels and the oracle, bit for bit, on sizes around its 512-leaf
+tiles and on inputs that take the bucket sort (random triangles, a
+degenerate axis) or its LSD fallback (duplicate centroids, one far outlier:
+buckets past 256 keys)."""
 import ctypes
 
 import numpy as np
@@ -17,7 +17,7 @@ from bajo_b200 import scenes  # noqa: E402
 
 from test_gpu_lbvh import assert_same_build, h  # noqa: E402
 
-SIZES = [2, 3, 31, 100, 2047, 2048, 2049, 4095, 4096, 6000, 65535, 65536, 65537, 100_003, 131071, 131072]
+SIZES = [2, 3, 31, 100, 511, 512, 513, 2047, 2048, 2049, 6000, 65535, 65536, 65537, 100_003, 131071, 131072]
 
 
 def _build(v, fused: bool):
@@ -60,7 +60,7 @@ def test_fused_equals_oracle_and_stage_kernels(oracle, n):
     v = _scene("random", n, seed=n)
     launches = ctypes.c_int32(0)
     assert L.bajo_lbvh_build_launches(n, 1, ctypes.byref(launches)) == _lib.OK
-    assert launches.value == 2
+    assert launches.value == 1
     f = _build(v, True)
     assert_same_build(f, oracle.lbvh_build(v))
     s = _build(v, False)
@@ -114,14 +114,14 @@ def test_fused_limits():
     L = _lib.load()
     assert L.bajo_lbvh_fused_max_set(_lib.FUSED_MAX_LEAVES + 1) == _lib.ERR_TOO_LARGE
     x = ctypes.c_int32(0)
-    assert L.bajo_lbvh_build_launches(_lib.FUSED_MAX_LEAVES + 1, 1, ctypes.byref(x)) == _lib.OK and x.value > 2
-    assert L.bajo_lbvh_build_launches(1000, 2, ctypes.byref(x)) == _lib.OK and x.value > 2  # segmented
-    assert L.bajo_lbvh_build_launches(1, 1, ctypes.byref(x)) == _lib.OK and x.value > 2
-    assert L.bajo_lbvh_stage_count(65536, 1, ctypes.byref(x)) == _lib.OK and x.value == 3
+    assert L.bajo_lbvh_build_launches(_lib.FUSED_MAX_LEAVES + 1, 1, ctypes.byref(x)) == _lib.OK and x.value > 1
+    assert L.bajo_lbvh_build_launches(1000, 2, ctypes.byref(x)) == _lib.OK and x.value > 1  # segmented
+    assert L.bajo_lbvh_build_launches(1, 1, ctypes.byref(x)) == _lib.OK and x.value > 1
+    assert L.bajo_lbvh_stage_count(65536, 1, ctypes.byref(x)) == _lib.OK and x.value == 2
 
 
 def test_fused_timed_build_events(oracle):
-    """The stage-timed build takes the same path: three events."""
+    """The stage-timed build takes the same path: two events."""
     from bajo_b200 import _lib, bvh
     L = _lib.load()
     n = 65536
@@ -129,15 +129,15 @@ def test_fused_timed_build_events(oracle):
     d = torch.from_numpy(v).cuda()
     ws = bvh.GpuBvhBuildWorkspace(n, 1)
     t = bvh.build_triangle_bvh(d, workspace=ws)
-    evs = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
     for e in evs:
         e.record()
-    arr = (ctypes.c_void_p * 3)(*[e.cuda_event for e in evs])
+    arr = (ctypes.c_void_p * 2)(*[e.cuda_event for e in evs])
     c = t.c_struct(stage_top=False)
     s = torch.cuda.current_stream().cuda_stream
     assert L.bajo_lbvh_build_timed(d.data_ptr(), ctypes.byref(c), ws.buffer.data_ptr(), ws.buffer.numel(), s, arr,
-                                   3) == _lib.OK
+                                   2) == _lib.OK
     torch.cuda.synchronize()
-    assert evs[0].elapsed_time(evs[1]) > 0 and evs[1].elapsed_time(evs[2]) > 0
+    assert evs[0].elapsed_time(evs[1]) > 0
     assert ws.status() == 0
     assert_same_build(t, oracle.lbvh_build(v))

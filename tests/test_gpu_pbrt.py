@@ -67,7 +67,7 @@ def scene():
     loader.add_file("box/objects.pbrt", OBJECTS)
     s = pbrt.read_pbrt("box/main.pbrt", loader)
     rs = s.to_rt_scene(3)
-    return s, rs, rt.GpuRtTriangleScene(rs)
+    return s, rs, rt.GpuRtTriangleScene(rs, bvh_policy="lbvh")
 
 
 @pytest.mark.parametrize("algorithm", [rt.PATH, rt.NEE, rt.MIS])

@@ -16,7 +16,7 @@ from bajo_b200 import rt, scenes  # noqa: E402
 @pytest.fixture(scope="module")
 def small():
     sc = scenes.small_rt_scene()
-    return sc, rt.GpuRtTriangleScene(sc)
+    return sc, rt.GpuRtTriangleScene(sc, bvh_policy="lbvh")
 
 
 def _direct(sc, gsc, settings, cam, algorithm=rt.MIS):

@@ -14,7 +14,7 @@ from bajo_b200 import scenes  # noqa: E402
 def small():
     from bajo_b200 import rt
     sc = scenes.small_rt_scene()
-    return sc, rt.GpuRtTriangleScene(sc)
+    return sc, rt.GpuRtTriangleScene(sc, bvh_policy="lbvh")
 
 
 @pytest.mark.parametrize("algorithm", [0, 3, 4])
@@ -65,7 +65,7 @@ def test_large_scene_render_matches_oracle(oracle):
     from bajo_b200 import rt
     sc = scenes.spheres_in_box()
     assert sc.n_tris == 12 + 2 + 64 * 20480
-    gsc = rt.GpuRtTriangleScene(sc)
+    gsc = rt.GpuRtTriangleScene(sc, bvh_policy="lbvh")
     w, h, spp = 32, 18, 2
     img = rt.render_gpu_triangles(rt.RenderSettings(w, h, spp), sc.camera, gsc, rt.MIS)
     torch.cuda.synchronize()
@@ -77,7 +77,7 @@ def test_large_scene_render_matches_oracle(oracle):
 def materials():
     from bajo_b200 import rt
     sc = scenes.materials_in_box(n_spheres=8, subdivisions=2)
-    return sc, rt.GpuRtTriangleScene(sc)
+    return sc, rt.GpuRtTriangleScene(sc, bvh_policy="lbvh")
 
 
 @pytest.mark.parametrize("algorithm", [0, 3, 4])

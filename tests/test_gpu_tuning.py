@@ -1,7 +1,7 @@
 """Every choice the autotuner can install gives the same results: the
 closest-hit kernels' block sizes (64 / 128 / 256 threads) leave the hits
-bit-identical, and the one-launch build front end on or off leaves the tree
-bit-identical (the front end's own parity is in test_gpu_lbvh_fused.py)."""
+bit-identical, and the one-launch build on or off leaves the tree
+bit-identical (its own parity is in test_gpu_lbvh_fused.py)."""
 import ctypes
 
 import numpy as np
@@ -73,14 +73,14 @@ def test_trace_tuning_limits():
 
 
 def test_tuner_runs_and_keeps_results(oracle):
-    """A short tuning run of the closest-hit blocks and the front-end limit
+    """A short tuning run of the closest-hit blocks and the one-launch limit
     installs choices that reproduce the oracle's tree and hits."""
     from bajo_b200 import _lib, autotune, bvh, camera
     L = _lib.load()
     try:
         res = autotune.tune_trace("trace_camera", [16], reps=2)
         assert res[16]["best"] in (64, 128, 256)
-        fe = autotune.tune_front_end(range(15, 17), reps=2)
+        fe = autotune.tune_one_launch(range(15, 17), reps=2)
         assert set(v["best"] for v in fe.values()) <= {0, 1 << 15, 1 << 16}
         v = scenes.random_triangles(1 << 16, seed=9)
         t = bvh.build_triangle_bvh(torch.from_numpy(v).cuda())
