@@ -922,6 +922,13 @@ def run_extras(args, local):
         r = run_guided(gargs)
     r["clocks"] = ck.summary()
     out["guided"] = r
+    # the same comparison on the box lit only indirectly (its light faces the
+    # ceiling), where the error is in the indirect light the guide learns
+    gargs = parse_args(["--scene", "indirect"])
+    with ClockSampler(local) as ck:
+        r = run_guided(gargs)
+    r["clocks"] = ck.summary()
+    out["guided_indirect"] = r
     return out
 
 
