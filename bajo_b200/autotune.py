@@ -222,19 +222,35 @@ def load(path: str = CACHE) -> int:
     return count
 
 
-def tune_all(reps: int = 5, save_cache: bool = True) -> dict:
-    """The shapes the LBVH build and the sort sweep use."""
-    # 64-bit keys: up to 2^18 with the 30 live bits of single-scene LBVH keys
-    # (where 10-bit digits compete), above with 44 bits (segmented builds)
-    u64 = tune_sort(8, True, range(10, 19), end_bit=30, reps=reps)
-    u64.update(tune_sort(8, True, range(19, 27), end_bit=44, reps=reps))
-    res = {
-        _kernel_key(8, True): u64,
-        _kernel_key(4, True): tune_sort(4, True, range(10, 27), reps=reps),
-        "trace_camera": tune_trace("trace_camera", range(16, 23, 2), reps=reps),
-        "trace_rays": tune_trace("trace_rays", range(16, 23, 2), reps=reps),
-        "lbvh_one_launch": tune_one_launch(reps=reps),
-    }
+PARTS = ("sort", "trace", "one_launch")
+
+
+def tune_all(reps: int = 5, save_cache: bool = True, parts=PARTS) -> dict:
+    """The sort shapes the LBVH build and the sort sweep use, the closest-hit
+    block sizes and the one-launch build's size limit (``parts`` selects)."""
+    res = {}
+    if "sort" in parts:
+        # 64-bit keys: up to 2^18 with the 30 live bits of single-scene LBVH
+        # keys (where 10-bit digits compete), above with 44 bits (segmented)
+        u64 = tune_sort(8, True, range(10, 19), end_bit=30, reps=reps)
+        u64.update(tune_sort(8, True, range(19, 27), end_bit=44, reps=reps))
+        res[_kernel_key(8, True)] = u64
+        res[_kernel_key(4, True)] = tune_sort(4, True, range(10, 27), reps=reps)
+    if "trace" in parts:
+        res["trace_camera"] = tune_trace("trace_camera", range(16, 23, 2), reps=reps)
+        res["trace_rays"] = tune_trace("trace_rays", range(16, 23, 2), reps=reps)
+    if "one_launch" in parts:
+        res["lbvh_one_launch"] = tune_one_launch(reps=reps)
     if save_cache:
         save(res)
     return res
+
+
+if __name__ == "__main__":
+    import argparse
+    ap = argparse.ArgumentParser(description="measure the tuned choices on this GPU and cache them")
+    ap.add_argument("--parts", default=",".join(PARTS), help="comma-separated subset of " + ",".join(PARTS))
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args()
+    out = tune_all(reps=a.reps, parts=tuple(p for p in a.parts.split(",") if p))
+    print(json.dumps({k: {str(lg): v["best"] for lg, v in t.items()} for k, t in out.items()}))
