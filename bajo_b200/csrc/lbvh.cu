@@ -296,7 +296,8 @@ __device__ __forceinline__ void hierarchy_tile(
     uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
     uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
     float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
-    uint32_t* __restrict__ roots, uint32_t* __restrict__ status, unsigned char* __restrict__ hier_smem) {
+    uint32_t* __restrict__ roots, uint32_t* __restrict__ status, unsigned char* __restrict__ hier_smem,
+    const uint32_t* bound2 = nullptr) {
   float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(hier_smem);                      // [B][side]
   uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(hier_smem + kRefitBlock * 48);   // far end
   int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(hier_smem + kRefitBlock * 56);            // its delta
@@ -318,8 +319,9 @@ __device__ __forceinline__ void hierarchy_tile(
 
   s_cnt[tid] = 0;
   s_code[tid + 1] = s < n ? codes[s] : 0u;
-  if (tid == 0) s_code[0] = (c0 > 0 && c0 - 1 < n) ? codes[c0 - 1] : 0u;
-  if (tid == kRefitBlock - 1) s_code[kRefitBlock + 1] = (s + 1 < n) ? codes[s + 1] : 0u;
+  // the sorted codes just outside the tile (bound2: given by the caller)
+  if (tid == 0) s_code[0] = (c0 > 0 && c0 - 1 < n) ? (bound2 ? bound2[0] : codes[c0 - 1]) : 0u;
+  if (tid == kRefitBlock - 1) s_code[kRefitBlock + 1] = (s + 1 < n) ? (bound2 ? bound2[1] : codes[s + 1]) : 0u;
 
   SegInfo g{0, 0, 0};
   bool active = s < n;
@@ -797,7 +799,7 @@ constexpr int kBucketBits = 12;                      // buckets: the top 12 of t
 constexpr uint32_t kBuckets = 1u << kBucketBits;
 constexpr uint32_t kBucketShift = 30 - kBucketBits;
 constexpr uint32_t kBucketMax = 256;                 // fast path: no bucket larger than this
-constexpr uint32_t kOwnedMax = kTile + kBucketMax;   // keys a CTA owns on the fast path, at most
+constexpr uint32_t kLoadMax = kTile + 2 + 2 * kBucketMax;  // keys a CTA ranks on the fast path, at most
 constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
 
 // Workspace (bytes from the start of the build workspace; word 0 is the
@@ -828,7 +830,7 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
 
 // Shared memory, one buffer reused by the phases.
 constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;                                 // phase A
-constexpr size_t kSmemFast = (size_t)kBuckets * 4 + 80 * 4 + (size_t)kOwnedMax * 8;  // fast sort
+constexpr size_t kSmemFast = (size_t)kBuckets * 4 + 80 * 4 + (size_t)kLoadMax * 8;  // fast sort
 constexpr size_t kSmemLsd = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
 constexpr size_t kSmemHier = (size_t)kRefitBlock * 72 + 8;                          // phase H
 constexpr size_t kSmemMax2 = kSmemFast > kSmemLsd ? kSmemFast : kSmemLsd;
@@ -909,6 +911,7 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t s_red[kWarps][12];
   __shared__ uint32_t s_flag;
+  __shared__ uint32_t s_bound[2];  // sorted codes at positions base - 1 and base + kTile
   constexpr Layout kL0 = layout(0);
   const Layout L = layout(n);
   uint32_t* bar = reinterpret_cast<uint32_t*>(ws + kL0.off_bar);
@@ -998,9 +1001,9 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
   }
   if (!grid_sync(bar, 1, status, &s_flag)) return;
 
-  // ---------------- phase B: Morton codes and every pass's digit histogram
+  // ---------------- phase B: Morton codes and the bucket histogram
   uint32_t key[kKpt], val[kKpt];
-  uint32_t* s_hist = reinterpret_cast<uint32_t*>(smem);  // [kPasses][256]
+  uint32_t nbar = 1;  // grid barriers passed
   {
     const f3 cmin = mk(dec_min(__ldcg(seg_ord + 6)), dec_min(__ldcg(seg_ord + 7)), dec_min(__ldcg(seg_ord + 8)));
     const f3 cmax = mk(dec_max(__ldcg(seg_ord + 9)), dec_max(__ldcg(seg_ord + 10)), dec_max(__ldcg(seg_ord + 11)));
@@ -1011,8 +1014,6 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
       const bool is_min = tid < 3 || (tid >= 6 && tid < 9);
       t.seg_bounds[tid] = is_min ? dec_min(u) : dec_max(u);
     }
-    for (uint32_t q = tid; q < kPasses * 256; q += kThreads) s_hist[q] = 0;
-    __syncthreads();
 #pragma unroll
     for (int k = 0; k < kKpt; ++k) {
       const uint32_t p = pos0 + 32 * k;
@@ -1021,23 +1022,17 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
         key[k] = morton3(d.x * inv.x, d.y * inv.y, d.z * inv.z);
         val[k] = base + p;
         atomicAdd(&bhist[key[k] >> kBucketShift], 1u);
-#pragma unroll
-        for (int ps = 0; ps < kPasses; ++ps) atomicAdd(&s_hist[ps * 256 + ((key[k] >> (8 * ps)) & 255u)], 1u);
       } else {
         key[k] = 0xFFFFFFFFu;  // padding: the top digit in every pass, after every real key
         val[k] = 0;
       }
     }
-    __syncthreads();
-    for (uint32_t q = tid; q < kPasses * 256; q += kThreads) {
-      const uint32_t h = s_hist[q];
-      if (h) atomicAdd(&ghist[q], h);
-      if (q < 256) counts[c * 256 + q] = h;  // pass 0: this tile's digit counts
-    }
   }
-  if (!grid_sync(bar, 2, status, &s_flag)) return;
+  if (!grid_sync(bar, ++nbar, status, &s_flag)) return;
 
-  // ---------------- sort, fast path: buckets of the top code bits
+  // ---------------- sort, fast path: buckets of the top code bits.  It ends
+  // with this CTA's tile of sorted keys written and the codes just before
+  // and after the tile in s_bound, so the hierarchy needs no more barriers.
   bool sorted = false;
   {
     uint32_t* s_b = reinterpret_cast<uint32_t*>(smem);  // [kBuckets] bucket starts
@@ -1059,24 +1054,25 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
           }
         }
       }
-      if (!grid_sync(bar, 3, status, &s_flag)) return;
-      // S2: the buckets that start inside this tile, ranked in shared memory
-      uint2* s_kv = reinterpret_cast<uint2*>(s_tmp + 64 + 16);  // [kOwnedMax] (code, item)
-      // owned positions [lo, hi): from the first bucket start >= base to the
-      // first bucket start >= base + kTile (n past the last one)
-      auto first_start_at_or_after = [&](uint32_t p) {
-        uint32_t a = 0, z = kBuckets;  // smallest b with s_b[b] >= p, kBuckets if none
+      if (!grid_sync(bar, ++nbar, status, &s_flag)) return;
+      // S2: the buckets that hold the sorted positions base - 1 .. base +
+      // kTile, ranked in shared memory by (code, item); a bucket that also
+      // reaches into a neighbouring tile is ranked by both CTAs
+      uint2* s_kv = reinterpret_cast<uint2*>(s_tmp + 64 + 16);  // [kLoadMax] (code, item)
+      auto bucket_at = [&](uint32_t p) {  // the (non-empty) bucket holding sorted position p
+        uint32_t a = 0, z = kBuckets;     // first b with s_b[b] > p
         while (a < z) {
           const uint32_t m = (a + z) >> 1;
-          if (s_b[m] >= p) z = m;
+          if (s_b[m] > p) z = m;
           else a = m + 1;
         }
-        return a < kBuckets ? s_b[a] : n;
+        return a - 1u;  // s_b[0] = 0 <= p
       };
-      const uint32_t lo = base == 0 ? 0u : first_start_at_or_after(base);
-      const uint32_t hi = base + kTile >= n ? n : first_start_at_or_after(base + kTile);
+      const uint32_t p0 = base > 0 ? base - 1 : 0u, p1 = min(base + kTile, n - 1);
+      const uint32_t b1 = bucket_at(p1);
+      const uint32_t lo = s_b[bucket_at(p0)], hi = b1 + 1 < kBuckets ? s_b[b1 + 1] : n;
       const uint32_t m = hi > lo ? hi - lo : 0u;
-      if (m > kOwnedMax) {  // cannot happen when every bucket fits kBucketMax
+      if (m > kLoadMax) {  // cannot happen when every bucket fits kBucketMax
         if (tid == 0) raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
         return;
       }
@@ -1094,13 +1090,16 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
           rank += (((uint64_t)o.x << 32) | o.y) < mine ? 1u : 0u;
         }
         const uint32_t dst = bs + rank;
-        if (dst < n) {
+        if (dst >= base && dst < base + cnt) {
           t.morton_codes[dst] = me.x;
           t.leaf_ids[dst] = me.y;
           t.sort_keys[dst] = (uint64_t)me.x;
+        } else if (dst + 1 == base) {
+          s_bound[0] = me.x;
+        } else if (dst == base + kTile) {
+          s_bound[1] = me.x;
         }
       }
-      if (!grid_sync(bar, 4, status, &s_flag)) return;
     }
     __syncthreads();  // the bucket starts are no longer read: the passes reuse the buffer
     sorted = fast;
@@ -1113,6 +1112,25 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
     uint32_t* s_pre = s_off + 256;                                 // [2][256] counts of the earlier tiles
     uint32_t* s_tmp = s_pre + 512;                                 // scan scratch
     const uint32_t d_own = tid & 255u, half = tid >> 8;
+    {
+      // every pass's digit histogram (ghist was zeroed before the launch)
+      // and this tile's digit counts of pass 0
+      uint32_t* s_hist = s_wh;  // [kPasses][256]
+      for (uint32_t q = tid; q < kPasses * 256; q += kThreads) s_hist[q] = 0;
+      __syncthreads();
+#pragma unroll
+      for (int k = 0; k < kKpt; ++k)
+        if (pos0 + 32 * k < cnt)
+#pragma unroll
+          for (int ps = 0; ps < kPasses; ++ps) atomicAdd(&s_hist[ps * 256 + ((key[k] >> (8 * ps)) & 255u)], 1u);
+      __syncthreads();
+      for (uint32_t q = tid; q < kPasses * 256; q += kThreads) {
+        const uint32_t h = s_hist[q];
+        if (h) atomicAdd(&ghist[q], h);
+        if (q < 256) counts[c * 256 + q] = h;
+      }
+      if (!grid_sync(bar, ++nbar, status, &s_flag)) return;
+    }
     for (int ps = 0; ps < kPasses; ++ps) {
       const uint32_t sh = 8u * ps;
       // counts of this pass's digit d_own in the earlier tiles (half of them per thread)
@@ -1195,14 +1213,18 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
             atomicAdd(next_counts + tag, (uint32_t)__popc(same));
         }
       }
-      if (!grid_sync(bar, 3 + ps, status, &s_flag)) return;
+      if (!grid_sync(bar, ++nbar, status, &s_flag)) return;
     }
   }
 
   // ---------------- phase H: the bottom-up hierarchy, refit and triangle
-  // records over this CTA's kTile sorted leaves (section 3)
+  // records over this CTA's kTile sorted leaves (section 3).  After the fast
+  // path the tile's sorted keys are this CTA's own writes and the two
+  // boundary codes are in s_bound; after the passes a barrier has ended them.
+  __syncthreads();
   hierarchy_tile(verts, t.leaf_ids, t.morton_codes, n, t.seg_offsets, 1, t.internal_offsets, t.node_meta,
-                 t.node_leaf_counts, t.leaf_parent, t.node_bounds, t.node_flags, t.leaf_tris, t.roots, status, smem);
+                 t.node_leaf_counts, t.leaf_parent, t.node_bounds, t.node_flags, t.leaf_tris, t.roots, status, smem,
+                 sorted ? s_bound : nullptr);
 }
 
 
