@@ -27,6 +27,7 @@ STATUS_STAGE_TIMEOUT = 0x80
 STATUS_WAIT_TIMEOUT = 0x100
 STATUS_GRID_TIMEOUT = 0x200
 FUSED_MAX_LEAVES = 1 << 17  # largest scene the one-launch build takes
+LBVH_TOP_CAP = 1536  # subtrees per CTA in the one-launch build's top stage
 TRI_MT = 0
 TRI_WATERTIGHT = 1
 SORT_MAX_KEYS = (1 << 30) - 1
@@ -123,6 +124,7 @@ SIGNATURES = {
     "bajo_lbvh_build_timed": (_I32, [_P, ctypes.POINTER(BajoLbvhC), _P, _SZ, _P, ctypes.POINTER(_P), _I32]),
     "bajo_lbvh_stage_count": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_fused_max_set": (_I32, [_U32]),
+    "bajo_lbvh_fused_top_cap_set": (_I32, [_U32]),
     "bajo_trace_tuning_set": (_I32, [_I32, _U32, _I32]),
     "bajo_trace_tuning_get": (_I32, [_I32, _U32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_build_launches": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),

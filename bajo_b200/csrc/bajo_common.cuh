@@ -128,6 +128,12 @@ __device__ __forceinline__ uint32_t atomic_add_acquire_gpu(uint32_t* p, uint32_t
   asm volatile("atom.add.acquire.gpu.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
   return old;
 }
+// Release / acquire fence among the threads of one CTA (the message-passing
+// pattern of a shared-memory arrival counter: data, fence, counter on one
+// side; counter, fence, data on the other).  Lighter than the sequentially
+// consistent fence that __threadfence_block() issues.
+__device__ __forceinline__ void fence_acq_rel_cta() { asm volatile("fence.acq_rel.cta;" ::: "memory"); }
+
 __device__ __forceinline__ void red_add_release_gpu(uint32_t* p, uint32_t v) {
   asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }

@@ -216,8 +216,8 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
 //    agglomerative LBVH construction", 2014): a node [f, l] is the left child
 //    of its parent iff delta(l, l+1) > delta(f-1, f), so its parent splits at
 //    l (left child) or f-1 (right child).  The two children of a split meet
-//    there; the second to arrive knows the parent's whole range, writes the
-//    parent in Karras numbering and continues upwards.  Karras numbering: a
+//    there; the second to arrive knows the parent's whole range and continues
+//    upwards with the union of the two boxes.  Karras numbering: a
 //    non-root internal node is indexed by its last position when it is a left
 //    child and by its first when it is a right child; the root is 0.  The
 //    arrays are bit-identical to the top-down construction (same ranges,
@@ -225,7 +225,10 @@ __global__ void __launch_bounds__(kBlock) morton_kernel(const float* __restrict_
 //
 //    A CTA owns kRefitBlock consecutive sorted leaves.  Splits whose
 //    sibling starts inside the CTA meet in shared memory (arrival counter,
-//    child boxes, far range ends and their deltas in shared slots).  A split
+//    child boxes, far range ends and their deltas in shared slots); a climb
+//    step there touches shared memory only, and once every climb of the CTA
+//    has ended, one pass writes the records of all parents built in it (a
+//    slot holds everything its parent's record needs).  A split
 //    whose sibling lies (partly) outside meets in global memory after the
 //    CTA's local climbs are done: node_flags of the split counts the
 //    arrivals (acquire), the first arrival publishes its subtree (already
@@ -265,20 +268,32 @@ __device__ __forceinline__ void write_parent(const SegInfo& g, uint32_t k, uint3
   uint32_t* m = node_meta + (size_t)k * 4;
   if (F == g.lb && L == g.lb + g.len - 1) m[0] = kSentinel;  // the root
   m[1] = left;
-  m[2] = right;
-  m[3] = L;  // fence = leaf_begin + last
+  *reinterpret_cast<uint2*>(m + 2) = make_uint2(right, L);  // right child, fence = leaf_begin + last
   node_leaf_counts[k] = L - F + 1;
-  float2* b = reinterpret_cast<float2*>(node_bounds + (size_t)k * 12);
-  b[0] = make_float2(lmn.x, lmn.y);
-  b[1] = make_float2(lmn.z, lmx.x);
-  b[2] = make_float2(lmx.y, lmx.z);
-  b[3] = make_float2(rmn.x, rmn.y);
-  b[4] = make_float2(rmn.z, rmx.x);
-  b[5] = make_float2(rmx.y, rmx.z);
+  float4* b = reinterpret_cast<float4*>(node_bounds + (size_t)k * 12);  // 16-byte aligned (checked by the build)
+  b[0] = make_float4(lmn.x, lmn.y, lmn.z, lmx.x);
+  b[1] = make_float4(lmx.y, lmx.z, rmn.x, rmn.y);
+  b[2] = make_float4(rmn.z, rmx.x, rmx.y, rmx.z);
   if (left_leaf) leaf_parent[gamma] = k;
   else node_meta[(size_t)(g.ib + lg) * 4] = k;
   if (right_leaf) leaf_parent[gamma + 1] = k;
   else node_meta[(size_t)(g.ib + lg + 1) * 4] = k;
+}
+
+// Writes the parent split at gamma whose children [F, gamma] and [gamma + 1,
+// L] met in a shared-memory slot: dL, dR are the deltas at F and after L,
+// lb / rb the children's boxes (min xyz, max xyz).  node_flags may be null.
+__device__ __forceinline__ void write_slot_parent(const SegInfo& g, uint32_t gamma, uint32_t F, uint32_t L, int dL,
+                                                  int dR, const float* lb, const float* rb,
+                                                  uint32_t* __restrict__ node_meta,
+                                                  uint32_t* __restrict__ node_leaf_counts,
+                                                  uint32_t* __restrict__ leaf_parent, float* __restrict__ node_bounds,
+                                                  uint32_t* __restrict__ node_flags) {
+  const bool root = F == g.lb && L == g.lb + g.len - 1;
+  const uint32_t k = g.ib + (root ? 0u : (dR > dL ? L - g.lb : F - g.lb));
+  write_parent(g, k, F, L, gamma, mk(lb[0], lb[1], lb[2]), mk(lb[3], lb[4], lb[5]), mk(rb[0], rb[1], rb[2]),
+               mk(rb[3], rb[4], rb[5]), node_meta, node_leaf_counts, leaf_parent, node_bounds);
+  if (node_flags) node_flags[g.ib + (gamma - g.lb)] = 2u;  // (the one-launch build sets them all up front)
 }
 
 __device__ __forceinline__ void tri_box(const float4* __restrict__ rec, f3& mn, f3& mx) {
@@ -288,16 +303,29 @@ __device__ __forceinline__ void tri_box(const float4* __restrict__ rec, f3& mn, 
   mx = vmax(vmax(va, vb), vc);
 }
 
-// One CTA's share: sorted leaves [blockIdx.x * kRefitBlock, +kRefitBlock) with
-// kRefitBlock threads and kRefitBlock * 72 + 8 bytes of shared memory.  Run
-// by hierarchy_kernel and as the last phase of the one-launch build.
-__device__ __forceinline__ void hierarchy_tile(
+// A subtree on its way up: sorted leaves [f, l] (global positions), the
+// deltas at its two ends (-1 at a segment end), its box, and whether it is a
+// single leaf.
+struct Climb {
+  uint32_t f, l;
+  int dl, dr;
+  f3 mn, mx;
+  bool leaf;
+};
+
+// The shared-memory phase of one CTA's share: sorted leaves [blockIdx.x *
+// kRefitBlock, +kRefitBlock) with kRefitBlock threads and kRefitBlock * 72 + 8
+// bytes of shared memory.  Returns true for a thread whose subtree c still
+// has to meet its sibling outside the CTA.  The subtrees returned by all
+// threads of a CTA are the largest ones inside its tile, so they cover the
+// tile's leaves once each, in disjoint ranges.
+__device__ __forceinline__ bool hierarchy_local(
     const float* __restrict__ verts, const uint32_t* __restrict__ leaf_ids, const uint32_t* __restrict__ codes,
     uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
     uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
     float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
     uint32_t* __restrict__ roots, uint32_t* __restrict__ status, unsigned char* __restrict__ hier_smem,
-    const uint32_t* bound2 = nullptr) {
+    const uint32_t* bound2, SegInfo& g, Climb& out) {
   float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(hier_smem);                      // [B][side]
   uint32_t(*s_far)[2] = reinterpret_cast<uint32_t(*)[2]>(hier_smem + kRefitBlock * 48);   // far end
   int(*s_dfar)[2] = reinterpret_cast<int(*)[2]>(hier_smem + kRefitBlock * 56);            // its delta
@@ -323,7 +351,7 @@ __device__ __forceinline__ void hierarchy_tile(
   if (tid == 0) s_code[0] = (c0 > 0 && c0 - 1 < n) ? (bound2 ? bound2[0] : codes[c0 - 1]) : 0u;
   if (tid == kRefitBlock - 1) s_code[kRefitBlock + 1] = (s + 1 < n) ? (bound2 ? bound2[1] : codes[s + 1]) : 0u;
 
-  SegInfo g{0, 0, 0};
+  g = SegInfo{0, 0, 0};
   bool active = s < n;
   f3 mn, mx;
   if (active) {
@@ -380,37 +408,53 @@ __device__ __forceinline__ void hierarchy_tile(
     mine[0] = mn.x; mine[1] = mn.y; mine[2] = mn.z; mine[3] = mx.x; mine[4] = mx.y; mine[5] = mx.z;
     s_far[slot][side] = is_left ? f : l;
     s_dfar[slot][side] = is_left ? dl : dr;
-    __threadfence_block();
+    fence_acq_rel_cta();
     if (atomicAdd(&s_cnt[slot], 1u) == 0) {
       pending = (int)slot;
       break;
     }
-    __threadfence_block();
+    fence_acq_rel_cta();
     const float* sib = s_box[slot][side ^ 1];
     const f3 smn = mk(sib[0], sib[1], sib[2]), smx = mk(sib[3], sib[4], sib[5]);
     const uint32_t sfar = s_far[slot][side ^ 1];
     const int sd = s_dfar[slot][side ^ 1];
+    // the parent [F, L] is complete in the slot (both children's boxes, far
+    // ends and deltas); its record is written after the climbs
     const uint32_t F = is_left ? f : sfar, L = is_left ? sfar : l;
-    const int dL = is_left ? dl : sd, dR = is_left ? sd : dr;
-    const bool root = F == g.lb && L == g.lb + g.len - 1;
-    const uint32_t k = g.ib + (root ? 0u : (dR > dL ? L - g.lb : F - g.lb));
-    if (is_left) write_parent(g, k, F, L, gamma, mn, mx, smn, smx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
-    else write_parent(g, k, F, L, gamma, smn, smx, mn, mx, node_meta, node_leaf_counts, leaf_parent, node_bounds);
-    node_flags[g.ib + (gamma - g.lb)] = 2u;
     mn = vmin(mn, smn);
     mx = vmax(mx, smx);
     f = F;
     l = L;
-    dl = dL;
-    dr = dR;
+    dl = is_left ? dl : sd;
+    dr = is_left ? sd : dr;
     leaf = false;
-    if (root) active = false;
+    if (F == g.lb && L == g.lb + g.len - 1) active = false;  // the root
   }
   __syncthreads();  // every local climb of this CTA has ended
+  // the records of the parents built here: slot tid is the split at this
+  // thread's leaf s, inside its segment g
+  if (tid + 1 < kRefitBlock && s_cnt[tid] == 2u)
+    write_slot_parent(g, s, s_far[tid][0], s_far[tid][1], s_dfar[tid][0], s_dfar[tid][1], s_box[tid][0],
+                      s_box[tid][1], node_meta, node_leaf_counts, leaf_parent, node_bounds, node_flags);
   if (pending >= 0 && s_cnt[pending] == 1) global = true;  // the sibling comes from outside
-  if (!global) return;
+  out = Climb{f, l, dl, dr, mn, mx, leaf};
+  __syncthreads();  // the records are written (a climber that goes on fences before its release)
+  return global;
+}
 
-  // phase 2: the splits that cross a CTA boundary, in global memory
+// The climb of subtree c through the splits whose children were built by
+// different CTAs, in global memory (the protocol described above), up to the
+// segment's root or to the first split where c arrives first.  flags: the
+// arrival counters, zero before the build (node_flags, or a scratch array).
+__device__ __forceinline__ void climb_global(const SegInfo& g, Climb c, uint32_t* __restrict__ node_meta,
+                                             uint32_t* __restrict__ node_leaf_counts,
+                                             uint32_t* __restrict__ leaf_parent, float* __restrict__ node_bounds,
+                                             uint32_t* __restrict__ flags, const float* __restrict__ leaf_tris,
+                                             uint32_t* __restrict__ status) {
+  uint32_t f = c.f, l = c.l;
+  int dl = c.dl, dr = c.dr;
+  f3 mn = c.mn, mx = c.mx;
+  bool leaf = c.leaf;
   for (int depth = 0;; ++depth) {
     if (depth > 128) {
       raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
@@ -419,7 +463,7 @@ __device__ __forceinline__ void hierarchy_tile(
     const bool is_left = dr > dl;
     const uint32_t gamma = is_left ? l : f - 1;
     const uint32_t lg = gamma - g.lb;
-    uint32_t* flag = node_flags + g.ib + lg;
+    uint32_t* flag = flags + g.ib + lg;
     const int dfar = is_left ? dl : dr;
     const uint32_t inc = kArrive | (leaf ? kLeafArrive : 0u) | ((uint32_t)(dfar + 1) << 16);
     const uint32_t old = atomic_add_acquire_gpu(flag, inc);
@@ -480,6 +524,22 @@ __device__ __forceinline__ void hierarchy_tile(
     dl = dL;
     dr = dR;
     leaf = false;
+  }
+}
+
+// One CTA's share of the hierarchy, both phases.
+__device__ __forceinline__ void hierarchy_tile(
+    const float* __restrict__ verts, const uint32_t* __restrict__ leaf_ids, const uint32_t* __restrict__ codes,
+    uint32_t n, const uint32_t* __restrict__ seg_offsets, uint32_t n_seg, const uint32_t* __restrict__ internal_offsets,
+    uint32_t* __restrict__ node_meta, uint32_t* __restrict__ node_leaf_counts, uint32_t* __restrict__ leaf_parent,
+    float* __restrict__ node_bounds, uint32_t* __restrict__ node_flags, float* __restrict__ leaf_tris,
+    uint32_t* __restrict__ roots, uint32_t* __restrict__ status, unsigned char* __restrict__ hier_smem) {
+  SegInfo g;
+  Climb c;
+  if (hierarchy_local(verts, leaf_ids, codes, n, seg_offsets, n_seg, internal_offsets, node_meta, node_leaf_counts,
+                      leaf_parent, node_bounds, node_flags, leaf_tris, roots, status, hier_smem, nullptr, g, c)) {
+    __threadfence();  // the records the CTA wrote, before the release that publishes the subtree
+    climb_global(g, c, node_meta, node_leaf_counts, leaf_parent, node_bounds, node_flags, leaf_tris, status);
   }
 }
 
@@ -708,9 +768,9 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
       const uint32_t k = lb + (parent - ib) - c0;
       float* mine = s_box[k][is_left ? 0 : 1];
       mine[0] = mn.x; mine[1] = mn.y; mine[2] = mn.z; mine[3] = mx.x; mine[4] = mx.y; mine[5] = mx.z;
-      __threadfence_block();
+      fence_acq_rel_cta();
       if (atomicAdd(&s_flag[k], 1u) == 0) return;
-      __threadfence_block();
+      fence_acq_rel_cta();
       const float* sib = s_box[k][is_left ? 1 : 0];
       smn = mk(sib[0], sib[1], sib[2]);
       smx = mk(sib[3], sib[4], sib[5]);
@@ -766,25 +826,28 @@ __global__ void __launch_bounds__(kRefitBlock) refit_kernel(const float* __restr
 //    runs the phases, which meet at grid-wide barriers (bounded waits,
 //    BAJO_STATUS_GRID_TIMEOUT):
 //      A  triangle bounds, root and centroid bounds              -> barrier 1
-//      B  Morton codes (kept in registers), the histogram of the top
-//         kBucketBits code bits, and every LSD pass's digit histogram
-//                                                                 -> barrier 2
+//      B  Morton codes (kept in registers) and the histogram of the top
+//         kBucketBits code bits                                   -> barrier 2
 //    Sort, fast path (every bucket holds at most kBucketMax keys, which
 //    every CTA reads off the same histogram):
 //      S1 each key goes to its bucket's range of a scratch buffer (slot from
 //         a per-bucket atomic counter, so the order inside a bucket is
 //         arbitrary)                                              -> barrier 3
-//      S2 each CTA takes the buckets that start inside its tile, loads them
-//         into shared memory and ranks every key inside its bucket by
-//         (code, item id).  Item ids are unique, so this is exactly the
-//         order of a stable sort by code: the multi-pass LSD sort's output.
-//                                                                 -> barrier 4
-//    Sort, otherwise: LSD radix passes over the 30-bit code (8-bit digits):
-//    each tile ranks its keys (stable, in position order) and scatters them
-//    to base(digit) + counts of the digit in earlier tiles + rank, counting
-//    the next pass's digits per destination tile as it scatters, so a pass
-//    needs one barrier                                            -> barriers 3-6
-//      H  hierarchy_tile (section 3) over the CTA's sorted leaves.
+//      S2 each CTA loads the buckets that cover its tile (and the positions
+//         just before and after it) into shared memory and ranks every key
+//         inside its bucket by (code, item id).  Item ids are unique, so this
+//         is exactly the order of a stable sort by code: the multi-pass LSD
+//         sort's output.  No barrier: the CTA goes on with its own tile.
+//    Sort, otherwise: every pass's digit histogram                -> barrier 3
+//    and LSD radix passes over the 30-bit code (8-bit digits): each tile
+//    ranks its keys (stable, in position order) and scatters them to
+//    base(digit) + counts of the digit in earlier tiles + rank, counting the
+//    next pass's digits per destination tile as it scatters, so a pass needs
+//    one barrier                                                  -> barriers 4-7
+//      H  hierarchy_local (section 3) over the CTA's sorted leaves; the
+//         largest subtrees inside the tile go to the tile's list  -> one barrier
+//      T  build_top: the splits between those subtrees, in shared memory of
+//         one CTA per kTopCap of them (global memory only between CTAs).
 //    Every output array is bit-identical to the per-stage build's.
 // ---------------------------------------------------------------------------
 namespace fused {
@@ -802,13 +865,25 @@ constexpr uint32_t kBucketMax = 256;                 // fast path: no bucket lar
 constexpr uint32_t kLoadMax = kTile + 2 + 2 * kBucketMax;  // keys a CTA ranks on the fast path, at most
 constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
 
+// Top of the hierarchy: every CTA lists the largest subtrees inside its tile
+// (at most kTileTops: a subtree hangs off one of the two paths from the tile's
+// end leaves up to their common ancestor, and every node on such a path has a
+// longer common key prefix than its parent, at most 64 bits), and one CTA
+// per kTopCap of them, in position order, builds the splits between them in
+// shared memory.
+constexpr uint32_t kTileTops = 136;
+constexpr uint32_t kTopCap = 1536;
+
 // Workspace (bytes from the start of the build workspace; word 0 is the
 // status word): barrier counter, ordered segment bounds and the LSD digit
 // histograms (zeroed before the launch); bucket histogram and fill counters
-// (zeroed by phase A); per-(pass, tile) digit counts; two key / item buffers.
+// (zeroed by phase A); per-(pass, tile) digit counts; two key / item buffers;
+// the tiles' subtree lists (first leaf | (delta at it + 1) << 24, and box)
+// and counts; arrival counters of the splits between two CTAs' ranges of the
+// top (zeroed by phase A).
 struct Layout {
   size_t off_bar, off_seg_ord, off_ghist, zero_end, off_bhist, off_bfill, off_counts, off_ka, off_va, off_kb, off_vb,
-      total;
+      off_top_fd, off_top_box, off_top_cnt, off_top_flags, total;
 };
 __host__ __device__ constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 __host__ __device__ constexpr Layout layout(uint32_t n) {
@@ -824,7 +899,12 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
   l.off_va = a256(l.off_ka + (size_t)n * 4);
   l.off_kb = a256(l.off_va + (size_t)n * 4);
   l.off_vb = a256(l.off_kb + (size_t)n * 4);
-  l.total = a256(l.off_vb + (size_t)n * 4);
+  const size_t tiles = (n + kTile - 1) / kTile;
+  l.off_top_fd = a256(l.off_vb + (size_t)n * 4);
+  l.off_top_box = a256(l.off_top_fd + tiles * kTileTops * 4);
+  l.off_top_cnt = a256(l.off_top_box + tiles * kTileTops * 24);
+  l.off_top_flags = a256(l.off_top_cnt + tiles * 4);
+  l.total = a256(l.off_top_flags + (size_t)n * 4);
   return l;
 }
 
@@ -832,10 +912,32 @@ __host__ __device__ constexpr Layout layout(uint32_t n) {
 constexpr size_t kSmemVerts = (size_t)kTile * 9 * 4;                                 // phase A
 constexpr size_t kSmemFast = (size_t)kBuckets * 4 + 80 * 4 + (size_t)kLoadMax * 8;  // fast sort
 constexpr size_t kSmemLsd = (size_t)kWarps * 256 * 4 + 256 * 4 * 5 + (size_t)kPasses * 256 * 4 + 64;
-constexpr size_t kSmemHier = (size_t)kRefitBlock * 72 + 8;                          // phase H
+constexpr size_t kSmemHier = (size_t)kRefitBlock * 72 + 8 + 64;                     // phase H + tile marks
+// phase T (top of the hierarchy): tile starts, then per subtree its first
+// leaf, delta and arrival counter, per split two far ends, deltas and boxes
+struct TopSmem {
+  size_t tstart, first, delta, cnt, far, dfar, box, edge, total;
+};
+__host__ __device__ constexpr TopSmem top_smem() {
+  TopSmem t{};
+  t.tstart = 0;
+  t.first = t.tstart + (kMaxTiles + 1) * 4 + 12;
+  t.delta = t.first + (kTopCap + 1) * 4;
+  t.cnt = (t.delta + kTopCap + 1 + 15) & ~(size_t)15;
+  t.far = t.cnt + kTopCap * 4;
+  t.dfar = t.far + kTopCap * 4;
+  t.box = (t.dfar + kTopCap * 2 + 15) & ~(size_t)15;
+  t.edge = t.box + kTopCap * 48;
+  t.total = t.edge + 2 * 48;
+  return t;
+}
+constexpr size_t kSmemTop = top_smem().total;
 constexpr size_t kSmemMax2 = kSmemFast > kSmemLsd ? kSmemFast : kSmemLsd;
 constexpr size_t kSmemMax3 = kSmemHier > kSmemMax2 ? kSmemHier : kSmemMax2;
-constexpr size_t kSmem = ((kSmemVerts > kSmemMax3 ? kSmemVerts : kSmemMax3) + 15) & ~(size_t)15;
+constexpr size_t kSmemMax4 = kSmemTop > kSmemMax3 ? kSmemTop : kSmemMax3;
+constexpr size_t kSmem = ((kSmemVerts > kSmemMax4 ? kSmemVerts : kSmemMax4) + 15) & ~(size_t)15;
+static_assert(kSmem <= 100 * 1024, "two CTAs per SM");
+static_assert(kTopCap == BAJO_LBVH_TOP_CAP, "header and kernel agree");
 
 // Grid-wide barrier number k (1, 2, ...) of a cooperative launch: every CTA
 // adds one to *bar (released) and waits until all of them have, for at most
@@ -904,10 +1006,260 @@ __device__ __forceinline__ void scan_buckets(uint32_t* s_b, uint32_t* s_tmp, uin
   __syncthreads();
 }
 
+// A subtree whose next split lies outside this CTA's range of the list.
+struct TopEdge {
+  uint32_t a, b;  // list positions (of this CTA's range)
+  int dl, dr;
+  float box[6];
+  uint32_t valid, pad;
+};
+static_assert(sizeof(TopEdge) == 48, "two edges in the shared layout");
+
+// Phase T: the splits between the tiles' largest subtrees, as a bottom-up
+// climb over them with the rules used inside a tile: the split between list
+// positions i and i + 1 lies at the last leaf of subtree i, its delta is the
+// one at subtree i + 1's first leaf, and slot i of shared memory is where the
+// two meet.  A climb step touches shared memory only; the parents' records
+// are written after the climbs, in one pass.
+//
+// When the list holds at most cap subtrees (the usual case: about 9 per
+// tile of random triangles), EVERY CTA climbs the whole list in its own
+// shared memory (the same tree each time) and writes its share of the
+// records, so no CTA waits on another and the writes are spread over all
+// SMs.  Otherwise the list is cut into ceil(total / cap) equal ranges, one
+// per CTA (at most one per CTA: a cap below kTile is only for tests), and
+// the splits between ranges meet in global memory (climb_global, arrival
+// counters in top_flags).
+__device__ __forceinline__ void build_top(uint32_t n, const BajoLbvh& t, const uint32_t* __restrict__ top_fd,
+                                          const float2* __restrict__ top_box, const uint32_t* __restrict__ top_cnt,
+                                          uint32_t* __restrict__ top_flags, uint32_t cap,
+                                          unsigned char* __restrict__ smem, uint32_t* __restrict__ status) {
+  constexpr TopSmem ly = top_smem();
+  constexpr uint32_t kNone = 0xFFFFFFFFu;
+  uint32_t* s_ts = reinterpret_cast<uint32_t*>(smem + ly.tstart);  // [tiles + 1] list start of every tile
+  uint32_t* s_first = reinterpret_cast<uint32_t*>(smem + ly.first);  // [m + 1] first leaf
+  int8_t* s_delta = reinterpret_cast<int8_t*>(smem + ly.delta);      // [m + 1] delta at the first leaf
+  uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + ly.cnt);      // [m - 1] arrivals + (first side << 8)
+  uint16_t(*s_far)[2] = reinterpret_cast<uint16_t(*)[2]>(smem + ly.far);   // [m - 1] far ends (list positions)
+  int8_t(*s_dfar)[2] = reinterpret_cast<int8_t(*)[2]>(smem + ly.dfar);     // [m - 1] deltas at them
+  float(*s_box)[2][6] = reinterpret_cast<float(*)[2][6]>(smem + ly.box);  // [m - 1] children's boxes
+  TopEdge* s_edge = reinterpret_cast<TopEdge*>(smem + ly.edge);            // [0] left end, [1] right end
+  const uint32_t tid = threadIdx.x, nt = gridDim.x;
+  const SegInfo g{0, n, 0};
+
+  const uint32_t v = tid < nt ? __ldcg(top_cnt + tid) : 0u;
+  const uint32_t ex = onesweep::scan256_exclusive<kThreads>(v, s_cnt);
+  if (tid < nt) s_ts[tid] = ex;
+  if (tid + 1 == nt) s_ts[nt] = ex + v;
+  if (tid < 2) s_edge[tid].valid = 0u;
+  __syncthreads();
+  const uint32_t total = s_ts[nt];
+  if (total < 2) return;  // the whole tree is inside one tile
+  const uint32_t nr = min((total + cap - 1) / cap, nt);  // ranges (cap >= kTile never needs the clamp)
+  if (nr > 1 && blockIdx.x >= nr) return;
+  const uint32_t j0 = nr == 1 ? 0u : (uint32_t)((uint64_t)blockIdx.x * total / nr);
+  const uint32_t m = (nr == 1 ? total : (uint32_t)((uint64_t)(blockIdx.x + 1) * total / nr)) - j0;
+  auto entry = [&](uint32_t j) {  // list position -> slot of its tile's list
+    uint32_t a = 0, z = nt + 1;   // first tile q with s_ts[q] > j
+    while (a < z) {
+      const uint32_t mid = (a + z) >> 1;
+      if (s_ts[mid] > j) z = mid;
+      else a = mid + 1;
+    }
+    return (a - 1u) * kTileTops + (j - s_ts[a - 1u]);
+  };
+
+  // every subtree of the range: its first leaf, the delta there and its box
+  // (kTopCap <= 3 * kThreads: three per thread, every load in flight at once)
+  static_assert(kTopCap <= 3 * kThreads, "three subtrees per thread");
+  uint32_t fd[3];
+  float2 bx[3][3];
+  const bool has_after = j0 + m < total;  // the subtree after the range
+  const uint32_t fd_after = (tid == 0 && has_after) ? __ldcg(top_fd + entry(j0 + m)) : 0u;
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const uint32_t i = tid + r * kThreads;
+    fd[r] = 0u;
+    bx[r][0] = bx[r][1] = bx[r][2] = make_float2(0.0f, 0.0f);
+    if (i < m) {
+      const uint32_t at = entry(j0 + i);
+      fd[r] = __ldcg(top_fd + at);
+      bx[r][0] = __ldcg(top_box + (size_t)at * 3 + 0);
+      bx[r][1] = __ldcg(top_box + (size_t)at * 3 + 1);
+      bx[r][2] = __ldcg(top_box + (size_t)at * 3 + 2);
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const uint32_t i = tid + r * kThreads;
+    if (i < m) {
+      s_first[i] = fd[r] & 0xFFFFFFu;
+      s_delta[i] = (int8_t)((int)(fd[r] >> 24) - 1);
+      s_cnt[i] = 0u;
+    }
+  }
+  if (tid == 0) {
+    s_first[m] = has_after ? (fd_after & 0xFFFFFFu) : n;
+    s_delta[m] = has_after ? (int8_t)((int)(fd_after >> 24) - 1) : (int8_t)-1;
+  }
+  __syncthreads();
+  // each box, far end and far delta into the split where the subtree
+  // arrives (or into an edge slot); then the arrival itself
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const uint32_t i = tid + r * kThreads;
+    if (i < m) {
+      const int dl = s_delta[i], dr = s_delta[i + 1];
+      const bool is_left = dr > dl;
+      float* dst;
+      if (is_left ? i + 1 >= m : i == 0) {
+        TopEdge& e = s_edge[is_left ? 1 : 0];
+        e.a = i;
+        e.b = i;
+        e.dl = dl;
+        e.dr = dr;
+        e.valid = 1u;
+        dst = e.box;
+      } else {
+        const uint32_t slot = is_left ? i : i - 1, side = is_left ? 0u : 1u;
+        s_far[slot][side] = (uint16_t)i;
+        s_dfar[slot][side] = (int8_t)(is_left ? dl : dr);
+        dst = s_box[slot][side];
+      }
+      dst[0] = bx[r][0].x;
+      dst[1] = bx[r][0].y;
+      dst[2] = bx[r][1].x;
+      dst[3] = bx[r][1].y;
+      dst[4] = bx[r][2].x;
+      dst[5] = bx[r][2].y;
+    }
+  }
+  __syncthreads();
+  uint32_t cur[3];  // per subtree of this thread: the split where it arrived second, or kNone
+#pragma unroll
+  for (int r = 0; r < 3; ++r) {
+    const uint32_t i = tid + r * kThreads;
+    cur[r] = kNone;
+    if (i < m) {
+      const bool is_left = s_delta[i + 1] > s_delta[i];
+      if (!(is_left ? i + 1 >= m : i == 0)) {
+        const uint32_t slot = is_left ? i : i - 1;
+        if (atomicAdd(&s_cnt[slot], 1u + ((is_left ? 0u : 1u) << 8)) != 0u) cur[r] = slot;
+      }
+    }
+  }
+  // One step: the second arrival at split q has both children in the slot;
+  // their union climbs to the next split (or ends at the root or an edge).
+  auto step = [&](uint32_t q) -> uint32_t {
+    fence_acq_rel_cta();  // after the arrival: the first one's writes
+    const uint32_t fa = *reinterpret_cast<const uint32_t*>(s_far[q]);
+    const uint32_t a = fa & 0xFFFFu, b = fa >> 16;
+    const int dl = s_dfar[q][0], dr = s_dfar[q][1];
+    if (nr == 1 && a == 0u && b + 1 == m) return kNone;  // the root
+    const float4* bq = reinterpret_cast<const float4*>(s_box[q]);
+    const float4 x0 = bq[0], x1 = bq[1], x2 = bq[2];
+    const f3 mn = vmin(mk(x0.x, x0.y, x0.z), mk(x1.z, x1.w, x2.x));
+    const f3 mx = vmax(mk(x0.w, x1.x, x1.y), mk(x2.y, x2.z, x2.w));
+    const bool is_left = dr > dl;
+    float* dst;
+    if (is_left ? b + 1 >= m : a == 0u) {  // the next split is outside this range
+      TopEdge& e = s_edge[is_left ? 1 : 0];
+      e.a = a;
+      e.b = b;
+      e.dl = dl;
+      e.dr = dr;
+      e.valid = 1u;
+      dst = e.box;
+    } else {
+      const uint32_t q2 = is_left ? b : a - 1u, side = is_left ? 0u : 1u;
+      dst = s_box[q2][side];
+      s_far[q2][side] = (uint16_t)(is_left ? a : b);
+      s_dfar[q2][side] = (int8_t)(is_left ? dl : dr);
+      float2* d2 = reinterpret_cast<float2*>(dst);
+      d2[0] = make_float2(mn.x, mn.y);
+      d2[1] = make_float2(mn.z, mx.x);
+      d2[2] = make_float2(mx.y, mx.z);
+      fence_acq_rel_cta();
+      return atomicAdd(&s_cnt[q2], 1u + (side << 8)) != 0u ? q2 : kNone;
+    }
+    dst[0] = mn.x; dst[1] = mn.y; dst[2] = mn.z; dst[3] = mx.x; dst[4] = mx.y; dst[5] = mx.z;
+    return kNone;
+  };
+  // the climbs: one step per round for every thread (its first climb still
+  // going), so the lanes of a warp take their steps together
+  for (int round = 0;; ++round) {
+    const uint32_t q = cur[0] != kNone ? cur[0] : (cur[1] != kNone ? cur[1] : cur[2]);
+    if (q == kNone) break;
+    if (round > 3 * 160) {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      break;
+    }
+    const uint32_t nq = step(q);
+    if (cur[0] != kNone) cur[0] = nq;
+    else if (cur[1] != kNone) cur[1] = nq;
+    else cur[2] = nq;
+  }
+  __syncthreads();
+
+  // the records of the parents built here; with one range, every CTA writes
+  // its share of them
+  const uint32_t ns = m - 1;
+  const uint32_t q0 = nr == 1 ? (uint32_t)((uint64_t)blockIdx.x * ns / nt) : 0u;
+  const uint32_t q1 = nr == 1 ? (uint32_t)((uint64_t)(blockIdx.x + 1) * ns / nt) : ns;
+  for (uint32_t q = q0 + tid; q < q1; q += kThreads)
+    if ((s_cnt[q] & 0xFFu) == 2u)
+      write_slot_parent(g, s_first[q + 1] - 1u, s_first[s_far[q][0]], s_first[s_far[q][1] + 1] - 1u, s_dfar[q][0],
+                        s_dfar[q][1], s_box[q][0], s_box[q][1], t.node_meta, t.node_leaf_counts, t.leaf_parent,
+                        t.node_bounds, nullptr);
+  if (nr == 1) return;  // the root is built
+  __syncthreads();
+  __threadfence();  // the records this CTA wrote, before any release below
+
+  // the subtrees whose sibling lies (partly) in another range climb on in
+  // global memory: first arrivals whose split saw no second one, and the edges
+  for (uint32_t q = tid; q < m + 1; q += kThreads) {
+    Climb c;
+    const float* o;
+    uint32_t a, b;
+    if (q + 1 < m) {
+      const uint32_t cv = s_cnt[q];
+      if ((cv & 0xFFu) != 1u) continue;
+      const uint32_t side = cv >> 8;
+      o = s_box[q][side];
+      if (side == 0u) {
+        a = s_far[q][0];
+        b = q;
+        c.dl = s_dfar[q][0];
+        c.dr = s_delta[q + 1];
+      } else {
+        a = q + 1;
+        b = s_far[q][1];
+        c.dl = s_delta[q + 1];
+        c.dr = s_dfar[q][1];
+      }
+    } else {
+      const TopEdge& e = s_edge[q + 1 - m];
+      if (!e.valid) continue;
+      o = e.box;
+      a = e.a;
+      b = e.b;
+      c.dl = e.dl;
+      c.dr = e.dr;
+    }
+    c.f = s_first[a];
+    c.l = s_first[b + 1] - 1u;
+    c.mn = mk(o[0], o[1], o[2]);
+    c.mx = mk(o[3], o[4], o[5]);
+    c.leaf = c.f == c.l;
+    climb_global(g, c, t.node_meta, t.node_leaf_counts, t.leaf_parent, t.node_bounds, top_flags, t.leaf_tris,
+                 status);
+  }
+}
+
 template <bool VEC>
 __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __restrict__ verts, uint32_t n,
                                                                  BajoLbvh t, unsigned char* __restrict__ ws,
-                                                                 uint32_t* __restrict__ status) {
+                                                                 uint32_t top_cap, uint32_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t s_red[kWarps][12];
   __shared__ uint32_t s_flag;
@@ -946,9 +1298,14 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
     } else {
       for (uint32_t q = tid; q < nf; q += kThreads) s_v[q] = __ldg(src + q);
     }
-    // arrival counters of the hierarchy's crossing splits start at zero; the
-    // next passes' digit counts of this tile are accumulated by atomics
-    for (uint32_t q = base + tid; q < min(base + kTile, n - 1); q += kThreads) t.node_flags[q] = 0u;
+    // node_flags end at 2 for every internal node (the per-stage build's
+    // arrival counters); the top's arrival counters start at zero; the next
+    // passes' digit counts of this tile are accumulated by atomics
+    uint32_t* top_flags = reinterpret_cast<uint32_t*>(ws + L.off_top_flags);
+    for (uint32_t q = base + tid; q < min(base + kTile, n - 1); q += kThreads) {
+      t.node_flags[q] = 2u;
+      top_flags[q] = 0u;
+    }
     for (uint32_t q = tid; q < (kPasses - 1) * 256; q += kThreads)
       counts[((q >> 8) + 1) * kMaxTiles * 256 + c * 256 + (q & 255)] = 0u;
     for (uint32_t q = c * kThreads + tid; q < 2 * kBuckets; q += gridDim.x * kThreads) bhist[q] = 0u;  // + bfill
@@ -1221,10 +1578,43 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
   // records over this CTA's kTile sorted leaves (section 3).  After the fast
   // path the tile's sorted keys are this CTA's own writes and the two
   // boundary codes are in s_bound; after the passes a barrier has ended them.
+  uint32_t* s_mark = reinterpret_cast<uint32_t*>(smem + (size_t)kRefitBlock * 72 + 8);  // starts of the tops
+  if (tid < kWarps) s_mark[tid] = 0u;
   __syncthreads();
-  hierarchy_tile(verts, t.leaf_ids, t.morton_codes, n, t.seg_offsets, 1, t.internal_offsets, t.node_meta,
-                 t.node_leaf_counts, t.leaf_parent, t.node_bounds, t.node_flags, t.leaf_tris, t.roots, status, smem,
-                 sorted ? s_bound : nullptr);
+  SegInfo g;
+  Climb top;
+  const bool is_top =
+      hierarchy_local(verts, t.leaf_ids, t.morton_codes, n, t.seg_offsets, 1, t.internal_offsets, t.node_meta,
+                      t.node_leaf_counts, t.leaf_parent, t.node_bounds, nullptr, t.leaf_tris, t.roots, status,
+                      smem, sorted ? s_bound : nullptr, g, top);
+  // this tile's largest subtrees go to its list, in position order
+  uint32_t* top_fd = reinterpret_cast<uint32_t*>(ws + L.off_top_fd);
+  float2* top_box = reinterpret_cast<float2*>(ws + L.off_top_box);
+  uint32_t* top_cnt = reinterpret_cast<uint32_t*>(ws + L.off_top_cnt);
+  if (is_top) atomicOr(&s_mark[(top.f - base) >> 5], 1u << ((top.f - base) & 31));
+  __syncthreads();
+  if (is_top) {
+    const uint32_t p = top.f - base, w = p >> 5;
+    uint32_t e = __popc(s_mark[w] & ((1u << (p & 31)) - 1u));
+    for (uint32_t q = 0; q < w; ++q) e += __popc(s_mark[q]);
+    if (e < kTileTops) {
+      const size_t at = (size_t)c * kTileTops + e;
+      top_fd[at] = top.f | ((uint32_t)(top.dl + 1) << 24);
+      top_box[at * 3 + 0] = make_float2(top.mn.x, top.mn.y);
+      top_box[at * 3 + 1] = make_float2(top.mn.z, top.mx.x);
+      top_box[at * 3 + 2] = make_float2(top.mx.y, top.mx.z);
+    } else {
+      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+    }
+  }
+  if (tid == 0) {
+    uint32_t e = 0;
+    for (int q = 0; q < kWarps; ++q) e += __popc(s_mark[q]);
+    top_cnt[c] = min(e, kTileTops);
+  }
+  if (!grid_sync(bar, ++nbar, status, &s_flag)) return;
+  build_top(n, t, top_fd, top_box, top_cnt, reinterpret_cast<uint32_t*>(ws + L.off_top_flags), top_cap, smem,
+            status);
 }
 
 
@@ -1236,6 +1626,7 @@ struct DeviceState {
 };
 DeviceState g_fused_state[64];
 std::atomic<uint32_t> g_fused_max_leaves{kMaxLeaves};
+std::atomic<uint32_t> g_top_cap{kTopCap};
 
 bool can_run(uint32_t n, uint32_t n_seg) {
   return n_seg == 1 && n >= 2 && n <= g_fused_max_leaves.load(std::memory_order_relaxed) && n <= kMaxLeaves;
@@ -1285,7 +1676,8 @@ cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws,
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   BajoLbvh tcopy = *bvh;
-  e = cudaLaunchKernelEx(&cfg, kern, d_verts, n, tcopy, ws, status);
+  const uint32_t cap = g_top_cap.load(std::memory_order_relaxed);
+  e = cudaLaunchKernelEx(&cfg, kern, d_verts, n, tcopy, ws, cap, status);
   if (e == cudaSuccess) *launched = true;
   return e;
 }
@@ -1486,6 +1878,9 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
                 !bvh->node_leaf_counts || !bvh->node_flags || !bvh->leaf_parent || !bvh->roots || !bvh->leaf_tris))
     return BAJO_ERR_INVALID_ARGUMENT;
   if (bvh->top_nodes && ((uintptr_t)bvh->top_nodes & 15)) return BAJO_ERR_INVALID_ARGUMENT;
+  if (n > 0 && (((uintptr_t)bvh->node_bounds & 15) || ((uintptr_t)bvh->node_meta & 15) ||
+                ((uintptr_t)bvh->leaf_tris & 15)))
+    return BAJO_ERR_INVALID_ARGUMENT;  // their records are read and written 16 bytes at a time
   BuildPlan plan = make_build_plan(n, S);
   const size_t need = hploc ? hploc_extra_offset(n, S) + hploc_workspace_bytes(n, S) : plan.total;
   if (ws_bytes < need) return BAJO_ERR_WORKSPACE_TOO_SMALL;
@@ -1616,6 +2011,12 @@ int32_t bajo_lbvh_stage_top(const BajoLbvh* bvh, void* stream) {
 int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves) {
   if (max_leaves > bajo::fused::kMaxLeaves) return BAJO_ERR_TOO_LARGE;
   bajo::fused::g_fused_max_leaves.store(max_leaves, std::memory_order_relaxed);
+  return BAJO_OK;
+}
+
+int32_t bajo_lbvh_fused_top_cap_set(uint32_t cap) {
+  if (cap > bajo::fused::kTopCap) return BAJO_ERR_TOO_LARGE;
+  bajo::fused::g_top_cap.store(cap ? cap : bajo::fused::kTopCap, std::memory_order_relaxed);
   return BAJO_OK;
 }
 

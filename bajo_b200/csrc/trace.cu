@@ -198,7 +198,8 @@ __global__ void __launch_bounds__(kTraceBlock) batch_trace_kernel(
 
 bool bvh_ok(const BajoLbvh* b) {
   return b && b->roots && b->node_bounds && b->node_meta && b->leaf_tris && b->n_segments >= 1 &&
-         !((uintptr_t)b->top_nodes & 15);
+         !((uintptr_t)b->top_nodes & 15) && !((uintptr_t)b->node_bounds & 15) && !((uintptr_t)b->node_meta & 15) &&
+         !((uintptr_t)b->leaf_tris & 15);  // records read 16 bytes at a time
 }
 
 // Grid of a TOP kernel: every resident block slot once, at most one ray per

@@ -132,6 +132,9 @@ typedef struct BajoLbvh {
   uint32_t* morton_codes;      /* N     low 32 bits of sort_keys                          */
   uint32_t* node_meta;         /* 4*M   [parent, left, right, fence], tagged child refs   */
   float* node_bounds;          /* 12*M  left-child AABB then right-child AABB             */
+                               /* node_meta, node_bounds and leaf_tris are read and       */
+                               /* written 16 bytes at a time: 16-byte aligned (the build  */
+                               /* and the traversals refuse others)                       */
   uint32_t* node_leaf_counts;  /* M     leaves under each internal node                   */
   uint32_t* node_flags;        /* M     refit arrival counters (2 after a build)          */
   uint32_t* leaf_parent;       /* N     parent internal node of each sorted leaf          */
@@ -184,6 +187,14 @@ int32_t bajo_lbvh_build(const float* d_verts, BajoLbvh* bvh, void* d_workspace, 
  * default); 0 sends every build through the per-stage kernels.  Process wide,
  * like the sort tuning table: set it before building, not concurrently. */
 int32_t bajo_lbvh_fused_max_set(uint32_t max_leaves);
+/* The one-launch build ends with the splits between the tiles' largest
+ * subtrees, built in shared memory by one CTA per `cap` of those subtrees
+ * (default and maximum BAJO_LBVH_TOP_CAP = 1536; 0 restores it); splits
+ * between two CTAs' ranges meet in global memory.  A smaller cap only moves
+ * work into global memory (the tree is the same): tests use it to exercise
+ * those splits.  Process wide; set it before building. */
+#define BAJO_LBVH_TOP_CAP 1536u
+int32_t bajo_lbvh_fused_top_cap_set(uint32_t cap);
 /* Kernel launches bajo_lbvh_build makes for n_tris triangles in n_segments
  * segments on the current device (1 for the one-launch build). */
 int32_t bajo_lbvh_build_launches(uint32_t n_tris, uint32_t n_segments, int32_t* launches);

@@ -76,6 +76,55 @@ def test_fused_hard_inputs(oracle, kind, n):
     assert_same_build(f, oracle.lbvh_build(v))
 
 
+@pytest.mark.parametrize("cap", [1, 2, 3, 64, 700])
+@pytest.mark.parametrize("kind,n", [("random", 513), ("random", 2049), ("random", 65536), ("duplicates", 65536),
+                                    ("outlier", 100_003), ("random", 131072)])
+def test_fused_top_ranges(oracle, cap, kind, n):
+    """The top of the tree over the tiles' largest subtrees, cut into ranges
+    of at most `cap` subtrees per CTA: the splits between ranges meet in
+    global memory, and the arrays stay identical to the per-stage build's."""
+    from bajo_b200 import _lib
+    L = _lib.load()
+    v = _scene(kind, n, seed=n + cap)
+    assert L.bajo_lbvh_fused_top_cap_set(cap) == _lib.OK
+    try:
+        f = _build(v, True)
+    finally:
+        assert L.bajo_lbvh_fused_top_cap_set(0) == _lib.OK
+    s = _build(v, False)
+    for a, b in zip(_arrays(f, n), _arrays(s, n)):
+        assert np.array_equal(a, b)
+    if n == 65536 and cap == 64:
+        assert_same_build(f, oracle.lbvh_build(v))
+
+
+def test_fused_top_cap_limits():
+    from bajo_b200 import _lib
+    L = _lib.load()
+    assert L.bajo_lbvh_fused_top_cap_set(_lib.LBVH_TOP_CAP + 1) == _lib.ERR_TOO_LARGE
+    assert L.bajo_lbvh_fused_top_cap_set(_lib.LBVH_TOP_CAP) == _lib.OK
+    assert L.bajo_lbvh_fused_top_cap_set(0) == _lib.OK
+
+
+@pytest.mark.parametrize("fn", ["bajo_lbvh_build", "bajo_hploc_build"])
+@pytest.mark.parametrize("field", ["node_bounds", "node_meta", "leaf_tris"])
+def test_build_rejects_unaligned_records(fn, field):
+    """Node boxes and triangle records are read and written 16 bytes at a
+    time: a record array that is not 16-byte aligned is refused up front."""
+    from bajo_b200 import _lib, bvh
+    L = _lib.load()
+    n = 1000
+    d = torch.from_numpy(scenes.random_triangles(n, seed=3)).cuda()
+    ws = bvh.GpuBvhBuildWorkspace(n, 1)
+    t = bvh.build_triangle_bvh(d, workspace=ws)
+    c = t.c_struct(stage_top=False)
+    setattr(c, field, getattr(t, field).data_ptr() + 4)
+    s = torch.cuda.current_stream().cuda_stream
+    assert getattr(L, fn)(d.data_ptr(), ctypes.byref(c), ws.buffer.data_ptr(), ws.buffer.numel(),
+                          s) == _lib.ERR_INVALID_ARGUMENT
+    torch.cuda.synchronize()
+
+
 def test_fused_rebuilds_reuse_workspace(oracle):
     """Repeated builds through one workspace (the barrier counter and
     histograms are cleared per build) and interleaved sizes."""
