@@ -3,6 +3,8 @@
 // bajo/bvh/gpu/builder/lbvh.mojo (GPU driver) and binary_layout.mojo with the
 // reference's buffer layouts; see include/bajo_b200.h for the boundary.
 #include <atomic>
+#include <chrono>
+#include <mutex>
 
 #include "onesweep.cuh"
 
@@ -875,24 +877,26 @@ constexpr uint32_t kTileTops = 136;
 constexpr uint32_t kTopCap = 1536;
 
 // Workspace (bytes from the start of the build workspace; word 0 is the
-// status word): barrier counter, ordered segment bounds and the LSD digit
-// histograms (zeroed before the launch); bucket histogram and fill counters
-// (zeroed by phase A); per-(pass, tile) digit counts; two key / item buffers;
-// the tiles' subtree lists (first leaf | (delta at it + 1) << 24, and box)
-// and counts; arrival counters of the splits between two CTAs' ranges of the
-// top (zeroed by phase A).
+// status word): the launch's epoch flag, the barrier counter and the
+// ordered root and centroid bounds (CTA 0 clears the last two, then stores
+// the epoch, which every CTA waits for before it first touches them, so no
+// clearing launch precedes the build); the LSD digit histograms, bucket
+// histogram and fill counters (zeroed by phase A); per-(pass, tile) digit
+// counts; two key / item buffers; the tiles' subtree lists (first leaf |
+// (delta at it + 1) << 24, and box) and counts; arrival counters of the
+// splits between two CTAs' ranges of the top (zeroed by phase A).
 struct Layout {
-  size_t off_bar, off_seg_ord, off_ghist, zero_end, off_bhist, off_bfill, off_counts, off_ka, off_va, off_kb, off_vb,
+  size_t off_epoch, off_bar, off_seg_ord, off_ghist, off_bhist, off_bfill, off_counts, off_ka, off_va, off_kb, off_vb,
       off_top_fd, off_top_box, off_top_cnt, off_top_flags, total;
 };
 __host__ __device__ constexpr size_t a256(size_t x) { return (x + 255) & ~(size_t)255; }
 __host__ __device__ constexpr Layout layout(uint32_t n) {
   Layout l{};
-  l.off_bar = 256;
-  l.off_seg_ord = 320;
-  l.off_ghist = 384;
-  l.zero_end = l.off_ghist + (size_t)kPasses * 256 * 4;
-  l.off_bhist = a256(l.zero_end);
+  l.off_epoch = 256;
+  l.off_bar = 384;
+  l.off_seg_ord = 512;
+  l.off_ghist = 768;
+  l.off_bhist = a256(l.off_ghist + (size_t)kPasses * 256 * 4);
   l.off_bfill = l.off_bhist + (size_t)kBuckets * 4;
   l.off_counts = a256(l.off_bfill + (size_t)kBuckets * 4);
   l.off_ka = a256(l.off_counts + (size_t)kPasses * kMaxTiles * 256 * 4);
@@ -965,6 +969,20 @@ __device__ __forceinline__ bool grid_sync(uint32_t* bar, uint32_t k, uint32_t* s
   }
   __syncthreads();
   return *s_flag != 0;
+}
+
+// Waits (one thread, at most kWaitNs) until CTA 0 has published this
+// launch's epoch; false, with the status bit raised, when it never came.
+__device__ __forceinline__ bool wait_epoch(const uint32_t* flag, uint32_t epoch, uint32_t* status) {
+  if (ld_acquire_gpu(flag) == epoch) return true;
+  const uint64_t t0 = global_timer_ns();
+  while (ld_acquire_gpu(flag) != epoch) {
+    if (global_timer_ns() - t0 > kWaitNs) {
+      raise_status(status, BAJO_STATUS_GRID_TIMEOUT);
+      return false;
+    }
+  }
+  return true;
 }
 
 // Exclusive scan over kBuckets entries in shared memory (in place), kThreads
@@ -1259,13 +1277,15 @@ __device__ __forceinline__ void build_top(uint32_t n, const BajoLbvh& t, const u
 template <bool VEC>
 __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __restrict__ verts, uint32_t n,
                                                                  BajoLbvh t, unsigned char* __restrict__ ws,
-                                                                 uint32_t top_cap, uint32_t* __restrict__ status) {
+                                                                 uint32_t top_cap, uint32_t epoch,
+                                                                 uint32_t* __restrict__ status) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ uint32_t s_red[kWarps][12];
   __shared__ uint32_t s_flag;
   __shared__ uint32_t s_bound[2];  // sorted codes at positions base - 1 and base + kTile
   constexpr Layout kL0 = layout(0);
   const Layout L = layout(n);
+  uint32_t* epoch_flag = reinterpret_cast<uint32_t*>(ws + kL0.off_epoch);
   uint32_t* bar = reinterpret_cast<uint32_t*>(ws + kL0.off_bar);
   uint32_t* seg_ord = reinterpret_cast<uint32_t*>(ws + kL0.off_seg_ord);
   uint32_t* ghist = reinterpret_cast<uint32_t*>(ws + kL0.off_ghist);
@@ -1309,11 +1329,18 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
     for (uint32_t q = tid; q < (kPasses - 1) * 256; q += kThreads)
       counts[((q >> 8) + 1) * kMaxTiles * 256 + c * 256 + (q & 255)] = 0u;
     for (uint32_t q = c * kThreads + tid; q < 2 * kBuckets; q += gridDim.x * kThreads) bhist[q] = 0u;  // + bfill
+    for (uint32_t q = c * kThreads + tid; q < kPasses * 256; q += gridDim.x * kThreads) ghist[q] = 0u;
     if (c == 0 && tid == 0) {
       t.internal_offsets[0] = 0;
       t.internal_offsets[1] = n - 1;
     }
+    if (c == 0 && tid < 13) (tid == 0 ? bar : seg_ord + tid - 1)[0] = 0u;  // the counter, the 12 bounds
+    if (tid == 0) s_flag = 1u;
     __syncthreads();
+    if (c == 0 && tid == 0) {  // the counter and the bounds are clear: this launch's epoch
+      __threadfence();
+      st_relaxed_gpu(epoch_flag, epoch);
+    }
   }
   float cx[kKpt], cy[kKpt], cz[kKpt];
   {
@@ -1349,6 +1376,9 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
       if (lane == 0) s_red[warp][q] = r;
     }
     __syncthreads();
+    if (tid == 0 && !wait_epoch(epoch_flag, epoch, status)) s_flag = 0u;
+    __syncthreads();  // the counter and the bounds are cleared for this launch
+    if (s_flag == 0u) return;  // (waited in vain: the status says so)
     if (tid < 12) {
       uint32_t r = 0;
 #pragma unroll
@@ -1470,7 +1500,7 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
     uint32_t* s_tmp = s_pre + 512;                                 // scan scratch
     const uint32_t d_own = tid & 255u, half = tid >> 8;
     {
-      // every pass's digit histogram (ghist was zeroed before the launch)
+      // every pass's digit histogram (ghist was zeroed by phase A)
       // and this tile's digit counts of pass 0
       uint32_t* s_hist = s_wh;  // [kPasses][256]
       for (uint32_t q = tid; q < kPasses * 256; q += kThreads) s_hist[q] = 0;
@@ -1628,6 +1658,21 @@ DeviceState g_fused_state[64];
 std::atomic<uint32_t> g_fused_max_leaves{kMaxLeaves};
 std::atomic<uint32_t> g_top_cap{kTopCap};
 
+// Launch epochs: unique per launch in this process, never 0, and started at
+// a value drawn from the clock so that a workspace left by another process
+// is unlikely to hold the epochs this one uses.
+std::atomic<uint32_t> g_epoch{0};
+std::once_flag g_epoch_once;
+uint32_t next_epoch() {
+  std::call_once(g_epoch_once, [] {
+    const uint64_t t = (uint64_t)std::chrono::steady_clock::now().time_since_epoch().count();
+    g_epoch.store((uint32_t)(t ^ (t >> 32)) | 1u);
+  });
+  uint32_t e = g_epoch.fetch_add(1u, std::memory_order_relaxed);
+  if (e == 0u) e = g_epoch.fetch_add(1u, std::memory_order_relaxed);
+  return e;
+}
+
 bool can_run(uint32_t n, uint32_t n_seg) {
   return n_seg == 1 && n >= 2 && n <= g_fused_max_leaves.load(std::memory_order_relaxed) && n <= kMaxLeaves;
 }
@@ -1663,8 +1708,6 @@ cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws,
     ds.ready = true;
   }
   if ((int)G > ds.max_ctas) return cudaSuccess;
-  constexpr Layout kL0 = layout(0);
-  if ((e = cudaMemsetAsync(ws + kL0.off_bar, 0, kL0.zero_end - kL0.off_bar, st)) != cudaSuccess) return e;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(G);
   cfg.blockDim = dim3(kThreads);
@@ -1677,7 +1720,8 @@ cudaError_t launch(const float* d_verts, const BajoLbvh* bvh, unsigned char* ws,
   cfg.numAttrs = 1;
   BajoLbvh tcopy = *bvh;
   const uint32_t cap = g_top_cap.load(std::memory_order_relaxed);
-  e = cudaLaunchKernelEx(&cfg, kern, d_verts, n, tcopy, ws, cap, status);
+  const uint32_t epoch = next_epoch();
+  e = cudaLaunchKernelEx(&cfg, kern, d_verts, n, tcopy, ws, cap, epoch, status);
   if (e == cudaSuccess) *launched = true;
   return e;
 }
