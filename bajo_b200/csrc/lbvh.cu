@@ -1933,7 +1933,8 @@ static int32_t lbvh_build_impl(const float* d_verts, BajoLbvh* bvh, void* ws_, s
   uint32_t* status = (uint32_t*)ws;
   // one scene of up to fused::kMaxLeaves triangles: the one-launch build;
   // its stage events are [start, build]
-  if (!hploc && fused::can_run(n, S) && (!ev || n_ev == 2)) {
+  // (the one-launch build keeps 8- and 16-byte records in the workspace)
+  if (!hploc && fused::can_run(n, S) && ((uintptr_t)ws & 15) == 0 && (!ev || n_ev == 2)) {
     if (ev && cudaEventRecord(ev[0], st) != cudaSuccess) return BAJO_ERR_CUDA;
     bool launched = false;
     if (fused::launch(d_verts, bvh, ws, status, st, &launched) != cudaSuccess) return BAJO_ERR_CUDA;
