@@ -235,7 +235,8 @@ def tune_all(reps: int = 5, save_cache: bool = True, parts=PARTS) -> dict:
         u64 = tune_sort(8, True, range(10, 19), end_bit=30, reps=reps)
         u64.update(tune_sort(8, True, range(19, 27), end_bit=44, reps=reps))
         res[_kernel_key(8, True)] = u64
-        res[_kernel_key(4, True)] = tune_sort(4, True, range(10, 27), reps=reps)
+        res[_kernel_key(4, True)] = tune_sort(4, True, range(10, 29), reps=reps)
+        res[_kernel_key(4, False)] = tune_sort(4, False, range(10, 29), reps=reps)
     if "trace" in parts:
         res["trace_camera"] = tune_trace("trace_camera", range(16, 23, 2), reps=reps)
         res["trace_rays"] = tune_trace("trace_rays", range(16, 23, 2), reps=reps)

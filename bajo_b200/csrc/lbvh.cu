@@ -1545,7 +1545,7 @@ __global__ void __launch_bounds__(kThreads, 2) lbvh_fused_kernel(const float* __
 #pragma unroll
       for (int k = 0; k < kKpt; ++k) {
         const uint32_t d = (key[k] >> sh) & 255u;
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+        const uint32_t peers = onesweep::match_label<8>(d);
         const uint32_t leader = __ffs(peers) - 1;
         uint32_t before = 0;
         if (lane == leader) before = atomicAdd(&wh[d], (uint32_t)__popc(peers));

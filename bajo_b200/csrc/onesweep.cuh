@@ -7,8 +7,9 @@
 //  - keys are staged in shared memory with their own type, so 64-bit keys are
 //    sorted correctly (the reference stages them through UInt32 shared memory,
 //    onesweep.mojo:244,311,321, which truncates 64-bit keys);
-//  - digit ranking uses __match_any_sync on the digit (one instruction)
-//    instead of 8 ballots per key (bajo/sort/gpu/utils.mojo:46-103);
+//  - digit ranking finds a key's peers with one ballot per digit bit, like
+//    the reference (bajo/sort/gpu/utils.mojo:46-103); the match instruction
+//    it replaces was measured twice as slow per pass on B200;
 //  - the look-back loads a batch of predecessor flags at once and is bounded
 //    by elapsed time (BAJO_STATUS_LOOKBACK_TIMEOUT) instead of spinning
 //    forever one flag at a time (onesweep.mojo:246-270);
@@ -49,27 +50,36 @@ struct KeyTraits<uint64_t> {
 };
 
 // ---------------------------------------------------------------------------
-// Tile shapes and digit widths.  Variant 0 is the large default; smaller
-// tiles give small sorts more CTAs.  max_log2n: the largest sort (log2 of n)
-// a variant may serve, which bounds the look-back memory a workspace must
-// hold.  bits: digit width.  Variant 4 of the 64-bit keys sorts 10-bit
+// Tile shapes, digit widths and pass kernels.  For 32-bit keys, variants 4-6
+// run onesweep_early_pass_kernel (variant 5 is the default from 2^20 keys);
+// variants 0-3 (and every 64-bit variant) run onesweep_pass_kernel or its
+// wide-digit form.  Smaller tiles give small sorts more CTAs.  max_log2n:
+// the largest sort (log2 of n) a variant may serve, which bounds the
+// look-back memory a workspace must hold.  bits: digit width.  Variant 4 of the 64-bit keys sorts 10-bit
 // digits, so the 30 live bits of single-scene LBVH keys take three passes
 // instead of four, but each pass does 1,024 digits of per-tile work.
 // Measured on B200 (30-bit keys + 32-bit values): 2^14 keys 54.8 vs 60.2 us
 // (best 8-bit variant), 2^16 68.3 vs 59.3, 2^18 87.8 vs 71.3; inside the
 // LBVH build 2^15 triangles 78.8 vs 80.9 us, 2^16 85-87 vs 85.0.
 // ---------------------------------------------------------------------------
-constexpr int kNumVariants = 5;  // the largest variant count of any key type
+constexpr int kNumVariants = 7;  // the largest variant count of any key type
 struct Shape {
-  int block, kpt, max_log2n, bits;
+  int block, kpt, max_log2n, bits, early, lb, match;  // early: onesweep_early_pass_kernel (8-bit digits);
+                                                      // lb: look-back flags per round trip (0: kLookbackBatch);
+                                                      // match: early pass peers by ballots (0) or shared OR
+                                                      // (1; 2: two alternating masks and the run by atomics)
 };
 template <typename K>
 struct Shapes;
 template <>
 struct Shapes<uint32_t> {
-  static constexpr int count = 4;
-  static constexpr Shape v[count] = {{512, 12, 30, 8}, {256, 12, 30, 8}, {256, 8, 24, 8}, {256, 4, 20, 8}};
+  static constexpr int count = 7;
+  static constexpr Shape v[count] = {{512, 12, 30, 8, 0, 0}, {256, 12, 30, 8, 0, 0}, {256, 8, 24, 8, 0, 0},
+                                     {256, 4, 20, 8, 0, 0},  {256, 20, 30, 8, 1, 8, 2}, {256, 24, 30, 8, 1, 8, 2},
+                                     {256, 32, 30, 8, 1, 8, 2}};
 };
+constexpr int kEarlyU32Default = 5;  // Shapes<uint32_t>::v[5]
+
 template <>
 struct Shapes<uint64_t> {
   static constexpr int count = 5;
@@ -132,6 +142,9 @@ inline int choose_variant(uint32_t n, int sm_count) {
   // to 2^15 keys), else the largest 8-bit tile that still gives every SM two
   // tiles
   if (sizeof(K) == 8 && HAS_V && n <= (1u << 15) && variant_allowed<K>(4, n)) return 4;
+  // 32-bit keys from 2^20 on: the early-count pass, 256 x 24 keys (measured
+  // fastest on B200 at 2^20-2^28, keys and pairs)
+  if (sizeof(K) == 4 && n >= (1u << 20) && variant_allowed<K>(kEarlyU32Default, n)) return kEarlyU32Default;
   for (int c = 0; c < Shapes<K>::count; ++c) {
     if (!variant_allowed<K>(c, n) || variant_bits<K>(c) != 8) continue;
     if ((n + variant_tile<K>(c) - 1) / variant_tile<K>(c) >= (uint32_t)(2 * sm_count)) return c;
@@ -139,6 +152,20 @@ inline int choose_variant(uint32_t n, int sm_count) {
   for (int c = Shapes<K>::count - 1; c >= 0; --c)
     if (variant_allowed<K>(c, n) && variant_bits<K>(c) == 8) return c;
   return 0;
+}
+
+// Lanes of the warp whose BITS-bit label equals this lane's: one ballot per
+// label bit (full-rate vote instructions; no match instruction).
+template <int BITS>
+__device__ __forceinline__ uint32_t match_label(uint32_t label) {
+  uint32_t peers = 0xFFFFFFFFu;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    const bool set = (label >> b) & 1u;
+    const uint32_t m = __ballot_sync(0xFFFFFFFFu, set);
+    peers &= set ? m : ~m;
+  }
+  return peers;
 }
 
 __device__ __forceinline__ uint32_t warp_inclusive_scan(uint32_t v) {
@@ -199,21 +226,47 @@ __global__ void __launch_bounds__(kHistBlock) global_histogram_kernel(const K* _
   for (uint32_t i = threadIdx.x; i < words; i += kHistBlock) s_hist[i] = 0;
   __syncthreads();
   const uint32_t copy = (threadIdx.x >> 5) % copies;
-  const uint32_t stride = gridDim.x * kHistBlock;
-  for (uint32_t i = blockIdx.x * kHistBlock + threadIdx.x; i < n; i += stride) {
-    K k = keys[i];
-    for (uint32_t p = 0; p < n_passes; ++p) {
-      uint32_t sh = begin_bit + digit_bits * p;
-      uint32_t bits = min(digit_bits, end_bit - sh);
-      uint32_t d = (uint32_t)(k >> sh) & ((1u << bits) - 1u);
-      atomicAdd(&s_hist[(p * copies + copy) * radix + d], 1u);
+  uint32_t* h = s_hist + copy * radix;
+  const uint32_t pstride = copies * radix;
+  auto count = [&](K k) {
+    uint32_t* hp = h;
+    for (uint32_t p = 0, sh = begin_bit; p < n_passes; ++p, sh += digit_bits, hp += pstride) {
+      const uint32_t bits = min(digit_bits, end_bit - sh);
+      atomicAdd(&hp[(uint32_t)(k >> sh) & ((1u << bits) - 1u)], 1u);
     }
+  };
+  const uint32_t stride = gridDim.x * kHistBlock;
+  const uint32_t g = blockIdx.x * kHistBlock + threadIdx.x;
+  // 16-byte loads (two in flight per thread) over the aligned bulk, single
+  // keys over the rest; the keys are read once, so the loads stream past L1
+  constexpr uint32_t kVec = 16 / sizeof(K);
+  const uint32_t head = (uint32_t)((((uintptr_t)keys + 15) & ~(uintptr_t)15) - (uintptr_t)keys) / sizeof(K);
+  const uint32_t h0 = min(head, n);
+  const uint32_t nvec = (n - h0) / kVec;
+  const uint4* kv = reinterpret_cast<const uint4*>(keys + h0);
+  uint32_t i = g;
+  for (; i + stride < nvec; i += 2 * stride) {
+    const uint4 a = __ldcs(kv + i), b = __ldcs(kv + i + stride);
+    const K* ka = reinterpret_cast<const K*>(&a);
+    const K* kb = reinterpret_cast<const K*>(&b);
+#pragma unroll
+    for (uint32_t j = 0; j < kVec; ++j) count(ka[j]);
+#pragma unroll
+    for (uint32_t j = 0; j < kVec; ++j) count(kb[j]);
   }
+  for (; i < nvec; i += stride) {
+    const uint4 a = __ldcs(kv + i);
+    const K* ka = reinterpret_cast<const K*>(&a);
+#pragma unroll
+    for (uint32_t j = 0; j < kVec; ++j) count(ka[j]);
+  }
+  for (uint32_t q = g; q < h0; q += stride) count(keys[q]);                           // unaligned head
+  for (uint32_t q = h0 + nvec * kVec + g; q < n; q += stride) count(keys[q]);  // ragged tail
   __syncthreads();
-  for (uint32_t i = threadIdx.x; i < n_passes * radix; i += kHistBlock) {
-    uint32_t p = i / radix, d = i % radix, s = 0;
-    for (uint32_t c = 0; c < copies; ++c) s += s_hist[(p * copies + c) * radix + d];
-    if (s) atomicAdd(&ghist[p * radix + d], s);
+  for (uint32_t q = threadIdx.x; q < n_passes * radix; q += kHistBlock) {
+    uint32_t p = q / radix, d = q % radix, sum = 0;
+    for (uint32_t c = 0; c < copies; ++c) sum += s_hist[(p * copies + c) * radix + d];
+    if (sum) atomicAdd(&ghist[p * radix + d], sum);
   }
 }
 
@@ -280,7 +333,7 @@ __device__ __forceinline__ void prefetch_l2_bulk(const void* p, uint32_t bytes) 
 
 // lookback: this pass's flags; lookback_next: the other region, whose slot of
 // this tile is cleared for the next pass.
-template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT>
+template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT, int LB = kLookbackBatch>
 __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
     const K* __restrict__ keys_in, K* __restrict__ keys_out, const uint32_t* __restrict__ vals_in,
     uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
@@ -326,7 +379,7 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
     const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t peers = match_label<8>(d);
     const uint32_t leader = __ffs(peers) - 1;
     uint32_t before = 0;
     if (lane == leader) before = atomicAdd(&wh[d], (uint32_t)__popc(peers));
@@ -366,9 +419,9 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
     rank[i] += s.u.warp_hist[warp * kRadix + d];
   }
 
-  // Decoupled look-back, one thread per digit.  The flags of up to
-  // kLookbackBatch predecessors are loaded at once (independent loads), so a
-  // chain of ready aggregates costs one L2 round trip per batch.
+  // Decoupled look-back, one thread per digit.  The flags of up to LB
+  // predecessors are loaded at once (independent loads), so a chain of ready
+  // aggregates costs one L2 round trip per batch.
   if (tid < kRadix) {
     uint32_t excl = 0;
     if (tile > 0) {
@@ -376,14 +429,14 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
       uint32_t spins = 0;
       uint64_t t0 = 0;
       while (k >= 0) {
-        uint32_t f[kLookbackBatch];
+        uint32_t f[LB];
 #pragma unroll
-        for (int q = 0; q < kLookbackBatch; ++q)
+        for (int q = 0; q < LB; ++q)
           f[q] = (k - q >= 0) ? ld_relaxed_gpu(&lookback[(uint32_t)(k - q) * kRadix + tid]) : kFlagInc;
         int consumed = 0;
         bool done = false;
 #pragma unroll
-        for (int q = 0; q < kLookbackBatch; ++q) {
+        for (int q = 0; q < LB; ++q) {
           if (done || consumed != q) continue;  // stop at the first flag not ready
           const uint32_t flag = f[q] & kFlagMask;
           if (flag == kFlagInc) {
@@ -437,6 +490,243 @@ __global__ void __launch_bounds__(BLOCK, 1024 / BLOCK) onesweep_pass_kernel(
   for (int i = 0; i < KPT; ++i) {
     const uint32_t j = tid + i * BLOCK;
     if (j < valid) {
+      const auto e = s.u.staged[j];
+      const K k = ST::key(e);
+      const uint32_t d = (uint32_t)(k >> shift) & digit_mask;
+      const uint32_t dst = s.digit_offset[d] + j;
+      if (dst < n) {  // holds whenever the digit counts are consistent
+        keys_out[dst] = k;
+        if constexpr (HAS_V) vals_out[dst] = ST::val(e);
+        if constexpr (EMIT_LOW32) low32_out[dst] = (uint32_t)k;
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One digit pass with early counts (8-bit digits; threads below 256: one per
+// digit).  The same result as onesweep_pass_kernel, in another order:
+//  1. every warp counts its keys' digits into its own shared histogram (one
+//     shared atomic per key, no ranking yet);
+//  2. thread d sums digit d over the warps, publishes the tile's aggregate
+//     at once (successors' look-backs need not wait for this tile's ranking)
+//     and turns the warp counts into each warp's first tile position of d;
+//  3. ranking: per key one match over the warp's digits, one shared load of
+//     the warp's running position of the digit and, by the highest peer,
+//     one shared store of the advanced position (no atomic, no shuffle);
+//  4. keys (and values) staged in tile order;
+//  5. the look-back (thread d), after the ranking, when the predecessors'
+//     prefixes are most likely complete, many predecessors' flags per round
+//     trip;
+//  6. the scatter of digit runs.
+// ---------------------------------------------------------------------------
+template <typename K, bool HAS_V, int BLOCK, int KPT>
+struct EarlySmem {
+  using T = typename Staged<K, HAS_V>::T;
+  static constexpr int kWarps = BLOCK / 32;
+  static constexpr int kTile = BLOCK * KPT;
+  union {
+    T staged[kTile];
+    struct {
+      uint32_t warp_run[kWarps * kRadix];  // per (warp, digit): count, then running tile position
+      uint32_t match[2][kWarps * kRadix];  // per (warp, digit): lanes whose key has the digit (MATCH 1, 2)
+    } r;
+  } u;
+  uint32_t digit_offset[kRadix];
+  uint32_t scan_tmp[8];
+  uint32_t tile;
+  uint32_t abort;
+};
+
+template <typename K, bool HAS_V, bool EMIT_LOW32, int BLOCK, int KPT, int LB = kLookbackBatch, int MATCH = 0>
+__global__ void __launch_bounds__(BLOCK, BLOCK >= 512 ? 1 : (KPT >= 32 ? 2 : 3)) onesweep_early_pass_kernel(
+    const K* __restrict__ keys_in, K* __restrict__ keys_out, const uint32_t* __restrict__ vals_in,
+    uint32_t* __restrict__ vals_out, uint32_t* __restrict__ low32_out, const uint32_t* __restrict__ ghist,
+    uint32_t* __restrict__ lookback, uint32_t* __restrict__ lookback_next, uint32_t* __restrict__ tile_counter,
+    uint32_t* __restrict__ status, uint32_t n, uint32_t shift, uint32_t digit_mask) {
+  static_assert(BLOCK % (int)kRadix == 0, "threads below kRadix: one per digit");
+  using S = EarlySmem<K, HAS_V, BLOCK, KPT>;
+  using ST = Staged<K, HAS_V>;
+  constexpr int kWarps = S::kWarps;
+  constexpr uint32_t kTile = S::kTile;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  S& s = *reinterpret_cast<S*>(smem_raw);
+
+  const uint32_t tid = threadIdx.x;
+  const uint32_t lane = tid & 31, warp = tid >> 5;
+
+  for (uint32_t q = tid; q < kWarps * kRadix; q += BLOCK) {
+    s.u.r.warp_run[q] = 0;
+    if constexpr (MATCH >= 1) s.u.r.match[0][q] = 0;
+    if constexpr (MATCH == 2) s.u.r.match[1][q] = 0;
+  }
+  if (tid == 0) {
+    s.tile = atomicAdd(tile_counter, 1u);  // tiles in launch order
+    s.abort = 0;
+  }
+  __syncthreads();
+  const uint32_t tile = s.tile;
+  const uint32_t tile_base = tile * kTile;
+  const uint32_t valid = min(kTile, n - tile_base);
+  if (HAS_V && tid == 0 && (((uintptr_t)(vals_in + tile_base)) & 15) == 0)
+    prefetch_l2_bulk(vals_in + tile_base, (valid * 4u) & ~15u);  // values are read after the look-back
+  if (lookback_next && tid < kRadix) lookback_next[tile * kRadix + tid] = 0;
+
+  // warp-striped load: key i of this thread sits at tile position
+  // warp*32*KPT + 32*i + lane, so (warp, i, lane) order is position order.
+  K key[KPT];
+  const uint32_t pos0 = tile_base + warp * 32 * KPT + lane;
+  const bool full = valid == kTile;  // every tile but the last: no bounds checks
+  if (full) {
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) key[i] = keys_in[pos0 + 32 * i];
+  } else {
+#pragma unroll
+    for (int i = 0; i < KPT; ++i) {
+      const uint32_t p = pos0 + 32 * i;
+      key[i] = (p < n) ? keys_in[p] : KeyTraits<K>::kMax;
+    }
+  }
+  // 1. the warp's digit counts
+  uint32_t* wr = s.u.r.warp_run + warp * kRadix;
+  uint32_t* wm = s.u.r.match[0] + warp * kRadix;
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) atomicAdd(&wr[(uint32_t)(key[i] >> shift) & digit_mask], 1u);
+  __syncthreads();
+
+  // 2. thread d: the tile's count of digit d, published at once, and each
+  // warp's first tile position of d
+  uint32_t cw[kWarps], total = 0, agg = 0, gcount = 0;
+  if (tid < kRadix) {
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      cw[w] = s.u.r.warp_run[w * kRadix + tid];
+      total += cw[w];
+    }
+    agg = total - ((tid == digit_mask) ? (kTile - valid) : 0u);  // padding keys: the top digit
+    st_relaxed_gpu(&lookback[tile * kRadix + tid], agg | (tile == 0 ? kFlagInc : kFlagAgg));
+    gcount = ghist[tid];
+  }
+  const uint32_t tstart = scan256_exclusive<BLOCK>(total, s.scan_tmp);
+  const uint32_t gstart = scan256_exclusive<BLOCK>(gcount, s.scan_tmp);
+  if (tid < kRadix) {
+    uint32_t run = tstart;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+      s.u.r.warp_run[w * kRadix + tid] = run;
+      run += cw[w];
+    }
+  }
+  __syncthreads();
+
+  // 3. ranks: tile positions, in position order within every digit
+  const uint32_t lt = lanemask_lt();
+  uint32_t rank[KPT];
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
+    if constexpr (MATCH == 2) {
+      // masks alternate between two arrays, so a mask cleared here is next
+      // written two keys later, after the next key's warp barrier; the
+      // run moves by the lowest peer's atomic add (atomics on one word keep
+      // their order), whose old value the peers take by shuffle
+      uint32_t* m = s.u.r.match[i & 1] + warp * kRadix;
+      atomicOr(&m[d], 1u << lane);
+      __syncwarp();
+      const uint32_t peers = m[d];
+      const uint32_t leader = __ffs(peers) - 1;
+      uint32_t at = 0;
+      if (lane == leader) {
+        at = atomicAdd(&wr[d], (uint32_t)__popc(peers));
+        m[d] = 0u;
+      }
+      rank[i] = __shfl_sync(0xFFFFFFFFu, at, leader) + __popc(peers & lt);
+      continue;
+    }
+    uint32_t peers;
+    if constexpr (MATCH == 1) {  // every lane ORs its bit into the digit's mask
+      atomicOr(&wm[d], 1u << lane);
+      __syncwarp();
+      peers = wm[d];
+    } else {
+      peers = match_label<8>(d);
+    }
+    const uint32_t at = wr[d];
+    rank[i] = at + __popc(peers & lt);
+    __syncwarp();  // every peer has read the run (and the mask) before they change
+    if ((peers >> lane) == 1u) {  // the highest peer advances the run
+      wr[d] = at + __popc(peers);
+      if constexpr (MATCH == 1) wm[d] = 0u;
+    }
+    __syncwarp();
+  }
+
+  __syncthreads();  // every warp has ranked: warp_run is not read again
+  // 4. stage key (+ value) at its tile position (so the look-back below runs
+  // with few live registers, and the value loads overlap it)
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    uint32_t v = 0;
+    if constexpr (HAS_V) {
+      const uint32_t p = pos0 + 32 * i;
+      v = (full || p < n) ? vals_in[p] : 0u;
+    }
+    s.u.staged[rank[i]] = ST::pack(key[i], v);
+  }
+
+  // 5. decoupled look-back, thread d (as in onesweep_pass_kernel)
+  if (tid < kRadix) {
+    uint32_t excl = 0;
+    if (tile > 0) {
+      int32_t k = (int32_t)tile - 1;
+      uint32_t spins = 0;
+      uint64_t t0 = 0;
+      while (k >= 0) {
+        uint32_t f[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q)
+          f[q] = (k - q >= 0) ? ld_relaxed_gpu(&lookback[(uint32_t)(k - q) * kRadix + tid]) : kFlagInc;
+        int consumed = 0;
+        bool done = false;
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          if (done || consumed != q) continue;  // stop at the first flag not ready
+          const uint32_t flag = f[q] & kFlagMask;
+          if (flag == kFlagInc) {
+            excl += f[q] & kValueMask;
+            done = true;
+          } else if (flag == kFlagAgg) {
+            excl += f[q] & kValueMask;
+            ++consumed;
+          }
+        }
+        if (done) break;
+        k -= consumed;
+        if (consumed > 0) {
+          spins = 0;
+          continue;
+        }
+        if (spins == 0) t0 = global_timer_ns();
+        ++spins;
+        if ((spins & 63u) == 0 && global_timer_ns() - t0 > kLookbackTimeoutNs) {
+          raise_status(status, BAJO_STATUS_LOOKBACK_TIMEOUT);
+          s.abort = 1;
+          break;
+        }
+        __nanosleep(spins < 64 ? 32 : 256);
+      }
+      st_relaxed_gpu(&lookback[tile * kRadix + tid], ((excl + agg) & kValueMask) | kFlagInc);
+    }
+    s.digit_offset[tid] = gstart + excl - tstart;
+  }
+  __syncthreads();  // the staged tile and the digit offsets are complete
+  if (s.abort) return;
+
+  // 6. scatter digit runs
+#pragma unroll
+  for (int i = 0; i < KPT; ++i) {
+    const uint32_t j = tid + i * BLOCK;
+    if (full || j < valid) {
       const auto e = s.u.staged[j];
       const K k = ST::key(e);
       const uint32_t d = (uint32_t)(k >> shift) & digit_mask;
@@ -564,7 +854,7 @@ __global__ void __launch_bounds__(BLOCK) onesweep_wide_pass_kernel(
 #pragma unroll
   for (int i = 0; i < KPT; ++i) {
     const uint32_t d = (uint32_t)(key[i] >> shift) & digit_mask;
-    const uint32_t peers = __match_any_sync(0xFFFFFFFFu, d);
+    const uint32_t peers = match_label<RBITS>(d);
     const uint32_t leader = __ffs(peers) - 1;
     uint32_t before = 0;
     if (lane == leader) {  // one leader per digit value: no two lanes share a counter
@@ -781,10 +1071,16 @@ inline cudaError_t launch_variant(const K* kin, K* kout, const uint32_t* vin, ui
   constexpr int B = Shapes<K>::v[V].block;
   constexpr int KPT = Shapes<K>::v[V].kpt;
   constexpr int BITS = Shapes<K>::v[V].bits;
-  using Smem = typename std::conditional<BITS == 8, BinSmem<K, HAS_V, B, KPT>,
-                                         WideBinSmem<K, HAS_V, B, KPT, (BITS == 8 ? 10 : BITS)>>::type;
+  constexpr bool EARLY = Shapes<K>::v[V].early != 0;
+  constexpr int LB = Shapes<K>::v[V].lb > 0 ? Shapes<K>::v[V].lb : kLookbackBatch;
+  constexpr int MATCH = Shapes<K>::v[V].match;
+  using Smem = typename std::conditional<
+      EARLY, EarlySmem<K, HAS_V, B, KPT>,
+      typename std::conditional<BITS == 8, BinSmem<K, HAS_V, B, KPT>,
+                                WideBinSmem<K, HAS_V, B, KPT, (BITS == 8 ? 10 : BITS)>>::type>::type;
   auto kern = [] {
-    if constexpr (BITS == 8) return onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT>;
+    if constexpr (EARLY) return onesweep_early_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT, LB, MATCH>;
+    else if constexpr (BITS == 8) return onesweep_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT, LB>;
     else return onesweep_wide_pass_kernel<K, HAS_V, EMIT_LOW32, B, KPT, BITS>;
   }();
   const size_t smem = sizeof(Smem);
@@ -820,6 +1116,16 @@ inline cudaError_t launch_pass(int variant, const K* kin, K* kout, const uint32_
     case 4:
       if constexpr (Shapes<K>::count > 4)
         return launch_variant<K, HAS_V, EMIT_LOW32, 4>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                       status, n, shift, digit_mask, stream);
+      return cudaErrorInvalidValue;
+    case 5:
+      if constexpr (Shapes<K>::count > 5)
+        return launch_variant<K, HAS_V, EMIT_LOW32, 5>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
+                                                       status, n, shift, digit_mask, stream);
+      return cudaErrorInvalidValue;
+    case 6:
+      if constexpr (Shapes<K>::count > 6)
+        return launch_variant<K, HAS_V, EMIT_LOW32, 6>(kin, kout, vin, vout, low32, ghist, lb, lb_next, counter,
                                                        status, n, shift, digit_mask, stream);
       return cudaErrorInvalidValue;
     default:

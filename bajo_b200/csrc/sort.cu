@@ -64,7 +64,7 @@ int32_t sort_impl(K* keys, uint32_t* vals, uint32_t n, int32_t begin_bit, int32_
   uint32_t* ghist = (uint32_t*)(w + p.off_ghist);
   const size_t hsmem = onesweep::hist_smem(vpasses, bits);
   uint32_t grid = (n + onesweep::kHistBlock * 16 - 1) / (onesweep::kHistBlock * 16);
-  uint32_t max_grid = (uint32_t)sm_count() * 4;
+  uint32_t max_grid = (uint32_t)sm_count() * 8;
   if (grid > max_grid) grid = max_grid;
   if (grid == 0) grid = 1;
   if (hsmem > 48 * 1024 &&

@@ -84,13 +84,17 @@ int32_t bajo_sort_keys_u64(uint64_t* d_keys, uint32_t n, int32_t begin_bit, int3
 int32_t bajo_sort_pairs_u64(uint64_t* d_keys, uint32_t* d_vals, uint32_t n, int32_t begin_bit, int32_t end_bit,
                             void* d_workspace, size_t workspace_bytes, void* stream);
 
-/* Autotuner hooks.  The sort kernels come in BAJO_SORT_VARIANTS compiled tile
- * shapes (threads x keys per thread); the library picks one per call from a
- * process-wide table indexed by (key bytes, values, ceil(log2 n)), filled by
- * the project's autotuner (bajo_b200/autotune.py) or left at -1 for the
- * built-in choice.  Set entries before sorting, not concurrently with sorts.
- * bajo_sort_tuning_get reports the variant a call of size n would use. */
-#define BAJO_SORT_VARIANTS 4
+/* Autotuner hooks.  The sort kernels come in compiled variants (tile shape:
+ * threads x keys per thread, digit width, pass kernel): BAJO_SORT_VARIANTS_U32
+ * for 32-bit keys and BAJO_SORT_VARIANTS_U64 for 64-bit keys; the library
+ * picks one per call from a process-wide table indexed by (key bytes, values,
+ * ceil(log2 n)), filled by the project's autotuner (bajo_b200/autotune.py) or
+ * left at -1 for the built-in choice.  Set entries before sorting, not
+ * concurrently with sorts.  bajo_sort_tuning_get reports the variant a call
+ * of size n would use. */
+#define BAJO_SORT_VARIANTS_U32 7
+#define BAJO_SORT_VARIANTS_U64 5
+#define BAJO_SORT_VARIANTS 7 /* the larger of the two */
 int32_t bajo_sort_tuning_set(uint32_t key_bytes, int32_t has_values, uint32_t log2n, int32_t variant);
 int32_t bajo_sort_tuning_get(uint32_t key_bytes, int32_t has_values, uint32_t n, int32_t* variant);
 

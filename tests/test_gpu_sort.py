@@ -144,10 +144,10 @@ def test_full_size_properties(n, kind):
     assert bool((vals[1:][eq] > vals[:-1][eq]).all())
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
-@pytest.mark.parametrize("kind", ["u32", "u64"])
+@pytest.mark.parametrize("kind,variant", [("u32", v) for v in range(7)] + [("u64", v) for v in range(4)])
 def test_every_tile_variant_matches_oracle(oracle, variant, kind):
-    """Each compiled tile shape the autotuner may pick sorts exactly."""
+    """Each compiled tile shape the autotuner may pick sorts exactly (the
+    32-bit keys' variants 4-6: early-count passes and wider look-backs)."""
     from bajo_b200 import _lib
     L = _lib.load()
     kb = 4 if kind == "u32" else 8
@@ -205,7 +205,8 @@ def test_wide_digit_variant_matches_oracle(oracle, bits):
 def test_wide_digit_variant_limits():
     from bajo_b200 import _lib
     L = _lib.load()
-    assert L.bajo_sort_tuning_set(4, 1, 16, 4) == _lib.ERR_INVALID_ARGUMENT   # 32-bit keys: 8-bit digits only
+    assert L.bajo_sort_tuning_set(4, 1, 16, _lib.SORT_VARIANTS_U32) == _lib.ERR_INVALID_ARGUMENT  # 32-bit: 7
+    assert L.bajo_sort_tuning_set(8, 1, 16, _lib.SORT_VARIANTS_U64) == _lib.ERR_INVALID_ARGUMENT  # 64-bit: 5
     assert L.bajo_sort_tuning_set(8, 1, 19, 4) == _lib.ERR_INVALID_ARGUMENT   # up to 2^18 keys
     assert L.bajo_sort_tuning_set(8, 1, 18, 4) == _lib.OK
     assert L.bajo_sort_tuning_set(8, 1, 18, -1) == _lib.OK
