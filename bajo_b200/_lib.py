@@ -34,7 +34,7 @@ SORT_MAX_KEYS = (1 << 30) - 1
 SORT_NOALLOC_MAX_KEYS = 1 << 20
 SORT_NOALLOC_SCRATCH_BYTES = 10490368  # BAJO_SORT_NOALLOC_SCRATCH_BYTES
 SORT_VARIANTS_U32 = 7  # BAJO_SORT_VARIANTS_U32: compiled variants of the 32-bit-key sort
-SORT_VARIANTS_U64 = 5  # BAJO_SORT_VARIANTS_U64
+SORT_VARIANTS_U64 = 7  # BAJO_SORT_VARIANTS_U64
 SORT_VARIANTS = 7  # the larger of the two
 
 _ERRORS = {

@@ -50,10 +50,10 @@ struct KeyTraits<uint64_t> {
 };
 
 // ---------------------------------------------------------------------------
-// Tile shapes, digit widths and pass kernels.  For 32-bit keys, variants 4-6
-// run onesweep_early_pass_kernel (variant 5 is the default from 2^20 keys);
-// variants 0-3 (and every 64-bit variant) run onesweep_pass_kernel or its
-// wide-digit form.  Smaller tiles give small sorts more CTAs.  max_log2n:
+// Tile shapes, digit widths and pass kernels.  Variants 4-6 of the 32-bit
+// keys and 5-6 of the 64-bit keys run onesweep_early_pass_kernel (variant 5
+// is the built-in choice from 2^20 and 2^19 keys); the others run
+// onesweep_pass_kernel or its wide-digit form.  Smaller tiles give small sorts more CTAs.  max_log2n:
 // the largest sort (log2 of n) a variant may serve, which bounds the
 // look-back memory a workspace must hold.  bits: digit width.  Variant 4 of the 64-bit keys sorts 10-bit
 // digits, so the 30 live bits of single-scene LBVH keys take three passes
@@ -79,12 +79,13 @@ struct Shapes<uint32_t> {
                                      {256, 32, 30, 8, 1, 8, 2}};
 };
 constexpr int kEarlyU32Default = 5;  // Shapes<uint32_t>::v[5]
+constexpr int kEarlyU64Default = 5;  // Shapes<uint64_t>::v[5]
 
 template <>
 struct Shapes<uint64_t> {
-  static constexpr int count = 5;
+  static constexpr int count = 7;
   static constexpr Shape v[count] = {{512, 8, 30, 8}, {256, 8, 30, 8}, {256, 5, 24, 8}, {256, 3, 20, 8},
-                                     {256, 4, 18, 10}};
+                                     {256, 4, 18, 10}, {256, 16, 30, 8, 1, 8, 2}, {256, 12, 30, 8, 1, 8, 2}};
 };
 
 constexpr uint32_t ceil_log2(uint32_t n) {
@@ -145,6 +146,8 @@ inline int choose_variant(uint32_t n, int sm_count) {
   // 32-bit keys from 2^20 on: the early-count pass, 256 x 24 keys (measured
   // fastest on B200 at 2^20-2^28, keys and pairs)
   if (sizeof(K) == 4 && n >= (1u << 20) && variant_allowed<K>(kEarlyU32Default, n)) return kEarlyU32Default;
+  // 64-bit keys from 2^19 on: the early-count pass, 256 x 16 keys
+  if (sizeof(K) == 8 && n >= (1u << 19) && variant_allowed<K>(kEarlyU64Default, n)) return kEarlyU64Default;
   for (int c = 0; c < Shapes<K>::count; ++c) {
     if (!variant_allowed<K>(c, n) || variant_bits<K>(c) != 8) continue;
     if ((n + variant_tile<K>(c) - 1) / variant_tile<K>(c) >= (uint32_t)(2 * sm_count)) return c;

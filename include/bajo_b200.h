@@ -93,7 +93,7 @@ int32_t bajo_sort_pairs_u64(uint64_t* d_keys, uint32_t* d_vals, uint32_t n, int3
  * concurrently with sorts.  bajo_sort_tuning_get reports the variant a call
  * of size n would use. */
 #define BAJO_SORT_VARIANTS_U32 7
-#define BAJO_SORT_VARIANTS_U64 5
+#define BAJO_SORT_VARIANTS_U64 7
 #define BAJO_SORT_VARIANTS 7 /* the larger of the two */
 int32_t bajo_sort_tuning_set(uint32_t key_bytes, int32_t has_values, uint32_t log2n, int32_t variant);
 int32_t bajo_sort_tuning_get(uint32_t key_bytes, int32_t has_values, uint32_t n, int32_t* variant);
