@@ -662,6 +662,89 @@ def sweep_keys(torch, kind, n, seed, dev):
     return torch.randint(-2**31, 2**31, (n,), dtype=torch.int32, device=dev, generator=g), 0, 32
 
 
+# CUB 12.9's radix sort (cub::DeviceRadixSort, the CUDA toolkit's library
+# sort) timed on the same device buffers as the sweep: the library baseline
+# the sweep is compared with.  Built on first use with the toolkit's nvcc.
+CUB_BASELINE_SRC = r"""
+#include <cub/cub.cuh>
+#include <algorithm>
+#include <vector>
+#include <cstdint>
+extern "C" int cub_sort_ms(int key_bytes, const void* keys, const uint32_t* vals, uint32_t n, int end_bit, int reps,
+                           void* flush, size_t flush_bytes, float* median_ms) {
+  void *kout = nullptr, *vout = nullptr, *tmp = nullptr;
+  size_t tb = 0;
+  cudaError_t e = cudaMalloc(&kout, (size_t)n * key_bytes);
+  if (e == cudaSuccess && vals) e = cudaMalloc(&vout, (size_t)n * 4);
+  auto run = [&](void* t, size_t& b) {
+    if (key_bytes == 4 && vals)
+      return cub::DeviceRadixSort::SortPairs(t, b, (const uint32_t*)keys, (uint32_t*)kout, vals, (uint32_t*)vout,
+                                             (int)n, 0, end_bit);
+    if (key_bytes == 4)
+      return cub::DeviceRadixSort::SortKeys(t, b, (const uint32_t*)keys, (uint32_t*)kout, (int)n, 0, end_bit);
+    if (vals)
+      return cub::DeviceRadixSort::SortPairs(t, b, (const uint64_t*)keys, (uint64_t*)kout, vals, (uint32_t*)vout,
+                                             (int)n, 0, end_bit);
+    return cub::DeviceRadixSort::SortKeys(t, b, (const uint64_t*)keys, (uint64_t*)kout, (int)n, 0, end_bit);
+  };
+  if (e == cudaSuccess) e = run(nullptr, tb);
+  if (e == cudaSuccess) e = cudaMalloc(&tmp, tb);
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  std::vector<float> ms;
+  for (int r = 0; e == cudaSuccess && r <= reps; ++r) {
+    cudaMemsetAsync(flush, r & 255, flush_bytes);
+    cudaEventRecord(a);
+    e = run(tmp, tb);
+    cudaEventRecord(b);
+    cudaEventSynchronize(b);
+    float t = 0;
+    cudaEventElapsedTime(&t, a, b);
+    if (r) ms.push_back(t);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(kout);
+  cudaFree(vout);
+  cudaFree(tmp);
+  if (e != cudaSuccess || ms.empty()) return 1;
+  std::sort(ms.begin(), ms.end());
+  *median_ms = ms[ms.size() / 2];
+  return 0;
+}
+"""
+
+
+def cub_baseline_lib():
+    """ctypes handle of the CUB timing library (built once into the package's
+    build folder), or None when nvcc or the build is not available."""
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    out_dir = os.path.join(here, "bajo_b200", "_build", "cub_baseline")
+    so = os.path.join(out_dir, "libcub_sort_baseline.so")
+    src = os.path.join(out_dir, "cub_sort_baseline.cu")
+    try:
+        os.makedirs(out_dir, exist_ok=True)
+        if not os.path.exists(so) or not os.path.exists(src) or open(src).read() != CUB_BASELINE_SRC:
+            with open(src, "w") as f:
+                f.write(CUB_BASELINE_SRC)
+            nvcc = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+            subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-shared", "-Xcompiler",
+                            "-fPIC", "-o", so, src], check=True, capture_output=True)
+        lib = ctypes.CDLL(so)
+        lib.cub_sort_ms.restype = ctypes.c_int
+        lib.cub_sort_ms.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int,
+                                    ctypes.c_int, ctypes.c_void_p, ctypes.c_size_t, ctypes.POINTER(ctypes.c_float)]
+        return lib
+    except Exception:  # noqa: BLE001 - a missing toolkit only drops the comparison
+        return None
+
+
+CUB_SWEEP_LOG2 = (20, 24, 26, 28)
+
+
 def run_sweep(torch, bvh, _lib, L, dev, stream, peak, reps=7):
     """Throughput of the sort sweep workload at every stated size and key
     kind, and of the LBVH build at larger sizes.  Each timed sample restores
@@ -671,6 +754,7 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak, reps=7):
     out = {k: {} for k in SWEEP_KINDS}
     out["build"] = {}
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=dev)
+    cub = cub_baseline_lib()
 
     def timeit(prepare, fn):
         prepare()
@@ -712,9 +796,19 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak, reps=7):
             del uk
             if ws.status() != 0 or not ok:
                 raise RuntimeError(f"sweep {kind} 2^{lg}: status {ws.status()}, sorted {ok}")
-            out[kind][f"2^{lg}"] = {"gkeys_s": round(n / med / 1e6, 3), "ms": round(med, 5),
-                                    "hbm_frac": round(bytes_per_key * n / (med / 1e3) / 1e9 / peak, 4),
-                                    "best_gkeys_s": round(n / best / 1e6, 3)}
+            point = {"gkeys_s": round(n / med / 1e6, 3), "ms": round(med, 5),
+                     "hbm_frac": round(bytes_per_key * n / (med / 1e3) / 1e9 / peak, 4),
+                     "best_gkeys_s": round(n / best / 1e6, 3)}
+            if cub is not None and lg in CUB_SWEEP_LOG2:
+                del ws
+                ws = None
+                torch.cuda.synchronize()
+                cms = ctypes.c_float(0.0)
+                if cub.cub_sort_ms(src_k.element_size(), src_k.data_ptr(), src_v.data_ptr() if pairs else None, n, e,
+                                   reps, flush.data_ptr(), flush.numel(), ctypes.byref(cms)) == 0:
+                    point["cub_gkeys_s"] = round(n / cms.value / 1e6, 3)
+                    point["vs_cub"] = round(cms.value / med, 3)
+            out[kind][f"2^{lg}"] = point
             del src_k, keys, vals, src_v, ws
     for lg in (20, 22, 24):
         n = 1 << lg
@@ -731,6 +825,9 @@ def run_sweep(torch, bvh, _lib, L, dev, stream, peak, reps=7):
         del c, off, v, ws, tree
     out["bytes_per_key"] = {k: v[0] for k, v in SWEEP_KINDS.items()}
     out["timing"] = f"median of {reps} event-timed sorts; unsorted keys restored and L2 flushed before each"
+    out["cub"] = ("cub::DeviceRadixSort of CUDA 12.9 (SortKeys / SortPairs, the same keys, bit range and L2 "
+                  "flush, median of the same count), at 2^" + ", 2^".join(map(str, CUB_SWEEP_LOG2)) +
+                  "; vs_cub = CUB time / this sort's time" if cub is not None else "nvcc unavailable: no CUB leg")
     return out
 
 
