@@ -170,6 +170,7 @@ SIGNATURES = {
                                         _P, _P]),
     "bajo_mlp_param_count": (_I32, [ctypes.POINTER(_U32)]),
     "bajo_mlp_forward": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
+    "bajo_mlp_forward_tc": (_I32, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "bajo_mlp_grad": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
     "bajo_mlp_adam": (_I32, [_P, _P, _P, _P, _P, _U32, _F, _F, _F, _F, _F, _P]),
     "bajo_guide_records_size": (_I32, [_U32, ctypes.POINTER(_SZ)]),

@@ -94,12 +94,22 @@ class GuideNetwork:
         return BajoGuideNetC(self.params32.data_ptr(), self.params16.data_ptr(), self.adam_m.data_ptr(),
                              self.adam_v.data_ptr(), self.grad_buf.data_ptr(), self.loss_buf.data_ptr(), self.step)
 
-    def forward(self, pos: torch.Tensor, nrm: torch.Tensor, box: torch.Tensor, stream=None) -> torch.Tensor:
+    def forward(self, pos: torch.Tensor, nrm: torch.Tensor, box: torch.Tensor, stream=None,
+                tensor_memory: bool = False, status: torch.Tensor | None = None) -> torch.Tensor:
+        """Raw outputs [n, 20]; ``tensor_memory`` runs the tcgen05 kernel
+        (``status``: an optional int32 device word for its timeout bit)."""
         n = pos.numel() // 3
         out = torch.empty((n, N_OUT), dtype=torch.float32, device=pos.device)
-        _lib.check(_lib.load().bajo_mlp_forward(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(), n,
-                                                box.data_ptr(), out.data_ptr(), _lib.stream_handle(stream)),
-                   "bajo_mlp_forward")
+        L = _lib.load()
+        if tensor_memory:
+            _lib.check(L.bajo_mlp_forward_tc(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(), n,
+                                             box.data_ptr(), out.data_ptr(),
+                                             status.data_ptr() if status is not None else None,
+                                             _lib.stream_handle(stream)), "bajo_mlp_forward_tc")
+        else:
+            _lib.check(L.bajo_mlp_forward(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(), n,
+                                          box.data_ptr(), out.data_ptr(), _lib.stream_handle(stream)),
+                       "bajo_mlp_forward")
         return out
 
     def gradient(self, pos, nrm, dirs, weights, box, stream=None):

@@ -222,17 +222,24 @@ class RtScene:
 
 
 def spheres_in_box(n_spheres: int = 64, subdivisions: int = 5, seed: int = 0, emission: float = 15.0,
-                   rmin: float = 0.03, rmax: float = 0.1) -> RtScene:
+                   rmin: float = 0.03, rmax: float = 0.1, light_up: bool = False) -> RtScene:
     """The procedural path-tracing workload: a 12-triangle unit box (albedo
     0.75) with a 0.25 x 0.25 emissive quad (emission 15) just below the
     ceiling, and n_spheres icospheres (radius uniform in [rmin, rmax], centres
     uniform inside the box and clear of the walls and of the camera) with
     Lambertian albedo uniform in [0.2, 0.8] per channel.  The camera sits just
-    inside the front wall looking at the back wall, 60 degree vertical FOV."""
+    inside the front wall looking at the back wall, 60 degree vertical FOV.
+
+    light_up: the same quad at height 0.85 facing the ceiling (emission 4x),
+    so the spheres and walls see only light that bounced off the ceiling
+    patch above it (the geometry is unchanged)."""
     rng = np.random.default_rng(seed)
     unit = icosphere(subdivisions)
-    parts, surf = [unit_box_inward(), ceiling_light()], [[surface_id(MAT_LAMBERTIAN, 0)] * 12,
-                                                        [surface_id(MAT_EMISSIVE, 0)] * 2]
+    light = ceiling_light(0.25, 0.85)[:, ::-1] if light_up else ceiling_light()
+    parts, surf = [unit_box_inward(), light], [[surface_id(MAT_LAMBERTIAN, 0)] * 12,
+                                              [surface_id(MAT_EMISSIVE, 0)] * 2]
+    if light_up:
+        emission = 4.0 * emission
     albedo = [[0.75, 0.75, 0.75]]
     for s in range(n_spheres):
         r = rng.uniform(rmin, rmax)
@@ -246,7 +253,8 @@ def spheres_in_box(n_spheres: int = 64, subdivisions: int = 5, seed: int = 0, em
     cam = camera_from_vfov([0.5, 0.5, 0.02], [0.5, 0.5, 1.0], [0.0, 1.0, 0.0], 60.0)
     return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
                    np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
-                   f"unit box + {n_spheres} icospheres (subdivision {subdivisions}) + ceiling light")
+                   f"unit box + {n_spheres} icospheres (subdivision {subdivisions}) + "
+                   + ("light facing the ceiling" if light_up else "ceiling light"))
 
 
 def indirect_box_scene(emission: float = 40.0, size: float = 0.2, y: float = 0.85, n_spheres: int = 3,
@@ -274,6 +282,44 @@ def indirect_box_scene(emission: float = 40.0, size: float = 0.2, y: float = 0.8
     return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
                    np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
                    f"unit box lit by an upward-facing {size} x {size} panel + {n_spheres} icospheres")
+
+
+def door_scene(n_spheres: int = 16, subdivisions: int = 4, emission: float = 60.0, door_w: float = 0.16,
+               door_h: float = 0.3, seed: int = 11) -> RtScene:
+    """The unit box split by a wall at z = 0.5 with a door_w x door_h opening
+    at the floor: the 0.25 x 0.25 ceiling light hangs over the back half, the
+    camera and n_spheres icospheres sit in the front half.  No point of the
+    front half sees the light (the line to it passes the wall above the
+    door), so its light has bounced in the back half and come through the
+    door: next-event estimation finds nothing there and cosine sampling
+    finds the door rarely, while the incident light is concentrated in the
+    door's direction -- the case path guiding is for."""
+    rng = np.random.default_rng(seed)
+    x0, x1 = 0.5 - door_w / 2, 0.5 + door_w / 2
+    wall = []
+    wall += _quad((0, 0, 0.5), (x0, 0, 0.5), (x0, 1, 0.5), (0, 1, 0.5))
+    wall += _quad((x1, 0, 0.5), (1, 0, 0.5), (1, 1, 0.5), (x1, 1, 0.5))
+    wall += _quad((x0, door_h, 0.5), (x1, door_h, 0.5), (x1, 1, 0.5), (x0, 1, 0.5))
+    h = 0.125
+    light = np.array(_quad((0.5 - h, 0.999, 0.78 - h), (0.5 + h, 0.999, 0.78 - h), (0.5 + h, 0.999, 0.78 + h),
+                           (0.5 - h, 0.999, 0.78 + h)), np.float64)
+    parts = [unit_box_inward(), np.array(wall, np.float64), light]
+    surf = [[surface_id(MAT_LAMBERTIAN, 0)] * 12, [surface_id(MAT_LAMBERTIAN, 0)] * len(wall),
+            [surface_id(MAT_EMISSIVE, 0)] * 2]
+    albedo = [[0.75, 0.75, 0.75]]
+    unit = icosphere(subdivisions)
+    for k in range(n_spheres):
+        r = rng.uniform(0.03, 0.07)
+        c = np.array([rng.uniform(r + 0.02, 1 - r - 0.02), rng.uniform(r + 0.01, 0.6), rng.uniform(0.15, 0.45 - r)])
+        parts.append(unit * r + c)
+        albedo.append(list(rng.uniform(0.3, 0.8, 3)))
+        surf.append([surface_id(MAT_LAMBERTIAN, k + 1)] * unit.shape[0])
+    from .camera import camera_from_vfov
+    cam = camera_from_vfov([0.5, 0.5, 0.02], [0.5, 0.35, 1.0], [0.0, 1.0, 0.0], 70.0)
+    return RtScene(np.concatenate(parts).astype(np.float32), np.concatenate(surf).astype(np.uint32),
+                   np.array(albedo, np.float32), np.array([[emission] * 3], np.float32), cam,
+                   f"unit box split by a wall with a {door_w} x {door_h} door; light behind the wall; "
+                   f"{n_spheres} icospheres in front")
 
 
 def materials_in_box(n_spheres: int = 12, subdivisions: int = 3, seed: int = 3, kinds=(0, 1, 2, 3)) -> RtScene:

@@ -102,7 +102,7 @@ def parse_args(argv=None):
     p.add_argument("--no-extras", action="store_true", help="skip the render, batched and guided workloads")
     p.add_argument("--case", default=None,
                    choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tlas", "tune", "render",
-                            "batched", "guided", "guided_pass"],
+                            "batched", "guided", "guided_pass", "mlp_forward"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -112,7 +112,9 @@ def parse_args(argv=None):
     p.add_argument("--method", default="lbvh", choices=["lbvh", "hploc"],
                    help="--case wide / cwbvh8: binary builder under the wide tree")
     p.add_argument("--max-leaf", type=int, default=4, choices=[1, 2, 3, 4], help="--case wide leaf block size")
-    p.add_argument("--scene", default="spheres", choices=["spheres", "indirect"], help="--case guided scene")
+    p.add_argument("--scene", default="spheres", choices=["spheres", "indirect", "spheres_up", "door"],
+                   help="--case guided scene (spheres_up: the path-tracing workload with its light facing the "
+                        "ceiling)")
     p.add_argument("--width", type=int, default=1280, help="--case guided image width")
     p.add_argument("--height", type=int, default=720, help="--case guided image height")
     p.add_argument("--ref-spp", type=int, default=4096, help="--case guided reference samples per pixel")
@@ -1050,6 +1052,15 @@ def run_extras(args, local):
     return out
 
 
+def guided_scene(name):
+    from bajo_b200 import scenes
+    if name == "indirect":
+        return scenes.indirect_box_scene()
+    if name == "door":
+        return scenes.door_scene()
+    return scenes.spheres_in_box(light_up=name == "spheres_up")
+
+
 def run_guided(args):
     """Learned guiding against plain MIS at equal wall time.
 
@@ -1066,7 +1077,7 @@ def run_guided(args):
     from bajo_b200 import guide, rt, scenes
     stream = torch.cuda.current_stream()
     w, h = args.width, args.height
-    sc = scenes.indirect_box_scene() if args.scene == "indirect" else scenes.spheres_in_box()
+    sc = guided_scene(args.scene)
     gsc = rt.GpuRtTriangleScene(sc)
 
     def ev_time(fn):
@@ -1139,7 +1150,7 @@ def run_guided_pass(args):
     from bajo_b200 import guide, rt, scenes
     stream = torch.cuda.current_stream()
     w, h, spp = args.width, args.height, args.spp_per_pass
-    sc = scenes.indirect_box_scene() if args.scene == "indirect" else scenes.spheres_in_box()
+    sc = guided_scene(args.scene)
     gsc = rt.GpuRtTriangleScene(sc)
     gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=spp, record_capacity=1 << 18, batch=1 << 14,
                               steps=args.train_steps)
@@ -1211,6 +1222,21 @@ def run_case(args):
         out = run_guided(args)
     elif args.case == "guided_pass":
         out = run_guided_pass(args)
+    elif args.case == "mlp_forward":
+        # the guiding network's batched forward: mma.sync kernel and tcgen05 kernel
+        from bajo_b200 import guide
+        g = torch.Generator(device="cuda").manual_seed(0)
+        pos = torch.rand((n, 3), generator=g, device="cuda")
+        nrm = torch.nn.functional.normalize(torch.randn((n, 3), generator=g, device="cuda"), dim=1)
+        box = torch.tensor([0, 0, 0, 1, 1, 1], dtype=torch.float32, device="cuda")
+        net = guide.GuideNetwork("cuda", seed=0)
+        status = torch.zeros(1, dtype=torch.int32, device="cuda")
+        ms_mma = timed(lambda: net.forward(pos, nrm, box))
+        ms_tc = timed(lambda: net.forward(pos, nrm, box, tensor_memory=True, status=status))
+        flops = 2.0 * n * (3 * 64 * 64 + 32 * 64)  # the dense layers (output padded to 32)
+        out.update({"ms_mma_sync": round(ms_mma, 5), "ms_tcgen05": round(ms_tc, 5),
+                    "rows_s_mma_sync": round(n / ms_mma * 1e3, 1), "rows_s_tcgen05": round(n / ms_tc * 1e3, 1),
+                    "tflops_tcgen05": round(flops / ms_tc / 1e9, 2), "status": int(status.item())})
     elif args.case == "tune":
         out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
         out["device"] = autotune.device_key()

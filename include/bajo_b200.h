@@ -579,6 +579,15 @@ int32_t bajo_mlp_param_count(uint32_t* count);
  * 3 f32 each, box6 = [min xyz, max xyz]). */
 int32_t bajo_mlp_forward(const void* d_params16, const float* d_pos, const float* d_nrm, uint32_t n,
                          const float* d_box6, float* d_out20, void* stream);
+/* The same outputs from the 5th-generation tensor cores: 128-sample tiles per
+ * CTA, each layer four tcgen05.mma (FP16 in, FP32 accumulator in tensor
+ * memory) issued by one thread, read back with tcgen05.ld for the bias and
+ * ReLU.  Agrees with bajo_mlp_forward to FP32 accumulation order.  d_status
+ * (may be NULL) gets BAJO_STATUS_WAIT_TIMEOUT if the tensor cores never
+ * signal completion (the launch then stops after freeing its tensor memory).
+ * New on this path (no counterpart in the reference). */
+int32_t bajo_mlp_forward_tc(const void* d_params16, const float* d_pos, const float* d_nrm, uint32_t n,
+                            const float* d_box6, float* d_out20, uint32_t* d_status, void* stream);
 
 /* d_grad32 = gradient of sum_i -w_i log pdf_i(dir_i) w.r.t. the parameters
  * (overwritten); *d_loss (may be NULL) = that sum. */

@@ -52,6 +52,31 @@ def test_forward_matches_oracle(n):
     assert np.all(err <= 1e-2 + 1e-2 * np.abs(ref)), err.max()
 
 
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 1000, 40000, 300_001])
+def test_tensor_memory_forward(n):
+    """The tcgen05 forward: the oracle's tolerance, and the mma.sync forward's
+    outputs up to FP32 accumulation order."""
+    rng = np.random.default_rng(n + 7)
+    net, p64 = _net(2)
+    pos, nrm, _, _ = _batch(rng, n)
+    box = torch.from_numpy(BOX).cuda()
+    status = torch.zeros(1, dtype=torch.int32, device="cuda")
+    dp, dn = _dev(pos, nrm)
+    out = net.forward(dp, dn, box, tensor_memory=True, status=status)
+    base = net.forward(dp, dn, box)
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    out, base = out.cpu().numpy(), base.cpu().numpy()
+    assert np.all(np.isfinite(out))
+    if n <= 40000:
+        ref = oracle.mlp_forward(p64, pos, nrm, BOX)
+        err = np.abs(out - ref)
+        assert np.all(err <= 1e-2 + 1e-2 * np.abs(ref)), err.max()
+    # both kernels round every activation to FP16 the same way; only the FP32
+    # sums' order differs, which can flip an FP16 rounding of a hidden unit
+    assert np.abs(out - base).max() <= 5e-3 + 5e-3 * np.abs(base).max()
+
+
 @pytest.mark.parametrize("n", [1, 200, 3000])
 def test_gradient_matches_oracle(n):
     rng = np.random.default_rng(7 + n)
