@@ -337,169 +337,32 @@ cudaError_t launch_adam(float* p32, __half* p16, const float* grad, float* m, fl
 }
 
 // ---------------------------------------------------------------------------
-// Forward on the 5th-generation tensor cores (tcgen05): 128-row tiles, one CTA
-// of 128 threads.  Each layer is four tcgen05.mma (kind::f16, M = 128, N = 64
-// or 32, K = 16) issued by thread 0 from shared-memory operands into a tensor
-// memory accumulator; tcgen05.commit arrives on an mbarrier when they are done.
-// Then every warp reads its 32 rows of the accumulator (tcgen05.ld 32x32b),
-// adds the bias, applies ReLU and writes the next layer's FP16 operand in
-// place.  Operands use the canonical interleaved (no swizzle) K-major layout:
-// 8 x 8 core matrices of 128 bytes, the cores of one 8-row group side by side
-// along K, so the leading (K) byte offset is 128 and the stride (8-row) byte
-// offset is 8 x 128 for a 64-wide K.
+// Forward on the 5th-generation tensor cores (tcgen05): tc::forward (mlp.cuh)
+// over 128-row tiles, one CTA of 128 threads per resident slot.
 // ---------------------------------------------------------------------------
 namespace tc {
 
-constexpr int kThreads = 128, kRows = 128;
-constexpr uint32_t kTmemCols = 64;  // one layer's FP32 accumulator (N <= 64)
-constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
-
-// byte offset of element (r, k) of an [rows][64] FP16 operand in core layout
-__device__ __forceinline__ uint32_t core_off(int r, int k) {
-  return (uint32_t)((((r >> 3) << 3) + (k >> 3)) * 128 + ((r & 7) << 4) + ((k & 7) << 1));
-}
-// shared-memory matrix descriptor: start >> 4, leading byte offset 128 >> 4,
-// stride byte offset 1024 >> 4, descriptor version 1 (bit 46), no swizzle
-__device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
-         (1ull << 46);
-}
-// instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B FP16
-// (bits 7-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at
-// bit 24
-__host__ __device__ constexpr uint32_t instr_desc(uint32_t n) {
-  return (1u << 4) | ((n >> 3) << 17) | ((uint32_t)(kRows >> 4) << 24);
-}
-
-__device__ __forceinline__ uint32_t saddr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mma_f16(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}" ::"r"(tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-__device__ __forceinline__ bool bar_try_wait(uint32_t bar, uint32_t parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-__device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {  // at most kWaitNs
-  if (bar_try_wait(bar, parity)) return true;
-  const uint64_t t0 = global_timer_ns();
-  while (!bar_try_wait(bar, parity))
-    if (global_timer_ns() - t0 > kWaitNs) return false;
-  return true;
-}
-// 16 consecutive FP32 accumulator columns of this thread's row
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-#pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
-}
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-// generic-proxy writes to shared memory, before the tensor cores read them
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-struct __align__(128) Smem {
-  __half w[3][kHid * kIn];  // hidden layers [out][in], core layout
-  __half w4[kOutPad * kIn];  // output layer
-  __half a[kRows * kIn];     // the tile's features, then each hidden layer's activations
-  float b[3][kHid];
-  float b4[kOutPad];
+struct __align__(128) FwdSmem {
+  Weights w;
+  __half a[kRows * kIn];  // the tile's features, activations, then staged outputs
   unsigned long long bar;
   uint32_t tmem;
 };
 
-// the 64 one-blob features of one sample as 32 FP16 pairs
-__device__ __forceinline__ void encode_pairs(const float* p, const float* n, const float* box, uint32_t f[32]) {
-#pragma unroll
-  for (int grp = 0; grp < 5; ++grp) {
-    float v;
-    int bins, col;
-    if (grp < 3) {
-      const float ext = box[3 + grp] - box[grp];
-      v = ext > 0.0f ? (p[grp] - box[grp]) / ext : 0.5f;
-      bins = kPosBins;
-      col = grp * kPosBins;
-    } else {
-      float u, w;
-      octahedral(n[0], n[1], n[2], u, w);
-      v = grp == 3 ? u : w;
-      bins = kDirBins;
-      col = 3 * kPosBins + (grp - 3) * kDirBins;
-    }
-    int i0, i1;
-    float fr;
-    blob_bins(v, bins, i0, i1, fr);
-#pragma unroll
-    for (int k = 0; k < kPosBins; k += 2)
-      if (k < bins) f[(col + k) >> 1] = pack_h2(blob_value(k, i0, i1, fr), blob_value(k + 1, i0, i1, fr));
-  }
-}
-
-__global__ void __launch_bounds__(kThreads) forward_tc_kernel(const __half* __restrict__ p16,
+__global__ void __launch_bounds__(kRows) forward_tc_kernel(const __half* __restrict__ p16,
                                                              const float* __restrict__ pos,
                                                              const float* __restrict__ nrm, const float* box,
                                                              uint32_t n, float* __restrict__ out20,
                                                              uint32_t* __restrict__ status) {
   extern __shared__ __align__(128) unsigned char raw[];
-  Smem& s = *reinterpret_cast<Smem*>(raw);
-  const int tid = threadIdx.x, warp = tid >> 5;
-  // weights into core layout (pairs of inputs), biases
-  const uint32_t* src = reinterpret_cast<const uint32_t*>(p16);
-  for (int i = tid; i < kHid * kIn / 2; i += kThreads) {
-    const int o = (2 * i) / kIn, k = (2 * i) % kIn;
-#pragma unroll
-    for (int l = 0; l < 3; ++l)
-      *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w[l]) + core_off(o, k)) = src[kOffW(l) / 2 + i];
-  }
-  for (int i = tid; i < kOutPad * kIn / 2; i += kThreads) {
-    const int o = (2 * i) / kIn, k = (2 * i) % kIn;
-    *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w4) + core_off(o, k)) = src[kOffW(3) / 2 + i];
-  }
-  for (int i = tid; i < kHid; i += kThreads)
-    for (int l = 0; l < 3; ++l) s.b[l][i] = __half2float(p16[kOffB(l) + i]);
-  for (int i = tid; i < kOutPad; i += kThreads) s.b4[i] = __half2float(p16[kOffB(3) + i]);
+  FwdSmem& s = *reinterpret_cast<FwdSmem*>(raw);
+  const int tid = threadIdx.x;
+  load_weights<kRows>(s.w, p16);
   const uint32_t bar = saddr(&s.bar);
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  }
-  if (warp == 0) {  // the accumulator's tensor memory, held to the end
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(&s.tmem)),
-                 "r"(kTmemCols)
-                 : "memory");
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-  }
-  fence_async_smem();
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  const uint32_t tmem = s.tmem;
-  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);  // this warp's 32 lanes
-  const uint32_t a_addr = saddr(s.a), w4_addr = saddr(s.w4);
+  const uint32_t tmem = setup<1>(bar, &s.tmem);
   uint32_t phase = 0;
-  bool failed = false;  // the same in every thread
   unsigned char* const abytes = reinterpret_cast<unsigned char*>(s.a);
-
-  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < n && !failed; base += (uint64_t)gridDim.x * kRows) {
-    // features of row tid
+  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < n; base += (uint64_t)gridDim.x * kRows) {
     {
       uint32_t f[32];
       const uint64_t i = base + tid;
@@ -511,73 +374,21 @@ __global__ void __launch_bounds__(kThreads) forward_tc_kernel(const __half* __re
 #pragma unroll
         for (int j = 0; j < 32; ++j) f[j] = 0u;
       }
-#pragma unroll
-      for (int q = 0; q < 8; ++q)  // 8 features = one 16-byte row of a core matrix
-        *reinterpret_cast<uint4*>(abytes + core_off(tid, 8 * q)) =
-            make_uint4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+      store_features(abytes, tid, f);
     }
-    for (int l = 0; l < 4; ++l) {
-      const uint32_t nn = l < 3 ? (uint32_t)kHid : (uint32_t)kOutPad;
-      fence_async_smem();
-      fence_before_sync();
-      __syncthreads();  // the operand is written; the previous layer's accumulator is read
-      fence_after_sync();
-      if (tid == 0) {
-        const uint32_t w_addr = l < 3 ? saddr(s.w[l]) : w4_addr;
+    float o[kOut];
+    if (!forward<1>(s.w, abytes, tmem, bar, phase, o, status)) break;
+    // the tile's outputs, staged row-major in the (now unread) operand buffer
+    // and written out coalesced
+    float* stage = reinterpret_cast<float*>(s.a);
 #pragma unroll
-        for (int ks = 0; ks < kIn / 16; ++ks)  // K = 16 per instruction: two cores along K
-          mma_f16(tmem, smem_desc(a_addr + 256u * ks), smem_desc(w_addr + 256u * ks), instr_desc(nn), ks > 0);
-        commit(bar);
-      }
-      const bool done = bar_wait(bar, phase);
-      if (__syncthreads_or(!done)) {  // the tensor cores never signalled: give up the launch
-        if (tid == 0) raise_status(status, BAJO_STATUS_WAIT_TIMEOUT);
-        bar_wait(bar, phase);  // once more, so no MMA is in flight when the memory is freed
-        failed = true;
-        break;
-      }
-      phase ^= 1u;
-      fence_after_sync();
-      const int r = tid;  // this thread's row = its accumulator lane
-      if (l < 3) {
-#pragma unroll
-        for (int c0 = 0; c0 < kHid; c0 += 16) {
-          float v[16];
-          tmem_ld16(trow + (uint32_t)c0, v);
-          tmem_wait_ld();
-          uint32_t h[8];
-#pragma unroll
-          for (int j = 0; j < 16; j += 2)
-            h[j >> 1] = pack_h2(fmaxf(v[j] + s.b[l][c0 + j], 0.0f), fmaxf(v[j + 1] + s.b[l][c0 + j + 1], 0.0f));
-          *reinterpret_cast<uint4*>(abytes + core_off(r, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4*>(abytes + core_off(r, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
-        }
-      } else {
-        float v[32];
-        tmem_ld16(trow, v);
-        tmem_ld16(trow + 16u, v + 16);
-        tmem_wait_ld();
-        // the tile's outputs, staged row-major in the (now unread) operand
-        // buffer and written out coalesced below
-        float* stage = reinterpret_cast<float*>(s.a);
-#pragma unroll
-        for (int c = 0; c < kOut; ++c) stage[r * kOut + c] = v[c] + s.b4[c];
-      }
-    }
-    if (failed) break;
+    for (int c = 0; c < kOut; ++c) stage[tid * kOut + c] = o[c];
     __syncthreads();
-    {
-      const float* stage = reinterpret_cast<const float*>(s.a);
-      const uint64_t rows = min((uint64_t)kRows, (uint64_t)n - base);
-      for (uint32_t k = tid; k < rows * kOut; k += kThreads) out20[base * kOut + k] = stage[k];
-    }
+    const uint64_t rows = min((uint64_t)kRows, (uint64_t)n - base);
+    for (uint32_t k = tid; k < rows * kOut; k += kRows) out20[base * kOut + k] = stage[k];
     __syncthreads();  // the next tile's features overwrite the staged outputs
   }
-  fence_before_sync();
-  __syncthreads();
-  fence_after_sync();
-  if (warp == 0)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+  teardown<1>(tmem);
 }
 
 }  // namespace tc
@@ -613,7 +424,7 @@ int32_t bajo_mlp_forward_tc(const void* d_params16, const float* d_pos, const fl
   using namespace bajo::mlp;
   if (!d_params16 || !d_box6 || (n && (!d_pos || !d_nrm || !d_out20))) return BAJO_ERR_INVALID_ARGUMENT;
   if (n == 0) return BAJO_OK;
-  const size_t smem = sizeof(tc::Smem);
+  const size_t smem = sizeof(tc::FwdSmem);
   if (cudaFuncSetAttribute(tc::forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return BAJO_ERR_CUDA;
@@ -631,7 +442,7 @@ int32_t bajo_mlp_forward_tc(const void* d_params16, const float* d_pos, const fl
   }
   uint64_t grid = ((uint64_t)n + tc::kRows - 1) / tc::kRows;
   if (grid > (uint64_t)per_sm[dev] * bajo::sm_count()) grid = (uint64_t)per_sm[dev] * bajo::sm_count();
-  tc::forward_tc_kernel<<<(uint32_t)grid, tc::kThreads, smem, (cudaStream_t)stream>>>(
+  tc::forward_tc_kernel<<<(uint32_t)grid, tc::kRows, smem, (cudaStream_t)stream>>>(
       (const __half*)d_params16, d_pos, d_nrm, d_box6, n, d_out20, d_status);
   return cudaGetLastError() == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }

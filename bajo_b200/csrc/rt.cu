@@ -693,53 +693,57 @@ __global__ void __launch_bounds__(kBlock) material_kernel(SceneView sc, Queues q
   }
 }
 
-struct ShadeSmem {
-  mlp::Net net;
-  mlp::WarpTile tile[kShadeThreads / 32];
+struct __align__(128) ShadeSmem {
+  mlp::tc::Weights w;
+  __half act[2 * mlp::tc::kRows * mlp::kIn];  // two 128-vertex tiles in core layout
+  unsigned long long bar;
+  uint32_t tmem;
 };
 
-// Guided shading.  Warp-autonomous: each warp takes 32 vertices, encodes one
-// per lane, runs the network on its 32 rows (two m16 tiles on the tensor
-// cores), then every lane shades its own vertex; only the weight load is
-// block-wide.
+// Guided shading.  Every CTA takes 256 vertices per step: each thread encodes
+// one, the network runs on the two 128-row tiles on the 5th-generation
+// tensor cores (mlp::tc::forward: tcgen05.mma into tensor memory), and each
+// thread then shades its own vertex from its row's 20 outputs.
 __global__ void __launch_bounds__(kShadeThreads, 2) guided_shade_kernel(SceneView sc, Queues q, ShadeCtx c,
                                                                         uint32_t bounce, uint32_t max_depth,
                                                                         uint32_t sample_base, uint64_t seed) {
-  extern __shared__ __align__(16) unsigned char raw[];
+  static_assert(kShadeThreads == 2 * mlp::tc::kRows, "two network tiles per step");
+  extern __shared__ __align__(128) unsigned char raw[];
   ShadeSmem& s = *reinterpret_cast<ShadeSmem*>(raw);
-  mlp::load_net<kShadeThreads>(s.net, c.params16);
-  __syncthreads();
+  mlp::tc::load_weights<kShadeThreads>(s.w, c.params16);
+  const uint32_t bar = mlp::tc::saddr(&s.bar);
+  const uint32_t tmem = mlp::tc::setup<2>(bar, &s.tmem);
+  uint32_t phase = 0;
   const uint32_t cap = q.capacity;
   const uint32_t count = min(c.vcount[bounce], cap);
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  mlp::WarpTile& tile = s.tile[warp];
-  const uint32_t warps = gridDim.x * (kShadeThreads / 32);
-  for (uint32_t base = (blockIdx.x * (kShadeThreads / 32) + warp) * 32; base < count; base += warps * 32) {
-    const uint32_t i = base + lane;
+  const int tid = threadIdx.x;
+  unsigned char* const act = reinterpret_cast<unsigned char*>(s.act);
+  unsigned char* const mine = act + (size_t)(tid / mlp::tc::kRows) * mlp::tc::kRows * mlp::kIn * 2;
+  for (uint32_t base = blockIdx.x * kShadeThreads; base < count; base += gridDim.x * kShadeThreads) {
+    const uint32_t i = base + tid;
     {
-      __half* row = tile.x + lane * mlp::kLd;
+      uint32_t f[32];
       if (i < count) {
         const float p[3] = {c.vtx[0 * cap + i], c.vtx[1 * cap + i], c.vtx[2 * cap + i]};
         const float n[3] = {c.vtx[3 * cap + i], c.vtx[4 * cap + i], c.vtx[5 * cap + i]};
-        mlp::encode_row(p, n, c.box, row);
+        mlp::tc::encode_pairs(p, n, c.box, f);
       } else {
-        for (int k = 0; k < mlp::kIn; k += 2) mlp::st32(row + k, 0u);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) f[j] = 0u;
       }
+      mlp::tc::store_features(mine, tid % mlp::tc::kRows, f);
     }
-    __syncwarp();
-    // one m16 tile at a time: two at once spill under the 128-register cap
-    mlp::forward_tile<1>(s.net, tile.x, 0, nullptr, tile.out);
-    mlp::forward_tile<1>(s.net, tile.x, 16, nullptr, tile.out);
-    __syncwarp();
+    float out[mlp::kOut];
+    if (!mlp::tc::forward<2>(s.w, act, tmem, bar, phase, out, q.status)) break;
     ShadeOut o;
     if (i < count) {
       mlp::Mixture mix;
-      mlp::mixture_from_outputs(&tile.out[lane * mlp::kOutLd], mix);
+      mlp::mixture_from_outputs(out, mix);
       shade_vertex<BAJO_RENDER_GUIDED>(sc, c, cap, i, bounce, max_depth, seed, mix, o);
     }
     emit<BAJO_RENDER_GUIDED>(q, c, bounce, sample_base, o);
-    __syncwarp();
   }
+  mlp::tc::teardown<2>(tmem);
 }
 
 // ---------------------------------------------------------------------------
@@ -1100,11 +1104,15 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   if (cudaFuncSetAttribute(guided_shade_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return BAJO_ERR_CUDA;
-  int per_sm = 0;
+  // resident CTAs per SM: shared memory bounds them, and so does tensor
+  // memory (128 of an SM's 512 columns per CTA)
+  int per_sm = 0, sm_bytes = 0, dev = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, guided_shade_kernel, kShadeThreads, smem) !=
           cudaSuccess ||
-      per_sm < 1)
+      cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sm_bytes, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess)
     return BAJO_ERR_CUDA;
+  per_sm = max(1, min(4, sm_bytes / (int)(smem + 1024)));
   uint32_t shade_grid = (L.cap + kShadeThreads - 1) / kShadeThreads;
   const uint32_t shade_max = (uint32_t)(sm_count() * per_sm);
   if (shade_grid > shade_max) shade_grid = shade_max;
