@@ -344,7 +344,7 @@ namespace tc {
 
 struct __align__(128) FwdSmem {
   Weights w;
-  __half a[kRows * kIn];  // the tile's features, activations, then staged outputs
+  __half a[kRows * kK];  // the tile's features, activations, then staged outputs
   unsigned long long bar;
   uint32_t tmem;
 };

@@ -257,30 +257,38 @@ struct WarpTile {
 // The network on the 5th-generation tensor cores (tcgen05), used by the
 // batched forward (mlp.cu) and the guided shading kernel (rt.cu).  NT tiles of
 // 128 rows per CTA of 128 NT threads: thread t owns row t % 128 of tile t /
-// 128.  Each layer is four tcgen05.mma per tile (kind::f16, M = 128, N = 64 or
+// 128.  Each layer is five tcgen05.mma per tile (kind::f16, M = 128, N = 64 or
 // 32, K = 16; FP16 operands in shared memory, FP32 accumulator in tensor
 // memory) issued by thread 0 and committed to one mbarrier; then every warp
-// reads its 32 accumulator lanes (tcgen05.ld 32x32b), adds the bias, applies
-// ReLU and writes the next layer's operand in place.  Operands use the
-// canonical interleaved (no swizzle) K-major layout: 8 x 8 core matrices of
-// 128 bytes, the cores of one 8-row group side by side along K, so the
-// leading (K) byte offset is 128 and the stride (8-row) byte offset 1,024.
+// reads its 32 accumulator lanes (tcgen05.ld 32x32b), applies ReLU while it
+// packs to FP16 (cvt.rn.relu.f16x2.f32) and writes the next layer's operand
+// in place.  The biases ride in the MMA: every operand row carries a
+// constant 1 in column 64 (columns 65-79 zero) and every weight row its bias
+// there, so K = 80 and the epilogue adds nothing (the biases are FP16 values,
+// so 1 x bias is exact in the FP32 sum).  Operands use the canonical
+// interleaved (no swizzle) K-major layout: 8 x 8 core matrices of 128 bytes,
+// the 10 cores of one 8-row group side by side along K, so the leading (K)
+// byte offset is 128 and the stride (8-row) byte offset 1,280.
 // ---------------------------------------------------------------------------
 namespace tc {
 
 constexpr int kRows = 128;
-constexpr uint32_t kColsPerTile = 64;  // one layer's FP32 accumulator (N <= 64)
+constexpr int kK = 80;                          // 64 inputs, the constant 1, zero padding
+constexpr int kKCores = kK / 8;                 // core matrices along K
+constexpr uint32_t kTileBytes = kRows * kK * 2;  // one operand tile
+constexpr uint32_t kColsPerTile = 64;           // one layer's FP32 accumulator (N <= 64)
 constexpr uint64_t kWaitNs = 200ull * 1000ull * 1000ull;
 
-// byte offset of element (r, k) of an [rows][64] FP16 operand in core layout
+// byte offset of element (r, k) of an [rows][kK] FP16 operand in core layout
 __device__ __forceinline__ uint32_t core_off(int r, int k) {
-  return (uint32_t)((((r >> 3) << 3) + (k >> 3)) * 128 + ((r & 7) << 4) + ((k & 7) << 1));
+  return (uint32_t)(((r >> 3) * kKCores + (k >> 3)) * 128 + ((r & 7) << 4) + ((k & 7) << 1));
 }
 // shared-memory matrix descriptor: start >> 4, leading byte offset 128 >> 4,
-// stride byte offset 1024 >> 4, descriptor version 1 (bit 46), no swizzle
+// stride byte offset (kKCores x 128) >> 4, descriptor version 1 (bit 46), no
+// swizzle
 __device__ __forceinline__ uint64_t smem_desc(uint32_t saddr) {
-  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(1024u >> 4) << 32) |
-         (1ull << 46);
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) |
+         ((uint64_t)((kKCores * 128u) >> 4) << 32) | (1ull << 46);
 }
 // instruction descriptor of kind::f16: D FP32 (bits 4-5 = 1), A and B FP16
 // (bits 7-12 = 0), both K-major (bits 15, 16 = 0), N >> 3 at bit 17, M >> 4 at
@@ -316,47 +324,54 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {  // at
     if (global_timer_ns() - t0 > kWaitNs) return false;
   return true;
 }
-// 16 consecutive FP32 accumulator columns of this thread's lane
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16]) {
-  uint32_t r[16];
+// 16 consecutive FP32 accumulator columns of this thread's lane (raw bits)
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16]) {
   asm volatile(
       "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
         "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
       : "r"(taddr));
-#pragma unroll
-  for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // generic-proxy writes to shared memory, before the tensor cores read them
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+// max(lo, 0) and max(hi, 0) rounded to FP16 and packed (lo in the low half)
+__device__ __forceinline__ uint32_t relu_pack(uint32_t lo, uint32_t hi) {
+  uint32_t d;
+  asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(d) : "r"(hi), "r"(lo));
+  return d;
+}
 
-// The network's weights in core layout and its biases in FP32.
+// The network's weights in core layout, each row's bias in column 64.
 struct __align__(128) Weights {
-  __half w[3][kHid * kIn];   // hidden layers [out][in]
-  __half w4[kOutPad * kIn];  // output layer
-  float b[3][kHid];
-  float b4[kOutPad];
+  __half w[3][kHid * kK];   // hidden layers [out][in | bias | 0]
+  __half w4[kOutPad * kK];  // output layer
 };
 
 template <int THREADS>
 __device__ void load_weights(Weights& s, const __half* __restrict__ p16) {
   const uint32_t* src = reinterpret_cast<const uint32_t*>(p16);
-  for (int i = threadIdx.x; i < kHid * kIn / 2; i += THREADS) {
-    const int o = (2 * i) / kIn, k = (2 * i) % kIn;
+  for (int i = threadIdx.x; i < kHid * kK / 2; i += THREADS) {
+    const int o = (2 * i) / kK, k = (2 * i) % kK;  // pairs (k, k + 1) of row o
 #pragma unroll
-    for (int l = 0; l < 3; ++l)
-      *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w[l]) + core_off(o, k)) = src[kOffW(l) / 2 + i];
+    for (int l = 0; l < 3; ++l) {
+      uint32_t v;
+      if (k < kIn) v = src[(kOffW(l) + o * kIn + k) / 2];
+      else if (k == kIn) v = (uint32_t)__half_as_ushort(p16[kOffB(l) + o]);  // (bias, 0)
+      else v = 0u;
+      *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w[l]) + core_off(o, k)) = v;
+    }
   }
-  for (int i = threadIdx.x; i < kOutPad * kIn / 2; i += THREADS) {
-    const int o = (2 * i) / kIn, k = (2 * i) % kIn;
-    *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w4) + core_off(o, k)) = src[kOffW(3) / 2 + i];
+  for (int i = threadIdx.x; i < kOutPad * kK / 2; i += THREADS) {
+    const int o = (2 * i) / kK, k = (2 * i) % kK;
+    uint32_t v;
+    if (k < kIn) v = src[(kOffW(3) + o * kIn + k) / 2];
+    else if (k == kIn) v = (uint32_t)__half_as_ushort(p16[kOffB(3) + o]);
+    else v = 0u;
+    *reinterpret_cast<uint32_t*>(reinterpret_cast<unsigned char*>(s.w4) + core_off(o, k)) = v;
   }
-  for (int i = threadIdx.x; i < kHid; i += THREADS)
-    for (int l = 0; l < 3; ++l) s.b[l][i] = __half2float(p16[kOffB(l) + i]);
-  for (int i = threadIdx.x; i < kOutPad; i += THREADS) s.b4[i] = __half2float(p16[kOffB(3) + i]);
 }
 
 // The 64 one-blob features of one sample as 32 FP16 pairs.
@@ -385,11 +400,14 @@ __device__ __forceinline__ void encode_pairs(const float* p, const float* n, con
       if (k < bins) f[(col + k) >> 1] = pack_h2(blob_value(k, i0, i1, fr), blob_value(k + 1, i0, i1, fr));
   }
 }
-// row r's features into a tile in core layout: one 16-byte store per 8
+// row r's features into a tile in core layout (one 16-byte store per 8),
+// with the constant 1 in column 64 and zeros up to 79
 __device__ __forceinline__ void store_features(unsigned char* tile, int r, const uint32_t f[32]) {
 #pragma unroll
   for (int q = 0; q < 8; ++q)
     *reinterpret_cast<uint4*>(tile + core_off(r, 8 * q)) = make_uint4(f[4 * q], f[4 * q + 1], f[4 * q + 2], f[4 * q + 3]);
+  *reinterpret_cast<uint4*>(tile + core_off(r, kIn)) = make_uint4(0x3C00u, 0u, 0u, 0u);  // FP16 1.0, zeros
+  *reinterpret_cast<uint4*>(tile + core_off(r, kIn + 8)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
 // Prologue of a CTA of 128 NT threads: the mbarrier (count 1) and NT x 64
@@ -424,18 +442,18 @@ __device__ __forceinline__ void teardown(uint32_t tmem) {
                  : "memory");
 }
 
-// The network on the NT tiles at `act` (each kRows x 64 FP16 in core layout,
-// 16 KB apart, features already written by their row threads); the calling
-// thread's row's 20 outputs land in `out`.  Every thread must call it; false
-// (in every thread) when the tensor cores never signalled completion (status
-// bit raised, the launch should stop).
+// The network on the NT tiles at `act` (kTileBytes apart, features already
+// written by their row threads); the calling thread's row's 20 outputs land
+// in `out`.  Every thread must call it; false (in every thread) when the
+// tensor cores never signalled completion (status bit raised, the launch
+// should stop).
 template <int NT>
 __device__ __forceinline__ bool forward(const Weights& w, unsigned char* act, uint32_t tmem, uint32_t bar,
                                         uint32_t& phase, float out[kOut], uint32_t* status) {
   const int tid = threadIdx.x, warp = tid >> 5;
   const int tile = tid / kRows, r = tid % kRows;
   const uint32_t trow = tmem + ((uint32_t)(32 * (warp & 3)) << 16) + (uint32_t)tile * kColsPerTile;
-  unsigned char* const mine = act + (size_t)tile * kRows * kIn * 2;
+  unsigned char* const mine = act + (size_t)tile * kTileBytes;
   const uint32_t act_addr = saddr(act);
 #pragma unroll 1
   for (int l = 0; l < 4; ++l) {
@@ -449,8 +467,8 @@ __device__ __forceinline__ bool forward(const Weights& w, unsigned char* act, ui
 #pragma unroll
       for (int t = 0; t < NT; ++t)
 #pragma unroll
-        for (int ks = 0; ks < kIn / 16; ++ks)  // K = 16 per instruction: two cores along K
-          mma_f16(tmem + (uint32_t)t * kColsPerTile, smem_desc(act_addr + (uint32_t)t * kRows * kIn * 2 + 256u * ks),
+        for (int ks = 0; ks < kK / 16; ++ks)  // K = 16 per instruction: two cores along K
+          mma_f16(tmem + (uint32_t)t * kColsPerTile, smem_desc(act_addr + (uint32_t)t * kTileBytes + 256u * ks),
                   smem_desc(w_addr + 256u * ks), instr_desc(nn), ks > 0);
       commit(bar);
     }
@@ -465,23 +483,22 @@ __device__ __forceinline__ bool forward(const Weights& w, unsigned char* act, ui
     if (l < 3) {
 #pragma unroll
       for (int c0 = 0; c0 < kHid; c0 += 16) {
-        float v[16];
+        uint32_t v[16];
         tmem_ld16(trow + (uint32_t)c0, v);
         tmem_wait_ld();
         uint32_t h[8];
 #pragma unroll
-        for (int j = 0; j < 16; j += 2)
-          h[j >> 1] = pack_h2(fmaxf(v[j] + w.b[l][c0 + j], 0.0f), fmaxf(v[j + 1] + w.b[l][c0 + j + 1], 0.0f));
+        for (int j = 0; j < 8; ++j) h[j] = relu_pack(v[2 * j], v[2 * j + 1]);
         *reinterpret_cast<uint4*>(mine + core_off(r, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
         *reinterpret_cast<uint4*>(mine + core_off(r, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
       }
     } else {
-      float v[32];
+      uint32_t v[32];
       tmem_ld16(trow, v);
       tmem_ld16(trow + 16u, v + 16);
       tmem_wait_ld();
 #pragma unroll
-      for (int c = 0; c < kOut; ++c) out[c] = v[c] + w.b4[c];
+      for (int c = 0; c < kOut; ++c) out[c] = __uint_as_float(v[c]);
     }
   }
   fence_before_sync();

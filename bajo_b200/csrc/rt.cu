@@ -695,7 +695,7 @@ __global__ void __launch_bounds__(kBlock) material_kernel(SceneView sc, Queues q
 
 struct __align__(128) ShadeSmem {
   mlp::tc::Weights w;
-  __half act[2 * mlp::tc::kRows * mlp::kIn];  // two 128-vertex tiles in core layout
+  __half act[2 * mlp::tc::kRows * mlp::tc::kK];  // two 128-vertex tiles in core layout
   unsigned long long bar;
   uint32_t tmem;
 };
@@ -718,7 +718,7 @@ __global__ void __launch_bounds__(kShadeThreads, 2) guided_shade_kernel(SceneVie
   const uint32_t count = min(c.vcount[bounce], cap);
   const int tid = threadIdx.x;
   unsigned char* const act = reinterpret_cast<unsigned char*>(s.act);
-  unsigned char* const mine = act + (size_t)(tid / mlp::tc::kRows) * mlp::tc::kRows * mlp::kIn * 2;
+  unsigned char* const mine = act + (size_t)(tid / mlp::tc::kRows) * mlp::tc::kTileBytes;
   for (uint32_t base = blockIdx.x * kShadeThreads; base < count; base += gridDim.x * kShadeThreads) {
     const uint32_t i = base + tid;
     {

@@ -121,7 +121,10 @@ def parse_args(argv=None):
     p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
     p.add_argument("--spp", type=int, default=64, help="--case render samples per pixel")
     p.add_argument("--scenes", type=int, default=4096, help="--case batched scene count")
-    p.add_argument("--train-passes", type=int, default=16, help="--case guided passes followed by training")
+    p.add_argument("--train-passes", type=int, default=6, help="--case guided passes followed by training")
+    p.add_argument("--first-guided", action="store_true",
+                   help="--case guided: guide the first pass too (by default it samples the BSDF only, since the "
+                        "network is untrained)")
     p.add_argument("--train-steps", type=int, default=32, help="--case guided Adam steps per training pass")
     return p.parse_args(argv)
 
@@ -1049,6 +1052,14 @@ def run_extras(args, local):
         r = run_guided(gargs)
     r["clocks"] = ck.summary()
     out["guided_indirect"] = r
+    # and on the path-tracing workload's geometry with its light turned to
+    # face the ceiling: 1.31M triangles, so a guided sample costs little
+    # more than a plain one, and all light is indirect
+    gargs = parse_args(["--scene", "spheres_up"])
+    with ClockSampler(local) as ck:
+        r = run_guided(gargs)
+    r["clocks"] = ck.summary()
+    out["guided_spheres_up"] = r
     return out
 
 
@@ -1070,6 +1081,8 @@ def run_guided(args):
     accumulated in FP64.  Plain: one 64-spp MIS render, device-timed.
     Guided: progressive passes of ``--spp-per-pass`` with the network trained
     after each of the first ``--train-passes`` passes (training time counted);
+    the first pass samples the BSDF only (``--first-guided`` guides it too),
+    since an untrained network only adds variance;
     after each pass the cumulative device time and the MSE (computed outside
     the timed region) are logged until the guided image is at least as good
     as the plain one or twice the plain time has passed."""
@@ -1114,7 +1127,8 @@ def run_guided(args):
     k = 0
     while t_g < 2.0 * t_plain and k < 4096:
         train = k < args.train_passes
-        t, _ = ev_time(lambda: gr.render_pass(70001 + 7919 * k, train=train))
+        frac = 0.0 if (k == 0 and not args.first_guided) else None  # the untrained network guides nothing
+        t, _ = ev_time(lambda: gr.render_pass(70001 + 7919 * k, train=train, guide_fraction=frac))
         t_g += t
         k += 1
         mse = float(((gr.image() - ref) ** 2).mean())
@@ -1138,6 +1152,7 @@ def run_guided(args):
            "plain_samples_s": round(w * h * 64 / t_plain * 1e3, 1),
            "guided_mrays_s": round((rays + shadows) / t_pass / 1e3, 1),
            "train_passes": args.train_passes, "spp_per_pass": args.spp_per_pass, "train_steps": args.train_steps,
+           "first_pass_guided": bool(args.first_guided),
            "log": log[:: max(1, len(log) // 40)], "status": gr.workspace.status()}
     return out
 

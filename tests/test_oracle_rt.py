@@ -105,3 +105,23 @@ def test_path_nee_mis_are_unbiased(oracle):
     (ma, sa), (mb, sb) = res[3], res[4]
     z = np.abs(ma - mb) / np.sqrt(sa ** 2 + sb ** 2 + 1e-12)
     assert (z > 4).mean() < 0.01
+
+
+def test_guiding_scene_variants():
+    """The indirectly lit scenes of the guiding comparisons: the sphere
+    workload with its light turned to face the ceiling (same geometry), and
+    the two-room door scene."""
+    from bajo_b200 import scenes
+    base = scenes.spheres_in_box()
+    up = scenes.spheres_in_box(light_up=True)
+    assert up.vertices.shape == base.vertices.shape
+    tri = up.vertices.reshape(-1, 3, 3).astype(np.float64)
+    light = tri[12:14]  # the light quad follows the 12 box triangles
+    nrm = np.cross(light[:, 1] - light[:, 0], light[:, 2] - light[:, 0])
+    assert np.all(nrm[:, 1] > 0) and np.allclose(light[:, :, 1], 0.85)
+    assert float(up.emissives.ravel()[0]) == 4 * float(base.emissives.ravel()[0])
+    door = scenes.door_scene()
+    t = door.vertices.reshape(-1, 3, 3)
+    assert np.all((t >= -1e-6) & (t <= 1 + 1e-6))
+    wall = t[12:18]
+    assert np.allclose(wall[:, :, 2], 0.5)
