@@ -172,6 +172,7 @@ SIGNATURES = {
     "bajo_mlp_forward": (_I32, [_P, _P, _P, _U32, _P, _P, _P]),
     "bajo_mlp_forward_tc": (_I32, [_P, _P, _P, _U32, _P, _P, _P, _P]),
     "bajo_mlp_grad": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P]),
+    "bajo_mlp_grad_tc": (_I32, [_P, _P, _P, _P, _P, _U32, _P, _P, _P, _P, _P]),
     "bajo_mlp_adam": (_I32, [_P, _P, _P, _P, _P, _U32, _F, _F, _F, _F, _F, _P]),
     "bajo_guide_records_size": (_I32, [_U32, ctypes.POINTER(_SZ)]),
     "bajo_render_guided": (_I32, [_P, _P, _P, _P, _P, _P, _P, _SZ, _P]),

@@ -391,6 +391,299 @@ __global__ void __launch_bounds__(kRows) forward_tc_kernel(const __half* __restr
   teardown<1>(tmem);
 }
 
+// ---------------------------------------------------------------------------
+// Gradient of sum_j -w_j log pdf_j(dir_j) on the tensor cores.  Per 128-row
+// tile: the forward with every layer's input A_l kept in shared memory
+// (A_0 = the features), D_3 = dL/dout per row, then for l = 3..0
+//   dW_l += D_l^T A_l   (M = 64 outputs, N = 80: 64 inputs, the column of
+//                        ones (its bias) and zeros, K = 128 rows)
+//   dA_l  = D_l W_l     (M = 128 rows, N = 64 inputs, K = outputs of l; l > 0)
+//   D_{l-1} = dA_l where A_l > 0.
+// The same shared-memory tiles serve both products.  A core matrix of a
+// [rows][features] tile holds 8 rows x 8 features, the 8 features of a row
+// in 16 contiguous bytes: K-major when the rows are M (the forward, dA_l),
+// MN-major when the rows are K (dW_l).  Likewise the weights' [out][in] tiles
+// are K-major with N = out (forward) and MN-major with N = in (dA_l).
+// The weight gradients accumulate in tensor memory over all of the CTA's
+// tiles (an M = 64 accumulator holds row 16 q + i in lane 32 q + i) and are
+// added to the global gradient once, unscaled, at the end.
+// ---------------------------------------------------------------------------
+constexpr int kDCols = 64;                           // columns of the D tiles (dL/dout uses 20)
+constexpr uint32_t kDBytes = kRows * kDCols * 2;     // 16 KB
+constexpr uint32_t kDSbo = (kDCols / 8) * 128;       // bytes between 8-row groups of a D tile
+constexpr uint32_t kActSbo = kKCores * 128;          // ... of an activation tile (1280)
+constexpr uint32_t kGradCols = 512;                  // tensor memory of a CTA
+__host__ __device__ constexpr uint32_t dw_col(int l) { return 64u + 96u * (uint32_t)l; }  // 80 columns each
+static_assert(dw_col(3) + 80 <= kGradCols, "weight-gradient accumulators exceed tensor memory");
+
+__device__ __forceinline__ uint32_t d_off(int r, int k) {
+  return (uint32_t)(((r >> 3) * (kDCols / 8) + (k >> 3)) * 128 + ((r & 7) << 4) + ((k & 7) << 1));
+}
+// matrix descriptor with explicit leading / stride byte offsets (no swizzle)
+__device__ __forceinline__ uint64_t desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+// kind::f16 instruction descriptor: D FP32, A and B FP16, A MN-major (bit 15)
+// and B MN-major (bit 16) when asked
+__host__ __device__ constexpr uint32_t idesc(uint32_t m, uint32_t n, bool a_mn, bool b_mn) {
+  return (1u << 4) | ((a_mn ? 1u : 0u) << 15) | ((b_mn ? 1u : 0u) << 16) | ((n >> 3) << 17) | ((m >> 4) << 24);
+}
+
+struct __align__(128) GradSmem {
+  Weights w;
+  unsigned char act[4][kTileBytes];  // A_0 (features), A_1..A_3; ones in column 64
+  unsigned char d3[kDBytes];         // dL/dout x kGradScale (columns 20..63 zero)
+  unsigned char d[kDBytes];          // D_2, D_1, D_0 in turn
+  unsigned long long bar;
+  uint32_t tmem;
+  float loss;
+};
+
+// the operands are written (generic proxy) and the accumulators read
+__device__ __forceinline__ void before_mma() {
+  fence_async_smem();
+  fence_before_sync();
+  __syncthreads();
+  fence_after_sync();
+}
+// true in every thread once the committed MMAs completed; false in every
+// thread (status raised, in-flight MMAs waited for once more) on a timeout
+__device__ __forceinline__ bool after_mma(uint32_t bar, uint32_t& phase, uint32_t* status) {
+  const bool done = bar_wait(bar, phase);
+  if (__syncthreads_or(!done)) {
+    if (threadIdx.x == 0) raise_status(status, BAJO_STATUS_WAIT_TIMEOUT);
+    bar_wait(bar, phase);
+    return false;
+  }
+  phase ^= 1u;
+  fence_after_sync();
+  return true;
+}
+
+__global__ void __launch_bounds__(kRows, 1) grad_tc_kernel(const __half* __restrict__ p16,
+                                                          const float* __restrict__ pos,
+                                                          const float* __restrict__ nrm,
+                                                          const float* __restrict__ dir,
+                                                          const float* __restrict__ weight, const float* box,
+                                                          uint32_t n_rows, uint32_t offset,
+                                                          const uint32_t* __restrict__ d_count, uint32_t count_cap,
+                                                          float* __restrict__ grad32, float* __restrict__ loss_out,
+                                                          uint32_t* __restrict__ status) {
+  extern __shared__ __align__(128) unsigned char raw[];
+  GradSmem& s = *reinterpret_cast<GradSmem*>(raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  load_weights<kRows>(s.w, p16);
+  // the ones column of A_1..A_3 and the zero columns of D_3 (written once)
+#pragma unroll
+  for (int l = 1; l < 4; ++l) {
+    *reinterpret_cast<uint4*>(s.act[l] + core_off(tid, kIn)) = make_uint4(0x3C00u, 0u, 0u, 0u);
+    *reinterpret_cast<uint4*>(s.act[l] + core_off(tid, kIn + 8)) = make_uint4(0u, 0u, 0u, 0u);
+  }
+#pragma unroll
+  for (int q = 0; q < kDCols / 8; ++q) *reinterpret_cast<uint4*>(s.d3 + d_off(tid, 8 * q)) = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) s.loss = 0.0f;
+  const uint32_t bar = saddr(&s.bar);
+  const uint32_t tmem = setup_cols(bar, &s.tmem, kGradCols);
+  const uint32_t trow = tmem + ((uint32_t)(32 * warp) << 16);  // this thread's lane
+  const uint32_t a_addr[4] = {saddr(s.act[0]), saddr(s.act[1]), saddr(s.act[2]), saddr(s.act[3])};
+  const uint32_t w_addr[4] = {saddr(s.w.w[0]), saddr(s.w.w[1]), saddr(s.w.w[2]), saddr(s.w.w4)};
+  const uint32_t d3_addr = saddr(s.d3), d_addr = saddr(s.d);
+  const bool wrap = d_count != nullptr;
+  const uint32_t count = wrap ? min(*d_count, count_cap) : n_rows;
+  const uint32_t rows = wrap ? min(n_rows, count) : n_rows;
+  uint32_t phase = 0;
+  bool ok = true, any = false;
+  float my_loss = 0.0f;
+  for (uint64_t base = (uint64_t)blockIdx.x * kRows; base < rows; base += (uint64_t)gridDim.x * kRows) {
+    const uint64_t j = base + tid;
+    const bool valid = j < rows;
+    const uint64_t i = valid ? (wrap ? ((uint64_t)offset + j) % count : j) : 0;
+    {
+      uint32_t f[32];
+      if (valid) {
+        const float p[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+        const float q[3] = {nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2]};
+        encode_pairs(p, q, box, f);
+      } else {
+#pragma unroll
+        for (int k = 0; k < 32; ++k) f[k] = 0u;
+      }
+      store_features(s.act[0], tid, f);
+    }
+    // forward: layer l reads A_l, writes A_{l+1} (l < 3) or the outputs
+    float o[kOut];
+#pragma unroll 1
+    for (int l = 0; l < 4 && ok; ++l) {
+      before_mma();
+      if (tid == 0) {
+#pragma unroll
+        for (int ks = 0; ks < kK / 16; ++ks)
+          mma_f16(tmem, desc(a_addr[l] + 256u * ks, 128u, kActSbo), desc(w_addr[l] + 256u * ks, 128u, kActSbo),
+                  idesc(kRows, l < 3 ? kHid : kOutPad, false, false), ks > 0);
+        commit(bar);
+      }
+      if (!(ok = after_mma(bar, phase, status))) break;
+      if (l < 3) {
+#pragma unroll
+        for (int c0 = 0; c0 < kHid; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(trow + (uint32_t)c0, v);
+          tmem_wait_ld();
+          uint32_t h[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) h[k] = relu_pack(v[2 * k], v[2 * k + 1]);
+          *reinterpret_cast<uint4*>(s.act[l + 1] + core_off(tid, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(s.act[l + 1] + core_off(tid, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
+        }
+      } else {
+        uint32_t v[32];
+        tmem_ld16(trow, v);
+        tmem_ld16(trow + 16u, v + 16);
+        tmem_wait_ld();
+#pragma unroll
+        for (int c = 0; c < kOut; ++c) o[c] = __uint_as_float(v[c]);
+      }
+    }
+    if (!ok) break;
+    // D_3: this row's dL/dout, scaled (columns 0..23 rewritten, 20..23 zero)
+    {
+      float gr[kOut];
+      if (valid) {
+        const float dd[3] = {dir[3 * i], dir[3 * i + 1], dir[3 * i + 2]};
+        my_loss += mixture_nll_grad(o, dd, weight[i], gr);
+      } else {
+#pragma unroll
+        for (int k = 0; k < kOut; ++k) gr[k] = 0.0f;
+      }
+      uint32_t h[12];
+#pragma unroll
+      for (int k = 0; k < 12; ++k)
+        h[k] = pack_h2_sat(2 * k < kOut ? gr[2 * k] * kGradScale : 0.0f,
+                           2 * k + 1 < kOut ? gr[2 * k + 1] * kGradScale : 0.0f);
+#pragma unroll
+      for (int q = 0; q < 3; ++q)
+        *reinterpret_cast<uint4*>(s.d3 + d_off(tid, 8 * q)) = make_uint4(h[4 * q], h[4 * q + 1], h[4 * q + 2],
+                                                                           h[4 * q + 3]);
+    }
+    // backward
+#pragma unroll 1
+    for (int l = 3; l >= 0; --l) {
+      before_mma();
+      if (tid == 0) {
+        const uint32_t dl = l == 3 ? d3_addr : d_addr;
+        // dW_l (+)= D_l^T A_l: D_l MN-major (M = out: 128 B apart; K = rows:
+        // 8-row groups kDSbo apart), A_l MN-major (N = in: 128 B; K: kActSbo)
+#pragma unroll
+        for (int ks = 0; ks < kRows / 16; ++ks)
+          mma_f16(tmem + dw_col(l), desc(dl + 2u * kDSbo * ks, kDSbo, 128u),
+                  desc(a_addr[l] + 2u * kActSbo * ks, kActSbo, 128u), idesc(64, 80, true, true), (ks > 0) || any);
+        if (l > 0) {
+          // dA_l = D_l W_l: D_l K-major (K = out: 128 B; M = rows: kDSbo),
+          // W_l MN-major (N = in: 128 B apart; K = out: 8-row groups kActSbo apart)
+          const int k_out = l == 3 ? kOutPad : kHid;
+          for (int ks = 0; ks < k_out / 16; ++ks)
+            mma_f16(tmem, desc(dl + 256u * ks, 128u, kDSbo), desc(w_addr[l] + 2u * kActSbo * ks, kActSbo, 128u),
+                    idesc(kRows, kIn, false, true), ks > 0);
+        }
+        commit(bar);
+      }
+      if (!(ok = after_mma(bar, phase, status))) break;
+      if (l > 0) {
+        // D_{l-1} = dA_l where A_l > 0 (FP16, saturated)
+#pragma unroll
+        for (int c0 = 0; c0 < kIn; c0 += 16) {
+          uint32_t v[16];
+          tmem_ld16(trow + (uint32_t)c0, v);
+          tmem_wait_ld();
+          const uint4 a0 = *reinterpret_cast<const uint4*>(s.act[l] + core_off(tid, c0));
+          const uint4 a1 = *reinterpret_cast<const uint4*>(s.act[l] + core_off(tid, c0 + 8));
+          const uint32_t av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+          uint32_t h[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const __half2 a = *reinterpret_cast<const __half2*>(&av[k]);
+            const float lo = __low2float(a) > 0.0f ? __uint_as_float(v[2 * k]) : 0.0f;
+            const float hi = __high2float(a) > 0.0f ? __uint_as_float(v[2 * k + 1]) : 0.0f;
+            h[k] = pack_h2_sat(lo, hi);
+          }
+          *reinterpret_cast<uint4*>(s.d + d_off(tid, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(s.d + d_off(tid, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
+        }
+      }
+    }
+    if (!ok) break;
+    any = true;
+  }
+  // loss of the CTA's rows
+#pragma unroll
+  for (int k = 16; k > 0; k >>= 1) my_loss += __shfl_xor_sync(0xFFFFFFFFu, my_loss, k);
+  if (lane == 0 && my_loss != 0.0f) atomicAdd(&s.loss, my_loss);
+  // flush the weight gradients: warp q reads lanes 32 q.., whose lanes 0..15
+  // hold rows 16 q + lane (column 64 = the bias); staged row-major in the
+  // (now unread) activation tiles, then added with coalesced 16-byte atomics
+  if (ok && any) {
+    float* stage = reinterpret_cast<float*>(s.act[0]);  // [4][64][kStageLd], 80 KB
+    constexpr int kStageLd = 80;
+    static_assert(4 * 64 * kStageLd * 4 <= 4 * kTileBytes, "gradient staging exceeds the activation tiles");
+    const int out = 16 * warp + lane;
+#pragma unroll 1
+    for (int l = 0; l < 4; ++l)
+#pragma unroll 1
+      for (int c0 = 0; c0 <= kIn; c0 += 16) {
+        uint32_t v[16];
+        tmem_ld16(trow + dw_col(l) + (uint32_t)c0, v);
+        tmem_wait_ld();
+        if (lane < 16) {
+          float4* dst = reinterpret_cast<float4*>(stage + (l * 64 + out) * kStageLd + c0);
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                 __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+        }
+      }
+    __syncthreads();
+    const float inv = 1.0f / kGradScale;
+    // per layer: rows x 16 chunks of 4 weights, then rows / 4 chunks of biases
+    for (int l = 0; l < 4; ++l) {
+      const int rows_l = l < 3 ? kHid : kOutPad;
+      const float* sl = stage + l * 64 * kStageLd;
+      float4* W = reinterpret_cast<float4*>(grad32 + kOffW(l));
+      for (int c = tid; c < rows_l * (kIn / 4); c += kRows) {
+        const int o = c / (kIn / 4), k = 4 * (c % (kIn / 4));
+        const float* x = sl + o * kStageLd + k;
+        atomicAdd(&W[c], make_float4(x[0] * inv, x[1] * inv, x[2] * inv, x[3] * inv));
+      }
+      float4* B = reinterpret_cast<float4*>(grad32 + kOffB(l));
+      for (int c = tid; c < rows_l / 4; c += kRows) {
+        const float* x = sl + 4 * c * kStageLd + kIn;
+        atomicAdd(&B[c], make_float4(x[0] * inv, x[kStageLd] * inv, x[2 * kStageLd] * inv, x[3 * kStageLd] * inv));
+      }
+    }
+  }
+  __syncthreads();
+  if (tid == 0 && loss_out && s.loss != 0.0f) atomicAdd(loss_out, s.loss);
+  teardown_cols(tmem, kGradCols);
+}
+
+// One CTA per SM (its tensor memory takes all 512 columns), tiles strided.
+cudaError_t launch_grad(const __half* p16, const float* pos, const float* nrm, const float* dir, const float* w,
+                        const float* box, uint32_t n, uint32_t offset, const uint32_t* d_count, uint32_t count_cap,
+                        float* grad, float* loss, uint32_t* status, cudaStream_t st) {
+  static_assert(sizeof(GradSmem) <= 227 * 1024, "gradient tile exceeds shared memory");
+  // the weight gradients are added with 16-byte atomics
+  if ((reinterpret_cast<uintptr_t>(grad) & 15u) != 0) return cudaErrorMisalignedAddress;
+  const size_t smem = sizeof(GradSmem);
+  cudaError_t e = cudaFuncSetAttribute(grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st)) != cudaSuccess) return e;
+  if (loss && (e = cudaMemsetAsync(loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+  if (n == 0) return cudaSuccess;
+  grad_tc_kernel<<<grid_for(n), kRows, smem, st>>>(p16, pos, nrm, dir, w, box, n, offset, d_count, count_cap, grad,
+                                                   loss, status);
+  return cudaGetLastError();
+}
+
 }  // namespace tc
 
 }  // namespace mlp
@@ -458,6 +751,18 @@ int32_t bajo_mlp_grad(const void* d_params16, const float* d_pos, const float* d
   return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
+int32_t bajo_mlp_grad_tc(const void* d_params16, const float* d_pos, const float* d_nrm, const float* d_dir,
+                         const float* d_weight, uint32_t n, const float* d_box6, float* d_grad32, float* d_loss,
+                         uint32_t* d_status, void* stream) {
+  using namespace bajo::mlp;
+  if (!d_params16 || !d_box6 || !d_grad32 || (n && (!d_pos || !d_nrm || !d_dir || !d_weight)))
+    return BAJO_ERR_INVALID_ARGUMENT;
+  if ((reinterpret_cast<uintptr_t>(d_grad32) & 15u) != 0) return BAJO_ERR_INVALID_ARGUMENT;
+  const cudaError_t e = tc::launch_grad((const __half*)d_params16, d_pos, d_nrm, d_dir, d_weight, d_box6, n, 0,
+                                        nullptr, 0, d_grad32, d_loss, d_status, (cudaStream_t)stream);
+  return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
 int32_t bajo_mlp_adam(float* d_params32, void* d_params16, const float* d_grad32, float* d_m, float* d_v,
                       uint32_t step, float lr, float beta1, float beta2, float eps, float grad_scale, void* stream) {
   if (!d_params32 || !d_params16 || !d_grad32 || !d_m || !d_v || step == 0) return BAJO_ERR_INVALID_ARGUMENT;
@@ -476,16 +781,17 @@ int32_t bajo_guide_train(BajoGuideNet* net, const void* d_records, uint32_t reco
                          uint32_t batch, uint32_t steps, float lr, void* stream) {
   using namespace bajo::mlp;
   if (!net || !net->params32 || !net->params16 || !net->adam_m || !net->adam_v || !net->grad || !d_records ||
-      !d_box6 || record_capacity == 0 || batch == 0)
+      !d_box6 || record_capacity == 0 || batch == 0 || (reinterpret_cast<uintptr_t>(net->grad) & 15u) != 0)
     return BAJO_ERR_INVALID_ARGUMENT;
   const RecordLayout L = record_layout(record_capacity);
   const unsigned char* r = (const unsigned char*)d_records;
   cudaStream_t st = (cudaStream_t)stream;
   for (uint32_t s = 0; s < steps; ++s) {
     const uint32_t offset = (uint32_t)((uint64_t)net->step * batch % 0xFFFFFFFFull);
-    cudaError_t e = launch_grad((const __half*)net->params16, (const float*)(r + L.pos), (const float*)(r + L.nrm),
-                                (const float*)(r + L.dir), (const float*)(r + L.weight), d_box6, batch, offset,
-                                (const uint32_t*)r, record_capacity, net->grad, net->loss, st);
+    cudaError_t e = tc::launch_grad((const __half*)net->params16, (const float*)(r + L.pos),
+                                    (const float*)(r + L.nrm), (const float*)(r + L.dir), (const float*)(r + L.weight),
+                                    d_box6, batch, offset, (const uint32_t*)r, record_capacity, net->grad, net->loss,
+                                    net->status, st);
     if (e != cudaSuccess) return BAJO_ERR_CUDA;
     net->step += 1;
     e = launch_adam(net->params32, (__half*)net->params16, net->grad, net->adam_m, net->adam_v, net->step, lr, 0.9f,

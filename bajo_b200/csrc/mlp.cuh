@@ -352,6 +352,24 @@ struct __align__(128) Weights {
 
 template <int THREADS>
 __device__ void load_weights(Weights& s, const __half* __restrict__ p16) {
+  if ((reinterpret_cast<uintptr_t>(p16) & 15u) == 0) {
+    // 16-byte chunks: 8 inputs of a row, the (bias, 0 x 7) chunk or zeros;
+    // every layer's rows start on 16 bytes (4160 halves apart, rows of 64)
+    constexpr int kChunks = kK / 8, kHidden = 3 * kHid * kChunks, kTotal = kHidden + kOutPad * kChunks;
+    const uint4* src = reinterpret_cast<const uint4*>(p16);
+#pragma unroll 4
+    for (int c = threadIdx.x; c < kTotal; c += THREADS) {
+      const int l = c < kHidden ? c / (kHid * kChunks) : 3;
+      const int rc = c < kHidden ? c % (kHid * kChunks) : c - kHidden;
+      const int o = rc / kChunks, kg = rc % kChunks;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (kg < kIn / 8) v = src[(kOffW(l) + o * kIn) / 8 + kg];
+      else if (kg == kIn / 8) v.x = (uint32_t)__half_as_ushort(p16[kOffB(l) + o]);
+      unsigned char* dst = reinterpret_cast<unsigned char*>(l < 3 ? s.w[l] : s.w4);
+      *reinterpret_cast<uint4*>(dst + core_off(o, 8 * kg)) = v;
+    }
+    return;
+  }
   const uint32_t* src = reinterpret_cast<const uint32_t*>(p16);
   for (int i = threadIdx.x; i < kHid * kK / 2; i += THREADS) {
     const int o = (2 * i) / kK, k = (2 * i) % kK;  // pairs (k, k + 1) of row o
@@ -410,18 +428,17 @@ __device__ __forceinline__ void store_features(unsigned char* tile, int r, const
   *reinterpret_cast<uint4*>(tile + core_off(r, kIn + 8)) = make_uint4(0u, 0u, 0u, 0u);
 }
 
-// Prologue of a CTA of 128 NT threads: the mbarrier (count 1) and NT x 64
-// tensor-memory columns (warp 0 allocates); returns the columns' address.
+// Prologue of a CTA: the mbarrier (count 1) and `cols` tensor-memory columns
+// (a power of two from 32 to 512; warp 0 allocates); returns their address.
 // Every thread must call it.
-template <int NT>
-__device__ __forceinline__ uint32_t setup(uint32_t bar, uint32_t* s_tmem) {
+__device__ __forceinline__ uint32_t setup_cols(uint32_t bar, uint32_t* s_tmem, uint32_t cols) {
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (threadIdx.x < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(s_tmem)),
-                 "r"(NT * kColsPerTile)
+                 "r"(cols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -432,14 +449,21 @@ __device__ __forceinline__ uint32_t setup(uint32_t bar, uint32_t* s_tmem) {
   return *s_tmem;
 }
 // Epilogue: frees the columns once no thread reads them.  Every thread must call it.
-template <int NT>
-__device__ __forceinline__ void teardown(uint32_t tmem) {
+__device__ __forceinline__ void teardown_cols(uint32_t tmem, uint32_t cols) {
   fence_before_sync();
   __syncthreads();
   fence_after_sync();
   if (threadIdx.x < 32)
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NT * kColsPerTile)
-                 : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols) : "memory");
+}
+// NT tiles of 128 rows: NT x 64 columns
+template <int NT>
+__device__ __forceinline__ uint32_t setup(uint32_t bar, uint32_t* s_tmem) {
+  return setup_cols(bar, s_tmem, NT * kColsPerTile);
+}
+template <int NT>
+__device__ __forceinline__ void teardown(uint32_t tmem) {
+  teardown_cols(tmem, NT * kColsPerTile);
 }
 
 // The network on the NT tiles at `act` (kTileBytes apart, features already

@@ -74,7 +74,7 @@ class BajoGuideC(ctypes.Structure):
 class BajoGuideNetC(ctypes.Structure):
     _fields_ = [("params32", ctypes.c_void_p), ("params16", ctypes.c_void_p), ("adam_m", ctypes.c_void_p),
                 ("adam_v", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("loss", ctypes.c_void_p),
-                ("step", ctypes.c_uint32)]
+                ("step", ctypes.c_uint32), ("status", ctypes.c_void_p)]
 
 
 class GuideNetwork:
@@ -88,11 +88,13 @@ class GuideNetwork:
         self.adam_v = torch.zeros_like(self.params32)
         self.grad_buf = torch.zeros_like(self.params32)
         self.loss_buf = torch.zeros(1, dtype=torch.float32, device=device)
+        self.status = torch.zeros(1, dtype=torch.int32, device=device)  # timeout bit of the gradient kernel
         self.step = 0
 
     def c(self) -> BajoGuideNetC:
         return BajoGuideNetC(self.params32.data_ptr(), self.params16.data_ptr(), self.adam_m.data_ptr(),
-                             self.adam_v.data_ptr(), self.grad_buf.data_ptr(), self.loss_buf.data_ptr(), self.step)
+                             self.adam_v.data_ptr(), self.grad_buf.data_ptr(), self.loss_buf.data_ptr(), self.step,
+                             self.status.data_ptr())
 
     def forward(self, pos: torch.Tensor, nrm: torch.Tensor, box: torch.Tensor, stream=None,
                 tensor_memory: bool = False, status: torch.Tensor | None = None) -> torch.Tensor:
@@ -112,13 +114,21 @@ class GuideNetwork:
                        "bajo_mlp_forward")
         return out
 
-    def gradient(self, pos, nrm, dirs, weights, box, stream=None):
-        """(gradient tensor, loss tensor) of sum -w log pdf(dir)."""
+    def gradient(self, pos, nrm, dirs, weights, box, stream=None, tensor_memory: bool = True):
+        """(gradient tensor, loss tensor) of sum -w log pdf(dir); the
+        tcgen05 kernel (the one training uses) unless ``tensor_memory`` is
+        false, then the mma.sync kernel."""
         n = pos.numel() // 3
-        _lib.check(_lib.load().bajo_mlp_grad(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(),
-                                             dirs.data_ptr(), weights.data_ptr(), n, box.data_ptr(),
-                                             self.grad_buf.data_ptr(), self.loss_buf.data_ptr(),
-                                             _lib.stream_handle(stream)), "bajo_mlp_grad")
+        L = _lib.load()
+        if tensor_memory:
+            _lib.check(L.bajo_mlp_grad_tc(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(), dirs.data_ptr(),
+                                          weights.data_ptr(), n, box.data_ptr(), self.grad_buf.data_ptr(),
+                                          self.loss_buf.data_ptr(), self.status.data_ptr(),
+                                          _lib.stream_handle(stream)), "bajo_mlp_grad_tc")
+        else:
+            _lib.check(L.bajo_mlp_grad(self.params16.data_ptr(), pos.data_ptr(), nrm.data_ptr(), dirs.data_ptr(),
+                                       weights.data_ptr(), n, box.data_ptr(), self.grad_buf.data_ptr(),
+                                       self.loss_buf.data_ptr(), _lib.stream_handle(stream)), "bajo_mlp_grad")
         return self.grad_buf, self.loss_buf
 
     def adam(self, lr: float = 1e-2, grad_scale: float = 1.0, beta1=0.9, beta2=0.999, eps=1e-8, stream=None):

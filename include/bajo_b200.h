@@ -595,6 +595,21 @@ int32_t bajo_mlp_grad(const void* d_params16, const float* d_pos, const float* d
                       const float* d_weight, uint32_t n, const float* d_box6, float* d_grad32, float* d_loss,
                       void* stream);
 
+/* The same gradient from the 5th-generation tensor cores: per 128-sample
+ * tile the forward keeps every layer's activations in shared memory, then
+ * per layer one tcgen05.mma chain for the weight gradient (M = 64 outputs,
+ * N = 80: inputs and the bias column, K = 128 samples, accumulated in tensor
+ * memory over the CTA's tiles) and one for the input gradient (M = 128
+ * samples, N = 64).  Agrees with bajo_mlp_grad to FP32 accumulation order.
+ * d_grad32 must be 16-byte aligned (the gradients are added with 16-byte
+ * atomics; else BAJO_ERR_INVALID_ARGUMENT), as must BajoGuideNet::grad.
+ * d_status (may be NULL) gets BAJO_STATUS_WAIT_TIMEOUT if the tensor cores
+ * never signal completion.  New on this path (no counterpart in the
+ * reference). */
+int32_t bajo_mlp_grad_tc(const void* d_params16, const float* d_pos, const float* d_nrm, const float* d_dir,
+                         const float* d_weight, uint32_t n, const float* d_box6, float* d_grad32, float* d_loss,
+                         uint32_t* d_status, void* stream);
+
 /* One Adam step (Kingma & Ba) on FP32 master weights with gradient
  * grad_scale * d_grad32; refreshes the FP16 copy.  step counts from 1. */
 int32_t bajo_mlp_adam(float* d_params32, void* d_params16, const float* d_grad32, float* d_m, float* d_v,
@@ -666,13 +681,15 @@ typedef struct BajoGuideNet {
   float* adam_m;
   float* adam_v;
   float* grad;
-  float* loss;   /* 1 f32: summed loss of the last step */
-  uint32_t step; /* Adam steps taken so far (advanced by bajo_guide_train) */
+  float* loss;      /* 1 f32: summed loss of the last step */
+  uint32_t step;    /* Adam steps taken so far (advanced by bajo_guide_train) */
+  uint32_t* status; /* device u32 (may be NULL): BAJO_STATUS_WAIT_TIMEOUT from the gradient kernel */
 } BajoGuideNet;
 
 /* `steps` Adam steps (beta 0.9 / 0.999, eps 1e-8, learning rate lr), each
  * on `batch` records taken cyclically from the buffer (count read on the
- * device, so no host synchronisation). */
+ * device, so no host synchronisation); the gradients come from the
+ * tensor-memory kernel of bajo_mlp_grad_tc. */
 int32_t bajo_guide_train(BajoGuideNet* net, const void* d_records, uint32_t record_capacity, const float* d_box6,
                          uint32_t batch, uint32_t steps, float lr, void* stream);
 

@@ -1,7 +1,7 @@
 """GPU parity of the guiding network's tensor-core kernels against the FP64
-oracle: forward outputs, loss and parameter gradients (mma.sync FP16 inputs,
-FP32 accumulation; tolerances below), Adam against its definition, and
-training that learns a known direction field."""
+oracle: forward outputs, loss and parameter gradients (mma.sync and tcgen05,
+FP16 inputs, FP32 accumulation; tolerances below), Adam against its
+definition, and training that learns a known direction field."""
 import numpy as np
 import pytest
 import torch
@@ -77,13 +77,16 @@ def test_tensor_memory_forward(n):
     assert np.abs(out - base).max() <= 5e-3 + 5e-3 * np.abs(base).max()
 
 
+@pytest.mark.parametrize("tensor_memory", [True, False])
 @pytest.mark.parametrize("n", [1, 200, 3000])
-def test_gradient_matches_oracle(n):
+def test_gradient_matches_oracle(n, tensor_memory):
     rng = np.random.default_rng(7 + n)
     net, p64 = _net(2)
     pos, nrm, d, w = _batch(rng, n)
     box = torch.from_numpy(BOX).cuda()
-    g, loss = net.gradient(*_dev(pos, nrm, d, w), box)
+    g, loss = net.gradient(*_dev(pos, nrm, d, w), box, tensor_memory=tensor_memory)
+    torch.cuda.synchronize()
+    assert int(net.status.item()) == 0
     g = g.double().cpu().numpy()
     gref, lref = oracle.mlp_grad(p64, pos, nrm, d, w, BOX)
     assert float(loss.item()) == pytest.approx(lref, rel=1e-2, abs=1e-2)
@@ -99,12 +102,38 @@ def test_gradient_matches_oracle(n):
     assert not np.any(g[w4 + 20 * 64:b4]) and not np.any(g[b4 + 20:])
 
 
-def test_gradient_of_empty_batch_is_zero():
+@pytest.mark.parametrize("n", [127, 128, 129, 40000, 200003])
+def test_gradient_kernels_agree(n):
+    """The tcgen05 gradient (weight gradients accumulated in tensor memory
+    over several tiles per CTA at the larger sizes) against the mma.sync one:
+    the same FP16 operands, FP32 sums in another order."""
+    rng = np.random.default_rng(11 + n)
+    net, _ = _net(5)
+    pos, nrm, d, w = _batch(rng, n)
+    box = torch.from_numpy(BOX).cuda()
+    args = _dev(pos, nrm, d, w)
+    g_tc, l_tc = net.gradient(*args, box, tensor_memory=True)
+    g_tc, l_tc = g_tc.clone(), float(l_tc.item())
+    g_mma, l_mma = net.gradient(*args, box, tensor_memory=False)
+    torch.cuda.synchronize()
+    assert int(net.status.item()) == 0
+    g_tc, g_mma = g_tc.double().cpu().numpy(), g_mma.double().cpu().numpy()
+    assert np.all(np.isfinite(g_tc))
+    assert l_tc == pytest.approx(float(l_mma.item()), rel=1e-4)
+    for wo, bo, rows, cols in guide.offsets():
+        a, b = g_tc[wo:wo + rows * cols], g_mma[wo:wo + rows * cols]
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b) + 1e-6
+        a, b = g_tc[bo:bo + rows], g_mma[bo:bo + rows]
+        assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(b) + 1e-6
+
+
+@pytest.mark.parametrize("tensor_memory", [True, False])
+def test_gradient_of_empty_batch_is_zero(tensor_memory):
     net, _ = _net(3)
     box = torch.from_numpy(BOX).cuda()
     e = torch.empty(0, dtype=torch.float32, device="cuda")
     net.grad_buf.fill_(1.0)
-    g, loss = net.gradient(e, e, e, e, box)
+    g, loss = net.gradient(e, e, e, e, box, tensor_memory=tensor_memory)
     assert not torch.any(g) and float(loss.item()) == 0.0
 
 
