@@ -285,19 +285,24 @@ __global__ void __launch_bounds__(kThreads) train_kernel(const __half* __restric
 // Adam (Kingma & Ba 2015) on the FP32 master weights; FP16 copies refreshed.
 // grad_scale multiplies the raw gradient; the padded rows of the output layer
 // stay zero.
-__global__ void adam_kernel(float* __restrict__ p32, __half* __restrict__ p16, const float* __restrict__ grad,
+// With `clear`, the gradient (and *loss, when given) is zeroed after use, so
+// that the next gradient launch may accumulate without a memset.
+__global__ void adam_kernel(float* __restrict__ p32, __half* __restrict__ p16, float* __restrict__ grad,
                             float* __restrict__ m, float* __restrict__ v, float lr, float b1, float b2, float eps,
-                            float bc1, float bc2, float grad_scale) {
+                            float bc1, float bc2, float grad_scale, bool clear, float* __restrict__ loss) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= kParams) return;
+  if (clear && i == 0 && loss) *loss = 0.0f;
   const bool pad_w = i >= kOffW(3) && i < kOffB(3) && (i - kOffW(3)) / kHid >= kOut;
   const bool pad_b = i >= kOffB(3) && i - kOffB(3) >= kOut;
   if (pad_w || pad_b) {
     p32[i] = 0.0f;
     p16[i] = __float2half(0.0f);
+    if (clear) grad[i] = 0.0f;
     return;
   }
   const float gr = grad[i] * grad_scale;
+  if (clear) grad[i] = 0.0f;
   const float mi = b1 * m[i] + (1.0f - b1) * gr;
   const float vi = b2 * v[i] + (1.0f - b2) * gr * gr;
   m[i] = mi;
@@ -329,10 +334,12 @@ cudaError_t launch_grad(const __half* p16, const float* pos, const float* nrm, c
   return cudaGetLastError();
 }
 
-cudaError_t launch_adam(float* p32, __half* p16, const float* grad, float* m, float* v, uint32_t step, float lr,
-                        float b1, float b2, float eps, float grad_scale, cudaStream_t st) {
+cudaError_t launch_adam(float* p32, __half* p16, float* grad, float* m, float* v, uint32_t step, float lr,
+                        float b1, float b2, float eps, float grad_scale, cudaStream_t st, bool clear = false,
+                        float* loss = nullptr) {
   const float bc1 = 1.0f - powf(b1, (float)step), bc2 = 1.0f - powf(b2, (float)step);
-  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(p32, p16, grad, m, v, lr, b1, b2, eps, bc1, bc2, grad_scale);
+  adam_kernel<<<(kParams + 255) / 256, 256, 0, st>>>(p32, p16, grad, m, v, lr, b1, b2, eps, bc1, bc2, grad_scale,
+                                                     clear, loss);
   return cudaGetLastError();
 }
 
@@ -414,7 +421,7 @@ constexpr uint32_t kDSbo = (kDCols / 8) * 128;       // bytes between 8-row grou
 constexpr uint32_t kActSbo = kKCores * 128;          // ... of an activation tile (1280)
 constexpr uint32_t kGradCols = 512;                  // tensor memory of a CTA
 __host__ __device__ constexpr uint32_t dw_col(int l) { return 64u + 96u * (uint32_t)l; }  // 80 columns each
-static_assert(dw_col(3) + 80 <= kGradCols, "weight-gradient accumulators exceed tensor memory");
+static_assert(dw_col(3) + 96 <= kGradCols, "weight-gradient accumulators exceed tensor memory");
 
 __device__ __forceinline__ uint32_t d_off(int r, int k) {
   return (uint32_t)(((r >> 3) * (kDCols / 8) + (k >> 3)) * 128 + ((r & 7) << 4) + ((k & 7) << 1));
@@ -526,21 +533,18 @@ __global__ void __launch_bounds__(kRows, 1) grad_tc_kernel(const __half* __restr
       if (!(ok = after_mma(bar, phase, status))) break;
       if (l < 3) {
 #pragma unroll
-        for (int c0 = 0; c0 < kHid; c0 += 16) {
-          uint32_t v[16];
-          tmem_ld16(trow + (uint32_t)c0, v);
-          tmem_wait_ld();
-          uint32_t h[8];
+        for (int c0 = 0; c0 < kHid; c0 += 32) {
+          uint32_t v[32];
+          tmem_ld32_wait(trow + (uint32_t)c0, v);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) h[k] = relu_pack(v[2 * k], v[2 * k + 1]);
-          *reinterpret_cast<uint4*>(s.act[l + 1] + core_off(tid, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4*>(s.act[l + 1] + core_off(tid, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
+          for (int q = 0; q < 4; ++q)
+            *reinterpret_cast<uint4*>(s.act[l + 1] + core_off(tid, c0 + 8 * q)) =
+                make_uint4(relu_pack(v[8 * q], v[8 * q + 1]), relu_pack(v[8 * q + 2], v[8 * q + 3]),
+                           relu_pack(v[8 * q + 4], v[8 * q + 5]), relu_pack(v[8 * q + 6], v[8 * q + 7]));
         }
       } else {
         uint32_t v[32];
-        tmem_ld16(trow, v);
-        tmem_ld16(trow + 16u, v + 16);
-        tmem_wait_ld();
+        tmem_ld32_wait(trow, v);
 #pragma unroll
         for (int c = 0; c < kOut; ++c) o[c] = __uint_as_float(v[c]);
       }
@@ -592,23 +596,23 @@ __global__ void __launch_bounds__(kRows, 1) grad_tc_kernel(const __half* __restr
       if (l > 0) {
         // D_{l-1} = dA_l where A_l > 0 (FP16, saturated)
 #pragma unroll
-        for (int c0 = 0; c0 < kIn; c0 += 16) {
-          uint32_t v[16];
-          tmem_ld16(trow + (uint32_t)c0, v);
-          tmem_wait_ld();
-          const uint4 a0 = *reinterpret_cast<const uint4*>(s.act[l] + core_off(tid, c0));
-          const uint4 a1 = *reinterpret_cast<const uint4*>(s.act[l] + core_off(tid, c0 + 8));
-          const uint32_t av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-          uint32_t h[8];
+        for (int c0 = 0; c0 < kIn; c0 += 32) {
+          uint32_t v[32];
+          tmem_ld32_wait(trow + (uint32_t)c0, v);
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const __half2 a = *reinterpret_cast<const __half2*>(&av[k]);
-            const float lo = __low2float(a) > 0.0f ? __uint_as_float(v[2 * k]) : 0.0f;
-            const float hi = __high2float(a) > 0.0f ? __uint_as_float(v[2 * k + 1]) : 0.0f;
-            h[k] = pack_h2_sat(lo, hi);
+          for (int q = 0; q < 4; ++q) {
+            const uint4 a4 = *reinterpret_cast<const uint4*>(s.act[l] + core_off(tid, c0 + 8 * q));
+            const uint32_t av[4] = {a4.x, a4.y, a4.z, a4.w};
+            uint32_t h[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const __half2 a = *reinterpret_cast<const __half2*>(&av[k]);
+              const float lo = __low2float(a) > 0.0f ? __uint_as_float(v[8 * q + 2 * k]) : 0.0f;
+              const float hi = __high2float(a) > 0.0f ? __uint_as_float(v[8 * q + 2 * k + 1]) : 0.0f;
+              h[k] = pack_h2_sat(lo, hi);
+            }
+            *reinterpret_cast<uint4*>(s.d + d_off(tid, c0 + 8 * q)) = make_uint4(h[0], h[1], h[2], h[3]);
           }
-          *reinterpret_cast<uint4*>(s.d + d_off(tid, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<uint4*>(s.d + d_off(tid, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
         }
       }
     }
@@ -630,16 +634,16 @@ __global__ void __launch_bounds__(kRows, 1) grad_tc_kernel(const __half* __restr
 #pragma unroll 1
     for (int l = 0; l < 4; ++l)
 #pragma unroll 1
-      for (int c0 = 0; c0 <= kIn; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(trow + dw_col(l) + (uint32_t)c0, v);
-        tmem_wait_ld();
+      for (int c0 = 0; c0 < 96; c0 += 32) {  // columns 0..95 (80..95 unused)
+        uint32_t v[32];
+        tmem_ld32_wait(trow + dw_col(l) + (uint32_t)c0, v);
         if (lane < 16) {
           float4* dst = reinterpret_cast<float4*>(stage + (l * 64 + out) * kStageLd + c0);
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
-                                 __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
+          for (int q = 0; q < 8; ++q)
+            if (c0 + 4 * q < kStageLd)
+              dst[q] = make_float4(__uint_as_float(v[4 * q]), __uint_as_float(v[4 * q + 1]),
+                                   __uint_as_float(v[4 * q + 2]), __uint_as_float(v[4 * q + 3]));
         }
       }
     __syncthreads();
@@ -669,15 +673,24 @@ __global__ void __launch_bounds__(kRows, 1) grad_tc_kernel(const __half* __restr
 // One CTA per SM (its tensor memory takes all 512 columns), tiles strided.
 cudaError_t launch_grad(const __half* p16, const float* pos, const float* nrm, const float* dir, const float* w,
                         const float* box, uint32_t n, uint32_t offset, const uint32_t* d_count, uint32_t count_cap,
-                        float* grad, float* loss, uint32_t* status, cudaStream_t st) {
+                        float* grad, float* loss, uint32_t* status, cudaStream_t st, bool zero = true) {
   static_assert(sizeof(GradSmem) <= 227 * 1024, "gradient tile exceeds shared memory");
   // the weight gradients are added with 16-byte atomics
   if ((reinterpret_cast<uintptr_t>(grad) & 15u) != 0) return cudaErrorMisalignedAddress;
   const size_t smem = sizeof(GradSmem);
-  cudaError_t e = cudaFuncSetAttribute(grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  static bool attr_set[64] = {};  // one attribute call per device (the value never changes)
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if ((e = cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st)) != cudaSuccess) return e;
-  if (loss && (e = cudaMemsetAsync(loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+  if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+    e = cudaFuncSetAttribute(grad_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64) attr_set[dev] = true;
+  }
+  if (zero) {
+    if ((e = cudaMemsetAsync(grad, 0, sizeof(float) * kParams, st)) != cudaSuccess) return e;
+    if (loss && (e = cudaMemsetAsync(loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+  }
   if (n == 0) return cudaSuccess;
   grad_tc_kernel<<<grid_for(n), kRows, smem, st>>>(p16, pos, nrm, dir, w, box, n, offset, d_count, count_cap, grad,
                                                    loss, status);
@@ -766,8 +779,9 @@ int32_t bajo_mlp_grad_tc(const void* d_params16, const float* d_pos, const float
 int32_t bajo_mlp_adam(float* d_params32, void* d_params16, const float* d_grad32, float* d_m, float* d_v,
                       uint32_t step, float lr, float beta1, float beta2, float eps, float grad_scale, void* stream) {
   if (!d_params32 || !d_params16 || !d_grad32 || !d_m || !d_v || step == 0) return BAJO_ERR_INVALID_ARGUMENT;
-  const cudaError_t e = bajo::mlp::launch_adam(d_params32, (__half*)d_params16, d_grad32, d_m, d_v, step, lr, beta1,
-                                               beta2, eps, grad_scale, (cudaStream_t)stream);
+  // clear = false: the gradient is only read
+  const cudaError_t e = bajo::mlp::launch_adam(d_params32, (__half*)d_params16, const_cast<float*>(d_grad32), d_m,
+                                               d_v, step, lr, beta1, beta2, eps, grad_scale, (cudaStream_t)stream);
   return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
 }
 
@@ -791,11 +805,13 @@ int32_t bajo_guide_train(BajoGuideNet* net, const void* d_records, uint32_t reco
     cudaError_t e = tc::launch_grad((const __half*)net->params16, (const float*)(r + L.pos),
                                     (const float*)(r + L.nrm), (const float*)(r + L.dir), (const float*)(r + L.weight),
                                     d_box6, batch, offset, (const uint32_t*)r, record_capacity, net->grad, net->loss,
-                                    net->status, st);
+                                    net->status, st, s == 0);
     if (e != cudaSuccess) return BAJO_ERR_CUDA;
     net->step += 1;
+    // Adam clears the gradient and the loss for the next step's accumulation;
+    // the last step's stay readable
     e = launch_adam(net->params32, (__half*)net->params16, net->grad, net->adam_m, net->adam_v, net->step, lr, 0.9f,
-                    0.999f, 1e-8f, 1.0f / (float)batch, st);
+                    0.999f, 1e-8f, 1.0f / (float)batch, st, s + 1 < steps, net->loss);
     if (e != cudaSuccess) return BAJO_ERR_CUDA;
   }
   return BAJO_OK;

@@ -7,8 +7,12 @@
 // Parameter layout (floats / halves): W1[64x64] b1[64] W2 b2 W3 b3 W4[32x64]
 // b4[32] (rows 20..31 of W4 and b4 are zero), weights row-major [out][in].
 //
-// Dense layers run on the tensor cores with mma.sync m16n8k16 (f16 inputs,
-// f32 accumulation).  Fragment layouts (PTX ISA), g = lane / 4, t = lane % 4:
+// Dense layers run on the 5th-generation tensor cores (namespace tc below:
+// tcgen05.mma with FP32 accumulators in tensor memory) in the guided shading,
+// the batched forward of bajo_mlp_forward_tc and the training gradient.  The
+// warp-level mma.sync m16n8k16 kernels (f16 inputs, f32 accumulation) remain
+// as bajo_mlp_forward / bajo_mlp_grad, the comparison for the tcgen05 ones.
+// mma.sync fragment layouts (PTX ISA), g = lane / 4, t = lane % 4:
 //   A (16x16): a0a1 = (g, 2t..2t+1), a2a3 = (g+8, 2t..), a4a5 = (g, 2t+8..),
 //              a6a7 = (g+8, 2t+8..)
 //   B (16x8):  b0b1 = (k 2t..2t+1, n g), b2b3 = (k 2t+8.., n g)
@@ -324,15 +328,20 @@ __device__ __forceinline__ bool bar_wait(uint32_t bar, uint32_t parity) {  // at
     if (global_timer_ns() - t0 > kWaitNs) return false;
   return true;
 }
-// 16 consecutive FP32 accumulator columns of this thread's lane (raw bits)
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t r[16]) {
+// 32 consecutive FP32 accumulator columns of this thread's lane, waited for
+// in the same statement (so no use of r can be scheduled before the wait)
+__device__ __forceinline__ void tmem_ld32_wait(uint32_t taddr, uint32_t r[32]) {
   asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,"
+      "%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+      "tcgen05.wait::ld.sync.aligned;"
       : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr)
+      : "memory");
 }
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 // generic-proxy writes to shared memory, before the tensor cores read them
@@ -506,21 +515,18 @@ __device__ __forceinline__ bool forward(const Weights& w, unsigned char* act, ui
     fence_after_sync();
     if (l < 3) {
 #pragma unroll
-      for (int c0 = 0; c0 < kHid; c0 += 16) {
-        uint32_t v[16];
-        tmem_ld16(trow + (uint32_t)c0, v);
-        tmem_wait_ld();
-        uint32_t h[8];
+      for (int c0 = 0; c0 < kHid; c0 += 32) {
+        uint32_t v[32];
+        tmem_ld32_wait(trow + (uint32_t)c0, v);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) h[j] = relu_pack(v[2 * j], v[2 * j + 1]);
-        *reinterpret_cast<uint4*>(mine + core_off(r, c0)) = make_uint4(h[0], h[1], h[2], h[3]);
-        *reinterpret_cast<uint4*>(mine + core_off(r, c0 + 8)) = make_uint4(h[4], h[5], h[6], h[7]);
+        for (int q = 0; q < 4; ++q)
+          *reinterpret_cast<uint4*>(mine + core_off(r, c0 + 8 * q)) =
+              make_uint4(relu_pack(v[8 * q], v[8 * q + 1]), relu_pack(v[8 * q + 2], v[8 * q + 3]),
+                         relu_pack(v[8 * q + 4], v[8 * q + 5]), relu_pack(v[8 * q + 6], v[8 * q + 7]));
       }
     } else {
       uint32_t v[32];
-      tmem_ld16(trow, v);
-      tmem_ld16(trow + 16u, v + 16);
-      tmem_wait_ld();
+      tmem_ld32_wait(trow, v);
 #pragma unroll
       for (int c = 0; c < kOut; ++c) out[c] = __uint_as_float(v[c]);
     }

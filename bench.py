@@ -102,7 +102,7 @@ def parse_args(argv=None):
     p.add_argument("--no-extras", action="store_true", help="skip the render, batched and guided workloads")
     p.add_argument("--case", default=None,
                    choices=["sort", "build", "trace", "wide", "cwbvh8", "hploc", "tlas", "tune", "render",
-                            "batched", "guided", "guided_pass", "mlp_forward"],
+                            "batched", "guided", "guided_pass", "mlp_forward", "mlp_train"],
                    help="time one piece alone (profiling runs) instead of the benchmark line")
     p.add_argument("--n", type=int, default=1 << 24, help="--case size (keys or triangles)")
     p.add_argument("--bits", type=int, default=32, choices=[32, 64], help="--case sort key width")
@@ -121,11 +121,13 @@ def parse_args(argv=None):
     p.add_argument("--spp-per-pass", type=int, default=2, help="--case guided samples per pixel per pass")
     p.add_argument("--spp", type=int, default=64, help="--case render samples per pixel")
     p.add_argument("--scenes", type=int, default=4096, help="--case batched scene count")
-    p.add_argument("--train-passes", type=int, default=6, help="--case guided passes followed by training")
+    p.add_argument("--train-passes", type=int, default=8, help="--case guided passes followed by training")
     p.add_argument("--first-guided", action="store_true",
                    help="--case guided: guide the first pass too (by default it samples the BSDF only, since the "
                         "network is untrained)")
-    p.add_argument("--train-steps", type=int, default=32, help="--case guided Adam steps per training pass")
+    p.add_argument("--train-steps", type=int, default=64, help="--case guided Adam steps per training pass")
+    p.add_argument("--records", type=int, default=1 << 20,
+                   help="--case guided training records kept per pass (batches of 2^14 are drawn from them)")
     return p.parse_args(argv)
 
 
@@ -1117,7 +1119,7 @@ def run_guided(args):
     t_plain, img = ev_time(lambda: rt.render_gpu_triangles(st_plain, sc.camera, gsc, rt.MIS, workspace=ws))
     mse_plain = float(((img.double() - ref) ** 2).mean())
     # guided, progressive
-    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=args.spp_per_pass, record_capacity=1 << 18,
+    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=args.spp_per_pass, record_capacity=args.records,
                               batch=1 << 14, steps=args.train_steps, lr=1e-2)
     gr.render_pass(1, train=False)  # warm-up: kernel attributes, tuning table
     torch.cuda.synchronize()
@@ -1152,6 +1154,7 @@ def run_guided(args):
            "plain_samples_s": round(w * h * 64 / t_plain * 1e3, 1),
            "guided_mrays_s": round((rays + shadows) / t_pass / 1e3, 1),
            "train_passes": args.train_passes, "spp_per_pass": args.spp_per_pass, "train_steps": args.train_steps,
+           "records_per_pass": args.records,
            "first_pass_guided": bool(args.first_guided),
            "log": log[:: max(1, len(log) // 40)], "status": gr.workspace.status()}
     return out
@@ -1167,7 +1170,7 @@ def run_guided_pass(args):
     w, h, spp = args.width, args.height, args.spp_per_pass
     sc = guided_scene(args.scene)
     gsc = rt.GpuRtTriangleScene(sc)
-    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=spp, record_capacity=1 << 18, batch=1 << 14,
+    gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=spp, record_capacity=args.records, batch=1 << 14,
                               steps=args.train_steps)
     for k in range(args.train_passes):
         gr.render_pass(11 + k, train=True)
@@ -1252,6 +1255,27 @@ def run_case(args):
         out.update({"ms_mma_sync": round(ms_mma, 5), "ms_tcgen05": round(ms_tc, 5),
                     "rows_s_mma_sync": round(n / ms_mma * 1e3, 1), "rows_s_tcgen05": round(n / ms_tc * 1e3, 1),
                     "tflops_tcgen05": round(flops / ms_tc / 1e9, 2), "status": int(status.item())})
+    elif args.case == "mlp_train":
+        # one training step of the guiding network on n records: gradient
+        # (mma.sync kernel and tcgen05 kernel) and Adam
+        from bajo_b200 import guide
+        g = torch.Generator(device="cuda").manual_seed(0)
+        pos = torch.rand((n, 3), generator=g, device="cuda")
+        nrm = torch.nn.functional.normalize(torch.randn((n, 3), generator=g, device="cuda"), dim=1)
+        dirs = torch.nn.functional.normalize(torch.randn((n, 3), generator=g, device="cuda"), dim=1)
+        wts = torch.rand(n, generator=g, device="cuda")
+        box = torch.tensor([0, 0, 0, 1, 1, 1], dtype=torch.float32, device="cuda")
+        net = guide.GuideNetwork("cuda", seed=0)
+        ms_mma = timed(lambda: net.gradient(pos, nrm, dirs, wts, box, tensor_memory=False))
+        ms_tc = timed(lambda: net.gradient(pos, nrm, dirs, wts, box, tensor_memory=True))
+        ms_adam = timed(lambda: net.adam(lr=0.0, grad_scale=0.0))
+        # tensor-core work issued per row: forward (K = 80 with the bias
+        # column), input gradients of layers 3..1, weight gradients (M = 64,
+        # N = 80) of all four layers
+        flops = 2.0 * n * ((3 * 64 * 80 + 32 * 80) + (2 * 64 * 64 + 64 * 32) + 4 * 64 * 80)
+        out.update({"ms_grad_mma_sync": round(ms_mma, 5), "ms_grad_tcgen05": round(ms_tc, 5),
+                    "ms_adam": round(ms_adam, 5), "rows_s_tcgen05": round(n / ms_tc * 1e3, 1),
+                    "tflops_tcgen05": round(flops / ms_tc / 1e9, 2), "status": int(net.status.item())})
     elif args.case == "tune":
         out["results"] = autotune.tune_all(reps=args.steps, save_cache=False)
         out["device"] = autotune.device_key()

@@ -240,3 +240,39 @@ def test_checkpoint_of_another_network_is_refused(tmp_path):
              adam_m=np.zeros(10, np.float32), adam_v=np.zeros(10, np.float32), step=np.int64(0), n_params=np.int64(10))
     with pytest.raises(ValueError):
         guide.GuideNetwork.load(path)
+
+
+def test_guide_train_matches_gradient_and_adam_steps():
+    """bajo_guide_train (one gradient memset per call, Adam clearing the
+    gradient and loss between steps) against explicit tcgen05 gradient +
+    Adam steps over the same cyclic record batches."""
+    rng = np.random.default_rng(21)
+    count, batch, steps = 5000, 2048, 5
+    pos, nrm, d, w = _batch(rng, count)
+    box = torch.from_numpy(BOX).cuda()
+    rec = guide.GuideRecords(8192)
+    for name, arr in zip(("pos", "nrm", "dir", "weight"), (pos, nrm, d, w)):
+        o = rec._off[name] // 4
+        rec.buffer.view(torch.float32)[o:o + arr.size] = torch.from_numpy(arr.reshape(-1)).cuda()
+    rec.buffer[:4].view(torch.int32)[0] = count
+    a = guide.GuideNetwork("cuda", seed=6)
+    b = guide.GuideNetwork("cuda", seed=6)
+    a.train_records(rec, box, batch, steps, lr=1e-2)
+    for s in range(steps):
+        idx = (s * batch + np.arange(batch)) % count
+        P, N, D, W = _dev(pos[idx], nrm[idx], d[idx], w[idx])
+        b.gradient(P, N, D, W, box)
+        b.adam(lr=1e-2, grad_scale=1.0 / batch)
+    torch.cuda.synchronize()
+    assert a.step == b.step == steps
+    assert int(a.status.item()) == 0
+    pa, pb = a.params32.double().cpu().numpy(), b.params32.double().cpu().numpy()
+    # atomics sum in any order, so the two gradients differ by FP32 rounding;
+    # Adam's first steps move every parameter by about lr whatever the
+    # gradient's size, so a gradient within rounding of zero may step either
+    # way: a handful of parameters may differ by up to 2 lr per step
+    diff = np.abs(pa - pb)
+    assert np.mean(diff > 1e-4) < 1e-3 and diff.max() <= 2e-2 * steps, (np.mean(diff > 1e-4), diff.max())
+    assert float(a.loss_buf.item()) == pytest.approx(float(b.loss_buf.item()), rel=1e-3)
+    ga, gb = a.grad_buf.double().cpu().numpy(), b.grad_buf.double().cpu().numpy()
+    assert np.linalg.norm(ga - gb) <= 1e-3 * np.linalg.norm(gb)
