@@ -13,6 +13,11 @@ sizes, and the size limit of the one-launch build.
 - The one-launch build is timed against the per-stage kernels at every
   power of two up to its limit, and the largest size up to which it wins is
   installed (``bajo_lbvh_fused_max_set``).
+- The wavefront tracer's bounce kernels (closest hit, shading, shadow rays)
+  are compiled for blocks of 64, 128 and 256 threads; the tuner renders the
+  path-tracing workload's scene (at a reduced resolution) with each block
+  size of each kernel, checks that the images are identical, and installs
+  the fastest (``bajo_render_tuning_set``).
 
 Results are cached as JSON keyed by (kernel, size bucket, GPU name and SM
 count) so a process can load them instead of re-measuring.
@@ -157,6 +162,42 @@ def tune_trace(kernel: str, log2rays, n_tris: int = 65536, reps: int = 5) -> dic
     return out
 
 
+_RENDER_KINDS = {"render_trace": 0, "render_shade": 1, "render_shadow": 2}
+RENDER_BLOCKS = (128, 64, 256)
+
+
+def tune_render(width: int = 640, height: int = 360, spp: int = 8, reps: int = 5) -> dict:
+    """Time every block size of each wavefront bounce kernel on the 64-sphere
+    path-tracing scene (MIS, depth 8, the default tree) and install the
+    fastest per kernel, the other kernels at their current choice; every
+    block size must give the same image bit for bit.  Returns
+    {kernel: {0: {"best": block, "ms": {...}}}}."""
+    from . import rt, scenes
+    L = _lib.load()
+    sc = scenes.spheres_in_box()
+    gsc = rt.GpuRtTriangleScene(sc)
+    settings = rt.RenderSettings(width, height, spp, rng_seed=3, max_depth=8)
+    ws = rt.RenderWorkspace(settings, rt.MIS)
+    pixels = torch.empty((height, width, 3), dtype=torch.float32, device="cuda")
+    cam = torch.from_numpy(sc.camera).cuda()
+    fn = lambda: rt.render_gpu_triangles(settings, cam, gsc, rt.MIS, workspace=ws, pixels=pixels)  # noqa: E731
+    out = {}
+    for kernel, kind in _RENDER_KINDS.items():
+        times, ref = {}, None
+        for blk in RENDER_BLOCKS:
+            _lib.check(L.bajo_render_tuning_set(kind, blk), "bajo_render_tuning_set")
+            times[blk] = _events_ms(fn, reps)
+            got = pixels.clone()
+            if ref is None:
+                ref = got
+            elif not torch.equal(got.view(torch.int32), ref.view(torch.int32)):
+                raise RuntimeError(f"{kernel}: block {blk} changed the image")
+        best = min(times, key=times.get)
+        _lib.check(L.bajo_render_tuning_set(kind, best), "bajo_render_tuning_set")
+        out[kernel] = {0: {"best": best, "ms": {str(k): round(t, 4) for k, t in times.items()}}}
+    return out
+
+
 def tune_one_launch(log2tris=range(11, 18), reps: int = 7) -> dict:
     """Build time of one scene through the one-launch build and through the
     per-stage kernels at each size; installs the largest size up to which
@@ -209,6 +250,10 @@ def load(path: str = CACHE) -> int:
             for lg, v in entries.items():
                 count += L.bajo_trace_tuning_set(_TRACE_KINDS[kernel], int(lg), int(v)) == _lib.OK
             continue
+        if kernel in _RENDER_KINDS:
+            for v in entries.values():
+                count += L.bajo_render_tuning_set(_RENDER_KINDS[kernel], int(v)) == _lib.OK
+            continue
         if kernel == "lbvh_one_launch":
             limits = set(entries.values())
             if len(limits) == 1:
@@ -222,12 +267,13 @@ def load(path: str = CACHE) -> int:
     return count
 
 
-PARTS = ("sort", "trace", "one_launch")
+PARTS = ("sort", "trace", "one_launch", "render")
 
 
 def tune_all(reps: int = 5, save_cache: bool = True, parts=PARTS) -> dict:
     """The sort shapes the LBVH build and the sort sweep use, the closest-hit
-    block sizes and the one-launch build's size limit (``parts`` selects)."""
+    block sizes, the one-launch build's size limit and the wavefront bounce
+    kernels' block sizes (``parts`` selects)."""
     res = {}
     if "sort" in parts:
         # 64-bit keys: up to 2^18 with the 30 live bits of single-scene LBVH
@@ -242,6 +288,8 @@ def tune_all(reps: int = 5, save_cache: bool = True, parts=PARTS) -> dict:
         res["trace_rays"] = tune_trace("trace_rays", range(16, 23, 2), reps=reps)
     if "one_launch" in parts:
         res["lbvh_one_launch"] = tune_one_launch(reps=reps)
+    if "render" in parts:
+        res.update(tune_render(reps=reps))
     if save_cache:
         save(res)
     return res

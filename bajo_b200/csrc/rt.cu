@@ -22,6 +22,7 @@
 //
 // Random streams and direction sampling: sampling.cuh.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -297,20 +298,21 @@ __device__ __forceinline__ f3 vmf_sample(const float* mu, float kappa, float u, 
   return normalize(d);
 }
 
-// 8 blocks of 128 per SM (64 registers, a few bytes spilled): the traversal is
-// latency bound and 32 resident warps hide more of it than 24 unspilled ones
-// (C2 render 142 ms against 159 ms at 80 registers).
-template <int ALGO, bool CW>
-__global__ void __launch_bounds__(kBlock, 8) trace_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
-                                                       uint32_t sample_base) {
+// 1,024 resident threads per SM whatever the block size BLK (64 registers, a
+// few bytes spilled): the traversal is latency bound and 32 resident warps
+// hide more of it than 24 unspilled ones (C2 render 142 ms against 159 ms at
+// 80 registers).
+template <int ALGO, bool CW, int BLK>
+__global__ void __launch_bounds__(BLK, 1024 / BLK) trace_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
+                                                             uint32_t sample_base) {
   constexpr bool kMisWeights = ALGO == BAJO_RENDER_MIS || ALGO == BAJO_RENDER_GUIDED;
   const uint32_t count = q.counters[2 * bounce];
   const uint32_t cap = q.capacity;
   const uint32_t* src_ids = q.ids[bounce & 1];
   const float* src = q.fields[bounce & 1];
   const uint32_t* src_rec = q.rec[bounce & 1];
-  const uint32_t stride = gridDim.x * kBlock;
-  for (uint32_t base = blockIdx.x * kBlock; base < count; base += stride) {
+  const uint32_t stride = gridDim.x * BLK;
+  for (uint32_t base = blockIdx.x * BLK; base < count; base += stride) {
     const uint32_t idx = base + threadIdx.x;
     bool want_vtx = false, want_mat = false;
     uint32_t path_id = 0, mat_leaf = 0;
@@ -595,13 +597,13 @@ __device__ __forceinline__ void emit(const Queues& q, const ShadeCtx& c, uint32_
   }
 }
 
-template <int ALGO>
-__global__ void __launch_bounds__(kBlock) shade_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
-                                                       uint32_t max_depth, uint32_t sample_base, uint64_t seed) {
+template <int ALGO, int BLK>
+__global__ void __launch_bounds__(BLK) shade_kernel(SceneView sc, Queues q, ShadeCtx c, uint32_t bounce,
+                                                    uint32_t max_depth, uint32_t sample_base, uint64_t seed) {
   const uint32_t cap = q.capacity;
   const uint32_t count = min(c.vcount[bounce], cap);
   const mlp::Mixture none{};
-  for (uint32_t base = blockIdx.x * kBlock; base < count; base += gridDim.x * kBlock) {
+  for (uint32_t base = blockIdx.x * BLK; base < count; base += gridDim.x * BLK) {
     const uint32_t i = base + threadIdx.x;
     ShadeOut o;
     if (i < count) shade_vertex<ALGO>(sc, c, cap, i, bounce, max_depth, seed, none, o);
@@ -749,13 +751,12 @@ __global__ void __launch_bounds__(kShadeThreads, 2) guided_shade_kernel(SceneVie
 // ---------------------------------------------------------------------------
 // any-hit shadow rays (gpu_rt_shadow_kernel, scene_trace.mojo:586)
 // ---------------------------------------------------------------------------
-template <bool CW>
-__global__ void __launch_bounds__(kBlock) shadow_kernel(SceneView sc, Queues q, uint32_t bounce,
-                                                        uint32_t sample_base) {
+template <bool CW, int BLK>
+__global__ void __launch_bounds__(BLK) shadow_kernel(SceneView sc, Queues q, uint32_t bounce, uint32_t sample_base) {
   const uint32_t count = q.counters[2 * bounce + 1];
   const uint32_t cap = q.capacity;
   const float* f = q.shadow_fields;
-  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < count; i += gridDim.x * kBlock) {
+  for (uint32_t i = blockIdx.x * BLK + threadIdx.x; i < count; i += gridDim.x * BLK) {
     const f3 o = mk(f[0 * cap + i], f[1 * cap + i], f[2 * cap + i]);
     const f3 d = mk(f[4 * cap + i], f[5 * cap + i], f[6 * cap + i]);
     bool open;
@@ -961,22 +962,81 @@ ShadeCtx shade_ctx(unsigned char* w, const Layout& L, const Queues& q, uint32_t 
   return c;
 }
 
+// Block sizes of the bounce kernels, chosen per launch from a process-wide
+// table the autotuner fills (bajo_render_tuning_set): kind 0 = closest hit
+// (trace_kernel), 1 = shading (shade_kernel), 2 = shadow rays
+// (shadow_kernel); -1 = the built-in 128.  The reference fixes 64
+// (GPU_RT_BLOCK_SIZE, bajo/rt/gpu/common_kernels.mojo:18).  The block size
+// changes only the launch shape: every path's work and random numbers depend
+// on its id, not on its queue slot, so every choice renders the same image.
+constexpr int kRenderKinds = 3, kRenderVariants = 3;
+constexpr int kRenderBlocks[kRenderVariants] = {128, 64, 256};
+std::atomic<int8_t> g_render_tuning[kRenderKinds] = {{-1}, {-1}, {-1}};
+
+int render_variant(int kind) {
+  const int v = g_render_tuning[kind].load(std::memory_order_relaxed);
+  return v >= 0 && v < kRenderVariants ? v : 0;
+}
+
+// grid of a grid-stride bounce kernel: one thread per queue slot, at most
+// 2,048 threads per SM
+uint32_t bounce_grid(uint32_t cap, int blk) {
+  uint32_t grid = (cap + blk - 1) / blk;
+  const uint32_t max_grid = (uint32_t)sm_count() * (2048u / (uint32_t)blk);
+  return grid > max_grid ? max_grid : grid;
+}
+
+template <int ALGO, bool CW>
+cudaError_t launch_trace(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t b, uint32_t sample_base,
+                         cudaStream_t st) {
+  const uint32_t cap = q.capacity;
+  switch (render_variant(0)) {
+    case 1: trace_kernel<ALGO, CW, 64><<<bounce_grid(cap, 64), 64, 0, st>>>(sc, q, c, b, sample_base); break;
+    case 2: trace_kernel<ALGO, CW, 256><<<bounce_grid(cap, 256), 256, 0, st>>>(sc, q, c, b, sample_base); break;
+    default: trace_kernel<ALGO, CW, 128><<<bounce_grid(cap, 128), 128, 0, st>>>(sc, q, c, b, sample_base);
+  }
+  return cudaGetLastError();
+}
+
+template <int ALGO>
+cudaError_t launch_shade(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t b, uint32_t max_depth,
+                         uint32_t sample_base, uint64_t seed, cudaStream_t st) {
+  const uint32_t cap = q.capacity;
+  switch (render_variant(1)) {
+    case 1:
+      shade_kernel<ALGO, 64><<<bounce_grid(cap, 64), 64, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
+      break;
+    case 2:
+      shade_kernel<ALGO, 256><<<bounce_grid(cap, 256), 256, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
+      break;
+    default:
+      shade_kernel<ALGO, 128><<<bounce_grid(cap, 128), 128, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
+  }
+  return cudaGetLastError();
+}
+
+template <bool CW>
+cudaError_t launch_shadow(const SceneView& sc, const Queues& q, uint32_t b, uint32_t sample_base, cudaStream_t st) {
+  const uint32_t cap = q.capacity;
+  switch (render_variant(2)) {
+    case 1: shadow_kernel<CW, 64><<<bounce_grid(cap, 64), 64, 0, st>>>(sc, q, b, sample_base); break;
+    case 2: shadow_kernel<CW, 256><<<bounce_grid(cap, 256), 256, 0, st>>>(sc, q, b, sample_base); break;
+    default: shadow_kernel<CW, 128><<<bounce_grid(cap, 128), 128, 0, st>>>(sc, q, b, sample_base);
+  }
+  return cudaGetLastError();
+}
+
 template <int ALGO, bool CW>
 cudaError_t launch_bounce_tree(const SceneView& sc, const Queues& q, const ShadeCtx& c, uint32_t grid, uint32_t b,
                                uint32_t max_depth, uint32_t sample_base, uint64_t seed, cudaStream_t st) {
-  trace_kernel<ALGO, CW><<<grid, kBlock, 0, st>>>(sc, q, c, b, sample_base);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = launch_trace<ALGO, CW>(sc, q, c, b, sample_base, st);
   if (e != cudaSuccess) return e;
-  shade_kernel<ALGO><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, sample_base, seed);
-  if ((e = cudaGetLastError()) != cudaSuccess) return e;
+  if ((e = launch_shade<ALGO>(sc, q, c, b, max_depth, sample_base, seed, st)) != cudaSuccess) return e;
   if (sc.has_materials) {
     material_kernel<ALGO, CW><<<grid, kBlock, 0, st>>>(sc, q, c, b, max_depth, seed);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
   }
-  if (ALGO != BAJO_RENDER_PATH) {
-    shadow_kernel<CW><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
-    e = cudaGetLastError();
-  }
+  if (ALGO != BAJO_RENDER_PATH) e = launch_shadow<CW>(sc, q, b, sample_base, st);
   return e;
 }
 
@@ -1015,11 +1075,6 @@ cudaError_t render_chunks(const BajoRenderSettings* s, const Layout& L, const Qu
   return cudaSuccess;
 }
 
-uint32_t bounce_grid(uint32_t cap) {
-  uint32_t grid = (cap + kBlock - 1) / kBlock;
-  const uint32_t max_grid = (uint32_t)sm_count() * 16;
-  return grid > max_grid ? max_grid : grid;
-}
 
 }  // namespace rt
 }  // namespace bajo
@@ -1047,7 +1102,7 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
   unsigned char* w = (unsigned char*)d_ws;
   if (!make_views(scene, w, L, sc, q)) return BAJO_ERR_INVALID_ARGUMENT;
   cudaStream_t st = (cudaStream_t)stream;
-  const uint32_t grid = bounce_grid(L.cap);
+  const uint32_t grid = bounce_grid(L.cap, kBlock);
   const int algo = s->algorithm;
   const ShadeCtx c = shade_ctx(w, L, q, s->max_depth);
   auto bounce = [&](uint32_t b, uint32_t sample_base) {
@@ -1116,12 +1171,11 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   uint32_t shade_grid = (L.cap + kShadeThreads - 1) / kShadeThreads;
   const uint32_t shade_max = (uint32_t)(sm_count() * per_sm);
   if (shade_grid > shade_max) shade_grid = shade_max;
-  const uint32_t grid = bounce_grid(L.cap);
+  const uint32_t grid = bounce_grid(L.cap, kBlock);
   if (!rb && cudaMemsetAsync(gc.rec_hdr, 0, 8, st) != cudaSuccess) return BAJO_ERR_CUDA;
   auto bounce = [&](uint32_t b, uint32_t sample_base) {
-    if (sc.use_cw) trace_kernel<BAJO_RENDER_GUIDED, true><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
-    else trace_kernel<BAJO_RENDER_GUIDED, false><<<grid, kBlock, 0, st>>>(sc, q, gc, b, sample_base);
-    cudaError_t e = cudaGetLastError();
+    cudaError_t e = sc.use_cw ? launch_trace<BAJO_RENDER_GUIDED, true>(sc, q, gc, b, sample_base, st)
+                              : launch_trace<BAJO_RENDER_GUIDED, false>(sc, q, gc, b, sample_base, st);
     if (e != cudaSuccess) return e;
     guided_shade_kernel<<<shade_grid, kShadeThreads, smem, st>>>(sc, q, gc, b, s->max_depth, sample_base, s->seed);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
@@ -1132,9 +1186,7 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
         material_kernel<BAJO_RENDER_GUIDED, false><<<grid, kBlock, 0, st>>>(sc, q, gc, b, s->max_depth, s->seed);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
     }
-    if (sc.use_cw) shadow_kernel<true><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
-    else shadow_kernel<false><<<grid, kBlock, 0, st>>>(sc, q, b, sample_base);
-    return cudaGetLastError();
+    return sc.use_cw ? launch_shadow<true>(sc, q, b, sample_base, st) : launch_shadow<false>(sc, q, b, sample_base, st);
   };
   auto before = [&]() {
     if (gc.rec_cap == 0) return cudaSuccess;
@@ -1149,6 +1201,24 @@ int32_t bajo_render_guided(const BajoRtScene* scene, const float* d_camera, cons
   const cudaError_t e = render_chunks(s, L, q, d_camera, d_pixels, d_pixels64, (unsigned long long*)(w + 8), st,
                                       bounce, before, after);
   return e == cudaSuccess ? BAJO_OK : BAJO_ERR_CUDA;
+}
+
+int32_t bajo_render_tuning_set(int32_t kernel, int32_t block) {
+  using namespace bajo::rt;
+  if (kernel < 0 || kernel >= kRenderKinds) return BAJO_ERR_INVALID_ARGUMENT;
+  int v = -1;
+  for (int k = 0; k < kRenderVariants; ++k)
+    if (kRenderBlocks[k] == block) v = k;
+  if (block != 0 && v < 0) return BAJO_ERR_INVALID_ARGUMENT;
+  g_render_tuning[kernel].store((int8_t)v);
+  return BAJO_OK;
+}
+
+int32_t bajo_render_tuning_get(int32_t kernel, int32_t* block) {
+  using namespace bajo::rt;
+  if (kernel < 0 || kernel >= kRenderKinds || !block) return BAJO_ERR_INVALID_ARGUMENT;
+  *block = kRenderBlocks[render_variant(kernel)];
+  return BAJO_OK;
 }
 
 int32_t bajo_render_stats(const void* d_ws, void* stream, uint64_t* rays, uint64_t* shadow_rays) {

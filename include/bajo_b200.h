@@ -559,6 +559,19 @@ int32_t bajo_render(const BajoRtScene* scene, const float* d_camera, const BajoR
  * the last bajo_render call on this workspace. */
 int32_t bajo_render_stats(const void* d_workspace, void* stream, uint64_t* rays, uint64_t* shadow_rays);
 
+/* Block sizes of the wavefront bounce kernels: 64, 128 or 256 threads (0
+ * restores the built-in 128), process-wide, per kernel: the path rays'
+ * closest hit, the shading of plain (non-guided) renders, the shadow rays.
+ * The reference fixes 64 (GPU_RT_BLOCK_SIZE,
+ * bajo/rt/gpu/common_kernels.mojo:18).  Every choice renders the same image
+ * bit for bit; the autotuner times them and installs the fastest.  Read when
+ * a render is launched (or recorded into a graph).  New on this path. */
+#define BAJO_RENDER_KERNEL_TRACE 0
+#define BAJO_RENDER_KERNEL_SHADE 1
+#define BAJO_RENDER_KERNEL_SHADOW 2
+int32_t bajo_render_tuning_set(int32_t kernel, int32_t block);
+int32_t bajo_render_tuning_get(int32_t kernel, int32_t* block);
+
 
 /* ======================================================================== */
 /* Path guiding: a small MLP proposal trained online (new on this path; the  */

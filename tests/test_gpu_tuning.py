@@ -1,5 +1,6 @@
 """Every choice the autotuner can install gives the same results: the
 closest-hit kernels' block sizes (64 / 128 / 256 threads) leave the hits
+bit-identical, the wavefront bounce kernels' block sizes leave the images
 bit-identical, and the one-launch build on or off leaves the tree
 bit-identical (its own parity is in test_gpu_lbvh_fused.py)."""
 import ctypes
@@ -98,3 +99,55 @@ def test_tuner_runs_and_keeps_results(oracle):
         for lg in range(33):
             L.bajo_trace_tuning_set(0, lg, 0)
         L.bajo_lbvh_fused_max_set(_lib.FUSED_MAX_LEAVES)
+
+
+@pytest.mark.parametrize("policy", ["lbvh", "cwbvh8"])
+def test_render_block_sizes_give_identical_images(policy):
+    """Every block size of the wavefront bounce kernels (closest hit,
+    shading, shadow rays) renders the same image bit for bit, for the plain
+    algorithms and the guided one, with materials and without."""
+    from bajo_b200 import _lib, guide, rt
+    L = _lib.load()
+    mats = scenes.materials_in_box(n_spheres=6, subdivisions=2)
+    lit = scenes.small_rt_scene()
+    w, h = 40, 24
+    images = {}
+    try:
+        for blocks in ((128, 128, 128), (64, 64, 64), (256, 256, 256), (64, 256, 128)):
+            for kind, blk in enumerate(blocks):
+                assert L.bajo_render_tuning_set(kind, blk) == _lib.OK
+                got = ctypes.c_int32(0)
+                assert L.bajo_render_tuning_get(kind, ctypes.byref(got)) == _lib.OK and got.value == blk
+            out = []
+            for sc in (lit, mats):
+                gsc = rt.GpuRtTriangleScene(sc, bvh_policy=policy)
+                for algorithm in (rt.PATH, rt.NEE, rt.MIS):
+                    settings = rt.RenderSettings(w, h, 4, rng_seed=7, max_depth=6)
+                    img = rt.render_gpu_triangles(settings, sc.camera, gsc, algorithm)
+                    out.append(img.cpu().numpy().view(np.uint32).copy())
+                gr = guide.GuidedRenderer(gsc, sc.camera, w, h, max_depth=6, record_capacity=1 << 12, steps=2,
+                                          batch=1 << 10, spp_per_pass=2)
+                # no training: its gradient atomics sum in any order
+                out.append(gr.render(passes=2, train_passes=0, seed=11).cpu().numpy().view(np.uint64).copy())
+                assert gr.workspace.status() == 0
+            torch.cuda.synchronize()
+            images[blocks] = out
+    finally:
+        for kind in range(3):
+            L.bajo_render_tuning_set(kind, 0)
+    ref = images[(128, 128, 128)]
+    for blocks, out in images.items():
+        for a, b in zip(out, ref):
+            assert np.array_equal(a, b), blocks
+
+
+def test_render_tuning_limits():
+    from bajo_b200 import _lib
+    L = _lib.load()
+    got = ctypes.c_int32(0)
+    assert L.bajo_render_tuning_set(0, 96) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_render_tuning_set(3, 64) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_render_tuning_set(-1, 64) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_render_tuning_get(0, None) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_render_tuning_set(2, 0) == _lib.OK
+    assert L.bajo_render_tuning_get(2, ctypes.byref(got)) == _lib.OK and got.value == 128
