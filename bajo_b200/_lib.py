@@ -129,6 +129,8 @@ SIGNATURES = {
     "bajo_lbvh_fused_top_cap_set": (_I32, [_U32]),
     "bajo_trace_tuning_set": (_I32, [_I32, _U32, _I32]),
     "bajo_trace_tuning_get": (_I32, [_I32, _U32, ctypes.POINTER(_I32)]),
+    "bajo_trace_stack_tuning_set": (_I32, [_I32, _U32, _I32]),
+    "bajo_trace_stack_tuning_get": (_I32, [_I32, _U32, ctypes.POINTER(_I32)]),
     "bajo_render_tuning_set": (_I32, [_I32, _I32]),
     "bajo_render_tuning_get": (_I32, [_I32, ctypes.POINTER(_I32)]),
     "bajo_lbvh_build_launches": (_I32, [_U32, _U32, ctypes.POINTER(_I32)]),

@@ -7,9 +7,11 @@ sizes, and the size limit of the one-launch build.
   allows on the current GPU with CUDA events and writes the fastest into the
   library's table (``bajo_sort_tuning_set``).
 - The unstaged closest-hit kernels (camera and general rays) are compiled
-  for blocks of 64, 128 and 256 threads; the tuner times each per ray-count
-  bucket on a tree of the plain workload's kind, checks that the hits are
-  identical, and installs the fastest (``bajo_trace_tuning_set``).
+  for blocks of 64, 128 and 256 threads and traversal stacks of 64, 24 and
+  12 entries (a ray that needs more entries is traced again with 64); the
+  tuner times each pair per ray-count bucket on a tree of the plain
+  workload's kind, checks that the hits are identical, and installs the
+  fastest (``bajo_trace_tuning_set``, ``bajo_trace_stack_tuning_set``).
 - The one-launch build is timed against the per-stage kernels at every
   power of two up to its limit, and the largest size up to which it wins is
   installed (``bajo_lbvh_fused_max_set``).
@@ -101,6 +103,7 @@ def tune_sort(key_bytes: int, has_values: bool, log2ns, end_bit: int | None = No
 
 
 TRACE_BLOCKS = (128, 64, 256)
+TRACE_STACKS = (64, 24, 12)
 _TRACE_KINDS = {"trace_camera": 0, "trace_rays": 1}
 
 
@@ -120,10 +123,11 @@ def _events_ms(fn, reps):
 
 
 def tune_trace(kernel: str, log2rays, n_tris: int = 65536, reps: int = 5) -> dict:
-    """Time every block size of one closest-hit kernel ("trace_camera" or
-    "trace_rays") at 2^log2rays rays over n_tris random triangles, check that
-    every block size gives the same hits bit for bit, and install the
-    fastest.  Returns {log2rays: {"best": block, "ms": {...}}}."""
+    """Time every block size x traversal stack depth of one closest-hit
+    kernel ("trace_camera" or "trace_rays") at 2^log2rays rays over n_tris
+    random triangles, check that every choice gives the same hits bit for
+    bit, and install the fastest pair.  Returns
+    {log2rays: {"best": block, "stack": depth, "ms": {"block/depth": ...}}}."""
     from . import bvh, camera, scenes
     L = _lib.load()
     kind = _TRACE_KINDS[kernel]
@@ -149,16 +153,20 @@ def tune_trace(kernel: str, log2rays, n_tris: int = 65536, reps: int = 5) -> dic
             fn = lambda: tree.launch_camera(cam, hits, n, w, h)  # noqa: E731
         times, ref = {}, None
         for blk in TRACE_BLOCKS:
-            _lib.check(L.bajo_trace_tuning_set(kind, lg, blk), "bajo_trace_tuning_set")
-            times[blk] = _events_ms(fn, reps)
-            got = hits.clone()
-            if ref is None:
-                ref = got
-            elif not torch.equal(got.view(torch.int32), ref.view(torch.int32)):
-                raise RuntimeError(f"{kernel}: block {blk} changed the hits")
-        best = min(times, key=times.get)
-        _lib.check(L.bajo_trace_tuning_set(kind, lg, best), "bajo_trace_tuning_set")
-        out[lg] = {"best": best, "ms": {str(k): round(t, 5) for k, t in times.items()}}
+            for depth in TRACE_STACKS:
+                _lib.check(L.bajo_trace_tuning_set(kind, lg, blk), "bajo_trace_tuning_set")
+                _lib.check(L.bajo_trace_stack_tuning_set(kind, lg, depth), "bajo_trace_stack_tuning_set")
+                times[(blk, depth)] = _events_ms(fn, reps)
+                got = hits.clone()
+                if ref is None:
+                    ref = got
+                elif not torch.equal(got.view(torch.int32), ref.view(torch.int32)):
+                    raise RuntimeError(f"{kernel}: block {blk}, stack {depth} changed the hits")
+        best_blk, best_depth = min(times, key=times.get)
+        _lib.check(L.bajo_trace_tuning_set(kind, lg, best_blk), "bajo_trace_tuning_set")
+        _lib.check(L.bajo_trace_stack_tuning_set(kind, lg, best_depth), "bajo_trace_stack_tuning_set")
+        ms = {f"{b}/{d}": round(t, 5) for (b, d), t in times.items()}
+        out[lg] = {"best": best_blk, "stack": best_depth, "ms": ms}
     return out
 
 
@@ -232,6 +240,9 @@ def save(results: dict, path: str = CACHE) -> None:
     dev = data.setdefault(device_key(), {})
     for kernel, table in results.items():
         dev.setdefault(kernel, {}).update({str(k): v["best"] for k, v in table.items()})
+        stacks = {str(k): v["stack"] for k, v in table.items() if "stack" in v}
+        if stacks:
+            dev.setdefault(kernel + "_stack", {}).update(stacks)
     with open(path, "w") as f:
         json.dump(data, f, indent=1, sort_keys=True)
 
@@ -249,6 +260,11 @@ def load(path: str = CACHE) -> int:
         if kernel in _TRACE_KINDS:
             for lg, v in entries.items():
                 count += L.bajo_trace_tuning_set(_TRACE_KINDS[kernel], int(lg), int(v)) == _lib.OK
+            continue
+        if kernel.endswith("_stack") and kernel[:-len("_stack")] in _TRACE_KINDS:
+            for lg, v in entries.items():
+                count += L.bajo_trace_stack_tuning_set(_TRACE_KINDS[kernel[:-len("_stack")]], int(lg),
+                                                       int(v)) == _lib.OK
             continue
         if kernel in _RENDER_KINDS:
             for v in entries.values():

@@ -48,7 +48,7 @@ struct StageSmem<true> {
   using type = TopSmem;
 };
 
-template <int MODE, bool TOP>
+template <int MODE, bool TOP, int STACK = kStack>
 __device__ __forceinline__ void ray_query(uint32_t i, const float* __restrict__ rays, uint32_t n, uint32_t n_nodes,
                                           uint32_t root, const float4* __restrict__ nb,
                                           const uint4* __restrict__ meta, const float4* __restrict__ tris,
@@ -62,14 +62,14 @@ __device__ __forceinline__ void ray_query(uint32_t i, const float* __restrict__ 
   Ray r = make_ray(o, d, tmin, tmax);
   Hit h;
   if constexpr (TOP) h = trace_bvh2_top<MODE>(r, root, nb, meta, tris, n_nodes, status, top);
-  else h = trace_bvh2<MODE>(r, root, nb, meta, tris, n_nodes, status);
+  else h = trace_bvh2<MODE, false, false, STACK>(r, root, nb, meta, tris, n_nodes, status);
   store_hit(h, tris, i, hits8, out_t, out_prim);
 }
 
 // Unstaged: 10 blocks of 128 per SM (48 registers): general rays are mostly
 // incoherent and latency bound, and the extra warps outweigh the spills
 // (+5% to +8% on random rays against 64 registers).
-template <int MODE, bool TOP, int BLK = kTraceBlock>
+template <int MODE, bool TOP, int BLK = kTraceBlock, int STACK = kStack>
 __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 1280 / BLK)
     trace_rays_kernel(const float* __restrict__ rays, uint32_t n, uint32_t n_nodes, const uint32_t* __restrict__ roots,
                       const float4* __restrict__ nb, const uint4* __restrict__ meta, const float4* __restrict__ tris,
@@ -84,15 +84,15 @@ __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 1
       ray_query<MODE, TOP>(i, rays, n, n_nodes, root, nb, meta, tris, top, hits8, out_t, out_prim, status);
     stage_top_drain(sm, top);
   } else if (i0 < n) {
-    ray_query<MODE, TOP>(i0, rays, n, n_nodes, __ldg(roots), nb, meta, tris, nullptr, hits8, out_t, out_prim,
-                         status);
+    ray_query<MODE, TOP, STACK>(i0, rays, n, n_nodes, __ldg(roots), nb, meta, tris, nullptr, hits8, out_t, out_prim,
+                                status);
   }
 }
 
 // camera.mojo:137-154 make_ray_raster; camera_launch.mojo:34-55.  With STATS
 // it also writes per-ray [node visits, triangle tests] like the reference's
 // instrumented kernel (triangle_bvh.mojo:813, GpuTraversalStats trace.mojo:62).
-template <int MODE, bool STATS, bool TOP>
+template <int MODE, bool STATS, bool TOP, int STACK = kStack>
 __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__ cams, uint32_t n_nodes,
                                            uint32_t width, uint32_t height, float inv_h, uint32_t root,
                                            const float4* __restrict__ nb, const uint4* __restrict__ meta,
@@ -115,7 +115,7 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   uint32_t st[kStatWords] = {0, 0, 0, 0, 0};
   Hit h;
   if constexpr (TOP) h = trace_bvh2_top<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, top, st);
-  else h = trace_bvh2<MODE, STATS>(r, root, nb, meta, tris, n_nodes, status, st);
+  else h = trace_bvh2<MODE, STATS, false, STACK>(r, root, nb, meta, tris, n_nodes, status, st);
   store_hit(h, tris, i, hits8, out_t, out_prim);
   if constexpr (STATS) {
 #pragma unroll
@@ -123,7 +123,7 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   }
 }
 
-template <int MODE, bool STATS, bool TOP, int BLK = kTraceBlock>
+template <int MODE, bool STATS, bool TOP, int BLK = kTraceBlock, int STACK = kStack>
 __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0)
     trace_camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t n_nodes, uint32_t width, uint32_t height,
                         float inv_h, const uint32_t* __restrict__ roots, const float4* __restrict__ nb,
@@ -141,8 +141,8 @@ __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0
                                    out_prim, status, stats);
     stage_top_drain(sm, top);
   } else if (i0 < n) {
-    camera_ray<MODE, STATS, TOP>(i0, cams, n_nodes, width, height, inv_h, __ldg(roots), nb, meta, tris, nullptr,
-                                 hits8, out_t, out_prim, status, stats);
+    camera_ray<MODE, STATS, TOP, STACK>(i0, cams, n_nodes, width, height, inv_h, __ldg(roots), nb, meta, tris,
+                                        nullptr, hits8, out_t, out_prim, status, stats);
   }
 }
 
@@ -235,7 +235,29 @@ int trace_variant(int kind, uint32_t n) {
   return v >= 0 && v < kTraceVariants ? v : 0;
 }
 
-template <int MODE, bool TOP, int BLK>
+// Traversal stack depths of the same kernels, from a second table of the
+// same shape (bajo_trace_stack_tuning_set); -1 means kStack (64).  A
+// shallower stack keeps the traversal's local-memory footprint small; a ray
+// that needs more entries is traced again with kStack, so every depth gives
+// the same hits.  24 is the reference's GPU_STACK_SIZE
+// (bajo/bvh/constants.mojo:16).
+constexpr int kStackVariants = 3;
+constexpr int kTraceStacks[kStackVariants] = {kStack, 24, 12};
+std::atomic<int8_t> g_stack_tuning[2][33];
+std::once_flag g_stack_tuning_once;
+
+int stack_variant(int kind, uint32_t n) {
+  std::call_once(g_stack_tuning_once, [] {
+    for (auto& row : g_stack_tuning)
+      for (auto& v : row) v.store(-1);
+  });
+  uint32_t lg = 0;
+  while (lg < 32 && (1ull << lg) < n) ++lg;
+  const int v = g_stack_tuning[kind][lg].load(std::memory_order_relaxed);
+  return v >= 0 && v < kStackVariants ? v : 0;
+}
+
+template <int MODE, bool TOP, int BLK, int STACK = kStack>
 void launch_rays_blk(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
                      uint32_t* status, cudaStream_t st) {
   const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
@@ -243,8 +265,18 @@ void launch_rays_blk(const BajoLbvh* b, const float* rays, uint32_t n, float* hi
   const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
   const uint32_t grid = TOP ? top_grid(trace_rays_kernel<MODE, TOP>, n) : (n + BLK - 1) / BLK;
-  trace_rays_kernel<MODE, TOP, BLK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(rays, n, b->n_leaves, b->roots, nb,
-                                                                            meta, tris, top, hits8, t, prim, status);
+  trace_rays_kernel<MODE, TOP, BLK, STACK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
+      rays, n, b->n_leaves, b->roots, nb, meta, tris, top, hits8, t, prim, status);
+}
+
+template <int MODE, int BLK>
+void launch_rays_stack(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8, float* t, uint32_t* prim,
+                       uint32_t* status, cudaStream_t st) {
+  switch (stack_variant(1, n)) {
+    case 1: return launch_rays_blk<MODE, false, BLK, 24>(b, rays, n, hits8, t, prim, status, st);
+    case 2: return launch_rays_blk<MODE, false, BLK, 12>(b, rays, n, hits8, t, prim, status, st);
+    default: return launch_rays_blk<MODE, false, BLK, kStack>(b, rays, n, hits8, t, prim, status, st);
+  }
 }
 
 template <int MODE, bool TOP>
@@ -254,14 +286,14 @@ void launch_rays(const BajoLbvh* b, const float* rays, uint32_t n, float* hits8,
     launch_rays_blk<MODE, TOP, kTraceBlock>(b, rays, n, hits8, t, prim, status, st);
   } else {
     switch (trace_variant(1, n)) {
-      case 1: return launch_rays_blk<MODE, TOP, 64>(b, rays, n, hits8, t, prim, status, st);
-      case 2: return launch_rays_blk<MODE, TOP, 256>(b, rays, n, hits8, t, prim, status, st);
-      default: return launch_rays_blk<MODE, TOP, 128>(b, rays, n, hits8, t, prim, status, st);
+      case 1: return launch_rays_stack<MODE, 64>(b, rays, n, hits8, t, prim, status, st);
+      case 2: return launch_rays_stack<MODE, 256>(b, rays, n, hits8, t, prim, status, st);
+      default: return launch_rays_stack<MODE, 128>(b, rays, n, hits8, t, prim, status, st);
     }
   }
 }
 
-template <int MODE, bool STATS, bool TOP, int BLK>
+template <int MODE, bool STATS, bool TOP, int BLK, int STACK = kStack>
 void launch_camera_blk(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height,
                        float* hits8, float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
   const float4* nb = reinterpret_cast<const float4*>(b->node_bounds);
@@ -270,8 +302,24 @@ void launch_camera_blk(const BajoLbvh* b, const float* cams, uint32_t n, uint32_
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
   const float inv_h = 1.0f / (float)height;
   const uint32_t grid = TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (n + BLK - 1) / BLK;
-  trace_camera_kernel<MODE, STATS, TOP, BLK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
+  trace_camera_kernel<MODE, STATS, TOP, BLK, STACK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
       cams, n, b->n_leaves, width, height, inv_h, b->roots, nb, meta, tris, top, hits8, t, prim, status, stats);
+}
+
+template <int MODE, int BLK>
+void launch_camera_stack(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t width, uint32_t height,
+                         float* hits8, float* t, uint32_t* prim, uint32_t* status, cudaStream_t st) {
+  switch (stack_variant(0, n)) {
+    case 1:
+      return launch_camera_blk<MODE, false, false, BLK, 24>(b, cams, n, width, height, hits8, t, prim, status,
+                                                            nullptr, st);
+    case 2:
+      return launch_camera_blk<MODE, false, false, BLK, 12>(b, cams, n, width, height, hits8, t, prim, status,
+                                                            nullptr, st);
+    default:
+      return launch_camera_blk<MODE, false, false, BLK, kStack>(b, cams, n, width, height, hits8, t, prim, status,
+                                                                nullptr, st);
+  }
 }
 
 template <int MODE, bool STATS, bool TOP>
@@ -281,14 +329,9 @@ void launch_camera(const BajoLbvh* b, const float* cams, uint32_t n, uint32_t wi
     launch_camera_blk<MODE, STATS, TOP, kTraceBlock>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
   } else {
     switch (trace_variant(0, n)) {
-      case 1:
-        return launch_camera_blk<MODE, STATS, TOP, 64>(b, cams, n, width, height, hits8, t, prim, status, stats, st);
-      case 2:
-        return launch_camera_blk<MODE, STATS, TOP, 256>(b, cams, n, width, height, hits8, t, prim, status, stats,
-                                                        st);
-      default:
-        return launch_camera_blk<MODE, STATS, TOP, 128>(b, cams, n, width, height, hits8, t, prim, status, stats,
-                                                        st);
+      case 1: return launch_camera_stack<MODE, 64>(b, cams, n, width, height, hits8, t, prim, status, st);
+      case 2: return launch_camera_stack<MODE, 256>(b, cams, n, width, height, hits8, t, prim, status, st);
+      default: return launch_camera_stack<MODE, 128>(b, cams, n, width, height, hits8, t, prim, status, st);
     }
   }
 }
@@ -348,6 +391,25 @@ int32_t bajo_trace_tuning_get(int32_t kind, uint32_t n, int32_t* block) {
   using namespace bajo;
   if ((kind != 0 && kind != 1) || !block) return BAJO_ERR_INVALID_ARGUMENT;
   *block = kTraceBlocks[trace_variant(kind, n)];
+  return BAJO_OK;
+}
+
+int32_t bajo_trace_stack_tuning_set(int32_t kind, uint32_t log2n, int32_t depth) {
+  using namespace bajo;
+  if ((kind != 0 && kind != 1) || log2n > 32) return BAJO_ERR_INVALID_ARGUMENT;
+  int v = -1;
+  for (int k = 0; k < kStackVariants; ++k)
+    if (kTraceStacks[k] == depth) v = k;
+  if (depth != 0 && v < 0) return BAJO_ERR_INVALID_ARGUMENT;
+  stack_variant(0, 1);  // initialise the table
+  g_stack_tuning[kind][log2n].store((int8_t)v);
+  return BAJO_OK;
+}
+
+int32_t bajo_trace_stack_tuning_get(int32_t kind, uint32_t n, int32_t* depth) {
+  using namespace bajo;
+  if ((kind != 0 && kind != 1) || !depth) return BAJO_ERR_INVALID_ARGUMENT;
+  *depth = kTraceStacks[stack_variant(kind, n)];
   return BAJO_OK;
 }
 

@@ -261,10 +261,16 @@ __device__ __forceinline__ void stage_top_drain(TopSmem& sm, const float4* stage
   if (staged == nullptr && threadIdx.x == 0) mbar_wait_bounded(smem_addr(&sm.bar), 0);
 }
 
+// A traversal with a stack shallower than kStack that runs out of entries
+// returns this in Hit::leaf; trace_bvh2 then traces the ray again with the
+// full stack, so every stack depth gives the same hit.
+constexpr uint32_t kRetrace = 0xFFFFFFFEu;
+
 // max_nodes: node visits allowed (the node count): a tree is never visited
 // twice per node, so more visits means a corrupt tree.  With TOP, `top` holds
-// the staged records and refs tagged BAJO_TOP_FLAG are read from it.
-template <int MODE, bool STATS, bool ANY, bool PAR, bool TOP = false>
+// the staged records and refs tagged BAJO_TOP_FLAG are read from it.  STACK
+// entries of traversal stack (kStack holds the deepest Karras tree).
+template <int MODE, bool STATS, bool ANY, bool PAR, bool TOP = false, int STACK = kStack>
 __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                                const uint4* __restrict__ meta, const float4* __restrict__ tris,
                                                uint32_t max_nodes, uint32_t* status, uint32_t* stats,
@@ -285,7 +291,8 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
   }
   // any-hit queries stop at the first accepted triangle; boxes are culled
   // against the ray's own t_max (bajo/bvh/gpu/trace.mojo:458-499)
-  uint32_t stack[kStack];
+  static_assert(STACK >= 1 && STACK <= kStack, "traversal stack depth");
+  uint32_t stack[STACK];
   int sp = 0;
   uint32_t cur = root;
   for (uint32_t visits = 0;; ++visits) {
@@ -346,8 +353,14 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
       const float far_t = near == 0 ? tr : tl;
       const float near_t = near == 0 ? tl : tr;
       if (far_valid && far_t <= limit) {
-        if (sp < kStack) stack[sp++] = near == 0 ? m.y : m.x;
-        else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+        if (sp < STACK) {
+          stack[sp++] = near == 0 ? m.y : m.x;
+        } else if constexpr (STACK < kStack) {
+          h.leaf = kRetrace;  // the caller traces this ray again with kStack entries
+          return h;
+        } else {
+          raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+        }
         if constexpr (STATS) stats[kStatMaxStack] = max(stats[kStatMaxStack], (uint32_t)sp);
       }
       if (near_t <= limit) {
@@ -362,13 +375,24 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
 }
 
 // Rays with an axis parallel to the boxes (|d| <= 1e-9) take the containment
-// slab; every other ray takes the select-free one.
-template <int MODE, bool STATS = false, bool ANY = false>
+// slab; every other ray takes the select-free one.  With STACK < kStack a ray
+// whose traversal needs more entries is traced again with kStack (counted
+// twice by STATS, which the instrumented kernels therefore never combine
+// with a short stack).
+template <int MODE, bool STATS = false, bool ANY = false, int STACK = kStack>
 __device__ __forceinline__ Hit trace_bvh2(const Ray& r, uint32_t root, const float4* __restrict__ nb,
                                           const uint4* __restrict__ meta, const float4* __restrict__ tris,
                                           uint32_t max_nodes, uint32_t* status, uint32_t* stats = nullptr) {
-  if (has_parallel_axis(r))
+  static_assert(STACK == kStack || !STATS, "instrumented traversals use the full stack");
+  if (has_parallel_axis(r)) {
+    const Hit h = trace_bvh2_impl<MODE, STATS, ANY, true, false, STACK>(r, root, nb, meta, tris, max_nodes, status,
+                                                                         stats);
+    if (STACK == kStack || h.leaf != kRetrace) return h;
     return trace_bvh2_impl<MODE, STATS, ANY, true>(r, root, nb, meta, tris, max_nodes, status, stats);
+  }
+  const Hit h = trace_bvh2_impl<MODE, STATS, ANY, false, false, STACK>(r, root, nb, meta, tris, max_nodes, status,
+                                                                        stats);
+  if (STACK == kStack || h.leaf != kRetrace) return h;
   return trace_bvh2_impl<MODE, STATS, ANY, false>(r, root, nb, meta, tris, max_nodes, status, stats);
 }
 

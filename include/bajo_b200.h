@@ -269,6 +269,13 @@ int32_t bajo_trace_rays(const BajoLbvh* bvh, const float* d_rays, uint32_t n_ray
  * a call of n rays would use. */
 int32_t bajo_trace_tuning_set(int32_t kind, uint32_t log2n, int32_t block);
 int32_t bajo_trace_tuning_get(int32_t kind, uint32_t n, int32_t* block);
+/* The same kernels' traversal stack depth: 64, 24 (the reference's
+ * GPU_STACK_SIZE, bajo/bvh/constants.mojo:16) or 12 entries (0 = 64), per
+ * kind and ceil(log2 n).  A ray whose traversal needs more entries than the
+ * chosen depth is traced again with 64, so the hits do not depend on it
+ * either.  New on this path. */
+int32_t bajo_trace_stack_tuning_set(int32_t kind, uint32_t log2n, int32_t depth);
+int32_t bajo_trace_stack_tuning_get(int32_t kind, uint32_t n, int32_t* depth);
 
 /* Replaces GpuTriangleBvh.launch_camera (bajo/bvh/gpu/triangle_bvh.mojo:520):
  * primary rays generated in-kernel from 20-float camera records

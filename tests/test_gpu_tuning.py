@@ -26,6 +26,94 @@ def _rays(n, seed):
     return r.reshape(-1)
 
 
+def _deep_stack_scene(p=(0.5, 0.5, 0.5)):
+    """64 triangles whose box centres give the Morton codes 0, 1, 2, 4, ...,
+    2^29 and all ones (two triangles each), every box containing `p`.  The
+    Karras tree is then a spine of 31 levels whose right children are 2-leaf
+    subtrees; a ray from `p` enters every box at t = 0, so it descends the
+    spine (ties go left) and pushes every right child: 30 stack entries."""
+    p = np.asarray(p, np.float64)
+    centres = [np.zeros(3)]  # code 0 (also the centroid bounds' minimum)
+    for k in range(30):  # code 1 << k: axis k % 3 (x least significant), quantised value 2^(k // 3)
+        u = np.full(3, 0.25 / 1024)
+        u[k % 3] = (2 ** (k // 3) + 0.5) / 1024
+        centres.append(u)
+    centres.append(np.ones(3))  # all ones (the maximum)
+    tris = []
+    for m in centres:
+        h = np.abs(p - m) + 0.01
+        for j in range(2):
+            tris.append(np.stack([m - h, m + h, m + np.array([h[0], -h[1], 0.0]) * (0.5 + 0.25 * j)]))
+    return np.array(tris, np.float32).reshape(-1)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_trace_stack_depths_give_identical_hits(oracle, mode):
+    """Every traversal stack depth (64, the reference's 24, 12) and block
+    size of the closest-hit kernels gives the oracle's hits bit for bit, on
+    a scene whose rays need 30 stack entries: with 24 or 12 every ray runs
+    out and is traced again with 64."""
+    from bajo_b200 import _lib, bvh, camera
+    L = _lib.load()
+    v = _deep_stack_scene()
+    tree = bvh.build_triangle_bvh(torch.from_numpy(v).cuda())
+    cam_np = camera.camera_from_vfov([0.5, 0.5, 0.5], [0.9, 0.7, 1.0], [0.0, 1.0, 0.0], 90.0)
+    cam = torch.from_numpy(cam_np).cuda()
+    w, h = 64, 48
+    n = w * h
+    m = 5000
+    g = np.random.default_rng(2)
+    r = np.zeros((8, m), np.float32)
+    r[0:3] = 0.5
+    d = g.normal(size=(3, m))
+    r[4:7] = d / np.linalg.norm(d, axis=0)
+    r[7] = 3.0e38
+    r = r.reshape(-1)
+    rays = torch.from_numpy(r).cuda()
+    stats = torch.zeros(bvh.STATS_WORDS * n, dtype=torch.int32, device="cuda")
+    tree.launch_camera_instrumented(cam, None, stats, n, w, h, tri_mode=mode)
+    assert int(stats.view(n, bvh.STATS_WORDS)[:, 4].min().item()) > 24
+    ob = oracle.lbvh_build(v)
+    ref_cam = oracle.trace_bvh2(ob, oracle.camera_rays(cam_np, n, w, h), mode).view(np.uint32)
+    ref_rays = oracle.trace_bvh2(ob, r, mode).view(np.uint32)
+    try:
+        for blk in (64, 128, 256):
+            for depth in (64, 24, 12):
+                for kind, cnt in ((0, n), (1, m)):
+                    lg = int(np.ceil(np.log2(cnt)))
+                    assert L.bajo_trace_tuning_set(kind, lg, blk) == _lib.OK
+                    assert L.bajo_trace_stack_tuning_set(kind, lg, depth) == _lib.OK
+                    got = ctypes.c_int32(0)
+                    assert L.bajo_trace_stack_tuning_get(kind, cnt, ctypes.byref(got)) == _lib.OK
+                    assert got.value == depth
+                status = torch.zeros(1, dtype=torch.int32, device="cuda")
+                hc = torch.empty(8 * n, dtype=torch.float32, device="cuda")
+                tree.launch_camera(cam, hc, n, w, h, tri_mode=mode, d_status=status)
+                hr = torch.empty(8 * m, dtype=torch.float32, device="cuda")
+                tree.launch_rays(rays, hr, m, tri_mode=mode, d_status=status)
+                torch.cuda.synchronize()
+                assert int(status.item()) == 0, (blk, depth)
+                assert np.array_equal(hc.cpu().numpy().view(np.uint32), ref_cam), (blk, depth)
+                assert np.array_equal(hr.cpu().numpy().view(np.uint32), ref_rays), (blk, depth)
+    finally:
+        for kind in (0, 1):
+            for lg in range(33):
+                L.bajo_trace_tuning_set(kind, lg, 0)
+                L.bajo_trace_stack_tuning_set(kind, lg, 0)
+
+
+def test_trace_stack_tuning_limits():
+    from bajo_b200 import _lib
+    L = _lib.load()
+    got = ctypes.c_int32(0)
+    assert L.bajo_trace_stack_tuning_set(0, 20, 16) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_stack_tuning_set(2, 20, 24) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_stack_tuning_set(1, 33, 24) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_stack_tuning_get(0, 100, None) == _lib.ERR_INVALID_ARGUMENT
+    assert L.bajo_trace_stack_tuning_set(1, 20, 0) == _lib.OK
+    assert L.bajo_trace_stack_tuning_get(1, 1 << 20, ctypes.byref(got)) == _lib.OK and got.value == 64
+
+
 @pytest.mark.parametrize("mode", [0, 1])
 def test_trace_block_sizes_give_identical_hits(oracle, mode):
     from bajo_b200 import _lib, bvh, camera
