@@ -42,6 +42,9 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
   uint2 stack[kStack];
   int sp = 0;
   uint32_t nbase = 0, nmask = 0x80000000u, tbase = 0, tmask = 0, visits = 0;
+  // a corrupt tree ends the walk; the status bit is raised after the loop,
+  // which keeps the atomic out of the loop's code
+  uint32_t fail = 0;
   for (;;) {
     if (nmask > 0x00FFFFFFu) {
       const uint32_t gm = nmask;
@@ -49,7 +52,7 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       nmask &= ~(1u << bit);
       if (nmask > 0x00FFFFFFu) {
         if (sp >= kStack) {
-          raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+          fail = BAJO_STATUS_STACK_OVERFLOW;
           break;
         }
         stack[sp++] = make_uint2(nbase, nmask);
@@ -57,7 +60,7 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       const uint32_t slot = ((uint32_t)bit - 24u) ^ oi;
       const uint32_t ni = nbase + (uint32_t)__popc(gm & ((1u << slot) - 1u));
       if (ni >= tr.n_nodes || ++visits > tr.n_nodes) {
-        raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+        fail = BAJO_STATUS_BAD_TOPOLOGY;
         break;
       }
       const float4* nd = tr.nodes + (size_t)ni * 5;
@@ -110,8 +113,8 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       tmask &= ~(1u << bit);
       const uint32_t ti = tbase + (uint32_t)bit;
       if (ti >= tr.n_tris) {
-        raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
-        return h;
+        fail = BAJO_STATUS_BAD_TOPOLOGY;
+        break;
       }
       const float4* rec = tr.tris + (size_t)ti * 3;
       const float4 a = __ldg(rec + 0), b = __ldg(rec + 1), c = __ldg(rec + 2);
@@ -139,6 +142,7 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       h.prim = __float_as_uint(c.w);
       h.tri = ti;
     }
+    if (fail) break;
     if (nmask <= 0x00FFFFFFu) {
       if (sp == 0) break;
       --sp;
@@ -146,6 +150,7 @@ __device__ __forceinline__ Hit trace(f3 o, f3 d, float tmin, float tmax, const T
       nmask = stack[sp].y;
     }
   }
+  if (fail) raise_status(status, fail);
   return h;
 }
 

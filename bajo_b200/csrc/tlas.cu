@@ -116,9 +116,10 @@ __device__ Hit trace_impl(const trav::Ray& r, const Top& top, const Blas& bl, ui
   uint32_t stack[trav::kStack];
   int sp = 0;
   uint32_t cur = root;
+  uint32_t fail = 0;  // status bits, raised after the loop (no atomic in the loop's code)
   for (uint32_t visits = 0;; ++visits) {
     if (visits >= top.max_nodes || cur >= top.max_nodes) {
-      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      fail |= BAJO_STATUS_BAD_TOPOLOGY;
       break;
     }
     const float4 b0 = __ldg(top.nb + (size_t)cur * 3 + 0), b1 = __ldg(top.nb + (size_t)cur * 3 + 1),
@@ -132,12 +133,18 @@ __device__ Hit trace_impl(const trav::Ray& r, const Top& top, const Blas& bl, ui
     bool vl = false, vr = false;
     if (hl) {
       if (m.x & kLeafFlag) {
-        if (test_instance<MODE, ANY>(r, m.x & kIndexMask, top, bl, h, status) && ANY) return h;
+        if (test_instance<MODE, ANY>(r, m.x & kIndexMask, top, bl, h, status) && ANY) {
+          if (fail) raise_status(status, fail);
+          return h;
+        }
       } else vl = true;
     }
     if (hr) {
       if (m.y & kLeafFlag) {
-        if (test_instance<MODE, ANY>(r, m.y & kIndexMask, top, bl, h, status) && ANY) return h;
+        if (test_instance<MODE, ANY>(r, m.y & kIndexMask, top, bl, h, status) && ANY) {
+          if (fail) raise_status(status, fail);
+          return h;
+        }
       } else vr = true;
     }
     int near = -1;
@@ -150,7 +157,7 @@ __device__ Hit trace_impl(const trav::Ray& r, const Top& top, const Blas& bl, ui
       const float near_t = near == 0 ? tl : tr;
       if (far_valid && far_t <= limit) {
         if (sp < trav::kStack) stack[sp++] = near == 0 ? m.y : m.x;
-        else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+        else fail |= BAJO_STATUS_STACK_OVERFLOW;
       }
       if (near_t <= limit) {
         cur = near == 0 ? m.x : m.y;
@@ -160,6 +167,7 @@ __device__ Hit trace_impl(const trav::Ray& r, const Top& top, const Blas& bl, ui
     if (sp == 0) break;
     cur = stack[--sp];
   }
+  if (fail) raise_status(status, fail);
   return h;
 }
 

@@ -295,10 +295,13 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
   uint32_t stack[STACK];
   int sp = 0;
   uint32_t cur = root;
+  // a corrupt tree or a full stack ends the walk; the status bit is raised
+  // after the loop, which keeps the atomic out of the loop's code
+  uint32_t fail = 0;
   for (uint32_t visits = 0;; ++visits) {
     const bool staged = TOP && (cur & BAJO_TOP_FLAG);
     if (visits >= max_nodes || (staged ? (cur & kTopMask) >= BAJO_TOP_NODES : cur >= max_nodes)) {
-      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      fail = BAJO_STATUS_BAD_TOPOLOGY;
       break;
     }
     if constexpr (STATS) ++stats[kStatNodeVisits];
@@ -358,8 +361,9 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
         } else if constexpr (STACK < kStack) {
           h.leaf = kRetrace;  // the caller traces this ray again with kStack entries
           return h;
-        } else {
-          raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+        } else {  // deeper than any Karras tree over 64-bit keys: a corrupt tree
+          fail = BAJO_STATUS_STACK_OVERFLOW;
+          break;
         }
         if constexpr (STATS) stats[kStatMaxStack] = max(stats[kStatMaxStack], (uint32_t)sp);
       }
@@ -371,6 +375,7 @@ __device__ __forceinline__ Hit trace_bvh2_impl(const Ray& r, uint32_t root, cons
     if (sp == 0) break;
     cur = stack[--sp];
   }
+  if (fail) raise_status(status, fail);
   return h;
 }
 

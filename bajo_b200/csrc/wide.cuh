@@ -149,9 +149,10 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
   uint2 stack[trav::kStack];
   int sp = 0;
   uint32_t cur = 0;
+  uint32_t fail = 0;  // status bits, raised after the loop (no atomic in the loop's code)
   for (uint32_t visits = 0;; ++visits) {
     if (visits >= v.n_nodes || cur >= v.n_nodes) {
-      raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+      fail |= BAJO_STATUS_BAD_TOPOLOGY;
       break;
     }
     if constexpr (STATS) ++stats[trav::kStatNodeVisits];
@@ -186,7 +187,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
         continue;
       }
       if (data >= v.n_blocks) {
-        raise_status(status, BAJO_STATUS_BAD_TOPOLOGY);
+        fail |= BAJO_STATUS_BAD_TOPOLOGY;
         continue;
       }
       if constexpr (STATS) ++stats[trav::kStatLeafBlocks];
@@ -217,7 +218,10 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
           h.v = vv;
           h.prim = prim;
           h.leaf = __ldg(v.leaf_sorted + (size_t)data * W + k);
-          if (ANY) return h;
+          if (ANY) {
+            if (fail) raise_status(status, fail);
+            return h;
+          }
         }
       }
     }
@@ -240,7 +244,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
     for (int k = nc - 1; k >= 1; --k) {
       if (ct[k] > limit) continue;
       if (sp < trav::kStack) stack[sp++] = make_uint2(ci[k], __float_as_uint(ct[k]));
-      else raise_status(status, BAJO_STATUS_STACK_OVERFLOW);
+      else fail |= BAJO_STATUS_STACK_OVERFLOW;
       if constexpr (STATS) stats[trav::kStatMaxStack] = max(stats[trav::kStatMaxStack], (uint32_t)sp);
     }
     if (nc > 0 && ct[0] <= limit) {
@@ -258,6 +262,7 @@ __device__ __forceinline__ trav::Hit trace_wide_impl(const trav::Ray& r, const V
     }
     if (!found) break;
   }
+  if (fail) raise_status(status, fail);
   return h;
 }
 
