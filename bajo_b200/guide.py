@@ -236,6 +236,8 @@ class GuidedRenderer:
         self.box = scene.tree.seg_bounds[:6]
         self.settings = rt.RenderSettings(width, height, spp_per_pass, max_depth=max_depth, chunk_paths=chunk_paths)
         self.workspace = rt.RenderWorkspace(self.settings, GUIDED, dev)
+        self._chunk_paths = chunk_paths
+        self._by_spp = {spp_per_pass: (self.settings, self.workspace)}
         self.pixels = torch.empty((height, width, 3), dtype=torch.float32, device=dev)
         self.sum64 = torch.zeros((height, width, 3), dtype=torch.float64, device=dev)
         self.samples = 0
@@ -245,11 +247,32 @@ class GuidedRenderer:
         return BajoGuideC(self.net.params16.data_ptr(), self.box.data_ptr(), fraction, self.record_fraction,
                           self.records.capacity if collect else 0, self.records.buffer.data_ptr() if collect else None)
 
-    def render_pass(self, seed: int, train: bool = True, guide_fraction: float | None = None, stream=None):
-        """One pass added into the FP64 sum; trains afterwards when asked."""
+    def prepare_pass(self, spp: int) -> None:
+        """Allocate the workspace of passes of `spp` samples per pixel now,
+        so that the first such pass does not pay for the allocation."""
+        self._settings_for(spp)
+
+    def _settings_for(self, spp: int):
+        """Settings and workspace of a pass of `spp` samples per pixel (the
+        workspace's path capacity depends on it)."""
+        if spp not in self._by_spp:
+            s = rt.RenderSettings(self.width, self.height, spp, max_depth=self.max_depth,
+                                  chunk_paths=self._chunk_paths)
+            self._by_spp[spp] = (s, rt.RenderWorkspace(s, GUIDED, self.workspace.buffer.device))
+        return self._by_spp[spp]
+
+    def render_pass(self, seed: int, train: bool = True, guide_fraction: float | None = None, stream=None,
+                    spp: int | None = None):
+        """One pass of `spp` samples per pixel (default spp_per_pass) added
+        into the FP64 sum; trains afterwards when asked.  Larger passes after
+        training use the GPU better: the later bounces' kernels of a small
+        pass run with few paths."""
         f = self.guide_fraction if guide_fraction is None else guide_fraction
-        self.settings.rng_seed = seed
-        c = self.settings.c(GUIDED)
+        spp = self.spp_per_pass if spp is None else spp
+        settings, workspace = self._settings_for(spp)
+        self.workspace = workspace
+        settings.rng_seed = seed
+        c = settings.c(GUIDED)
         if train:
             self.records.reset()
         g = self.guide_c(f, train)
@@ -261,7 +284,7 @@ class GuidedRenderer:
                                         _lib.stream_handle(stream)), "bajo_render_guided")
         if train:
             self.net.train_records(self.records, self.box, self.batch, self.steps, self.lr, stream)
-        self.samples += self.spp_per_pass
+        self.samples += spp
         self.passes += 1
 
     def render(self, passes: int, train_passes: int, seed: int = 2026) -> torch.Tensor:

@@ -126,6 +126,8 @@ def parse_args(argv=None):
                    help="--case guided: guide the first pass too (by default it samples the BSDF only, since the "
                         "network is untrained)")
     p.add_argument("--train-steps", type=int, default=64, help="--case guided Adam steps per training pass")
+    p.add_argument("--late-spp", type=int, default=4,
+                   help="--case guided samples per pixel of the passes after the training passes")
     p.add_argument("--records", type=int, default=1 << 20,
                    help="--case guided training records kept per pass (batches of 2^14 are drawn from them)")
     return p.parse_args(argv)
@@ -1082,12 +1084,17 @@ def run_guided(args):
     1280x720, depth 8.  Error = MSE against a ``--ref-spp`` plain MIS render
     accumulated in FP64.  Plain: one 64-spp MIS render, device-timed.
     Guided: progressive passes of ``--spp-per-pass`` with the network trained
-    after each of the first ``--train-passes`` passes (training time counted);
-    the first pass samples the BSDF only (``--first-guided`` guides it too),
-    since an untrained network only adds variance;
+    after each of the first ``--train-passes`` passes (training time counted),
+    then passes of ``--late-spp`` (larger passes keep the GPU busier in the
+    later bounces); the first pass samples the BSDF only (``--first-guided``
+    guides it too), since an untrained network only adds variance;
     after each pass the cumulative device time and the MSE (computed outside
     the timed region) are logged until the guided image is at least as good
-    as the plain one or twice the plain time has passed."""
+    as the plain one or twice the plain time has passed.  The time to the
+    plain MSE is the end of the first pass at or below it; the key
+    ``guided_ms_to_plain_mse_interp`` also gives the crossing interpolated
+    between that pass and the one before, with the error taken as
+    proportional to 1 / time between them."""
     import torch
     from bajo_b200 import guide, rt, scenes
     stream = torch.cuda.current_stream()
@@ -1122,6 +1129,7 @@ def run_guided(args):
     gr = guide.GuidedRenderer(gsc, sc.camera, w, h, spp_per_pass=args.spp_per_pass, record_capacity=args.records,
                               batch=1 << 14, steps=args.train_steps, lr=1e-2)
     gr.render_pass(1, train=False)  # warm-up: kernel attributes, tuning table
+    gr.prepare_pass(args.late_spp)  # the later passes' workspace, allocated before the clock starts
     torch.cuda.synchronize()
     gr.reset_image()
     gr.net = guide.GuideNetwork("cuda", seed=0)
@@ -1130,7 +1138,8 @@ def run_guided(args):
     while t_g < 2.0 * t_plain and k < 4096:
         train = k < args.train_passes
         frac = 0.0 if (k == 0 and not args.first_guided) else None  # the untrained network guides nothing
-        t, _ = ev_time(lambda: gr.render_pass(70001 + 7919 * k, train=train, guide_fraction=frac))
+        spp_k = args.spp_per_pass if train else args.late_spp
+        t, _ = ev_time(lambda: gr.render_pass(70001 + 7919 * k, train=train, guide_fraction=frac, spp=spp_k))
         t_g += t
         k += 1
         mse = float(((gr.image() - ref) ** 2).mean())
@@ -1138,22 +1147,32 @@ def run_guided(args):
         if reached is None and mse <= mse_plain:
             reached = t_g
             break
+    # crossing interpolated between the last pass above the plain MSE and the
+    # first at or below it, with MSE ~ 1 / time between the two
+    interp = None
+    if reached is not None and len(log) >= 2:
+        (t0, _, m0), (t1, _, m1) = log[-2], log[-1]
+        if m0 > mse_plain >= m1 > 0.0 and t1 > t0:
+            interp = t0 + (t1 - t0) * (1.0 / mse_plain - 1.0 / m0) / (1.0 / m1 - 1.0 / m0)
     # MSE at equal time: last logged point not past t_plain
     eq = [m for (t, _, m) in log if t <= t_plain]
     # guided throughput with a trained network and no training
-    t_pass, _ = ev_time(lambda: gr.render_pass(5, train=False))
-    samples = w * h * args.spp_per_pass
+    t_pass, _ = ev_time(lambda: gr.render_pass(5, train=False, spp=args.late_spp))
+    samples = w * h * args.late_spp
     rays, shadows = gr.workspace.ray_counts()
     out = {"case": "guided", "scene": args.scene, "width": w, "height": h, "ref_spp": args.ref_spp,
            "ref_ms": round(t_ref, 1), "plain_ms": round(t_plain, 2), "plain_mse": mse_plain,
            "guided_ms_to_plain_mse": None if reached is None else round(reached, 2),
            "time_ratio": None if reached is None else round(reached / t_plain, 3),
+           "guided_ms_to_plain_mse_interp": None if interp is None else round(interp, 2),
+           "time_ratio_interp": None if interp is None else round(interp / t_plain, 3),
            "guided_mse_at_plain_time": eq[-1] if eq else None,
            "guided_spp_at_plain_time": max([s for (t, s, _) in log if t <= t_plain], default=0),
            "guided_samples_s": round(samples / t_pass * 1e3, 1),
            "plain_samples_s": round(w * h * 64 / t_plain * 1e3, 1),
            "guided_mrays_s": round((rays + shadows) / t_pass / 1e3, 1),
-           "train_passes": args.train_passes, "spp_per_pass": args.spp_per_pass, "train_steps": args.train_steps,
+           "train_passes": args.train_passes, "spp_per_pass": args.spp_per_pass, "late_spp": args.late_spp,
+           "train_steps": args.train_steps,
            "records_per_pass": args.records,
            "first_pass_guided": bool(args.first_guided),
            "log": log[:: max(1, len(log) // 40)], "status": gr.workspace.status()}
