@@ -93,3 +93,35 @@ def test_camera_records_match_oracle(lib, oracle):
     a = camera.camera([1.0, 2.0, -3.0], [0.2, 0.1, 0.7], [0.0, 1.0, 0.0], 0.75)
     b = oracle.camera_make([1.0, 2.0, -3.0], [0.2, 0.1, 0.7], [0.0, 1.0, 0.0], 0.75)
     assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_tuning_cache_round_trip(lib, monkeypatch, tmp_path):
+    """autotune.save / load carry the closest-hit block and stack choices
+    and the bounce kernels' block sizes through the JSON cache into the
+    library's tables (host-side setters; no device work)."""
+    from bajo_b200 import autotune
+    monkeypatch.setattr(autotune, "device_key", lambda: "TEST GPU|1")
+    path = str(tmp_path / "cache.json")
+    results = {"trace_camera": {20: {"best": 256, "stack": 24, "ms": {}}},
+               "trace_rays": {18: {"best": 64, "stack": 12, "ms": {}}},
+               "render_trace": {0: {"best": 64, "ms": {}}},
+               "render_shadow": {0: {"best": 256, "ms": {}}}}
+    got = ctypes.c_int32(0)
+    try:
+        autotune.save(results, path)
+        assert autotune.load(path) == 6
+        assert lib.bajo_trace_tuning_get(0, 1 << 20, ctypes.byref(got)) == _lib.OK and got.value == 256
+        assert lib.bajo_trace_stack_tuning_get(0, 1 << 20, ctypes.byref(got)) == _lib.OK and got.value == 24
+        assert lib.bajo_trace_tuning_get(1, 1 << 18, ctypes.byref(got)) == _lib.OK and got.value == 64
+        assert lib.bajo_trace_stack_tuning_get(1, 1 << 18, ctypes.byref(got)) == _lib.OK and got.value == 12
+        assert lib.bajo_trace_stack_tuning_get(1, 1 << 20, ctypes.byref(got)) == _lib.OK and got.value == 64
+        assert lib.bajo_render_tuning_get(0, ctypes.byref(got)) == _lib.OK and got.value == 64
+        assert lib.bajo_render_tuning_get(1, ctypes.byref(got)) == _lib.OK and got.value == 128
+        assert lib.bajo_render_tuning_get(2, ctypes.byref(got)) == _lib.OK and got.value == 256
+    finally:
+        for kind in (0, 1):
+            for lg in range(33):
+                lib.bajo_trace_tuning_set(kind, lg, 0)
+                lib.bajo_trace_stack_tuning_set(kind, lg, 0)
+        for kind in range(3):
+            lib.bajo_render_tuning_set(kind, 0)

@@ -168,7 +168,7 @@ def test_tuner_runs_and_keeps_results(oracle):
     L = _lib.load()
     try:
         res = autotune.tune_trace("trace_camera", [16], reps=2)
-        assert res[16]["best"] in (64, 128, 256)
+        assert res[16]["best"] in (64, 128, 256) and res[16]["stack"] in (64, 24, 12)
         fe = autotune.tune_one_launch(range(15, 17), reps=2)
         assert set(v["best"] for v in fe.values()) <= {0, 1 << 15, 1 << 16}
         v = scenes.random_triangles(1 << 16, seed=9)
@@ -186,6 +186,7 @@ def test_tuner_runs_and_keeps_results(oracle):
     finally:
         for lg in range(33):
             L.bajo_trace_tuning_set(0, lg, 0)
+            L.bajo_trace_stack_tuning_set(0, lg, 0)
         L.bajo_lbvh_fused_max_set(_lib.FUSED_MAX_LEAVES)
 
 
