@@ -40,6 +40,24 @@ def test_fraction_zero_is_the_mis_tracer(indirect):
         assert gr.records.count() > 0
 
 
+def test_passes_of_different_sizes_accumulate_samples(indirect):
+    """A 2-spp pass then a 4-spp pass (its own workspace) at guide fraction
+    0: the FP64 sum is the two MIS renders' sample sums and the image their
+    6-sample mean."""
+    s, gs = indirect
+    cam = s.camera
+    _, sum2 = _mis(gs, cam, 2, 11)
+    _, sum4 = _mis(gs, cam, 4, 12)
+    gr = guide.GuidedRenderer(gs, cam, W, H, guide_fraction=0.0, spp_per_pass=2)
+    gr.prepare_pass(4)
+    gr.render_pass(11, train=False, guide_fraction=0.0)
+    gr.render_pass(12, train=False, guide_fraction=0.0, spp=4)
+    torch.cuda.synchronize()
+    assert gr.samples == 6 and gr.workspace.status() == 0
+    assert torch.equal(gr.sum64, sum2 + sum4)
+    assert torch.equal(gr.image(), (sum2 + sum4) / 6)
+
+
 def test_records_are_well_formed(indirect):
     s, gs = indirect
     gr = guide.GuidedRenderer(gs, s.camera, W, H, record_capacity=1 << 14, spp_per_pass=4)
