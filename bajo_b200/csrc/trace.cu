@@ -123,6 +123,29 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   }
 }
 
+// Unstaged camera launches give each warp an 8 x 4 tile of pixels (tiles in
+// rows, views one after another), so that a warp's rays leave the camera
+// side by side instead of along one image row; ray i is still pixel i of the
+// row-major image, so the hits do not depend on it.  False for lanes past
+// the image or past n.
+constexpr uint32_t kTileW = 8, kTileH = 4;
+__host__ __device__ __forceinline__ uint64_t camera_tiles(uint32_t width, uint32_t height) {
+  return (uint64_t)((width + kTileW - 1) / kTileW) * ((height + kTileH - 1) / kTileH);
+}
+__device__ __forceinline__ bool tile_ray(uint64_t g, uint32_t n, uint32_t width, uint32_t height, uint32_t& i) {
+  const uint32_t tiles_x = (width + kTileW - 1) / kTileW;
+  const uint64_t per_view = camera_tiles(width, height);
+  const uint64_t warp = g >> 5, view = warp / per_view, tv = warp - view * per_view;
+  const uint32_t lane = (uint32_t)(g & 31u);
+  const uint32_t px = (uint32_t)(tv % tiles_x) * kTileW + lane % kTileW;
+  const uint32_t py = (uint32_t)(tv / tiles_x) * kTileH + lane / kTileW;
+  if (px >= width || py >= height) return false;
+  const uint64_t at = view * ((uint64_t)width * height) + (uint64_t)py * width + px;
+  if (at >= n) return false;
+  i = (uint32_t)at;
+  return true;
+}
+
 template <int MODE, bool STATS, bool TOP, int BLK = kTraceBlock, int STACK = kStack>
 __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0)
     trace_camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t n_nodes, uint32_t width, uint32_t height,
@@ -140,9 +163,11 @@ __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0
       camera_ray<MODE, STATS, TOP>(i, cams, n_nodes, width, height, inv_h, root, nb, meta, tris, top, hits8, out_t,
                                    out_prim, status, stats);
     stage_top_drain(sm, top);
-  } else if (i0 < n) {
-    camera_ray<MODE, STATS, TOP, STACK>(i0, cams, n_nodes, width, height, inv_h, __ldg(roots), nb, meta, tris,
-                                        nullptr, hits8, out_t, out_prim, status, stats);
+  } else {
+    uint32_t i;
+    if (tile_ray((uint64_t)blockIdx.x * blockDim.x + threadIdx.x, n, width, height, i))
+      camera_ray<MODE, STATS, TOP, STACK>(i, cams, n_nodes, width, height, inv_h, __ldg(roots), nb, meta, tris,
+                                          nullptr, hits8, out_t, out_prim, status, stats);
   }
 }
 
@@ -301,7 +326,10 @@ void launch_camera_blk(const BajoLbvh* b, const float* cams, uint32_t n, uint32_
   const float4* tris = reinterpret_cast<const float4*>(b->leaf_tris);
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
   const float inv_h = 1.0f / (float)height;
-  const uint32_t grid = TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (n + BLK - 1) / BLK;
+  // unstaged: 32 threads per 8 x 4 tile of every view
+  const uint64_t ppv = (uint64_t)width * height, views = (n + ppv - 1) / ppv;
+  const uint64_t threads = views * camera_tiles(width, height) * 32u;
+  const uint32_t grid = TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (uint32_t)((threads + BLK - 1) / BLK);
   trace_camera_kernel<MODE, STATS, TOP, BLK, STACK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
       cams, n, b->n_leaves, width, height, inv_h, b->roots, nb, meta, tris, top, hits8, t, prim, status, stats);
 }
