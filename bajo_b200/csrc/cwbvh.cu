@@ -67,8 +67,8 @@ __global__ void __launch_bounds__(kBlock) camera_kernel(const float* __restrict_
                                                         float* __restrict__ hits8, float* __restrict__ out_t,
                                                         uint32_t* __restrict__ out_prim,
                                                         uint32_t* __restrict__ status) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
+  uint32_t i;  // every warp an 8 x 4 pixel tile (trav::tile_ray)
+  if (!trav::tile_ray((uint64_t)blockIdx.x * kBlock + threadIdx.x, n, width, height, i)) return;
   const uint32_t ppv = width * height;
   const uint32_t view = i / ppv, local = i - view * ppv;
   const float* c = cams + (size_t)view * 20;
@@ -124,7 +124,7 @@ int32_t bajo_trace_cwbvh8_camera(const BajoCwbvh8* c, uint32_t n_nodes, const fl
     return BAJO_ERR_INVALID_ARGUMENT;
   if (n == 0) return BAJO_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  const uint32_t grid = (n + kBlock - 1) / kBlock;
+  const uint32_t grid = (uint32_t)((bajo::trav::camera_threads(n, width, height) + kBlock - 1) / kBlock);
   const float inv_h = 1.0f / (float)height;
   if (any_hit)
     camera_kernel<true><<<grid, kBlock, 0, st>>>(d_cameras, n, width, height, inv_h, tr, d_hits8, d_t, d_prim,

@@ -123,29 +123,6 @@ __device__ __forceinline__ void camera_ray(uint32_t i, const float* __restrict__
   }
 }
 
-// Unstaged camera launches give each warp an 8 x 4 tile of pixels (tiles in
-// rows, views one after another), so that a warp's rays leave the camera
-// side by side instead of along one image row; ray i is still pixel i of the
-// row-major image, so the hits do not depend on it.  False for lanes past
-// the image or past n.
-constexpr uint32_t kTileW = 8, kTileH = 4;
-__host__ __device__ __forceinline__ uint64_t camera_tiles(uint32_t width, uint32_t height) {
-  return (uint64_t)((width + kTileW - 1) / kTileW) * ((height + kTileH - 1) / kTileH);
-}
-__device__ __forceinline__ bool tile_ray(uint64_t g, uint32_t n, uint32_t width, uint32_t height, uint32_t& i) {
-  const uint32_t tiles_x = (width + kTileW - 1) / kTileW;
-  const uint64_t per_view = camera_tiles(width, height);
-  const uint64_t warp = g >> 5, view = warp / per_view, tv = warp - view * per_view;
-  const uint32_t lane = (uint32_t)(g & 31u);
-  const uint32_t px = (uint32_t)(tv % tiles_x) * kTileW + lane % kTileW;
-  const uint32_t py = (uint32_t)(tv / tiles_x) * kTileH + lane / kTileW;
-  if (px >= width || py >= height) return false;
-  const uint64_t at = view * ((uint64_t)width * height) + (uint64_t)py * width + px;
-  if (at >= n) return false;
-  i = (uint32_t)at;
-  return true;
-}
-
 template <int MODE, bool STATS, bool TOP, int BLK = kTraceBlock, int STACK = kStack>
 __global__ void __launch_bounds__(TOP ? kTopBlock : BLK, TOP ? kTopMinBlocks : 0)
     trace_camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t n_nodes, uint32_t width, uint32_t height,
@@ -184,7 +161,12 @@ __global__ void __launch_bounds__(kTraceBlock) batch_trace_kernel(
     const uint4* __restrict__ meta, const float4* __restrict__ tris, uint64_t seed, float* __restrict__ t0,
     uint32_t* __restrict__ p0, float* __restrict__ t1, uint32_t* __restrict__ p1, uint32_t* __restrict__ status) {
   const uint32_t ppv = width * height;
-  for (uint32_t i = blockIdx.x * kTraceBlock + threadIdx.x; i < n; i += gridDim.x * kTraceBlock) {
+  // every warp an 8 x 4 pixel tile of one scene's image (tile_ray)
+  const uint64_t threads = camera_threads(n, width, height);
+  for (uint64_t g = (uint64_t)blockIdx.x * kTraceBlock + threadIdx.x; g < threads;
+       g += (uint64_t)gridDim.x * kTraceBlock) {
+    uint32_t i;
+    if (!tile_ray(g, n, width, height, i)) continue;
     const uint32_t view = i / ppv, local = i - view * ppv;
     const float* c = cams + (size_t)view * cam_stride;
     const uint32_t px = local % width, py = local / width;
@@ -327,8 +309,7 @@ void launch_camera_blk(const BajoLbvh* b, const float* cams, uint32_t n, uint32_
   const float4* top = reinterpret_cast<const float4*>(b->top_nodes);
   const float inv_h = 1.0f / (float)height;
   // unstaged: 32 threads per 8 x 4 tile of every view
-  const uint64_t ppv = (uint64_t)width * height, views = (n + ppv - 1) / ppv;
-  const uint64_t threads = views * camera_tiles(width, height) * 32u;
+  const uint64_t threads = camera_threads(n, width, height);
   const uint32_t grid = TOP ? top_grid(trace_camera_kernel<MODE, STATS, TOP>, n) : (uint32_t)((threads + BLK - 1) / BLK);
   trace_camera_kernel<MODE, STATS, TOP, BLK, STACK><<<grid, TOP ? kTopBlock : BLK, 0, st>>>(
       cams, n, b->n_leaves, width, height, inv_h, b->roots, nb, meta, tris, top, hits8, t, prim, status, stats);
@@ -466,9 +447,10 @@ int32_t bajo_trace_batch(const BajoLbvh* bvh, const float* d_cams, uint32_t cam_
   if (n64 > 0xFFFFFFFFull) return BAJO_ERR_TOO_LARGE;
   const uint32_t n = (uint32_t)n64;
   if (n == 0) return BAJO_OK;
-  uint32_t grid = (n + kTraceBlock - 1) / kTraceBlock;
-  const uint32_t cap = (uint32_t)sm_count() * 32;
-  if (grid > cap) grid = cap;
+  const uint64_t threads = camera_threads(n, width, height);
+  uint64_t grid64 = (threads + kTraceBlock - 1) / kTraceBlock;
+  const uint64_t cap = (uint64_t)sm_count() * 32;
+  const uint32_t grid = (uint32_t)(grid64 > cap ? cap : grid64);
   const float inv_h = 1.0f / (float)height;
   const float4* nb = reinterpret_cast<const float4*>(bvh->node_bounds);
   const uint4* meta = reinterpret_cast<const uint4*>(bvh->node_meta);

@@ -261,6 +261,35 @@ __device__ __forceinline__ void stage_top_drain(TopSmem& sm, const float4* stage
   if (staged == nullptr && threadIdx.x == 0) mbar_wait_bounded(smem_addr(&sm.bar), 0);
 }
 
+// Camera launches give each warp an 8 x 4 tile of pixels (tiles in rows,
+// views one after another), so that a warp's rays leave the camera side by
+// side instead of along one image row (1024^2 camera rays over the 65,536
+// triangle workload: 0.316 against 0.349 ms).  Ray i is still pixel i of the
+// row-major image, so the results do not depend on it.  tile_ray maps the
+// launch's thread g to its ray i; false for lanes past the image or past n.
+// A launch needs camera_threads(...) threads (whole warps of every view).
+constexpr uint32_t kTileW = 8, kTileH = 4;
+__host__ __device__ __forceinline__ uint64_t camera_tiles(uint32_t width, uint32_t height) {
+  return (uint64_t)((width + kTileW - 1) / kTileW) * ((height + kTileH - 1) / kTileH);
+}
+__device__ __forceinline__ bool tile_ray(uint64_t g, uint32_t n, uint32_t width, uint32_t height, uint32_t& i) {
+  const uint32_t tiles_x = (width + kTileW - 1) / kTileW;
+  const uint64_t per_view = camera_tiles(width, height);
+  const uint64_t warp = g >> 5, view = warp / per_view, tv = warp - view * per_view;
+  const uint32_t lane = (uint32_t)(g & 31u);
+  const uint32_t px = (uint32_t)(tv % tiles_x) * kTileW + lane % kTileW;
+  const uint32_t py = (uint32_t)(tv / tiles_x) * kTileH + lane / kTileW;
+  if (px >= width || py >= height) return false;
+  const uint64_t at = view * ((uint64_t)width * height) + (uint64_t)py * width + px;
+  if (at >= n) return false;
+  i = (uint32_t)at;
+  return true;
+}
+__host__ __device__ __forceinline__ uint64_t camera_threads(uint32_t n, uint32_t width, uint32_t height) {
+  const uint64_t ppv = (uint64_t)width * height;
+  return ppv ? (n + ppv - 1) / ppv * camera_tiles(width, height) * 32u : 0u;
+}
+
 // A traversal with a stack shallower than kStack that runs out of entries
 // returns this in Hit::leaf; trace_bvh2 then traces the ray again with the
 // full stack, so every stack depth gives the same hit.

@@ -666,8 +666,8 @@ __global__ void __launch_bounds__(trav::kTraceBlock) wide_camera_kernel(
     const float* __restrict__ cams, uint32_t n, uint32_t width, uint32_t height, float inv_h, View v,
     float* __restrict__ hits8, float* __restrict__ out_t, uint32_t* __restrict__ out_prim,
     uint32_t* __restrict__ status, uint32_t* __restrict__ stats) {
-  const uint32_t i = blockIdx.x * trav::kTraceBlock + threadIdx.x;
-  if (i >= n) return;
+  uint32_t i;  // every warp an 8 x 4 pixel tile (trav::tile_ray)
+  if (!trav::tile_ray((uint64_t)blockIdx.x * trav::kTraceBlock + threadIdx.x, n, width, height, i)) return;
   const uint32_t ppv = width * height;
   const uint32_t view = i / ppv, local = i - view * ppv;
   const float* c = cams + (size_t)view * 20;
@@ -794,8 +794,9 @@ cudaError_t launch_rays(const View& v, const float* rays, uint32_t n, float* hit
 template <int W, int MODE, bool STATS>
 cudaError_t launch_camera(const View& v, const float* cams, uint32_t n, uint32_t w, uint32_t h, float* hits8,
                           float* t, uint32_t* prim, uint32_t* status, uint32_t* stats, cudaStream_t st) {
-  wide_camera_kernel<W, MODE, STATS><<<(n + trav::kTraceBlock - 1) / trav::kTraceBlock, trav::kTraceBlock, 0, st>>>(
-      cams, n, w, h, 1.0f / (float)h, v, hits8, t, prim, status, stats);
+  const uint32_t grid = (uint32_t)((trav::camera_threads(n, w, h) + trav::kTraceBlock - 1) / trav::kTraceBlock);
+  wide_camera_kernel<W, MODE, STATS><<<grid, trav::kTraceBlock, 0, st>>>(cams, n, w, h, 1.0f / (float)h, v, hits8, t,
+                                                                        prim, status, stats);
   return cudaGetLastError();
 }
 
