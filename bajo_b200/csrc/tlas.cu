@@ -220,8 +220,8 @@ template <int MODE, bool ANY>
 __global__ void __launch_bounds__(kBlock) camera_kernel(const float* __restrict__ cams, uint32_t n, uint32_t width,
                                                         uint32_t height, float inv_h, Top top, Blas bl,
                                                         float* __restrict__ hits8, uint32_t* __restrict__ status) {
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i >= n) return;
+  uint32_t i;  // every warp an 8 x 4 pixel tile (trav::tile_ray)
+  if (!trav::tile_ray((uint64_t)blockIdx.x * kBlock + threadIdx.x, n, width, height, i)) return;
   const uint32_t ppv = width * height;
   const uint32_t view = i / ppv, local = i - view * ppv;
   const float* c = cams + (size_t)view * 20;
@@ -352,7 +352,7 @@ int32_t bajo_trace_tlas_camera(const BajoLbvh* tlas, const BajoLbvh* blas_set, c
     return BAJO_ERR_INVALID_ARGUMENT;
   if (n_rays == 0) return BAJO_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  const uint32_t grid = (n_rays + kBlock - 1) / kBlock;
+  const uint32_t grid = (uint32_t)((bajo::trav::camera_threads(n_rays, width, height) + kBlock - 1) / kBlock);
   const float inv_h = 1.0f / (float)height;
   const bool mt = tri_mode == BAJO_TRI_MT;
 #define BAJO_TLAS_CAM(MM, AA) \
