@@ -223,3 +223,23 @@ def test_invalid_arguments():
     t = tree.c_struct()
     assert L.bajo_cwbvh8_build(ctypes.byref(t), ctypes.byref(c), cw.workspace.data_ptr(), 16, None) == \
         _lib.ERR_WORKSPACE_TOO_SMALL
+
+
+@pytest.mark.parametrize("w,h,short", [(37, 23, 5), (1, 1, 0), (129, 2, 77)])
+def test_camera_tiles_at_image_edges(oracle, w, h, short):
+    """8 x 4 pixel tiles per warp at image sizes that are not whole tiles and
+    with a last view cut short: the oracle's CWBVH8 walk, ray by ray."""
+    v = scenes.random_triangles(3000, seed=32, spread=0.04)
+    _, cw = gpu_cw(v)
+    cams = np.stack([camera.plain_lbvh_camera(),
+                     camera.camera([1.6, 0.4, -1.2], [0.5, 0.5, 0.5], [0, 1, 0], 0.8)]).astype(np.float32)
+    n = 2 * w * h - short
+    hits = torch.full((8 * n + 8,), -7.0, dtype=torch.float32, device="cuda")
+    st = cw.launch_camera(dev(cams.reshape(-1)), hits, n, w, h, False)
+    torch.cuda.synchronize()
+    assert int(st.item()) == 0
+    rays = oracle.camera_rays(cams.reshape(-1), n, w, h)
+    ref = oracle.trace_cwbvh8(oracle.cwbvh8_build(oracle.lbvh_build(v)), rays, False)
+    got = hits.cpu().numpy()
+    assert np.array_equal(got[:8 * n].view(np.uint32), ref.view(np.uint32))
+    assert np.all(got[8 * n:] == -7.0)

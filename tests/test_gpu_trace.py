@@ -178,3 +178,31 @@ def test_three_camera_views_match_oracle(oracle, mode):
     assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
     per_view = (oracle.hits_prim(got).reshape(3, -1) != oracle.EMPTY).mean(axis=1)
     assert np.all(per_view > 0.02)  # every view sees geometry
+
+
+@pytest.mark.parametrize("w,h,short", [(37, 23, 5), (9, 4, 0), (1, 1, 0), (8, 5, 3), (129, 2, 77)])
+def test_camera_tiles_at_image_edges(oracle, w, h, short):
+    """The camera kernels give each warp an 8 x 4 pixel tile; images that are
+    not whole tiles, a 1 x 1 image and a last view cut short (n three views
+    minus `short` rays) still trace exactly ray i = pixel i, with hits and
+    traversal counters equal to the oracle's."""
+    from bajo_b200 import bvh as _bvh, camera
+    v = scenes.random_triangles(3000, seed=31, spread=0.04)
+    b = build(v)
+    cams = np.concatenate([
+        camera.camera_from_vfov([0.5, 0.5, -1.5], [0.5, 0.5, 0.5], [0.0, 1.0, 0.0], 60.0),
+        camera.camera_from_vfov([2.0, 0.7, 0.5], [0.5, 0.5, 0.5], [0.0, 1.0, 0.0], 45.0),
+        camera.camera_from_vfov([0.4, 2.5, 0.6], [0.5, 0.5, 0.5], [0.0, 0.0, 1.0], 75.0),
+    ]).astype(np.float32)
+    n = 3 * w * h - short
+    hits = torch.full((8 * n + 8,), -7.0, dtype=torch.float32, device="cuda")  # one guard record past n
+    b.launch_camera(dev(cams), hits, n, w, h)
+    stats = torch.zeros(_bvh.STATS_WORDS * n, dtype=torch.int32, device="cuda")
+    b.launch_camera_instrumented(dev(cams), None, stats, n, w, h)
+    torch.cuda.synchronize()
+    ob = oracle.lbvh_build(v)
+    rays = oracle.camera_rays(cams, n, w, h)
+    got = hits.cpu().numpy()
+    assert np.array_equal(got[:8 * n].view(np.uint32), oracle.trace_bvh2(ob, rays).view(np.uint32))
+    assert np.all(got[8 * n:] == -7.0)  # nothing written past ray n - 1
+    assert np.array_equal(stats.cpu().numpy().view(np.uint32), oracle.trace_bvh2_stats(ob, rays))
