@@ -179,14 +179,28 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 // Camera.make_ray_sampled, camera.mojo:156-209; random_in_unit_disk,
 // bajo/core/random.mojo:56)
 // ---------------------------------------------------------------------------
+// With tile_w > 0 (a chunk of whole rows of tile_w x tile_h tiles, spp
+// dividing 32), queue slot idx holds the samples of an 8 x 4, 4 x 4, 4 x 2 or
+// 2 x 2 pixel tile per warp instead of 32 consecutive samples of one row, so
+// that a warp's rays leave the camera side by side.  A path's id, and with it
+// its random numbers and radiance slot, stays its sample index: the image
+// does not depend on the order.
 __global__ void __launch_bounds__(kBlock) primary_kernel(const float* __restrict__ cam, Queues q, uint32_t count,
                                                          uint32_t sample_base, uint32_t width, uint32_t height,
-                                                         uint32_t spp, uint64_t seed) {
+                                                         uint32_t spp, uint64_t seed, uint32_t tile_w,
+                                                         uint32_t tile_h) {
   const uint32_t idx = blockIdx.x * kBlock + threadIdx.x;
   if (idx == 0) q.counters[0] = count;
   if (idx >= count) return;
   const uint32_t cap = q.capacity;
-  const uint32_t path_id = sample_base + idx;
+  uint32_t local = idx;  // sample index within the chunk
+  if (tile_w) {
+    const uint32_t warp = idx >> 5, lane = idx & 31u, p = lane / spp, smp_k = lane - p * spp;
+    const uint32_t tiles_x = width / tile_w;
+    const uint32_t px = (warp % tiles_x) * tile_w + p % tile_w, py = (warp / tiles_x) * tile_h + p / tile_w;
+    local = (py * width + px) * spp + smp_k;
+  }
+  const uint32_t path_id = sample_base + local;
   const uint32_t pixel = path_id / spp;
   const uint32_t px = pixel % width, py = pixel / width;
   const float4 r = uniform4(seed, path_id, 0);
@@ -211,9 +225,9 @@ __global__ void __launch_bounds__(kBlock) primary_kernel(const float* __restrict
   f[0 * cap + idx] = ro.x; f[1 * cap + idx] = ro.y; f[2 * cap + idx] = ro.z; f[3 * cap + idx] = 0.001f;
   f[4 * cap + idx] = d.x; f[5 * cap + idx] = d.y; f[6 * cap + idx] = d.z; f[7 * cap + idx] = FLT_MAX;
   f[8 * cap + idx] = 1.0f; f[9 * cap + idx] = 1.0f; f[10 * cap + idx] = 1.0f; f[11 * cap + idx] = 0.0f;
-  q.radiance[0 * cap + idx] = 0.0f;
-  q.radiance[1 * cap + idx] = 0.0f;
-  q.radiance[2 * cap + idx] = 0.0f;
+  q.radiance[0 * cap + local] = 0.0f;
+  q.radiance[1 * cap + local] = 0.0f;
+  q.radiance[2 * cap + local] = 0.0f;
   if (q.rec[0]) q.rec[0][idx] = kNoRecord;
 }
 
@@ -1062,8 +1076,19 @@ cudaError_t render_chunks(const BajoRenderSettings* s, const Layout& L, const Qu
     const uint32_t sample_base = pb * s->spp;
     if ((e = cudaMemsetAsync(q.counters, 0, (size_t)L.n_counters * 4, st)) != cudaSuccess) return e;
     if ((e = before()) != cudaSuccess) return e;
+    // tiles when spp divides 32 (8 or fewer) and the chunk is whole rows of whole tiles
+    uint32_t tw = 0, th = 0;
+    switch (s->spp) {
+      case 1: tw = 8; th = 4; break;
+      case 2: tw = 4; th = 4; break;
+      case 4: tw = 4; th = 2; break;
+      case 8: tw = 2; th = 2; break;
+      default: break;
+    }
+    if (tw && (pb % s->width != 0 || pc % s->width != 0 || s->width % tw != 0 || (pc / s->width) % th != 0))
+      tw = th = 0;
     primary_kernel<<<(count + kBlock - 1) / kBlock, kBlock, 0, st>>>(d_camera, q, count, sample_base, s->width,
-                                                                    s->height, s->spp, s->seed);
+                                                                    s->height, s->spp, s->seed, tw, th);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     for (uint32_t bnc = 0; bnc < s->max_depth; ++bnc)
       if ((e = bounce(bnc, sample_base)) != cudaSuccess) return e;

@@ -104,3 +104,22 @@ def test_guided_render_runs_with_materials(materials):
     gr = guide.GuidedRenderer(gsc, sc.camera, 32, 20, max_depth=8, record_capacity=1 << 14, steps=2, batch=1 << 10)
     img = gr.render(passes=3, train_passes=2).cpu().numpy()
     assert gr.workspace.status() == 0 and np.all(np.isfinite(img)) and img.mean() > 0.05
+
+
+@pytest.mark.parametrize("spp,chunk_rows", [(1, 0), (2, 0), (4, 0), (8, 0), (2, 8), (4, 4)])
+def test_tiled_primary_rays_match_oracle(oracle, small, spp, chunk_rows):
+    """At 1, 2, 4 or 8 samples per pixel, with chunks of whole tile rows,
+    the primary rays are queued by pixel tiles (a warp's samples cover a 2-D
+    block of pixels); the image stays the oracle's bit for bit, also when
+    the image is rendered in chunks of `chunk_rows` rows."""
+    from bajo_b200 import rt
+    sc, gsc = small
+    w, h = 64, 32
+    chunk = chunk_rows * w * spp
+    settings = rt.RenderSettings(w, h, spp, rng_seed=77, max_depth=6, chunk_paths=chunk)
+    ws = rt.RenderWorkspace(settings, rt.MIS)
+    img = rt.render_gpu_triangles(settings, sc.camera, gsc, rt.MIS, workspace=ws)
+    torch.cuda.synchronize()
+    assert ws.status() == 0
+    ref = oracle.render(sc, sc.camera, w, h, spp, max_depth=6, seed=77, algorithm=rt.MIS)
+    assert np.array_equal(img.cpu().numpy().view(np.uint32), ref.view(np.uint32))
